@@ -1,0 +1,286 @@
+/*
+ * luce_render_b200 — the C ABI of a B200-native (sm_100a) implementation of
+ * luce-render's wavefront path-tracing hot path.
+ *
+ * Every entry point mirrors one of luce-render's `render` package API for this path
+ * (package.prisma:13, public = ["render"]); each declaration cites the reference
+ * interface it replaces. Conventions:
+ *   - Status codes: 0 success; 400 invalid input, 401 past a limit, 402 stopped
+ *     (src/render/module.lucb:60-63); 500 a CUDA call failed; 504 a bounded device
+ *     wait gave up. The message of the last failing call on this thread is
+ *     lr_last_error().
+ *   - Handles are opaque. One host thread drives a context and the objects made on
+ *     it (the reference's rule: device calls from the main thread, device.lucb:12).
+ *   - Plain pointers and sizes only; "device" in a name means CUDA device memory.
+ */
+#ifndef LUCE_RENDER_B200_H
+#define LUCE_RENDER_B200_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* Every declaration below is exported from the shared library. */
+#if defined(__GNUC__)
+#pragma GCC visibility push(default)
+#endif
+
+#define LR_OK 0
+#define LR_INVALID 400 /* render.invalid (src/render/module.lucb:60) */
+#define LR_LIMIT 401   /* render.limit (module.lucb:61) */
+#define LR_STOPPED 402 /* render.stopped (module.lucb:63) */
+#define LR_DEVICE 500  /* a CUDA runtime call failed */
+#define LR_TIMEOUT 504 /* a device-side bounded wait gave up */
+
+/* The message of the last failing call on this thread ("" when none). */
+const char *lr_last_error(void);
+/* The library version string. */
+const char *lr_version(void);
+
+/* ---- Context: one device and one stream (replaces luce-gpu's gpu.Device) --------- */
+
+typedef struct lr_context lr_context;
+
+/* gpu.Device.open (used at tests/gpu/main.lucb:18): a context on CUDA device `device`. */
+int lr_context_create(int device, lr_context **out);
+void lr_context_destroy(lr_context *ctx);
+/* Wait for all work queued on the context's stream. */
+int lr_context_synchronize(lr_context *ctx);
+/* The context's CUDA stream (a cudaStream_t), for callers that order their own work. */
+void *lr_context_stream(lr_context *ctx);
+
+/* Device memory for callers without an allocator of their own (tests, benches). */
+int lr_device_alloc(lr_context *ctx, size_t bytes, void **out);
+int lr_device_free(lr_context *ctx, void *ptr);
+int lr_memcpy_htod(lr_context *ctx, void *dst, const void *src, size_t bytes);
+int lr_memcpy_dtoh(lr_context *ctx, void *dst, const void *src, size_t bytes);
+int lr_memset_device(lr_context *ctx, void *dst, int value, size_t bytes);
+int lr_host_alloc_pinned(size_t bytes, void **out);
+int lr_host_free_pinned(void *ptr);
+/* CUDA-event timing on the context's stream: lr_timer_stop synchronizes and gives
+ * the milliseconds since lr_timer_start. */
+int lr_timer_start(lr_context *ctx);
+int lr_timer_stop(lr_context *ctx, float *ms);
+
+/* ---- Scene compile (src/render/scene.lucb:31-129, bvh.lucb:66-217) --------------- */
+
+/* One mesh: the flat-array stand-in for a luce-geocore Mesh component placed in a
+ * GeometrySet (scene.lucb:246-295). */
+typedef struct {
+    const float *positions;          /* xyz per point, in the mesh's space */
+    uint64_t point_count;
+    const uint32_t *indices;         /* 3 point indices per triangle (counter-clockwise) */
+    uint64_t triangle_count;
+    const uint32_t *triangle_faces;  /* the polygon of each triangle (NULL: its own index) */
+    uint32_t face_count;             /* polygons in the mesh (0: triangle_count) */
+    const float *normals;            /* shading normals xyz (NULL: each triangle's flat normal) */
+    int32_t normals_per_corner;      /* 0: one normal per point; 1: three per triangle */
+    const uint32_t *face_materials;  /* per polygon: 0 the default, k the library's k-th (NULL: 0) */
+    double transform[12];            /* columns x, y, z, translation; all zeros: identity */
+} lr_mesh;
+
+/* A camera scene object (luce-geocore Camera as ray_frame reads it, camera.lucb:57-76). */
+typedef struct {
+    double matrix[12];        /* columns x (right), y (up), z (back), translation */
+    int32_t projection;       /* 0 perspective, 1 orthographic */
+    double focal_length;      /* mm */
+    double horizontal_aperture; /* mm (orthographic: tenths of a scene unit) */
+    double f_stop;            /* 0: a pinhole */
+    double focus_distance;
+} lr_camera;
+
+/* A UsdLux light (lights.lucb:29-131). */
+#define LR_LIGHT_RECT 0
+#define LR_LIGHT_DISK 1
+#define LR_LIGHT_SPHERE 2
+#define LR_LIGHT_DISTANT 3
+typedef struct {
+    double matrix[12];  /* columns x, y, z (the light shines down its -Z), translation */
+    int32_t shape;      /* LR_LIGHT_* */
+    double color[3];    /* linear ACEScg */
+    double intensity, exposure, temperature; /* temperature in kelvin, 0: none */
+    double width, height, radius, angle;     /* rect size, disk/sphere radius, distant angle (deg) */
+    int32_t normalize, visible;              /* UsdLux normalize; visible to the camera */
+} lr_light;
+
+/* OpenPBR Surface parameters (src/render/materials.lucb:17-53). This build shades the
+ * Lambertian subset: specular_weight, base_metalness, transmission_weight and
+ * coat_weight 0, geometry_opacity 1; base_diffuse_roughness is EON's. */
+typedef struct {
+    double base_weight, base_color[3], base_metalness, base_diffuse_roughness;
+    double specular_weight, specular_color[3], specular_roughness, specular_roughness_anisotropy,
+        specular_ior;
+    double transmission_weight, transmission_color[3];
+    double coat_weight, coat_color[3], coat_roughness, coat_roughness_anisotropy, coat_ior,
+        coat_darkening;
+    double emission_luminance, emission_color[3];
+    double geometry_opacity;
+    int32_t geometry_thin_walled;
+    double transmission_dispersion_scale, transmission_dispersion_abbe_number;
+} lr_openpbr;
+
+/* OpenPbr.standard (materials.lucb:46-53). */
+void lr_openpbr_standard(lr_openpbr *out);
+
+/* The reference's 32-byte BVH node (bvh.lucb:23-27). */
+typedef struct {
+    float lo[3];
+    uint32_t first; /* interior: first child of the pair; leaf: first triangle (leaf order) */
+    float hi[3];
+    uint32_t count; /* 0: interior; else triangles in the leaf */
+} lr_bvh_node;
+
+typedef struct lr_scene lr_scene;
+
+/* render.compile_scene (scene.lucb:111): world-space triangles in BVH leaf order,
+ * their polygons and shading attributes, the binned-SAH BVH2, cameras, lights and
+ * the material library. The caller owns the result (CompiledScene.close ->
+ * lr_scene_free). */
+int lr_scene_compile(const lr_mesh *meshes, size_t mesh_count, const lr_camera *cameras,
+                     size_t camera_count, const lr_light *lights, size_t light_count,
+                     const lr_openpbr *materials, size_t material_count, lr_scene **out);
+/* CompiledScene.close (scene.lucb:87-98). */
+void lr_scene_free(lr_scene *scene);
+
+typedef struct {
+    uint64_t point_count, triangle_count, node_count;
+    uint32_t face_count, camera_count, light_count, material_count, bvh_depth;
+} lr_scene_info;
+/* CompiledScene.triangle_count / point_count (scene.lucb:81-85) and the BVH's size. */
+int lr_scene_info_get(const lr_scene *scene, lr_scene_info *out);
+/* The compiled arrays (CompiledScene fields, scene.lucb:31-63), owned by the scene:
+ * positions (3 floats a point), indices (3 a triangle, leaf order), faces (1 a
+ * triangle), shading (4 a triangle: three octahedral normals, material), nodes and
+ * order (the source triangle at each leaf slot). Any output may be NULL. */
+int lr_scene_arrays(const lr_scene *scene, const float **positions, const uint32_t **indices,
+                    const uint32_t **faces, const uint32_t **shading, const lr_bvh_node **nodes,
+                    const uint32_t **order);
+
+/* ---- Ray frames (src/render/camera.lucb) ------------------------------------------- */
+
+/* RayFrame (camera.lucb:26-54). */
+typedef struct {
+    double position[3], corner[3], du[3], dv[3], forward[3];
+    int32_t orthographic;
+    uint32_t width, height;
+    double lens_radius, focus_distance;
+} lr_frame;
+
+/* render.ray_frame (camera.lucb:57): the frame of camera `camera` for width x height. */
+int lr_ray_frame(const lr_camera *camera, uint32_t width, uint32_t height, lr_frame *out);
+/* render.look_frame (camera.lucb:84). */
+int lr_look_frame(const double position[3], const double forward[3], const double up[3],
+                  double tan_half_height, uint32_t width, uint32_t height, int32_t orthographic,
+                  lr_frame *out);
+/* RayFrame.pack (camera.lucb:41-47): the 16-float block the kernels read. */
+int lr_frame_pack(const lr_frame *frame, float out[16]);
+/* The scene's camera `index` (-1: the first camera; Renderer's find_camera,
+ * integrator.lucb:955-961). */
+int lr_scene_camera(const lr_scene *scene, int32_t index, lr_camera *out);
+
+/* ---- The scene on the device (src/render/device.lucb) ----------------------------- */
+
+typedef struct lr_gpu_scene lr_gpu_scene;
+
+/* GpuScene.upload (device.lucb:41): the scene's traversal and shading buffers in HBM.
+ * The scene may be freed afterwards. */
+int lr_gpu_scene_upload(lr_context *ctx, const lr_scene *scene, lr_gpu_scene **out);
+/* GpuScene.destroy (device.lucb:108-121). */
+void lr_gpu_scene_destroy(lr_gpu_scene *scene);
+
+/* Query flags. LR_TRACE_ANY: any-hit (trace_any, bvh.glsl:93-122) instead of the
+ * closest hit. LR_TRACE_REFERENCE: the reference's own traversal and Moller-Trumbore
+ * test (bvh.glsl:17-90, box order and tie rule included) instead of the default
+ * watertight test with ties going to the smaller triangle id. */
+#define LR_TRACE_ANY 1u
+#define LR_TRACE_REFERENCE 2u
+
+/* render.probe (device.lucb:138-160): the pixel-centre ray of every pixel of
+ * `frame` (probe.comp:21-34), row by row from the top; per pixel the polygon hit
+ * (0xffffffff: none) and its distance along the frame's unnormalized direction
+ * (3e38 on a miss). Host buffers of width*height entries; waits for the result. */
+int lr_probe(lr_context *ctx, const lr_gpu_scene *scene, const lr_frame *frame, uint32_t flags,
+             uint32_t *faces, float *distances);
+
+/* Ray queries, the ray-list form of the probe. A ray is 8 floats (origin xyz, tmin,
+ * direction xyz, tmax; hits have tmin < t < tmax); a hit is 4 words (t, triangle id as
+ * int32 -- the caller's triangle numbering, -1 none --, barycentrics u and v of the
+ * second and third vertices). lr_trace_rays copies host rays in and hits out and
+ * waits; lr_trace_rays_device works on device buffers, queued on the context's
+ * stream without waiting. */
+int lr_trace_rays(lr_context *ctx, const lr_gpu_scene *scene, const float *rays, uint64_t count,
+                  float *hits, uint32_t flags);
+int lr_trace_rays_device(lr_context *ctx, const lr_gpu_scene *scene, const void *rays,
+                         uint64_t count, void *hits, uint32_t flags);
+
+/* ---- The renderer (src/render/integrator.lucb) -------------------------------------- */
+
+/* RenderSettings (integrator.lucb:42-82). */
+typedef struct {
+    uint32_t width, height, samples, max_bounces;
+    int32_t spectral;
+    int32_t camera; /* -1: the first camera */
+    double background[3];
+    lr_openpbr material;
+    uint32_t pool, seed;
+    int32_t software_bvh;
+    uint32_t diffuse_bounces, glossy_bounces, transmission_bounces;
+    double clamp_indirect, noise_threshold;
+    uint32_t adaptive_minimum;
+    int32_t profile, guiding;
+    double light_tracing;
+} lr_settings;
+
+/* RenderSettings.of (integrator.lucb:84-85), with the reference's defaults. */
+void lr_settings_default(lr_settings *out, uint32_t width, uint32_t height, uint32_t samples);
+
+typedef struct lr_renderer lr_renderer;
+
+/* Renderer.create (integrator.lucb:343): a renderer of `scene` through its camera.
+ * The scene's buffers are uploaded; the scene may be freed afterwards. */
+int lr_renderer_create(lr_context *ctx, const lr_scene *scene, const lr_settings *settings,
+                       lr_renderer **out);
+/* Renderer.create_viewed (integrator.lucb:375): through a caller's frame. */
+int lr_renderer_create_viewed(lr_context *ctx, const lr_scene *scene, const lr_settings *settings,
+                              const lr_frame *frame, lr_renderer **out);
+/* Renderer.advance (integrator.lucb:649-693): queue the next pass (one sample of
+ * one band) without waiting; *more is 1 while passes are running or to come. */
+int lr_renderer_advance(lr_renderer *renderer, int32_t *more);
+/* Renderer.finish (integrator.lucb:724-729): run every remaining pass and wait. */
+int lr_renderer_finish(lr_renderer *renderer);
+/* Renderer.samples_done (integrator.lucb:732-733). */
+uint32_t lr_renderer_samples_done(const lr_renderer *renderer);
+/* Renderer.image (integrator.lucb:737-738): the rgba32f ACEScg image in device
+ * memory, width*height*16 bytes, row by row from the top. */
+int lr_renderer_image(lr_renderer *renderer, void **device_rgba);
+/* Renderer.read (integrator.lucb:778-782): the image copied to `rgba` (4 floats a
+ * pixel); waits for work in flight. */
+int lr_renderer_read(lr_renderer *renderer, float *rgba, uint64_t float_count);
+/* Renderer.set_samples (integrator.lucb:609-611). */
+int lr_renderer_set_samples(lr_renderer *renderer, uint32_t samples);
+/* Renderer.kernel_times (integrator.lucb:873-875): milliseconds per kernel kind
+ * over finished passes with settings.profile on, in the order camera, intersect
+ * closest, shade surface, shade miss, intersect shadow, light emission, finish,
+ * film convert, adaptive, later rounds. */
+int lr_renderer_kernel_times(lr_renderer *renderer, double out[10]);
+
+/* Counters of the work finished passes did: rays traced for closest hits and for
+ * shadows, path vertices shaded, and passes. Waits for work in flight. */
+typedef struct {
+    uint64_t closest_rays, shadow_rays, shaded, passes;
+} lr_render_stats;
+int lr_renderer_stats(lr_renderer *renderer, lr_render_stats *out);
+/* Renderer.destroy (integrator.lucb:887-900). */
+void lr_renderer_destroy(lr_renderer *renderer);
+
+#if defined(__GNUC__)
+#pragma GCC visibility pop
+#endif
+
+#ifdef __cplusplus
+}
+#endif
+#endif

@@ -1,0 +1,651 @@
+"""luce_render_b200: a B200-native (sm_100a) implementation of luce-render's wavefront
+path-tracing hot path, behind a C ABI (include/luce_render_b200.h).
+
+This module is the ctypes harness over that ABI, mirroring luce-render's ``render``
+package for the path (package.prisma:13):
+
+=====================================  ===============================================
+luce-render (src/render/...)            here
+=====================================  ===============================================
+``compile_scene`` (scene.lucb:111)      :func:`compile_scene` -> :class:`CompiledScene`
+``GpuScene.upload`` (device.lucb:41)    :meth:`GpuScene.upload`
+``probe`` (device.lucb:138)             :func:`probe`
+``ray_frame`` / ``look_frame``          :func:`ray_frame` / :func:`look_frame`
+(camera.lucb:57, 84)
+``RenderSettings.of`` (integr.:84)      :meth:`RenderSettings.of`
+``Renderer.create/advance/finish/       :class:`Renderer`
+samples_done/image/read``
+=====================================  ===============================================
+
+Errors raise :class:`RenderError` with the reference's codes (400 invalid, 401 limit,
+402 stopped; module.lucb:60-63) or 500/504 for device failures. The CUDA library is
+required: importing this package fails loudly when it has not been built.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+from pathlib import Path
+from typing import Iterable, Sequence
+
+import numpy as np
+
+_HERE = Path(__file__).resolve().parent
+LIBRARY_PATH = _HERE / "libluce_render_b200.so"
+
+INVALID, LIMIT, STOPPED, DEVICE, TIMEOUT = 400, 401, 402, 500, 504
+TRACE_ANY, TRACE_REFERENCE = 1, 2
+LIGHT_RECT, LIGHT_DISK, LIGHT_SPHERE, LIGHT_DISTANT = 0, 1, 2, 3
+
+
+class RenderError(RuntimeError):
+    """A failing call of the C ABI: ``code`` is its status, the message its text."""
+
+    def __init__(self, code: int, message: str):
+        super().__init__(f"[{code}] {message}")
+        self.code = code
+        self.message = message
+
+
+def _load() -> C.CDLL:
+    if not LIBRARY_PATH.exists():
+        raise ImportError(
+            f"{LIBRARY_PATH} is missing: build it with `python -m luce_render_b200.build` "
+            "(nvcc for sm_100a). There is no CPU fallback.")
+    return C.CDLL(str(LIBRARY_PATH))
+
+
+lib = _load()
+
+
+# ---- structures (include/luce_render_b200.h) ------------------------------------------
+
+class Mesh(C.Structure):
+    _fields_ = [("positions", C.POINTER(C.c_float)), ("point_count", C.c_uint64),
+                ("indices", C.POINTER(C.c_uint32)), ("triangle_count", C.c_uint64),
+                ("triangle_faces", C.POINTER(C.c_uint32)), ("face_count", C.c_uint32),
+                ("normals", C.POINTER(C.c_float)), ("normals_per_corner", C.c_int32),
+                ("face_materials", C.POINTER(C.c_uint32)), ("transform", C.c_double * 12)]
+
+
+class Camera(C.Structure):
+    _fields_ = [("matrix", C.c_double * 12), ("projection", C.c_int32), ("focal_length", C.c_double),
+                ("horizontal_aperture", C.c_double), ("f_stop", C.c_double), ("focus_distance", C.c_double)]
+
+
+class Light(C.Structure):
+    _fields_ = [("matrix", C.c_double * 12), ("shape", C.c_int32), ("color", C.c_double * 3),
+                ("intensity", C.c_double), ("exposure", C.c_double), ("temperature", C.c_double),
+                ("width", C.c_double), ("height", C.c_double), ("radius", C.c_double), ("angle", C.c_double),
+                ("normalize", C.c_int32), ("visible", C.c_int32)]
+
+
+class OpenPbr(C.Structure):
+    _fields_ = [("base_weight", C.c_double), ("base_color", C.c_double * 3), ("base_metalness", C.c_double),
+                ("base_diffuse_roughness", C.c_double), ("specular_weight", C.c_double),
+                ("specular_color", C.c_double * 3), ("specular_roughness", C.c_double),
+                ("specular_roughness_anisotropy", C.c_double), ("specular_ior", C.c_double),
+                ("transmission_weight", C.c_double), ("transmission_color", C.c_double * 3),
+                ("coat_weight", C.c_double), ("coat_color", C.c_double * 3), ("coat_roughness", C.c_double),
+                ("coat_roughness_anisotropy", C.c_double), ("coat_ior", C.c_double),
+                ("coat_darkening", C.c_double), ("emission_luminance", C.c_double),
+                ("emission_color", C.c_double * 3), ("geometry_opacity", C.c_double),
+                ("geometry_thin_walled", C.c_int32), ("transmission_dispersion_scale", C.c_double),
+                ("transmission_dispersion_abbe_number", C.c_double)]
+
+    @staticmethod
+    def standard() -> "OpenPbr":
+        """OpenPbr.standard (materials.lucb:46-53)."""
+        m = OpenPbr()
+        lib.lr_openpbr_standard(C.byref(m))
+        return m
+
+    @staticmethod
+    def lambert(color=(0.8, 0.8, 0.8), emission: float = 0.0, emission_color=(1.0, 1.0, 1.0),
+                roughness: float = 0.0) -> "OpenPbr":
+        """A diffuse-only material: the standard one with specular_weight 0."""
+        m = OpenPbr.standard()
+        m.base_color[:] = list(color)
+        m.specular_weight = 0.0
+        m.base_diffuse_roughness = roughness
+        m.emission_luminance = emission
+        m.emission_color[:] = list(emission_color)
+        return m
+
+
+class BvhNode(C.Structure):
+    _fields_ = [("lo", C.c_float * 3), ("first", C.c_uint32), ("hi", C.c_float * 3), ("count", C.c_uint32)]
+
+
+NODE_DTYPE = np.dtype([("lo", "<f4", 3), ("first", "<u4"), ("hi", "<f4", 3), ("count", "<u4")])
+
+
+class SceneInfo(C.Structure):
+    _fields_ = [("point_count", C.c_uint64), ("triangle_count", C.c_uint64), ("node_count", C.c_uint64),
+                ("face_count", C.c_uint32), ("camera_count", C.c_uint32), ("light_count", C.c_uint32),
+                ("material_count", C.c_uint32), ("bvh_depth", C.c_uint32)]
+
+
+class Frame(C.Structure):
+    """RayFrame (camera.lucb:26-54)."""
+    _fields_ = [("position", C.c_double * 3), ("corner", C.c_double * 3), ("du", C.c_double * 3),
+                ("dv", C.c_double * 3), ("forward", C.c_double * 3), ("orthographic", C.c_int32),
+                ("width", C.c_uint32), ("height", C.c_uint32), ("lens_radius", C.c_double),
+                ("focus_distance", C.c_double)]
+
+    def pack(self) -> np.ndarray:
+        """RayFrame.pack (camera.lucb:41-47): the 16 floats the kernels read."""
+        out = np.zeros(16, np.float32)
+        _check(lib.lr_frame_pack(C.byref(self), _fptr(out)))
+        return out
+
+    def ray(self, x: float, y: float):
+        """RayFrame.ray (camera.lucb:51-54): origin and unnormalized direction, f64."""
+        film = np.array(self.corner) + np.array(self.du) * x + np.array(self.dv) * y
+        if self.orthographic:
+            return np.array(self.position) + film, np.array(self.forward)
+        return np.array(self.position), film
+
+
+class Settings(C.Structure):
+    _fields_ = [("width", C.c_uint32), ("height", C.c_uint32), ("samples", C.c_uint32),
+                ("max_bounces", C.c_uint32), ("spectral", C.c_int32), ("camera", C.c_int32),
+                ("background", C.c_double * 3), ("material", OpenPbr), ("pool", C.c_uint32),
+                ("seed", C.c_uint32), ("software_bvh", C.c_int32), ("diffuse_bounces", C.c_uint32),
+                ("glossy_bounces", C.c_uint32), ("transmission_bounces", C.c_uint32),
+                ("clamp_indirect", C.c_double), ("noise_threshold", C.c_double),
+                ("adaptive_minimum", C.c_uint32), ("profile", C.c_int32), ("guiding", C.c_int32),
+                ("light_tracing", C.c_double)]
+
+
+class RenderStats(C.Structure):
+    _fields_ = [("closest_rays", C.c_uint64), ("shadow_rays", C.c_uint64), ("shaded", C.c_uint64),
+                ("passes", C.c_uint64)]
+
+
+# ---- signatures ---------------------------------------------------------------------------
+
+_vp, _i32, _u32, _u64, _sz = C.c_void_p, C.c_int32, C.c_uint32, C.c_uint64, C.c_size_t
+_SIGNATURES = {
+    "lr_last_error": (C.c_char_p, []),
+    "lr_version": (C.c_char_p, []),
+    "lr_context_create": (C.c_int, [C.c_int, C.POINTER(_vp)]),
+    "lr_context_destroy": (None, [_vp]),
+    "lr_context_synchronize": (C.c_int, [_vp]),
+    "lr_context_stream": (_vp, [_vp]),
+    "lr_device_alloc": (C.c_int, [_vp, _sz, C.POINTER(_vp)]),
+    "lr_device_free": (C.c_int, [_vp, _vp]),
+    "lr_memcpy_htod": (C.c_int, [_vp, _vp, _vp, _sz]),
+    "lr_memcpy_dtoh": (C.c_int, [_vp, _vp, _vp, _sz]),
+    "lr_memset_device": (C.c_int, [_vp, _vp, C.c_int, _sz]),
+    "lr_host_alloc_pinned": (C.c_int, [_sz, C.POINTER(_vp)]),
+    "lr_host_free_pinned": (C.c_int, [_vp]),
+    "lr_timer_start": (C.c_int, [_vp]),
+    "lr_timer_stop": (C.c_int, [_vp, C.POINTER(C.c_float)]),
+    "lr_openpbr_standard": (None, [C.POINTER(OpenPbr)]),
+    "lr_scene_compile": (C.c_int, [C.POINTER(Mesh), _sz, C.POINTER(Camera), _sz, C.POINTER(Light), _sz,
+                                   C.POINTER(OpenPbr), _sz, C.POINTER(_vp)]),
+    "lr_scene_free": (None, [_vp]),
+    "lr_scene_info_get": (C.c_int, [_vp, C.POINTER(SceneInfo)]),
+    "lr_scene_arrays": (C.c_int, [_vp] + [C.POINTER(_vp)] * 6),
+    "lr_ray_frame": (C.c_int, [C.POINTER(Camera), _u32, _u32, C.POINTER(Frame)]),
+    "lr_look_frame": (C.c_int, [C.POINTER(C.c_double), C.POINTER(C.c_double), C.POINTER(C.c_double),
+                                C.c_double, _u32, _u32, _i32, C.POINTER(Frame)]),
+    "lr_frame_pack": (C.c_int, [C.POINTER(Frame), C.POINTER(C.c_float)]),
+    "lr_scene_camera": (C.c_int, [_vp, _i32, C.POINTER(Camera)]),
+    "lr_gpu_scene_upload": (C.c_int, [_vp, _vp, C.POINTER(_vp)]),
+    "lr_gpu_scene_destroy": (None, [_vp]),
+    "lr_probe": (C.c_int, [_vp, _vp, C.POINTER(Frame), _u32, C.POINTER(C.c_uint32), C.POINTER(C.c_float)]),
+    "lr_trace_rays": (C.c_int, [_vp, _vp, C.POINTER(C.c_float), _u64, C.POINTER(C.c_float), _u32]),
+    "lr_trace_rays_device": (C.c_int, [_vp, _vp, _vp, _u64, _vp, _u32]),
+    "lr_settings_default": (None, [C.POINTER(Settings), _u32, _u32, _u32]),
+    "lr_renderer_create": (C.c_int, [_vp, _vp, C.POINTER(Settings), C.POINTER(_vp)]),
+    "lr_renderer_create_viewed": (C.c_int, [_vp, _vp, C.POINTER(Settings), C.POINTER(Frame), C.POINTER(_vp)]),
+    "lr_renderer_advance": (C.c_int, [_vp, C.POINTER(_i32)]),
+    "lr_renderer_finish": (C.c_int, [_vp]),
+    "lr_renderer_samples_done": (_u32, [_vp]),
+    "lr_renderer_image": (C.c_int, [_vp, C.POINTER(_vp)]),
+    "lr_renderer_read": (C.c_int, [_vp, C.POINTER(C.c_float), _u64]),
+    "lr_renderer_set_samples": (C.c_int, [_vp, _u32]),
+    "lr_renderer_kernel_times": (C.c_int, [_vp, C.POINTER(C.c_double)]),
+    "lr_renderer_stats": (C.c_int, [_vp, C.POINTER(RenderStats)]),
+    "lr_renderer_destroy": (None, [_vp]),
+}
+
+for _name, (_res, _args) in _SIGNATURES.items():
+    _fn = getattr(lib, _name, None)
+    if _fn is None:
+        continue
+    _fn.restype = _res
+    _fn.argtypes = _args
+
+
+def exported_symbols() -> list[str]:
+    """The entry points this harness binds (every one the header declares)."""
+    return list(_SIGNATURES)
+
+
+def _check(status: int) -> None:
+    if status != 0:
+        raise RenderError(status, (lib.lr_last_error() or b"").decode())
+
+
+def _fptr(a: np.ndarray):
+    return a.ctypes.data_as(C.POINTER(C.c_float))
+
+
+def _uptr(a: np.ndarray):
+    return a.ctypes.data_as(C.POINTER(C.c_uint32))
+
+
+def _matrix12(m) -> "C.Array":
+    arr = (C.c_double * 12)()
+    if m is not None:
+        arr[:] = [float(v) for v in np.asarray(m, np.float64).reshape(12)]
+    return arr
+
+
+# ---- context ----------------------------------------------------------------------------
+
+class Context:
+    """One CUDA device and stream (the reference's gpu.Device)."""
+
+    def __init__(self, device: int = 0):
+        handle = _vp()
+        _check(lib.lr_context_create(device, C.byref(handle)))
+        self.handle = handle
+        self.device = device
+
+    def synchronize(self) -> None:
+        _check(lib.lr_context_synchronize(self.handle))
+
+    def close(self) -> None:
+        if self.handle:
+            lib.lr_context_destroy(self.handle)
+            self.handle = None
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    # Device memory, for benches and tests that keep inputs resident in HBM.
+    def alloc(self, nbytes: int) -> int:
+        p = _vp()
+        _check(lib.lr_device_alloc(self.handle, nbytes, C.byref(p)))
+        return p.value
+
+    def free(self, ptr: int) -> None:
+        _check(lib.lr_device_free(self.handle, ptr))
+
+    def upload(self, dst: int, array: np.ndarray) -> None:
+        a = np.ascontiguousarray(array)
+        _check(lib.lr_memcpy_htod(self.handle, dst, a.ctypes.data, a.nbytes))
+
+    def download(self, src: int, out: np.ndarray) -> np.ndarray:
+        _check(lib.lr_memcpy_dtoh(self.handle, out.ctypes.data, src, out.nbytes))
+        return out
+
+    def memset(self, dst: int, value: int, nbytes: int) -> None:
+        _check(lib.lr_memset_device(self.handle, dst, value, nbytes))
+
+    def timer_start(self) -> None:
+        _check(lib.lr_timer_start(self.handle))
+
+    def timer_stop(self) -> float:
+        ms = C.c_float()
+        _check(lib.lr_timer_stop(self.handle, C.byref(ms)))
+        return ms.value
+
+
+class PinnedArray:
+    """A page-locked host buffer viewed as a numpy array."""
+
+    def __init__(self, shape, dtype):
+        dtype = np.dtype(dtype)
+        nbytes = int(np.prod(shape)) * dtype.itemsize
+        p = _vp()
+        _check(lib.lr_host_alloc_pinned(max(nbytes, 16), C.byref(p)))
+        self.ptr = p.value
+        buf = (C.c_char * max(nbytes, 16)).from_address(self.ptr)
+        self.array = np.frombuffer(buf, dtype=dtype, count=int(np.prod(shape))).reshape(shape)
+
+    def close(self) -> None:
+        if self.ptr:
+            self.array = None
+            lib.lr_host_free_pinned(self.ptr)
+            self.ptr = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+# ---- scene description -----------------------------------------------------------------
+
+class MeshData:
+    """A mesh as flat arrays: the stand-in for a luce-geocore Mesh in a GeometrySet."""
+
+    def __init__(self, positions, indices, faces=None, face_count: int = 0, normals=None,
+                 normals_per_corner: bool = False, face_materials=None, transform=None):
+        self.positions = np.ascontiguousarray(positions, np.float32).reshape(-1, 3)
+        self.indices = np.ascontiguousarray(indices, np.uint32).reshape(-1, 3)
+        self.faces = None if faces is None else np.ascontiguousarray(faces, np.uint32).reshape(-1)
+        self.face_count = int(face_count)
+        self.normals = None if normals is None else np.ascontiguousarray(normals, np.float32).reshape(-1, 3)
+        self.normals_per_corner = bool(normals_per_corner)
+        self.face_materials = None if face_materials is None else np.ascontiguousarray(face_materials, np.uint32)
+        self.transform = transform
+
+    def to_c(self) -> Mesh:
+        m = Mesh()
+        m.positions = _fptr(self.positions)
+        m.point_count = len(self.positions)
+        m.indices = _uptr(self.indices)
+        m.triangle_count = len(self.indices)
+        if self.faces is not None:
+            m.triangle_faces = _uptr(self.faces)
+        m.face_count = self.face_count
+        if self.normals is not None:
+            m.normals = _fptr(self.normals)
+            m.normals_per_corner = 1 if self.normals_per_corner else 0
+        if self.face_materials is not None:
+            m.face_materials = _uptr(self.face_materials)
+        m.transform = _matrix12(self.transform)
+        return m
+
+
+def placement(position=(0.0, 0.0, 0.0), rotation=(0.0, 0.0, 0.0), scale=(1.0, 1.0, 1.0)) -> np.ndarray:
+    """A 12-double placement (columns x, y, z, translation): scale, then rotation about
+    X, then Y, then Z (radians), then translation."""
+    rx, ry, rz = rotation
+    cx, sx, cy, sy, cz, sz = np.cos(rx), np.sin(rx), np.cos(ry), np.sin(ry), np.cos(rz), np.sin(rz)
+    Rx = np.array([[1, 0, 0], [0, cx, -sx], [0, sx, cx]])
+    Ry = np.array([[cy, 0, sy], [0, 1, 0], [-sy, 0, cy]])
+    Rz = np.array([[cz, -sz, 0], [sz, cz, 0], [0, 0, 1]])
+    M = Rz @ Ry @ Rx @ np.diag(np.asarray(scale, np.float64))
+    return np.concatenate([M[:, 0], M[:, 1], M[:, 2], np.asarray(position, np.float64)])
+
+
+def camera(position, rotation=(0.0, 0.0, 0.0), projection: int = 0, focal_length: float = 50.0,
+           horizontal_aperture: float = 36.0, f_stop: float = 0.0, focus_distance: float = 5.0,
+           matrix=None) -> Camera:
+    c = Camera()
+    c.matrix = _matrix12(matrix if matrix is not None else placement(position, rotation))
+    c.projection = projection
+    c.focal_length = focal_length
+    c.horizontal_aperture = horizontal_aperture
+    c.f_stop = f_stop
+    c.focus_distance = focus_distance
+    return c
+
+
+def light(shape: int, position=(0.0, 0.0, 0.0), rotation=(0.0, 0.0, 0.0), color=(1.0, 1.0, 1.0),
+          intensity: float = 1.0, exposure: float = 0.0, temperature: float = 0.0, width: float = 1.0,
+          height: float = 1.0, radius: float = 0.5, angle: float = 0.0, normalize: bool = False,
+          visible: bool = True, matrix=None) -> Light:
+    l = Light()
+    l.matrix = _matrix12(matrix if matrix is not None else placement(position, rotation))
+    l.shape = shape
+    l.color[:] = list(color)
+    l.intensity, l.exposure, l.temperature = intensity, exposure, temperature
+    l.width, l.height, l.radius, l.angle = width, height, radius, angle
+    l.normalize = 1 if normalize else 0
+    l.visible = 1 if visible else 0
+    return l
+
+
+class CompiledScene:
+    """render.CompiledScene (scene.lucb:31-63): owned here, freed by close()."""
+
+    def __init__(self, handle):
+        self.handle = handle
+
+    @property
+    def info(self) -> SceneInfo:
+        info = SceneInfo()
+        _check(lib.lr_scene_info_get(self.handle, C.byref(info)))
+        return info
+
+    def triangle_count(self) -> int:
+        return int(self.info.triangle_count)
+
+    def point_count(self) -> int:
+        return int(self.info.point_count)
+
+    def arrays(self) -> dict:
+        """Copies of the compiled arrays: positions, indices, faces, shading, nodes, order."""
+        info = self.info
+        ptrs = [_vp() for _ in range(6)]
+        _check(lib.lr_scene_arrays(self.handle, *[C.byref(p) for p in ptrs]))
+        T, P, N = int(info.triangle_count), int(info.point_count), int(info.node_count)
+
+        def view(ptr, count, dtype):
+            if count == 0 or not ptr.value:
+                return np.zeros(0, dtype)
+            dt = np.dtype(dtype)
+            buf = (C.c_char * (count * dt.itemsize)).from_address(ptr.value)
+            return np.frombuffer(buf, dtype=dt, count=count).copy()
+
+        return {
+            "positions": view(ptrs[0], P * 3, np.float32).reshape(-1, 3),
+            "indices": view(ptrs[1], T * 3, np.uint32).reshape(-1, 3),
+            "faces": view(ptrs[2], T, np.uint32),
+            "shading": view(ptrs[3], T * 4, np.uint32).reshape(-1, 4),
+            "nodes": view(ptrs[4], N, NODE_DTYPE),
+            "order": view(ptrs[5], T, np.uint32),
+        }
+
+    def camera(self, index: int = -1) -> Camera:
+        c = Camera()
+        _check(lib.lr_scene_camera(self.handle, index, C.byref(c)))
+        return c
+
+    def close(self) -> None:
+        if self.handle:
+            lib.lr_scene_free(self.handle)
+            self.handle = None
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+def compile_scene(meshes: Sequence[MeshData], cameras: Sequence[Camera] = (), lights: Sequence[Light] = (),
+                  materials: Sequence[OpenPbr] = ()) -> CompiledScene:
+    """render.compile_scene (scene.lucb:111-129)."""
+    cm = (Mesh * max(1, len(meshes)))(*[m.to_c() for m in meshes])
+    cc = (Camera * max(1, len(cameras)))(*cameras)
+    cl = (Light * max(1, len(lights)))(*lights)
+    cmat = (OpenPbr * max(1, len(materials)))(*materials)
+    handle = _vp()
+    _check(lib.lr_scene_compile(cm, len(meshes), cc, len(cameras), cl, len(lights), cmat, len(materials),
+                                C.byref(handle)))
+    return CompiledScene(handle)
+
+
+def ray_frame(cam: Camera, width: int, height: int) -> Frame:
+    """render.ray_frame (camera.lucb:57-76)."""
+    f = Frame()
+    _check(lib.lr_ray_frame(C.byref(cam), width, height, C.byref(f)))
+    return f
+
+
+def look_frame(position, forward, up, tan_half_height: float, width: int, height: int,
+               orthographic: bool = False) -> Frame:
+    """render.look_frame (camera.lucb:84-95)."""
+    f = Frame()
+    p, fw, u = ((C.c_double * 3)(*map(float, v)) for v in (position, forward, up))
+    _check(lib.lr_look_frame(p, fw, u, float(tan_half_height), width, height, 1 if orthographic else 0,
+                             C.byref(f)))
+    return f
+
+
+class GpuScene:
+    """render.GpuScene (device.lucb:16-38)."""
+
+    def __init__(self, handle, ctx: Context):
+        self.handle = handle
+        self.ctx = ctx
+
+    @staticmethod
+    def upload(ctx: Context, scene: CompiledScene) -> "GpuScene":
+        handle = _vp()
+        _check(lib.lr_gpu_scene_upload(ctx.handle, scene.handle, C.byref(handle)))
+        return GpuScene(handle, ctx)
+
+    def destroy(self) -> None:
+        if self.handle:
+            lib.lr_gpu_scene_destroy(self.handle)
+            self.handle = None
+
+    close = destroy
+
+    def __del__(self):
+        try:
+            self.destroy()
+        except Exception:
+            pass
+
+
+def probe(ctx: Context, scene: GpuScene, frame: Frame, reference: bool = False):
+    """render.probe (device.lucb:138-160): per pixel (row-major from the top) the polygon
+    hit (0xffffffff none) and its distance along the frame's unnormalized direction."""
+    n = int(frame.width) * int(frame.height)
+    faces = np.empty(n, np.uint32)
+    distances = np.empty(n, np.float32)
+    _check(lib.lr_probe(ctx.handle, scene.handle, C.byref(frame), TRACE_REFERENCE if reference else 0,
+                        _uptr(faces), _fptr(distances)))
+    return faces, distances
+
+
+def trace_rays(ctx: Context, scene: GpuScene, rays: np.ndarray, any_hit: bool = False,
+               reference: bool = False) -> np.ndarray:
+    """Closest (or any) hits of rays (n x 8 floats: origin, tmin, direction, tmax):
+    n x 4 words (t, triangle id as int32, u, v)."""
+    rays = np.ascontiguousarray(rays, np.float32).reshape(-1, 8)
+    hits = np.empty((len(rays), 4), np.float32)
+    flags = (TRACE_ANY if any_hit else 0) | (TRACE_REFERENCE if reference else 0)
+    _check(lib.lr_trace_rays(ctx.handle, scene.handle, _fptr(rays), len(rays), _fptr(hits), flags))
+    return hits
+
+
+def hit_ids(hits: np.ndarray) -> np.ndarray:
+    """The triangle ids (int32, -1 none) of a hits array."""
+    return hits.view(np.int32)[:, 1].copy()
+
+
+# ---- the renderer ------------------------------------------------------------------------
+
+class RenderSettings:
+    """RenderSettings (integrator.lucb:42-85)."""
+
+    def __init__(self, settings: Settings):
+        self.c = settings
+
+    @staticmethod
+    def of(width: int, height: int, samples: int) -> "RenderSettings":
+        s = Settings()
+        lib.lr_settings_default(C.byref(s), width, height, samples)
+        return RenderSettings(s)
+
+    def __getattr__(self, name):
+        return getattr(self.__dict__["c"], name)
+
+    def __setattr__(self, name, value):
+        if name == "c":
+            self.__dict__["c"] = value
+        elif name in ("background",):
+            self.c.background[:] = list(value)
+        else:
+            setattr(self.c, name, value)
+
+
+class Renderer:
+    """render.Renderer (integrator.lucb:259-900)."""
+
+    def __init__(self, handle, ctx: Context, width: int, height: int):
+        self.handle = handle
+        self.ctx = ctx
+        self.width, self.height = width, height
+
+    @staticmethod
+    def create(ctx: Context, scene: CompiledScene, settings: RenderSettings, frame: Frame | None = None) -> "Renderer":
+        handle = _vp()
+        if frame is None:
+            _check(lib.lr_renderer_create(ctx.handle, scene.handle, C.byref(settings.c), C.byref(handle)))
+            w, h = settings.c.width, settings.c.height
+        else:
+            _check(lib.lr_renderer_create_viewed(ctx.handle, scene.handle, C.byref(settings.c), C.byref(frame),
+                                                 C.byref(handle)))
+            w, h = frame.width, frame.height
+        return Renderer(handle, ctx, int(w), int(h))
+
+    def advance(self) -> bool:
+        more = C.c_int32()
+        _check(lib.lr_renderer_advance(self.handle, C.byref(more)))
+        return bool(more.value)
+
+    def finish(self) -> None:
+        _check(lib.lr_renderer_finish(self.handle))
+
+    def samples_done(self) -> int:
+        return int(lib.lr_renderer_samples_done(self.handle))
+
+    def image(self) -> int:
+        """The device address of the rgba32f image."""
+        p = _vp()
+        _check(lib.lr_renderer_image(self.handle, C.byref(p)))
+        return p.value
+
+    def read(self) -> np.ndarray:
+        out = np.empty((self.height, self.width, 4), np.float32)
+        _check(lib.lr_renderer_read(self.handle, _fptr(out), out.size))
+        return out
+
+    def set_samples(self, samples: int) -> None:
+        _check(lib.lr_renderer_set_samples(self.handle, samples))
+
+    def kernel_times(self) -> np.ndarray:
+        out = (C.c_double * 10)()
+        _check(lib.lr_renderer_kernel_times(self.handle, out))
+        return np.array(out[:])
+
+    def stats(self) -> RenderStats:
+        s = RenderStats()
+        _check(lib.lr_renderer_stats(self.handle, C.byref(s)))
+        return s
+
+    def destroy(self) -> None:
+        if self.handle:
+            lib.lr_renderer_destroy(self.handle)
+            self.handle = None
+
+    close = destroy
+
+    def __del__(self):
+        try:
+            self.destroy()
+        except Exception:
+            pass
+
+
+KERNEL_NAMES = ["camera", "intersect closest", "shade surface", "shade miss", "intersect shadow",
+                "light emission", "finish", "film convert", "adaptive", "later rounds"]

@@ -1,0 +1,480 @@
+// The context, the scene in HBM (GpuScene.upload, src/render/device.lucb:41-89), the
+// primary-ray probe (device.lucb:138-160, shaders/probe.comp) and ray-list queries.
+#include <algorithm>
+#include <cmath>
+#include <cstring>
+#include <memory>
+#include <vector>
+
+#include "device.hpp"
+#include "traverse.cuh"
+
+namespace lr {
+
+thread_local std::string g_last_error;
+void set_last_error(const char *message) { g_last_error = message; }
+
+namespace {
+
+constexpr int kBlock = 128;
+
+struct ProbeFrame {
+    float b[16];
+};
+
+__device__ __forceinline__ void note_overflow(int *status, bool overflow) {
+    if (overflow) atomicAdd(status, 1);
+}
+
+// probe.comp:21-34: one pixel-centre ray per pixel, row-major from the top.
+template <bool kRef, int kStack>
+__global__ void __launch_bounds__(kBlock) probe_kernel(DeviceScene s, ProbeFrame f, uint32_t *faces, float *ts,
+                                                      int *status) {
+    __shared__ int stack[kStack * kBlock];
+    const uint32_t width = (uint32_t)f.b[11], height = (uint32_t)f.b[15];
+    const uint64_t pixel = (uint64_t)blockIdx.x * kBlock + threadIdx.x;
+    if (pixel >= (uint64_t)width * height) return;
+    const uint32_t x = (uint32_t)(pixel % width), y = (uint32_t)(pixel / width);
+    const float fx = fadd_((float)x, 0.5f), fy = fadd_((float)y, 0.5f);
+    float film[3], o[3], d[3];
+    const bool ortho = f.b[3] > 0.5f;
+    for (int k = 0; k < 3; k++) film[k] = fadd_(fadd_(f.b[4 + k], fmul_(fx, f.b[8 + k])), fmul_(fy, f.b[12 + k]));
+    float fw[3] = {fsub_(fmul_(f.b[9], f.b[14]), fmul_(f.b[10], f.b[13])),
+                   fsub_(fmul_(f.b[10], f.b[12]), fmul_(f.b[8], f.b[14])),
+                   fsub_(fmul_(f.b[8], f.b[13]), fmul_(f.b[9], f.b[12]))};
+    const float fl = __fsqrt_rn(fadd_(fadd_(fmul_(fw[0], fw[0]), fmul_(fw[1], fw[1])), fmul_(fw[2], fw[2])));
+    for (int k = 0; k < 3; k++) {
+        o[k] = ortho ? fadd_(f.b[k], film[k]) : f.b[k];
+        d[k] = ortho ? __fdiv_rn(fw[k], fl) : film[k];
+    }
+    Ray r{make_float3(o[0], o[1], o[2]), 0.0f, make_float3(d[0], d[1], d[2]), kNoHitT};
+    bool overflow = false;
+    Hit h = kRef ? trace_reference<false, kStack>(s, r, stack + threadIdx.x, kBlock, overflow)
+                 : trace_exact<false, kStack>(s, r, stack + threadIdx.x, kBlock, overflow);
+    note_overflow(status, overflow);
+    faces[pixel] = h.slot >= 0 ? __ldg(&s.faces[h.slot]) : 0xffffffffu;
+    ts[pixel] = h.t;
+}
+
+// A list of rays (two float4 each) to hits (t, source id bits, u, v).
+template <bool kRef, bool kAny, int kStack>
+__global__ void __launch_bounds__(kBlock) trace_kernel(DeviceScene s, const float4 *__restrict__ rays, uint64_t n,
+                                                      float4 *__restrict__ hits, int *status) {
+    __shared__ int stack[kStack * kBlock];
+    const uint64_t i = (uint64_t)blockIdx.x * kBlock + threadIdx.x;
+    if (i >= n) return;
+    const float4 a = __ldg(&rays[2 * i]), b = __ldg(&rays[2 * i + 1]);
+    Ray r{make_float3(a.x, a.y, a.z), a.w, make_float3(b.x, b.y, b.z), b.w};
+    bool overflow = false;
+    Hit h = kRef ? trace_reference<kAny, kStack>(s, r, stack + threadIdx.x, kBlock, overflow)
+                 : trace_exact<kAny, kStack>(s, r, stack + threadIdx.x, kBlock, overflow);
+    note_overflow(status, overflow);
+    hits[i] = make_float4(h.t, __int_as_float(h.id), h.u, h.v);
+}
+
+int stack_for(uint32_t depth) {
+    if (depth + 2 <= 32) return 32;
+    if (depth + 2 <= 64) return 64;
+    if (depth + 2 <= 96) return 96;
+    fail(LR_LIMIT, "the BVH is deeper than 94 levels");
+}
+
+template <bool kRef, int kStack>
+void launch_probe(const lr_gpu_scene *gs, const ProbeFrame &f, uint64_t count, uint32_t *faces, float *ts,
+                  int *status, cudaStream_t stream) {
+    const unsigned grid = (unsigned)((count + kBlock - 1) / kBlock);
+    probe_kernel<kRef, kStack><<<grid, kBlock, 0, stream>>>(gs->scene, f, faces, ts, status);
+}
+
+template <bool kRef, bool kAny, int kStack>
+void launch_trace(const lr_gpu_scene *gs, const float4 *rays, uint64_t n, float4 *hits, int *status,
+                  cudaStream_t stream) {
+    const unsigned grid = (unsigned)((n + kBlock - 1) / kBlock);
+    trace_kernel<kRef, kAny, kStack><<<grid, kBlock, 0, stream>>>(gs->scene, rays, n, hits, status);
+}
+
+template <bool kRef, bool kAny>
+void dispatch_trace(const lr_gpu_scene *gs, const float4 *rays, uint64_t n, float4 *hits, int *status,
+                    cudaStream_t stream) {
+    switch (stack_for(gs->scene.depth)) {
+        case 32: launch_trace<kRef, kAny, 32>(gs, rays, n, hits, status, stream); break;
+        case 64: launch_trace<kRef, kAny, 64>(gs, rays, n, hits, status, stream); break;
+        default: launch_trace<kRef, kAny, 96>(gs, rays, n, hits, status, stream); break;
+    }
+}
+
+template <bool kRef>
+void dispatch_probe(const lr_gpu_scene *gs, const ProbeFrame &f, uint64_t count, uint32_t *faces, float *ts,
+                    int *status, cudaStream_t stream) {
+    switch (stack_for(gs->scene.depth)) {
+        case 32: launch_probe<kRef, 32>(gs, f, count, faces, ts, status, stream); break;
+        case 64: launch_probe<kRef, 64>(gs, f, count, faces, ts, status, stream); break;
+        default: launch_probe<kRef, 96>(gs, f, count, faces, ts, status, stream); break;
+    }
+}
+
+float bits_as_float(int v) {
+    float f;
+    std::memcpy(&f, &v, sizeof f);
+    return f;
+}
+
+// Rounds outward by `delta`, then one more float step.
+float widen_down(float v, float delta) { return std::nextafter(v - delta, -INFINITY); }
+float widen_up(float v, float delta) { return std::nextafter(v + delta, INFINITY); }
+
+struct HostLayout {
+    std::vector<float4> entries, ref_entries, tris;
+    std::vector<uint4> shading;
+    int root = 0;
+    float root_lo[3], root_hi[3];
+    float delta = 0.0f;
+};
+
+int leaf_link(const lr_bvh_node &n) {
+    if (n.count == 0 || n.count > 16) fail(LR_INVALID, "a BVH leaf holds 1 to 16 triangles");
+    if (n.first > kMaxLeafFirst) fail(LR_LIMIT, "a scene holds at most 2^27 triangles");
+    return -1 - (int)((n.first << kLeafShift) | (n.count - 1));
+}
+
+void build_layout(const lr::Scene &scene, HostLayout &L) {
+    const auto &nodes = scene.nodes;
+    const size_t T = scene.triangle_count();
+    // The widening that keeps the box test conservative for the watertight triangle
+    // test: 2^-16 of the scene's coordinate scale (its largest magnitude or extent).
+    double scale = 1.0;
+    for (int k = 0; k < 3; k++) {
+        scale = std::max(scale, (double)std::fabs(nodes[0].lo[k]));
+        scale = std::max(scale, (double)std::fabs(nodes[0].hi[k]));
+        scale = std::max(scale, (double)(nodes[0].hi[k] - nodes[0].lo[k]));
+    }
+    L.delta = T ? (float)std::ldexp(scale, -16) : 0.0f;
+    std::vector<int> entry(nodes.size(), -1);
+    int interior = 0;
+    for (size_t n = 0; n < nodes.size(); n++)
+        if (T && nodes[n].count == 0) entry[n] = interior++;
+    auto link = [&](uint32_t c) { return nodes[c].count == 0 ? entry[c] : leaf_link(nodes[c]); };
+    L.entries.resize((size_t)interior * 4);
+    L.ref_entries.resize((size_t)interior * 4);
+    for (size_t n = 0; n < nodes.size(); n++) {
+        if (entry[n] < 0) continue;
+        const lr_bvh_node &a = nodes[nodes[n].first], &b = nodes[nodes[n].first + 1];
+        const float d = L.delta;
+        float4 *e = &L.entries[(size_t)entry[n] * 4];
+        e[0] = make_float4(widen_down(a.lo[0], d), widen_up(a.hi[0], d), widen_down(a.lo[1], d), widen_up(a.hi[1], d));
+        e[1] = make_float4(widen_down(b.lo[0], d), widen_up(b.hi[0], d), widen_down(b.lo[1], d), widen_up(b.hi[1], d));
+        e[2] = make_float4(widen_down(a.lo[2], d), widen_up(a.hi[2], d), widen_down(b.lo[2], d), widen_up(b.hi[2], d));
+        float4 links = make_float4(bits_as_float(link(nodes[n].first)), bits_as_float(link(nodes[n].first + 1)), 0.0f, 0.0f);
+        e[3] = links;
+        float4 *r = &L.ref_entries[(size_t)entry[n] * 4];
+        r[0] = make_float4(a.lo[0], a.hi[0], a.lo[1], a.hi[1]);
+        r[1] = make_float4(b.lo[0], b.hi[0], b.lo[1], b.hi[1]);
+        r[2] = make_float4(a.lo[2], a.hi[2], b.lo[2], b.hi[2]);
+        r[3] = links;
+    }
+    for (int k = 0; k < 3; k++) {
+        L.root_lo[k] = nodes[0].lo[k];
+        L.root_hi[k] = nodes[0].hi[k];
+    }
+    L.root = T == 0 ? 0 : link(0);
+    L.tris.resize(T * 3);
+    const float *p = scene.positions.data();
+    for (size_t t = 0; t < T; t++) {
+        for (int c = 0; c < 3; c++) {
+            const float *v = &p[(size_t)scene.indices[t * 3 + c] * 3];
+            float w = c == 0 ? bits_as_float((int)scene.order[t]) : 0.0f;
+            L.tris[t * 3 + c] = make_float4(v[0], v[1], v[2], w);
+        }
+    }
+    L.shading.resize(T);
+    for (size_t t = 0; t < T; t++)
+        L.shading[t] = make_uint4(scene.shading[t * 4], scene.shading[t * 4 + 1], scene.shading[t * 4 + 2],
+                                  scene.shading[t * 4 + 3]);
+}
+
+size_t align256(size_t v) { return (v + 255) & ~(size_t)255; }
+
+}  // namespace
+
+}  // namespace lr
+
+using namespace lr;
+
+namespace lr {
+void check_status(lr_context *ctx) {
+    int words[2] = {0, 0};
+    LR_CUDA(cudaMemcpyAsync(words, ctx->status, sizeof words, cudaMemcpyDeviceToHost, ctx->stream));
+    LR_CUDA(cudaStreamSynchronize(ctx->stream));
+    if (words[0] || words[1]) {
+        LR_CUDA(cudaMemsetAsync(ctx->status, 0, sizeof words, ctx->stream));
+        LR_CUDA(cudaStreamSynchronize(ctx->stream));
+        if (words[0]) fail(LR_LIMIT, "a traversal stack overflowed: " + std::to_string(words[0]) + " pushes lost");
+        fail(LR_TIMEOUT, "a device-side bounded wait gave up " + std::to_string(words[1]) + " times");
+    }
+}
+}  // namespace lr
+
+extern "C" {
+
+const char *lr_last_error(void) { return lr::g_last_error.c_str(); }
+const char *lr_version(void) { return "luce_render_b200 0.1 (sm_100a)"; }
+
+int lr_context_create(int device, lr_context **out) {
+    return guarded([&] {
+        if (!out) fail(LR_INVALID, "no place for the context");
+        *out = nullptr;
+        int count = 0;
+        LR_CUDA(cudaGetDeviceCount(&count));
+        if (device < 0 || device >= count) fail(LR_INVALID, "no such CUDA device");
+        LR_CUDA(cudaSetDevice(device));
+        auto ctx = std::make_unique<lr_context>();
+        ctx->device = device;
+        LR_CUDA(cudaDeviceGetAttribute(&ctx->sm_count, cudaDevAttrMultiProcessorCount, device));
+        LR_CUDA(cudaStreamCreateWithFlags(&ctx->stream, cudaStreamNonBlocking));
+        LR_CUDA(cudaEventCreate(&ctx->start));
+        LR_CUDA(cudaEventCreate(&ctx->stop));
+        LR_CUDA(cudaMalloc(&ctx->status, 2 * sizeof(int)));
+        LR_CUDA(cudaMemsetAsync(ctx->status, 0, 2 * sizeof(int), ctx->stream));
+        LR_CUDA(cudaStreamSynchronize(ctx->stream));
+        *out = ctx.release();
+    });
+}
+
+void lr_context_destroy(lr_context *ctx) {
+    if (!ctx) return;
+    cudaSetDevice(ctx->device);
+    if (ctx->stream) cudaStreamSynchronize(ctx->stream);
+    if (ctx->status) cudaFree(ctx->status);
+    if (ctx->start) cudaEventDestroy(ctx->start);
+    if (ctx->stop) cudaEventDestroy(ctx->stop);
+    if (ctx->stream) cudaStreamDestroy(ctx->stream);
+    delete ctx;
+}
+
+int lr_context_synchronize(lr_context *ctx) {
+    return guarded([&] {
+        if (!ctx) fail(LR_INVALID, "no context");
+        LR_CUDA(cudaStreamSynchronize(ctx->stream));
+        check_status(ctx);
+    });
+}
+
+void *lr_context_stream(lr_context *ctx) { return ctx ? (void *)ctx->stream : nullptr; }
+
+int lr_device_alloc(lr_context *ctx, size_t bytes, void **out) {
+    return guarded([&] {
+        if (!ctx || !out) fail(LR_INVALID, "no context");
+        *out = nullptr;
+        LR_CUDA(cudaSetDevice(ctx->device));
+        LR_CUDA(cudaMalloc(out, bytes ? bytes : 16));
+    });
+}
+
+int lr_device_free(lr_context *ctx, void *ptr) {
+    return guarded([&] {
+        if (!ctx) fail(LR_INVALID, "no context");
+        if (ptr) {
+            LR_CUDA(cudaStreamSynchronize(ctx->stream));
+            LR_CUDA(cudaFree(ptr));
+        }
+    });
+}
+
+int lr_memcpy_htod(lr_context *ctx, void *dst, const void *src, size_t bytes) {
+    return guarded([&] {
+        if (!ctx) fail(LR_INVALID, "no context");
+        LR_CUDA(cudaMemcpyAsync(dst, src, bytes, cudaMemcpyHostToDevice, ctx->stream));
+        LR_CUDA(cudaStreamSynchronize(ctx->stream));
+    });
+}
+
+int lr_memcpy_dtoh(lr_context *ctx, void *dst, const void *src, size_t bytes) {
+    return guarded([&] {
+        if (!ctx) fail(LR_INVALID, "no context");
+        LR_CUDA(cudaMemcpyAsync(dst, src, bytes, cudaMemcpyDeviceToHost, ctx->stream));
+        LR_CUDA(cudaStreamSynchronize(ctx->stream));
+    });
+}
+
+int lr_memset_device(lr_context *ctx, void *dst, int value, size_t bytes) {
+    return guarded([&] {
+        if (!ctx) fail(LR_INVALID, "no context");
+        LR_CUDA(cudaMemsetAsync(dst, value, bytes, ctx->stream));
+    });
+}
+
+int lr_host_alloc_pinned(size_t bytes, void **out) {
+    return guarded([&] {
+        if (!out) fail(LR_INVALID, "no place for the pointer");
+        LR_CUDA(cudaMallocHost(out, bytes ? bytes : 16));
+    });
+}
+
+int lr_host_free_pinned(void *ptr) {
+    return guarded([&] {
+        if (ptr) LR_CUDA(cudaFreeHost(ptr));
+    });
+}
+
+int lr_timer_start(lr_context *ctx) {
+    return guarded([&] {
+        if (!ctx) fail(LR_INVALID, "no context");
+        LR_CUDA(cudaEventRecord(ctx->start, ctx->stream));
+    });
+}
+
+int lr_timer_stop(lr_context *ctx, float *ms) {
+    return guarded([&] {
+        if (!ctx || !ms) fail(LR_INVALID, "no context");
+        LR_CUDA(cudaEventRecord(ctx->stop, ctx->stream));
+        LR_CUDA(cudaEventSynchronize(ctx->stop));
+        LR_CUDA(cudaEventElapsedTime(ms, ctx->start, ctx->stop));
+    });
+}
+
+int lr_gpu_scene_upload(lr_context *ctx, const lr_scene *scene, lr_gpu_scene **out) {
+    return guarded([&] {
+        if (!ctx || !scene || !out) fail(LR_INVALID, "upload needs a context and a scene");
+        *out = nullptr;
+        if (scene->nodes.empty()) fail(LR_INVALID, "a scene compiled without its BVH");
+        LR_CUDA(cudaSetDevice(ctx->device));
+        HostLayout L;
+        build_layout(*scene, L);
+        const size_t T = scene->triangle_count(), P = scene->point_count();
+        // One allocation, arrays at 256-byte offsets; empty arrays still get room.
+        struct Part {
+            const void *src;
+            size_t bytes;
+            size_t offset;
+        };
+        std::vector<Part> parts = {
+            {L.entries.data(), L.entries.size() * sizeof(float4), 0},
+            {L.ref_entries.data(), L.ref_entries.size() * sizeof(float4), 0},
+            {L.tris.data(), L.tris.size() * sizeof(float4), 0},
+            {scene->positions.data(), P * 3 * sizeof(float), 0},
+            {scene->indices.data(), T * 3 * sizeof(uint32_t), 0},
+            {scene->faces.data(), T * sizeof(uint32_t), 0},
+            {scene->order.data(), T * sizeof(uint32_t), 0},
+            {L.shading.data(), T * sizeof(uint4), 0},
+        };
+        size_t total = 0;
+        for (auto &p : parts) {
+            p.offset = total;
+            total += align256(std::max<size_t>(p.bytes, 64));
+        }
+        auto gs = std::make_unique<lr_gpu_scene>();
+        gs->ctx = ctx;
+        LR_CUDA(cudaMalloc(&gs->allocation, total));
+        gs->bytes = total;
+        char *base = (char *)gs->allocation;
+        LR_CUDA(cudaMemsetAsync(base, 0, total, ctx->stream));
+        for (auto &p : parts)
+            if (p.bytes) LR_CUDA(cudaMemcpyAsync(base + p.offset, p.src, p.bytes, cudaMemcpyHostToDevice, ctx->stream));
+        LR_CUDA(cudaStreamSynchronize(ctx->stream));
+        DeviceScene &s = gs->scene;
+        s.bvh.entries = (const float4 *)(base + parts[0].offset);
+        s.ref_bvh.entries = (const float4 *)(base + parts[1].offset);
+        s.tris = (const float4 *)(base + parts[2].offset);
+        s.positions = (const float *)(base + parts[3].offset);
+        s.indices = (const uint32_t *)(base + parts[4].offset);
+        s.faces = (const uint32_t *)(base + parts[5].offset);
+        s.ids = (const uint32_t *)(base + parts[6].offset);
+        s.shading = (const uint4 *)(base + parts[7].offset);
+        for (DeviceBvh *b : {&s.bvh, &s.ref_bvh}) {
+            b->root = L.root;
+            b->empty = T == 0 ? 1 : 0;
+            for (int k = 0; k < 3; k++) {
+                b->root_lo[k] = L.root_lo[k];
+                b->root_hi[k] = L.root_hi[k];
+            }
+        }
+        for (int k = 0; k < 3; k++) {
+            s.bvh.root_lo[k] = widen_down(L.root_lo[k], L.delta);
+            s.bvh.root_hi[k] = widen_up(L.root_hi[k], L.delta);
+        }
+        s.triangle_count = T;
+        s.point_count = P;
+        s.entry_count = L.entries.size() / 4;
+        s.depth = scene->bvh_depth;
+        stack_for(s.depth);
+        *out = gs.release();
+    });
+}
+
+void lr_gpu_scene_destroy(lr_gpu_scene *gs) {
+    if (!gs) return;
+    if (gs->ctx) {
+        cudaSetDevice(gs->ctx->device);
+        cudaStreamSynchronize(gs->ctx->stream);
+    }
+    if (gs->allocation) cudaFree(gs->allocation);
+    delete gs;
+}
+
+int lr_probe(lr_context *ctx, const lr_gpu_scene *gs, const lr_frame *frame, uint32_t flags, uint32_t *faces,
+             float *distances) {
+    return guarded([&] {
+        if (!ctx || !gs || !frame || !faces || !distances) fail(LR_INVALID, "a probe needs one result per pixel");
+        if (frame->width == 0 || frame->height == 0) fail(LR_INVALID, "an image needs pixels");
+        const uint64_t count = (uint64_t)frame->width * frame->height;
+        ProbeFrame f;
+        pack_frame(*frame, f.b);
+        LR_CUDA(cudaSetDevice(ctx->device));
+        void *buffer = nullptr;
+        LR_CUDA(cudaMallocAsync(&buffer, count * 8, ctx->stream));
+        uint32_t *d_faces = (uint32_t *)buffer;
+        float *d_ts = (float *)((char *)buffer + count * 4);
+        if (flags & LR_TRACE_REFERENCE)
+            dispatch_probe<true>(gs, f, count, d_faces, d_ts, ctx->status, ctx->stream);
+        else
+            dispatch_probe<false>(gs, f, count, d_faces, d_ts, ctx->status, ctx->stream);
+        LR_CUDA(cudaGetLastError());
+        LR_CUDA(cudaMemcpyAsync(faces, d_faces, count * 4, cudaMemcpyDeviceToHost, ctx->stream));
+        LR_CUDA(cudaMemcpyAsync(distances, d_ts, count * 4, cudaMemcpyDeviceToHost, ctx->stream));
+        LR_CUDA(cudaFreeAsync(buffer, ctx->stream));
+        LR_CUDA(cudaStreamSynchronize(ctx->stream));
+        check_status(ctx);
+    });
+}
+
+static void trace_device(lr_context *ctx, const lr_gpu_scene *gs, const void *rays, uint64_t n, void *hits,
+                         uint32_t flags) {
+    if (n == 0) return;
+    const float4 *r = (const float4 *)rays;
+    float4 *h = (float4 *)hits;
+    const bool any = flags & LR_TRACE_ANY, ref = flags & LR_TRACE_REFERENCE;
+    if (ref && any) dispatch_trace<true, true>(gs, r, n, h, ctx->status, ctx->stream);
+    else if (ref) dispatch_trace<true, false>(gs, r, n, h, ctx->status, ctx->stream);
+    else if (any) dispatch_trace<false, true>(gs, r, n, h, ctx->status, ctx->stream);
+    else dispatch_trace<false, false>(gs, r, n, h, ctx->status, ctx->stream);
+    LR_CUDA(cudaGetLastError());
+}
+
+int lr_trace_rays(lr_context *ctx, const lr_gpu_scene *gs, const float *rays, uint64_t count, float *hits,
+                  uint32_t flags) {
+    return guarded([&] {
+        if (!ctx || !gs || (count && (!rays || !hits))) fail(LR_INVALID, "a ray query needs rays and room for hits");
+        if (count == 0) return;
+        LR_CUDA(cudaSetDevice(ctx->device));
+        void *buffer = nullptr;
+        LR_CUDA(cudaMallocAsync(&buffer, count * 48, ctx->stream));
+        void *d_hits = (char *)buffer + count * 32;
+        LR_CUDA(cudaMemcpyAsync(buffer, rays, count * 32, cudaMemcpyHostToDevice, ctx->stream));
+        trace_device(ctx, gs, buffer, count, d_hits, flags);
+        LR_CUDA(cudaMemcpyAsync(hits, d_hits, count * 16, cudaMemcpyDeviceToHost, ctx->stream));
+        LR_CUDA(cudaFreeAsync(buffer, ctx->stream));
+        LR_CUDA(cudaStreamSynchronize(ctx->stream));
+        check_status(ctx);
+    });
+}
+
+int lr_trace_rays_device(lr_context *ctx, const lr_gpu_scene *gs, const void *rays, uint64_t count, void *hits,
+                         uint32_t flags) {
+    return guarded([&] {
+        if (!ctx || !gs || (count && (!rays || !hits))) fail(LR_INVALID, "a ray query needs rays and room for hits");
+        if (((uintptr_t)rays & 15) || ((uintptr_t)hits & 15)) fail(LR_INVALID, "rays and hits must be 16-byte aligned");
+        trace_device(ctx, gs, rays, count, hits, flags);
+    });
+}
+
+}  // extern "C"

@@ -1,0 +1,69 @@
+// Device-side state shared by the CUDA translation units: the context (device + stream
+// + timing events), the scene as it lives in HBM, and CUDA error checking.
+#pragma once
+
+#include <cuda_runtime.h>
+
+#include <string>
+
+#include "common.hpp"
+
+namespace lr {
+
+#define LR_CUDA(call)                                                                      \
+    do {                                                                                   \
+        cudaError_t lr_status_ = (call);                                                   \
+        if (lr_status_ != cudaSuccess)                                                     \
+            ::lr::fail(LR_DEVICE, std::string(#call) + ": " + cudaGetErrorString(lr_status_)); \
+    } while (0)
+
+// Leaf links: a child link >= 0 is an interior entry; a negative link is a leaf whose
+// triangles are `first .. first + count` in leaf order, packed as -1 - (first << 4 | count - 1).
+constexpr int kLeafShift = 4;
+constexpr uint32_t kMaxLeafFirst = (1u << (31 - kLeafShift)) - 1;
+
+// The BVH2 in traversal form: one 64-byte entry per interior node holding both children's
+// boxes and links (the 64 bytes an interior visit reads), plus the root's box and link.
+struct DeviceBvh {
+    const float4 *entries = nullptr;  // 4 float4 per interior node
+    float root_lo[3] = {1, 1, 1}, root_hi[3] = {-1, -1, -1};
+    int root = 0;                      // root link (entry 0, or a leaf link)
+    int empty = 1;                     // no triangles: every ray misses
+};
+
+// A scene in HBM (GpuScene, device.lucb:16-38).
+struct DeviceScene {
+    DeviceBvh bvh;        // boxes widened outward for the watertight path
+    DeviceBvh ref_bvh;    // the reference's exact boxes (LR_TRACE_REFERENCE)
+    const float4 *tris = nullptr;      // 3 float4 per leaf slot: v0 (w: source id bits), v1, v2
+    const float *positions = nullptr;  // xyz per point
+    const uint32_t *indices = nullptr; // 3 per leaf slot
+    const uint32_t *faces = nullptr;   // polygon per leaf slot
+    const uint32_t *ids = nullptr;     // source triangle per leaf slot
+    const uint4 *shading = nullptr;    // 3 octahedral normals + material per leaf slot
+    uint64_t triangle_count = 0, point_count = 0, entry_count = 0;
+    uint32_t depth = 0;                // the BVH2's deepest leaf
+};
+
+}  // namespace lr
+
+struct lr_context {
+    int device = 0;
+    cudaStream_t stream = nullptr;
+    cudaEvent_t start = nullptr, stop = nullptr;
+    int sm_count = 148;
+    // Device status words: [0] traversal stack pushes lost, [1] bounded waits that gave up.
+    int *status = nullptr;
+};
+
+namespace lr {
+// Reads and clears the context's status words; fails when one is set.
+void check_status(lr_context *ctx);
+}  // namespace lr
+
+struct lr_gpu_scene {
+    lr_context *ctx = nullptr;
+    lr::DeviceScene scene;
+    void *allocation = nullptr;  // one device block holds every array
+    size_t bytes = 0;
+};

@@ -1,0 +1,324 @@
+// Ray traversal of the BVH2 on sm_100a: the device half of probe, the ray queries and
+// the integrator's closest-hit and shadow kernels.
+//
+// Two triangle tests share one traversal loop:
+//   - the default, watertight FP32 test (Woop, Benthin and Wald, JCGT 2013) over
+//     48-byte triangle records, with boxes widened outward and slab exits scaled up
+//     so the box test never culls a hit the triangle test would report; ties in t
+//     go to the smaller source triangle id, so the closest hit does not depend on
+//     the visiting order and equals an FP32 brute force over all triangles;
+//   - the reference's own Moller-Trumbore test and box test (shaders/bvh.glsl:17-90)
+//     over exact boxes, visiting nearer children first and keeping the first tested
+//     on equal t, for bit-level parity with the reference's traversal.
+// All arithmetic that decides a hit or a distance uses explicitly rounded intrinsics,
+// so no multiply-add contraction changes a result between this code and its CPU
+// restatement.
+#pragma once
+
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+#include "device.hpp"
+
+namespace lr {
+
+constexpr float kNoHitT = 3.0e38f;
+
+struct Ray {
+    float3 o;
+    float tmin;
+    float3 d;
+    float tmax;
+};
+
+struct Hit {
+    float t;
+    int id;    // source triangle id, -1 none
+    int slot;  // leaf slot, -1 none
+    float u, v;
+};
+
+__device__ __forceinline__ float fmul_(float a, float b) { return __fmul_rn(a, b); }
+__device__ __forceinline__ float fadd_(float a, float b) { return __fadd_rn(a, b); }
+__device__ __forceinline__ float fsub_(float a, float b) { return __fsub_rn(a, b); }
+__device__ __forceinline__ float comp(const float3 &v, int k) { return k == 0 ? v.x : (k == 1 ? v.y : v.z); }
+
+// bvh.glsl:55-56: components below 1e-20 in magnitude become +-1e-20 (+ for zero).
+__device__ __forceinline__ float3 safe_inverse(float3 d) {
+    auto one = [](float x) {
+        if (fabsf(x) < 1e-20f) x = x > 0.0f ? 1e-20f : (x < 0.0f ? -1e-20f : 1e-20f);
+        return __frcp_rn(x);
+    };
+    return make_float3(one(d.x), one(d.y), one(d.z));
+}
+
+// The ray's shear for the watertight test: kz the largest |d| component (the first on
+// ties), kx and ky the next two (swapped when d[kz] < 0).
+struct Shear {
+    int kx, ky, kz;
+    float sx, sy, sz;
+    float ox, oy, oz;  // the origin's permuted components
+};
+
+__device__ __forceinline__ Shear make_shear(float3 o, float3 d) {
+    Shear s;
+    int kz = 0;
+    if (fabsf(d.y) > fabsf(comp(d, kz))) kz = 1;
+    if (fabsf(d.z) > fabsf(comp(d, kz))) kz = 2;
+    int kx = kz == 2 ? 0 : kz + 1;
+    int ky = kx == 2 ? 0 : kx + 1;
+    if (comp(d, kz) < 0.0f) {
+        int t = kx;
+        kx = ky;
+        ky = t;
+    }
+    float dz = comp(d, kz);
+    s.kx = kx;
+    s.ky = ky;
+    s.kz = kz;
+    s.sx = __fdiv_rn(comp(d, kx), dz);
+    s.sy = __fdiv_rn(comp(d, ky), dz);
+    s.sz = __frcp_rn(dz);
+    s.ox = comp(o, kx);
+    s.oy = comp(o, ky);
+    s.oz = comp(o, kz);
+    return s;
+}
+
+// One triangle, watertight; true with t in (tmin, tmax).
+__device__ __forceinline__ bool watertight(const Shear &s, float tmin, float tmax, float4 a4, float4 b4,
+                                           float4 c4, float &t_out, float &u_out, float &v_out) {
+    float3 a = make_float3(a4.x, a4.y, a4.z), b = make_float3(b4.x, b4.y, b4.z),
+           c = make_float3(c4.x, c4.y, c4.z);
+    float Ax = fsub_(comp(a, s.kx), s.ox), Ay = fsub_(comp(a, s.ky), s.oy), Az = fsub_(comp(a, s.kz), s.oz);
+    float Bx = fsub_(comp(b, s.kx), s.ox), By = fsub_(comp(b, s.ky), s.oy), Bz = fsub_(comp(b, s.kz), s.oz);
+    float Cx = fsub_(comp(c, s.kx), s.ox), Cy = fsub_(comp(c, s.ky), s.oy), Cz = fsub_(comp(c, s.kz), s.oz);
+    float ax = fsub_(Ax, fmul_(s.sx, Az)), ay = fsub_(Ay, fmul_(s.sy, Az));
+    float bx = fsub_(Bx, fmul_(s.sx, Bz)), by = fsub_(By, fmul_(s.sy, Bz));
+    float cx = fsub_(Cx, fmul_(s.sx, Cz)), cy = fsub_(Cy, fmul_(s.sy, Cz));
+    float U = fsub_(fmul_(cx, by), fmul_(cy, bx));
+    float V = fsub_(fmul_(ax, cy), fmul_(ay, cx));
+    float W = fsub_(fmul_(bx, ay), fmul_(by, ax));
+    if (U == 0.0f || V == 0.0f || W == 0.0f) {
+        // Edge functions at exactly zero: settle them in double (the products of two
+        // floats are exact there), as Woop et al. prescribe.
+        U = __double2float_rn(__dsub_rn(__dmul_rn(cx, by), __dmul_rn(cy, bx)));
+        V = __double2float_rn(__dsub_rn(__dmul_rn(ax, cy), __dmul_rn(ay, cx)));
+        W = __double2float_rn(__dsub_rn(__dmul_rn(bx, ay), __dmul_rn(by, ax)));
+    }
+    if ((U < 0.0f || V < 0.0f || W < 0.0f) && (U > 0.0f || V > 0.0f || W > 0.0f)) return false;
+    float det = fadd_(fadd_(U, V), W);
+    if (det == 0.0f) return false;
+    float az = fmul_(s.sz, Az), bz = fmul_(s.sz, Bz), cz = fmul_(s.sz, Cz);
+    float T = fadd_(fadd_(fmul_(U, az), fmul_(V, bz)), fmul_(W, cz));
+    float rcp = __frcp_rn(det);
+    float t = fmul_(T, rcp);
+    if (!(t > tmin && t < tmax)) return false;
+    t_out = t;
+    u_out = fmul_(V, rcp);
+    v_out = fmul_(W, rcp);
+    return true;
+}
+
+// The slab test of the watertight path: exits scaled by 1 + 2*gamma(3) (Ize 2013),
+// boxes already widened at upload. Returns the entry, or a negative value on a miss.
+__device__ __forceinline__ bool box_exact(float lox, float hix, float loy, float hiy, float loz, float hiz,
+                                          const float3 &o, const float3 &inv, float tmin, float tmax,
+                                          float &enter) {
+    const float kScale = 1.0000003576f;
+    float x0 = fmul_(fsub_(lox, o.x), inv.x), x1 = fmul_(fsub_(hix, o.x), inv.x);
+    float y0 = fmul_(fsub_(loy, o.y), inv.y), y1 = fmul_(fsub_(hiy, o.y), inv.y);
+    float z0 = fmul_(fsub_(loz, o.z), inv.z), z1 = fmul_(fsub_(hiz, o.z), inv.z);
+    float e = fmaxf(fmaxf(fminf(x0, x1), fminf(y0, y1)), fmaxf(fminf(z0, z1), tmin));
+    float l = fminf(fminf(fmaxf(x0, x1), fmaxf(y0, y1)), fminf(fmaxf(z0, z1), tmax)) * kScale;
+    enter = e;
+    return e <= l;
+}
+
+// box_entry (bvh.glsl:17-25), exactly: the entry (0 when inside) or -1.
+__device__ __forceinline__ float box_reference(float lox, float hix, float loy, float hiy, float loz, float hiz,
+                                               const float3 &o, const float3 &inv, float t_max) {
+    float x0 = fmul_(fsub_(lox, o.x), inv.x), x1 = fmul_(fsub_(hix, o.x), inv.x);
+    float y0 = fmul_(fsub_(loy, o.y), inv.y), y1 = fmul_(fsub_(hiy, o.y), inv.y);
+    float z0 = fmul_(fsub_(loz, o.z), inv.z), z1 = fmul_(fsub_(hiz, o.z), inv.z);
+    float enter = fmaxf(fmaxf(fminf(x0, x1), fminf(y0, y1)), fmaxf(fminf(z0, z1), 0.0f));
+    float leave = fminf(fminf(fmaxf(x0, x1), fmaxf(y0, y1)), fminf(fmaxf(z0, z1), t_max));
+    return enter <= leave ? enter : -1.0f;
+}
+
+__device__ __forceinline__ float3 point_at(const float *p, uint32_t i) {
+    return make_float3(__ldg(&p[i * 3]), __ldg(&p[i * 3 + 1]), __ldg(&p[i * 3 + 2]));
+}
+
+__device__ __forceinline__ float3 sub3(float3 a, float3 b) { return make_float3(fsub_(a.x, b.x), fsub_(a.y, b.y), fsub_(a.z, b.z)); }
+__device__ __forceinline__ float3 cross3(float3 a, float3 b) {
+    return make_float3(fsub_(fmul_(a.y, b.z), fmul_(a.z, b.y)), fsub_(fmul_(a.z, b.x), fmul_(a.x, b.z)),
+                       fsub_(fmul_(a.x, b.y), fmul_(a.y, b.x)));
+}
+__device__ __forceinline__ float dot3(float3 a, float3 b) {
+    return fadd_(fadd_(fmul_(a.x, b.x), fmul_(a.y, b.y)), fmul_(a.z, b.z));
+}
+
+// triangle_hit (bvh.glsl:27-47), exactly.
+__device__ __forceinline__ bool triangle_reference(const DeviceScene &s, uint32_t slot, const float3 &o,
+                                                   const float3 &d, Hit &hit) {
+    float3 p0 = point_at(s.positions, __ldg(&s.indices[slot * 3]));
+    float3 e1 = sub3(point_at(s.positions, __ldg(&s.indices[slot * 3 + 1])), p0);
+    float3 e2 = sub3(point_at(s.positions, __ldg(&s.indices[slot * 3 + 2])), p0);
+    float3 p = cross3(d, e2);
+    float determinant = dot3(e1, p);
+    if (fabsf(determinant) < 1e-20f) return false;
+    float inverse = __frcp_rn(determinant);
+    float3 sv = sub3(o, p0);
+    float u = fmul_(dot3(sv, p), inverse);
+    if (u < 0.0f || u > 1.0f) return false;
+    float3 q = cross3(sv, e1);
+    float v = fmul_(dot3(d, q), inverse);
+    if (v < 0.0f || fadd_(u, v) > 1.0f) return false;
+    float t = fmul_(dot3(e2, q), inverse);
+    if (t <= 0.0f || t >= hit.t) return false;
+    hit.t = t;
+    hit.slot = (int)slot;
+    hit.u = u;
+    hit.v = v;
+    return true;
+}
+
+__device__ __forceinline__ void leaf_range(int link, uint32_t &first, uint32_t &count) {
+    uint32_t code = (uint32_t)(-1 - link);
+    first = code >> kLeafShift;
+    count = (code & ((1u << kLeafShift) - 1)) + 1;
+}
+
+// The stack lives in shared memory, one column per thread: element k of thread i at
+// stack[k * stride + i]. `overflow` counts pushes past kStack (never expected: the host
+// picks kStack above the tree's depth).
+template <int kStack>
+struct SharedStack {
+    int *base;
+    int stride;
+    int sp = 0;
+    __device__ __forceinline__ SharedStack(int *b, int s) : base(b), stride(s) {}
+    __device__ __forceinline__ bool push(int v) {
+        if (sp >= kStack) return false;
+        base[sp * stride] = v;
+        sp++;
+        return true;
+    }
+    __device__ __forceinline__ int pop() { return base[--sp * stride]; }
+    __device__ __forceinline__ bool empty() const { return sp == 0; }
+};
+
+// The closest (or any) hit along r, watertight. `overflow` is set when a push was lost.
+template <bool kAny, int kStack>
+__device__ __forceinline__ Hit trace_exact(const DeviceScene &s, const Ray &r, int *stack_base, int stride,
+                                           bool &overflow) {
+    Hit h{r.tmax, -1, -1, 0.0f, 0.0f};
+    const DeviceBvh &b = s.bvh;
+    if (b.empty) return h;
+    const float3 inv = safe_inverse(r.d);
+    const Shear sh = make_shear(r.o, r.d);
+    float enter;
+    if (!box_exact(b.root_lo[0], b.root_hi[0], b.root_lo[1], b.root_hi[1], b.root_lo[2], b.root_hi[2], r.o, inv,
+                   r.tmin, r.tmax, enter))
+        return h;
+    SharedStack<kStack> st(stack_base, stride);
+    int node = b.root;
+    for (;;) {
+        while (node >= 0) {
+            const float4 *e = b.entries + (size_t)node * 4;
+            const float4 n0 = __ldg(e), n1 = __ldg(e + 1), n2 = __ldg(e + 2), n3 = __ldg(e + 3);
+            float ea, eb;
+            const bool ha = box_exact(n0.x, n0.y, n0.z, n0.w, n2.x, n2.y, r.o, inv, r.tmin, h.t, ea);
+            const bool hb = box_exact(n1.x, n1.y, n1.z, n1.w, n2.z, n2.w, r.o, inv, r.tmin, h.t, eb);
+            const int l0 = __float_as_int(n3.x), l1 = __float_as_int(n3.y);
+            if (ha && hb) {
+                const bool left_first = ea <= eb;
+                if (!st.push(left_first ? l1 : l0)) overflow = true;
+                node = left_first ? l0 : l1;
+            } else if (ha) {
+                node = l0;
+            } else if (hb) {
+                node = l1;
+            } else {
+                if (st.empty()) return h;
+                node = st.pop();
+            }
+        }
+        uint32_t first, count;
+        leaf_range(node, first, count);
+        for (uint32_t i = 0; i < count; i++) {
+            const float4 *tri = s.tris + (size_t)(first + i) * 3;
+            const float4 a = __ldg(tri), bb = __ldg(tri + 1), c = __ldg(tri + 2);
+            // Equal t may still win on a smaller id: test up to the next float above h.t.
+            const float limit = h.id >= 0 ? __int_as_float(__float_as_int(h.t) + 1) : r.tmax;
+            float t, u, v;
+            if (!watertight(sh, r.tmin, limit, a, bb, c, t, u, v)) continue;
+            const int id = __float_as_int(a.w);
+            if (h.id >= 0 && t == h.t && id > h.id) continue;
+            h.t = t;
+            h.id = id;
+            h.slot = (int)(first + i);
+            h.u = u;
+            h.v = v;
+            if (kAny) return h;
+        }
+        if (st.empty()) return h;
+        node = st.pop();
+    }
+}
+
+// trace_closest / trace_any (bvh.glsl:51-122) over the reference's exact boxes.
+template <bool kAny, int kStack>
+__device__ __forceinline__ Hit trace_reference(const DeviceScene &s, const Ray &r, int *stack_base, int stride,
+                                               bool &overflow) {
+    Hit h{r.tmax, -1, -1, 0.0f, 0.0f};
+    const DeviceBvh &b = s.ref_bvh;
+    if (b.empty) return h;
+    const float3 inv = safe_inverse(r.d);
+    if (box_reference(b.root_lo[0], b.root_hi[0], b.root_lo[1], b.root_hi[1], b.root_lo[2], b.root_hi[2], r.o,
+                      inv, h.t) < 0.0f)
+        return h;
+    SharedStack<kStack> st(stack_base, stride);
+    int node = b.root;
+    for (;;) {
+        if (node < 0) {
+            uint32_t first, count;
+            leaf_range(node, first, count);
+            for (uint32_t i = 0; i < count; i++) {
+                if (triangle_reference(s, first + i, r.o, r.d, h) && kAny) {
+                    h.id = (int)__ldg(&s.ids[h.slot]);
+                    return h;
+                }
+            }
+        } else {
+            const float4 *e = b.entries + (size_t)node * 4;
+            const float4 n0 = __ldg(e), n1 = __ldg(e + 1), n2 = __ldg(e + 2), n3 = __ldg(e + 3);
+            const float tl = kAny ? r.tmax : h.t;
+            const float a = box_reference(n0.x, n0.y, n0.z, n0.w, n2.x, n2.y, r.o, inv, tl);
+            const float bb = box_reference(n1.x, n1.y, n1.z, n1.w, n2.z, n2.w, r.o, inv, tl);
+            const int l0 = __float_as_int(n3.x), l1 = __float_as_int(n3.y);
+            const bool take_left = a >= 0.0f, take_right = bb >= 0.0f;
+            if (take_left && take_right) {
+                const bool left_near = kAny ? true : a <= bb;
+                if (!st.push(left_near ? l1 : l0)) overflow = true;
+                node = left_near ? l0 : l1;
+                continue;
+            }
+            if (take_left) {
+                node = l0;
+                continue;
+            }
+            if (take_right) {
+                node = l1;
+                continue;
+            }
+        }
+        if (st.empty()) break;
+        node = st.pop();
+    }
+    if (h.slot >= 0) h.id = (int)__ldg(&s.ids[h.slot]);
+    return h;
+}
+
+}  // namespace lr

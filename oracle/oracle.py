@@ -1,0 +1,340 @@
+"""ctypes binding of the CPU oracle (oracle/_build/liboracle.so): TEST INFRASTRUCTURE.
+
+Only tests/, the smoke check and bench.py's CPU-baseline leg use this module, as the
+checker and the CPU baseline; the product never does. Build with ``make -C oracle``.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+import subprocess
+from pathlib import Path
+
+import numpy as np
+
+HERE = Path(__file__).resolve().parent
+LIB_PATH = HERE / "_build" / "liboracle.so"
+
+
+def build() -> Path:
+    subprocess.run(["make", "-s", "-C", str(HERE)], check=True)
+    return LIB_PATH
+
+
+def _load() -> C.CDLL:
+    if not LIB_PATH.exists():
+        build()
+    return C.CDLL(str(LIB_PATH))
+
+
+lib = _load()
+
+NODE_DTYPE = np.dtype([("lo", "<f4", 3), ("first", "<u4"), ("hi", "<f4", 3), ("count", "<u4")])
+HIT_DTYPE = np.dtype([("t", "<f4"), ("triangle", "<u4"), ("u", "<f4"), ("v", "<f4")])
+
+
+class Counts(C.Structure):
+    _fields_ = [("interior", C.c_uint64), ("triangles", C.c_uint64), ("dropped", C.c_uint64)]
+
+
+class OrFrame(C.Structure):
+    _fields_ = [("position", C.c_double * 3), ("corner", C.c_double * 3), ("du", C.c_double * 3),
+                ("dv", C.c_double * 3), ("forward", C.c_double * 3), ("orthographic", C.c_int),
+                ("width", C.c_uint32), ("height", C.c_uint32), ("lens_radius", C.c_double),
+                ("focus_distance", C.c_double)]
+
+
+class OrLight(C.Structure):
+    _fields_ = [("matrix", C.c_double * 12), ("shape", C.c_int), ("color", C.c_double * 3),
+                ("intensity", C.c_double), ("exposure", C.c_double), ("temperature", C.c_double),
+                ("width", C.c_double), ("height", C.c_double), ("radius", C.c_double), ("angle", C.c_double),
+                ("normalize", C.c_int), ("visible", C.c_int)]
+
+
+class OrMaterial(C.Structure):
+    _fields_ = [("base_weight", C.c_double), ("base_color", C.c_double * 3), ("base_metalness", C.c_double),
+                ("base_diffuse_roughness", C.c_double), ("specular_weight", C.c_double),
+                ("specular_color", C.c_double * 3), ("specular_roughness", C.c_double),
+                ("specular_roughness_anisotropy", C.c_double), ("specular_ior", C.c_double),
+                ("transmission_weight", C.c_double), ("transmission_color", C.c_double * 3),
+                ("coat_weight", C.c_double), ("coat_color", C.c_double * 3), ("coat_roughness", C.c_double),
+                ("coat_roughness_anisotropy", C.c_double), ("coat_ior", C.c_double),
+                ("coat_darkening", C.c_double), ("emission_luminance", C.c_double),
+                ("emission_color", C.c_double * 3), ("geometry_opacity", C.c_double),
+                ("geometry_thin_walled", C.c_int), ("transmission_dispersion_scale", C.c_double),
+                ("transmission_dispersion_abbe_number", C.c_double)]
+
+
+class OrTree(C.Structure):
+    _fields_ = [("nodes", C.POINTER(C.c_float)), ("links", C.POINTER(C.c_uint32)),
+                ("records", C.POINTER(C.c_uint32)), ("node_count", C.c_size_t),
+                ("emitter_count", C.c_size_t), ("triangle_count", C.c_size_t), ("energy", C.c_double)]
+
+
+def _p(a, ctype):
+    return a.ctypes.data_as(C.POINTER(ctype))
+
+
+_f, _u, _d = C.c_float, C.c_uint32, C.c_double
+lib.or_build_bvh.restype = C.c_size_t
+lib.or_bvh_depth.restype = C.c_uint32
+lib.or_hash_u32.restype = C.c_uint32
+lib.or_hash_combine.restype = C.c_uint32
+lib.or_sobol.restype = C.c_uint32
+lib.or_sobol_directions.restype = C.POINTER(C.c_uint32)
+lib.or_octahedral.restype = C.c_uint32
+lib.or_blackbody.restype = C.c_double
+lib.or_blackbody.argtypes = [C.c_double, C.c_double]
+lib.or_wavelength_pdf.restype = C.c_double
+lib.or_wavelength_pdf.argtypes = [C.c_double]
+lib.or_sample_wavelengths.argtypes = [C.c_double, C.POINTER(C.c_double)]
+lib.or_pack_lights.restype = C.c_size_t
+lib.or_pack_lights.argtypes = [C.POINTER(OrLight), C.c_size_t, C.c_double, C.POINTER(C.c_float),
+                               C.POINTER(C.c_double)]
+lib.or_ray_frame.argtypes = [C.POINTER(C.c_double), C.c_int, C.c_double, C.c_double, C.c_double, C.c_double,
+                             C.c_uint32, C.c_uint32, C.POINTER(OrFrame)]
+lib.or_look_frame.argtypes = [C.POINTER(C.c_double), C.POINTER(C.c_double), C.POINTER(C.c_double), C.c_double,
+                              C.c_uint32, C.c_uint32, C.c_int, C.POINTER(OrFrame)]
+
+
+def build_bvh(positions: np.ndarray, indices: np.ndarray):
+    """The reference's BVH (bvh.lucb:66-217): nodes, order, and indices in leaf order."""
+    positions = np.ascontiguousarray(positions, np.float32)
+    indices = np.ascontiguousarray(indices, np.uint32).reshape(-1, 3)
+    T = len(indices)
+    nodes = np.zeros(2 * max(T, 1), NODE_DTYPE)
+    order = np.zeros(max(T, 1), np.uint32)
+    n = lib.or_build_bvh(_p(positions, _f), _p(indices, _u), C.c_size_t(T), nodes.ctypes.data_as(C.c_void_p),
+                         _p(order, _u))
+    return nodes[:n].copy(), order[:T].copy()
+
+
+def bvh_depth(nodes: np.ndarray) -> int:
+    return int(lib.or_bvh_depth(nodes.ctypes.data_as(C.c_void_p), C.c_size_t(len(nodes))))
+
+
+def trace(nodes, positions, indices, rays, any_hit=False, stack_limit=0, threads=0):
+    """The reference's trace_closest / trace_any (bvh.glsl:51-122) over rays (n x 8).
+    Returns (hits or booleans, Counts)."""
+    rays = np.ascontiguousarray(rays, np.float32)
+    positions = np.ascontiguousarray(positions, np.float32)
+    indices = np.ascontiguousarray(indices, np.uint32)
+    nodes = np.ascontiguousarray(nodes, NODE_DTYPE)
+    n = len(rays)
+    counts = Counts()
+    if any_hit:
+        out = np.zeros(n, np.uint8)
+        lib.or_trace_any_batch(nodes.ctypes.data_as(C.c_void_p), _p(positions, _f), _p(indices, _u), _p(rays, _f),
+                               C.c_size_t(n), stack_limit, _p(out, C.c_uint8), C.byref(counts), threads)
+    else:
+        out = np.zeros(n, HIT_DTYPE)
+        lib.or_trace_closest_batch(nodes.ctypes.data_as(C.c_void_p), _p(positions, _f), _p(indices, _u),
+                                   _p(rays, _f), C.c_size_t(n), stack_limit, out.ctypes.data_as(C.c_void_p),
+                                   C.byref(counts), threads)
+    return out, counts
+
+
+def nearest_f64(positions, indices, faces, rays, threads=0):
+    """tests/gpu/main.lucb:82-119 per ray: (face or -1, distance, margin)."""
+    rays = np.ascontiguousarray(rays, np.float32)
+    positions = np.ascontiguousarray(positions, np.float32)
+    indices = np.ascontiguousarray(indices, np.uint32)
+    faces = np.ascontiguousarray(faces, np.uint32)
+    n = len(rays)
+    face = np.zeros(n, np.int64)
+    dist = np.zeros(n, np.float64)
+    margin = np.zeros(n, np.float64)
+    lib.or_nearest_f64(_p(positions, _f), _p(indices, _u), _p(faces, _u), C.c_size_t(len(indices)), _p(rays, _f),
+                       C.c_size_t(n), _p(face, C.c_int64), _p(dist, _d), _p(margin, _d), threads)
+    return face, dist, margin
+
+
+def brute_watertight(positions, indices, ids, rays, any_hit=False, threads=0):
+    """FP32 watertight brute force: (prim int32, t, u, v)."""
+    rays = np.ascontiguousarray(rays, np.float32)
+    positions = np.ascontiguousarray(positions, np.float32)
+    indices = np.ascontiguousarray(indices, np.uint32)
+    n = len(rays)
+    prim = np.zeros(n, np.int32)
+    t = np.zeros(n, np.float32)
+    u = np.zeros(n, np.float32)
+    v = np.zeros(n, np.float32)
+    ids_p = None if ids is None else _p(np.ascontiguousarray(ids, np.uint32), _u)
+    lib.or_brute_watertight(_p(positions, _f), _p(indices, _u), ids_p, C.c_size_t(len(indices)), _p(rays, _f),
+                            C.c_size_t(n), 1 if any_hit else 0, _p(prim, C.c_int32), _p(t, _f), _p(u, _f), _p(v, _f),
+                            threads)
+    return prim, t, u, v
+
+
+def probe_rays(block16: np.ndarray) -> np.ndarray:
+    b = np.ascontiguousarray(block16, np.float32)
+    w, h = int(b[11]), int(b[15])
+    rays = np.zeros((w * h, 8), np.float32)
+    lib.or_probe_rays(_p(b, _f), _p(rays, _f))
+    return rays
+
+
+def frame_of_camera(matrix12, projection, focal_length, horizontal_aperture, f_stop, focus_distance, w, h):
+    f = OrFrame()
+    m = (C.c_double * 12)(*[float(v) for v in matrix12])
+    status = lib.or_ray_frame(m, projection, focal_length, horizontal_aperture, f_stop, focus_distance, w, h,
+                              C.byref(f))
+    return status, f
+
+
+def look_frame(position, forward, up, tan_half_height, w, h, orthographic=False):
+    f = OrFrame()
+    p, fw, u = ((C.c_double * 3)(*map(float, v)) for v in (position, forward, up))
+    status = lib.or_look_frame(p, fw, u, tan_half_height, w, h, 1 if orthographic else 0, C.byref(f))
+    return status, f
+
+
+def frame_pack(f: OrFrame) -> np.ndarray:
+    out = np.zeros(16, np.float32)
+    lib.or_frame_pack(C.byref(f), _p(out, _f))
+    return out
+
+
+def frame_ray(f: OrFrame, x, y):
+    o = (C.c_double * 3)()
+    d = (C.c_double * 3)()
+    lib.or_frame_ray(C.byref(f), C.c_double(x), C.c_double(y), o, d)
+    return np.array(o[:]), np.array(d[:])
+
+
+def sobol_directions() -> np.ndarray:
+    p = lib.or_sobol_directions()
+    return np.array([p[i] for i in range(128)], np.uint32)
+
+
+def sample4_bits(seed, pixel, index, group) -> np.ndarray:
+    out = (C.c_uint32 * 4)()
+    lib.or_sample4_bits(C.c_uint32(seed), C.c_uint32(pixel), C.c_uint32(index), C.c_uint32(group), out)
+    return np.array(out[:], np.uint32)
+
+
+def hash_u32(x: int) -> int:
+    return int(lib.or_hash_u32(C.c_uint32(x)))
+
+
+def film_matrix() -> np.ndarray:
+    out = (C.c_double * 9)()
+    lib.or_film_matrix(out)
+    return np.array(out[:]).reshape(3, 3)
+
+
+def acescg_to_xyz_e() -> np.ndarray:
+    out = (C.c_double * 9)()
+    lib.or_acescg_to_xyz_e(out)
+    return np.array(out[:]).reshape(3, 3)
+
+
+def cmf(lam: float) -> np.ndarray:
+    out = (C.c_double * 3)()
+    lib.or_cmf(C.c_double(lam), out)
+    return np.array(out[:])
+
+
+def cmf_integrals() -> np.ndarray:
+    out = (C.c_double * 3)()
+    lib.or_cmf_integrals(out)
+    return np.array(out[:])
+
+
+def fit_spectrum(rgb) -> np.ndarray:
+    out = (C.c_double * 4)()
+    lib.or_fit_spectrum((C.c_double * 3)(*map(float, rgb)), out)
+    return np.array(out[:])
+
+
+def blackbody_xyz(kelvin: float) -> np.ndarray:
+    out = (C.c_double * 3)()
+    lib.or_blackbody_xyz(C.c_double(kelvin), out)
+    return np.array(out[:])
+
+
+def sample_wavelengths(u: float) -> np.ndarray:
+    out = (C.c_double * 4)()
+    lib.or_sample_wavelengths(u, out)
+    return np.array(out[:])
+
+
+def wavelength_pdf(lam: float) -> float:
+    return float(lib.or_wavelength_pdf(lam))
+
+
+def octahedral(n) -> int:
+    return int(lib.or_octahedral((C.c_double * 3)(*map(float, n))))
+
+
+def octahedral_decode(packed: int) -> np.ndarray:
+    out = (C.c_double * 3)()
+    lib.or_octahedral_decode(C.c_uint32(packed), out)
+    return np.array(out[:])
+
+
+def material_standard() -> OrMaterial:
+    m = OrMaterial()
+    lib.or_material_standard(C.byref(m))
+    return m
+
+
+def material_from(openpbr) -> OrMaterial:
+    """An oracle material with the same fields as a luce_render_b200.OpenPbr."""
+    m = OrMaterial()
+    for name, _ in OrMaterial._fields_:
+        value = getattr(openpbr, name)
+        if hasattr(value, "__len__"):
+            getattr(m, name)[:] = list(value)
+        else:
+            setattr(m, name, value)
+    return m
+
+
+def pack_material(m: OrMaterial, program: float = -1.0) -> np.ndarray:
+    out = np.zeros(64, np.float32)
+    lib.or_pack_material(C.byref(m), C.c_float(program), _p(out, _f))
+    return out
+
+
+def light_from(l) -> OrLight:
+    o = OrLight()
+    for name, _ in OrLight._fields_:
+        value = getattr(l, name)
+        if hasattr(value, "__len__"):
+            getattr(o, name)[:] = list(value)
+        else:
+            setattr(o, name, value)
+    return o
+
+
+def pack_lights(lights, radius: float):
+    arr = (OrLight * max(1, len(lights)))(*[light_from(l) for l in lights])
+    out = np.zeros(max(1, len(lights)) * 28, np.float32)
+    power = C.c_double()
+    n = lib.or_pack_lights(arr, len(lights), radius, _p(out, _f), C.byref(power))
+    return out[: n * 28].reshape(-1, 28).copy(), power.value
+
+
+def light_tree(positions, indices, shading, light_rows, materials):
+    """build_light_tree (light_tree.lucb:91-199): dict of nodes, links, records, counts."""
+    positions = np.ascontiguousarray(positions, np.float32)
+    indices = np.ascontiguousarray(indices, np.uint32)
+    shading = np.ascontiguousarray(shading, np.uint32)
+    rows = np.ascontiguousarray(light_rows, np.float32).reshape(-1)
+    lib_mats = (OrMaterial * max(1, len(materials)))(*materials)
+    tree = OrTree()
+    T = len(indices) // 3 if indices.ndim == 1 else len(indices)
+    lib.or_build_light_tree(_p(positions, _f), _p(indices, _u), _p(shading, _u), C.c_size_t(T), _p(rows, _f),
+                            C.c_size_t(len(rows) // 28), lib_mats, C.c_size_t(len(materials)), C.byref(tree))
+    n, e = tree.node_count, tree.emitter_count
+    out = {
+        "nodes": np.array([tree.nodes[i] for i in range(n * 12)], np.float32).reshape(-1, 12),
+        "links": np.array([tree.links[i] for i in range(n * 2)], np.uint32).reshape(-1, 2),
+        "records": np.array([tree.records[i] for i in range(e * 4 + T)], np.uint32),
+        "emitter_count": int(e),
+        "node_count": int(n),
+        "energy": float(tree.energy),
+    }
+    lib.or_light_tree_free(C.byref(tree))
+    return out

@@ -1,0 +1,188 @@
+"""The oracle pinned against the reference's own golden table and known-answer tests
+(src/render/tests.lucb), and the product's host side held to the same answers.
+CPU only."""
+import json
+import math
+from pathlib import Path
+
+import numpy as np
+import pytest
+
+import luce_render_b200 as lr
+from luce_render_b200 import scenes
+from oracle import oracle as orc
+
+GOLDEN = Path(__file__).resolve().parent / "golden"
+
+
+def test_sobol_table_matches_reference_generator():
+    table = json.loads((GOLDEN / "sobol_directions.json").read_text())["directions"]
+    assert orc.sobol_directions().tolist() == table
+
+
+def test_sample4_is_24_bit_and_stratified():
+    # sampler.glsl:47-55: four dimensions, top 24 bits; the first dimension of a
+    # pixel's first 2^k samples covers the 2^k strata exactly once (Owen-scrambled Sobol).
+    vals = np.array([orc.sample4_bits(1, 77, i, 0) for i in range(256)])
+    assert vals.max() < (1 << 24)
+    for d in range(2):
+        strata = np.sort(vals[:, d] >> 16)
+        assert np.array_equal(strata, np.arange(256))
+
+
+def check_bvh(nodes, positions, indices):
+    """check_bvh (tests.lucb:9-28)."""
+    count = len(indices)
+    seen = np.zeros(count, np.int64)
+    for n in nodes:
+        if n["count"] == 0:
+            if count == 0:
+                continue
+            for child in (n["first"], n["first"] + 1):
+                inner = nodes[child]
+                assert np.all(inner["lo"] >= n["lo"]) and np.all(inner["hi"] <= n["hi"])
+            continue
+        for slot in range(n["first"], n["first"] + n["count"]):
+            seen[slot] += 1
+            for k in range(3):
+                p = positions[indices[slot][k]]
+                assert np.all(p >= n["lo"]) and np.all(p <= n["hi"])
+    assert np.all(seen == 1)
+
+
+def test_cube_compiles_to_12_triangles_of_6_faces():
+    # tests.lucb:30-41, through the product's compile_scene and the oracle's build.
+    p, t, f = scenes.cube(2.0)
+    sc = lr.compile_scene([lr.MeshData(p, t, faces=f, face_count=6)])
+    a = sc.arrays()
+    assert sc.triangle_count() == 12 and sc.point_count() == 8
+    assert np.array_equal(np.bincount(a["faces"], minlength=6), [2] * 6)
+    check_bvh(a["nodes"], a["positions"], a["indices"])
+    nodes, order = orc.build_bvh(p, t)
+    assert np.array_equal(nodes.view(np.uint8), a["nodes"].view(np.uint8))
+
+
+def test_instances_placed_and_leaves_at_most_16():
+    # tests.lucb:43-61: a 40x40 grid and a copy 5 units up.
+    p, t, f = scenes.grid(10.0, 40)
+    sc = lr.compile_scene([lr.MeshData(p, t, faces=f, face_count=1600),
+                           lr.MeshData(p, t, faces=f, face_count=1600, transform=lr.placement((0.0, 5.0, 0.0)))])
+    a = sc.arrays()
+    assert sc.triangle_count() == 2 * 2 * 40 * 40
+    assert a["positions"][:, 1].max() == 5.0
+    assert a["nodes"]["count"].max() <= 16 and len(a["nodes"]) > 100
+    check_bvh(a["nodes"], a["positions"], a["indices"])
+
+
+def test_camera_frame_fits_film_horizontally():
+    # tests.lucb:63-81: 36 mm across at 18 mm is 90 deg horizontally.
+    cam = lr.camera((0.0, 0.0, 5.0), focal_length=18.0, horizontal_aperture=36.0)
+    for frame in (lr.ray_frame(cam, 200, 100),):
+        origin, left = frame.ray(0.0, 50.0)
+        assert origin[2] == 5.0 and abs(left[0] + 1.0) < 1e-9 and abs(left[2] + 1.0) < 1e-9
+        _, center = frame.ray(100.0, 50.0)
+        assert abs(center[0]) < 1e-9 and abs(center[1]) < 1e-9 and center[2] == -1.0
+        _, top = frame.ray(100.0, 0.0)
+        assert abs(top[1] - 0.5) < 1e-9
+    status, f = orc.frame_of_camera(cam.matrix, 0, 18.0, 36.0, 0.0, 5.0, 200, 100)
+    assert status == 0
+    o, d = orc.frame_ray(f, 0.0, 50.0)
+    assert o[2] == 5.0 and abs(d[0] + 1.0) < 1e-9 and abs(d[2] + 1.0) < 1e-9
+    assert np.array_equal(orc.frame_pack(f), lr.ray_frame(cam, 200, 100).pack())
+
+
+def test_orthographic_view_looks_along_forward():
+    # tests.lucb:83-91
+    frame = lr.look_frame((0.0, 10.0, 0.0), (0.0, -1.0, 0.0), (0.0, 0.0, -1.0), 2.0, 200, 100, orthographic=True)
+    assert frame.orthographic
+    corner, along = frame.ray(0.0, 0.0)
+    assert abs(corner[0] + 4.0) < 1e-9 and abs(corner[2] + 2.0) < 1e-9 and corner[1] == 10.0
+    assert along[1] == -1.0 and along[0] == 0.0
+    middle, _ = frame.ray(100.0, 50.0)
+    assert abs(middle[0]) < 1e-9 and abs(middle[2]) < 1e-9
+    status, f = orc.look_frame((0.0, 10.0, 0.0), (0.0, -1.0, 0.0), (0.0, 0.0, -1.0), 2.0, 200, 100, True)
+    assert status == 0 and np.array_equal(orc.frame_pack(f), frame.pack())
+
+
+def test_invalid_frames_raise_400():
+    with pytest.raises(lr.RenderError) as e:
+        lr.look_frame((0, 0, 0), (0, 0, -1), (0, 1, 0), 0.0, 10, 10)
+    assert e.value.code == 400
+    with pytest.raises(lr.RenderError) as e:
+        lr.ray_frame(lr.camera((0, 0, 0)), 0, 10)
+    assert e.value.code == 400
+
+
+def test_spectrum_fit_round_trips_through_the_film():
+    # tests.lucb:93-109
+    to_acescg = orc.film_matrix()
+    white = orc.fit_spectrum((1.0, 1.0, 1.0))
+    assert white[0] == 0 and white[1] == 0 and white[2] == 0 and abs(white[3] * 0.5 - 1.0) < 1e-12
+    back = to_acescg @ np.ones(3)
+    assert np.all(np.abs(back - 1.0) < 1e-6)
+    integrals = orc.cmf_integrals()
+    lam = np.arange(360.0, 831.0, 1.0)
+    obs = np.array([orc.cmf(l) for l in lam])
+    for color in [(0.8, 0.2, 0.1), (0.05, 0.5, 0.2), (0.1, 0.2, 0.9), (0.9, 0.9, 0.2)]:
+        c0, c1, c2, scale = orc.fit_spectrum(color)
+        x = (lam - 360.0) / 470.0
+        z = (c0 * x + c1) * x + c2
+        s = scale * (0.5 + z / (2.0 * np.sqrt(1.0 + z * z)))
+        xyz = (obs * s[:, None]).sum(0) / integrals
+        rgb = to_acescg @ xyz
+        assert np.all(np.abs(rgb - np.array(color)) < 0.01)
+
+
+def test_blackbody_hues():
+    # tests.lucb:111-122
+    to_acescg = orc.film_matrix()
+    n = to_acescg @ (orc.blackbody_xyz(5455.0) / orc.blackbody_xyz(5455.0)[1])
+    assert np.all(np.abs(n - 1.0) < 0.06)
+    w = to_acescg @ (orc.blackbody_xyz(3000.0) / orc.blackbody_xyz(3000.0)[1])
+    assert w[0] > 1.2 * w[1] and w[1] > w[2]
+    k = to_acescg @ (orc.blackbody_xyz(9000.0) / orc.blackbody_xyz(9000.0)[1])
+    assert k[2] > k[1] > k[0]
+
+
+def test_octahedral_normals_round_trip():
+    # tests.lucb:126-144
+    for d in [(0.3, -0.5, 0.8), (-1.0, 0.0, 0.0), (0.0, 0.0, -1.0), (0.6, 0.6, -0.5)]:
+        e = np.array(d) / np.linalg.norm(d)
+        assert np.linalg.norm(orc.octahedral_decode(orc.octahedral(e)) - e) < 1e-3
+
+
+def test_sphere_shading_normals_point_outward():
+    # tests.lucb:134-153: compiled shading normals of a sphere point away from its centre.
+    p, t, n = scenes.icosphere(2, 1.0)
+    sc = lr.compile_scene([lr.MeshData(p, t, normals=n, transform=lr.placement((0.0, 1.0, 0.0)))])
+    a = sc.arrays()
+    for tri in range(sc.triangle_count()):
+        for k in range(3):
+            pos = a["positions"][a["indices"][tri][k]] - np.array([0.0, 1.0, 0.0])
+            normal = orc.octahedral_decode(int(a["shading"][tri][k]))
+            assert normal @ pos > 0.9
+
+
+def test_light_tree_trails_and_energy():
+    # tests.lucb:155-183: a 9x9 grid, every triangle emitting.
+    p, t, f = scenes.grid(4.0, 9)
+    sc = lr.compile_scene([lr.MeshData(p, t, faces=f, face_count=81)])
+    a = sc.arrays()
+    glowing = orc.material_standard()
+    glowing.emission_luminance = 2.0
+    tree = orc.light_tree(a["positions"], a["indices"], a["shading"], np.zeros(0, np.float32), [glowing])
+    count = tree["emitter_count"]
+    assert count == sc.triangle_count() == 162
+    records, links, nodes = tree["records"], tree["links"], tree["nodes"]
+    total = 0.0
+    for index in range(count):
+        trail, depth = records[index * 4 + 1], records[index * 4 + 2]
+        assert depth <= 8
+        node = 0
+        for level in range(depth):
+            node = int(links[node][0]) + int((trail >> level) & 1)
+        assert links[node][1] == 0x80000000 and links[node][0] == index
+        code = records[index * 4]
+        assert code & 0x80000000 and records[count * 4 + (code & 0x7FFFFFFF)] == index
+        total += float(nodes[node][3])
+    assert abs(float(nodes[0][3]) / total - 1.0) < 1e-4
