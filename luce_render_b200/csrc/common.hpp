@@ -80,6 +80,9 @@ void fit_spectrum(const V3 &rgb, double out[4]);
 V3 blackbody_xyz(double kelvin);
 uint32_t octahedral(const V3 &n);
 
+// sampler.cpp: the 128 Sobol direction numbers (4 dimensions x 32 bits).
+const uint32_t *sobol_table();
+
 // The compiled scene (src/render/scene.lucb:31-63).
 struct Scene {
     std::vector<float> positions;        // xyz per point, world space

@@ -1,0 +1,349 @@
+// What a renderer loads besides geometry (src/render/loading.lucb:51-161): the UsdLux
+// light records (lights.lucb:29-131), the light tree over placed lights and emissive
+// triangles (light_tree.lucb:41-244), the OpenPBR material records
+// (materials.lucb:105-119), and the scene-wide constants (loading.lucb:253-272).
+#include "loading.hpp"
+
+#include <algorithm>
+#include <numeric>
+
+namespace lr {
+namespace {
+
+constexpr double kPi = 3.14159265358979323846;
+constexpr uint32_t kEmitterTriangle = 0x80000000u;
+constexpr uint32_t kLeafNode = 0x80000000u;
+
+double luminance(const V3 &rgb) { return 0.2722287168 * rgb.x + 0.6740817658 * rgb.y + 0.0536895174 * rgb.z; }
+
+struct Emitter {
+    V3 lo, hi, axis;
+    double theta_o, theta_e, energy;
+    uint32_t code;
+    double center(int k) const { return (lo[k] + hi[k]) * 0.5; }
+};
+
+// The cone holding both cones of normals (pbrt-v4's DirectionCone::Union;
+// light_tree.lucb:41-56).
+void cone_union(V3 &axis, double &theta, const V3 &b_axis, double b_theta) {
+    double theta_d = std::acos(std::min(std::max(axis.dot(b_axis), -1.0), 1.0));
+    if (std::min(theta_d + b_theta, kPi) <= theta) return;
+    if (std::min(theta_d + theta, kPi) <= b_theta) {
+        axis = b_axis;
+        theta = b_theta;
+        return;
+    }
+    double theta_o = 0.5 * (theta + theta_d + b_theta);
+    if (theta_o >= kPi) {
+        theta = kPi;
+        return;
+    }
+    double rotate = theta_o - theta;
+    V3 w = axis.cross(b_axis);
+    double wl = w.length();
+    if (wl < 1e-12) {
+        theta = kPi;
+        return;
+    }
+    V3 k = w * (1.0 / wl);
+    V3 turned = axis * std::cos(rotate) + k.cross(axis) * std::sin(rotate) + k * (k.dot(axis) * (1.0 - std::cos(rotate)));
+    double tl = turned.length();
+    if (tl > 0.0 && std::isfinite(tl)) axis = {turned.x / tl, turned.y / tl, turned.z / tl};
+    theta = theta_o;
+}
+
+// Three-way quickselect of the k-th emitter by centre along `axis`
+// (light_tree.lucb:217-239): the same partition steps, so the same tree.
+void select_kth(const std::vector<Emitter> &e, uint32_t *order, size_t length, size_t k, int axis) {
+    size_t low = 0, high = length;
+    while (high - low > 1) {
+        double pivot = e[order[(low + high) / 2]].center(axis);
+        size_t less = low, at = low, more = high;
+        while (at < more) {
+            double key = e[order[at]].center(axis);
+            if (key < pivot) {
+                std::swap(order[at], order[less]);
+                less++;
+                at++;
+            } else if (key > pivot) {
+                more--;
+                std::swap(order[at], order[more]);
+            } else {
+                at++;
+            }
+        }
+        if (k < less) high = less;
+        else if (k >= more) low = more;
+        else return;
+    }
+}
+
+}  // namespace
+
+LightRecords pack_lights(const std::vector<lr_light> &lights, double radius) {
+    LightRecords out;
+    const M3 to_acescg = film_matrix();
+    std::vector<double> powers;
+    for (const lr_light &light : lights) {
+        const double *m = light.matrix;
+        V3 position(m[9], m[10], m[11]);
+        V3 mz(-m[6], -m[7], -m[8]);
+        double l = mz.length();
+        if (!(l > 0.0)) fail(LR_INVALID, "a light's placement has no z axis");
+        V3 emits(mz.x / l, mz.y / l, mz.z / l);
+        V3 u, v;
+        double size = 0.0, area = 0.0, cos_half = 1.0, kind = 0.0;
+        if (light.shape == LR_LIGHT_RECT) {
+            u = V3(m[0], m[1], m[2]) * (0.5 * light.width);
+            v = V3(m[3], m[4], m[5]) * (0.5 * light.height);
+            area = 4.0 * u.cross(v).length();
+        } else if (light.shape == LR_LIGHT_DISK) {
+            kind = 1.0;
+            u = V3(m[0], m[1], m[2]) * light.radius;
+            v = V3(m[3], m[4], m[5]) * light.radius;
+            area = kPi * u.cross(v).length();
+        } else if (light.shape == LR_LIGHT_SPHERE) {
+            kind = 2.0;
+            double det = V3(m[0], m[1], m[2]).dot(V3(m[3], m[4], m[5]).cross(V3(m[6], m[7], m[8])));
+            size = light.radius * std::cbrt(std::fabs(det));
+            area = 4.0 * kPi * size * size;
+        } else {
+            kind = 3.0;
+            cos_half = std::cos(0.5 * light.angle * kPi / 180.0);
+        }
+        double scale = light.intensity * std::exp2(light.exposure);
+        if (kind < 3.0 && light.normalize) {
+            if (area <= 0.0) continue;
+            scale = scale / area;
+        }
+        if (kind == 3.0 && cos_half < 1.0 - 1e-7) scale = scale / (2.0 * kPi * (1.0 - cos_half));
+        V3 color(light.color[0], light.color[1], light.color[2]);
+        V3 rgb = color * scale;
+        double fit[4];
+        fit_spectrum(color, fit);
+        fit[3] = fit[3] * scale;
+        double flags = light.visible ? 1.0 : 0.0;
+        if (light.temperature > 0.0) {
+            V3 tint = blackbody_xyz(light.temperature);
+            fit[3] = fit[3] / tint.y;
+            V3 tinted = to_acescg.apply(tint * (1.0 / tint.y));
+            rgb = V3(rgb.x * tinted.x, rgb.y * tinted.y, rgb.z * tinted.z);
+            flags += 2.0;
+        }
+        double power = -1.0;
+        if (kind == 3.0)
+            power = std::max(0.0, luminance(rgb)) * (cos_half < 1.0 - 1e-7 ? 2.0 * kPi * (1.0 - cos_half) : 1.0) * kPi *
+                    radius * radius;
+        powers.push_back(power);
+        const double rows[28] = {position.x, position.y, position.z, kind,   u.x,    u.y,    u.z,    size,
+                                 v.x,        v.y,        v.z,        cos_half, emits.x, emits.y, emits.z, area,
+                                 fit[0],     fit[1],     fit[2],     fit[3], rgb.x,  rgb.y,  rgb.z,  flags,
+                                 light.temperature, 0.0, 0.0, 0.0};
+        for (double value : rows) out.rows.push_back((float)value);
+    }
+    out.count = powers.size();
+    double total = 0.0;
+    size_t distant = 0;
+    for (double p : powers)
+        if (p >= 0.0) {
+            total += p;
+            distant++;
+        }
+    double running = 0.0;
+    uint32_t emitter = 0;
+    for (size_t i = 0; i < powers.size(); i++) {
+        float *row6 = &out.rows[i * 28 + 24];
+        if (powers[i] < 0.0) {
+            row6[3] = (float)emitter++;
+            continue;
+        }
+        double share = total > 0.0 ? powers[i] / total : 1.0 / (double)distant;
+        running += share;
+        row6[1] = (float)share;
+        row6[2] = (float)running;
+    }
+    out.distant_power = total;
+    return out;
+}
+
+LightTree build_light_tree(const Scene &scene, const LightRecords &lights, const std::vector<lr_openpbr> &library) {
+    LightTree tree;
+    std::vector<Emitter> emitters;
+    for (size_t index = 0; index < lights.count; index++) {
+        const float *row = &lights.rows[index * 28];
+        double kind = row[3];
+        if (kind >= 3.0) continue;
+        V3 position(row[0], row[1], row[2]), u(row[4], row[5], row[6]), v(row[8], row[9], row[10]);
+        V3 normal(row[12], row[13], row[14]);
+        double area = row[15];
+        V3 rgb(row[20], row[21], row[22]);
+        V3 extent(std::fabs(u.x) + std::fabs(v.x), std::fabs(u.y) + std::fabs(v.y), std::fabs(u.z) + std::fabs(v.z));
+        double theta_o = 0.0;
+        if (kind == 2.0) {
+            double r = row[7];
+            extent = V3(r, r, r);
+            theta_o = kPi;
+        }
+        emitters.push_back({position - extent, position + extent, normal, theta_o, 0.5 * kPi,
+                            std::max(0.0, luminance(rgb)) * area * kPi, (uint32_t)index});
+    }
+    bool emissive = false;
+    for (const auto &m : library) emissive = emissive || m.emission_luminance > 0.0;
+    const size_t T = scene.triangle_count();
+    const float *p = scene.positions.data();
+    for (size_t t = 0; emissive && t < T; t++) {
+        uint32_t material = scene.shading[t * 4 + 3];
+        if ((size_t)material >= library.size()) continue;
+        const lr_openpbr &m = library[material];
+        if (m.emission_luminance <= 0.0) continue;
+        V3 c[3];
+        for (int k = 0; k < 3; k++) {
+            const float *q = &p[(size_t)scene.indices[t * 3 + k] * 3];
+            c[k] = V3(q[0], q[1], q[2]);
+        }
+        V3 cross = (c[1] - c[0]).cross(c[2] - c[0]);
+        double area = 0.5 * cross.length();
+        if (area <= 0.0) continue;
+        V3 lo(std::min(c[0].x, std::min(c[1].x, c[2].x)), std::min(c[0].y, std::min(c[1].y, c[2].y)),
+              std::min(c[0].z, std::min(c[1].z, c[2].z)));
+        V3 hi(std::max(c[0].x, std::max(c[1].x, c[2].x)), std::max(c[0].y, std::max(c[1].y, c[2].y)),
+              std::max(c[0].z, std::max(c[1].z, c[2].z)));
+        V3 emission = V3(m.emission_color[0], m.emission_color[1], m.emission_color[2]) * m.emission_luminance;
+        emitters.push_back({lo, hi, cross * (0.5 / area), kPi, 0.5 * kPi,
+                            std::max(0.0, luminance(emission)) * area * 2.0 * kPi, kEmitterTriangle | (uint32_t)t});
+    }
+    const size_t count = emitters.size();
+    tree.emitter_count = count;
+    tree.records.assign(count * 4, 0u);
+    tree.triangle_map.assign(T, 0xffffffffu);
+    for (size_t i = 0; i < count; i++) {
+        uint32_t code = emitters[i].code;
+        tree.records[i * 4] = code;
+        if (code & kEmitterTriangle) tree.triangle_map[code & ~kEmitterTriangle] = (uint32_t)i;
+    }
+    if (count == 0) return tree;
+    std::vector<uint32_t> order(count);
+    std::iota(order.begin(), order.end(), 0u);
+    tree.nodes.assign(12, 0.0f);
+    tree.links.assign(2, 0u);
+    struct Job {
+        size_t node, first, count;
+        uint32_t trail, depth;
+    };
+    std::vector<Job> stack{{0, 0, count, 0, 0}};
+    while (!stack.empty()) {
+        Job job = stack.back();
+        stack.pop_back();
+        uint32_t *range = order.data() + job.first;
+        const Emitter &head = emitters[range[0]];
+        V3 lo = head.lo, hi = head.hi, axis = head.axis;
+        double theta_o = head.theta_o, theta_e = head.theta_e, energy = 0.0;
+        for (size_t i = 0; i < job.count; i++) {
+            const Emitter &e = emitters[range[i]];
+            for (int k = 0; k < 3; k++) {
+                lo[k] = std::min(lo[k], e.lo[k]);
+                hi[k] = std::max(hi[k], e.hi[k]);
+            }
+            cone_union(axis, theta_o, e.axis, e.theta_o);
+            theta_e = std::max(theta_e, e.theta_e);
+            energy += e.energy;
+        }
+        const double values[12] = {lo.x, lo.y, lo.z, energy, hi.x, hi.y, hi.z, std::cos(theta_o),
+                                   axis.x, axis.y, axis.z, std::cos(theta_e)};
+        for (int k = 0; k < 12; k++) tree.nodes[job.node * 12 + k] = (float)values[k];
+        if (job.node == 0) tree.energy = energy;
+        if (job.count == 1) {
+            uint32_t emitter = range[0];
+            tree.links[job.node * 2] = emitter;
+            tree.links[job.node * 2 + 1] = kLeafNode;
+            tree.records[emitter * 4 + 1] = job.trail;
+            tree.records[emitter * 4 + 2] = job.depth;
+            continue;
+        }
+        V3 size = hi - lo;
+        int axis_index = 0;
+        if (size.y > size.x && size.y >= size.z) axis_index = 1;
+        else if (size.z > size.x && size.z > size.y) axis_index = 2;
+        size_t half = job.count / 2;
+        select_kth(emitters, range, job.count, half, axis_index);
+        size_t child = tree.links.size() / 2;
+        tree.nodes.resize(tree.nodes.size() + 24, 0.0f);
+        tree.links.resize(tree.links.size() + 4, 0u);
+        tree.links[job.node * 2] = (uint32_t)child;
+        tree.links[job.node * 2 + 1] = 0;
+        stack.push_back({child + 1, job.first + half, job.count - half, job.trail | (1u << job.depth), job.depth + 1});
+        stack.push_back({child, job.first, half, job.trail, job.depth + 1});
+    }
+    tree.node_count = tree.links.size() / 2;
+    return tree;
+}
+
+void pack_material(const lr_openpbr &m, float program, std::vector<float> &out) {
+    const V3 colors[5] = {V3(m.base_color[0], m.base_color[1], m.base_color[2]),
+                          V3(m.specular_color[0], m.specular_color[1], m.specular_color[2]),
+                          V3(m.coat_color[0], m.coat_color[1], m.coat_color[2]),
+                          V3(m.emission_color[0], m.emission_color[1], m.emission_color[2]) * m.emission_luminance,
+                          V3(m.transmission_color[0], m.transmission_color[1], m.transmission_color[2])};
+    const double weights[5] = {m.base_weight, m.specular_weight, m.coat_weight, m.emission_luminance,
+                               m.transmission_weight};
+    for (int i = 0; i < 5; i++) {
+        const V3 &c = colors[i];
+        double fit[4];
+        fit_spectrum(V3(std::max(c.x, 0.0), std::max(c.y, 0.0), std::max(c.z, 0.0)), fit);
+        const double row[8] = {fit[0], fit[1], fit[2], fit[3], c.x, c.y, c.z, weights[i]};
+        for (double v : row) out.push_back((float)v);
+    }
+    double cauchy = 0.0;
+    if (m.transmission_dispersion_scale > 0.0 && m.transmission_dispersion_abbe_number > 0.0 && m.transmission_weight > 0.0)
+        cauchy = (m.specular_ior - 1.0) * m.transmission_dispersion_scale /
+                 (m.transmission_dispersion_abbe_number * (1.0 / (486.1 * 486.1) - 1.0 / (656.3 * 656.3)));
+    const double rest[24] = {m.base_metalness, m.base_diffuse_roughness, m.specular_roughness,
+                             m.specular_roughness_anisotropy, m.specular_ior, m.coat_roughness, m.coat_ior,
+                             m.coat_darkening, m.geometry_opacity, m.geometry_thin_walled ? 1.0 : 0.0,
+                             m.coat_roughness_anisotropy, cauchy, (double)program, 0, 0, 0,
+                             0, 0, 0, 0, 0, 0, 0, 0};
+    for (double v : rest) out.push_back((float)v);
+}
+
+// Scenes this build shades: Lambertian OpenPBR (EON diffuse with emission), opaque.
+void check_material(const lr_openpbr &m, size_t index) {
+    auto bad = [&](const char *what) {
+        fail(LR_INVALID, "material " + std::to_string(index) + ": " + what +
+                             " is not part of this build's Lambertian shading (set it to its neutral value)");
+    };
+    if (m.specular_weight != 0.0) bad("specular_weight");
+    if (m.base_metalness != 0.0) bad("base_metalness");
+    if (m.transmission_weight != 0.0) bad("transmission_weight");
+    if (m.coat_weight != 0.0) bad("coat_weight");
+    if (m.geometry_opacity < 1.0) bad("geometry_opacity below 1");
+    if (m.base_diffuse_roughness < 0.0 || m.base_diffuse_roughness > 1.0) bad("base_diffuse_roughness outside 0..1");
+}
+
+double scene_radius(const Scene &scene) {
+    if (scene.point_count() == 0 || scene.nodes.empty()) return 1.0;
+    const lr_bvh_node &root = scene.nodes[0];
+    if (root.lo[0] > root.hi[0]) return 1.0;
+    V3 d((double)(root.hi[0] - root.lo[0]), (double)(root.hi[1] - root.lo[1]), (double)(root.hi[2] - root.lo[2]));
+    return std::max(1.0, 0.5 * d.length());
+}
+
+Loaded load(const Scene &scene, const lr_settings &settings) {
+    Loaded L;
+    L.library.push_back(settings.material);
+    for (const auto &m : scene.materials) L.library.push_back(m);
+    for (size_t i = 0; i < L.library.size(); i++)
+        if (i >= scene.used.size() || scene.used[i]) check_material(L.library[i], i);
+    L.radius = scene_radius(scene);
+    L.lights = pack_lights(scene.lights, L.radius);
+    L.tree = build_light_tree(scene, L.lights, L.library);
+    for (size_t i = 0; i < L.library.size(); i++) pack_material(L.library[i], -1.0f, L.materials);
+    const double total = L.lights.distant_power + L.tree.energy;
+    L.p_distant = L.tree.emitter_count > 0 ? (total > 0.0 ? L.lights.distant_power / total : 0.0)
+                                           : (L.lights.distant_power > 0.0 ? 1.0 : 0.0);
+    fit_spectrum(V3(settings.background[0], settings.background[1], settings.background[2]), L.background_fit);
+    L.film = film_matrix();
+    L.cmf_integrals = cmf_integrals();
+    return L;
+}
+
+}  // namespace lr

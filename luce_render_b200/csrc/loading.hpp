@@ -1,0 +1,44 @@
+// Host-side loading of a renderer's lights, light tree, materials and constants.
+#pragma once
+
+#include <vector>
+
+#include "common.hpp"
+
+namespace lr {
+
+// Light records: 7 vec4 (28 floats) per light, as shaders/lights.glsl:1-22 lays them out.
+struct LightRecords {
+    std::vector<float> rows;
+    size_t count = 0;
+    double distant_power = 0.0;
+};
+
+// The light tree (light_tree.lucb:16-20): 12 floats per node (lo, energy; hi, cos theta_o;
+// axis, cos theta_e), 2 links per node, 4 words per emitter (code, trail, depth, 0) and
+// one emitter per triangle slot (0xffffffff: none).
+struct LightTree {
+    std::vector<float> nodes;
+    std::vector<uint32_t> links, records, triangle_map;
+    size_t node_count = 0, emitter_count = 0;
+    double energy = 0.0;
+};
+
+struct Loaded {
+    std::vector<lr_openpbr> library;  // the default material first
+    LightRecords lights;
+    LightTree tree;
+    std::vector<float> materials;     // 64 floats per material
+    double radius = 1.0, p_distant = 0.0;
+    double background_fit[4] = {0, 0, 0, 0};
+    M3 film{};
+    V3 cmf_integrals;
+};
+
+LightRecords pack_lights(const std::vector<lr_light> &lights, double radius);
+LightTree build_light_tree(const Scene &scene, const LightRecords &lights, const std::vector<lr_openpbr> &library);
+void pack_material(const lr_openpbr &m, float program, std::vector<float> &out);
+double scene_radius(const Scene &scene);
+Loaded load(const Scene &scene, const lr_settings &settings);
+
+}  // namespace lr

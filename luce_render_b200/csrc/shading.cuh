@@ -1,0 +1,516 @@
+// Device math of the integrator's shading: the stateless Owen-scrambled Sobol sampler
+// (shaders/sampler.glsl:8-55), hero-wavelength spectra (spectrum.glsl:10-118), UsdLux
+// lights (lights.glsl:24-282), the light tree (lighttree.glsl:18-137), EON/Lambert
+// diffuse (openpbr.glsl:87-113, 460-547 at the Lambertian settings) and the path
+// helpers of common.glsl:103-276.
+#pragma once
+
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+namespace lr {
+
+constexpr float kPi = 3.14159265358979323846f;
+constexpr float kInfinity = 3.0e38f;
+constexpr uint32_t kNone = 0xffffffffu;
+constexpr uint32_t kLightHit = 0x80000000u;
+constexpr uint32_t kEmitterTriangle = 0x80000000u;
+constexpr uint32_t kLeafNode = 0x80000000u;
+
+// ---- vectors ---------------------------------------------------------------------------
+
+__device__ __forceinline__ float3 operator+(float3 a, float3 b) { return make_float3(a.x + b.x, a.y + b.y, a.z + b.z); }
+__device__ __forceinline__ float3 operator-(float3 a, float3 b) { return make_float3(a.x - b.x, a.y - b.y, a.z - b.z); }
+__device__ __forceinline__ float3 operator-(float3 a) { return make_float3(-a.x, -a.y, -a.z); }
+__device__ __forceinline__ float3 operator*(float3 a, float s) { return make_float3(a.x * s, a.y * s, a.z * s); }
+__device__ __forceinline__ float3 operator*(float s, float3 a) { return make_float3(a.x * s, a.y * s, a.z * s); }
+__device__ __forceinline__ float4 operator+(float4 a, float4 b) { return make_float4(a.x + b.x, a.y + b.y, a.z + b.z, a.w + b.w); }
+__device__ __forceinline__ float4 operator*(float4 a, float4 b) { return make_float4(a.x * b.x, a.y * b.y, a.z * b.z, a.w * b.w); }
+__device__ __forceinline__ float4 operator*(float4 a, float s) { return make_float4(a.x * s, a.y * s, a.z * s, a.w * s); }
+__device__ __forceinline__ float dot(float3 a, float3 b) { return a.x * b.x + a.y * b.y + a.z * b.z; }
+__device__ __forceinline__ float3 cross(float3 a, float3 b) {
+    return make_float3(a.y * b.z - a.z * b.y, a.z * b.x - a.x * b.z, a.x * b.y - a.y * b.x);
+}
+__device__ __forceinline__ float length(float3 a) { return sqrtf(dot(a, a)); }
+__device__ __forceinline__ float3 normalize(float3 a) { return a * rsqrtf(dot(a, a)); }
+__device__ __forceinline__ float3 xyz(float4 a) { return make_float3(a.x, a.y, a.z); }
+
+// ---- sampler.glsl --------------------------------------------------------------------
+
+__constant__ uint32_t c_sobol[128];
+
+__device__ __forceinline__ uint32_t hash_u32(uint32_t x) {
+    x ^= x >> 16;
+    x *= 0x21f0aaadu;
+    x ^= x >> 15;
+    x *= 0x735a2d97u;
+    x ^= x >> 15;
+    return x;
+}
+
+__device__ __forceinline__ uint32_t hash_combine(uint32_t seed, uint32_t value) {
+    return seed ^ (hash_u32(value) + 0x9e3779b9u + (seed << 6) + (seed >> 2));
+}
+
+__device__ __forceinline__ uint32_t nested_uniform_scramble(uint32_t x, uint32_t seed) {
+    x = __brev(x);
+    x += seed;
+    x ^= x * 0x6c50b47cu;
+    x ^= x * 0xb82f1e52u;
+    x ^= x * 0xc7afe638u;
+    x ^= x * 0x8d22f6e6u;
+    return __brev(x);
+}
+
+__device__ __forceinline__ uint32_t sobol(uint32_t index, uint32_t dimension) {
+    uint32_t x = 0;
+    const uint32_t *dirs = c_sobol + dimension * 32;
+    while (index) {
+        const int bit = __ffs(index) - 1;
+        x ^= dirs[bit];
+        index &= index - 1;
+    }
+    return x;
+}
+
+// sample4 (sampler.glsl:47-55): the 4-D point of `group` for this pixel's sample.
+__device__ __forceinline__ float4 sample4(uint32_t seed, uint32_t pixel, uint32_t index, uint32_t group) {
+    const uint32_t s = hash_combine(hash_combine(seed, pixel), group);
+    const uint32_t shuffled = nested_uniform_scramble(index, hash_u32(s));
+    float v[4];
+#pragma unroll
+    for (uint32_t d = 0; d < 4; d++)
+        v[d] = (float)(nested_uniform_scramble(sobol(shuffled, d), hash_combine(s, d + 1u)) >> 8) * (1.0f / 16777216.0f);
+    return make_float4(v[0], v[1], v[2], v[3]);
+}
+
+constexpr uint32_t kGroupCamera = 0, kGroupWavelength = 1;
+__device__ __forceinline__ uint32_t group_light(uint32_t b) { return 2u + 3u * b; }
+__device__ __forceinline__ uint32_t group_bsdf(uint32_t b) { return 3u + 3u * b; }
+
+// ---- common.glsl ---------------------------------------------------------------------
+
+__device__ __forceinline__ float2 concentric(float2 u) {
+    const float ox = 2.0f * u.x - 1.0f, oy = 2.0f * u.y - 1.0f;
+    if (ox == 0.0f && oy == 0.0f) return make_float2(0.0f, 0.0f);
+    float r, theta;
+    if (fabsf(ox) > fabsf(oy)) {
+        r = ox;
+        theta = (kPi / 4.0f) * (oy / ox);
+    } else {
+        r = oy;
+        theta = (kPi / 2.0f) - (kPi / 4.0f) * (ox / oy);
+    }
+    float s, c;
+    sincosf(theta, &s, &c);
+    return make_float2(r * c, r * s);
+}
+
+__device__ __forceinline__ float mis_weight(float a, float b) {
+    a = fminf(a, 1e18f);
+    b = fminf(b, 1e18f);
+    return 1.0f / (1.0f + a * a + b * b);
+}
+
+__device__ __forceinline__ float3 offset_origin(float3 p, float3 n) {
+    const float scale = fmaxf(1.0f, fmaxf(fabsf(p.x), fmaxf(fabsf(p.y), fabsf(p.z))));
+    return p + n * (1e-4f * scale);
+}
+
+__device__ __forceinline__ uint32_t octahedral_encode(float3 n) {
+    const float inv = 1.0f / (fabsf(n.x) + fabsf(n.y) + fabsf(n.z));
+    float px = n.x * inv, py = n.y * inv;
+    if (n.z < 0.0f) {
+        const float qx = (1.0f - fabsf(py)) * (px >= 0.0f ? 1.0f : -1.0f);
+        const float qy = (1.0f - fabsf(px)) * (py >= 0.0f ? 1.0f : -1.0f);
+        px = qx;
+        py = qy;
+    }
+    // packSnorm2x16: round(clamp(v, -1, 1) * 32767)
+    const int ix = __float2int_rn(fminf(fmaxf(px, -1.0f), 1.0f) * 32767.0f);
+    const int iy = __float2int_rn(fminf(fmaxf(py, -1.0f), 1.0f) * 32767.0f);
+    return ((uint32_t)ix & 0xffffu) | ((uint32_t)iy << 16);
+}
+
+__device__ __forceinline__ float3 octahedral_decode(uint32_t packed) {
+    // unpackSnorm2x16: clamp(v / 32767, -1, 1)
+    float x = fmaxf((float)(int16_t)(packed & 0xffffu) / 32767.0f, -1.0f);
+    float y = fmaxf((float)(int16_t)(packed >> 16) / 32767.0f, -1.0f);
+    float3 n = make_float3(x, y, 1.0f - fabsf(x) - fabsf(y));
+    if (n.z < 0.0f) {
+        const float nx = (1.0f - fabsf(y)) * (x >= 0.0f ? 1.0f : -1.0f);
+        const float ny = (1.0f - fabsf(x)) * (y >= 0.0f ? 1.0f : -1.0f);
+        n.x = nx;
+        n.y = ny;
+    }
+    return normalize(n);
+}
+
+// An orthonormal basis around n (Duff et al. 2017; common.glsl:270-276).
+__device__ __forceinline__ void basis(float3 n, float3 &t, float3 &b) {
+    const float s = n.z >= 0.0f ? 1.0f : -1.0f;
+    const float a = -1.0f / (s + n.z);
+    const float c = n.x * n.y * a;
+    t = make_float3(1.0f + s * n.x * n.x * a, s * c, -s * n.x);
+    b = make_float3(c, s + n.y * n.y * a, -n.y);
+}
+
+// next_bounce (common.glsl:229-234): one more bounce of `lobe`, or kNone past a limit.
+__device__ __forceinline__ uint32_t next_bounce(uint32_t bounces, uint32_t lobe, const float *limits) {
+    const uint32_t shift = 8u * (lobe + 1u);
+    const uint32_t kind = ((bounces >> shift) & 0xffu) + 1u;
+    if ((float)kind > limits[lobe] || (bounces & 0xffu) >= 255u) return kNone;
+    return (bounces & ~(0xffu << shift)) + (kind << shift) + 1u;
+}
+
+// ---- spectrum.glsl -------------------------------------------------------------------
+
+__device__ __forceinline__ float4 sample_wavelengths(float u) {
+    float l[4];
+#pragma unroll
+    for (int i = 0; i < 4; i++) {
+        float v = u + (float)i * 0.25f;
+        v = v - floorf(v);
+        l[i] = 538.0f - 138.888889f * atanhf(0.85691062f - 1.82750197f * v);
+    }
+    return make_float4(l[0], l[1], l[2], l[3]);
+}
+
+__device__ __forceinline__ float wavelength_pdf(float lambda) {
+    if (lambda < 360.0f || lambda > 830.0f) return 0.0f;
+    const float c = coshf(0.0072f * (lambda - 538.0f));
+    return 0.0039398042f / (c * c);
+}
+
+__device__ __forceinline__ float cmf_lobe(float x, float mean, float below, float above) {
+    const float t = (x - mean) / (x < mean ? below : above);
+    return expf(-0.5f * t * t);
+}
+
+__device__ __forceinline__ float3 cmf(float l) {
+    return make_float3(1.056f * cmf_lobe(l, 599.8f, 37.9f, 31.0f) + 0.362f * cmf_lobe(l, 442.0f, 16.0f, 26.7f) -
+                           0.065f * cmf_lobe(l, 501.1f, 20.4f, 26.2f),
+                       0.821f * cmf_lobe(l, 568.8f, 46.9f, 40.5f) + 0.286f * cmf_lobe(l, 530.9f, 16.3f, 31.1f),
+                       1.217f * cmf_lobe(l, 437.0f, 11.8f, 36.0f) + 0.681f * cmf_lobe(l, 459.0f, 26.0f, 13.8f));
+}
+
+template <bool kSpectral>
+__device__ __forceinline__ float4 spec_of(float4 fit, float3 rgb, float4 lambda) {
+    if (!kSpectral) return make_float4(rgb.x, rgb.y, rgb.z, 0.0f);
+    float l[4] = {lambda.x, lambda.y, lambda.z, lambda.w}, o[4];
+#pragma unroll
+    for (int i = 0; i < 4; i++) {
+        const float x = (l[i] - 360.0f) / (830.0f - 360.0f);
+        const float z = (fit.x * x + fit.y) * x + fit.z;
+        o[i] = fit.w * (0.5f + z / (2.0f * sqrtf(1.0f + z * z)));
+    }
+    return make_float4(o[0], o[1], o[2], o[3]);
+}
+
+__device__ __forceinline__ float blackbody(float lambda, float kelvin) {
+    const float peak = 2.8977721e6f / kelvin;
+    const float x = 1.4387769e7f / (lambda * kelvin);
+    const float r = peak / lambda;
+    return r * r * r * r * r * (142.32492f / (expf(x) - 1.0f));
+}
+
+template <bool kSpectral>
+__device__ __forceinline__ float spec_max(float4 s) {
+    return kSpectral ? fmaxf(fmaxf(s.x, s.y), fmaxf(s.z, s.w)) : fmaxf(s.x, fmaxf(s.y, s.z));
+}
+
+// The constants the integrator kernels read (spectral film, bounce limits, light
+// selection), after the K_* rows of common.glsl:79-86 and loading.lucb:253-272.
+struct Constants {
+    float film[9];          // XYZ under E -> ACEScg, by rows
+    float cmf_integrals[3];
+    float limits[3];        // the most diffuse, glossy, transmission bounces
+    float clamp_indirect;   // 0: off
+    float4 background_fit;
+    float3 background_rgb;
+    float p_distant;        // the chance a light sample takes a distant light
+    uint32_t max_bounces;
+    uint32_t light_count;
+    uint32_t tree_nodes;
+    uint32_t seed;
+};
+
+template <bool kSpectral>
+__device__ __forceinline__ float3 spec_to_film(float4 radiance, float4 lambda, const Constants &k) {
+    if (!kSpectral) return xyz(radiance);
+    float3 sum = make_float3(0.0f, 0.0f, 0.0f);
+    const float l[4] = {lambda.x, lambda.y, lambda.z, lambda.w}, r[4] = {radiance.x, radiance.y, radiance.z, radiance.w};
+#pragma unroll
+    for (int i = 0; i < 4; i++) {
+        const float pdf = wavelength_pdf(l[i]);
+        if (pdf > 0.0f) sum = sum + cmf(l[i]) * (r[i] / pdf);
+    }
+    return make_float3(sum.x * 0.25f / k.cmf_integrals[0], sum.y * 0.25f / k.cmf_integrals[1],
+                       sum.z * 0.25f / k.cmf_integrals[2]);
+}
+
+// ---- lights.glsl ---------------------------------------------------------------------
+
+constexpr uint32_t kLightStride = 7;
+constexpr uint32_t kLightRect = 0, kLightDisk = 1, kLightSphere = 2, kLightDistant = 3;
+
+struct LightSample {
+    float3 direction;
+    float distance;
+    float pdf;
+    float cos_light;
+    bool delta;
+};
+
+__device__ __forceinline__ float4 light_at(const float4 *lights, uint32_t light, uint32_t row) {
+    return __ldg(&lights[light * kLightStride + row]);
+}
+__device__ __forceinline__ uint32_t light_type(const float4 *lights, uint32_t l) { return (uint32_t)light_at(lights, l, 0).w; }
+__device__ __forceinline__ bool light_visible(const float4 *lights, uint32_t l) {
+    return ((uint32_t)light_at(lights, l, 5).w & 1u) != 0u;
+}
+
+template <bool kSpectral>
+__device__ __forceinline__ float4 light_radiance(const float4 *lights, uint32_t light, float4 lambda) {
+    const float4 rgb = light_at(lights, light, 5);
+    float4 radiance = spec_of<kSpectral>(light_at(lights, light, 4), xyz(rgb), lambda);
+    if (kSpectral && ((uint32_t)rgb.w & 2u) != 0u) {
+        const float kelvin = light_at(lights, light, 6).x;
+        radiance.x *= blackbody(lambda.x, kelvin);
+        radiance.y *= blackbody(lambda.y, kelvin);
+        radiance.z *= blackbody(lambda.z, kelvin);
+        radiance.w *= blackbody(lambda.w, kelvin);
+    }
+    return radiance;
+}
+
+__device__ __forceinline__ uint32_t pick_distant(const float4 *lights, uint32_t count, float u, float &pdf) {
+    uint32_t chosen = kNone;
+    for (uint32_t light = 0; light < count; light++) {
+        if (light_type(lights, light) < kLightDistant) continue;
+        chosen = light;
+        if (u < light_at(lights, light, 6).z) break;
+    }
+    pdf = chosen == kNone ? 0.0f : light_at(lights, chosen, 6).y;
+    return chosen;
+}
+
+__device__ __forceinline__ float3 sample_cone(float3 axis, float cos_max, float2 u) {
+    const float c = 1.0f - u.x * (1.0f - cos_max);
+    const float s = sqrtf(fmaxf(0.0f, 1.0f - c * c));
+    const float phi = 2.0f * kPi * u.y;
+    float3 t, b;
+    basis(axis, t, b);
+    float sp, cp;
+    sincosf(phi, &sp, &cp);
+    return normalize(t * (s * cp) + b * (s * sp) + axis * c);
+}
+
+__device__ __forceinline__ float sphere_hit(float3 center, float radius, float3 o, float3 d) {
+    const float3 oc = o - center;
+    const float b = dot(oc, d);
+    const float c = dot(oc, oc) - radius * radius;
+    float h = b * b - c;
+    if (h < 0.0f) return kInfinity;
+    h = sqrtf(h);
+    float t = -b - h;
+    if (t > 0.0f) return t;
+    t = -b + h;
+    return t > 0.0f ? t : kInfinity;
+}
+
+__device__ __forceinline__ bool sample_light(const float4 *lights, uint32_t light, float3 p, float2 u, LightSample &s) {
+    const float4 row0 = light_at(lights, light, 0), row1 = light_at(lights, light, 1), row2 = light_at(lights, light, 2),
+                 row3 = light_at(lights, light, 3);
+    const uint32_t type = (uint32_t)row0.w;
+    s.delta = false;
+    s.cos_light = 1.0f;
+    if (type == kLightRect || type == kLightDisk) {
+        const float2 a = type == kLightRect ? make_float2(2.0f * u.x - 1.0f, 2.0f * u.y - 1.0f) : concentric(u);
+        const float3 q = xyz(row0) + a.x * xyz(row1) + a.y * xyz(row2);
+        const float3 d = q - p;
+        const float d2 = dot(d, d);
+        s.distance = sqrtf(d2);
+        s.direction = d * (1.0f / s.distance);
+        const float cos_light = -dot(s.direction, xyz(row3));
+        if (cos_light <= 0.0f || row3.w <= 0.0f) return false;
+        s.pdf = d2 / (cos_light * row3.w);
+        s.cos_light = cos_light;
+        return true;
+    }
+    if (type == kLightSphere) {
+        const float3 to_center = xyz(row0) - p;
+        const float d2 = dot(to_center, to_center);
+        const float r = row1.w;
+        if (d2 <= r * r) return false;
+        const float cos_max = sqrtf(fmaxf(0.0f, 1.0f - r * r / d2));
+        s.direction = sample_cone(to_center * rsqrtf(d2), cos_max, u);
+        s.distance = sphere_hit(xyz(row0), r, p, s.direction);
+        if (s.distance >= kInfinity) return false;
+        s.pdf = 1.0f / (2.0f * kPi * (1.0f - cos_max));
+        s.cos_light = fmaxf(0.0f, -dot(s.direction, normalize(p + s.direction * s.distance - xyz(row0))));
+        return true;
+    }
+    const float3 axis = -xyz(row3);
+    const float cos_half = row2.w;
+    s.distance = kInfinity;
+    if (cos_half >= 1.0f - 1e-7f) {
+        s.direction = axis;
+        s.pdf = 1.0f;
+        s.delta = true;
+        return true;
+    }
+    s.direction = sample_cone(axis, cos_half, u);
+    s.pdf = 1.0f / (2.0f * kPi * (1.0f - cos_half));
+    return true;
+}
+
+// intersect_light (lights.glsl:239-259) for a camera path (light_flow false).
+__device__ __forceinline__ float intersect_light(const float4 *lights, uint32_t light, float3 o, float3 d, float t_max) {
+    const float4 row0 = light_at(lights, light, 0);
+    const uint32_t type = (uint32_t)row0.w;
+    if (type == kLightSphere) {
+        const float t = sphere_hit(xyz(row0), light_at(lights, light, 1).w, o, d);
+        return t < t_max ? t : kInfinity;
+    }
+    if (type >= kLightDistant) return kInfinity;
+    const float3 u = xyz(light_at(lights, light, 1)), v = xyz(light_at(lights, light, 2)),
+                 n = xyz(light_at(lights, light, 3));
+    const float facing = dot(d, n);
+    if (facing >= 0.0f) return kInfinity;
+    const float t = dot(xyz(row0) - o, n) / facing;
+    if (t <= 0.0f || t >= t_max) return kInfinity;
+    const float3 q = o + t * d - xyz(row0);
+    const float a = dot(q, u) / dot(u, u);
+    const float b = dot(q, v) / dot(v, v);
+    const bool inside = type == kLightRect ? (fabsf(a) <= 1.0f && fabsf(b) <= 1.0f) : (a * a + b * b <= 1.0f);
+    return inside ? t : kInfinity;
+}
+
+__device__ __forceinline__ float light_hit_pdf(const float4 *lights, uint32_t light, float3 o, float3 d, float t) {
+    const float4 row0 = light_at(lights, light, 0);
+    const uint32_t type = (uint32_t)row0.w;
+    if (type == kLightSphere) {
+        const float3 to_center = xyz(row0) - o;
+        const float r = light_at(lights, light, 1).w;
+        const float cos_max = sqrtf(fmaxf(0.0f, 1.0f - r * r / dot(to_center, to_center)));
+        return 1.0f / (2.0f * kPi * fmaxf(1e-12f, 1.0f - cos_max));
+    }
+    if (type == kLightDistant) return 1.0f / (2.0f * kPi * fmaxf(1e-12f, 1.0f - light_at(lights, light, 2).w));
+    const float4 row3 = light_at(lights, light, 3);
+    const float cos_light = fmaxf(1e-12f, -dot(d, xyz(row3)));
+    return t * t / (cos_light * row3.w);
+}
+
+// ---- lighttree.glsl ------------------------------------------------------------------
+
+struct TreeView {
+    const float4 *nodes;     // 3 per node
+    const uint2 *links;      // per node: first child or emitter, leaf flag
+    const uint4 *records;    // per emitter: code, trail, depth, -
+    const uint32_t *triangle_map;  // per triangle slot: emitter or kNone
+    uint32_t node_count;
+};
+
+__device__ __forceinline__ float safe_sqrt(float x) { return sqrtf(fmaxf(0.0f, x)); }
+
+__device__ __forceinline__ float tree_importance(const TreeView &t, uint32_t node, float3 p, float3 n) {
+    const float4 a = __ldg(&t.nodes[node * 3]), b = __ldg(&t.nodes[node * 3 + 1]), c = __ldg(&t.nodes[node * 3 + 2]);
+    if (a.w <= 0.0f) return 0.0f;
+    const float3 center = 0.5f * (xyz(a) + xyz(b));
+    const float3 offset = p - center;
+    const float radius = 0.5f * length(xyz(b) - xyz(a));
+    const float oo = dot(offset, offset);
+    const float distance2 = fmaxf(oo, radius);
+    const float3 wi = oo > 0.0f ? normalize(offset) : xyz(c);
+    const float cos_w = dot(xyz(c), wi);
+    const float sin_w = safe_sqrt(1.0f - cos_w * cos_w);
+    const float cos_b = oo < radius * radius ? -1.0f : safe_sqrt(1.0f - radius * radius / oo);
+    const float sin_b = safe_sqrt(1.0f - cos_b * cos_b);
+    const float cos_o = b.w;
+    const float sin_o = safe_sqrt(1.0f - cos_o * cos_o);
+    const float cos_x = cos_w > cos_o ? 1.0f : cos_w * cos_o + sin_w * sin_o;
+    const float sin_x = cos_w > cos_o ? 0.0f : sin_w * cos_o - cos_w * sin_o;
+    const float cos_p = cos_x > cos_b ? 1.0f : cos_x * cos_b + sin_x * sin_b;
+    if (cos_p <= c.w) return 0.0f;
+    const float importance = a.w * cos_p / distance2;
+    const float cos_i = fabsf(dot(wi, n));
+    const float sin_i = safe_sqrt(1.0f - cos_i * cos_i);
+    const float cos_pi = cos_i > cos_b ? 1.0f : cos_i * cos_b + sin_i * sin_b;
+    return fmaxf(importance * cos_pi, 0.0f);
+}
+
+__device__ __forceinline__ bool tree_sample(const TreeView &t, float u, float3 p, float3 n, uint32_t &emitter, float &pdf) {
+    pdf = 1.0f;
+    emitter = 0;
+    if (t.node_count < 1) return false;
+    uint32_t node = 0;
+    for (uint32_t depth = 0; depth < 64u; depth++) {
+        const uint2 link = __ldg(&t.links[node]);
+        if ((link.y & kLeafNode) != 0u) {
+            emitter = link.x;
+            return pdf > 0.0f;
+        }
+        const float left = tree_importance(t, link.x, p, n);
+        const float right = tree_importance(t, link.x + 1u, p, n);
+        if (left + right <= 0.0f) return false;
+        const float chance = left / (left + right);
+        if (u < chance) {
+            u = fminf(u / chance, 0.99999994f);
+            pdf *= chance;
+            node = link.x;
+        } else {
+            u = fminf((u - chance) / (1.0f - chance), 0.99999994f);
+            pdf *= 1.0f - chance;
+            node = link.x + 1u;
+        }
+    }
+    return false;
+}
+
+__device__ __forceinline__ float tree_pdf(const TreeView &t, uint32_t emitter, float3 p, float3 n) {
+    const uint4 record = __ldg(&t.records[emitter]);
+    const uint32_t trail = record.y, depth = record.z;
+    uint32_t node = 0;
+    float pdf = 1.0f;
+    for (uint32_t level = 0; level < depth; level++) {
+        const uint32_t link = __ldg(&t.links[node]).x;
+        const float left = tree_importance(t, link, p, n);
+        const float right = tree_importance(t, link + 1u, p, n);
+        if (left + right <= 0.0f) return 0.0f;
+        const uint32_t bit = (trail >> level) & 1u;
+        pdf *= bit == 0u ? left / (left + right) : right / (left + right);
+        node = link + bit;
+    }
+    return pdf;
+}
+
+// ---- EON diffuse at the Lambertian settings (openpbr.glsl:87-113) ---------------------
+
+constexpr float kFonC1 = 0.5f - 2.0f / (3.0f * kPi);
+constexpr float kFonC2 = 2.0f / 3.0f - 28.0f / (15.0f * kPi);
+
+__device__ __forceinline__ float fon_albedo(float mu, float r) {
+    const float m = 1.0f - mu;
+    const float g_over_pi = m * (0.0571085289f + m * (0.491881867f + m * (-0.332181442f + m * 0.0714429953f)));
+    return (1.0f + r * g_over_pi) / (1.0f + kFonC1 * r);
+}
+
+__device__ __forceinline__ float4 eon(float4 rho, float r, float3 wi, float3 wo) {
+    const float mu_i = wi.z, mu_o = wo.z;
+    const float s = dot(wi, wo) - mu_i * mu_o;
+    const float s_over_t = s > 0.0f ? s / fmaxf(mu_i, mu_o) : s;
+    const float a = 1.0f / (1.0f + kFonC1 * r);
+    const float4 single = rho * (a * (1.0f + r * s_over_t) / kPi);
+    const float e_o = fon_albedo(mu_o, r), e_i = fon_albedo(mu_i, r);
+    const float average = a * (1.0f + kFonC2 * r);
+    const float k = fmaxf(1e-7f, 1.0f - e_o) * fmaxf(1e-7f, 1.0f - e_i) / (kPi * fmaxf(1e-7f, 1.0f - average));
+    float4 multiple;
+    multiple.x = rho.x * rho.x * average / (1.0f - rho.x * (1.0f - average)) * k;
+    multiple.y = rho.y * rho.y * average / (1.0f - rho.y * (1.0f - average)) * k;
+    multiple.z = rho.z * rho.z * average / (1.0f - rho.z * (1.0f - average)) * k;
+    multiple.w = rho.w * rho.w * average / (1.0f - rho.w * (1.0f - average)) * k;
+    return single + multiple;
+}
+
+}  // namespace lr
