@@ -1,0 +1,60 @@
+"""Scenes of the reference's closed-form integrator checks (tests/gpu/integrator.lucb),
+rebuilt from this package's own primitives: a 20 x 20 floor of 8 divisions under a
+1 x 1 light at height 1, seen from the side; the same light as an emissive quad; and a
+coloured (or blackbody) 2 x 2 light over a white floor."""
+from __future__ import annotations
+
+import math
+
+import numpy as np
+
+from . import (LIGHT_RECT, MeshData, OpenPbr, camera, light, placement)
+from .scenes import grid
+
+
+def corner_irradiance(x: float, y: float, h: float) -> float:
+    """Irradiance under the corner of an x by y rectangle of radiance 1 at height h
+    (integrator.lucb:252-255)."""
+    a = math.sqrt(x * x + h * h)
+    b = math.sqrt(y * y + h * h)
+    return 0.5 * (x / a * math.atan(y / a) + y / b * math.atan(x / b))
+
+
+AREA_LIGHT_EXPECTED = 0.5 / math.pi * 4.0 * 4.0 * corner_irradiance(0.5, 0.5, 1.0)
+
+
+def _floor():
+    p, t, f = grid(20.0, 8)
+    return MeshData(p, t, faces=f, face_count=64)
+
+
+def side_camera():
+    """At (0, 0.5, 3), pitched down toward the origin, 200 mm on a 36 mm back."""
+    pitch = -math.atan2(0.5, 3.0)
+    return camera((0.0, 0.5, 3.0), (pitch, 0.0, 0.0), focal_length=200.0, horizontal_aperture=36.0)
+
+
+def area_light_scene():
+    """integrator.lucb:743-769: a 1 x 1 rect light of radiance 4 at height 1 over the floor."""
+    lamp = light(LIGHT_RECT, position=(0.0, 1.0, 0.0), rotation=(-0.5 * math.pi, 0.0, 0.0), intensity=4.0,
+                 width=1.0, height=1.0, normalize=False, visible=False)
+    return [_floor()], [side_camera()], [lamp], []
+
+
+def emissive_quad_scene():
+    """integrator.lucb:259-289: the same square as an emissive mesh (luminance 4, base
+    weight 0), sampled through the light tree."""
+    p, t, f = grid(1.0, 1)
+    glow = OpenPbr.lambert((0.8, 0.8, 0.8), emission=4.0)
+    glow.base_weight = 0.0
+    quad = MeshData(p, t, faces=f, face_count=1, face_materials=[1], transform=placement((0.0, 1.0, 0.0)))
+    return [_floor(), quad], [side_camera()], [], [glow]
+
+
+def colored_light_scene(color=(1.0, 0.4, 0.1), kelvin: float = 0.0):
+    """integrator.lucb:773-798: a 2 x 2 light of intensity 10 (normalized) at height 2."""
+    pitch = -math.atan2(2.0, 4.0)
+    cam = camera((0.0, 2.0, 4.0), (pitch, 0.0, 0.0), focal_length=35.0, horizontal_aperture=36.0)
+    lamp = light(LIGHT_RECT, position=(0.0, 2.0, 0.0), rotation=(-0.5 * math.pi, 0.0, 0.0), color=color,
+                 intensity=10.0, temperature=kelvin, width=2.0, height=2.0, normalize=True, visible=False)
+    return [_floor()], [cam], [lamp], []

@@ -1,0 +1,721 @@
+/*
+ * Oracle (test infrastructure): the reference's path-tracing estimator restated in f64,
+ * one path at a time over the same Owen-scrambled Sobol samples the kernels draw:
+ * camera.comp:14-50, intersect_closest.comp:45-76, shade_surface.comp:48-312 at the
+ * Lambertian settings, shade_miss.comp:12-51, intersect_shadow.comp:51-92 (opaque),
+ * finish.comp:13-39 and film_convert.comp:36-53, with the helpers of common.glsl,
+ * spectrum.glsl, lights.glsl, lighttree.glsl and openpbr.glsl (EON, 87-113).
+ * Traversal walks the same BVH nodes in f64 (box tests and Moller-Trumbore in f64).
+ * Per pixel it returns the mean and the variance of the per-sample ACEScg values.
+ */
+#include <math.h>
+#include <pthread.h>
+#include <stdlib.h>
+#include <string.h>
+#include <unistd.h>
+
+#include "oracle.h"
+#include "oracle_render.h"
+
+#define PI 3.14159265358979323846
+#define INF 3.0e38
+#define NONE 0xffffffffu
+#define LIGHT_HIT 0x80000000u
+
+typedef struct {
+    double x, y, z;
+} d3;
+
+static d3 v3(double x, double y, double z) { d3 r = {x, y, z}; return r; }
+static d3 add(d3 a, d3 b) { return v3(a.x + b.x, a.y + b.y, a.z + b.z); }
+static d3 sub(d3 a, d3 b) { return v3(a.x - b.x, a.y - b.y, a.z - b.z); }
+static d3 mul(d3 a, double s) { return v3(a.x * s, a.y * s, a.z * s); }
+static double dot(d3 a, d3 b) { return a.x * b.x + a.y * b.y + a.z * b.z; }
+static d3 cross(d3 a, d3 b) { return v3(a.y * b.z - a.z * b.y, a.z * b.x - a.x * b.z, a.x * b.y - a.y * b.x); }
+static double len(d3 a) { return sqrt(dot(a, a)); }
+static d3 norm(d3 a) { return mul(a, 1.0 / len(a)); }
+static d3 neg(d3 a) { return v3(-a.x, -a.y, -a.z); }
+
+typedef struct {
+    double s[4];
+} spec;
+
+static spec spec_scale(spec a, double k) { for (int i = 0; i < 4; i++) a.s[i] *= k; return a; }
+static spec spec_mul(spec a, spec b) { for (int i = 0; i < 4; i++) a.s[i] *= b.s[i]; return a; }
+static spec spec_add(spec a, spec b) { for (int i = 0; i < 4; i++) a.s[i] += b.s[i]; return a; }
+static spec spec_zero(void) { spec z = {{0, 0, 0, 0}}; return z; }
+
+/* ---- scene access ----------------------------------------------------------------- */
+
+static d3 point(const or_render_desc *r, uint32_t i) {
+    const float *p = &r->positions[(size_t)i * 3];
+    return v3(p[0], p[1], p[2]);
+}
+
+static double box_entry64(const or_node *n, d3 o, d3 inv, double tmax) {
+    double lo[3] = {n->lo[0], n->lo[1], n->lo[2]}, hi[3] = {n->hi[0], n->hi[1], n->hi[2]};
+    double oo[3] = {o.x, o.y, o.z}, iv[3] = {inv.x, inv.y, inv.z};
+    double enter = 0.0, leave = tmax;
+    for (int k = 0; k < 3; k++) {
+        double a = (lo[k] - oo[k]) * iv[k], b = (hi[k] - oo[k]) * iv[k];
+        double n0 = a < b ? a : b, f0 = a < b ? b : a;
+        if (n0 > enter) enter = n0;
+        if (f0 < leave) leave = f0;
+    }
+    /* A little slack for f64 rounding at box faces. */
+    return enter <= leave * (1.0 + 1e-12) + 1e-12 ? enter : -1.0;
+}
+
+static double tri_hit64(const or_render_desc *r, uint32_t slot, d3 o, d3 d, double tmax, double *u_out, double *v_out) {
+    d3 a = point(r, r->indices[slot * 3]);
+    d3 e1 = sub(point(r, r->indices[slot * 3 + 1]), a), e2 = sub(point(r, r->indices[slot * 3 + 2]), a);
+    d3 q = cross(d, e2);
+    double det = dot(e1, q);
+    if (fabs(det) < 1e-30) return -1.0;
+    d3 s = sub(o, a);
+    double u = dot(s, q) / det;
+    if (u < 0.0 || u > 1.0) return -1.0;
+    d3 rr = cross(s, e1);
+    double v = dot(d, rr) / det;
+    if (v < 0.0 || u + v > 1.0) return -1.0;
+    double t = dot(e2, rr) / det;
+    if (!(t > 0.0 && t < tmax)) return -1.0;
+    *u_out = u;
+    *v_out = v;
+    return t;
+}
+
+/* trace_closest / trace_any over the BVH, in f64. Returns the slot or NONE. */
+static uint32_t trace64(const or_render_desc *r, d3 o, d3 d, double tmax, int any, double *t_out, double *u_out,
+                        double *v_out) {
+    const or_node *nodes = r->nodes;
+    *t_out = tmax;
+    if (r->triangle_count == 0) return NONE;
+    d3 inv;
+    double dd[3] = {d.x, d.y, d.z}, iv[3];
+    for (int k = 0; k < 3; k++) {
+        double x = dd[k];
+        if (fabs(x) < 1e-20) x = x > 0 ? 1e-20 : (x < 0 ? -1e-20 : 1e-20);
+        iv[k] = 1.0 / x;
+    }
+    inv = v3(iv[0], iv[1], iv[2]);
+    if (box_entry64(&nodes[0], o, inv, tmax) < 0.0) return NONE;
+    uint32_t stack[128];
+    int depth = 0;
+    uint32_t node = 0, best = NONE;
+    double best_t = tmax;
+    for (;;) {
+        const or_node *n = &nodes[node];
+        if (n->count > 0) {
+            for (uint32_t i = 0; i < n->count; i++) {
+                double u, v;
+                double t = tri_hit64(r, n->first + i, o, d, best_t, &u, &v);
+                if (t > 0.0) {
+                    best_t = t;
+                    best = n->first + i;
+                    *u_out = u;
+                    *v_out = v;
+                    if (any) {
+                        *t_out = best_t;
+                        return best;
+                    }
+                }
+            }
+        } else {
+            double a = box_entry64(&nodes[n->first], o, inv, best_t);
+            double b = box_entry64(&nodes[n->first + 1], o, inv, best_t);
+            if (a >= 0.0 && b >= 0.0) {
+                uint32_t near_ = a <= b ? n->first : n->first + 1;
+                stack[depth++] = near_ == n->first ? n->first + 1 : n->first;
+                node = near_;
+                continue;
+            }
+            if (a >= 0.0) { node = n->first; continue; }
+            if (b >= 0.0) { node = n->first + 1; continue; }
+        }
+        if (depth == 0) break;
+        node = stack[--depth];
+    }
+    *t_out = best_t;
+    return best;
+}
+
+/* ---- spectra and lights ---------------------------------------------------------------- */
+
+static spec spec_of(const or_render_desc *r, const float fit[4], const float rgb[3], const double lambda[4]) {
+    spec s;
+    if (!r->spectral) {
+        s.s[0] = rgb[0], s.s[1] = rgb[1], s.s[2] = rgb[2], s.s[3] = 0.0;
+        return s;
+    }
+    for (int i = 0; i < 4; i++) {
+        double x = (lambda[i] - 360.0) / (830.0 - 360.0);
+        double z = ((double)fit[0] * x + fit[1]) * x + fit[2];
+        s.s[i] = fit[3] * (0.5 + z / (2.0 * sqrt(1.0 + z * z)));
+    }
+    return s;
+}
+
+static double spec_max(const or_render_desc *r, spec s) {
+    double m = fmax(s.s[0], fmax(s.s[1], s.s[2]));
+    return r->spectral ? fmax(m, s.s[3]) : m;
+}
+
+static double blackbody_f(double lambda, double kelvin) {
+    double peak = 2.8977721e6 / kelvin, x = 1.4387769e7 / (lambda * kelvin), q = peak / lambda;
+    return q * q * q * q * q * (142.32492 / (exp(x) - 1.0));
+}
+
+static const float *row(const or_render_desc *r, uint32_t light, int k) { return &r->light_rows[light * 28 + k * 4]; }
+static uint32_t light_type(const or_render_desc *r, uint32_t l) { return (uint32_t)row(r, l, 0)[3]; }
+static int light_visible(const or_render_desc *r, uint32_t l) { return ((uint32_t)row(r, l, 5)[3] & 1u) != 0; }
+static d3 rv(const float *x) { return v3(x[0], x[1], x[2]); }
+
+static spec light_radiance(const or_render_desc *r, uint32_t light, const double lambda[4]) {
+    const float *rgb = row(r, light, 5);
+    spec s = spec_of(r, row(r, light, 4), rgb, lambda);
+    if (r->spectral && ((uint32_t)rgb[3] & 2u))
+        for (int i = 0; i < 4; i++) s.s[i] *= blackbody_f(lambda[i], row(r, light, 6)[0]);
+    return s;
+}
+
+typedef struct {
+    d3 direction;
+    double distance, pdf;
+    int delta;
+} lsample;
+
+static void onb(d3 n, d3 *t, d3 *b) {
+    double s = n.z >= 0.0 ? 1.0 : -1.0, a = -1.0 / (s + n.z), c = n.x * n.y * a;
+    *t = v3(1.0 + s * n.x * n.x * a, s * c, -s * n.x);
+    *b = v3(c, s + n.y * n.y * a, -n.y);
+}
+
+static d3 sample_cone(d3 axis, double cos_max, double u0, double u1) {
+    double c = 1.0 - u0 * (1.0 - cos_max), s = sqrt(fmax(0.0, 1.0 - c * c)), phi = 2.0 * PI * u1;
+    d3 t, b;
+    onb(axis, &t, &b);
+    return norm(add(add(mul(t, s * cos(phi)), mul(b, s * sin(phi))), mul(axis, c)));
+}
+
+static void concentric(double u0, double u1, double *x, double *y) {
+    double ox = 2.0 * u0 - 1.0, oy = 2.0 * u1 - 1.0, rr, th;
+    if (ox == 0.0 && oy == 0.0) { *x = *y = 0.0; return; }
+    if (fabs(ox) > fabs(oy)) { rr = ox; th = (PI / 4.0) * (oy / ox); }
+    else { rr = oy; th = (PI / 2.0) - (PI / 4.0) * (ox / oy); }
+    *x = rr * cos(th);
+    *y = rr * sin(th);
+}
+
+static double sphere_hit(d3 c, double radius, d3 o, d3 d) {
+    d3 oc = sub(o, c);
+    double b = dot(oc, d), cc = dot(oc, oc) - radius * radius, h = b * b - cc;
+    if (h < 0.0) return INF;
+    h = sqrt(h);
+    double t = -b - h;
+    if (t > 0.0) return t;
+    t = -b + h;
+    return t > 0.0 ? t : INF;
+}
+
+static int sample_light(const or_render_desc *r, uint32_t light, d3 p, double u0, double u1, lsample *s) {
+    const float *r0 = row(r, light, 0), *r1 = row(r, light, 1), *r2 = row(r, light, 2), *r3 = row(r, light, 3);
+    uint32_t type = (uint32_t)r0[3];
+    s->delta = 0;
+    if (type == 0 || type == 1) {
+        double ax, ay;
+        if (type == 0) ax = 2.0 * u0 - 1.0, ay = 2.0 * u1 - 1.0;
+        else concentric(u0, u1, &ax, &ay);
+        d3 q = add(add(rv(r0), mul(rv(r1), ax)), mul(rv(r2), ay));
+        d3 d = sub(q, p);
+        double d2 = dot(d, d);
+        s->distance = sqrt(d2);
+        s->direction = mul(d, 1.0 / s->distance);
+        double cl = -dot(s->direction, rv(r3));
+        if (cl <= 0.0 || r3[3] <= 0.0) return 0;
+        s->pdf = d2 / (cl * r3[3]);
+        return 1;
+    }
+    if (type == 2) {
+        d3 tc = sub(rv(r0), p);
+        double d2 = dot(tc, tc), rad = r1[3];
+        if (d2 <= rad * rad) return 0;
+        double cos_max = sqrt(fmax(0.0, 1.0 - rad * rad / d2));
+        s->direction = sample_cone(mul(tc, 1.0 / sqrt(d2)), cos_max, u0, u1);
+        s->distance = sphere_hit(rv(r0), rad, p, s->direction);
+        if (s->distance >= INF) return 0;
+        s->pdf = 1.0 / (2.0 * PI * (1.0 - cos_max));
+        return 1;
+    }
+    d3 axis = neg(rv(r3));
+    double cos_half = r2[3];
+    s->distance = INF;
+    if (cos_half >= 1.0 - 1e-7) {
+        s->direction = axis;
+        s->pdf = 1.0;
+        s->delta = 1;
+        return 1;
+    }
+    s->direction = sample_cone(axis, cos_half, u0, u1);
+    s->pdf = 1.0 / (2.0 * PI * (1.0 - cos_half));
+    return 1;
+}
+
+static double intersect_light(const or_render_desc *r, uint32_t light, d3 o, d3 d, double t_max) {
+    const float *r0 = row(r, light, 0);
+    uint32_t type = (uint32_t)r0[3];
+    if (type == 2) {
+        double t = sphere_hit(rv(r0), row(r, light, 1)[3], o, d);
+        return t < t_max ? t : INF;
+    }
+    if (type >= 3) return INF;
+    d3 u = rv(row(r, light, 1)), v = rv(row(r, light, 2)), n = rv(row(r, light, 3));
+    double facing = dot(d, n);
+    if (facing >= 0.0) return INF;
+    double t = dot(sub(rv(r0), o), n) / facing;
+    if (t <= 0.0 || t >= t_max) return INF;
+    d3 q = sub(add(o, mul(d, t)), rv(r0));
+    double a = dot(q, u) / dot(u, u), b = dot(q, v) / dot(v, v);
+    int inside = type == 0 ? (fabs(a) <= 1.0 && fabs(b) <= 1.0) : (a * a + b * b <= 1.0);
+    return inside ? t : INF;
+}
+
+static double light_hit_pdf(const or_render_desc *r, uint32_t light, d3 o, d3 d, double t) {
+    const float *r0 = row(r, light, 0);
+    uint32_t type = (uint32_t)r0[3];
+    if (type == 2) {
+        d3 tc = sub(rv(r0), o);
+        double rad = row(r, light, 1)[3];
+        double cos_max = sqrt(fmax(0.0, 1.0 - rad * rad / dot(tc, tc)));
+        return 1.0 / (2.0 * PI * fmax(1e-12, 1.0 - cos_max));
+    }
+    if (type == 3) return 1.0 / (2.0 * PI * fmax(1e-12, 1.0 - row(r, light, 2)[3]));
+    const float *r3 = row(r, light, 3);
+    double cl = fmax(1e-12, -dot(d, rv(r3)));
+    return t * t / (cl * r3[3]);
+}
+
+static uint32_t pick_distant(const or_render_desc *r, double u, double *pdf) {
+    uint32_t chosen = NONE;
+    for (uint32_t l = 0; l < r->light_count; l++) {
+        if (light_type(r, l) < 3) continue;
+        chosen = l;
+        if (u < row(r, l, 6)[2]) break;
+    }
+    *pdf = chosen == NONE ? 0.0 : row(r, chosen, 6)[1];
+    return chosen;
+}
+
+static double ssqrt(double x) { return sqrt(fmax(0.0, x)); }
+
+static double tree_importance(const or_render_desc *r, uint32_t node, d3 p, d3 n) {
+    const float *a = &r->tree_nodes[node * 12], *b = a + 4, *c = a + 8;
+    if (a[3] <= 0.0f) return 0.0;
+    d3 center = mul(add(rv(a), rv(b)), 0.5);
+    d3 offset = sub(p, center);
+    double radius = 0.5 * len(sub(rv(b), rv(a)));
+    double oo = dot(offset, offset);
+    double distance2 = fmax(oo, radius);
+    d3 wi = oo > 0.0 ? norm(offset) : rv(c);
+    double cos_w = dot(rv(c), wi), sin_w = ssqrt(1.0 - cos_w * cos_w);
+    double cos_b = oo < radius * radius ? -1.0 : ssqrt(1.0 - radius * radius / oo);
+    double sin_b = ssqrt(1.0 - cos_b * cos_b);
+    double cos_o = b[3], sin_o = ssqrt(1.0 - cos_o * cos_o);
+    double cos_x = cos_w > cos_o ? 1.0 : cos_w * cos_o + sin_w * sin_o;
+    double sin_x = cos_w > cos_o ? 0.0 : sin_w * cos_o - cos_w * sin_o;
+    double cos_p = cos_x > cos_b ? 1.0 : cos_x * cos_b + sin_x * sin_b;
+    if (cos_p <= c[3]) return 0.0;
+    double importance = a[3] * cos_p / distance2;
+    double cos_i = fabs(dot(wi, n)), sin_i = ssqrt(1.0 - cos_i * cos_i);
+    double cos_pi = cos_i > cos_b ? 1.0 : cos_i * cos_b + sin_i * sin_b;
+    return fmax(importance * cos_pi, 0.0);
+}
+
+static int tree_sample(const or_render_desc *r, double u, d3 p, d3 n, uint32_t *emitter, double *pdf) {
+    *pdf = 1.0;
+    *emitter = 0;
+    if (r->tree_node_count < 1) return 0;
+    uint32_t node = 0;
+    for (int depth = 0; depth < 64; depth++) {
+        uint32_t link = r->tree_links[node * 2];
+        if (r->tree_links[node * 2 + 1] & 0x80000000u) {
+            *emitter = link;
+            return *pdf > 0.0;
+        }
+        double left = tree_importance(r, link, p, n), right = tree_importance(r, link + 1, p, n);
+        if (left + right <= 0.0) return 0;
+        double chance = left / (left + right);
+        if (u < chance) {
+            u = fmin(u / chance, 0.99999994);
+            *pdf *= chance;
+            node = link;
+        } else {
+            u = fmin((u - chance) / (1.0 - chance), 0.99999994);
+            *pdf *= 1.0 - chance;
+            node = link + 1;
+        }
+    }
+    return 0;
+}
+
+static double tree_pdf(const or_render_desc *r, uint32_t emitter, d3 p, d3 n) {
+    uint32_t trail = r->tree_records[emitter * 4 + 1], depth = r->tree_records[emitter * 4 + 2];
+    uint32_t node = 0;
+    double pdf = 1.0;
+    for (uint32_t level = 0; level < depth; level++) {
+        uint32_t link = r->tree_links[node * 2];
+        double left = tree_importance(r, link, p, n), right = tree_importance(r, link + 1, p, n);
+        if (left + right <= 0.0) return 0.0;
+        uint32_t bit = (trail >> level) & 1u;
+        pdf *= bit == 0 ? left / (left + right) : right / (left + right);
+        node = link + bit;
+    }
+    return pdf;
+}
+
+static const float *material(const or_render_desc *r, uint32_t m, int k) { return &r->materials[m * 64 + k * 4]; }
+
+static double mis_weight(double a, double b) {
+    a = fmin(a, 1e18);
+    b = fmin(b, 1e18);
+    return 1.0 / (1.0 + a * a + b * b);
+}
+
+static d3 offset_origin(d3 p, d3 n) {
+    double s = fmax(1.0, fmax(fabs(p.x), fmax(fabs(p.y), fabs(p.z))));
+    return add(p, mul(n, 1e-4 * s));
+}
+
+static spec clamped(const or_render_desc *r, spec c, uint32_t total) {
+    if (total == 0 || r->clamp <= 0.0) return c;
+    double m = spec_max(r, c);
+    return m > r->clamp ? spec_scale(c, r->clamp / m) : c;
+}
+
+static double fon_albedo(double mu, double rr) {
+    double m = 1.0 - mu;
+    double g = m * (0.0571085289 + m * (0.491881867 + m * (-0.332181442 + m * 0.0714429953)));
+    return (1.0 + rr * g) / (1.0 + (0.5 - 2.0 / (3.0 * PI)) * rr);
+}
+
+static spec eon(spec rho, double rr, d3 wi, d3 wo) {
+    const double c1 = 0.5 - 2.0 / (3.0 * PI), c2 = 2.0 / 3.0 - 28.0 / (15.0 * PI);
+    double s = dot(wi, wo) - wi.z * wo.z;
+    double st = s > 0.0 ? s / fmax(wi.z, wo.z) : s;
+    double a = 1.0 / (1.0 + c1 * rr);
+    double eo = fon_albedo(wo.z, rr), ei = fon_albedo(wi.z, rr);
+    double avg = a * (1.0 + c2 * rr);
+    double k = fmax(1e-7, 1.0 - eo) * fmax(1e-7, 1.0 - ei) / (PI * fmax(1e-7, 1.0 - avg));
+    spec out;
+    for (int i = 0; i < 4; i++) {
+        double single = rho.s[i] * (a * (1.0 + rr * st) / PI);
+        double ms = rho.s[i] * rho.s[i] * avg / (1.0 - rho.s[i] * (1.0 - avg));
+        out.s[i] = single + ms * k;
+    }
+    return out;
+}
+
+static d3 oct_decode(uint32_t packed) {
+    double n[3];
+    /* The kernels decode in f32; f64 here. */
+    double x = fmax((double)(int16_t)(packed & 0xffff) / 32767.0, -1.0);
+    double y = fmax((double)(int16_t)(packed >> 16) / 32767.0, -1.0);
+    n[0] = x, n[1] = y, n[2] = 1.0 - fabs(x) - fabs(y);
+    if (n[2] < 0.0) {
+        double nx = (1.0 - fabs(y)) * (x >= 0.0 ? 1.0 : -1.0), ny = (1.0 - fabs(x)) * (y >= 0.0 ? 1.0 : -1.0);
+        n[0] = nx, n[1] = ny;
+    }
+    return norm(v3(n[0], n[1], n[2]));
+}
+
+static double tri_hit_pdf(const or_render_desc *r, uint32_t slot, d3 d, double t) {
+    d3 a = point(r, r->indices[slot * 3]);
+    d3 cr = cross(sub(point(r, r->indices[slot * 3 + 1]), a), sub(point(r, r->indices[slot * 3 + 2]), a));
+    double area = 0.5 * len(cr);
+    double cl = fabs(dot(d, cr)) / fmax(1e-20, 2.0 * area);
+    return t * t / fmax(1e-20, cl * area);
+}
+
+static void spec_to_film(const or_render_desc *r, spec rad, const double lambda[4], double out[3]) {
+    if (!r->spectral) {
+        out[0] = rad.s[0], out[1] = rad.s[1], out[2] = rad.s[2];
+        return;
+    }
+    double sum[3] = {0, 0, 0};
+    for (int i = 0; i < 4; i++) {
+        double pdf = or_wavelength_pdf(lambda[i]);
+        if (pdf > 0.0) {
+            double c[3];
+            or_cmf(lambda[i], c);
+            for (int k = 0; k < 3; k++) sum[k] += c[k] * (rad.s[i] / pdf);
+        }
+    }
+    for (int k = 0; k < 3; k++) out[k] = sum[k] * 0.25 / r->cmf_integrals[k];
+}
+
+/* One sample of one pixel: its ACEScg value. */
+static void render_sample(const or_render_desc *r, uint32_t pixel, uint32_t sample, double out[3]) {
+    const float *f = r->frame;
+    double u4[4];
+    or_sample4(r->seed, pixel, sample, 0, u4);
+    double fx = (double)(pixel % r->width) + u4[0], fy = (double)(pixel / r->width) + u4[1];
+    d3 position = v3(f[0], f[1], f[2]), corner = v3(f[4], f[5], f[6]), du = v3(f[8], f[9], f[10]),
+       dv = v3(f[12], f[13], f[14]);
+    d3 film = add(add(corner, mul(du, fx)), mul(dv, fy));
+    int ortho = f[3] > 0.5f;
+    d3 origin = ortho ? add(position, film) : position;
+    d3 dir = norm(ortho ? cross(du, dv) : film);
+    if (!ortho && r->lens_radius > 0.0) {
+        d3 fw = v3(r->forward[0], r->forward[1], r->forward[2]);
+        d3 focused = add(position, mul(dir, r->focus_distance / dot(dir, fw)));
+        double dx, dy;
+        concentric(u4[2], u4[3], &dx, &dy);
+        origin = add(add(position, mul(norm(du), dx * r->lens_radius)), mul(norm(dv), dy * r->lens_radius));
+        dir = norm(sub(focused, origin));
+    }
+    double lambda[4] = {0, 0, 0, 0};
+    if (r->spectral) {
+        double w[4];
+        or_sample4(r->seed, pixel, sample, 1, w);
+        or_sample_wavelengths(w[0], lambda);
+    }
+    spec throughput = {{1, 1, 1, 1}}, radiance = spec_zero();
+    uint32_t bounces = 0;
+    d3 vertex = origin, prev_normal = v3(0, 0, 1);
+    double survival = 1.0, ray_pdf = 0.0;
+    for (uint32_t round = 0; round <= r->max_bounces; round++) {
+        uint32_t total = bounces & 0xffu;
+        double t, hu = 0, hv = 0;
+        uint32_t what = trace64(r, origin, dir, INF, 0, &t, &hu, &hv);
+        for (uint32_t l = 0; l < r->light_count; l++) {
+            if (round == 0 && !light_visible(r, l)) continue;
+            double tl = intersect_light(r, l, origin, dir, t);
+            if (tl < t) {
+                t = tl;
+                what = LIGHT_HIT | l;
+            }
+        }
+        if (what == NONE) {
+            spec bg = spec_of(r, r->background_fit, r->background_rgb, lambda);
+            for (uint32_t l = 0; l < r->light_count; l++) {
+                if (light_type(r, l) < 3) continue;
+                double cos_half = row(r, l, 2)[3];
+                if (cos_half >= 1.0 - 1e-7 || dot(dir, neg(rv(row(r, l, 3)))) < cos_half) continue;
+                double weight = 1.0;
+                if (total == 0) {
+                    if (!light_visible(r, l)) continue;
+                } else if (ray_pdf > 0.0) {
+                    weight = mis_weight(light_hit_pdf(r, l, v3(0, 0, 0), dir, INF) * (r->p_distant * row(r, l, 6)[1]) / ray_pdf, 0.0);
+                }
+                bg = spec_add(bg, spec_scale(light_radiance(r, l, lambda), weight));
+            }
+            spec c = spec_mul(throughput, bg);
+            double m = spec_max(r, c);
+            if (total > 0 && r->clamp > 0.0 && m > r->clamp) c = spec_scale(c, r->clamp / m);
+            radiance = spec_add(radiance, c);
+            break;
+        }
+        if (what & LIGHT_HIT) {
+            uint32_t l = what & ~LIGHT_HIT;
+            double weight = 1.0;
+            if (total == 0) {
+                if (!light_visible(r, l)) break;
+            } else if (ray_pdf > 0.0) {
+                uint32_t emitter = (uint32_t)row(r, l, 6)[3];
+                double reach = len(sub(vertex, add(origin, mul(dir, t))));
+                double chance = (1.0 - r->p_distant) * tree_pdf(r, emitter, vertex, prev_normal);
+                weight = mis_weight(light_hit_pdf(r, l, vertex, dir, reach) * chance / ray_pdf, 0.0);
+            }
+            radiance = spec_add(radiance, clamped(r, spec_scale(spec_mul(throughput, light_radiance(r, l, lambda)), weight), total));
+            break;
+        }
+        uint32_t slot = what;
+        d3 p0 = point(r, r->indices[slot * 3]);
+        d3 geometric = norm(cross(sub(point(r, r->indices[slot * 3 + 1]), p0), sub(point(r, r->indices[slot * 3 + 2]), p0)));
+        if (dot(geometric, dir) > 0.0) geometric = neg(geometric);
+        const uint32_t *attr = &r->shading[slot * 4];
+        uint32_t m = attr[3];
+        d3 p = add(origin, mul(dir, t));
+        double reach = len(sub(vertex, p));
+        const float *em = material(r, m, 7);
+        if (em[3] > 0.0f) {
+            double weight = 1.0;
+            uint32_t emitter = r->tree_records && slot < r->triangle_count ? r->tree_records[r->emitter_count * 4 + slot] : NONE;
+            if (total > 0 && ray_pdf > 0.0 && emitter != NONE) {
+                double chance = (1.0 - r->p_distant) * tree_pdf(r, emitter, vertex, prev_normal);
+                weight = mis_weight(tri_hit_pdf(r, slot, dir, reach) * chance / ray_pdf, 0.0);
+            }
+            radiance = spec_add(radiance, clamped(r, spec_scale(spec_mul(throughput, spec_of(r, material(r, m, 6), em, lambda)), weight), total));
+        }
+        if (total >= r->max_bounces) break;
+        d3 normal = norm(add(add(mul(oct_decode(attr[0]), 1.0 - hu - hv), mul(oct_decode(attr[1]), hu)), mul(oct_decode(attr[2]), hv)));
+        if (dot(normal, geometric) < 0.0) normal = neg(normal);
+        d3 tg, bt;
+        onb(normal, &tg, &bt);
+        d3 wo = v3(-dot(dir, tg), -dot(dir, bt), -dot(dir, normal));
+        const float *brgb = material(r, m, 1);
+        spec base = spec_scale(spec_of(r, material(r, m, 0), brgb, lambda), brgb[3]);
+        double rough = material(r, m, 10)[1];
+        double lum = (brgb[0] * 0.2722287168 + brgb[1] * 0.6740817658 + brgb[2] * 0.0536895174) * brgb[3];
+        double p_diffuse = fmax(lum, 0.0) > 0.0 ? 1.0 : 0.0;
+        d3 from = offset_origin(p, geometric);
+        double ul[4];
+        or_sample4(r->seed, pixel, sample, 2 + 3 * total, ul);
+        lsample s;
+        spec emitted = spec_zero();
+        double chance = 0.0;
+        int sampled = 0;
+        if (ul[0] < r->p_distant) {
+            double share;
+            uint32_t l = pick_distant(r, ul[0] / r->p_distant, &share);
+            if (l != NONE && share > 0.0 && sample_light(r, l, p, ul[1], ul[2], &s)) {
+                chance = r->p_distant * share;
+                emitted = light_radiance(r, l, lambda);
+                sampled = 1;
+            }
+        } else {
+            uint32_t emitter;
+            double tc;
+            if (tree_sample(r, (ul[0] - r->p_distant) / fmax(1e-7, 1.0 - r->p_distant), from, normal, &emitter, &tc)) {
+                chance = (1.0 - r->p_distant) * tc;
+                uint32_t code = r->tree_records[emitter * 4];
+                if (code & 0x80000000u) {
+                    uint32_t ts = code & 0x7fffffffu;
+                    d3 a = point(r, r->indices[ts * 3]), b = point(r, r->indices[ts * 3 + 1]), c = point(r, r->indices[ts * 3 + 2]);
+                    double rr = sqrt(ul[1]);
+                    d3 q = add(add(mul(a, 1.0 - rr), mul(b, rr * (1.0 - ul[2]))), mul(c, rr * ul[2]));
+                    d3 cr = cross(sub(b, a), sub(c, a));
+                    double area = 0.5 * len(cr);
+                    d3 d = sub(q, p);
+                    double d2 = dot(d, d);
+                    if (area > 0.0 && d2 > 0.0) {
+                        s.distance = sqrt(d2);
+                        s.direction = mul(d, 1.0 / s.distance);
+                        double cl = fabs(dot(s.direction, cr)) / (2.0 * area);
+                        if (cl > 0.0) {
+                            s.pdf = d2 / (cl * area);
+                            s.delta = 0;
+                            uint32_t tm = r->shading[ts * 4 + 3];
+                            emitted = spec_of(r, material(r, tm, 6), material(r, tm, 7), lambda);
+                            sampled = 1;
+                        }
+                    }
+                } else if (sample_light(r, code, p, ul[1], ul[2], &s)) {
+                    emitted = light_radiance(r, code, lambda);
+                    sampled = 1;
+                }
+            }
+        }
+        if (sampled && chance > 0.0) {
+            double side = dot(s.direction, geometric);
+            d3 wi = v3(dot(s.direction, tg), dot(s.direction, bt), dot(s.direction, normal));
+            if (side > 0.0 && wi.z > 0.0 && wo.z > 0.0) {
+                double bsdf_pdf = p_diffuse * wi.z / PI;
+                if (bsdf_pdf > 0.0) {
+                    spec fv = eon(base, rough, wi, wo);
+                    double light_pdf = s.pdf * chance;
+                    double weight = s.delta ? 1.0 : mis_weight(bsdf_pdf / light_pdf, 0.0);
+                    spec c = clamped(r, spec_scale(spec_mul(spec_mul(throughput, fv), emitted), fabs(wi.z) * (weight / light_pdf)), total);
+                    d3 target = add(p, mul(s.direction, s.distance));
+                    double margin = 4e-4 * fmax(1.0, fmax(fabs(target.x), fmax(fabs(target.y), fabs(target.z))));
+                    double sreach = s.distance >= INF ? INF : fmax(0.0, s.distance - margin);
+                    double tt, uu, vv;
+                    if (trace64(r, offset_origin(p, geometric), s.direction, sreach, 1, &tt, &uu, &vv) == NONE)
+                        radiance = spec_add(radiance, c);
+                }
+            }
+        }
+        double u[4];
+        or_sample4(r->seed, pixel, sample, 3 + 3 * total, u);
+        if (wo.z <= 0.0 || !(u[3] < p_diffuse)) break;
+        double dx, dy;
+        concentric(u[0], u[1], &dx, &dy);
+        d3 wi = v3(dx, dy, sqrt(fmax(0.0, 1.0 - (dx * dx + dy * dy))));
+        if (wi.z == 0.0) break;
+        double pdf = p_diffuse * wi.z / PI;
+        if (!(pdf > 0.0)) break;
+        spec weight = spec_scale(eon(base, rough, wi, wo), fabs(wi.z) / pdf);
+        d3 direction = add(add(mul(tg, wi.x), mul(bt, wi.y)), mul(normal, wi.z));
+        double side = dot(direction, geometric);
+        if ((side > 0.0) != (wi.z > 0.0)) break;
+        uint32_t kind = ((bounces >> 8) & 0xffu) + 1u;
+        if ((double)kind > r->diffuse_limit || (bounces & 0xffu) >= 255u) break;
+        bounces = (bounces & ~(0xffu << 8)) + (kind << 8) + 1u;
+        throughput = spec_mul(throughput, weight);
+        double scale = fmin(survival, 1e6);
+        if (total + 1 >= 3) {
+            double survive = fmin(0.95, spec_max(r, throughput) * scale);
+            if (u[2] >= survive) break;
+            throughput = spec_scale(throughput, 1.0 / survive);
+        }
+        d3 next = side > 0.0 ? from : offset_origin(p, neg(geometric));
+        prev_normal = normal;
+        origin = next;
+        vertex = next;
+        survival = scale;
+        dir = direction;
+        ray_pdf = pdf;
+    }
+    double value[3];
+    spec_to_film(r, radiance, lambda, value);
+    if (!isfinite(value[0]) || !isfinite(value[1]) || !isfinite(value[2])) value[0] = value[1] = value[2] = 0.0;
+    if (r->spectral) {
+        for (int i = 0; i < 3; i++) out[i] = r->film[i * 3] * value[0] + r->film[i * 3 + 1] * value[1] + r->film[i * 3 + 2] * value[2];
+    } else {
+        out[0] = value[0], out[1] = value[1], out[2] = value[2];
+    }
+}
+
+typedef struct {
+    const or_render_desc *r;
+    uint32_t samples;
+    double *mean, *var;
+    size_t next, n;
+    pthread_mutex_t lock;
+} render_job;
+
+static void *render_worker(void *arg) {
+    render_job *j = arg;
+    for (;;) {
+        pthread_mutex_lock(&j->lock);
+        size_t begin = j->next;
+        j->next = begin + 16 < j->n ? begin + 16 : j->n;
+        size_t end = j->next;
+        pthread_mutex_unlock(&j->lock);
+        if (begin >= end) break;
+        for (size_t pixel = begin; pixel < end; pixel++) {
+            double m[3] = {0, 0, 0}, m2[3] = {0, 0, 0};
+            for (uint32_t s = 0; s < j->samples; s++) {
+                double v[3];
+                render_sample(j->r, (uint32_t)pixel, s, v);
+                for (int k = 0; k < 3; k++) {
+                    double delta = v[k] - m[k];
+                    m[k] += delta / (double)(s + 1);
+                    m2[k] += delta * (v[k] - m[k]);
+                }
+            }
+            for (int k = 0; k < 3; k++) {
+                j->mean[pixel * 3 + k] = m[k];
+                j->var[pixel * 3 + k] = j->samples > 1 ? m2[k] / (double)(j->samples - 1) : 0.0;
+            }
+        }
+    }
+    return NULL;
+}
+
+void or_render(const or_render_desc *r, uint32_t samples, double *mean, double *var, int threads) {
+    if (threads <= 0) threads = (int)sysconf(_SC_NPROCESSORS_ONLN);
+    if (threads > 256) threads = 256;
+    render_job j;
+    j.r = r;
+    j.samples = samples;
+    j.mean = mean;
+    j.var = var;
+    j.next = 0;
+    j.n = (size_t)r->width * r->height;
+    pthread_mutex_init(&j.lock, NULL);
+    pthread_t ids[256];
+    for (int i = 0; i < threads; i++) pthread_create(&ids[i], NULL, render_worker, &j);
+    for (int i = 0; i < threads; i++) pthread_join(ids[i], NULL);
+    pthread_mutex_destroy(&j.lock);
+}

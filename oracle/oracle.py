@@ -338,3 +338,82 @@ def light_tree(positions, indices, shading, light_rows, materials):
     }
     lib.or_light_tree_free(C.byref(tree))
     return out
+
+
+class RenderDesc(C.Structure):
+    _fields_ = [("positions", C.POINTER(C.c_float)), ("indices", C.POINTER(C.c_uint32)),
+                ("shading", C.POINTER(C.c_uint32)), ("triangle_count", C.c_size_t), ("nodes", C.c_void_p),
+                ("light_rows", C.POINTER(C.c_float)), ("light_count", C.c_uint32),
+                ("tree_nodes", C.POINTER(C.c_float)), ("tree_links", C.POINTER(C.c_uint32)),
+                ("tree_records", C.POINTER(C.c_uint32)), ("tree_node_count", C.c_uint32),
+                ("emitter_count", C.c_uint32), ("materials", C.POINTER(C.c_float)), ("p_distant", C.c_double),
+                ("background_fit", C.c_float * 4), ("background_rgb", C.c_float * 3), ("film", C.c_double * 9),
+                ("cmf_integrals", C.c_double * 3), ("frame", C.c_float * 16), ("lens_radius", C.c_double),
+                ("focus_distance", C.c_double), ("forward", C.c_double * 3), ("width", C.c_uint32),
+                ("height", C.c_uint32), ("max_bounces", C.c_uint32), ("spectral", C.c_uint32), ("seed", C.c_uint32),
+                ("diffuse_limit", C.c_double), ("clamp", C.c_double)]
+
+
+def render(arrays: dict, lights, library, frame, samples: int, max_bounces: int, spectral: bool, seed: int = 1,
+           background=(0.0, 0.0, 0.0), clamp: float = 0.0, diffuse_limit: float = 1024.0, threads: int = 0):
+    """The f64 estimator over a compiled scene's arrays (leaf order), the scene's lights
+    (luce_render_b200.Light), the material library (default first, OrMaterial or
+    luce_render_b200.OpenPbr) and a luce_render_b200.Frame. Returns (mean, variance),
+    each height x width x 3 (ACEScg)."""
+    positions = np.ascontiguousarray(arrays["positions"], np.float32).reshape(-1)
+    indices = np.ascontiguousarray(arrays["indices"], np.uint32).reshape(-1)
+    shading = np.ascontiguousarray(arrays["shading"], np.uint32).reshape(-1)
+    nodes = np.ascontiguousarray(arrays["nodes"], NODE_DTYPE)
+    T = len(indices) // 3
+    root = nodes[0]
+    radius = 1.0
+    if T and root["lo"][0] <= root["hi"][0]:
+        d = (root["hi"].astype(np.float64) - root["lo"].astype(np.float64))
+        radius = max(1.0, 0.5 * float(np.sqrt((d * d).sum())))
+    rows, distant_power = pack_lights(list(lights), radius)
+    mats = [m if isinstance(m, OrMaterial) else material_from(m) for m in library]
+    tree = light_tree(positions, indices, shading, rows, mats)
+    total = distant_power + tree["energy"]
+    if tree["emitter_count"] > 0:
+        p_distant = distant_power / total if total > 0 else 0.0
+    else:
+        p_distant = 1.0 if distant_power > 0 else 0.0
+    material_rows = np.concatenate([pack_material(m) for m in mats]).astype(np.float32)
+    rows = np.ascontiguousarray(rows.reshape(-1), np.float32)
+    tnodes = np.ascontiguousarray(tree["nodes"].reshape(-1), np.float32)
+    tlinks = np.ascontiguousarray(tree["links"].reshape(-1), np.uint32)
+    trec = np.ascontiguousarray(tree["records"], np.uint32)
+    keep = [positions, indices, shading, nodes, rows, tnodes, tlinks, trec, material_rows]
+    r = RenderDesc()
+    r.positions, r.indices, r.shading = _p(positions, _f), _p(indices, _u), _p(shading, _u)
+    r.triangle_count = T
+    r.nodes = nodes.ctypes.data_as(C.c_void_p)
+    r.light_rows = _p(rows, _f)
+    r.light_count = len(rows) // 28
+    r.tree_nodes = _p(tnodes, _f) if len(tnodes) else None
+    r.tree_links = _p(tlinks, _u) if len(tlinks) else None
+    r.tree_records = _p(trec, _u) if len(trec) else None
+    r.tree_node_count = tree["node_count"]
+    r.emitter_count = tree["emitter_count"]
+    r.materials = _p(material_rows, _f)
+    r.p_distant = p_distant
+    r.background_fit[:] = [float(x) for x in fit_spectrum(background)]
+    r.background_rgb[:] = [float(x) for x in background]
+    r.film[:] = list(film_matrix().reshape(-1))
+    r.cmf_integrals[:] = list(cmf_integrals())
+    r.frame[:] = [float(x) for x in frame.pack()]
+    r.lens_radius = frame.lens_radius
+    r.focus_distance = frame.focus_distance
+    r.forward[:] = list(frame.forward)
+    r.width, r.height = frame.width, frame.height
+    r.max_bounces = max_bounces
+    r.spectral = 1 if spectral else 0
+    r.seed = seed
+    r.diffuse_limit = diffuse_limit
+    r.clamp = clamp
+    n = frame.width * frame.height
+    mean = np.zeros(n * 3, np.float64)
+    var = np.zeros(n * 3, np.float64)
+    lib.or_render(C.byref(r), C.c_uint32(samples), _p(mean, C.c_double), _p(var, C.c_double), threads)
+    del keep
+    return mean.reshape(frame.height, frame.width, 3), var.reshape(frame.height, frame.width, 3)

@@ -1,0 +1,46 @@
+/*
+ * Oracle (test infrastructure): the f64 restatement of the integrator's estimator
+ * (oracle/integrator.c). The caller passes the compiled scene (leaf order), the loaded
+ * records (light rows, light tree, material records as the reference packs them) and the
+ * view; the oracle returns per pixel the mean and variance of the samples' ACEScg values.
+ */
+#ifndef LUCE_ORACLE_RENDER_H
+#define LUCE_ORACLE_RENDER_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#include "oracle.h"
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+typedef struct {
+    const float *positions;
+    const uint32_t *indices;
+    const uint32_t *shading;
+    size_t triangle_count;
+    const or_node *nodes;
+    const float *light_rows; /* 28 floats per light */
+    uint32_t light_count;
+    const float *tree_nodes; /* 12 floats per node */
+    const uint32_t *tree_links;
+    const uint32_t *tree_records; /* 4 per emitter, then the triangle map */
+    uint32_t tree_node_count, emitter_count;
+    const float *materials; /* 64 floats per material */
+    double p_distant;
+    float background_fit[4], background_rgb[3];
+    double film[9], cmf_integrals[3];
+    float frame[16];
+    double lens_radius, focus_distance, forward[3];
+    uint32_t width, height, max_bounces, spectral, seed;
+    double diffuse_limit, clamp;
+} or_render_desc;
+
+void or_render(const or_render_desc *r, uint32_t samples, double *mean, double *var, int threads);
+
+#ifdef __cplusplus
+}
+#endif
+#endif
