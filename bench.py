@@ -1,0 +1,372 @@
+#!/usr/bin/env python
+"""Throughput of the wavefront path tracer on one B200: Mrays/s of closest-hit plus
+shadow rays on the incoherent 1,048,576-triangle scene at 1920x1080, depth 6.
+
+A step is one pass of the hot path over one batch: one sample of every pixel of the
+1080p frame (camera -> 7 rounds of closest / shade / shadow -> film). `value` is the
+rays of all ranks over the slowest rank's device time (CUDA events on the renderer's
+stream, inputs resident in HBM); `e2e` is the same metric through the public API
+(Renderer.advance + Renderer.read into pinned host memory every step).
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl reference]
+
+Under torchrun (N > 1) each rank renders its own replica (no data exchange: the path
+shards by scene) and the time is the maximum over ranks.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import time
+from pathlib import Path
+
+ROOT = Path(__file__).resolve().parent
+sys.path.insert(0, str(ROOT))
+
+METRIC = "Mrays/s closest+shadow; batched vs per-scene spp/s at equal RMSE; p50/p99 ms"
+WIDTH, HEIGHT, BOUNCES = 1920, 1080, 6
+WORKLOAD = ("incoherent traversal: 1,048,576 triangles (512 icospheres of 1,280 and 512 tori of 768, "
+            "seeded placement in a 100-unit box), 4 rect + 1 distant light, Lambertian albedo U(0.2,0.9), "
+            "1920x1080, one sample per pixel per step (a 16-spp render is 16 steps), depth 6")
+
+
+def parse():
+    p = argparse.ArgumentParser()
+    p.add_argument("--gpus", type=int, default=1)
+    p.add_argument("--steps", type=int, default=100)
+    p.add_argument("--warmup", type=int, default=5)
+    p.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    p.add_argument("--rgb", action="store_true", help="the RGB build instead of the spectral one")
+    return p.parse_args()
+
+
+class Dist:
+    """torch.distributed plumbing for N > 1: barrier and max over ranks."""
+
+    def __init__(self, gpus: int):
+        self.world = int(os.environ.get("WORLD_SIZE", "1"))
+        self.rank = int(os.environ.get("RANK", "0"))
+        self.local = int(os.environ.get("LOCAL_RANK", "0"))
+        self.pg = None
+        if self.world > 1:
+            import datetime
+
+            import torch
+            import torch.distributed as dist
+
+            torch.cuda.set_device(self.local)
+            dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300))
+            self.torch, self.dist = torch, dist
+            self.pg = True
+
+    def barrier(self):
+        if self.pg:
+            self.dist.barrier()
+
+    def max(self, value: float) -> float:
+        if not self.pg:
+            return value
+        t = self.torch.tensor([value], dtype=self.torch.float64, device=f"cuda:{self.local}")
+        self.dist.all_reduce(t, op=self.dist.ReduceOp.MAX)
+        return float(t.item())
+
+    def sum(self, value: float) -> float:
+        if not self.pg:
+            return value
+        t = self.torch.tensor([value], dtype=self.torch.float64, device=f"cuda:{self.local}")
+        self.dist.all_reduce(t, op=self.dist.ReduceOp.SUM)
+        return float(t.item())
+
+    def close(self):
+        if self.pg:
+            self.dist.destroy_process_group()
+
+
+class Clocks:
+    """nvidia-smi samples of SM clocks and throttle reasons during the timed region."""
+
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, device: int):
+        self.device = device
+        self.proc = None
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", f"--query-gpu={self.FIELDS}", "--format=csv,noheader,nounits", "-lms", "200",
+                 "-i", str(device)], stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+        except (FileNotFoundError, OSError):
+            self.proc = None
+
+    def stop(self) -> dict:
+        if not self.proc:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        self.proc.terminate()
+        try:
+            out, _ = self.proc.communicate(timeout=10)
+        except subprocess.TimeoutExpired:
+            self.proc.kill()
+            out, _ = self.proc.communicate()
+        sm, mx, reasons = [], [], set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for line in out.strip().splitlines():
+            parts = [x.strip() for x in line.split(",")]
+            if len(parts) < 9:
+                continue
+            try:
+                sm.append(float(parts[1]))
+                mx.append(float(parts[2]))
+            except ValueError:
+                continue
+            for name, flag in zip(names, parts[5:9]):
+                if flag.lower() == "active":
+                    reasons.add(name)
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": max(mx) if mx else None,
+                "reasons": sorted(reasons), "samples": len(sm)}
+
+
+def measured_peaks() -> dict:
+    path = ROOT / "MEASURED_PEAKS.json"
+    if path.exists():
+        return json.loads(path.read_text())
+    return {}
+
+
+def profile_traffic():
+    """DRAM bytes per closest-hit ray of the closest-hit kernel, from the committed ncu
+    summary (profiles/closest_kernel.md), or None."""
+    path = ROOT / "profiles" / "closest_kernel.md"
+    if not path.exists():
+        return None
+    for line in path.read_text().splitlines():
+        if line.startswith("dram_bytes_per_ray:"):
+            try:
+                return float(line.split(":", 1)[1].split()[0])
+            except ValueError:
+                return None
+    return None
+
+
+def build_scene(lr, scenes):
+    meshes, mats, lights, cam = scenes.incoherent_scene()
+    return lr.compile_scene(meshes, [cam], lights, mats), lights, mats
+
+
+def settings_for(lr, samples: int, spectral: bool, profile: int = 0):
+    s = lr.RenderSettings.of(WIDTH, HEIGHT, samples)
+    s.max_bounces = BOUNCES
+    s.spectral = 1 if spectral else 0
+    s.light_tracing = 0.0
+    s.profile = profile
+    s.c.material = lr.OpenPbr.lambert()
+    return s
+
+
+class CpuReference:
+    """The oracle's f64 path tracer (the reference's estimator and BVH2 traversal restated
+    on the host) over strips of pixels of the same frame, on all host cores."""
+
+    def __init__(self, sc, lights, mats, spectral: bool, oracle):
+        import luce_render_b200 as lr
+
+        frame = lr.ray_frame(sc.camera(), WIDTH, HEIGHT)
+        self.job = oracle.RenderJob(sc.arrays(), lights, [lr.OpenPbr.lambert()] + list(mats), frame, BOUNCES,
+                                    spectral)
+        self.cores = os.cpu_count() or 1
+        self.pixels = 2048
+        self.step = 0
+
+    def calibrate(self, seconds_per_step: float) -> None:
+        """Sizes a step to about `seconds_per_step` of wall time."""
+        _, secs, _ = self.run(1)
+        self.pixels = int(min(WIDTH * HEIGHT // 4, max(256, self.pixels * seconds_per_step / max(secs, 1e-3))))
+
+    def run(self, steps: int):
+        """(seconds, rays) of `steps` strips, one sample per pixel."""
+        total_rays, seconds = 0, 0.0
+        for _ in range(steps):
+            first = (self.step * 7919 * 64) % (WIDTH * HEIGHT - self.pixels)
+            self.step += 1
+            t0 = time.perf_counter()
+            _, _, rays = self.job.region(1, 0, first, self.pixels, self.cores)
+            seconds += time.perf_counter() - t0
+            total_rays += rays[0] + rays[1]
+        return total_rays / seconds / 1e6, seconds, total_rays
+
+
+def main():
+    args = parse()
+    spectral = not args.rgb
+    dist = Dist(args.gpus)
+    if args.impl == "reference":
+        return reference_arm(args, dist, spectral)
+
+    import numpy as np
+
+    import luce_render_b200 as lr
+    from luce_render_b200 import scenes
+
+    ctx = lr.Context(dist.local)
+    sc, lights, mats = build_scene(lr, scenes)
+    info = sc.info
+    W, K = max(3, args.warmup), args.steps
+
+    # Work per ray, counted by the traversal kernels on one pass of the same workload.
+    counter = lr.Renderer.create(ctx, sc, settings_for(lr, 1, spectral, profile=2))
+    counter.finish()
+    cs = counter.stats()
+    counter.destroy()
+    closest_nodes = cs.closest_nodes / max(1, cs.closest_rays)
+    closest_tests = cs.closest_tests / max(1, cs.closest_rays)
+    shadow_nodes = cs.shadow_nodes / max(1, cs.shadow_rays)
+    shadow_tests = cs.shadow_tests / max(1, cs.shadow_rays)
+
+    # Device-timed region: per-kernel CUDA events on the renderer's stream.
+    r = lr.Renderer.create(ctx, sc, settings_for(lr, W + K, spectral, profile=1))
+    for _ in range(W):
+        r.advance_one()
+    r.wait()
+    s0, t0 = r.stats(), r.kernel_times()
+    dist.barrier()
+    clocks = Clocks(dist.local)
+    ctx.synchronize()
+    ctx.timer_start()
+    for _ in range(K):
+        r.advance_one()
+    ms = ctx.timer_stop()
+    clock_info = clocks.stop()
+    r.finish()
+    s1, t1 = r.stats(), r.kernel_times()
+    r.destroy()
+    closest = s1.closest_rays - s0.closest_rays
+    shadow = s1.shadow_rays - s0.shadow_rays
+    kernel_ms = t1 - t0
+    slowest = dist.max(ms)
+    rays_all = dist.sum(closest + shadow)
+    value = rays_all / (slowest / 1e3) / 1e6
+
+    # Roofline of the dominant kernel (closest hit): algorithmic bytes per ray
+    # 48 + 64 N_int + 48 N_tri (ray in and hit out, both children's boxes per interior
+    # visit, three indices and three vertices per triangle test).
+    peaks = measured_peaks()
+    hbm = peaks.get("hbm_gbs")
+    launches = K * (BOUNCES + 1)
+    closest_bytes = closest * (48.0 + 64.0 * closest_nodes + 48.0 * closest_tests)
+    closest_s = kernel_ms[1] / 1e3
+    achieved = closest_bytes / closest_s / 1e9 if closest_s > 0 else None
+    traffic_per_ray = profile_traffic()
+    roofline = {
+        "kernel": "closest_kernel (intersect closest)",
+        "bound": "hbm",
+        "achieved": achieved,
+        "peak": hbm if hbm else 6650.0,
+        "peak_source": "MEASURED_PEAKS.json hbm_gbs (of measured)" if hbm else "fallback 6.65 TB/s",
+        "unit": "GB/s",
+        "frac": (achieved / (hbm if hbm else 6650.0)) if achieved else None,
+        "traffic": (traffic_per_ray * closest / launches) if traffic_per_ray else None,
+        "algorithmic_bytes_per_launch": closest_bytes / launches,
+        "launch_ms": kernel_ms[1] / launches,
+        "bytes_per_ray": 48.0 + 64.0 * closest_nodes + 48.0 * closest_tests,
+        "interior_visits_per_ray": closest_nodes,
+        "triangle_tests_per_ray": closest_tests,
+        "shadow_interior_visits_per_ray": shadow_nodes,
+        "shadow_triangle_tests_per_ray": shadow_tests,
+        "kernel_share": kernel_ms[1] / max(1e-9, kernel_ms.sum()),
+    }
+
+    # End to end through the public API: each step one pass and the image read back into
+    # pinned host memory (the pass takes no new input: the scene stays resident).
+    e2e_r = lr.Renderer.create(ctx, sc, settings_for(lr, W + K, spectral, profile=0))
+    host = lr.PinnedArray((HEIGHT, WIDTH, 4), np.float32)
+    for _ in range(W):
+        e2e_r.advance_one()
+        e2e_r.read_into(host.array)
+    e0 = e2e_r.stats()
+    dist.barrier()
+    start = time.perf_counter()
+    for _ in range(K):
+        e2e_r.advance_one()
+        e2e_r.read_into(host.array)
+    e2e_s = time.perf_counter() - start
+    e1 = e2e_r.stats()
+    e2e_r.destroy()
+    e2e_rays = dist.sum((e1.closest_rays - e0.closest_rays) + (e1.shadow_rays - e0.shadow_rays))
+    e2e_value = e2e_rays / dist.max(e2e_s) / 1e6
+
+    cpu = None
+    if dist.rank == 0 and dist.world == 1:
+        from oracle import oracle
+
+        ref = CpuReference(sc, lights, mats, spectral, oracle)
+        ref.calibrate(1.0)
+        mrays, secs, rays = ref.run(3)
+        cpu = {"value": mrays, "unit": "Mrays/s", "cores": ref.cores, "kind": "port",
+               "sample": f"3 strips of {ref.pixels} pixels x 1 spp of the same frame ({rays} closest+shadow rays, "
+                         f"{secs:.1f} s wall on {ref.cores} threads): the f64 restatement of the reference's "
+                         f"estimator and BVH2 traversal"}
+
+    if dist.rank == 0:
+        line = {
+            "metric": METRIC, "value": value, "unit": "Mrays/s", "n_gpus": dist.world, "steps": K, "warmup": W,
+            "ms_per_step": slowest / K, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+            "dtype": "f32", "data": "synthetic (seeded generator of the workload's shapes)",
+            "config": {"workload": WORKLOAD, "triangles": int(info.triangle_count), "width": WIDTH, "height": HEIGHT,
+                       "max_bounces": BOUNCES, "spectral": spectral, "samples_per_step": 1,
+                       "l2": "inputs larger than L2: each pass streams ~0.9 GB of path state, ray queues and film",
+                       "parallelism": f"replicas x{dist.world}"},
+            "closest_mrays_s": dist.sum(closest) / (slowest / 1e3) / 1e6,
+            "shadow_mrays_s": dist.sum(shadow) / (slowest / 1e3) / 1e6,
+            "spp_per_s": K / (slowest / 1e3),
+            "kernel_ms_per_step": {n: kernel_ms[i] / K for i, n in enumerate(lr.KERNEL_NAMES) if kernel_ms[i] > 0},
+            "roofline": roofline,
+            "cpu_baseline": cpu,
+            "e2e": {"value": e2e_value, "unit": "Mrays/s", "h2d_bytes_per_step": 0,
+                    "d2h_bytes_per_step": WIDTH * HEIGHT * 16},
+            "gpu_launches": K * (2 + 3 * (BOUNCES + 1) + 2),
+            "clocks": clock_info,
+        }
+        print(json.dumps(line))
+    ctx.close()
+    dist.close()
+
+
+def reference_arm(args, dist, spectral: bool):
+    """The reference's path on the host cores: its CPU restatement (the oracle port; the
+    reference itself runs only on Vulkan/Metal, unavailable here), timed on the same
+    workload, a bounded strip of pixels per step."""
+    if dist.rank != 0:
+        dist.close()
+        return
+    import luce_render_b200 as lr
+    from luce_render_b200 import scenes
+    from oracle import oracle
+
+    sc, lights, mats = build_scene(lr, scenes)
+    W, K = max(3, args.warmup), args.steps
+    ref = CpuReference(sc, lights, mats, spectral, oracle)
+    # A step is a strip sized to ~0.4 s, so the whole run stays within a few minutes.
+    ref.calibrate(min(0.4, 120.0 / max(1, K + W)))
+    ref.run(W)
+    mrays, secs, rays = ref.run(K)
+    cores, pixels = ref.cores, ref.pixels
+    line = {
+        "impl": "reference", "metric": METRIC, "value": mrays, "unit": "Mrays/s", "n_gpus": dist.world, "steps": K,
+        "warmup": W, "ms_per_step": secs * 1e3 / K, "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "f64", "data": "synthetic (seeded generator of the workload's shapes)",
+        "config": {"workload": WORKLOAD, "width": WIDTH, "height": HEIGHT, "max_bounces": BOUNCES,
+                   "spectral": spectral, "pixels_per_step": pixels},
+        "cpu_baseline": {"value": mrays, "unit": "Mrays/s", "cores": cores, "kind": "port",
+                         "sample": f"{K} strips of {pixels} pixels x 1 spp ({rays} rays, {secs:.1f} s)"},
+        "e2e": {"value": mrays, "unit": "Mrays/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line))
+    dist.close()
+
+
+if __name__ == "__main__":
+    main()

@@ -194,9 +194,12 @@ void lr_gpu_scene_destroy(lr_gpu_scene *scene);
 /* Query flags. LR_TRACE_ANY: any-hit (trace_any, bvh.glsl:93-122) instead of the
  * closest hit. LR_TRACE_REFERENCE: the reference's own traversal and Moller-Trumbore
  * test (bvh.glsl:17-90, box order and tie rule included) instead of the default
- * watertight test with ties going to the smaller triangle id. */
+ * watertight test with ties going to the smaller triangle id. LR_TRACE_COUNT: also add
+ * the traversal's work (interior nodes visited, triangle tests) to the context's
+ * counters, read by lr_trace_counts. */
 #define LR_TRACE_ANY 1u
 #define LR_TRACE_REFERENCE 2u
+#define LR_TRACE_COUNT 4u
 
 /* render.probe (device.lucb:138-160): the pixel-centre ray of every pixel of
  * `frame` (probe.comp:21-34), row by row from the top; per pixel the polygon hit
@@ -215,6 +218,10 @@ int lr_trace_rays(lr_context *ctx, const lr_gpu_scene *scene, const float *rays,
                   float *hits, uint32_t flags);
 int lr_trace_rays_device(lr_context *ctx, const lr_gpu_scene *scene, const void *rays,
                          uint64_t count, void *hits, uint32_t flags);
+/* The interior visits and triangle tests of LR_TRACE_COUNT queries since the last
+ * call (the work shaders/bvh.glsl's trace_closest / trace_any do: 64 bytes of child
+ * boxes per visit, 48 bytes of triangle per test); resets them. */
+int lr_trace_counts(lr_context *ctx, uint64_t out[2]);
 
 /* ---- The renderer (src/render/integrator.lucb) -------------------------------------- */
 
@@ -253,6 +260,10 @@ int lr_renderer_advance(lr_renderer *renderer, int32_t *more);
 int lr_renderer_finish(lr_renderer *renderer);
 /* Renderer.samples_done (integrator.lucb:732-733). */
 uint32_t lr_renderer_samples_done(const lr_renderer *renderer);
+/* The pass bookkeeping behind advance (integrator.lucb:297-313, 622-645): passes
+ * recorded so far, passes finished and retired, and bands a sample (passes per sample).
+ * Any output may be NULL. */
+int lr_renderer_passes(const lr_renderer *renderer, uint64_t *recorded, uint64_t *finished, uint32_t *bands);
 /* Renderer.image (integrator.lucb:737-738): the rgba32f ACEScg image in device
  * memory, width*height*16 bytes, row by row from the top. */
 int lr_renderer_image(lr_renderer *renderer, void **device_rgba);
@@ -268,9 +279,12 @@ int lr_renderer_set_samples(lr_renderer *renderer, uint32_t samples);
 int lr_renderer_kernel_times(lr_renderer *renderer, double out[10]);
 
 /* Counters of the work finished passes did: rays traced for closest hits and for
- * shadows, path vertices shaded, and passes. Waits for work in flight. */
+ * shadows, paths started, and passes; with settings.profile = 2 also the traversal's
+ * interior visits and triangle tests for closest and shadow rays. Waits for work in
+ * flight. */
 typedef struct {
     uint64_t closest_rays, shadow_rays, shaded, passes;
+    uint64_t closest_nodes, closest_tests, shadow_nodes, shadow_tests;
 } lr_render_stats;
 int lr_renderer_stats(lr_renderer *renderer, lr_render_stats *out);
 /* Renderer.destroy (integrator.lucb:887-900). */

@@ -34,7 +34,7 @@ _HERE = Path(__file__).resolve().parent
 LIBRARY_PATH = _HERE / "libluce_render_b200.so"
 
 INVALID, LIMIT, STOPPED, DEVICE, TIMEOUT = 400, 401, 402, 500, 504
-TRACE_ANY, TRACE_REFERENCE = 1, 2
+TRACE_ANY, TRACE_REFERENCE, TRACE_COUNT = 1, 2, 4
 LIGHT_RECT, LIGHT_DISK, LIGHT_SPHERE, LIGHT_DISTANT = 0, 1, 2, 3
 
 
@@ -160,7 +160,8 @@ class Settings(C.Structure):
 
 class RenderStats(C.Structure):
     _fields_ = [("closest_rays", C.c_uint64), ("shadow_rays", C.c_uint64), ("shaded", C.c_uint64),
-                ("passes", C.c_uint64)]
+                ("passes", C.c_uint64), ("closest_nodes", C.c_uint64), ("closest_tests", C.c_uint64),
+                ("shadow_nodes", C.c_uint64), ("shadow_tests", C.c_uint64)]
 
 
 # ---- signatures ---------------------------------------------------------------------------
@@ -198,12 +199,14 @@ _SIGNATURES = {
     "lr_probe": (C.c_int, [_vp, _vp, C.POINTER(Frame), _u32, C.POINTER(C.c_uint32), C.POINTER(C.c_float)]),
     "lr_trace_rays": (C.c_int, [_vp, _vp, C.POINTER(C.c_float), _u64, C.POINTER(C.c_float), _u32]),
     "lr_trace_rays_device": (C.c_int, [_vp, _vp, _vp, _u64, _vp, _u32]),
+    "lr_trace_counts": (C.c_int, [_vp, C.POINTER(C.c_uint64)]),
     "lr_settings_default": (None, [C.POINTER(Settings), _u32, _u32, _u32]),
     "lr_renderer_create": (C.c_int, [_vp, _vp, C.POINTER(Settings), C.POINTER(_vp)]),
     "lr_renderer_create_viewed": (C.c_int, [_vp, _vp, C.POINTER(Settings), C.POINTER(Frame), C.POINTER(_vp)]),
     "lr_renderer_advance": (C.c_int, [_vp, C.POINTER(_i32)]),
     "lr_renderer_finish": (C.c_int, [_vp]),
     "lr_renderer_samples_done": (_u32, [_vp]),
+    "lr_renderer_passes": (C.c_int, [_vp, C.POINTER(C.c_uint64), C.POINTER(C.c_uint64), C.POINTER(C.c_uint32)]),
     "lr_renderer_image": (C.c_int, [_vp, C.POINTER(_vp)]),
     "lr_renderer_read": (C.c_int, [_vp, C.POINTER(C.c_float), _u64]),
     "lr_renderer_set_samples": (C.c_int, [_vp, _u32]),
@@ -537,14 +540,21 @@ def probe(ctx: Context, scene: GpuScene, frame: Frame, reference: bool = False):
 
 
 def trace_rays(ctx: Context, scene: GpuScene, rays: np.ndarray, any_hit: bool = False,
-               reference: bool = False) -> np.ndarray:
+               reference: bool = False, count: bool = False) -> np.ndarray:
     """Closest (or any) hits of rays (n x 8 floats: origin, tmin, direction, tmax):
     n x 4 words (t, triangle id as int32, u, v)."""
     rays = np.ascontiguousarray(rays, np.float32).reshape(-1, 8)
     hits = np.empty((len(rays), 4), np.float32)
-    flags = (TRACE_ANY if any_hit else 0) | (TRACE_REFERENCE if reference else 0)
+    flags = (TRACE_ANY if any_hit else 0) | (TRACE_REFERENCE if reference else 0) | (TRACE_COUNT if count else 0)
     _check(lib.lr_trace_rays(ctx.handle, scene.handle, _fptr(rays), len(rays), _fptr(hits), flags))
     return hits
+
+
+def trace_counts(ctx: Context):
+    """Interior visits and triangle tests of counted queries since the last call."""
+    out = (C.c_uint64 * 2)()
+    _check(lib.lr_trace_counts(ctx.handle, out))
+    return int(out[0]), int(out[1])
 
 
 def hit_ids(hits: np.ndarray) -> np.ndarray:
@@ -608,6 +618,33 @@ class Renderer:
 
     def samples_done(self) -> int:
         return int(lib.lr_renderer_samples_done(self.handle))
+
+    def passes(self):
+        """(passes recorded, passes finished, bands a sample)."""
+        rec, fin, bands = C.c_uint64(), C.c_uint64(), C.c_uint32()
+        _check(lib.lr_renderer_passes(self.handle, C.byref(rec), C.byref(fin), C.byref(bands)))
+        return int(rec.value), int(fin.value), int(bands.value)
+
+    def advance_one(self) -> bool:
+        """Advance until one more pass has been queued (False when none is left)."""
+        recorded = self.passes()[0]
+        while True:
+            more = self.advance()
+            if self.passes()[0] > recorded:
+                return True
+            if not more:
+                return False
+
+    def wait(self) -> None:
+        """Wait for the passes queued so far."""
+        self.ctx.synchronize()
+
+    def read_into(self, out: np.ndarray) -> np.ndarray:
+        """Renderer.read into a caller's float32 array of height x width x 4."""
+        if out.dtype != np.float32 or out.size != self.width * self.height * 4 or not out.flags.c_contiguous:
+            raise RenderError(INVALID, "reading the image needs four floats a pixel")
+        _check(lib.lr_renderer_read(self.handle, _fptr(out), out.size))
+        return out
 
     def image(self) -> int:
         """The device address of the rgba32f image."""

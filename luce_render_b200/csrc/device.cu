@@ -49,27 +49,33 @@ __global__ void __launch_bounds__(kBlock) probe_kernel(DeviceScene s, ProbeFrame
     }
     Ray r{make_float3(o[0], o[1], o[2]), 0.0f, make_float3(d[0], d[1], d[2]), kNoHitT};
     bool overflow = false;
-    Hit h = kRef ? trace_reference<false, kStack>(s, r, stack + threadIdx.x, kBlock, overflow)
-                 : trace_exact<false, kStack>(s, r, stack + threadIdx.x, kBlock, overflow);
+    Visits visits;
+    Hit h = kRef ? trace_reference<false, kStack>(s, r, stack + threadIdx.x, kBlock, overflow, visits)
+                 : trace_exact<false, kStack>(s, r, stack + threadIdx.x, kBlock, overflow, visits);
     note_overflow(status, overflow);
     faces[pixel] = h.slot >= 0 ? __ldg(&s.faces[h.slot]) : 0xffffffffu;
     ts[pixel] = h.t;
 }
 
-// A list of rays (two float4 each) to hits (t, source id bits, u, v).
-template <bool kRef, bool kAny, int kStack>
+// A list of rays (two float4 each) to hits (t, source id bits, u, v). With kCount the
+// traversal's interior visits and triangle tests add into counts[0..1].
+template <bool kRef, bool kAny, int kStack, bool kCount>
 __global__ void __launch_bounds__(kBlock) trace_kernel(DeviceScene s, const float4 *__restrict__ rays, uint64_t n,
-                                                      float4 *__restrict__ hits, int *status) {
+                                                      float4 *__restrict__ hits, int *status,
+                                                      unsigned long long *counts) {
     __shared__ int stack[kStack * kBlock];
     const uint64_t i = (uint64_t)blockIdx.x * kBlock + threadIdx.x;
-    if (i >= n) return;
-    const float4 a = __ldg(&rays[2 * i]), b = __ldg(&rays[2 * i + 1]);
-    Ray r{make_float3(a.x, a.y, a.z), a.w, make_float3(b.x, b.y, b.z), b.w};
-    bool overflow = false;
-    Hit h = kRef ? trace_reference<kAny, kStack>(s, r, stack + threadIdx.x, kBlock, overflow)
-                 : trace_exact<kAny, kStack>(s, r, stack + threadIdx.x, kBlock, overflow);
-    note_overflow(status, overflow);
-    hits[i] = make_float4(h.t, __int_as_float(h.id), h.u, h.v);
+    Visits visits;
+    if (i < n) {
+        const float4 a = __ldg(&rays[2 * i]), b = __ldg(&rays[2 * i + 1]);
+        Ray r{make_float3(a.x, a.y, a.z), a.w, make_float3(b.x, b.y, b.z), b.w};
+        bool overflow = false;
+        Hit h = kRef ? trace_reference<kAny, kStack, kCount>(s, r, stack + threadIdx.x, kBlock, overflow, visits)
+                     : trace_exact<kAny, kStack, kCount>(s, r, stack + threadIdx.x, kBlock, overflow, visits);
+        note_overflow(status, overflow);
+        hits[i] = make_float4(h.t, __int_as_float(h.id), h.u, h.v);
+    }
+    if (kCount) add_visits(counts, visits);
 }
 
 int stack_for(uint32_t depth) {
@@ -86,20 +92,20 @@ void launch_probe(const lr_gpu_scene *gs, const ProbeFrame &f, uint64_t count, u
     probe_kernel<kRef, kStack><<<grid, kBlock, 0, stream>>>(gs->scene, f, faces, ts, status);
 }
 
-template <bool kRef, bool kAny, int kStack>
+template <bool kRef, bool kAny, int kStack, bool kCount>
 void launch_trace(const lr_gpu_scene *gs, const float4 *rays, uint64_t n, float4 *hits, int *status,
-                  cudaStream_t stream) {
+                  unsigned long long *counts, cudaStream_t stream) {
     const unsigned grid = (unsigned)((n + kBlock - 1) / kBlock);
-    trace_kernel<kRef, kAny, kStack><<<grid, kBlock, 0, stream>>>(gs->scene, rays, n, hits, status);
+    trace_kernel<kRef, kAny, kStack, kCount><<<grid, kBlock, 0, stream>>>(gs->scene, rays, n, hits, status, counts);
 }
 
-template <bool kRef, bool kAny>
+template <bool kRef, bool kAny, bool kCount>
 void dispatch_trace(const lr_gpu_scene *gs, const float4 *rays, uint64_t n, float4 *hits, int *status,
-                    cudaStream_t stream) {
+                    unsigned long long *counts, cudaStream_t stream) {
     switch (stack_for(gs->scene.depth)) {
-        case 32: launch_trace<kRef, kAny, 32>(gs, rays, n, hits, status, stream); break;
-        case 64: launch_trace<kRef, kAny, 64>(gs, rays, n, hits, status, stream); break;
-        default: launch_trace<kRef, kAny, 96>(gs, rays, n, hits, status, stream); break;
+        case 32: launch_trace<kRef, kAny, 32, kCount>(gs, rays, n, hits, status, counts, stream); break;
+        case 64: launch_trace<kRef, kAny, 64, kCount>(gs, rays, n, hits, status, counts, stream); break;
+        default: launch_trace<kRef, kAny, 96, kCount>(gs, rays, n, hits, status, counts, stream); break;
     }
 }
 
@@ -233,8 +239,10 @@ int lr_context_create(int device, lr_context **out) {
         LR_CUDA(cudaStreamCreateWithFlags(&ctx->stream, cudaStreamNonBlocking));
         LR_CUDA(cudaEventCreate(&ctx->start));
         LR_CUDA(cudaEventCreate(&ctx->stop));
-        LR_CUDA(cudaMalloc(&ctx->status, 2 * sizeof(int)));
-        LR_CUDA(cudaMemsetAsync(ctx->status, 0, 2 * sizeof(int), ctx->stream));
+        // Status words at byte 0, traversal counts at byte 16.
+        LR_CUDA(cudaMalloc(&ctx->status, 64));
+        LR_CUDA(cudaMemsetAsync(ctx->status, 0, 64, ctx->stream));
+        ctx->counts = (unsigned long long *)((char *)ctx->status + 16);
         LR_CUDA(cudaStreamSynchronize(ctx->stream));
         *out = ctx.release();
     });
@@ -442,12 +450,32 @@ static void trace_device(lr_context *ctx, const lr_gpu_scene *gs, const void *ra
     if (n == 0) return;
     const float4 *r = (const float4 *)rays;
     float4 *h = (float4 *)hits;
-    const bool any = flags & LR_TRACE_ANY, ref = flags & LR_TRACE_REFERENCE;
-    if (ref && any) dispatch_trace<true, true>(gs, r, n, h, ctx->status, ctx->stream);
-    else if (ref) dispatch_trace<true, false>(gs, r, n, h, ctx->status, ctx->stream);
-    else if (any) dispatch_trace<false, true>(gs, r, n, h, ctx->status, ctx->stream);
-    else dispatch_trace<false, false>(gs, r, n, h, ctx->status, ctx->stream);
+    const bool any = flags & LR_TRACE_ANY, ref = flags & LR_TRACE_REFERENCE, count = flags & LR_TRACE_COUNT;
+    unsigned long long *c = ctx->counts;
+    if (count) {
+        if (ref && any) dispatch_trace<true, true, true>(gs, r, n, h, ctx->status, c, ctx->stream);
+        else if (ref) dispatch_trace<true, false, true>(gs, r, n, h, ctx->status, c, ctx->stream);
+        else if (any) dispatch_trace<false, true, true>(gs, r, n, h, ctx->status, c, ctx->stream);
+        else dispatch_trace<false, false, true>(gs, r, n, h, ctx->status, c, ctx->stream);
+    } else {
+        if (ref && any) dispatch_trace<true, true, false>(gs, r, n, h, ctx->status, c, ctx->stream);
+        else if (ref) dispatch_trace<true, false, false>(gs, r, n, h, ctx->status, c, ctx->stream);
+        else if (any) dispatch_trace<false, true, false>(gs, r, n, h, ctx->status, c, ctx->stream);
+        else dispatch_trace<false, false, false>(gs, r, n, h, ctx->status, c, ctx->stream);
+    }
     LR_CUDA(cudaGetLastError());
+}
+
+int lr_trace_counts(lr_context *ctx, uint64_t out[2]) {
+    return guarded([&] {
+        if (!ctx || !out) fail(LR_INVALID, "trace counts need two words");
+        unsigned long long words[2] = {0, 0};
+        LR_CUDA(cudaMemcpyAsync(words, ctx->counts, sizeof words, cudaMemcpyDeviceToHost, ctx->stream));
+        LR_CUDA(cudaMemsetAsync(ctx->counts, 0, sizeof words, ctx->stream));
+        LR_CUDA(cudaStreamSynchronize(ctx->stream));
+        out[0] = words[0];
+        out[1] = words[1];
+    });
 }
 
 int lr_trace_rays(lr_context *ctx, const lr_gpu_scene *gs, const float *rays, uint64_t count, float *hits,

@@ -54,6 +54,8 @@ struct lr_context {
     int sm_count = 148;
     // Device status words: [0] traversal stack pushes lost, [1] bounded waits that gave up.
     int *status = nullptr;
+    // Traversal work of counted ray queries: interior visits, triangle tests.
+    unsigned long long *counts = nullptr;
 };
 
 namespace lr {

@@ -127,17 +127,18 @@ __global__ void __launch_bounds__(kShadeBlock) camera_kernel(View v) {
 
 // intersect_closest.comp:45-76: the nearest triangle, then the analytic lights
 // before it (camera rays skip lights invisible to the camera).
-template <int kStack>
+template <int kStack, bool kCount>
 __global__ void __launch_bounds__(kTraceBlock) closest_kernel(View v, uint32_t round) {
     __shared__ int stack[kStack * kTraceBlock];
     const uint32_t q = round & 1u;
     const uint32_t count = v.counters[round];
     const uint32_t stride = gridDim.x * blockDim.x;
     bool overflow = false;
+    Visits visits;
     for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < count; i += stride) {
         const float4 o = v.ray_o[q][i], d = v.ray_d[q][i];
         const Ray r{xyz(o), 0.0f, xyz(d), d.w};
-        const Hit h = trace_exact<false, kStack>(v.scene, r, stack + threadIdx.x, kTraceBlock, overflow);
+        const Hit h = trace_exact<false, kStack, kCount>(v.scene, r, stack + threadIdx.x, kTraceBlock, overflow, visits);
         uint32_t what = h.slot >= 0 ? (uint32_t)h.slot : kNone;
         float t = h.t;
         for (uint32_t light = 0; light < v.light_count; light++) {
@@ -151,25 +152,28 @@ __global__ void __launch_bounds__(kTraceBlock) closest_kernel(View v, uint32_t r
         v.hits[q][i] = make_float4(t, __uint_as_float(what), h.u, h.v);
     }
     if (overflow) atomicAdd(&v.status[0], 1);
+    if (kCount) add_visits(&v.stats[4], visits);
 }
 
 // intersect_shadow.comp:51-92: unblocked light samples join their path's radiance.
-template <int kStack>
+template <int kStack, bool kCount>
 __global__ void __launch_bounds__(kTraceBlock) shadow_kernel(View v, uint32_t round) {
     __shared__ int stack[kStack * kTraceBlock];
     const uint32_t count = v.counters[v.rounds + 1 + round];
     const uint32_t stride = gridDim.x * blockDim.x;
     bool overflow = false;
+    Visits visits;
     for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < count; i += stride) {
         const float4 o = v.shadow_o[i], d = v.shadow_d[i];
         const Ray r{xyz(o), 0.0f, xyz(d), d.w};
-        const Hit h = trace_exact<true, kStack>(v.scene, r, stack + threadIdx.x, kTraceBlock, overflow);
+        const Hit h = trace_exact<true, kStack, kCount>(v.scene, r, stack + threadIdx.x, kTraceBlock, overflow, visits);
         if (h.id < 0) {
             const uint32_t path = __float_as_uint(o.w);
             v.radiance[path] = v.radiance[path] + v.shadow_c[i];
         }
     }
     if (overflow) atomicAdd(&v.status[0], 1);
+    if (kCount) add_visits(&v.stats[6], visits);
 }
 
 template <bool kSpectral>
@@ -529,7 +533,9 @@ struct lr_renderer {
 namespace lr {
 namespace {
 
-template <bool kSpectral, int kStack>
+// Records one pass on `stream`. With `marks`, an event follows each kernel (profiling);
+// kCount instantiates the traversal kernels that count their work.
+template <bool kSpectral, int kStack, bool kCount>
 void record_pass(lr_renderer *r, cudaStream_t stream, std::vector<std::pair<cudaEvent_t, int>> *marks) {
     View &v = r->view;
     auto mark = [&](int kind) {
@@ -544,11 +550,11 @@ void record_pass(lr_renderer *r, cudaStream_t stream, std::vector<std::pair<cuda
     camera_kernel<kSpectral><<<r->grid_shade, kShadeBlock, 0, stream>>>(v);
     mark(kCamera);
     for (uint32_t round = 0; round < v.rounds; round++) {
-        closest_kernel<kStack><<<r->grid_trace, kTraceBlock, 0, stream>>>(v, round);
+        closest_kernel<kStack, kCount><<<r->grid_trace, kTraceBlock, 0, stream>>>(v, round);
         mark(kClosest);
         shade_kernel<kSpectral><<<r->grid_shade, kShadeBlock, 0, stream>>>(v, round);
         mark(kSurface);
-        shadow_kernel<kStack><<<r->grid_trace, kTraceBlock, 0, stream>>>(v, round);
+        shadow_kernel<kStack, kCount><<<r->grid_trace, kTraceBlock, 0, stream>>>(v, round);
         mark(kShadow);
     }
     finish_kernel<kSpectral><<<r->grid_shade, kShadeBlock, 0, stream>>>(v);
@@ -558,24 +564,30 @@ void record_pass(lr_renderer *r, cudaStream_t stream, std::vector<std::pair<cuda
     LR_CUDA(cudaGetLastError());
 }
 
-template <bool kSpectral>
+template <bool kSpectral, bool kCount>
 void record_any(lr_renderer *r, cudaStream_t stream, std::vector<std::pair<cudaEvent_t, int>> *marks) {
     switch (r->stack) {
-        case 32: record_pass<kSpectral, 32>(r, stream, marks); break;
-        case 64: record_pass<kSpectral, 64>(r, stream, marks); break;
-        default: record_pass<kSpectral, 96>(r, stream, marks); break;
+        case 32: record_pass<kSpectral, 32, kCount>(r, stream, marks); break;
+        case 64: record_pass<kSpectral, 64, kCount>(r, stream, marks); break;
+        default: record_pass<kSpectral, 96, kCount>(r, stream, marks); break;
     }
 }
 
 void record(lr_renderer *r, cudaStream_t stream, std::vector<std::pair<cudaEvent_t, int>> *marks) {
-    if (r->settings.spectral) record_any<true>(r, stream, marks);
-    else record_any<false>(r, stream, marks);
+    const bool count = r->settings.profile == 2;
+    if (r->settings.spectral) {
+        if (count) record_any<true, true>(r, stream, marks);
+        else record_any<true, false>(r, stream, marks);
+    } else {
+        if (count) record_any<false, true>(r, stream, marks);
+        else record_any<false, false>(r, stream, marks);
+    }
 }
 
 template <bool kSpectral, int kStack>
 void size_grids(lr_renderer *r) {
     const int sms = r->ctx->sm_count;
-    r->grid_trace = grid_of(closest_kernel<kStack>, kTraceBlock, sms);
+    r->grid_trace = grid_of(closest_kernel<kStack, false>, kTraceBlock, sms);
     r->grid_shade = grid_of(shade_kernel<kSpectral>, kShadeBlock, sms);
 }
 
@@ -709,7 +721,7 @@ void create(lr_context *ctx, const lr_scene *scene, const lr_settings &settings,
     const size_t p_pass_counter = add(nullptr, 8);
     const size_t p_film = add(nullptr, pixels * 16);
     const size_t p_image = add(nullptr, pixels * 16);
-    const size_t p_stats = add(nullptr, 4 * 8);
+    const size_t p_stats = add(nullptr, 8 * 8);
     size_t total = 0;
     for (auto &p : parts) {
         p.offset = total;
@@ -856,7 +868,9 @@ int lr_renderer_advance(lr_renderer *r, int32_t *more) {
         if (!r || !more) fail(LR_INVALID, "no renderer");
         while (retire_one(r, false)) {
         }
-        const size_t depth = r->settings.profile ? 1 : 2;
+        // Two passes in flight (integrator.lucb:651-655); profiling keeps its events per
+        // pass, so it may too.
+        const size_t depth = 2;
         if (r->in_flight.size() >= depth) {
             *more = 1;
             return;
@@ -886,6 +900,15 @@ int lr_renderer_finish(lr_renderer *r) {
 }
 
 uint32_t lr_renderer_samples_done(const lr_renderer *r) { return r ? (uint32_t)(r->retired / r->bands) : 0u; }
+
+int lr_renderer_passes(const lr_renderer *r, uint64_t *recorded, uint64_t *finished, uint32_t *bands) {
+    return guarded([&] {
+        if (!r) fail(LR_INVALID, "no renderer");
+        if (recorded) *recorded = r->recorded;
+        if (finished) *finished = r->retired;
+        if (bands) *bands = r->bands;
+    });
+}
 
 int lr_renderer_image(lr_renderer *r, void **device_rgba) {
     return guarded([&] {
@@ -922,13 +945,17 @@ int lr_renderer_stats(lr_renderer *r, lr_render_stats *out) {
     return guarded([&] {
         if (!r || !out) fail(LR_INVALID, "no renderer");
         settle(r);
-        unsigned long long s[4];
+        unsigned long long s[8];
         LR_CUDA(cudaMemcpyAsync(s, r->view.stats, sizeof s, cudaMemcpyDeviceToHost, r->ctx->stream));
         LR_CUDA(cudaStreamSynchronize(r->ctx->stream));
         out->closest_rays = s[0];
         out->shadow_rays = s[1];
         out->shaded = s[2];
         out->passes = s[3];
+        out->closest_nodes = s[4];
+        out->closest_tests = s[5];
+        out->shadow_nodes = s[6];
+        out->shadow_tests = s[7];
     });
 }
 

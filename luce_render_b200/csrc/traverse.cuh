@@ -209,10 +209,16 @@ struct SharedStack {
     __device__ __forceinline__ bool empty() const { return sp == 0; }
 };
 
+// Work a traversal did: interior nodes visited (both children's boxes read) and
+// triangle tests. Counted only when the traversal is instantiated with kCount.
+struct Visits {
+    uint32_t nodes = 0, tests = 0;
+};
+
 // The closest (or any) hit along r, watertight. `overflow` is set when a push was lost.
-template <bool kAny, int kStack>
+template <bool kAny, int kStack, bool kCount = false>
 __device__ __forceinline__ Hit trace_exact(const DeviceScene &s, const Ray &r, int *stack_base, int stride,
-                                           bool &overflow) {
+                                           bool &overflow, Visits &visits) {
     Hit h{r.tmax, -1, -1, 0.0f, 0.0f};
     const DeviceBvh &b = s.bvh;
     if (b.empty) return h;
@@ -226,6 +232,7 @@ __device__ __forceinline__ Hit trace_exact(const DeviceScene &s, const Ray &r, i
     int node = b.root;
     for (;;) {
         while (node >= 0) {
+            if (kCount) visits.nodes++;
             const float4 *e = b.entries + (size_t)node * 4;
             const float4 n0 = __ldg(e), n1 = __ldg(e + 1), n2 = __ldg(e + 2), n3 = __ldg(e + 3);
             float ea, eb;
@@ -247,6 +254,7 @@ __device__ __forceinline__ Hit trace_exact(const DeviceScene &s, const Ray &r, i
         }
         uint32_t first, count;
         leaf_range(node, first, count);
+        if (kCount) visits.tests += count;
         for (uint32_t i = 0; i < count; i++) {
             const float4 *tri = s.tris + (size_t)(first + i) * 3;
             const float4 a = __ldg(tri), bb = __ldg(tri + 1), c = __ldg(tri + 2);
@@ -269,9 +277,9 @@ __device__ __forceinline__ Hit trace_exact(const DeviceScene &s, const Ray &r, i
 }
 
 // trace_closest / trace_any (bvh.glsl:51-122) over the reference's exact boxes.
-template <bool kAny, int kStack>
+template <bool kAny, int kStack, bool kCount = false>
 __device__ __forceinline__ Hit trace_reference(const DeviceScene &s, const Ray &r, int *stack_base, int stride,
-                                               bool &overflow) {
+                                               bool &overflow, Visits &visits) {
     Hit h{r.tmax, -1, -1, 0.0f, 0.0f};
     const DeviceBvh &b = s.ref_bvh;
     if (b.empty) return h;
@@ -286,12 +294,14 @@ __device__ __forceinline__ Hit trace_reference(const DeviceScene &s, const Ray &
             uint32_t first, count;
             leaf_range(node, first, count);
             for (uint32_t i = 0; i < count; i++) {
+                if (kCount) visits.tests++;
                 if (triangle_reference(s, first + i, r.o, r.d, h) && kAny) {
                     h.id = (int)__ldg(&s.ids[h.slot]);
                     return h;
                 }
             }
         } else {
+            if (kCount) visits.nodes++;
             const float4 *e = b.entries + (size_t)node * 4;
             const float4 n0 = __ldg(e), n1 = __ldg(e + 1), n2 = __ldg(e + 2), n3 = __ldg(e + 3);
             const float tl = kAny ? r.tmax : h.t;
@@ -319,6 +329,21 @@ __device__ __forceinline__ Hit trace_reference(const DeviceScene &s, const Ray &
     }
     if (h.slot >= 0) h.id = (int)__ldg(&s.ids[h.slot]);
     return h;
+}
+
+// Adds each lane's visits into two 64-bit counters with one atomic per warp. Every
+// lane of the warp must call it.
+__device__ __forceinline__ void add_visits(unsigned long long *counters, const Visits &v) {
+    unsigned long long nodes = v.nodes, tests = v.tests;
+#pragma unroll
+    for (int offset = 16; offset > 0; offset >>= 1) {
+        nodes += __shfl_down_sync(0xffffffffu, nodes, offset);
+        tests += __shfl_down_sync(0xffffffffu, tests, offset);
+    }
+    if ((threadIdx.x & 31) == 0 && (nodes || tests)) {
+        atomicAdd(&counters[0], nodes);
+        atomicAdd(&counters[1], tests);
+    }
 }
 
 }  // namespace lr

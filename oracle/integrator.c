@@ -454,7 +454,7 @@ static void spec_to_film(const or_render_desc *r, spec rad, const double lambda[
 }
 
 /* One sample of one pixel: its ACEScg value. */
-static void render_sample(const or_render_desc *r, uint32_t pixel, uint32_t sample, double out[3]) {
+static void render_sample(const or_render_desc *r, uint32_t pixel, uint32_t sample, double out[3], uint64_t rays[2]) {
     const float *f = r->frame;
     double u4[4];
     or_sample4(r->seed, pixel, sample, 0, u4);
@@ -487,6 +487,7 @@ static void render_sample(const or_render_desc *r, uint32_t pixel, uint32_t samp
         uint32_t total = bounces & 0xffu;
         double t, hu = 0, hv = 0;
         uint32_t what = trace64(r, origin, dir, INF, 0, &t, &hu, &hv);
+        rays[0]++;
         for (uint32_t l = 0; l < r->light_count; l++) {
             if (round == 0 && !light_visible(r, l)) continue;
             double tl = intersect_light(r, l, origin, dir, t);
@@ -620,6 +621,7 @@ static void render_sample(const or_render_desc *r, uint32_t pixel, uint32_t samp
                     double margin = 4e-4 * fmax(1.0, fmax(fabs(target.x), fmax(fabs(target.y), fabs(target.z))));
                     double sreach = s.distance >= INF ? INF : fmax(0.0, s.distance - margin);
                     double tt, uu, vv;
+                    rays[1]++;
                     if (trace64(r, offset_origin(p, geometric), s.direction, sreach, 1, &tt, &uu, &vv) == NONE)
                         radiance = spec_add(radiance, c);
                 }
@@ -668,14 +670,17 @@ static void render_sample(const or_render_desc *r, uint32_t pixel, uint32_t samp
 
 typedef struct {
     const or_render_desc *r;
-    uint32_t samples;
+    uint32_t samples, sample_first;
+    size_t first;
     double *mean, *var;
     size_t next, n;
+    uint64_t rays[2];
     pthread_mutex_t lock;
 } render_job;
 
 static void *render_worker(void *arg) {
     render_job *j = arg;
+    uint64_t rays[2] = {0, 0};
     for (;;) {
         pthread_mutex_lock(&j->lock);
         size_t begin = j->next;
@@ -683,11 +688,11 @@ static void *render_worker(void *arg) {
         size_t end = j->next;
         pthread_mutex_unlock(&j->lock);
         if (begin >= end) break;
-        for (size_t pixel = begin; pixel < end; pixel++) {
+        for (size_t at = begin; at < end; at++) {
             double m[3] = {0, 0, 0}, m2[3] = {0, 0, 0};
             for (uint32_t s = 0; s < j->samples; s++) {
                 double v[3];
-                render_sample(j->r, (uint32_t)pixel, s, v);
+                render_sample(j->r, (uint32_t)(j->first + at), j->sample_first + s, v, rays);
                 for (int k = 0; k < 3; k++) {
                     double delta = v[k] - m[k];
                     m[k] += delta / (double)(s + 1);
@@ -695,27 +700,43 @@ static void *render_worker(void *arg) {
                 }
             }
             for (int k = 0; k < 3; k++) {
-                j->mean[pixel * 3 + k] = m[k];
-                j->var[pixel * 3 + k] = j->samples > 1 ? m2[k] / (double)(j->samples - 1) : 0.0;
+                j->mean[at * 3 + k] = m[k];
+                j->var[at * 3 + k] = j->samples > 1 ? m2[k] / (double)(j->samples - 1) : 0.0;
             }
         }
     }
+    pthread_mutex_lock(&j->lock);
+    j->rays[0] += rays[0];
+    j->rays[1] += rays[1];
+    pthread_mutex_unlock(&j->lock);
     return NULL;
 }
 
-void or_render(const or_render_desc *r, uint32_t samples, double *mean, double *var, int threads) {
+void or_render_region(const or_render_desc *r, uint32_t samples, uint32_t sample_first, size_t first, size_t count,
+                      double *mean, double *var, uint64_t rays[2], int threads) {
     if (threads <= 0) threads = (int)sysconf(_SC_NPROCESSORS_ONLN);
     if (threads > 256) threads = 256;
     render_job j;
     j.r = r;
     j.samples = samples;
+    j.sample_first = sample_first;
+    j.first = first;
     j.mean = mean;
     j.var = var;
     j.next = 0;
-    j.n = (size_t)r->width * r->height;
+    j.n = count;
+    j.rays[0] = j.rays[1] = 0;
     pthread_mutex_init(&j.lock, NULL);
     pthread_t ids[256];
     for (int i = 0; i < threads; i++) pthread_create(&ids[i], NULL, render_worker, &j);
     for (int i = 0; i < threads; i++) pthread_join(ids[i], NULL);
     pthread_mutex_destroy(&j.lock);
+    if (rays) {
+        rays[0] = j.rays[0];
+        rays[1] = j.rays[1];
+    }
+}
+
+void or_render(const or_render_desc *r, uint32_t samples, double *mean, double *var, int threads) {
+    or_render_region(r, samples, 0, 0, (size_t)r->width * r->height, mean, var, NULL, threads);
 }

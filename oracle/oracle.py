@@ -360,6 +360,32 @@ def render(arrays: dict, lights, library, frame, samples: int, max_bounces: int,
     (luce_render_b200.Light), the material library (default first, OrMaterial or
     luce_render_b200.OpenPbr) and a luce_render_b200.Frame. Returns (mean, variance),
     each height x width x 3 (ACEScg)."""
+    job = RenderJob(arrays, lights, library, frame, max_bounces, spectral, seed, background, clamp, diffuse_limit)
+    n = frame.width * frame.height
+    mean, var, _ = job.region(samples, 0, 0, n, threads)
+    return mean.reshape(frame.height, frame.width, 3), var.reshape(frame.height, frame.width, 3)
+
+
+class RenderJob:
+    """A prepared f64 render: the loaded records built once, then any pixel range."""
+
+    def __init__(self, arrays: dict, lights, library, frame, max_bounces: int, spectral: bool, seed: int = 1,
+                 background=(0.0, 0.0, 0.0), clamp: float = 0.0, diffuse_limit: float = 1024.0):
+        self.desc, self.keep = _render_desc(arrays, lights, library, frame, max_bounces, spectral, seed, background,
+                                            clamp, diffuse_limit)
+
+    def region(self, samples: int, sample_first: int, first: int, count: int, threads: int = 0):
+        """Pixels [first, first + count), samples [sample_first, + samples): (mean, var,
+        (closest rays, shadow rays))."""
+        mean = np.zeros(count * 3, np.float64)
+        var = np.zeros(count * 3, np.float64)
+        rays = (C.c_uint64 * 2)()
+        lib.or_render_region(C.byref(self.desc), C.c_uint32(samples), C.c_uint32(sample_first), C.c_size_t(first),
+                             C.c_size_t(count), _p(mean, C.c_double), _p(var, C.c_double), rays, threads)
+        return mean.reshape(-1, 3), var.reshape(-1, 3), (int(rays[0]), int(rays[1]))
+
+
+def _render_desc(arrays, lights, library, frame, max_bounces, spectral, seed, background, clamp, diffuse_limit):
     positions = np.ascontiguousarray(arrays["positions"], np.float32).reshape(-1)
     indices = np.ascontiguousarray(arrays["indices"], np.uint32).reshape(-1)
     shading = np.ascontiguousarray(arrays["shading"], np.uint32).reshape(-1)
@@ -411,9 +437,4 @@ def render(arrays: dict, lights, library, frame, samples: int, max_bounces: int,
     r.seed = seed
     r.diffuse_limit = diffuse_limit
     r.clamp = clamp
-    n = frame.width * frame.height
-    mean = np.zeros(n * 3, np.float64)
-    var = np.zeros(n * 3, np.float64)
-    lib.or_render(C.byref(r), C.c_uint32(samples), _p(mean, C.c_double), _p(var, C.c_double), threads)
-    del keep
-    return mean.reshape(frame.height, frame.width, 3), var.reshape(frame.height, frame.width, 3)
+    return r, keep

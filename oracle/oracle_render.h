@@ -39,6 +39,10 @@ typedef struct {
 } or_render_desc;
 
 void or_render(const or_render_desc *r, uint32_t samples, double *mean, double *var, int threads);
+/* The same over pixels [first, first + count) and samples [sample_first, sample_first +
+ * samples); `rays` (may be NULL) counts the closest and shadow rays traced. */
+void or_render_region(const or_render_desc *r, uint32_t samples, uint32_t sample_first, size_t first, size_t count,
+                      double *mean, double *var, uint64_t rays[2], int threads);
 
 #ifdef __cplusplus
 }

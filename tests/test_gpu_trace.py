@@ -198,6 +198,27 @@ def test_million_triangles_reference_traversal(ctx, incoherent):
     _check_reference(ctx, a, gs, scenes.incoherent_rays(1 << 18, seed=7))
 
 
+def test_traversal_work_counts_match_oracle(ctx, incoherent, cornell):
+    # The reference path's interior visits and triangle tests equal the oracle's
+    # restatement of trace_closest / trace_any exactly (the work the roofline's
+    # algorithmic bytes are counted from); the watertight path, over boxes widened by a
+    # few ulps of the scene scale, does at least that work and not much more.
+    for fixture, rays in ((incoherent, scenes.incoherent_rays(1 << 16, seed=5)),
+                          (cornell, scenes.random_rays(1 << 16))):
+        sc, a, gs = fixture
+        lr.trace_counts(ctx)
+        for any_hit in (False, True):
+            lr.trace_rays(ctx, gs, rays, any_hit=any_hit, reference=True, count=True)
+            nodes, tests = lr.trace_counts(ctx)
+            _, counts = orc.trace(a["nodes"], a["positions"], a["indices"], rays, any_hit=any_hit)
+            assert (nodes, tests) == (counts.interior, counts.triangles)
+            lr.trace_rays(ctx, gs, rays, any_hit=any_hit, count=True)
+            enodes, etests = lr.trace_counts(ctx)
+            if not any_hit:
+                assert counts.interior <= enodes <= 1.05 * counts.interior
+                assert counts.triangles <= etests <= 1.05 * counts.triangles
+
+
 def test_million_triangles_properties_at_full_size(ctx, incoherent):
     # 2^21 incoherent rays: any-hit agrees with the existence of a closest hit, and
     # every closest hit re-tested alone (the oracle's watertight test on that one
