@@ -937,6 +937,10 @@ int lr_renderer_set_samples(lr_renderer *r, uint32_t samples) {
 int lr_renderer_kernel_times(lr_renderer *r, double out[10]) {
     return guarded([&] {
         if (!r || !out) fail(LR_INVALID, "kernel times need ten numbers");
+        // Finished passes count: wait for those in flight and retire them.
+        settle(r);
+        while (retire_one(r, false)) {
+        }
         for (int i = 0; i < 10; i++) out[i] = r->kernel_ms[i];
     });
 }
@@ -945,6 +949,8 @@ int lr_renderer_stats(lr_renderer *r, lr_render_stats *out) {
     return guarded([&] {
         if (!r || !out) fail(LR_INVALID, "no renderer");
         settle(r);
+        while (retire_one(r, false)) {
+        }
         unsigned long long s[8];
         LR_CUDA(cudaMemcpyAsync(s, r->view.stats, sizeof s, cudaMemcpyDeviceToHost, r->ctx->stream));
         LR_CUDA(cudaStreamSynchronize(r->ctx->stream));
