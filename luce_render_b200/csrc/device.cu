@@ -78,6 +78,27 @@ __global__ void __launch_bounds__(kBlock) trace_kernel(DeviceScene s, const floa
     if (kCount) add_visits(counts, visits);
 }
 
+// The watertight path over a ray list: a grid sized to the GPU's resident blocks, each
+// warp taking 32 consecutive rays at a time.
+template <bool kAny, int kStack, bool kCount>
+__global__ void __launch_bounds__(kBlock) trace_resident_kernel(DeviceScene s, const float4 *__restrict__ rays,
+                                                               uint32_t n, float4 *__restrict__ hits, int *status,
+                                                               unsigned long long *counts) {
+    __shared__ int stack[kStack * kBlock];
+    bool overflow = false;
+    Visits visits;
+    auto load = [&](uint32_t i) {
+        const float4 a = __ldg(&rays[2 * i]), b = __ldg(&rays[2 * i + 1]);
+        return Ray{make_float3(a.x, a.y, a.z), a.w, make_float3(b.x, b.y, b.z), b.w};
+    };
+    auto store = [&](uint32_t i, const Hit &h, const Ray &) {
+        hits[i] = make_float4(h.t, __int_as_float(h.id), h.u, h.v);
+    };
+    trace_strided<kAny, kStack, kCount>(s, n, stack + threadIdx.x, kBlock, load, store, overflow, visits);
+    note_overflow(status, overflow);
+    if (kCount) add_visits(counts, visits);
+}
+
 int stack_for(uint32_t depth) {
     if (depth + 2 <= 32) return 32;
     if (depth + 2 <= 64) return 64;
@@ -95,8 +116,24 @@ void launch_probe(const lr_gpu_scene *gs, const ProbeFrame &f, uint64_t count, u
 template <bool kRef, bool kAny, int kStack, bool kCount>
 void launch_trace(const lr_gpu_scene *gs, const float4 *rays, uint64_t n, float4 *hits, int *status,
                   unsigned long long *counts, cudaStream_t stream) {
-    const unsigned grid = (unsigned)((n + kBlock - 1) / kBlock);
-    trace_kernel<kRef, kAny, kStack, kCount><<<grid, kBlock, 0, stream>>>(gs->scene, rays, n, hits, status, counts);
+    if (kRef) {
+        const unsigned grid = (unsigned)((n + kBlock - 1) / kBlock);
+        trace_kernel<kRef, kAny, kStack, kCount><<<grid, kBlock, 0, stream>>>(gs->scene, rays, n, hits, status, counts);
+        return;
+    }
+    if (n > 0xffffffffull) fail(LR_LIMIT, "a ray query holds at most 2^32 - 1 rays");
+    static int resident = 0;
+    if (!resident) {
+        int per_sm = 0, device = 0, sms = 0;
+        LR_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, trace_resident_kernel<kAny, kStack, kCount>, kBlock, 0));
+        LR_CUDA(cudaGetDevice(&device));
+        LR_CUDA(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device));
+        resident = std::max(1, per_sm) * sms;
+    }
+    const uint64_t needed = (n + kBlock - 1) / kBlock;
+    const unsigned grid = (unsigned)std::min<uint64_t>(needed, (uint64_t)resident);
+    trace_resident_kernel<kAny, kStack, kCount><<<grid, kBlock, 0, stream>>>(gs->scene, rays, (uint32_t)n, hits, status,
+                                                                            counts);
 }
 
 template <bool kRef, bool kAny, bool kCount>

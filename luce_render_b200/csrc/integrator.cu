@@ -85,7 +85,7 @@ __global__ void begin_kernel(View v) {
         *v.pass = s;
         *v.pass_counter = p + 1;
     }
-    for (uint32_t i = threadIdx.x; i < 2 * v.rounds + 2; i += blockDim.x) v.counters[i] = 0;
+    for (uint32_t i = threadIdx.x; i < 4 * v.rounds + 2; i += blockDim.x) v.counters[i] = 0;
 }
 
 // camera.comp:14-50: a jittered primary ray per pixel of the band.
@@ -132,13 +132,15 @@ __global__ void __launch_bounds__(kTraceBlock) closest_kernel(View v, uint32_t r
     __shared__ int stack[kStack * kTraceBlock];
     const uint32_t q = round & 1u;
     const uint32_t count = v.counters[round];
-    const uint32_t stride = gridDim.x * blockDim.x;
     bool overflow = false;
     Visits visits;
-    for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < count; i += stride) {
-        const float4 o = v.ray_o[q][i], d = v.ray_d[q][i];
-        const Ray r{xyz(o), 0.0f, xyz(d), d.w};
-        const Hit h = trace_exact<false, kStack, kCount>(v.scene, r, stack + threadIdx.x, kTraceBlock, overflow, visits);
+    const float4 *ray_o = v.ray_o[q], *ray_d = v.ray_d[q];
+    float4 *hits = v.hits[q];
+    auto load = [&](uint32_t i) {
+        const float4 o = ray_o[i], d = ray_d[i];
+        return Ray{xyz(o), 0.0f, xyz(d), d.w};
+    };
+    auto store = [&](uint32_t i, const Hit &h, const Ray &r) {
         uint32_t what = h.slot >= 0 ? (uint32_t)h.slot : kNone;
         float t = h.t;
         for (uint32_t light = 0; light < v.light_count; light++) {
@@ -149,8 +151,10 @@ __global__ void __launch_bounds__(kTraceBlock) closest_kernel(View v, uint32_t r
                 what = kLightHit | light;
             }
         }
-        v.hits[q][i] = make_float4(t, __uint_as_float(what), h.u, h.v);
-    }
+        hits[i] = make_float4(t, __uint_as_float(what), h.u, h.v);
+    };
+    trace_strided<false, kStack, kCount>(v.scene, count, stack + threadIdx.x, kTraceBlock, load, store, overflow,
+                                         visits);
     if (overflow) atomicAdd(&v.status[0], 1);
     if (kCount) add_visits(&v.stats[4], visits);
 }
@@ -160,18 +164,20 @@ template <int kStack, bool kCount>
 __global__ void __launch_bounds__(kTraceBlock) shadow_kernel(View v, uint32_t round) {
     __shared__ int stack[kStack * kTraceBlock];
     const uint32_t count = v.counters[v.rounds + 1 + round];
-    const uint32_t stride = gridDim.x * blockDim.x;
     bool overflow = false;
     Visits visits;
-    for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < count; i += stride) {
+    auto load = [&](uint32_t i) {
         const float4 o = v.shadow_o[i], d = v.shadow_d[i];
-        const Ray r{xyz(o), 0.0f, xyz(d), d.w};
-        const Hit h = trace_exact<true, kStack, kCount>(v.scene, r, stack + threadIdx.x, kTraceBlock, overflow, visits);
+        return Ray{xyz(o), 0.0f, xyz(d), d.w};
+    };
+    auto store = [&](uint32_t i, const Hit &h, const Ray &) {
         if (h.id < 0) {
-            const uint32_t path = __float_as_uint(o.w);
+            const uint32_t path = __float_as_uint(v.shadow_o[i].w);
             v.radiance[path] = v.radiance[path] + v.shadow_c[i];
         }
-    }
+    };
+    trace_strided<true, kStack, kCount>(v.scene, count, stack + threadIdx.x, kTraceBlock, load, store, overflow,
+                                        visits);
     if (overflow) atomicAdd(&v.status[0], 1);
     if (kCount) add_visits(&v.stats[6], visits);
 }
@@ -716,7 +722,7 @@ void create(lr_context *ctx, const lr_scene *scene, const lr_settings &settings,
     const size_t p_shadow_o = add(nullptr, pool * 16);
     const size_t p_shadow_d = add(nullptr, pool * 16);
     const size_t p_shadow_c = add(nullptr, pool * 16);
-    const size_t p_counters = add(nullptr, (2 * rounds + 2) * 4);
+    const size_t p_counters = add(nullptr, (4 * rounds + 2) * 4);
     const size_t p_pass = add(nullptr, sizeof(PassState));
     const size_t p_pass_counter = add(nullptr, 8);
     const size_t p_film = add(nullptr, pixels * 16);
@@ -732,7 +738,21 @@ void create(lr_context *ctx, const lr_scene *scene, const lr_settings &settings,
     LR_CUDA(cudaMemsetAsync(base, 0, total, ctx->stream));
     for (auto &p : parts)
         if (p.src && p.bytes) LR_CUDA(cudaMemcpyAsync(base + p.offset, p.src, p.bytes, cudaMemcpyHostToDevice, ctx->stream));
-    LR_CUDA(cudaMemcpyToSymbolAsync(c_sobol, sobol_table(), 128 * sizeof(uint32_t), 0, cudaMemcpyHostToDevice, ctx->stream));
+    static std::vector<uint32_t> sobol_bytes;
+    if (sobol_bytes.empty()) {
+        const uint32_t *dirs = sobol_table();
+        sobol_bytes.assign(3 * 4 * 256, 0u);
+        for (int d = 1; d < 4; d++)
+            for (int b = 0; b < 4; b++)
+                for (int value = 0; value < 256; value++) {
+                    uint32_t x = 0;
+                    for (int bit = 0; bit < 8; bit++)
+                        if (value & (1 << bit)) x ^= dirs[d * 32 + b * 8 + bit];
+                    sobol_bytes[(d - 1) * 1024 + b * 256 + value] = x;
+                }
+    }
+    LR_CUDA(cudaMemcpyToSymbolAsync(g_sobol_bytes, sobol_bytes.data(), sobol_bytes.size() * sizeof(uint32_t), 0,
+                                    cudaMemcpyHostToDevice, ctx->stream));
     LR_CUDA(cudaStreamSynchronize(ctx->stream));
     auto at = [&](size_t i) { return (void *)(base + parts[i].offset); };
 

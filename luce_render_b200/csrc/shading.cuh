@@ -37,7 +37,11 @@ __device__ __forceinline__ float3 xyz(float4 a) { return make_float3(a.x, a.y, a
 
 // ---- sampler.glsl --------------------------------------------------------------------
 
-__constant__ uint32_t c_sobol[128];
+// Sobol dimensions 1..3 by bytes of the index: g_sobol_bytes[(d - 1) * 1024 + b * 256 + v]
+// is the XOR of the direction numbers of the set bits of byte value v at byte position b,
+// so a 32-bit index costs four lookups (XOR is associative: the same value as the
+// bit-by-bit sum of sampler.glsl:32-37). Dimension 0 is van der Corput, a bit reversal.
+__device__ uint32_t g_sobol_bytes[3 * 4 * 256];
 
 __device__ __forceinline__ uint32_t hash_u32(uint32_t x) {
     x ^= x >> 16;
@@ -63,14 +67,10 @@ __device__ __forceinline__ uint32_t nested_uniform_scramble(uint32_t x, uint32_t
 }
 
 __device__ __forceinline__ uint32_t sobol(uint32_t index, uint32_t dimension) {
-    uint32_t x = 0;
-    const uint32_t *dirs = c_sobol + dimension * 32;
-    while (index) {
-        const int bit = __ffs(index) - 1;
-        x ^= dirs[bit];
-        index &= index - 1;
-    }
-    return x;
+    if (dimension == 0) return __brev(index);
+    const uint32_t *t = g_sobol_bytes + (dimension - 1) * 1024;
+    return __ldg(&t[index & 0xffu]) ^ __ldg(&t[256 + ((index >> 8) & 0xffu)]) ^ __ldg(&t[512 + ((index >> 16) & 0xffu)]) ^
+           __ldg(&t[768 + (index >> 24)]);
 }
 
 // sample4 (sampler.glsl:47-55): the 4-D point of `group` for this pixel's sample.

@@ -120,19 +120,28 @@ __device__ __forceinline__ bool watertight(const Shear &s, float tmin, float tma
     return true;
 }
 
-// The slab test of the watertight path: exits scaled by 1 + 2*gamma(3) (Ize 2013),
-// boxes already widened at upload. Returns the entry, or a negative value on a miss.
+// The slab test of the watertight path, one fused multiply-add per plane:
+// t = lo * inv + (-o * inv). The boxes are widened at upload by 2^-16 of the scene's
+// coordinate scale, which covers the rounding of this form (it moves a plane by at most
+// 4 ulps of the largest coordinate involved) and the watertight test's own (a hit lies
+// within a few ulps of |v - o| of its triangle) for origins within 64 scene scales;
+// exits are also scaled by 1 + 2*gamma(3) (Ize 2013). True when [tmin, tmax] meets the
+// box; `enter` is the entry distance.
 __device__ __forceinline__ bool box_exact(float lox, float hix, float loy, float hiy, float loz, float hiz,
-                                          const float3 &o, const float3 &inv, float tmin, float tmax,
+                                          const float3 &inv, const float3 &oinv, float tmin, float tmax,
                                           float &enter) {
     const float kScale = 1.0000003576f;
-    float x0 = fmul_(fsub_(lox, o.x), inv.x), x1 = fmul_(fsub_(hix, o.x), inv.x);
-    float y0 = fmul_(fsub_(loy, o.y), inv.y), y1 = fmul_(fsub_(hiy, o.y), inv.y);
-    float z0 = fmul_(fsub_(loz, o.z), inv.z), z1 = fmul_(fsub_(hiz, o.z), inv.z);
-    float e = fmaxf(fmaxf(fminf(x0, x1), fminf(y0, y1)), fmaxf(fminf(z0, z1), tmin));
-    float l = fminf(fminf(fmaxf(x0, x1), fmaxf(y0, y1)), fminf(fmaxf(z0, z1), tmax)) * kScale;
+    const float x0 = fmaf(lox, inv.x, oinv.x), x1 = fmaf(hix, inv.x, oinv.x);
+    const float y0 = fmaf(loy, inv.y, oinv.y), y1 = fmaf(hiy, inv.y, oinv.y);
+    const float z0 = fmaf(loz, inv.z, oinv.z), z1 = fmaf(hiz, inv.z, oinv.z);
+    const float e = fmaxf(fmaxf(fminf(x0, x1), fminf(y0, y1)), fmaxf(fminf(z0, z1), tmin));
+    const float l = fminf(fminf(fmaxf(x0, x1), fmaxf(y0, y1)), fminf(fmaxf(z0, z1), tmax)) * kScale;
     enter = e;
     return e <= l;
+}
+
+__device__ __forceinline__ float3 neg_origin_times(const float3 &o, const float3 &inv) {
+    return make_float3(-fmul_(o.x, inv.x), -fmul_(o.y, inv.y), -fmul_(o.z, inv.z));
 }
 
 // box_entry (bvh.glsl:17-25), exactly: the entry (0 when inside) or -1.
@@ -215,29 +224,46 @@ struct Visits {
     uint32_t nodes = 0, tests = 0;
 };
 
-// The closest (or any) hit along r, watertight. `overflow` is set when a push was lost.
-template <bool kAny, int kStack, bool kCount = false>
-__device__ __forceinline__ Hit trace_exact(const DeviceScene &s, const Ray &r, int *stack_base, int stride,
-                                           bool &overflow, Visits &visits) {
-    Hit h{r.tmax, -1, -1, 0.0f, 0.0f};
-    const DeviceBvh &b = s.bvh;
-    if (b.empty) return h;
-    const float3 inv = safe_inverse(r.d);
-    const Shear sh = make_shear(r.o, r.d);
-    float enter;
-    if (!box_exact(b.root_lo[0], b.root_hi[0], b.root_lo[1], b.root_hi[1], b.root_lo[2], b.root_hi[2], r.o, inv,
-                   r.tmin, r.tmax, enter))
-        return h;
-    SharedStack<kStack> st(stack_base, stride);
-    int node = b.root;
-    for (;;) {
+// One ray's watertight traversal as resumable state: `start` tests the root, `step` runs
+// interior visits down to a leaf and tests that leaf's triangles, and reports whether
+// the ray is done. The closest hit keeps ties in t for the smaller source id, so the
+// result is independent of the visiting order.
+template <bool kAny, int kStack, bool kCount>
+struct ExactTracer {
+    Ray r;
+    float3 inv, oinv;
+    Shear sh;
+    Hit h;
+    int node;
+    SharedStack<kStack> st;
+
+    __device__ __forceinline__ ExactTracer(int *stack_base, int stride) : st(stack_base, stride) {}
+
+    // False when the ray misses the scene's root box (h is then the miss).
+    __device__ __forceinline__ bool start(const DeviceBvh &b, const Ray &ray) {
+        r = ray;
+        h = Hit{r.tmax, -1, -1, 0.0f, 0.0f};
+        st.sp = 0;
+        if (b.empty) return false;
+        inv = safe_inverse(r.d);
+        oinv = neg_origin_times(r.o, inv);
+        sh = make_shear(r.o, r.d);
+        float enter;
+        node = b.root;
+        return box_exact(b.root_lo[0], b.root_hi[0], b.root_lo[1], b.root_hi[1], b.root_lo[2], b.root_hi[2], inv, oinv,
+                         r.tmin, r.tmax, enter);
+    }
+
+    // Interior visits until a leaf, then that leaf. True when the ray is done.
+    __device__ __forceinline__ bool step(const DeviceScene &s, bool &overflow, Visits &visits) {
+        const DeviceBvh &b = s.bvh;
         while (node >= 0) {
             if (kCount) visits.nodes++;
             const float4 *e = b.entries + (size_t)node * 4;
             const float4 n0 = __ldg(e), n1 = __ldg(e + 1), n2 = __ldg(e + 2), n3 = __ldg(e + 3);
             float ea, eb;
-            const bool ha = box_exact(n0.x, n0.y, n0.z, n0.w, n2.x, n2.y, r.o, inv, r.tmin, h.t, ea);
-            const bool hb = box_exact(n1.x, n1.y, n1.z, n1.w, n2.z, n2.w, r.o, inv, r.tmin, h.t, eb);
+            const bool ha = box_exact(n0.x, n0.y, n0.z, n0.w, n2.x, n2.y, inv, oinv, r.tmin, h.t, ea);
+            const bool hb = box_exact(n1.x, n1.y, n1.z, n1.w, n2.z, n2.w, inv, oinv, r.tmin, h.t, eb);
             const int l0 = __float_as_int(n3.x), l1 = __float_as_int(n3.y);
             if (ha && hb) {
                 const bool left_first = ea <= eb;
@@ -248,7 +274,7 @@ __device__ __forceinline__ Hit trace_exact(const DeviceScene &s, const Ray &r, i
             } else if (hb) {
                 node = l1;
             } else {
-                if (st.empty()) return h;
+                if (st.empty()) return true;
                 node = st.pop();
             }
         }
@@ -269,10 +295,41 @@ __device__ __forceinline__ Hit trace_exact(const DeviceScene &s, const Ray &r, i
             h.slot = (int)(first + i);
             h.u = u;
             h.v = v;
-            if (kAny) return h;
+            if (kAny) return true;
         }
-        if (st.empty()) return h;
+        if (st.empty()) return true;
         node = st.pop();
+        return false;
+    }
+};
+
+// The closest (or any) hit along r, watertight. `overflow` is set when a push was lost.
+template <bool kAny, int kStack, bool kCount = false>
+__device__ __forceinline__ Hit trace_exact(const DeviceScene &s, const Ray &r, int *stack_base, int stride,
+                                           bool &overflow, Visits &visits) {
+    ExactTracer<kAny, kStack, kCount> tr(stack_base, stride);
+    if (!tr.start(s.bvh, r)) return tr.h;
+    while (!tr.step(s, overflow, visits)) {
+    }
+    return tr.h;
+}
+
+// A resident grid over a queue of `count` rays: each warp takes 32 consecutive queue
+// entries at a time (neighbouring primary rays, or rays a shading warp pushed together),
+// which keeps its lanes on similar nodes. `load(i)` gives ray i and
+// `store(i, hit, ray)` takes its result. (Refilling lanes individually from the queue as
+// they finish was measured slower here: it breaks that coherence.)
+template <bool kAny, int kStack, bool kCount, class Load, class Store>
+__device__ __forceinline__ void trace_strided(const DeviceScene &s, uint32_t count, int *stack_base, int stride,
+                                              Load load, Store store, bool &overflow, Visits &visits) {
+    ExactTracer<kAny, kStack, kCount> tr(stack_base, stride);
+    const uint32_t step = gridDim.x * blockDim.x;
+    for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < count; i += step) {
+        if (tr.start(s.bvh, load(i))) {
+            while (!tr.step(s, overflow, visits)) {
+            }
+        }
+        store(i, tr.h, tr.r);
     }
 }
 
