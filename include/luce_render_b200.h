@@ -191,6 +191,18 @@ int lr_gpu_scene_upload(lr_context *ctx, const lr_scene *scene, lr_gpu_scene **o
 /* GpuScene.destroy (device.lucb:108-121). */
 void lr_gpu_scene_destroy(lr_gpu_scene *scene);
 
+/* What a scene holds on the device (no reference counterpart: the wide BVHs are this
+ * build's): bytes, the BVH2's depth, the 4- and 8-wide collapses' node counts and
+ * traversal stack bounds, and the width the watertight path takes by default. */
+typedef struct {
+    uint64_t bytes;
+    uint32_t bvh2_depth;
+    uint64_t wide4_nodes, wide8_nodes;
+    uint32_t wide4_stack, wide8_stack;
+    uint32_t width, stack;
+} lr_gpu_scene_info;
+int lr_gpu_scene_info_get(const lr_gpu_scene *scene, lr_gpu_scene_info *out);
+
 /* Query flags. LR_TRACE_ANY: any-hit (trace_any, bvh.glsl:93-122) instead of the
  * closest hit. LR_TRACE_REFERENCE: the reference's own traversal and Moller-Trumbore
  * test (bvh.glsl:17-90, box order and tie rule included) instead of the default
@@ -200,6 +212,13 @@ void lr_gpu_scene_destroy(lr_gpu_scene *scene);
 #define LR_TRACE_ANY 1u
 #define LR_TRACE_REFERENCE 2u
 #define LR_TRACE_COUNT 4u
+/* The watertight path's BVH width (at most one): the reference's BVH2, or its 4- or 8-wide
+ * collapse (a wide request whose traversal stack does not fit falls back to 4, then 2).
+ * None: the BVH2, the fastest on sm_100a. Results are the same bit for bit; only speed
+ * differs. */
+#define LR_TRACE_BVH2 8u
+#define LR_TRACE_BVH4 16u
+#define LR_TRACE_BVH8 32u
 
 /* render.probe (device.lucb:138-160): the pixel-centre ray of every pixel of
  * `frame` (probe.comp:21-34), row by row from the top; per pixel the polygon hit

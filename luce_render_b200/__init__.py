@@ -126,6 +126,12 @@ class SceneInfo(C.Structure):
                 ("material_count", C.c_uint32), ("bvh_depth", C.c_uint32)]
 
 
+class GpuSceneInfo(C.Structure):
+    _fields_ = [("bytes", C.c_uint64), ("bvh2_depth", C.c_uint32), ("wide4_nodes", C.c_uint64),
+                ("wide8_nodes", C.c_uint64), ("wide4_stack", C.c_uint32), ("wide8_stack", C.c_uint32),
+                ("width", C.c_uint32), ("stack", C.c_uint32)]
+
+
 class Frame(C.Structure):
     """RayFrame (camera.lucb:26-54)."""
     _fields_ = [("position", C.c_double * 3), ("corner", C.c_double * 3), ("du", C.c_double * 3),
@@ -196,6 +202,7 @@ _SIGNATURES = {
     "lr_scene_camera": (C.c_int, [_vp, _i32, C.POINTER(Camera)]),
     "lr_gpu_scene_upload": (C.c_int, [_vp, _vp, C.POINTER(_vp)]),
     "lr_gpu_scene_destroy": (None, [_vp]),
+    "lr_gpu_scene_info_get": (C.c_int, [_vp, C.POINTER(GpuSceneInfo)]),
     "lr_probe": (C.c_int, [_vp, _vp, C.POINTER(Frame), _u32, C.POINTER(C.c_uint32), C.POINTER(C.c_float)]),
     "lr_trace_rays": (C.c_int, [_vp, _vp, C.POINTER(C.c_float), _u64, C.POINTER(C.c_float), _u32]),
     "lr_trace_rays_device": (C.c_int, [_vp, _vp, _vp, _u64, _vp, _u32]),
@@ -521,6 +528,12 @@ class GpuScene:
 
     close = destroy
 
+    @property
+    def info(self) -> GpuSceneInfo:
+        info = GpuSceneInfo()
+        _check(lib.lr_gpu_scene_info_get(self.handle, C.byref(info)))
+        return info
+
     def __del__(self):
         try:
             self.destroy()
@@ -539,13 +552,18 @@ def probe(ctx: Context, scene: GpuScene, frame: Frame, reference: bool = False):
     return faces, distances
 
 
+TRACE_BVH = {0: 0, 2: 8, 4: 16, 8: 32}
+
+
 def trace_rays(ctx: Context, scene: GpuScene, rays: np.ndarray, any_hit: bool = False,
-               reference: bool = False, count: bool = False) -> np.ndarray:
+               reference: bool = False, count: bool = False, width: int = 0) -> np.ndarray:
     """Closest (or any) hits of rays (n x 8 floats: origin, tmin, direction, tmax):
-    n x 4 words (t, triangle id as int32, u, v)."""
+    n x 4 words (t, triangle id as int32, u, v). `width` picks the watertight path's BVH
+    (2, 4 or 8; 0 the default)."""
     rays = np.ascontiguousarray(rays, np.float32).reshape(-1, 8)
     hits = np.empty((len(rays), 4), np.float32)
     flags = (TRACE_ANY if any_hit else 0) | (TRACE_REFERENCE if reference else 0) | (TRACE_COUNT if count else 0)
+    flags |= TRACE_BVH[width]
     _check(lib.lr_trace_rays(ctx.handle, scene.handle, _fptr(rays), len(rays), _fptr(hits), flags))
     return hits
 

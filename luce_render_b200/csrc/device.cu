@@ -8,6 +8,7 @@
 
 #include "device.hpp"
 #include "traverse.cuh"
+#include "wide.hpp"
 
 namespace lr {
 
@@ -80,11 +81,11 @@ __global__ void __launch_bounds__(kBlock) trace_kernel(DeviceScene s, const floa
 
 // The watertight path over a ray list: a grid sized to the GPU's resident blocks, each
 // warp taking 32 consecutive rays at a time.
-template <bool kAny, int kStack, bool kCount>
+template <int W, bool kAny, int kStack, bool kCount>
 __global__ void __launch_bounds__(kBlock) trace_resident_kernel(DeviceScene s, const float4 *__restrict__ rays,
                                                                uint32_t n, float4 *__restrict__ hits, int *status,
                                                                unsigned long long *counts) {
-    __shared__ int stack[kStack * kBlock];
+    __shared__ int stack[TracerOf<W, kAny, kStack, kCount>::kInts * kBlock];
     bool overflow = false;
     Visits visits;
     auto load = [&](uint32_t i) {
@@ -94,7 +95,7 @@ __global__ void __launch_bounds__(kBlock) trace_resident_kernel(DeviceScene s, c
     auto store = [&](uint32_t i, const Hit &h, const Ray &) {
         hits[i] = make_float4(h.t, __int_as_float(h.id), h.u, h.v);
     };
-    trace_strided<kAny, kStack, kCount>(s, n, stack + threadIdx.x, kBlock, load, store, overflow, visits);
+    trace_strided<W, kAny, kStack, kCount>(s, n, stack + threadIdx.x, kBlock, load, store, overflow, visits);
     note_overflow(status, overflow);
     if (kCount) add_visits(counts, visits);
 }
@@ -106,6 +107,63 @@ int stack_for(uint32_t depth) {
     fail(LR_LIMIT, "the BVH is deeper than 94 levels");
 }
 
+}  // namespace
+
+// The width the watertight path uses when the caller names none: the BVH2, which on
+// sm_100a traces incoherent rays faster than the 4- and 8-wide collapses (1.96 against
+// 1.49 Grays/s on the 1M-triangle scene). A wide request falls back to 4, then to the
+// BVH2, when the scene's stack bound does not fit. The environment variable
+// LUCE_RENDER_B200_BVH_WIDTH (2, 4 or 8) overrides the default, for tuning.
+TraversalChoice choose_traversal(const DeviceScene &s, int requested) {
+    if (requested == 0) {
+        requested = 2;
+        if (const char *env = std::getenv("LUCE_RENDER_B200_BVH_WIDTH")) {
+            const int w = std::atoi(env);
+            if (w == 2 || w == 4 || w == 8) requested = w;
+        }
+    }
+    auto wide_stack = [](uint32_t bound) { return bound + 1 <= 32 ? 32 : (bound + 1 <= 48 ? 48 : 0); };
+    if (requested == 8 && wide_stack(s.wide8.max_stack)) return {8, wide_stack(s.wide8.max_stack)};
+    if (requested >= 4 && wide_stack(s.wide4.max_stack)) return {4, wide_stack(s.wide4.max_stack)};
+    return {2, stack_for(s.depth)};
+}
+
+namespace {
+
+template <int W, bool kAny, int kStack, bool kCount>
+void launch_resident(const lr_gpu_scene *gs, const float4 *rays, uint64_t n, float4 *hits, int *status,
+                     unsigned long long *counts, cudaStream_t stream) {
+    static int resident = 0;
+    if (!resident) {
+        int per_sm = 0, device = 0, sms = 0;
+        LR_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, trace_resident_kernel<W, kAny, kStack, kCount>,
+                                                              kBlock, 0));
+        LR_CUDA(cudaGetDevice(&device));
+        LR_CUDA(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device));
+        resident = std::max(1, per_sm) * sms;
+    }
+    const uint64_t needed = (n + kBlock - 1) / kBlock;
+    const unsigned grid = (unsigned)std::min<uint64_t>(needed, (uint64_t)resident);
+    trace_resident_kernel<W, kAny, kStack, kCount><<<grid, kBlock, 0, stream>>>(gs->scene, rays, (uint32_t)n, hits,
+                                                                               status, counts);
+}
+
+template <bool kAny, bool kCount>
+void dispatch_exact(const lr_gpu_scene *gs, const float4 *rays, uint64_t n, float4 *hits, int *status,
+                    unsigned long long *counts, cudaStream_t stream, int requested_width) {
+    if (n > 0xffffffffull) fail(LR_LIMIT, "a ray query holds at most 2^32 - 1 rays");
+    const TraversalChoice c = choose_traversal(gs->scene, requested_width);
+    switch (c.width * 1000 + c.stack) {
+        case 8032: launch_resident<8, kAny, 32, kCount>(gs, rays, n, hits, status, counts, stream); break;
+        case 8048: launch_resident<8, kAny, 48, kCount>(gs, rays, n, hits, status, counts, stream); break;
+        case 4032: launch_resident<4, kAny, 32, kCount>(gs, rays, n, hits, status, counts, stream); break;
+        case 4048: launch_resident<4, kAny, 48, kCount>(gs, rays, n, hits, status, counts, stream); break;
+        case 2032: launch_resident<2, kAny, 32, kCount>(gs, rays, n, hits, status, counts, stream); break;
+        case 2064: launch_resident<2, kAny, 64, kCount>(gs, rays, n, hits, status, counts, stream); break;
+        default: launch_resident<2, kAny, 96, kCount>(gs, rays, n, hits, status, counts, stream); break;
+    }
+}
+
 template <bool kRef, int kStack>
 void launch_probe(const lr_gpu_scene *gs, const ProbeFrame &f, uint64_t count, uint32_t *faces, float *ts,
                   int *status, cudaStream_t stream) {
@@ -113,36 +171,20 @@ void launch_probe(const lr_gpu_scene *gs, const ProbeFrame &f, uint64_t count, u
     probe_kernel<kRef, kStack><<<grid, kBlock, 0, stream>>>(gs->scene, f, faces, ts, status);
 }
 
-template <bool kRef, bool kAny, int kStack, bool kCount>
-void launch_trace(const lr_gpu_scene *gs, const float4 *rays, uint64_t n, float4 *hits, int *status,
-                  unsigned long long *counts, cudaStream_t stream) {
-    if (kRef) {
-        const unsigned grid = (unsigned)((n + kBlock - 1) / kBlock);
-        trace_kernel<kRef, kAny, kStack, kCount><<<grid, kBlock, 0, stream>>>(gs->scene, rays, n, hits, status, counts);
-        return;
-    }
-    if (n > 0xffffffffull) fail(LR_LIMIT, "a ray query holds at most 2^32 - 1 rays");
-    static int resident = 0;
-    if (!resident) {
-        int per_sm = 0, device = 0, sms = 0;
-        LR_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, trace_resident_kernel<kAny, kStack, kCount>, kBlock, 0));
-        LR_CUDA(cudaGetDevice(&device));
-        LR_CUDA(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device));
-        resident = std::max(1, per_sm) * sms;
-    }
-    const uint64_t needed = (n + kBlock - 1) / kBlock;
-    const unsigned grid = (unsigned)std::min<uint64_t>(needed, (uint64_t)resident);
-    trace_resident_kernel<kAny, kStack, kCount><<<grid, kBlock, 0, stream>>>(gs->scene, rays, (uint32_t)n, hits, status,
-                                                                            counts);
+template <bool kAny, int kStack, bool kCount>
+void launch_reference(const lr_gpu_scene *gs, const float4 *rays, uint64_t n, float4 *hits, int *status,
+                      unsigned long long *counts, cudaStream_t stream) {
+    const unsigned grid = (unsigned)((n + kBlock - 1) / kBlock);
+    trace_kernel<true, kAny, kStack, kCount><<<grid, kBlock, 0, stream>>>(gs->scene, rays, n, hits, status, counts);
 }
 
-template <bool kRef, bool kAny, bool kCount>
-void dispatch_trace(const lr_gpu_scene *gs, const float4 *rays, uint64_t n, float4 *hits, int *status,
-                    unsigned long long *counts, cudaStream_t stream) {
+template <bool kAny, bool kCount>
+void dispatch_reference(const lr_gpu_scene *gs, const float4 *rays, uint64_t n, float4 *hits, int *status,
+                        unsigned long long *counts, cudaStream_t stream) {
     switch (stack_for(gs->scene.depth)) {
-        case 32: launch_trace<kRef, kAny, 32, kCount>(gs, rays, n, hits, status, counts, stream); break;
-        case 64: launch_trace<kRef, kAny, 64, kCount>(gs, rays, n, hits, status, counts, stream); break;
-        default: launch_trace<kRef, kAny, 96, kCount>(gs, rays, n, hits, status, counts, stream); break;
+        case 32: launch_reference<kAny, 32, kCount>(gs, rays, n, hits, status, counts, stream); break;
+        case 64: launch_reference<kAny, 64, kCount>(gs, rays, n, hits, status, counts, stream); break;
+        default: launch_reference<kAny, 96, kCount>(gs, rays, n, hits, status, counts, stream); break;
     }
 }
 
@@ -385,6 +427,8 @@ int lr_gpu_scene_upload(lr_context *ctx, const lr_scene *scene, lr_gpu_scene **o
         LR_CUDA(cudaSetDevice(ctx->device));
         HostLayout L;
         build_layout(*scene, L);
+        const WideBvh w4 = build_wide(scene->nodes, 4, L.delta, widen_down, widen_up, leaf_link);
+        const WideBvh w8 = build_wide(scene->nodes, 8, L.delta, widen_down, widen_up, leaf_link);
         const size_t T = scene->triangle_count(), P = scene->point_count();
         // One allocation, arrays at 256-byte offsets; empty arrays still get room.
         struct Part {
@@ -401,6 +445,8 @@ int lr_gpu_scene_upload(lr_context *ctx, const lr_scene *scene, lr_gpu_scene **o
             {scene->faces.data(), T * sizeof(uint32_t), 0},
             {scene->order.data(), T * sizeof(uint32_t), 0},
             {L.shading.data(), T * sizeof(uint4), 0},
+            {w4.nodes.data(), w4.nodes.size() * sizeof(float), 0},
+            {w8.nodes.data(), w8.nodes.size() * sizeof(float), 0},
         };
         size_t total = 0;
         for (auto &p : parts) {
@@ -425,6 +471,10 @@ int lr_gpu_scene_upload(lr_context *ctx, const lr_scene *scene, lr_gpu_scene **o
         s.faces = (const uint32_t *)(base + parts[5].offset);
         s.ids = (const uint32_t *)(base + parts[6].offset);
         s.shading = (const uint4 *)(base + parts[7].offset);
+        s.wide4 = DeviceWide{(const float4 *)(base + parts[8].offset), T ? 4 : 0, w4.max_stack};
+        s.wide8 = DeviceWide{(const float4 *)(base + parts[9].offset), T ? 8 : 0, w8.max_stack};
+        gs->wide4_nodes = w4.node_count;
+        gs->wide8_nodes = w8.node_count;
         for (DeviceBvh *b : {&s.bvh, &s.ref_bvh}) {
             b->root = L.root;
             b->empty = T == 0 ? 1 : 0;
@@ -443,6 +493,21 @@ int lr_gpu_scene_upload(lr_context *ctx, const lr_scene *scene, lr_gpu_scene **o
         s.depth = scene->bvh_depth;
         stack_for(s.depth);
         *out = gs.release();
+    });
+}
+
+int lr_gpu_scene_info_get(const lr_gpu_scene *gs, lr_gpu_scene_info *out) {
+    return guarded([&] {
+        if (!gs || !out) fail(LR_INVALID, "no scene");
+        out->bytes = gs->bytes;
+        out->bvh2_depth = gs->scene.depth;
+        out->wide4_nodes = gs->wide4_nodes;
+        out->wide8_nodes = gs->wide8_nodes;
+        out->wide4_stack = gs->scene.wide4.max_stack;
+        out->wide8_stack = gs->scene.wide8.max_stack;
+        const TraversalChoice c = choose_traversal(gs->scene, 0);
+        out->width = (uint32_t)c.width;
+        out->stack = (uint32_t)c.stack;
     });
 }
 
@@ -488,17 +553,20 @@ static void trace_device(lr_context *ctx, const lr_gpu_scene *gs, const void *ra
     const float4 *r = (const float4 *)rays;
     float4 *h = (float4 *)hits;
     const bool any = flags & LR_TRACE_ANY, ref = flags & LR_TRACE_REFERENCE, count = flags & LR_TRACE_COUNT;
+    const int width = (flags & LR_TRACE_BVH2) ? 2 : (flags & LR_TRACE_BVH4) ? 4 : (flags & LR_TRACE_BVH8) ? 8 : 0;
     unsigned long long *c = ctx->counts;
-    if (count) {
-        if (ref && any) dispatch_trace<true, true, true>(gs, r, n, h, ctx->status, c, ctx->stream);
-        else if (ref) dispatch_trace<true, false, true>(gs, r, n, h, ctx->status, c, ctx->stream);
-        else if (any) dispatch_trace<false, true, true>(gs, r, n, h, ctx->status, c, ctx->stream);
-        else dispatch_trace<false, false, true>(gs, r, n, h, ctx->status, c, ctx->stream);
+    int *st = ctx->status;
+    cudaStream_t s = ctx->stream;
+    if (ref) {
+        if (any && count) dispatch_reference<true, true>(gs, r, n, h, st, c, s);
+        else if (any) dispatch_reference<true, false>(gs, r, n, h, st, c, s);
+        else if (count) dispatch_reference<false, true>(gs, r, n, h, st, c, s);
+        else dispatch_reference<false, false>(gs, r, n, h, st, c, s);
     } else {
-        if (ref && any) dispatch_trace<true, true, false>(gs, r, n, h, ctx->status, c, ctx->stream);
-        else if (ref) dispatch_trace<true, false, false>(gs, r, n, h, ctx->status, c, ctx->stream);
-        else if (any) dispatch_trace<false, true, false>(gs, r, n, h, ctx->status, c, ctx->stream);
-        else dispatch_trace<false, false, false>(gs, r, n, h, ctx->status, c, ctx->stream);
+        if (any && count) dispatch_exact<true, true>(gs, r, n, h, st, c, s, width);
+        else if (any) dispatch_exact<true, false>(gs, r, n, h, st, c, s, width);
+        else if (count) dispatch_exact<false, true>(gs, r, n, h, st, c, s, width);
+        else dispatch_exact<false, false>(gs, r, n, h, st, c, s, width);
     }
     LR_CUDA(cudaGetLastError());
 }

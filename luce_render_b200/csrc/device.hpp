@@ -31,10 +31,19 @@ struct DeviceBvh {
     int empty = 1;                     // no triangles: every ray misses
 };
 
+// A wide BVH (wide.cpp) in HBM: `width` children a node, nodes of 7 (W=4) or 14 (W=8)
+// float4s; the root is node 0.
+struct DeviceWide {
+    const float4 *nodes = nullptr;
+    int width = 0;
+    uint32_t max_stack = 0;  // the most stack entries a traversal can hold
+};
+
 // A scene in HBM (GpuScene, device.lucb:16-38).
 struct DeviceScene {
     DeviceBvh bvh;        // boxes widened outward for the watertight path
     DeviceBvh ref_bvh;    // the reference's exact boxes (LR_TRACE_REFERENCE)
+    DeviceWide wide4, wide8;  // the watertight path's 4- and 8-wide collapses of bvh
     const float4 *tris = nullptr;      // 3 float4 per leaf slot: v0 (w: source id bits), v1, v2
     const float *positions = nullptr;  // xyz per point
     const uint32_t *indices = nullptr; // 3 per leaf slot
@@ -68,4 +77,15 @@ struct lr_gpu_scene {
     lr::DeviceScene scene;
     void *allocation = nullptr;  // one device block holds every array
     size_t bytes = 0;
+    size_t wide4_nodes = 0, wide8_nodes = 0;
 };
+
+namespace lr {
+// The traversal the watertight path uses for a scene: BVH width 2, 4 or 8 and stack
+// entries (`requested` 0 picks the widest whose stack bound fits shared memory).
+struct TraversalChoice {
+    int width;
+    int stack;
+};
+TraversalChoice choose_traversal(const DeviceScene &s, int requested);
+}  // namespace lr

@@ -127,9 +127,9 @@ __global__ void __launch_bounds__(kShadeBlock) camera_kernel(View v) {
 
 // intersect_closest.comp:45-76: the nearest triangle, then the analytic lights
 // before it (camera rays skip lights invisible to the camera).
-template <int kStack, bool kCount>
+template <int W, int kStack, bool kCount>
 __global__ void __launch_bounds__(kTraceBlock) closest_kernel(View v, uint32_t round) {
-    __shared__ int stack[kStack * kTraceBlock];
+    __shared__ int stack[TracerOf<W, false, kStack, kCount>::kInts * kTraceBlock];
     const uint32_t q = round & 1u;
     const uint32_t count = v.counters[round];
     bool overflow = false;
@@ -153,16 +153,16 @@ __global__ void __launch_bounds__(kTraceBlock) closest_kernel(View v, uint32_t r
         }
         hits[i] = make_float4(t, __uint_as_float(what), h.u, h.v);
     };
-    trace_strided<false, kStack, kCount>(v.scene, count, stack + threadIdx.x, kTraceBlock, load, store, overflow,
+    trace_strided<W, false, kStack, kCount>(v.scene, count, stack + threadIdx.x, kTraceBlock, load, store, overflow,
                                          visits);
     if (overflow) atomicAdd(&v.status[0], 1);
     if (kCount) add_visits(&v.stats[4], visits);
 }
 
 // intersect_shadow.comp:51-92: unblocked light samples join their path's radiance.
-template <int kStack, bool kCount>
+template <int W, int kStack, bool kCount>
 __global__ void __launch_bounds__(kTraceBlock) shadow_kernel(View v, uint32_t round) {
-    __shared__ int stack[kStack * kTraceBlock];
+    __shared__ int stack[TracerOf<W, true, kStack, kCount>::kInts * kTraceBlock];
     const uint32_t count = v.counters[v.rounds + 1 + round];
     bool overflow = false;
     Visits visits;
@@ -176,7 +176,7 @@ __global__ void __launch_bounds__(kTraceBlock) shadow_kernel(View v, uint32_t ro
             v.radiance[path] = v.radiance[path] + v.shadow_c[i];
         }
     };
-    trace_strided<true, kStack, kCount>(v.scene, count, stack + threadIdx.x, kTraceBlock, load, store, overflow,
+    trace_strided<W, true, kStack, kCount>(v.scene, count, stack + threadIdx.x, kTraceBlock, load, store, overflow,
                                         visits);
     if (overflow) atomicAdd(&v.status[0], 1);
     if (kCount) add_visits(&v.stats[6], visits);
@@ -521,7 +521,7 @@ struct lr_renderer {
     Loaded loaded;
     void *block = nullptr;  // one device allocation for everything below the scene
     View view{};
-    int stack = 32;
+    int width = 2, stack = 32;  // the traversal variant (BVH width, stack entries)
     int grid_trace = 0, grid_shade = 0;
     cudaGraph_t graph = nullptr;
     cudaGraphExec_t exec = nullptr;
@@ -541,7 +541,7 @@ namespace {
 
 // Records one pass on `stream`. With `marks`, an event follows each kernel (profiling);
 // kCount instantiates the traversal kernels that count their work.
-template <bool kSpectral, int kStack, bool kCount>
+template <bool kSpectral, int W, int kStack, bool kCount>
 void record_pass(lr_renderer *r, cudaStream_t stream, std::vector<std::pair<cudaEvent_t, int>> *marks) {
     View &v = r->view;
     auto mark = [&](int kind) {
@@ -556,11 +556,11 @@ void record_pass(lr_renderer *r, cudaStream_t stream, std::vector<std::pair<cuda
     camera_kernel<kSpectral><<<r->grid_shade, kShadeBlock, 0, stream>>>(v);
     mark(kCamera);
     for (uint32_t round = 0; round < v.rounds; round++) {
-        closest_kernel<kStack, kCount><<<r->grid_trace, kTraceBlock, 0, stream>>>(v, round);
+        closest_kernel<W, kStack, kCount><<<r->grid_trace, kTraceBlock, 0, stream>>>(v, round);
         mark(kClosest);
         shade_kernel<kSpectral><<<r->grid_shade, kShadeBlock, 0, stream>>>(v, round);
         mark(kSurface);
-        shadow_kernel<kStack, kCount><<<r->grid_trace, kTraceBlock, 0, stream>>>(v, round);
+        shadow_kernel<W, kStack, kCount><<<r->grid_trace, kTraceBlock, 0, stream>>>(v, round);
         mark(kShadow);
     }
     finish_kernel<kSpectral><<<r->grid_shade, kShadeBlock, 0, stream>>>(v);
@@ -570,12 +570,19 @@ void record_pass(lr_renderer *r, cudaStream_t stream, std::vector<std::pair<cuda
     LR_CUDA(cudaGetLastError());
 }
 
+// The traversal variants a renderer can take: (BVH width, stack entries).
+#define LR_TRAVERSALS(X) X(8, 32) X(8, 48) X(4, 32) X(4, 48) X(2, 32) X(2, 64) X(2, 96)
+
 template <bool kSpectral, bool kCount>
 void record_any(lr_renderer *r, cudaStream_t stream, std::vector<std::pair<cudaEvent_t, int>> *marks) {
-    switch (r->stack) {
-        case 32: record_pass<kSpectral, 32, kCount>(r, stream, marks); break;
-        case 64: record_pass<kSpectral, 64, kCount>(r, stream, marks); break;
-        default: record_pass<kSpectral, 96, kCount>(r, stream, marks); break;
+    switch (r->width * 1000 + r->stack) {
+#define LR_CASE(w, k)                                                   \
+    case w * 1000 + k:                                                  \
+        record_pass<kSpectral, w, k, kCount>(r, stream, marks);         \
+        break;
+        LR_TRAVERSALS(LR_CASE)
+#undef LR_CASE
+        default: fail(LR_LIMIT, "no traversal variant for this scene");
     }
 }
 
@@ -590,10 +597,18 @@ void record(lr_renderer *r, cudaStream_t stream, std::vector<std::pair<cudaEvent
     }
 }
 
-template <bool kSpectral, int kStack>
+template <bool kSpectral>
 void size_grids(lr_renderer *r) {
     const int sms = r->ctx->sm_count;
-    r->grid_trace = grid_of(closest_kernel<kStack, false>, kTraceBlock, sms);
+    switch (r->width * 1000 + r->stack) {
+#define LR_CASE(w, k)                                                            \
+    case w * 1000 + k:                                                           \
+        r->grid_trace = grid_of(closest_kernel<w, k, false>, kTraceBlock, sms);  \
+        break;
+        LR_TRAVERSALS(LR_CASE)
+#undef LR_CASE
+        default: fail(LR_LIMIT, "no traversal variant for this scene");
+    }
     r->grid_shade = grid_of(shade_kernel<kSpectral>, kShadeBlock, sms);
 }
 
@@ -798,17 +813,11 @@ void create(lr_context *ctx, const lr_scene *scene, const lr_settings &settings,
     v.stats = (unsigned long long *)at(p_stats);
     v.status = ctx->status;
 
-    r->stack = gs->scene.depth + 2 <= 32 ? 32 : (gs->scene.depth + 2 <= 64 ? 64 : 96);
-    if (gs->scene.depth + 2 > 96) fail(LR_LIMIT, "the BVH is deeper than 94 levels");
-    if (settings.spectral) {
-        if (r->stack == 32) size_grids<true, 32>(r.get());
-        else if (r->stack == 64) size_grids<true, 64>(r.get());
-        else size_grids<true, 96>(r.get());
-    } else {
-        if (r->stack == 32) size_grids<false, 32>(r.get());
-        else if (r->stack == 64) size_grids<false, 64>(r.get());
-        else size_grids<false, 96>(r.get());
-    }
+    const TraversalChoice traversal = choose_traversal(gs->scene, 0);
+    r->width = traversal.width;
+    r->stack = traversal.stack;
+    if (settings.spectral) size_grids<true>(r.get());
+    else size_grids<false>(r.get());
     r->done_events.resize(2);
     for (auto &e : r->done_events) LR_CUDA(cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
     if (settings.profile) {

@@ -240,7 +240,8 @@ struct ExactTracer {
     __device__ __forceinline__ ExactTracer(int *stack_base, int stride) : st(stack_base, stride) {}
 
     // False when the ray misses the scene's root box (h is then the miss).
-    __device__ __forceinline__ bool start(const DeviceBvh &b, const Ray &ray) {
+    __device__ __forceinline__ bool start(const DeviceScene &s, const Ray &ray) {
+        const DeviceBvh &b = s.bvh;
         r = ray;
         h = Hit{r.tmax, -1, -1, 0.0f, 0.0f};
         st.sp = 0;
@@ -303,29 +304,211 @@ struct ExactTracer {
     }
 };
 
+__device__ __forceinline__ float fmax3(float a, float b, float c) {
+    float r;
+    asm("max.f32 %0, %1, %2, %3;" : "=f"(r) : "f"(a), "f"(b), "f"(c));
+    return r;
+}
+
+__device__ __forceinline__ float fmin3(float a, float b, float c) {
+    float r;
+    asm("min.f32 %0, %1, %2, %3;" : "=f"(r) : "f"(a), "f"(b), "f"(c));
+    return r;
+}
+
+// A per-thread stack of (link, entry distance) pairs in local memory (L1-cached and
+// interleaved across a warp's lanes, so same-depth accesses coalesce); unlike shared
+// memory it does not cap how many blocks an SM holds.
+template <int kStack>
+struct PairStack {
+    int2 items[kStack];
+    int sp = 0;
+    __device__ __forceinline__ PairStack(int *, int) {}
+    __device__ __forceinline__ bool push(int link, float t) {
+        if (sp >= kStack) return false;
+        items[sp] = make_int2(link, __float_as_int(t));
+        sp++;
+        return true;
+    }
+    __device__ __forceinline__ void pop(int &link, float &t) {
+        sp--;
+        const int2 e = items[sp];
+        link = e.x;
+        t = __int_as_float(e.y);
+    }
+    __device__ __forceinline__ bool empty() const { return sp == 0; }
+};
+
+// The watertight traversal over a wide BVH (wide.cpp): each node's W child boxes are
+// tested together (one fused multiply-add per plane, the near and far planes picked once
+// per ray by the direction's signs), the nearest hit child is taken next and the others
+// are pushed far to near with their entry distances, so a popped subtree that starts
+// beyond the current hit is skipped without fetching it. Leaves and triangles are the
+// BVH2's, with the same tie rule, so results equal the BVH2 path's bit for bit.
+template <int W, bool kAny, int kStack, bool kCount>
+struct WideTracer {
+    Ray r;
+    float3 inv, oinv;
+    Shear sh;
+    Hit h;
+    int node;
+    PairStack<kStack> st;
+
+    __device__ __forceinline__ WideTracer(int *stack_base, int stride) : st(stack_base, stride) {}
+
+    __device__ __forceinline__ bool start(const DeviceScene &s, const Ray &ray) {
+        r = ray;
+        h = Hit{r.tmax, -1, -1, 0.0f, 0.0f};
+        st.sp = 0;
+        const DeviceBvh &b = s.bvh;
+        if (b.empty) return false;
+        inv = safe_inverse(r.d);
+        oinv = neg_origin_times(r.o, inv);
+        sh = make_shear(r.o, r.d);
+        node = 0;
+        float enter;
+        return box_exact(b.root_lo[0], b.root_hi[0], b.root_lo[1], b.root_hi[1], b.root_lo[2], b.root_hi[2], inv, oinv,
+                         r.tmin, r.tmax, enter);
+    }
+
+    // Compare-and-swap of (entry, link) pairs in registers, for the sorting networks.
+    static __device__ __forceinline__ void order(float &ka, int &la, float &kb, int &lb) {
+        const bool swap = ka > kb;
+        const float k = swap ? kb : ka;
+        const int l = swap ? lb : la;
+        kb = swap ? ka : kb;
+        lb = swap ? la : lb;
+        ka = k;
+        la = l;
+    }
+
+    // Runs to the end of the ray's traversal (`step` keeps the two-phase interface of
+    // ExactTracer: here one call finishes the ray).
+    __device__ __forceinline__ bool step(const DeviceScene &s, bool &overflow, Visits &visits) {
+        const DeviceWide &wide = W == 4 ? s.wide4 : s.wide8;
+        constexpr int kPlanes = W / 4;
+        constexpr int kFloat4s = 7 * kPlanes;
+        const float kMiss = __int_as_float(0x7f800000);  // +infinity: a child not hit
+        // The near and far plane of each axis for this ray's direction signs.
+        const int nx = inv.x >= 0.0f ? 0 : kPlanes, fx = kPlanes - nx;
+        const int ny = (inv.y >= 0.0f ? 2 : 3) * kPlanes, fy = 5 * kPlanes - ny;
+        const int nz = (inv.z >= 0.0f ? 4 : 5) * kPlanes, fz = 9 * kPlanes - nz;
+        for (;;) {
+            if (node >= 0) {
+                if (kCount) visits.nodes++;
+                const float4 *n = wide.nodes + (size_t)node * kFloat4s;
+                float key[W];
+                int link[W];
+#pragma unroll
+                for (int p = 0; p < kPlanes; p++) {
+                    const float4 Nx = __ldg(n + nx + p), Fx = __ldg(n + fx + p);
+                    const float4 Ny = __ldg(n + ny + p), Fy = __ldg(n + fy + p);
+                    const float4 Nz = __ldg(n + nz + p), Fz = __ldg(n + fz + p);
+                    const int4 ln = __ldg(reinterpret_cast<const int4 *>(n + 6 * kPlanes + p));
+                    const float nxs[4] = {Nx.x, Nx.y, Nx.z, Nx.w}, fxs[4] = {Fx.x, Fx.y, Fx.z, Fx.w};
+                    const float nys[4] = {Ny.x, Ny.y, Ny.z, Ny.w}, fys[4] = {Fy.x, Fy.y, Fy.z, Fy.w};
+                    const float nzs[4] = {Nz.x, Nz.y, Nz.z, Nz.w}, fzs[4] = {Fz.x, Fz.y, Fz.z, Fz.w};
+                    const int ls[4] = {ln.x, ln.y, ln.z, ln.w};
+#pragma unroll
+                    for (int c = 0; c < 4; c++) {
+                        const float e = fmax3(fmaf(nxs[c], inv.x, oinv.x), fmaf(nys[c], inv.y, oinv.y),
+                                              fmaxf(fmaf(nzs[c], inv.z, oinv.z), r.tmin));
+                        const float l = fmin3(fmaf(fxs[c], inv.x, oinv.x), fmaf(fys[c], inv.y, oinv.y),
+                                              fminf(fmaf(fzs[c], inv.z, oinv.z), h.t)) * 1.0000003576f;
+                        key[p * 4 + c] = e <= l ? e : kMiss;
+                        link[p * 4 + c] = ls[c];
+                    }
+                }
+                // Sort the children by entry (misses last), all in registers.
+                if (W == 4) {
+                    order(key[0], link[0], key[1], link[1]);
+                    order(key[2], link[2], key[3], link[3]);
+                    order(key[0], link[0], key[2], link[2]);
+                    order(key[1], link[1], key[3], link[3]);
+                    order(key[1], link[1], key[2], link[2]);
+                } else {
+                    constexpr int kNet[19][2] = {{0, 2}, {1, 3}, {4, 6}, {5, 7}, {0, 4}, {1, 5}, {2, 6},
+                                                 {3, 7}, {0, 1}, {2, 3}, {4, 5}, {6, 7}, {2, 4}, {3, 5},
+                                                 {1, 4}, {3, 6}, {1, 2}, {3, 4}, {5, 6}};
+#pragma unroll
+                    for (int i = 0; i < 19; i++)
+                        order(key[kNet[i][0]], link[kNet[i][0]], key[kNet[i][1]], link[kNet[i][1]]);
+                }
+                if (key[0] != kMiss) {
+                    // The rest onto the stack, farthest first; the nearest goes next.
+#pragma unroll
+                    for (int k = W - 1; k >= 1; k--)
+                        if (key[k] != kMiss && !st.push(link[k], key[k])) overflow = true;
+                    node = link[0];
+                    continue;
+                }
+            } else {
+                uint32_t first, count;
+                leaf_range(node, first, count);
+                if (kCount) visits.tests += count;
+                for (uint32_t i = 0; i < count; i++) {
+                    const float4 *tri = s.tris + (size_t)(first + i) * 3;
+                    const float4 a = __ldg(tri), bb = __ldg(tri + 1), c = __ldg(tri + 2);
+                    const float limit = h.id >= 0 ? __int_as_float(__float_as_int(h.t) + 1) : r.tmax;
+                    float t, u, v;
+                    if (!watertight(sh, r.tmin, limit, a, bb, c, t, u, v)) continue;
+                    const int id = __float_as_int(a.w);
+                    if (h.id >= 0 && t == h.t && id > h.id) continue;
+                    h.t = t;
+                    h.id = id;
+                    h.slot = (int)(first + i);
+                    h.u = u;
+                    h.v = v;
+                    if (kAny) return true;
+                }
+            }
+            // Next from the stack, skipping subtrees that start beyond the hit so far.
+            for (;;) {
+                if (st.empty()) return true;
+                float t;
+                st.pop(node, t);
+                if (!(t > h.t)) break;
+            }
+        }
+    }
+};
+
 // The closest (or any) hit along r, watertight. `overflow` is set when a push was lost.
 template <bool kAny, int kStack, bool kCount = false>
 __device__ __forceinline__ Hit trace_exact(const DeviceScene &s, const Ray &r, int *stack_base, int stride,
                                            bool &overflow, Visits &visits) {
     ExactTracer<kAny, kStack, kCount> tr(stack_base, stride);
-    if (!tr.start(s.bvh, r)) return tr.h;
+    if (!tr.start(s, r)) return tr.h;
     while (!tr.step(s, overflow, visits)) {
     }
     return tr.h;
 }
+
+// The watertight tracer of a BVH width: 2 (the BVH2 itself), 4 or 8 (wide.cpp), and the
+// shared-memory ints per thread its stack takes.
+template <int W, bool kAny, int kStack, bool kCount>
+struct TracerOf {
+    using type = WideTracer<W, kAny, kStack, kCount>;
+    static constexpr int kInts = 1;  // the wide tracer's stack is in local memory
+};
+template <bool kAny, int kStack, bool kCount>
+struct TracerOf<2, kAny, kStack, kCount> {
+    using type = ExactTracer<kAny, kStack, kCount>;
+    static constexpr int kInts = kStack;
+};
 
 // A resident grid over a queue of `count` rays: each warp takes 32 consecutive queue
 // entries at a time (neighbouring primary rays, or rays a shading warp pushed together),
 // which keeps its lanes on similar nodes. `load(i)` gives ray i and
 // `store(i, hit, ray)` takes its result. (Refilling lanes individually from the queue as
 // they finish was measured slower here: it breaks that coherence.)
-template <bool kAny, int kStack, bool kCount, class Load, class Store>
+template <int W, bool kAny, int kStack, bool kCount, class Load, class Store>
 __device__ __forceinline__ void trace_strided(const DeviceScene &s, uint32_t count, int *stack_base, int stride,
                                               Load load, Store store, bool &overflow, Visits &visits) {
-    ExactTracer<kAny, kStack, kCount> tr(stack_base, stride);
+    typename TracerOf<W, kAny, kStack, kCount>::type tr(stack_base, stride);
     const uint32_t step = gridDim.x * blockDim.x;
     for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < count; i += step) {
-        if (tr.start(s.bvh, load(i))) {
+        if (tr.start(s, load(i))) {
             while (!tr.step(s, overflow, visits)) {
             }
         }

@@ -1,0 +1,129 @@
+// A wide BVH for the watertight traversal path, collapsed from the reference's BVH2: each
+// wide node holds up to W (4 or 8) children, taken by repeatedly opening the child with the
+// largest surface area (the greedy collapse of Wald et al. 2008 and Ylitie et al. 2017).
+// Leaves are the BVH2's leaves unchanged, so the wide tree reaches the same triangle
+// records in the same leaf order; only interior levels are merged, which cuts the
+// dependent node fetches along a ray by about log2(W).
+//
+// Node layout (float4s, structure of arrays over the children so one load brings a plane
+// of every child): for W = 4, 7 float4 = 112 bytes -- lo.x, hi.x, lo.y, hi.y, lo.z, hi.z
+// of the 4 children, then their 4 links; for W = 8, 14 float4 = 224 bytes in the same
+// order, each plane two float4. Links: >= 0 a wide node, < 0 a leaf
+// (-1 - (first << 4 | count - 1)); an empty slot has an inverted box (lo +inf, hi -inf).
+// Boxes are widened outward like the BVH2 path's.
+#include "wide.hpp"
+
+#include <algorithm>
+#include <cmath>
+#include <cstring>
+
+namespace lr {
+namespace {
+
+float area_of(const lr_bvh_node &n) {
+    const float x = n.hi[0] - n.lo[0], y = n.hi[1] - n.lo[1], z = n.hi[2] - n.lo[2];
+    return 2.0f * (x * y + y * z + z * x);
+}
+
+float bits(int v) {
+    float f;
+    std::memcpy(&f, &v, sizeof f);
+    return f;
+}
+
+}  // namespace
+
+WideBvh build_wide(const std::vector<lr_bvh_node> &nodes, int width, float delta,
+                   float (*widen_down)(float, float), float (*widen_up)(float, float),
+                   int (*leaf_link)(const lr_bvh_node &)) {
+    WideBvh w;
+    w.width = width;
+    const int per_node = width == 4 ? 7 : 14;
+    w.floats_per_node = per_node;
+    if (nodes.empty() || nodes[0].lo[0] > nodes[0].hi[0]) return w;  // no triangles
+    struct Job {
+        uint32_t bvh2;    // the BVH2 node this wide node stands for
+        uint32_t wide;    // its index
+    };
+    std::vector<Job> queue;
+    std::vector<std::vector<uint32_t>> children_of;  // per wide node, the BVH2 nodes it holds
+    auto collapse = [&](uint32_t n) {
+        std::vector<uint32_t> list;
+        if (nodes[n].count > 0) {
+            list.push_back(n);  // a leaf root: one leaf child
+            return list;
+        }
+        list = {nodes[n].first, nodes[n].first + 1};
+        while ((int)list.size() < width) {
+            int best = -1;
+            float best_area = -1.0f;
+            for (size_t i = 0; i < list.size(); i++) {
+                const lr_bvh_node &c = nodes[list[i]];
+                if (c.count > 0) continue;
+                const float a = area_of(c);
+                if (a > best_area) {
+                    best_area = a;
+                    best = (int)i;
+                }
+            }
+            if (best < 0) break;
+            const uint32_t open = list[best];
+            list.erase(list.begin() + best);
+            list.insert(list.begin() + best, {nodes[open].first, nodes[open].first + 1});
+        }
+        return list;
+    };
+    // Breadth first: a node's interior children get consecutive indices.
+    children_of.push_back(collapse(0));
+    queue.push_back({0, 0});
+    for (size_t head = 0; head < queue.size(); head++) {
+        const uint32_t wide = queue[head].wide;
+        for (uint32_t c : children_of[wide]) {
+            if (nodes[c].count > 0) continue;
+            const uint32_t index = (uint32_t)children_of.size();
+            children_of.push_back(collapse(c));
+            queue.push_back({c, index});
+        }
+    }
+    const size_t count = children_of.size();
+    w.node_count = count;
+    w.nodes.assign(count * per_node * 4, 0.0f);
+    std::vector<uint32_t> index_of_bvh2(nodes.size(), 0xffffffffu);
+    for (const Job &j : queue) index_of_bvh2[j.bvh2] = j.wide;
+    // The wide root stands for BVH2 node 0 even when it is a leaf.
+    std::vector<uint32_t> bound(count, 0);
+    for (size_t n = 0; n < count; n++) {
+        float *base = &w.nodes[n * per_node * 4];
+        const auto &list = children_of[n];
+        const int planes = width / 4;  // float4s per plane
+        for (int slot = 0; slot < width; slot++) {
+            float lo[3] = {INFINITY, INFINITY, INFINITY}, hi[3] = {-INFINITY, -INFINITY, -INFINITY};
+            int link = 0;
+            if (slot < (int)list.size()) {
+                const lr_bvh_node &c = nodes[list[slot]];
+                for (int k = 0; k < 3; k++) {
+                    lo[k] = widen_down(c.lo[k], delta);
+                    hi[k] = widen_up(c.hi[k], delta);
+                }
+                link = c.count > 0 ? leaf_link(c) : (int)index_of_bvh2[list[slot]];
+            }
+            for (int k = 0; k < 3; k++) {
+                base[((2 * k) * planes) * 4 + slot] = lo[k];
+                base[((2 * k + 1) * planes) * 4 + slot] = hi[k];
+            }
+            base[(6 * planes) * 4 + slot] = bits(link);
+        }
+    }
+    // The deepest stack a traversal can need: at each node it keeps all but one of the
+    // hit children, so along a path the entries add up to sum(children - 1).
+    for (size_t n = count; n-- > 0;) {
+        uint32_t deepest = 0;
+        for (uint32_t c : children_of[n])
+            if (nodes[c].count == 0) deepest = std::max(deepest, bound[index_of_bvh2[c]]);
+        bound[n] = (uint32_t)children_of[n].size() - 1 + deepest;
+    }
+    w.max_stack = bound[0];
+    return w;
+}
+
+}  // namespace lr

@@ -212,11 +212,32 @@ def test_traversal_work_counts_match_oracle(ctx, incoherent, cornell):
             nodes, tests = lr.trace_counts(ctx)
             _, counts = orc.trace(a["nodes"], a["positions"], a["indices"], rays, any_hit=any_hit)
             assert (nodes, tests) == (counts.interior, counts.triangles)
-            lr.trace_rays(ctx, gs, rays, any_hit=any_hit, count=True)
+            lr.trace_rays(ctx, gs, rays, any_hit=any_hit, count=True, width=2)
             enodes, etests = lr.trace_counts(ctx)
             if not any_hit:
                 assert counts.interior <= enodes <= 1.05 * counts.interior
                 assert counts.triangles <= etests <= 1.05 * counts.triangles
+
+
+def test_bvh_widths_agree_bit_for_bit(ctx, incoherent, cornell):
+    # The 4- and 8-wide collapses reach the same leaves and keep the same tie rule, so
+    # closest and any hits equal the BVH2 path's exactly; they visit fewer nodes.
+    for fixture, rays in ((incoherent, scenes.incoherent_rays(1 << 18, seed=9)),
+                          (cornell, scenes.random_rays(1 << 16, seed=3))):
+        sc, a, gs = fixture
+        info = gs.info
+        assert info.width in (2, 4, 8)
+        base = lr.trace_rays(ctx, gs, rays, width=2, count=True)
+        base_nodes, base_tests = lr.trace_counts(ctx)
+        base_any = lr.trace_rays(ctx, gs, rays, width=2, any_hit=True)
+        for w in (4, 8):
+            hits = lr.trace_rays(ctx, gs, rays, width=w, count=True)
+            nodes, tests = lr.trace_counts(ctx)
+            assert np.array_equal(_as_bits(hits), _as_bits(base)), w
+            anyh = lr.trace_rays(ctx, gs, rays, width=w, any_hit=True)
+            assert np.array_equal(lr.hit_ids(anyh) >= 0, lr.hit_ids(base_any) >= 0), w
+            if sc.triangle_count() > 1000:
+                assert nodes < base_nodes, (w, nodes, base_nodes)
 
 
 def test_million_triangles_properties_at_full_size(ctx, incoherent):
