@@ -227,6 +227,20 @@ int lr_gpu_scene_info_get(const lr_gpu_scene *scene, lr_gpu_scene_info *out);
 int lr_probe(lr_context *ctx, const lr_gpu_scene *scene, const lr_frame *frame, uint32_t flags,
              uint32_t *faces, float *distances);
 
+/* lr_probe without device allocation: the same results, bit for bit, staged through a
+ * static device array of LR_PROBE_STATIC_PIXELS pixels (16 MiB, reserved when the
+ * library's module loads on a device) instead of stream-ordered scratch. No counterpart
+ * in the reference, whose probe allocates its result buffers per call; this one is for
+ * callers that must not allocate device memory, such as a serving loop whose scene cache
+ * holds the GPU at its memory budget. Larger frames are refused with LR_LIMIT. The
+ * first call on a device does set-up (looks up the array's address, which may load the
+ * module), so make it before any stream capture. All calls on one device share the
+ * array: calls that overlap in time, from any thread or context on that device, race;
+ * each call waits for its result, so calls made one after another are safe. */
+#define LR_PROBE_STATIC_PIXELS 2097152u
+int lr_probe_static(lr_context *ctx, const lr_gpu_scene *scene, const lr_frame *frame,
+                    uint32_t flags, uint32_t *faces, float *distances);
+
 /* Ray queries, the ray-list form of the probe. A ray is 8 floats (origin xyz, tmin,
  * direction xyz, tmax; hits have tmin < t < tmax); a hit is 4 words (t, triangle id as
  * int32 -- the caller's triangle numbering, -1 none --, barycentrics u and v of the

@@ -204,6 +204,8 @@ _SIGNATURES = {
     "lr_gpu_scene_destroy": (None, [_vp]),
     "lr_gpu_scene_info_get": (C.c_int, [_vp, C.POINTER(GpuSceneInfo)]),
     "lr_probe": (C.c_int, [_vp, _vp, C.POINTER(Frame), _u32, C.POINTER(C.c_uint32), C.POINTER(C.c_float)]),
+    "lr_probe_static": (C.c_int, [_vp, _vp, C.POINTER(Frame), _u32, C.POINTER(C.c_uint32),
+                                  C.POINTER(C.c_float)]),
     "lr_trace_rays": (C.c_int, [_vp, _vp, C.POINTER(C.c_float), _u64, C.POINTER(C.c_float), _u32]),
     "lr_trace_rays_device": (C.c_int, [_vp, _vp, _vp, _u64, _vp, _u32]),
     "lr_trace_counts": (C.c_int, [_vp, C.POINTER(C.c_uint64)]),
@@ -549,6 +551,20 @@ def probe(ctx: Context, scene: GpuScene, frame: Frame, reference: bool = False):
     distances = np.empty(n, np.float32)
     _check(lib.lr_probe(ctx.handle, scene.handle, C.byref(frame), TRACE_REFERENCE if reference else 0,
                         _uptr(faces), _fptr(distances)))
+    return faces, distances
+
+
+PROBE_STATIC_PIXELS = 1 << 21
+
+
+def probe_static(ctx: Context, scene: GpuScene, frame: Frame, reference: bool = False):
+    """probe() staged through the library's static device scratch (no device allocation;
+    at most PROBE_STATIC_PIXELS pixels; calls on one device must not overlap)."""
+    n = int(frame.width) * int(frame.height)
+    faces = np.empty(n, np.uint32)
+    distances = np.empty(n, np.float32)
+    _check(lib.lr_probe_static(ctx.handle, scene.handle, C.byref(frame), TRACE_REFERENCE if reference else 0,
+                               _uptr(faces), _fptr(distances)))
     return faces, distances
 
 

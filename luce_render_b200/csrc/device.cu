@@ -4,6 +4,8 @@
 #include <cmath>
 #include <cstring>
 #include <memory>
+#include <mutex>
+#include <string>
 #include <vector>
 
 #include "device.hpp"
@@ -542,6 +544,66 @@ int lr_probe(lr_context *ctx, const lr_gpu_scene *gs, const lr_frame *frame, uin
         LR_CUDA(cudaMemcpyAsync(faces, d_faces, count * 4, cudaMemcpyDeviceToHost, ctx->stream));
         LR_CUDA(cudaMemcpyAsync(distances, d_ts, count * 4, cudaMemcpyDeviceToHost, ctx->stream));
         LR_CUDA(cudaFreeAsync(buffer, ctx->stream));
+        LR_CUDA(cudaStreamSynchronize(ctx->stream));
+        check_status(ctx);
+    });
+}
+
+}  // extern "C"
+
+// The device scratch of lr_probe_static: LR_PROBE_STATIC_PIXELS face ids, then as many
+// distances (16 MiB), reserved when the module loads on a device and never freed.
+static __device__ __align__(256) unsigned char g_probe_scratch[(size_t)LR_PROBE_STATIC_PIXELS * 8];
+
+namespace {
+
+constexpr int kScratchDevices = 64;
+std::mutex g_scratch_mutex;
+void *g_scratch_of[kScratchDevices] = {};
+
+// The address of g_probe_scratch on `device`, looked up once per device with that
+// device current (the first lookup may load the module there).
+void *probe_scratch(int device) {
+    if (device < 0 || device >= kScratchDevices) fail(LR_LIMIT, "lr_probe_static serves devices 0 to 63");
+    std::lock_guard<std::mutex> lock(g_scratch_mutex);
+    if (!g_scratch_of[device]) {
+        void *address = nullptr;
+        LR_CUDA(cudaGetSymbolAddress(&address, g_probe_scratch));
+        if (!address) fail(LR_DEVICE, "no address for the static probe scratch");
+        g_scratch_of[device] = address;
+    }
+    return g_scratch_of[device];
+}
+
+}  // namespace
+
+extern "C" {
+
+int lr_probe_static(lr_context *ctx, const lr_gpu_scene *gs, const lr_frame *frame, uint32_t flags,
+                    uint32_t *faces, float *distances) {
+    return guarded([&] {
+        if (!ctx || !gs || !frame || !faces || !distances) fail(LR_INVALID, "a probe needs one result per pixel");
+        if (frame->width == 0 || frame->height == 0) fail(LR_INVALID, "an image needs pixels");
+        const uint64_t count = (uint64_t)frame->width * frame->height;
+        if (count > LR_PROBE_STATIC_PIXELS)
+            fail(LR_LIMIT, "lr_probe_static takes at most " + std::to_string(LR_PROBE_STATIC_PIXELS) +
+                               " pixels (its static scratch); this frame has " + std::to_string(count) +
+                               ": use lr_probe");
+        ProbeFrame f;
+        pack_frame(*frame, f.b);
+        LR_CUDA(cudaSetDevice(ctx->device));
+        char *scratch = (char *)probe_scratch(ctx->device);
+        // The kernel writes every pixel's face and distance, so nothing in the scratch has
+        // to start at zero; the status words it may raise are the context's, kept at zero.
+        uint32_t *d_faces = (uint32_t *)scratch;
+        float *d_ts = (float *)(scratch + (size_t)LR_PROBE_STATIC_PIXELS * 4);
+        if (flags & LR_TRACE_REFERENCE)
+            dispatch_probe<true>(gs, f, count, d_faces, d_ts, ctx->status, ctx->stream);
+        else
+            dispatch_probe<false>(gs, f, count, d_faces, d_ts, ctx->status, ctx->stream);
+        LR_CUDA(cudaGetLastError());
+        LR_CUDA(cudaMemcpyAsync(faces, d_faces, count * 4, cudaMemcpyDeviceToHost, ctx->stream));
+        LR_CUDA(cudaMemcpyAsync(distances, d_ts, count * 4, cudaMemcpyDeviceToHost, ctx->stream));
         LR_CUDA(cudaStreamSynchronize(ctx->stream));
         check_status(ctx);
     });
