@@ -327,7 +327,7 @@ def main():
             "cpu_baseline": cpu,
             "e2e": {"value": e2e_value, "unit": "Mrays/s", "h2d_bytes_per_step": 0,
                     "d2h_bytes_per_step": WIDTH * HEIGHT * 16},
-            "gpu_launches": K * (2 + 3 * (BOUNCES + 1) + 2),
+            "gpu_launches": K * (1 + 3 * (BOUNCES + 1) + 2),
             "clocks": clock_info,
         }
         print(json.dumps(line))

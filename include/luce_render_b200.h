@@ -323,6 +323,49 @@ int lr_renderer_stats(lr_renderer *renderer, lr_render_stats *out);
 /* Renderer.destroy (integrator.lucb:887-900). */
 void lr_renderer_destroy(lr_renderer *renderer);
 
+/* ---- Batches: many renders in one wavefront ------------------------------------------
+ * No counterpart in the reference, which renders one scene per Renderer. A batch is a
+ * pool of paths shared by its members (a member: an uploaded scene seen through one
+ * camera into its own film, with its own RenderSettings). Every pass traces one sample
+ * for as many members' pixels as the pool holds, all in the same kernel launches; each
+ * member's image is bit for bit the image an lr_renderer of the same scene, frame and
+ * settings makes, whatever else shares the batch. Members may join and leave between
+ * passes. All calls on one batch from one host thread. */
+typedef struct {
+    uint32_t pool;        /* paths per pass (at most 4,194,304) */
+    uint32_t max_bounces; /* the most bounces any member may ask for */
+    uint32_t capacity;    /* the most members at once */
+    int32_t profile;      /* as lr_settings.profile */
+} lr_batch_settings;
+typedef struct lr_batch lr_batch;
+
+/* pool 2^21, max_bounces 12, capacity 256, profile 0. */
+void lr_batch_settings_default(lr_batch_settings *out);
+int lr_batch_create(lr_context *ctx, const lr_batch_settings *settings, lr_batch **out);
+/* Adds `scene` (uploaded as `gpu_scene` through the batch's context; both stay the
+ * caller's and must outlive the member) with `settings`, seen through `frame` or, when
+ * it is NULL, through the camera settings name. *member: its index. */
+int lr_batch_add(lr_batch *batch, const lr_gpu_scene *gpu_scene, const lr_scene *scene,
+                 const lr_settings *settings, const lr_frame *frame, uint32_t *member);
+/* The member plans no more passes; its memory goes when its passes in flight finish. */
+int lr_batch_remove(lr_batch *batch, uint32_t member);
+/* Queues the next pass without waiting (two in flight at most); *more is 1 while
+ * passes are running or any member has samples to come. */
+int lr_batch_advance(lr_batch *batch, int32_t *more);
+/* Runs every remaining pass and waits. */
+int lr_batch_finish(lr_batch *batch);
+/* Samples finished, samples planned so far and samples asked for. Any may be NULL. */
+int lr_batch_member_info(const lr_batch *batch, uint32_t member, uint32_t *samples_done,
+                         uint32_t *samples_planned, uint32_t *samples);
+int lr_batch_set_samples(lr_batch *batch, uint32_t member, uint32_t samples);
+/* As lr_renderer_image / lr_renderer_read, for one member. */
+int lr_batch_image(lr_batch *batch, uint32_t member, void **device_rgba);
+int lr_batch_read(lr_batch *batch, uint32_t member, float *rgba, uint64_t float_count);
+int lr_batch_passes(const lr_batch *batch, uint64_t *recorded, uint64_t *finished);
+int lr_batch_kernel_times(lr_batch *batch, double out[10]);
+int lr_batch_stats(lr_batch *batch, lr_render_stats *out);
+void lr_batch_destroy(lr_batch *batch);
+
 #if defined(__GNUC__)
 #pragma GCC visibility pop
 #endif

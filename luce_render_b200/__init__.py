@@ -172,6 +172,21 @@ class RenderStats(C.Structure):
 
 # ---- signatures ---------------------------------------------------------------------------
 
+class BatchSettings(C.Structure):
+    """lr_batch_settings: paths a pass, the most bounces a member may ask for, the most
+    members at once, profiling."""
+    _fields_ = [("pool", C.c_uint32), ("max_bounces", C.c_uint32), ("capacity", C.c_uint32),
+                ("profile", C.c_int32)]
+
+    @staticmethod
+    def default(**overrides) -> "BatchSettings":
+        b = BatchSettings()
+        lib.lr_batch_settings_default(C.byref(b))
+        for key, value in overrides.items():
+            setattr(b, key, value)
+        return b
+
+
 _vp, _i32, _u32, _u64, _sz = C.c_void_p, C.c_int32, C.c_uint32, C.c_uint64, C.c_size_t
 _SIGNATURES = {
     "lr_last_error": (C.c_char_p, []),
@@ -222,6 +237,21 @@ _SIGNATURES = {
     "lr_renderer_kernel_times": (C.c_int, [_vp, C.POINTER(C.c_double)]),
     "lr_renderer_stats": (C.c_int, [_vp, C.POINTER(RenderStats)]),
     "lr_renderer_destroy": (None, [_vp]),
+    "lr_batch_settings_default": (None, [C.POINTER(BatchSettings)]),
+    "lr_batch_create": (C.c_int, [_vp, C.POINTER(BatchSettings), C.POINTER(_vp)]),
+    "lr_batch_add": (C.c_int, [_vp, _vp, _vp, C.POINTER(Settings), C.POINTER(Frame), C.POINTER(C.c_uint32)]),
+    "lr_batch_remove": (C.c_int, [_vp, _u32]),
+    "lr_batch_advance": (C.c_int, [_vp, C.POINTER(_i32)]),
+    "lr_batch_finish": (C.c_int, [_vp]),
+    "lr_batch_member_info": (C.c_int, [_vp, _u32, C.POINTER(C.c_uint32), C.POINTER(C.c_uint32),
+                                       C.POINTER(C.c_uint32)]),
+    "lr_batch_set_samples": (C.c_int, [_vp, _u32, _u32]),
+    "lr_batch_image": (C.c_int, [_vp, _u32, C.POINTER(_vp)]),
+    "lr_batch_read": (C.c_int, [_vp, _u32, C.POINTER(C.c_float), _u64]),
+    "lr_batch_passes": (C.c_int, [_vp, C.POINTER(C.c_uint64), C.POINTER(C.c_uint64)]),
+    "lr_batch_kernel_times": (C.c_int, [_vp, C.POINTER(C.c_double)]),
+    "lr_batch_stats": (C.c_int, [_vp, C.POINTER(RenderStats)]),
+    "lr_batch_destroy": (None, [_vp]),
 }
 
 for _name, (_res, _args) in _SIGNATURES.items():
@@ -707,6 +737,100 @@ class Renderer:
     def destroy(self) -> None:
         if self.handle:
             lib.lr_renderer_destroy(self.handle)
+            self.handle = None
+
+    close = destroy
+
+    def __del__(self):
+        try:
+            self.destroy()
+        except Exception:
+            pass
+
+
+class Batch:
+    """Many renders in one wavefront (lr_batch): members join with a GPU scene, the
+    compiled scene it came from, RenderSettings and an optional frame, and each comes out
+    as the image a Renderer of its own would make."""
+
+    def __init__(self, ctx: Context, settings: BatchSettings | None = None):
+        self.ctx = ctx
+        self.handle = None
+        self.sizes = {}
+        h = _vp()
+        _check(lib.lr_batch_create(ctx.handle, C.byref(settings or BatchSettings.default()), C.byref(h)))
+        self.handle = h
+
+    def add(self, gpu_scene: GpuScene, scene: CompiledScene, settings: RenderSettings,
+            frame: Frame | None = None) -> int:
+        member = C.c_uint32()
+        _check(lib.lr_batch_add(self.handle, gpu_scene.handle, scene.handle, C.byref(settings.c),
+                                C.byref(frame) if frame is not None else None, C.byref(member)))
+        if frame is not None:
+            self.sizes[member.value] = (int(frame.height), int(frame.width))
+        else:
+            self.sizes[member.value] = (int(settings.c.height), int(settings.c.width))
+        return int(member.value)
+
+    def remove(self, member: int) -> None:
+        _check(lib.lr_batch_remove(self.handle, member))
+        self.sizes.pop(member, None)
+
+    def advance(self) -> bool:
+        more = C.c_int32()
+        _check(lib.lr_batch_advance(self.handle, C.byref(more)))
+        return bool(more.value)
+
+    def finish(self) -> None:
+        _check(lib.lr_batch_finish(self.handle))
+
+    def info(self, member: int):
+        """(samples done, samples planned, samples asked for)."""
+        d, p, n = C.c_uint32(), C.c_uint32(), C.c_uint32()
+        _check(lib.lr_batch_member_info(self.handle, member, C.byref(d), C.byref(p), C.byref(n)))
+        return int(d.value), int(p.value), int(n.value)
+
+    def samples_done(self, member: int) -> int:
+        return self.info(member)[0]
+
+    def set_samples(self, member: int, samples: int) -> None:
+        _check(lib.lr_batch_set_samples(self.handle, member, samples))
+
+    def passes(self):
+        rec, fin = C.c_uint64(), C.c_uint64()
+        _check(lib.lr_batch_passes(self.handle, C.byref(rec), C.byref(fin)))
+        return int(rec.value), int(fin.value)
+
+    def image(self, member: int) -> int:
+        p = _vp()
+        _check(lib.lr_batch_image(self.handle, member, C.byref(p)))
+        return p.value
+
+    def read(self, member: int) -> np.ndarray:
+        h, w = self.sizes[member]
+        out = np.empty((h, w, 4), np.float32)
+        _check(lib.lr_batch_read(self.handle, member, _fptr(out), out.size))
+        return out
+
+    def read_into(self, member: int, out: np.ndarray) -> np.ndarray:
+        if out.dtype != np.float32 or not out.flags.c_contiguous:
+            raise RenderError(INVALID, "reading the image needs four floats a pixel")
+        _check(lib.lr_batch_read(self.handle, member, _fptr(out), out.size))
+        return out
+
+    def kernel_times(self) -> np.ndarray:
+        out = (C.c_double * 10)()
+        _check(lib.lr_batch_kernel_times(self.handle, out))
+        return np.array(out[:])
+
+    def stats(self) -> RenderStats:
+        s = RenderStats()
+        _check(lib.lr_batch_stats(self.handle, C.byref(s)))
+        return s
+
+    def destroy(self) -> None:
+        if self.handle:
+            lib.lr_batch_destroy(self.handle)
             self.handle = None
 
     close = destroy

@@ -1,18 +1,32 @@
 // The wavefront path tracer (src/render/integrator.lucb, shaders/camera.comp,
 // intersect_closest.comp, shade_surface.comp, shade_miss.comp, intersect_shadow.comp,
-// finish.comp, film_convert.comp) on sm_100a.
+// finish.comp, film_convert.comp) on sm_100a, for one scene or many at once.
 //
-// A pass traces one sample for one band of at most `pool` pixels:
-//   begin -> camera -> (closest -> shade -> shadow) x (max_bounces + 1) -> finish -> convert
-// Rays live in two ping-pong queues of structure-of-arrays float4 records (origin + path
-// id, direction + t_max) that the traversal kernel reads with coalesced 128-bit loads;
-// hits are written at the ray's queue index. The shade kernel takes every queue entry
-// -- surface hit, light hit or miss (shade_surface + shade_miss of the reference) --
-// and pushes surviving paths' next rays and shadow rays into compact queues with one
-// atomic per warp. Queue sizes never leave the device: every kernel is a persistent
-// grid-stride loop over the count its producer left, so the whole pass is one CUDA
-// graph whose begin kernel derives the band and sample from a device pass counter.
+// A wave is a pool of paths shared by its members (a member: one scene seen through one
+// camera into one film). Each pass traces one sample for a set of segments -- a segment
+// is a range of one member's pixels at one sample index -- laid end to end in the pool:
+//   camera -> (closest -> shade -> shadow) x rounds -> finish -> convert
+// The host plans the segments of every pass and copies the plan (a few hundred bytes)
+// ahead of it on the stream; the pass itself is one CUDA graph per traversal variant.
+// Rays live in two ping-pong queues of structure-of-arrays float4 records (origin + tag,
+// direction + t_max) that the traversal kernels read with coalesced 128-bit loads; the
+// tag holds the path's pool index and its segment, so a ray finds its scene with one
+// lookup. The shade kernel takes every queue entry -- surface hit, light hit or miss
+// (shade_surface + shade_miss of the reference) -- and pushes surviving paths' next rays
+// and shadow rays into compact queues with one atomic per warp. Queue sizes never leave
+// the device: every kernel is a persistent grid-stride loop over the count its producer
+// left.
+//
+// Every path's arithmetic depends only on its member, pixel and sample, and a pixel gets
+// its samples in order, one per pass at most, so an image comes out bit for bit the same
+// whichever members share the wave with it and however the pool splits its pixels.
+//
+// lr_renderer (Renderer of the reference) is a wave with one member whose segments are
+// the reference's bands; lr_batch is a wave of many members that come and go.
 #include <algorithm>
+#include <cstddef>
+#include <deque>
+#include <map>
 #include <memory>
 #include <vector>
 
@@ -28,25 +42,54 @@ constexpr int kTraceBlock = 128;
 constexpr int kShadeBlock = 128;
 constexpr uint32_t kMaterialStride = 16;  // vec4 rows per material (openpbr.glsl:28)
 constexpr size_t kDefaultPool = 2097152;  // 2^21 paths (integrator.lucb:98)
+// A ray's tag: the path's pool index in the low bits, its segment in the high bits.
+constexpr uint32_t kPathBits = 22;
+constexpr uint32_t kPathMask = (1u << kPathBits) - 1u;
+constexpr uint32_t kMaxPool = 1u << kPathBits;             // 4,194,304 paths
+constexpr uint32_t kMaxSegments = 1u << (32 - kPathBits);  // 1,024 segments a pass
 
-struct PassState {
-    uint32_t band_start, band_count, sample, convert;
-};
-
-// Everything a pass's kernels read: passed by value, fixed for the renderer's life.
-struct View {
+// One member of a wave: everything its paths read, fixed while it is a member.
+struct Member {
     DeviceScene scene;
     const float4 *lights;
     uint32_t light_count;
+    uint32_t spectral;
     TreeView tree;
     const float4 *materials;
     const Constants *k;
     float frame[16];
     float lens_radius, focus_distance;
     float forward[3];
-    uint32_t width, height, pool, bands, rounds;
+    uint32_t width, height;
     uint64_t pixels;
-    // path state, one slot per path of the band
+    float4 *film, *image;
+};
+
+// `count` pixels of member `member` from `first_pixel`, at sample `sample`, in pool
+// paths path_base .. path_base + count. `convert`: this segment ends the member's
+// sample, so its image is brought up to date after the pass.
+struct Segment {
+    uint32_t member, first_pixel, count, sample;
+    uint32_t path_base, convert, reserved0, reserved1;
+};
+
+struct PlanHeader {
+    uint32_t segments, paths, converts, reserved;
+};
+
+// A pass's plan: its segments, and the members whose images it brings up to date.
+struct Plan {
+    PlanHeader head;
+    uint32_t convert[kMaxSegments];
+    Segment seg[kMaxSegments];
+};
+
+// What a pass's kernels read besides the members: passed by value, fixed for the wave.
+struct Wave {
+    const Member *members;
+    const Plan *plan;
+    uint32_t pool, rounds;
+    // path state, one slot per pool path
     float4 *throughput, *radiance, *lambda, *vertex;  // vertex: last scattering point, w survival scale
     uint4 *path;                                      // pixel, bounces, previous normal, ray pdf bits
     // ray queues (ping-pong by round) and their hits
@@ -54,10 +97,7 @@ struct View {
     float4 *shadow_o, *shadow_d, *shadow_c;
     // counters[r]: rays of round r; counters[rounds + 1 + r]: shadow rays of round r
     uint32_t *counters;
-    PassState *pass;
-    unsigned long long *pass_counter;
-    float4 *film, *image;
-    unsigned long long *stats;  // closest rays, shadow rays, shaded, passes
+    unsigned long long *stats;  // closest rays, shadow rays, paths, passes, then traversal work
     int *status;
 };
 
@@ -72,114 +112,129 @@ __device__ __forceinline__ uint32_t warp_push(uint32_t *counter, bool want) {
     return base + (uint32_t)__popc(mask & ((1u << lane) - 1u));
 }
 
-__global__ void begin_kernel(View v) {
-    if (threadIdx.x == 0) {
-        const unsigned long long p = *v.pass_counter;
-        const uint32_t band = (uint32_t)(p % v.bands);
-        PassState s;
-        s.sample = (uint32_t)(p / v.bands);
-        const uint64_t start = (uint64_t)band * v.pool;
-        s.band_start = (uint32_t)start;
-        s.band_count = (uint32_t)min((uint64_t)v.pool, v.pixels - start);
-        s.convert = band + 1 == v.bands ? 1u : 0u;
-        *v.pass = s;
-        *v.pass_counter = p + 1;
+// The segment holding pool path `path` (segments lie end to end from path 0).
+__device__ __forceinline__ uint32_t segment_of(const Plan *plan, uint32_t path) {
+    uint32_t lo = 0, hi = plan->head.segments;
+    while (hi - lo > 1u) {
+        const uint32_t mid = (lo + hi) >> 1;
+        if (plan->seg[mid].path_base <= path) lo = mid;
+        else hi = mid;
     }
-    for (uint32_t i = threadIdx.x; i < 4 * v.rounds + 2; i += blockDim.x) v.counters[i] = 0;
+    return lo;
 }
 
-// camera.comp:14-50: a jittered primary ray per pixel of the band.
-template <bool kSpectral>
-__global__ void __launch_bounds__(kShadeBlock) camera_kernel(View v) {
-    const PassState ps = *v.pass;
-    const Constants *k = v.k;
-    const uint32_t seed = k->seed;
-    const float3 position = make_float3(v.frame[0], v.frame[1], v.frame[2]);
-    const float3 corner = make_float3(v.frame[4], v.frame[5], v.frame[6]);
-    const float3 du = make_float3(v.frame[8], v.frame[9], v.frame[10]);
-    const float3 dv = make_float3(v.frame[12], v.frame[13], v.frame[14]);
-    const bool ortho = v.frame[3] > 0.5f;
+__device__ __forceinline__ const Member &member_of_tag(const Wave &w, uint32_t tag) {
+    return w.members[w.plan->seg[tag >> kPathBits].member];
+}
+
+// camera.comp:14-50: a jittered primary ray per pixel of every segment. Block 0 also
+// starts the pass's queue counters.
+__global__ void __launch_bounds__(kShadeBlock) camera_kernel(Wave w) {
+    const Plan *plan = w.plan;
+    const uint32_t paths = plan->head.paths;
+    if (blockIdx.x == 0) {
+        for (uint32_t i = threadIdx.x; i < 4 * w.rounds + 2; i += blockDim.x) w.counters[i] = i == 0 ? paths : 0u;
+    }
     const uint32_t stride = gridDim.x * blockDim.x;
-    for (uint32_t path = blockIdx.x * blockDim.x + threadIdx.x; path < ps.band_count; path += stride) {
-        const uint32_t pixel = ps.band_start + path;
-        const float4 u = sample4(seed, pixel, ps.sample, kGroupCamera);
-        const float fx = (float)(pixel % v.width) + u.x, fy = (float)(pixel / v.width) + u.y;
+    for (uint32_t path = blockIdx.x * blockDim.x + threadIdx.x; path < paths; path += stride) {
+        const uint32_t si = segment_of(plan, path);
+        const Segment &sg = plan->seg[si];
+        const Member &m = w.members[sg.member];
+        const uint32_t pixel = sg.first_pixel + (path - sg.path_base);
+        const uint32_t sample = sg.sample;
+        const uint32_t seed = m.k->seed;
+        const float3 position = make_float3(m.frame[0], m.frame[1], m.frame[2]);
+        const float3 corner = make_float3(m.frame[4], m.frame[5], m.frame[6]);
+        const float3 du = make_float3(m.frame[8], m.frame[9], m.frame[10]);
+        const float3 dv = make_float3(m.frame[12], m.frame[13], m.frame[14]);
+        const bool ortho = m.frame[3] > 0.5f;
+        const float4 u = sample4(seed, pixel, sample, kGroupCamera);
+        const float fx = (float)(pixel % m.width) + u.x, fy = (float)(pixel / m.width) + u.y;
         const float3 film = corner + fx * du + fy * dv;
         float3 origin = ortho ? position + film : position;
         float3 direction = normalize(ortho ? cross(du, dv) : film);
-        if (!ortho && v.lens_radius > 0.0f) {
-            const float3 forward = make_float3(v.forward[0], v.forward[1], v.forward[2]);
-            const float3 focused = position + direction * (v.focus_distance / dot(direction, forward));
+        if (!ortho && m.lens_radius > 0.0f) {
+            const float3 forward = make_float3(m.forward[0], m.forward[1], m.forward[2]);
+            const float3 focused = position + direction * (m.focus_distance / dot(direction, forward));
             const float2 disk = concentric(make_float2(u.z, u.w));
-            origin = position + normalize(du) * (disk.x * v.lens_radius) + normalize(dv) * (disk.y * v.lens_radius);
+            origin = position + normalize(du) * (disk.x * m.lens_radius) + normalize(dv) * (disk.y * m.lens_radius);
             direction = normalize(focused - origin);
         }
-        v.path[path] = make_uint4(pixel, 0u, 0u, 0u);
-        v.throughput[path] = make_float4(1.0f, 1.0f, 1.0f, 1.0f);
-        v.radiance[path] = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
-        v.vertex[path] = make_float4(origin.x, origin.y, origin.z, 1.0f);
-        if (kSpectral) v.lambda[path] = sample_wavelengths(sample4(seed, pixel, ps.sample, kGroupWavelength).x);
-        v.ray_o[0][path] = make_float4(origin.x, origin.y, origin.z, __uint_as_float(path));
-        v.ray_d[0][path] = make_float4(direction.x, direction.y, direction.z, kInfinity);
+        w.path[path] = make_uint4(pixel, 0u, 0u, 0u);
+        w.throughput[path] = make_float4(1.0f, 1.0f, 1.0f, 1.0f);
+        w.radiance[path] = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
+        w.vertex[path] = make_float4(origin.x, origin.y, origin.z, 1.0f);
+        if (m.spectral) w.lambda[path] = sample_wavelengths(sample4(seed, pixel, sample, kGroupWavelength).x);
+        w.ray_o[0][path] = make_float4(origin.x, origin.y, origin.z, __uint_as_float(path | (si << kPathBits)));
+        w.ray_d[0][path] = make_float4(direction.x, direction.y, direction.z, kInfinity);
     }
-    if (blockIdx.x == 0 && threadIdx.x == 0) v.counters[0] = ps.band_count;
 }
 
 // intersect_closest.comp:45-76: the nearest triangle, then the analytic lights
-// before it (camera rays skip lights invisible to the camera).
+// before it (camera rays skip lights invisible to the camera). The grid-stride walk
+// hands each warp 32 neighbouring queue entries at a time (neighbouring primary rays,
+// or rays a shading warp pushed together), which keeps its lanes on similar nodes.
 template <int W, int kStack, bool kCount>
-__global__ void __launch_bounds__(kTraceBlock) closest_kernel(View v, uint32_t round) {
+__global__ void __launch_bounds__(kTraceBlock) closest_kernel(Wave w, uint32_t round) {
     __shared__ int stack[TracerOf<W, false, kStack, kCount>::kInts * kTraceBlock];
     const uint32_t q = round & 1u;
-    const uint32_t count = v.counters[round];
+    const uint32_t count = w.counters[round];
     bool overflow = false;
     Visits visits;
-    const float4 *ray_o = v.ray_o[q], *ray_d = v.ray_d[q];
-    float4 *hits = v.hits[q];
-    auto load = [&](uint32_t i) {
+    const float4 *ray_o = w.ray_o[q], *ray_d = w.ray_d[q];
+    float4 *hits = w.hits[q];
+    typename TracerOf<W, false, kStack, kCount>::type tr(stack + threadIdx.x, kTraceBlock);
+    const uint32_t step = gridDim.x * blockDim.x;
+    for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < count; i += step) {
         const float4 o = ray_o[i], d = ray_d[i];
-        return Ray{xyz(o), 0.0f, xyz(d), d.w};
-    };
-    auto store = [&](uint32_t i, const Hit &h, const Ray &r) {
-        uint32_t what = h.slot >= 0 ? (uint32_t)h.slot : kNone;
-        float t = h.t;
-        for (uint32_t light = 0; light < v.light_count; light++) {
-            if (round == 0 && !light_visible(v.lights, light)) continue;
-            const float tl = intersect_light(v.lights, light, r.o, r.d, t);
+        const Member &m = member_of_tag(w, __float_as_uint(o.w));
+        const DeviceScene s = m.scene;
+        if (tr.start(s, Ray{xyz(o), 0.0f, xyz(d), d.w})) {
+            while (!tr.step(s, overflow, visits)) {
+            }
+        }
+        uint32_t what = tr.h.slot >= 0 ? (uint32_t)tr.h.slot : kNone;
+        float t = tr.h.t;
+        const float4 *lights = m.lights;
+        const uint32_t light_count = m.light_count;
+        for (uint32_t light = 0; light < light_count; light++) {
+            if (round == 0 && !light_visible(lights, light)) continue;
+            const float tl = intersect_light(lights, light, tr.r.o, tr.r.d, t);
             if (tl < t) {
                 t = tl;
                 what = kLightHit | light;
             }
         }
-        hits[i] = make_float4(t, __uint_as_float(what), h.u, h.v);
-    };
-    trace_strided<W, false, kStack, kCount>(v.scene, count, stack + threadIdx.x, kTraceBlock, load, store, overflow,
-                                         visits);
-    if (overflow) atomicAdd(&v.status[0], 1);
-    if (kCount) add_visits(&v.stats[4], visits);
+        hits[i] = make_float4(t, __uint_as_float(what), tr.h.u, tr.h.v);
+    }
+    if (overflow) atomicAdd(&w.status[0], 1);
+    if (kCount) add_visits(&w.stats[4], visits);
 }
 
 // intersect_shadow.comp:51-92: unblocked light samples join their path's radiance.
 template <int W, int kStack, bool kCount>
-__global__ void __launch_bounds__(kTraceBlock) shadow_kernel(View v, uint32_t round) {
+__global__ void __launch_bounds__(kTraceBlock) shadow_kernel(Wave w, uint32_t round) {
     __shared__ int stack[TracerOf<W, true, kStack, kCount>::kInts * kTraceBlock];
-    const uint32_t count = v.counters[v.rounds + 1 + round];
+    const uint32_t count = w.counters[w.rounds + 1 + round];
     bool overflow = false;
     Visits visits;
-    auto load = [&](uint32_t i) {
-        const float4 o = v.shadow_o[i], d = v.shadow_d[i];
-        return Ray{xyz(o), 0.0f, xyz(d), d.w};
-    };
-    auto store = [&](uint32_t i, const Hit &h, const Ray &) {
-        if (h.id < 0) {
-            const uint32_t path = __float_as_uint(v.shadow_o[i].w);
-            v.radiance[path] = v.radiance[path] + v.shadow_c[i];
+    typename TracerOf<W, true, kStack, kCount>::type tr(stack + threadIdx.x, kTraceBlock);
+    const uint32_t step = gridDim.x * blockDim.x;
+    for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < count; i += step) {
+        const float4 o = w.shadow_o[i], d = w.shadow_d[i];
+        const uint32_t tag = __float_as_uint(o.w);
+        const DeviceScene s = member_of_tag(w, tag).scene;
+        if (tr.start(s, Ray{xyz(o), 0.0f, xyz(d), d.w})) {
+            while (!tr.step(s, overflow, visits)) {
+            }
         }
-    };
-    trace_strided<W, true, kStack, kCount>(v.scene, count, stack + threadIdx.x, kTraceBlock, load, store, overflow,
-                                        visits);
-    if (overflow) atomicAdd(&v.status[0], 1);
-    if (kCount) add_visits(&v.stats[6], visits);
+        if (tr.h.id < 0) {
+            const uint32_t path = tag & kPathMask;
+            w.radiance[path] = w.radiance[path] + w.shadow_c[i];
+        }
+    }
+    if (overflow) atomicAdd(&w.status[0], 1);
+    if (kCount) add_visits(&w.stats[6], visits);
 }
 
 template <bool kSpectral>
@@ -189,19 +244,19 @@ __device__ __forceinline__ float4 clamped(float4 c, uint32_t total, float clamp_
     return largest > clamp_value ? c * (clamp_value / largest) : c;
 }
 
-__device__ __forceinline__ float4 material_at(const View &v, uint32_t m, uint32_t row) {
-    return __ldg(&v.materials[m * kMaterialStride + row]);
+__device__ __forceinline__ float4 material_at(const Member &m, uint32_t material, uint32_t row) {
+    return __ldg(&m.materials[material * kMaterialStride + row]);
 }
 
-__device__ __forceinline__ float3 position_of(const View &v, uint32_t index) {
-    return make_float3(__ldg(&v.scene.positions[index * 3]), __ldg(&v.scene.positions[index * 3 + 1]),
-                       __ldg(&v.scene.positions[index * 3 + 2]));
+__device__ __forceinline__ float3 position_of(const Member &m, uint32_t index) {
+    return make_float3(__ldg(&m.scene.positions[index * 3]), __ldg(&m.scene.positions[index * 3 + 1]),
+                       __ldg(&m.scene.positions[index * 3 + 2]));
 }
 
 // triangle_hit_pdf (lighttree.glsl:131-137)
-__device__ __forceinline__ float triangle_hit_pdf(const View &v, uint32_t slot, float3 d, float t) {
-    const float3 a = position_of(v, v.scene.indices[slot * 3]);
-    const float3 cr = cross(position_of(v, v.scene.indices[slot * 3 + 1]) - a, position_of(v, v.scene.indices[slot * 3 + 2]) - a);
+__device__ __forceinline__ float triangle_hit_pdf(const Member &m, uint32_t slot, float3 d, float t) {
+    const float3 a = position_of(m, m.scene.indices[slot * 3]);
+    const float3 cr = cross(position_of(m, m.scene.indices[slot * 3 + 1]) - a, position_of(m, m.scene.indices[slot * 3 + 2]) - a);
     const float area = 0.5f * length(cr);
     const float cos_light = fabsf(dot(d, cr)) / fmaxf(1e-20f, 2.0f * area);
     return t * t / fmaxf(1e-20f, cos_light * area);
@@ -209,11 +264,11 @@ __device__ __forceinline__ float triangle_hit_pdf(const View &v, uint32_t slot, 
 
 // sample_triangle (lighttree.glsl:107-128)
 template <bool kSpectral>
-__device__ __forceinline__ bool sample_triangle(const View &v, uint32_t slot, float3 p, float2 u, float4 lambda,
+__device__ __forceinline__ bool sample_triangle(const Member &m, uint32_t slot, float3 p, float2 u, float4 lambda,
                                                 LightSample &s, float4 &radiance) {
-    const float3 a = position_of(v, v.scene.indices[slot * 3]);
-    const float3 b = position_of(v, v.scene.indices[slot * 3 + 1]);
-    const float3 c = position_of(v, v.scene.indices[slot * 3 + 2]);
+    const float3 a = position_of(m, m.scene.indices[slot * 3]);
+    const float3 b = position_of(m, m.scene.indices[slot * 3 + 1]);
+    const float3 c = position_of(m, m.scene.indices[slot * 3 + 2]);
     const float r = sqrtf(u.x);
     const float3 q = a * (1.0f - r) + b * (r * (1.0f - u.y)) + c * (r * u.y);
     const float3 cr = cross(b - a, c - a);
@@ -228,8 +283,8 @@ __device__ __forceinline__ bool sample_triangle(const View &v, uint32_t slot, fl
     s.pdf = d2 / (cos_light * area);
     s.cos_light = cos_light;
     s.delta = false;
-    const uint32_t m = __ldg(&v.scene.shading[slot]).w;
-    radiance = spec_of<kSpectral>(material_at(v, m, 6), xyz(material_at(v, m, 7)), lambda);
+    const uint32_t material = __ldg(&m.scene.shading[slot]).w;
+    radiance = spec_of<kSpectral>(material_at(m, material, 6), xyz(material_at(m, material, 7)), lambda);
     return true;
 }
 
@@ -245,87 +300,90 @@ __device__ __forceinline__ float rgb_luminance(float3 c) {
 // One queue entry: a miss (shade_miss.comp:12-51), a light hit or a surface hit
 // (shade_surface.comp:48-312 at the Lambertian settings).
 template <bool kSpectral>
-__device__ __forceinline__ void shade_one(const View &v, const Constants &k, const PassState &ps, uint32_t round,
-                                          uint32_t i, ShadeOut &out) {
+__device__ __forceinline__ void shade_one(const Wave &w, const Member &m, uint32_t sample, uint32_t round, uint32_t i,
+                                          float4 ro, ShadeOut &out) {
+    const Constants &k = *m.k;
     const uint32_t q = round & 1u;
-    const float4 ro = v.ray_o[q][i], rd = v.ray_d[q][i], hit = v.hits[q][i];
-    const uint32_t path = __float_as_uint(ro.w);
-    uint4 pu = v.path[path];
+    const float4 rd = w.ray_d[q][i], hit = w.hits[q][i];
+    const uint32_t tag = __float_as_uint(ro.w);
+    const uint32_t path = tag & kPathMask;
+    uint4 pu = w.path[path];
     const uint32_t pixel = pu.x, bounces = pu.y, total = bounces & 0xffu;
     const float ray_pdf = __uint_as_float(pu.w);
     const float3 origin = xyz(ro), dir = xyz(rd);
-    float4 throughput = v.throughput[path];
-    const float4 lambda = kSpectral ? v.lambda[path] : make_float4(0.0f, 0.0f, 0.0f, 0.0f);
+    float4 throughput = w.throughput[path];
+    const float4 lambda = kSpectral ? w.lambda[path] : make_float4(0.0f, 0.0f, 0.0f, 0.0f);
     const uint32_t what = __float_as_uint(hit.y);
     const float t = hit.x;
-    float4 radiance = v.radiance[path];
+    float4 radiance = w.radiance[path];
+    const float4 *lights = m.lights;
 
     if (what == kNone) {
         float4 r = spec_of<kSpectral>(k.background_fit, k.background_rgb, lambda);
-        for (uint32_t light = 0; light < v.light_count; light++) {
-            const uint32_t type = light_type(v.lights, light);
+        for (uint32_t light = 0; light < m.light_count; light++) {
+            const uint32_t type = light_type(lights, light);
             if (type < kLightDistant) continue;
-            const float cos_half = light_at(v.lights, light, 2).w;
-            if (cos_half >= 1.0f - 1e-7f || dot(dir, -xyz(light_at(v.lights, light, 3))) < cos_half) continue;
+            const float cos_half = light_at(lights, light, 2).w;
+            if (cos_half >= 1.0f - 1e-7f || dot(dir, -xyz(light_at(lights, light, 3))) < cos_half) continue;
             float weight = 1.0f;
             if (total == 0u) {
-                if (!light_visible(v.lights, light)) continue;
+                if (!light_visible(lights, light)) continue;
             } else if (ray_pdf > 0.0f) {
-                const float select = k.p_distant * light_at(v.lights, light, 6).y;
-                weight = mis_weight(light_hit_pdf(v.lights, light, make_float3(0.0f, 0.0f, 0.0f), dir, kInfinity) *
+                const float select = k.p_distant * light_at(lights, light, 6).y;
+                weight = mis_weight(light_hit_pdf(lights, light, make_float3(0.0f, 0.0f, 0.0f), dir, kInfinity) *
                                         select / ray_pdf, 0.0f);
             }
-            r = r + light_radiance<kSpectral>(v.lights, light, lambda) * weight;
+            r = r + light_radiance<kSpectral>(lights, light, lambda) * weight;
         }
         float4 contribution = throughput * r;
         const float largest = spec_max<kSpectral>(contribution);
         if (total > 0u && k.clamp_indirect > 0.0f && largest > k.clamp_indirect)
             contribution = contribution * (k.clamp_indirect / largest);
-        v.radiance[path] = radiance + contribution;
+        w.radiance[path] = radiance + contribution;
         return;
     }
-    const float4 vertex_row = v.vertex[path];
+    const float4 vertex_row = w.vertex[path];
     const float3 vertex = xyz(vertex_row);
     if (what & kLightHit) {
         const uint32_t light = what & ~kLightHit;
         float weight = 1.0f;
         if (total == 0u) {
-            if (!light_visible(v.lights, light)) return;
+            if (!light_visible(lights, light)) return;
         } else if (ray_pdf > 0.0f) {
-            const uint32_t emitter = (uint32_t)light_at(v.lights, light, 6).w;
+            const uint32_t emitter = (uint32_t)light_at(lights, light, 6).w;
             const float reach = length(vertex - (origin + t * dir));
-            const float chance = (1.0f - k.p_distant) * tree_pdf(v.tree, emitter, vertex, octahedral_decode(pu.z));
-            weight = mis_weight(light_hit_pdf(v.lights, light, vertex, dir, reach) * chance / ray_pdf, 0.0f);
+            const float chance = (1.0f - k.p_distant) * tree_pdf(m.tree, emitter, vertex, octahedral_decode(pu.z));
+            weight = mis_weight(light_hit_pdf(lights, light, vertex, dir, reach) * chance / ray_pdf, 0.0f);
         }
-        v.radiance[path] = radiance + clamped<kSpectral>(throughput * light_radiance<kSpectral>(v.lights, light, lambda) * weight,
+        w.radiance[path] = radiance + clamped<kSpectral>(throughput * light_radiance<kSpectral>(lights, light, lambda) * weight,
                                                           total, k.clamp_indirect);
         return;
     }
 
     // A surface.
     const uint32_t slot = what;
-    const float3 p0 = position_of(v, v.scene.indices[slot * 3]);
-    float3 geometric = normalize(cross(position_of(v, v.scene.indices[slot * 3 + 1]) - p0,
-                                       position_of(v, v.scene.indices[slot * 3 + 2]) - p0));
+    const float3 p0 = position_of(m, m.scene.indices[slot * 3]);
+    float3 geometric = normalize(cross(position_of(m, m.scene.indices[slot * 3 + 1]) - p0,
+                                       position_of(m, m.scene.indices[slot * 3 + 2]) - p0));
     if (dot(geometric, dir) > 0.0f) geometric = -geometric;
-    const uint4 attributes = __ldg(&v.scene.shading[slot]);
-    const uint32_t m = attributes.w;
+    const uint4 attributes = __ldg(&m.scene.shading[slot]);
+    const uint32_t material = attributes.w;
     const float3 p = origin + t * dir;
     const float reach = length(vertex - p);
 
-    const float4 emission_row = material_at(v, m, 7);
+    const float4 emission_row = material_at(m, material, 7);
     if (emission_row.w > 0.0f) {
         float weight = 1.0f;
-        const uint32_t emitter = v.tree.triangle_map ? __ldg(&v.tree.triangle_map[slot]) : kNone;
+        const uint32_t emitter = m.tree.triangle_map ? __ldg(&m.tree.triangle_map[slot]) : kNone;
         if (total > 0u && ray_pdf > 0.0f && emitter != kNone) {
-            const float chance = (1.0f - k.p_distant) * tree_pdf(v.tree, emitter, vertex, octahedral_decode(pu.z));
-            weight = mis_weight(triangle_hit_pdf(v, slot, dir, reach) * chance / ray_pdf, 0.0f);
+            const float chance = (1.0f - k.p_distant) * tree_pdf(m.tree, emitter, vertex, octahedral_decode(pu.z));
+            weight = mis_weight(triangle_hit_pdf(m, slot, dir, reach) * chance / ray_pdf, 0.0f);
         }
-        radiance = radiance + clamped<kSpectral>(throughput * spec_of<kSpectral>(material_at(v, m, 6), xyz(emission_row), lambda) * weight,
+        radiance = radiance + clamped<kSpectral>(throughput * spec_of<kSpectral>(material_at(m, material, 6), xyz(emission_row), lambda) * weight,
                                                  total, k.clamp_indirect);
     }
     if (total >= k.max_bounces) {
-        v.radiance[path] = radiance;
+        w.radiance[path] = radiance;
         return;
     }
     const float hu = hit.z, hv = hit.w;
@@ -335,36 +393,36 @@ __device__ __forceinline__ void shade_one(const View &v, const Constants &k, con
     float3 tangent, bitangent;
     basis(normal, tangent, bitangent);
     const float3 wo = make_float3(-dot(dir, tangent), -dot(dir, bitangent), -dot(dir, normal));
-    const float4 base_rgb = material_at(v, m, 1);
-    const float4 base = spec_of<kSpectral>(material_at(v, m, 0), xyz(base_rgb), lambda) * base_rgb.w;
-    const float roughness = material_at(v, m, 10).y;
+    const float4 base_rgb = material_at(m, material, 1);
+    const float4 base = spec_of<kSpectral>(material_at(m, material, 0), xyz(base_rgb), lambda) * base_rgb.w;
+    const float roughness = material_at(m, material, 10).y;
     const float p_diffuse = fmaxf(rgb_luminance(xyz(base_rgb) * base_rgb.w), 0.0f) > 0.0f ? 1.0f : 0.0f;
     const float3 from = offset_origin(p, geometric);
 
     // One light sample: a distant light by power, or an emitter of the light tree.
-    const float4 u_light = sample4(k.seed, pixel, ps.sample, group_light(total));
+    const float4 u_light = sample4(k.seed, pixel, sample, group_light(total));
     LightSample s;
     float4 emitted = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
     float chance = 0.0f;
     bool sampled = false;
     if (u_light.x < k.p_distant) {
         float share;
-        const uint32_t light = pick_distant(v.lights, v.light_count, u_light.x / k.p_distant, share);
-        if (light != kNone && share > 0.0f && sample_light(v.lights, light, p, make_float2(u_light.y, u_light.z), s)) {
+        const uint32_t light = pick_distant(lights, m.light_count, u_light.x / k.p_distant, share);
+        if (light != kNone && share > 0.0f && sample_light(lights, light, p, make_float2(u_light.y, u_light.z), s)) {
             chance = k.p_distant * share;
-            emitted = light_radiance<kSpectral>(v.lights, light, lambda);
+            emitted = light_radiance<kSpectral>(lights, light, lambda);
             sampled = true;
         }
     } else {
         uint32_t emitter;
         float tree_chance;
-        if (tree_sample(v.tree, (u_light.x - k.p_distant) / fmaxf(1e-7f, 1.0f - k.p_distant), from, normal, emitter, tree_chance)) {
+        if (tree_sample(m.tree, (u_light.x - k.p_distant) / fmaxf(1e-7f, 1.0f - k.p_distant), from, normal, emitter, tree_chance)) {
             chance = (1.0f - k.p_distant) * tree_chance;
-            const uint32_t code = __ldg(&v.tree.records[emitter]).x;
+            const uint32_t code = __ldg(&m.tree.records[emitter]).x;
             if (code & kEmitterTriangle) {
-                sampled = sample_triangle<kSpectral>(v, code & ~kEmitterTriangle, p, make_float2(u_light.y, u_light.z), lambda, s, emitted);
-            } else if (sample_light(v.lights, code, p, make_float2(u_light.y, u_light.z), s)) {
-                emitted = light_radiance<kSpectral>(v.lights, code, lambda);
+                sampled = sample_triangle<kSpectral>(m, code & ~kEmitterTriangle, p, make_float2(u_light.y, u_light.z), lambda, s, emitted);
+            } else if (sample_light(lights, code, p, make_float2(u_light.y, u_light.z), s)) {
+                emitted = light_radiance<kSpectral>(lights, code, lambda);
                 sampled = true;
             }
         }
@@ -385,16 +443,16 @@ __device__ __forceinline__ void shade_one(const View &v, const Constants &k, con
                 const float shadow_reach = s.distance >= kInfinity ? kInfinity : fmaxf(0.0f, s.distance - margin);
                 const float3 so = offset_origin(p, geometric);
                 out.shadow = true;
-                out.so = make_float4(so.x, so.y, so.z, __uint_as_float(path));
+                out.so = make_float4(so.x, so.y, so.z, ro.w);
                 out.sd = make_float4(s.direction.x, s.direction.y, s.direction.z, shadow_reach);
                 out.sc = contribution;
             }
         }
     }
-    v.radiance[path] = radiance;
+    w.radiance[path] = radiance;
 
     // One BSDF sample (sample_surface with u.xyw: the lobe pick is u.w).
-    const float4 u = sample4(k.seed, pixel, ps.sample, group_bsdf(total));
+    const float4 u = sample4(k.seed, pixel, sample, group_bsdf(total));
     if (wo.z <= 0.0f || !(u.w < p_diffuse)) return;
     const float2 disk = concentric(make_float2(u.x, u.y));
     const float3 wi = make_float3(disk.x, disk.y, sqrtf(fmaxf(0.0f, 1.0f - (disk.x * disk.x + disk.y * disk.y))));
@@ -415,83 +473,91 @@ __device__ __forceinline__ void shade_one(const View &v, const Constants &k, con
         throughput = make_float4(throughput.x / survive, throughput.y / survive, throughput.z / survive, throughput.w / survive);
     }
     const float3 next = side > 0.0f ? from : offset_origin(p, -geometric);
-    v.path[path] = make_uint4(pixel, next_bounces, octahedral_encode(normal), __float_as_uint(pdf));
-    v.throughput[path] = throughput;
-    v.vertex[path] = make_float4(next.x, next.y, next.z, survival_scale);
+    w.path[path] = make_uint4(pixel, next_bounces, octahedral_encode(normal), __float_as_uint(pdf));
+    w.throughput[path] = throughput;
+    w.vertex[path] = make_float4(next.x, next.y, next.z, survival_scale);
     out.next = true;
-    out.o = make_float4(next.x, next.y, next.z, __uint_as_float(path));
+    out.o = make_float4(next.x, next.y, next.z, ro.w);
     out.d = make_float4(direction.x, direction.y, direction.z, kInfinity);
 }
 
-template <bool kSpectral>
-__global__ void __launch_bounds__(kShadeBlock) shade_kernel(View v, uint32_t round) {
-    const uint32_t count = v.counters[round];
-    const PassState ps = *v.pass;
-    const Constants &k = *v.k;
-    const uint32_t nq = (round & 1u) ^ 1u;
+__global__ void __launch_bounds__(kShadeBlock) shade_kernel(Wave w, uint32_t round) {
+    const uint32_t count = w.counters[round];
+    const uint32_t q = round & 1u, nq = q ^ 1u;
     const uint32_t lane = threadIdx.x & 31u;
     const uint32_t stride = gridDim.x * blockDim.x;
-    uint32_t *next_counter = &v.counters[round + 1];
-    uint32_t *shadow_counter = &v.counters[v.rounds + 1 + round];
+    uint32_t *next_counter = &w.counters[round + 1];
+    uint32_t *shadow_counter = &w.counters[w.rounds + 1 + round];
     for (uint32_t base = blockIdx.x * blockDim.x + (threadIdx.x & ~31u); base < count; base += stride) {
         const uint32_t i = base + lane;
         ShadeOut out;
-        if (i < count) shade_one<kSpectral>(v, k, ps, round, i, out);
+        if (i < count) {
+            const float4 ro = w.ray_o[q][i];
+            const Segment &sg = w.plan->seg[__float_as_uint(ro.w) >> kPathBits];
+            const Member &m = w.members[sg.member];
+            if (m.spectral) shade_one<true>(w, m, sg.sample, round, i, ro, out);
+            else shade_one<false>(w, m, sg.sample, round, i, ro, out);
+        }
         const uint32_t at = warp_push(next_counter, out.next);
         if (out.next) {
-            v.ray_o[nq][at] = out.o;
-            v.ray_d[nq][at] = out.d;
+            w.ray_o[nq][at] = out.o;
+            w.ray_d[nq][at] = out.d;
         }
         const uint32_t sat = warp_push(shadow_counter, out.shadow);
         if (out.shadow) {
-            v.shadow_o[sat] = out.so;
-            v.shadow_d[sat] = out.sd;
-            v.shadow_c[sat] = out.sc;
+            w.shadow_o[sat] = out.so;
+            w.shadow_d[sat] = out.sd;
+            w.shadow_c[sat] = out.sc;
         }
     }
 }
 
-// finish.comp:13-39: each path's radiance into its pixel (one sample per pixel per pass).
-template <bool kSpectral>
-__global__ void __launch_bounds__(kShadeBlock) finish_kernel(View v) {
-    const PassState ps = *v.pass;
-    const Constants &k = *v.k;
+// finish.comp:13-39: each path's radiance into its pixel (one sample per pixel a pass).
+__global__ void __launch_bounds__(kShadeBlock) finish_kernel(Wave w) {
+    const Plan *plan = w.plan;
+    const uint32_t paths = plan->head.paths;
     const uint32_t stride = gridDim.x * blockDim.x;
-    for (uint32_t path = blockIdx.x * blockDim.x + threadIdx.x; path < ps.band_count; path += stride) {
-        const uint32_t pixel = v.path[path].x;
-        float3 value = spec_to_film<kSpectral>(v.radiance[path], kSpectral ? v.lambda[path] : make_float4(0, 0, 0, 0), k);
+    for (uint32_t path = blockIdx.x * blockDim.x + threadIdx.x; path < paths; path += stride) {
+        const Member &m = w.members[plan->seg[segment_of(plan, path)].member];
+        const uint32_t pixel = w.path[path].x;
+        float3 value = m.spectral ? spec_to_film<true>(w.radiance[path], w.lambda[path], *m.k)
+                                  : spec_to_film<false>(w.radiance[path], make_float4(0, 0, 0, 0), *m.k);
         if (!isfinite(value.x) || !isfinite(value.y) || !isfinite(value.z)) value = make_float3(0.0f, 0.0f, 0.0f);
-        const float4 f = v.film[pixel];
-        v.film[pixel] = make_float4(f.x + value.x, f.y + value.y, f.z + value.z, f.w + 1.0f);
+        const float4 f = m.film[pixel];
+        m.film[pixel] = make_float4(f.x + value.x, f.y + value.y, f.z + value.z, f.w + 1.0f);
     }
     if (blockIdx.x == 0 && threadIdx.x == 0) {
         unsigned long long closest = 0, shadow = 0;
-        for (uint32_t r = 0; r < v.rounds; r++) {
-            closest += v.counters[r];
-            shadow += v.counters[v.rounds + 1 + r];
+        for (uint32_t r = 0; r < w.rounds; r++) {
+            closest += w.counters[r];
+            shadow += w.counters[w.rounds + 1 + r];
         }
-        v.stats[0] += closest;
-        v.stats[1] += shadow;
-        v.stats[2] += ps.band_count;
-        v.stats[3] += 1;
+        w.stats[0] += closest;
+        w.stats[1] += shadow;
+        w.stats[2] += paths;
+        w.stats[3] += 1;
     }
 }
 
-// film_convert.comp:36-53: the film's average into the rgba32f ACEScg image.
-template <bool kSpectral>
-__global__ void __launch_bounds__(kShadeBlock) convert_kernel(View v) {
-    if (!v.pass->convert) return;
-    const Constants &k = *v.k;
+// film_convert.comp:36-53: the film's average into the rgba32f ACEScg image, for every
+// member whose sample ended in this pass.
+__global__ void __launch_bounds__(kShadeBlock) convert_kernel(Wave w) {
+    const Plan *plan = w.plan;
+    const uint32_t converts = plan->head.converts;
     const uint64_t stride = (uint64_t)gridDim.x * blockDim.x;
-    for (uint64_t pixel = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; pixel < v.pixels; pixel += stride) {
-        const float4 sum = v.film[pixel];
-        const float w = fmaxf(sum.w, 1.0f);
-        float3 value = make_float3(sum.x / w, sum.y / w, sum.z / w);
-        if (kSpectral)
-            value = make_float3(k.film[0] * value.x + k.film[1] * value.y + k.film[2] * value.z,
-                                k.film[3] * value.x + k.film[4] * value.y + k.film[5] * value.z,
-                                k.film[6] * value.x + k.film[7] * value.y + k.film[8] * value.z);
-        v.image[pixel] = make_float4(value.x, value.y, value.z, 1.0f);
+    for (uint32_t c = 0; c < converts; c++) {
+        const Member &m = w.members[plan->convert[c]];
+        const Constants &k = *m.k;
+        for (uint64_t pixel = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; pixel < m.pixels; pixel += stride) {
+            const float4 sum = m.film[pixel];
+            const float wsum = fmaxf(sum.w, 1.0f);
+            float3 value = make_float3(sum.x / wsum, sum.y / wsum, sum.z / wsum);
+            if (m.spectral)
+                value = make_float3(k.film[0] * value.x + k.film[1] * value.y + k.film[2] * value.z,
+                                    k.film[3] * value.x + k.film[4] * value.y + k.film[5] * value.z,
+                                    k.film[6] * value.x + k.film[7] * value.y + k.film[8] * value.z);
+            m.image[pixel] = make_float4(value.x, value.y, value.z, 1.0f);
+        }
     }
 }
 
@@ -502,48 +568,120 @@ enum Kind { kCamera = 0, kClosest = 1, kSurface = 2, kMiss = 3, kShadow = 4, kLi
 template <typename K>
 int grid_of(K kernel, int block, int sm_count) {
     int per_sm = 0;
-    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kernel, block, 0);
+    LR_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kernel, block, 0));
     return std::max(1, per_sm) * sm_count;
 }
 
 size_t align256(size_t v) { return (v + 255) & ~(size_t)255; }
 
-}  // namespace
-}  // namespace lr
-
-using namespace lr;
-
-struct lr_renderer {
-    lr_context *ctx = nullptr;
-    lr_settings settings{};
-    lr_frame frame{};
-    lr_gpu_scene *gs = nullptr;
-    Loaded loaded;
-    void *block = nullptr;  // one device allocation for everything below the scene
-    View view{};
-    int width = 2, stack = 32;  // the traversal variant (BVH width, stack entries)
-    int grid_trace = 0, grid_shade = 0;
-    cudaGraph_t graph = nullptr;
-    cudaGraphExec_t exec = nullptr;
-    // passes: recorded, retired; in flight (oldest first) with their end events
-    uint64_t recorded = 0, retired = 0;
-    std::vector<cudaEvent_t> done_events;  // a ring of two
-    std::vector<uint64_t> in_flight;       // pass numbers
-    uint32_t bands = 1;
-    // profiling: events after each kernel of the pass in flight, and ms per kind
-    std::vector<std::vector<std::pair<cudaEvent_t, int>>> marks;
-    cudaEvent_t mark_start[2] = {nullptr, nullptr};
-    double kernel_ms[10] = {0};
+// Device memory carved into 256-byte aligned parts: add the parts, then allocate once.
+struct Layout {
+    struct Part {
+        const void *src;
+        size_t bytes, offset;
+    };
+    std::vector<Part> parts;
+    size_t add(const void *src, size_t bytes) {
+        parts.push_back({src, bytes, 0});
+        return parts.size() - 1;
+    }
+    // One allocation, zeroed, with the host parts copied in; waits for the copies.
+    void *allocate(cudaStream_t stream, size_t &total) {
+        total = 0;
+        for (auto &p : parts) {
+            p.offset = total;
+            total += align256(std::max<size_t>(p.bytes, 64));
+        }
+        void *block = nullptr;
+        LR_CUDA(cudaMalloc(&block, total));
+        char *base = (char *)block;
+        LR_CUDA(cudaMemsetAsync(base, 0, total, stream));
+        for (auto &p : parts)
+            if (p.src && p.bytes) LR_CUDA(cudaMemcpyAsync(base + p.offset, p.src, p.bytes, cudaMemcpyHostToDevice, stream));
+        LR_CUDA(cudaStreamSynchronize(stream));
+        return block;
+    }
 };
 
-namespace lr {
+// The Owen-scrambled Sobol sampler's byte tables (dimensions 1-3), set once per process
+// and device.
+void upload_sobol_tables(cudaStream_t stream) {
+    static std::vector<uint32_t> sobol_bytes;
+    if (sobol_bytes.empty()) {
+        const uint32_t *dirs = sobol_table();
+        sobol_bytes.assign(3 * 4 * 256, 0u);
+        for (int d = 1; d < 4; d++)
+            for (int b = 0; b < 4; b++)
+                for (int value = 0; value < 256; value++) {
+                    uint32_t x = 0;
+                    for (int bit = 0; bit < 8; bit++)
+                        if (value & (1 << bit)) x ^= dirs[d * 32 + b * 8 + bit];
+                    sobol_bytes[(d - 1) * 1024 + b * 256 + value] = x;
+                }
+    }
+    LR_CUDA(cudaMemcpyToSymbolAsync(g_sobol_bytes, sobol_bytes.data(), sobol_bytes.size() * sizeof(uint32_t), 0,
+                                    cudaMemcpyHostToDevice, stream));
+}
+
+}  // namespace
+
+// ---- Host side ------------------------------------------------------------------------
+
+// A member as the host keeps it: its device record and block, and where its sampling
+// stands (`sample`, `next_pixel`: the next segment to plan; `done`: samples whose last
+// pass has finished).
+struct MemberHost {
+    bool used = false, leaving = false;
+    Member dev{};
+    void *block = nullptr;
+    lr_gpu_scene *owned = nullptr;  // a renderer's own upload (null when borrowed)
+    uint32_t samples = 0, sample = 0, next_pixel = 0, done = 0;
+    uint32_t max_bounces = 0;
+    TraversalChoice traversal{2, 32};
+    uint64_t last_pass = 0;  // the last pass (plus one) that traced it; 0: none
+};
+
+// The traversal variants a pass can take: (BVH width, stack entries).
+#define LR_TRAVERSALS(X) X(8, 32) X(8, 48) X(4, 32) X(4, 48) X(2, 32) X(2, 64) X(2, 96)
+
+struct PassRecord {
+    uint64_t number;
+    std::vector<std::pair<uint32_t, bool>> members;  // member, sample ended
+    std::vector<std::pair<cudaEvent_t, int>> marks;  // profiling
+};
+
+struct WaveHost {
+    lr_context *ctx = nullptr;
+    uint32_t pool = 0, rounds = 0, capacity = 0;
+    int profile = 0;
+    void *block = nullptr;
+    Wave w{};
+    Member *d_members = nullptr;
+    Plan *d_plan = nullptr;
+    Plan *h_plan[2] = {nullptr, nullptr};  // pinned staging, by pass parity
+    std::vector<MemberHost> members;
+    int grid_shade = 0;
+    struct Exec {
+        cudaGraph_t graph = nullptr;
+        cudaGraphExec_t exec = nullptr;
+        int grid_trace = 0;
+    };
+    std::map<int, Exec> execs;  // by variant: width * 1000 + stack
+    uint64_t recorded = 0, retired = 0;
+    cudaEvent_t done_events[2] = {nullptr, nullptr};
+    cudaEvent_t mark_start[2] = {nullptr, nullptr};
+    std::deque<PassRecord> in_flight;
+    double kernel_ms[10] = {0};
+    uint32_t rotate = 0;  // the member the next plan starts from
+};
+
 namespace {
 
-// Records one pass on `stream`. With `marks`, an event follows each kernel (profiling);
-// kCount instantiates the traversal kernels that count their work.
-template <bool kSpectral, int W, int kStack, bool kCount>
-void record_pass(lr_renderer *r, cudaStream_t stream, std::vector<std::pair<cudaEvent_t, int>> *marks) {
-    View &v = r->view;
+// Records one pass on `stream` with traversal variant (W, kStack). With `marks`, an
+// event follows each kernel (profiling); kCount instantiates the counting traversals.
+template <int W, int kStack, bool kCount>
+void record_pass(WaveHost *h, int grid_trace, cudaStream_t stream, std::vector<std::pair<cudaEvent_t, int>> *marks) {
+    const Wave &w = h->w;
     auto mark = [&](int kind) {
         if (!marks) return;
         cudaEvent_t e;
@@ -551,34 +689,41 @@ void record_pass(lr_renderer *r, cudaStream_t stream, std::vector<std::pair<cuda
         LR_CUDA(cudaEventRecord(e, stream));
         marks->push_back({e, kind});
     };
-    begin_kernel<<<1, 256, 0, stream>>>(v);
-    mark(kRest);
-    camera_kernel<kSpectral><<<r->grid_shade, kShadeBlock, 0, stream>>>(v);
+    camera_kernel<<<h->grid_shade, kShadeBlock, 0, stream>>>(w);
     mark(kCamera);
-    for (uint32_t round = 0; round < v.rounds; round++) {
-        closest_kernel<W, kStack, kCount><<<r->grid_trace, kTraceBlock, 0, stream>>>(v, round);
+    for (uint32_t round = 0; round < w.rounds; round++) {
+        closest_kernel<W, kStack, kCount><<<grid_trace, kTraceBlock, 0, stream>>>(w, round);
         mark(kClosest);
-        shade_kernel<kSpectral><<<r->grid_shade, kShadeBlock, 0, stream>>>(v, round);
+        shade_kernel<<<h->grid_shade, kShadeBlock, 0, stream>>>(w, round);
         mark(kSurface);
-        shadow_kernel<W, kStack, kCount><<<r->grid_trace, kTraceBlock, 0, stream>>>(v, round);
+        shadow_kernel<W, kStack, kCount><<<grid_trace, kTraceBlock, 0, stream>>>(w, round);
         mark(kShadow);
     }
-    finish_kernel<kSpectral><<<r->grid_shade, kShadeBlock, 0, stream>>>(v);
+    finish_kernel<<<h->grid_shade, kShadeBlock, 0, stream>>>(w);
     mark(kFinish);
-    convert_kernel<kSpectral><<<r->grid_shade, kShadeBlock, 0, stream>>>(v);
+    convert_kernel<<<h->grid_shade, kShadeBlock, 0, stream>>>(w);
     mark(kConvert);
     LR_CUDA(cudaGetLastError());
 }
 
-// The traversal variants a renderer can take: (BVH width, stack entries).
-#define LR_TRAVERSALS(X) X(8, 32) X(8, 48) X(4, 32) X(4, 48) X(2, 32) X(2, 64) X(2, 96)
+int trace_grid(int variant, int sms) {
+    switch (variant) {
+#define LR_CASE(wd, k) \
+    case wd * 1000 + k: return grid_of(closest_kernel<wd, k, false>, kTraceBlock, sms);
+        LR_TRAVERSALS(LR_CASE)
+#undef LR_CASE
+        default: fail(LR_LIMIT, "no traversal variant for this scene");
+    }
+}
 
-template <bool kSpectral, bool kCount>
-void record_any(lr_renderer *r, cudaStream_t stream, std::vector<std::pair<cudaEvent_t, int>> *marks) {
-    switch (r->width * 1000 + r->stack) {
-#define LR_CASE(w, k)                                                   \
-    case w * 1000 + k:                                                  \
-        record_pass<kSpectral, w, k, kCount>(r, stream, marks);         \
+void record(WaveHost *h, int variant, int grid_trace, cudaStream_t stream,
+            std::vector<std::pair<cudaEvent_t, int>> *marks) {
+    const bool count = h->profile == 2;
+    switch (variant) {
+#define LR_CASE(wd, k)                                                                        \
+    case wd * 1000 + k:                                                                       \
+        if (count) record_pass<wd, k, true>(h, grid_trace, stream, marks);                    \
+        else record_pass<wd, k, false>(h, grid_trace, stream, marks);                         \
         break;
         LR_TRAVERSALS(LR_CASE)
 #undef LR_CASE
@@ -586,77 +731,80 @@ void record_any(lr_renderer *r, cudaStream_t stream, std::vector<std::pair<cudaE
     }
 }
 
-void record(lr_renderer *r, cudaStream_t stream, std::vector<std::pair<cudaEvent_t, int>> *marks) {
-    const bool count = r->settings.profile == 2;
-    if (r->settings.spectral) {
-        if (count) record_any<true, true>(r, stream, marks);
-        else record_any<true, false>(r, stream, marks);
-    } else {
-        if (count) record_any<false, true>(r, stream, marks);
-        else record_any<false, false>(r, stream, marks);
+WaveHost::Exec &exec_for(WaveHost *h, int variant) {
+    auto it = h->execs.find(variant);
+    if (it != h->execs.end()) return it->second;
+    WaveHost::Exec e;
+    e.grid_trace = trace_grid(variant, h->ctx->sm_count);
+    if (!h->profile) {
+        // The pass as one graph, captured on a private stream.
+        cudaStream_t capture;
+        LR_CUDA(cudaStreamCreateWithFlags(&capture, cudaStreamNonBlocking));
+        LR_CUDA(cudaStreamBeginCapture(capture, cudaStreamCaptureModeThreadLocal));
+        record(h, variant, e.grid_trace, capture, nullptr);
+        LR_CUDA(cudaStreamEndCapture(capture, &e.graph));
+        LR_CUDA(cudaStreamDestroy(capture));
+        LR_CUDA(cudaGraphInstantiate(&e.exec, e.graph, 0));
     }
+    return h->execs.emplace(variant, e).first->second;
 }
 
-template <bool kSpectral>
-void size_grids(lr_renderer *r) {
-    const int sms = r->ctx->sm_count;
-    switch (r->width * 1000 + r->stack) {
-#define LR_CASE(w, k)                                                            \
-    case w * 1000 + k:                                                           \
-        r->grid_trace = grid_of(closest_kernel<w, k, false>, kTraceBlock, sms);  \
-        break;
-        LR_TRAVERSALS(LR_CASE)
-#undef LR_CASE
-        default: fail(LR_LIMIT, "no traversal variant for this scene");
+void wave_create(WaveHost *h, lr_context *ctx, uint64_t pool, uint32_t rounds, uint32_t capacity, int profile) {
+    if (pool == 0 || rounds == 0 || capacity == 0) fail(LR_INVALID, "a wave needs paths, rounds and members");
+    h->ctx = ctx;
+    h->pool = (uint32_t)std::min<uint64_t>(pool, kMaxPool);
+    h->rounds = rounds;
+    h->capacity = capacity;
+    h->profile = profile;
+    LR_CUDA(cudaSetDevice(ctx->device));
+    const uint64_t P = h->pool;
+    Layout L;
+    const size_t p_throughput = L.add(nullptr, P * 16), p_radiance = L.add(nullptr, P * 16);
+    const size_t p_lambda = L.add(nullptr, P * 16), p_vertex = L.add(nullptr, P * 16), p_path = L.add(nullptr, P * 16);
+    size_t p_ray[2][3];
+    for (int q = 0; q < 2; q++)
+        for (int j = 0; j < 3; j++) p_ray[q][j] = L.add(nullptr, P * 16);
+    const size_t p_shadow_o = L.add(nullptr, P * 16), p_shadow_d = L.add(nullptr, P * 16);
+    const size_t p_shadow_c = L.add(nullptr, P * 16);
+    const size_t p_counters = L.add(nullptr, (4 * (size_t)rounds + 2) * 4);
+    const size_t p_stats = L.add(nullptr, 8 * 8);
+    const size_t p_members = L.add(nullptr, (size_t)capacity * sizeof(Member));
+    const size_t p_plan = L.add(nullptr, sizeof(Plan));
+    size_t total = 0;
+    h->block = L.allocate(ctx->stream, total);
+    char *base = (char *)h->block;
+    auto at = [&](size_t i) { return (void *)(base + L.parts[i].offset); };
+    Wave &w = h->w;
+    w.pool = h->pool;
+    w.rounds = rounds;
+    w.throughput = (float4 *)at(p_throughput);
+    w.radiance = (float4 *)at(p_radiance);
+    w.lambda = (float4 *)at(p_lambda);
+    w.vertex = (float4 *)at(p_vertex);
+    w.path = (uint4 *)at(p_path);
+    for (int q = 0; q < 2; q++) {
+        w.ray_o[q] = (float4 *)at(p_ray[q][0]);
+        w.ray_d[q] = (float4 *)at(p_ray[q][1]);
+        w.hits[q] = (float4 *)at(p_ray[q][2]);
     }
-    r->grid_shade = grid_of(shade_kernel<kSpectral>, kShadeBlock, sms);
-}
-
-void settle(lr_renderer *r) {
-    for (size_t i = 0; i < r->in_flight.size(); i++) LR_CUDA(cudaEventSynchronize(r->done_events[r->in_flight[i] & 1]));
-}
-
-// Retire the oldest pass in flight if it has finished (integrator.lucb:622-645).
-bool retire_one(lr_renderer *r, bool wait) {
-    if (r->in_flight.empty()) return false;
-    const uint64_t pass = r->in_flight.front();
-    cudaEvent_t e = r->done_events[pass & 1];
-    if (wait) {
-        LR_CUDA(cudaEventSynchronize(e));
-    } else {
-        cudaError_t q = cudaEventQuery(e);
-        if (q == cudaErrorNotReady) return false;
-        LR_CUDA(q);
-    }
-    if (r->settings.profile && !r->marks.empty()) {
-        auto &ms = r->marks[pass & 1];
-        cudaEvent_t prev = r->mark_start[pass & 1];
-        for (auto &[ev, kind] : ms) {
-            float t = 0.0f;
-            LR_CUDA(cudaEventElapsedTime(&t, prev, ev));
-            r->kernel_ms[kind] += t;
-            prev = ev;
-        }
-        for (auto &[ev, kind] : ms) cudaEventDestroy(ev);
-        ms.clear();
-    }
-    r->in_flight.erase(r->in_flight.begin());
-    r->retired = pass + 1;
-    return true;
-}
-
-void launch_pass(lr_renderer *r) {
-    cudaStream_t stream = r->ctx->stream;
-    const uint64_t pass = r->recorded;
-    if (r->settings.profile) {
-        LR_CUDA(cudaEventRecord(r->mark_start[pass & 1], stream));
-        record(r, stream, &r->marks[pass & 1]);
-    } else {
-        LR_CUDA(cudaGraphLaunch(r->exec, stream));
-    }
-    LR_CUDA(cudaEventRecord(r->done_events[pass & 1], stream));
-    r->in_flight.push_back(pass);
-    r->recorded = pass + 1;
+    w.shadow_o = (float4 *)at(p_shadow_o);
+    w.shadow_d = (float4 *)at(p_shadow_d);
+    w.shadow_c = (float4 *)at(p_shadow_c);
+    w.counters = (uint32_t *)at(p_counters);
+    w.stats = (unsigned long long *)at(p_stats);
+    w.status = ctx->status;
+    h->d_members = (Member *)at(p_members);
+    h->d_plan = (Plan *)at(p_plan);
+    w.members = h->d_members;
+    w.plan = h->d_plan;
+    for (auto &p : h->h_plan) LR_CUDA(cudaMallocHost((void **)&p, sizeof(Plan)));
+    upload_sobol_tables(ctx->stream);
+    LR_CUDA(cudaStreamSynchronize(ctx->stream));
+    h->grid_shade = grid_of(shade_kernel, kShadeBlock, ctx->sm_count);
+    for (auto &e : h->done_events) LR_CUDA(cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
+    if (profile)
+        for (auto &e : h->mark_start) LR_CUDA(cudaEventCreate(&e));
+    h->members.resize(capacity);
 }
 
 void validate(const lr_settings &s, const lr_frame &f) {
@@ -669,28 +817,22 @@ void validate(const lr_settings &s, const lr_frame &f) {
     if (s.max_bounces > 253) fail(LR_INVALID, "this build traces at most 253 bounces");
 }
 
-void create(lr_context *ctx, const lr_scene *scene, const lr_settings &settings, const lr_frame &frame, lr_renderer **out) {
+// Makes `scene` (uploaded as `gs`) seen through `frame` a member; returns its index.
+uint32_t member_add(WaveHost *h, const lr_gpu_scene *gs, lr_gpu_scene *owned, const lr_scene *scene,
+                    const lr_settings &settings, const lr_frame &frame) {
     validate(settings, frame);
-    auto r = std::make_unique<lr_renderer>();
-    r->ctx = ctx;
-    r->settings = settings;
-    r->settings.width = frame.width;
-    r->settings.height = frame.height;
-    r->frame = frame;
-    LR_CUDA(cudaSetDevice(ctx->device));
-    r->loaded = load(*scene, settings);
-    lr_gpu_scene *gs = nullptr;
-    int status = lr_gpu_scene_upload(ctx, scene, &gs);
-    if (status != LR_OK) fail(status, lr_last_error());
-    r->gs = gs;
-
-    const Loaded &L = r->loaded;
+    if (settings.max_bounces + 1 > h->rounds)
+        fail(LR_LIMIT, "this wave traces at most " + std::to_string(h->rounds - 1) + " bounces");
+    if (gs->ctx != h->ctx) fail(LR_INVALID, "the scene was uploaded through another context");
+    uint32_t index = h->capacity;
+    for (uint32_t i = 0; i < h->capacity; i++)
+        if (!h->members[i].used) {
+            index = i;
+            break;
+        }
+    if (index == h->capacity) fail(LR_LIMIT, "the wave holds " + std::to_string(h->capacity) + " members");
+    const Loaded L = load(*scene, settings);
     const uint64_t pixels = (uint64_t)frame.width * frame.height;
-    const uint64_t pool = std::min<uint64_t>(settings.pool ? settings.pool : kDefaultPool, pixels);
-    r->bands = (uint32_t)((pixels + pool - 1) / pool);
-    const uint32_t rounds = settings.max_bounces + 1;
-
-    // Device layout: one allocation, arrays at 256-byte offsets.
     Constants k{};
     for (int i = 0; i < 9; i++) k.film[i] = (float)L.film.m[i];
     k.cmf_integrals[0] = (float)L.cmf_integrals.x;
@@ -709,129 +851,284 @@ void create(lr_context *ctx, const lr_scene *scene, const lr_settings &settings,
     k.tree_nodes = (uint32_t)L.tree.node_count;
     k.seed = settings.seed;
 
-    struct Part {
-        const void *src;
-        size_t bytes;
-        size_t offset;
-    };
-    std::vector<Part> parts;
-    auto add = [&](const void *src, size_t bytes) {
-        parts.push_back({src, bytes, 0});
-        return parts.size() - 1;
-    };
-    const size_t p_lights = add(L.lights.rows.data(), L.lights.rows.size() * 4);
-    const size_t p_tree_nodes = add(L.tree.nodes.data(), L.tree.nodes.size() * 4);
-    const size_t p_tree_links = add(L.tree.links.data(), L.tree.links.size() * 4);
-    const size_t p_tree_records = add(L.tree.records.data(), L.tree.records.size() * 4);
-    const size_t p_tree_map = add(L.tree.triangle_map.data(), L.tree.triangle_map.size() * 4);
-    const size_t p_materials = add(L.materials.data(), L.materials.size() * 4);
-    const size_t p_constants = add(&k, sizeof k);
-    const size_t p_throughput = add(nullptr, pool * 16);
-    const size_t p_radiance = add(nullptr, pool * 16);
-    const size_t p_lambda = add(nullptr, settings.spectral ? pool * 16 : 16);
-    const size_t p_vertex = add(nullptr, pool * 16);
-    const size_t p_path = add(nullptr, pool * 16);
-    size_t p_ray[2][3];
-    for (int q = 0; q < 2; q++)
-        for (int j = 0; j < 3; j++) p_ray[q][j] = add(nullptr, pool * 16);
-    const size_t p_shadow_o = add(nullptr, pool * 16);
-    const size_t p_shadow_d = add(nullptr, pool * 16);
-    const size_t p_shadow_c = add(nullptr, pool * 16);
-    const size_t p_counters = add(nullptr, (4 * rounds + 2) * 4);
-    const size_t p_pass = add(nullptr, sizeof(PassState));
-    const size_t p_pass_counter = add(nullptr, 8);
-    const size_t p_film = add(nullptr, pixels * 16);
-    const size_t p_image = add(nullptr, pixels * 16);
-    const size_t p_stats = add(nullptr, 8 * 8);
+    Layout lay;
+    const size_t p_lights = lay.add(L.lights.rows.data(), L.lights.rows.size() * 4);
+    const size_t p_tree_nodes = lay.add(L.tree.nodes.data(), L.tree.nodes.size() * 4);
+    const size_t p_tree_links = lay.add(L.tree.links.data(), L.tree.links.size() * 4);
+    const size_t p_tree_records = lay.add(L.tree.records.data(), L.tree.records.size() * 4);
+    const size_t p_tree_map = lay.add(L.tree.triangle_map.data(), L.tree.triangle_map.size() * 4);
+    const size_t p_materials = lay.add(L.materials.data(), L.materials.size() * 4);
+    const size_t p_constants = lay.add(&k, sizeof k);
+    const size_t p_film = lay.add(nullptr, pixels * 16);
+    const size_t p_image = lay.add(nullptr, pixels * 16);
+    MemberHost &mh = h->members[index];
     size_t total = 0;
-    for (auto &p : parts) {
-        p.offset = total;
-        total += align256(std::max<size_t>(p.bytes, 64));
-    }
-    LR_CUDA(cudaMalloc(&r->block, total));
-    char *base = (char *)r->block;
-    LR_CUDA(cudaMemsetAsync(base, 0, total, ctx->stream));
-    for (auto &p : parts)
-        if (p.src && p.bytes) LR_CUDA(cudaMemcpyAsync(base + p.offset, p.src, p.bytes, cudaMemcpyHostToDevice, ctx->stream));
-    static std::vector<uint32_t> sobol_bytes;
-    if (sobol_bytes.empty()) {
-        const uint32_t *dirs = sobol_table();
-        sobol_bytes.assign(3 * 4 * 256, 0u);
-        for (int d = 1; d < 4; d++)
-            for (int b = 0; b < 4; b++)
-                for (int value = 0; value < 256; value++) {
-                    uint32_t x = 0;
-                    for (int bit = 0; bit < 8; bit++)
-                        if (value & (1 << bit)) x ^= dirs[d * 32 + b * 8 + bit];
-                    sobol_bytes[(d - 1) * 1024 + b * 256 + value] = x;
-                }
-    }
-    LR_CUDA(cudaMemcpyToSymbolAsync(g_sobol_bytes, sobol_bytes.data(), sobol_bytes.size() * sizeof(uint32_t), 0,
-                                    cudaMemcpyHostToDevice, ctx->stream));
-    LR_CUDA(cudaStreamSynchronize(ctx->stream));
-    auto at = [&](size_t i) { return (void *)(base + parts[i].offset); };
+    mh.block = lay.allocate(h->ctx->stream, total);
+    char *base = (char *)mh.block;
+    auto at = [&](size_t i) { return (void *)(base + lay.parts[i].offset); };
+    Member &m = mh.dev;
+    m = Member{};
+    m.scene = gs->scene;
+    m.lights = (const float4 *)at(p_lights);
+    m.light_count = (uint32_t)L.lights.count;
+    m.spectral = settings.spectral ? 1u : 0u;
+    m.tree.nodes = (const float4 *)at(p_tree_nodes);
+    m.tree.links = (const uint2 *)at(p_tree_links);
+    m.tree.records = (const uint4 *)at(p_tree_records);
+    m.tree.triangle_map = L.tree.triangle_map.empty() ? nullptr : (const uint32_t *)at(p_tree_map);
+    m.tree.node_count = (uint32_t)L.tree.node_count;
+    m.materials = (const float4 *)at(p_materials);
+    m.k = (const Constants *)at(p_constants);
+    pack_frame(frame, m.frame);
+    m.lens_radius = (float)frame.lens_radius;
+    m.focus_distance = (float)frame.focus_distance;
+    for (int i = 0; i < 3; i++) m.forward[i] = (float)frame.forward[i];
+    m.width = frame.width;
+    m.height = frame.height;
+    m.pixels = pixels;
+    m.film = (float4 *)at(p_film);
+    m.image = (float4 *)at(p_image);
+    LR_CUDA(cudaMemcpyAsync(h->d_members + index, &m, sizeof m, cudaMemcpyHostToDevice, h->ctx->stream));
+    LR_CUDA(cudaStreamSynchronize(h->ctx->stream));
+    mh.used = true;
+    mh.leaving = false;
+    mh.owned = owned;
+    mh.samples = settings.samples;
+    mh.sample = mh.next_pixel = mh.done = 0;
+    mh.max_bounces = settings.max_bounces;
+    mh.traversal = choose_traversal(gs->scene, 0);
+    mh.last_pass = 0;
+    return index;
+}
 
-    View &v = r->view;
-    v.scene = gs->scene;
-    v.lights = (const float4 *)at(p_lights);
-    v.light_count = (uint32_t)L.lights.count;
-    v.tree.nodes = (const float4 *)at(p_tree_nodes);
-    v.tree.links = (const uint2 *)at(p_tree_links);
-    v.tree.records = (const uint4 *)at(p_tree_records);
-    v.tree.triangle_map = L.tree.triangle_map.empty() ? nullptr : (const uint32_t *)at(p_tree_map);
-    v.tree.node_count = (uint32_t)L.tree.node_count;
-    v.materials = (const float4 *)at(p_materials);
-    v.k = (const Constants *)at(p_constants);
-    pack_frame(frame, v.frame);
-    v.lens_radius = (float)frame.lens_radius;
-    v.focus_distance = (float)frame.focus_distance;
-    for (int i = 0; i < 3; i++) v.forward[i] = (float)frame.forward[i];
-    v.width = frame.width;
-    v.height = frame.height;
-    v.pool = (uint32_t)pool;
-    v.bands = r->bands;
-    v.rounds = rounds;
-    v.pixels = pixels;
-    v.throughput = (float4 *)at(p_throughput);
-    v.radiance = (float4 *)at(p_radiance);
-    v.lambda = (float4 *)at(p_lambda);
-    v.vertex = (float4 *)at(p_vertex);
-    v.path = (uint4 *)at(p_path);
-    for (int q = 0; q < 2; q++) {
-        v.ray_o[q] = (float4 *)at(p_ray[q][0]);
-        v.ray_d[q] = (float4 *)at(p_ray[q][1]);
-        v.hits[q] = (float4 *)at(p_ray[q][2]);
-    }
-    v.shadow_o = (float4 *)at(p_shadow_o);
-    v.shadow_d = (float4 *)at(p_shadow_d);
-    v.shadow_c = (float4 *)at(p_shadow_c);
-    v.counters = (uint32_t *)at(p_counters);
-    v.pass = (PassState *)at(p_pass);
-    v.pass_counter = (unsigned long long *)at(p_pass_counter);
-    v.film = (float4 *)at(p_film);
-    v.image = (float4 *)at(p_image);
-    v.stats = (unsigned long long *)at(p_stats);
-    v.status = ctx->status;
+void member_free(MemberHost &mh) {
+    if (mh.block) cudaFree(mh.block);
+    if (mh.owned) lr_gpu_scene_destroy(mh.owned);
+    mh = MemberHost{};
+}
 
-    const TraversalChoice traversal = choose_traversal(gs->scene, 0);
-    r->width = traversal.width;
-    r->stack = traversal.stack;
-    if (settings.spectral) size_grids<true>(r.get());
-    else size_grids<false>(r.get());
-    r->done_events.resize(2);
-    for (auto &e : r->done_events) LR_CUDA(cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
-    if (settings.profile) {
-        r->marks.resize(2);
-        for (auto &e : r->mark_start) LR_CUDA(cudaEventCreate(&e));
+// Frees members that asked to leave once no pass in flight traces them.
+void collect(WaveHost *h) {
+    for (auto &mh : h->members)
+        if (mh.used && mh.leaving && mh.last_pass <= h->retired) member_free(mh);
+}
+
+bool has_work(const MemberHost &mh) { return mh.used && !mh.leaving && mh.sample < mh.samples; }
+
+// Retires the oldest pass in flight if it has finished (integrator.lucb:622-645).
+bool retire_one(WaveHost *h, bool wait) {
+    if (h->in_flight.empty()) return false;
+    PassRecord &p = h->in_flight.front();
+    cudaEvent_t e = h->done_events[p.number & 1];
+    if (wait) {
+        LR_CUDA(cudaEventSynchronize(e));
     } else {
-        // The pass as one graph, captured on a private stream.
-        cudaStream_t capture;
-        LR_CUDA(cudaStreamCreateWithFlags(&capture, cudaStreamNonBlocking));
-        LR_CUDA(cudaStreamBeginCapture(capture, cudaStreamCaptureModeThreadLocal));
-        record(r.get(), capture, nullptr);
-        LR_CUDA(cudaStreamEndCapture(capture, &r->graph));
-        LR_CUDA(cudaStreamDestroy(capture));
-        LR_CUDA(cudaGraphInstantiate(&r->exec, r->graph, 0));
+        cudaError_t q = cudaEventQuery(e);
+        if (q == cudaErrorNotReady) return false;
+        LR_CUDA(q);
+    }
+    if (h->profile && !p.marks.empty()) {
+        cudaEvent_t prev = h->mark_start[p.number & 1];
+        for (auto &[ev, kind] : p.marks) {
+            float t = 0.0f;
+            LR_CUDA(cudaEventElapsedTime(&t, prev, ev));
+            h->kernel_ms[kind] += t;
+            prev = ev;
+        }
+        for (auto &[ev, kind] : p.marks) cudaEventDestroy(ev);
+    }
+    for (auto &[m, ended] : p.members)
+        if (ended) h->members[m].done++;
+    h->retired = p.number + 1;
+    h->in_flight.pop_front();
+    collect(h);
+    return true;
+}
+
+void settle(WaveHost *h) {
+    while (!h->in_flight.empty()) retire_one(h, true);
+}
+
+// Plans and launches one pass: each member with work left adds its next segment, in
+// turn from `rotate`, until the pool is full. A member takes one segment a pass at
+// most, so a pixel never gets two samples in one pass. Returns false with no work.
+bool launch_pass(WaveHost *h) {
+    Plan *staging = h->h_plan[h->recorded & 1];
+    Segment *seg = staging->seg;
+    uint32_t n = 0, used = 0, converts = 0;
+    int width = 0, stack = 32;
+    bool mixed = false;
+    PassRecord rec;
+    rec.number = h->recorded;
+    const uint32_t cap = h->capacity;
+    uint32_t last = h->rotate;
+    for (uint32_t step = 0; step < cap && used < h->pool && n < kMaxSegments; step++) {
+        const uint32_t index = (h->rotate + step) % cap;
+        MemberHost &mh = h->members[index];
+        if (!has_work(mh)) continue;
+        const uint64_t left = mh.dev.pixels - mh.next_pixel;
+        const uint32_t count = (uint32_t)std::min<uint64_t>(left, h->pool - used);
+        const bool ends = count == left;
+        seg[n] = Segment{index, mh.next_pixel, count, mh.sample, used, ends ? 1u : 0u, 0u, 0u};
+        rec.members.push_back({index, ends});
+        if (ends) staging->convert[converts++] = index;
+        n++;
+        used += count;
+        if (ends) {
+            mh.sample++;
+            mh.next_pixel = 0;
+        } else {
+            mh.next_pixel += count;
+        }
+        mh.last_pass = h->recorded + 1;
+        if (width == 0) width = mh.traversal.width;
+        else if (width != mh.traversal.width) mixed = true;
+        stack = std::max(stack, mh.traversal.stack);
+        last = index;
+    }
+    if (n == 0) return false;
+    h->rotate = (last + 1) % cap;
+    // One traversal variant serves the pass: the members' common width with the deepest
+    // stack among them, or the BVH2 when their widths differ.
+    if (mixed) {
+        width = 2;
+        stack = 32;
+        for (auto &[m, ended] : rec.members) {
+            const TraversalChoice c = choose_traversal(h->members[m].dev.scene, 2);
+            stack = std::max(stack, c.stack);
+        }
+    }
+    const int variant = width * 1000 + stack;
+    staging->head = PlanHeader{n, used, converts, 0u};
+    cudaStream_t stream = h->ctx->stream;
+    WaveHost::Exec &ex = exec_for(h, variant);
+    // The header and convert list, then the segments in use.
+    LR_CUDA(cudaMemcpyAsync(h->d_plan, staging, offsetof(Plan, seg) + n * sizeof(Segment), cudaMemcpyHostToDevice,
+                            stream));
+    if (h->profile) {
+        LR_CUDA(cudaEventRecord(h->mark_start[rec.number & 1], stream));
+        record(h, variant, ex.grid_trace, stream, &rec.marks);
+    } else {
+        LR_CUDA(cudaGraphLaunch(ex.exec, stream));
+    }
+    LR_CUDA(cudaEventRecord(h->done_events[rec.number & 1], stream));
+    h->in_flight.push_back(std::move(rec));
+    h->recorded++;
+    return true;
+}
+
+// Renderer.advance (integrator.lucb:649-693): never waits; two passes in flight.
+bool wave_advance(WaveHost *h) {
+    while (retire_one(h, false)) {
+    }
+    if (h->in_flight.size() >= 2) return true;
+    if (launch_pass(h)) return true;
+    return !h->in_flight.empty();
+}
+
+void wave_finish(WaveHost *h) {
+    for (;;) {
+        if (!wave_advance(h)) break;
+        if (h->in_flight.size() >= 2) retire_one(h, true);
+        else if (!h->in_flight.empty() && !std::any_of(h->members.begin(), h->members.end(), has_work))
+            retire_one(h, true);
+    }
+    check_status(h->ctx);
+}
+
+void wave_destroy(WaveHost *h) {
+    if (!h->ctx) return;
+    cudaSetDevice(h->ctx->device);
+    cudaStreamSynchronize(h->ctx->stream);
+    for (auto &p : h->in_flight)
+        for (auto &[e, k] : p.marks) cudaEventDestroy(e);
+    for (auto e : h->mark_start)
+        if (e) cudaEventDestroy(e);
+    for (auto e : h->done_events)
+        if (e) cudaEventDestroy(e);
+    for (auto &[v, e] : h->execs) {
+        if (e.exec) cudaGraphExecDestroy(e.exec);
+        if (e.graph) cudaGraphDestroy(e.graph);
+    }
+    for (auto &mh : h->members)
+        if (mh.used) member_free(mh);
+    for (auto p : h->h_plan)
+        if (p) cudaFreeHost(p);
+    if (h->block) cudaFree(h->block);
+}
+
+void wave_stats(WaveHost *h, lr_render_stats *out) {
+    settle(h);
+    unsigned long long s[8];
+    LR_CUDA(cudaMemcpyAsync(s, h->w.stats, sizeof s, cudaMemcpyDeviceToHost, h->ctx->stream));
+    LR_CUDA(cudaStreamSynchronize(h->ctx->stream));
+    out->closest_rays = s[0];
+    out->shadow_rays = s[1];
+    out->shaded = s[2];
+    out->passes = s[3];
+    out->closest_nodes = s[4];
+    out->closest_tests = s[5];
+    out->shadow_nodes = s[6];
+    out->shadow_tests = s[7];
+}
+
+void wave_kernel_times(WaveHost *h, double out[10]) {
+    // Finished passes count: wait for those in flight and retire them.
+    settle(h);
+    for (int i = 0; i < 10; i++) out[i] = h->kernel_ms[i];
+}
+
+MemberHost &member_at(WaveHost *h, uint32_t member) {
+    if (member >= h->capacity || !h->members[member].used || h->members[member].leaving)
+        fail(LR_INVALID, "no such member");
+    return h->members[member];
+}
+
+void member_read(WaveHost *h, uint32_t member, float *rgba, uint64_t count) {
+    MemberHost &mh = member_at(h, member);
+    if (count != mh.dev.pixels * 4) fail(LR_INVALID, "reading the image needs four floats a pixel");
+    LR_CUDA(cudaMemcpyAsync(rgba, mh.dev.image, count * 4, cudaMemcpyDeviceToHost, h->ctx->stream));
+    LR_CUDA(cudaStreamSynchronize(h->ctx->stream));
+}
+
+}  // namespace
+}  // namespace lr
+
+using namespace lr;
+
+struct lr_renderer {
+    WaveHost wave;
+    uint32_t bands = 1;
+};
+
+struct lr_batch {
+    WaveHost wave;
+};
+
+namespace lr {
+namespace {
+
+void create(lr_context *ctx, const lr_scene *scene, const lr_settings &settings, const lr_frame &frame, lr_renderer **out) {
+    validate(settings, frame);
+    auto r = std::make_unique<lr_renderer>();
+    LR_CUDA(cudaSetDevice(ctx->device));
+    const uint64_t pixels = (uint64_t)frame.width * frame.height;
+    const uint64_t pool = std::min<uint64_t>(std::min<uint64_t>(settings.pool ? settings.pool : kDefaultPool, kMaxPool), pixels);
+    r->bands = (uint32_t)((pixels + pool - 1) / pool);
+    lr_gpu_scene *gs = nullptr;
+    int status = lr_gpu_scene_upload(ctx, scene, &gs);
+    if (status != LR_OK) fail(status, lr_last_error());
+    try {
+        wave_create(&r->wave, ctx, pool, settings.max_bounces + 1, 1, settings.profile);
+        member_add(&r->wave, gs, gs, scene, settings, frame);
+        // The graph for the scene's traversal variant, made now rather than at the first pass.
+        const TraversalChoice c = r->wave.members[0].traversal;
+        exec_for(&r->wave, c.width * 1000 + c.stack);
+    } catch (...) {
+        const bool owned = !r->wave.members.empty() && r->wave.members[0].used;
+        wave_destroy(&r->wave);
+        if (!owned) lr_gpu_scene_destroy(gs);
+        throw;
     }
     *out = r.release();
 }
@@ -863,22 +1160,26 @@ void lr_settings_default(lr_settings *s, uint32_t width, uint32_t height, uint32
     s->light_tracing = 0.5;
 }
 
+static void camera_of(const lr_scene *scene, const lr_settings *settings, lr_frame &frame) {
+    if (settings->width == 0 || settings->height == 0 || settings->width > 16384 || settings->height > 16384)
+        fail(LR_INVALID, "an image is 1 to 16384 pixels on a side");
+    lr_camera cam;
+    if (settings->camera >= 0) {
+        if ((size_t)settings->camera >= scene->cameras.size()) fail(LR_INVALID, "the scene object is not a camera");
+        cam = scene->cameras[(size_t)settings->camera];
+    } else {
+        if (scene->cameras.empty()) fail(LR_INVALID, "the scene has no camera");
+        cam = scene->cameras[0];
+    }
+    camera_frame(cam, settings->width, settings->height, frame);
+}
+
 int lr_renderer_create(lr_context *ctx, const lr_scene *scene, const lr_settings *settings, lr_renderer **out) {
     return guarded([&] {
         if (!ctx || !scene || !settings || !out) fail(LR_INVALID, "a renderer needs a context, a scene and settings");
         *out = nullptr;
-        if (settings->width == 0 || settings->height == 0 || settings->width > 16384 || settings->height > 16384)
-            fail(LR_INVALID, "an image is 1 to 16384 pixels on a side");
-        lr_camera cam;
-        if (settings->camera >= 0) {
-            if ((size_t)settings->camera >= scene->cameras.size()) fail(LR_INVALID, "the scene object is not a camera");
-            cam = scene->cameras[(size_t)settings->camera];
-        } else {
-            if (scene->cameras.empty()) fail(LR_INVALID, "the scene has no camera");
-            cam = scene->cameras[0];
-        }
         lr_frame frame;
-        camera_frame(cam, settings->width, settings->height, frame);
+        camera_of(scene, settings, frame);
         create(ctx, scene, *settings, frame, out);
     });
 }
@@ -895,46 +1196,24 @@ int lr_renderer_create_viewed(lr_context *ctx, const lr_scene *scene, const lr_s
 int lr_renderer_advance(lr_renderer *r, int32_t *more) {
     return guarded([&] {
         if (!r || !more) fail(LR_INVALID, "no renderer");
-        while (retire_one(r, false)) {
-        }
-        // Two passes in flight (integrator.lucb:651-655); profiling keeps its events per
-        // pass, so it may too.
-        const size_t depth = 2;
-        if (r->in_flight.size() >= depth) {
-            *more = 1;
-            return;
-        }
-        const uint64_t total_passes = (uint64_t)r->settings.samples * r->bands;
-        if (r->recorded >= total_passes) {
-            *more = r->in_flight.empty() ? 0 : 1;
-            return;
-        }
-        launch_pass(r);
-        *more = 1;
+        *more = wave_advance(&r->wave) ? 1 : 0;
     });
 }
 
 int lr_renderer_finish(lr_renderer *r) {
     return guarded([&] {
         if (!r) fail(LR_INVALID, "no renderer");
-        for (;;) {
-            int32_t more = 0;
-            int status = lr_renderer_advance(r, &more);
-            if (status != LR_OK) fail(status, lr_last_error());
-            if (!more) break;
-            if (!r->in_flight.empty()) retire_one(r, true);
-        }
-        check_status(r->ctx);
+        wave_finish(&r->wave);
     });
 }
 
-uint32_t lr_renderer_samples_done(const lr_renderer *r) { return r ? (uint32_t)(r->retired / r->bands) : 0u; }
+uint32_t lr_renderer_samples_done(const lr_renderer *r) { return r ? r->wave.members[0].done : 0u; }
 
 int lr_renderer_passes(const lr_renderer *r, uint64_t *recorded, uint64_t *finished, uint32_t *bands) {
     return guarded([&] {
         if (!r) fail(LR_INVALID, "no renderer");
-        if (recorded) *recorded = r->recorded;
-        if (finished) *finished = r->retired;
+        if (recorded) *recorded = r->wave.recorded;
+        if (finished) *finished = r->wave.retired;
         if (bands) *bands = r->bands;
     });
 }
@@ -942,16 +1221,14 @@ int lr_renderer_passes(const lr_renderer *r, uint64_t *recorded, uint64_t *finis
 int lr_renderer_image(lr_renderer *r, void **device_rgba) {
     return guarded([&] {
         if (!r || !device_rgba) fail(LR_INVALID, "no renderer");
-        *device_rgba = r->view.image;
+        *device_rgba = r->wave.members[0].dev.image;
     });
 }
 
 int lr_renderer_read(lr_renderer *r, float *rgba, uint64_t count) {
     return guarded([&] {
         if (!r || !rgba) fail(LR_INVALID, "no renderer");
-        if (count != r->view.pixels * 4) fail(LR_INVALID, "reading the image needs four floats a pixel");
-        LR_CUDA(cudaMemcpyAsync(rgba, r->view.image, count * 4, cudaMemcpyDeviceToHost, r->ctx->stream));
-        LR_CUDA(cudaStreamSynchronize(r->ctx->stream));
+        member_read(&r->wave, 0, rgba, count);
     });
 }
 
@@ -959,55 +1236,152 @@ int lr_renderer_set_samples(lr_renderer *r, uint32_t samples) {
     return guarded([&] {
         if (!r) fail(LR_INVALID, "no renderer");
         if (samples == 0) fail(LR_INVALID, "a render needs samples");
-        r->settings.samples = samples;
+        r->wave.members[0].samples = samples;
     });
 }
 
 int lr_renderer_kernel_times(lr_renderer *r, double out[10]) {
     return guarded([&] {
         if (!r || !out) fail(LR_INVALID, "kernel times need ten numbers");
-        // Finished passes count: wait for those in flight and retire them.
-        settle(r);
-        while (retire_one(r, false)) {
-        }
-        for (int i = 0; i < 10; i++) out[i] = r->kernel_ms[i];
+        wave_kernel_times(&r->wave, out);
     });
 }
 
 int lr_renderer_stats(lr_renderer *r, lr_render_stats *out) {
     return guarded([&] {
         if (!r || !out) fail(LR_INVALID, "no renderer");
-        settle(r);
-        while (retire_one(r, false)) {
-        }
-        unsigned long long s[8];
-        LR_CUDA(cudaMemcpyAsync(s, r->view.stats, sizeof s, cudaMemcpyDeviceToHost, r->ctx->stream));
-        LR_CUDA(cudaStreamSynchronize(r->ctx->stream));
-        out->closest_rays = s[0];
-        out->shadow_rays = s[1];
-        out->shaded = s[2];
-        out->passes = s[3];
-        out->closest_nodes = s[4];
-        out->closest_tests = s[5];
-        out->shadow_nodes = s[6];
-        out->shadow_tests = s[7];
+        wave_stats(&r->wave, out);
     });
 }
 
 void lr_renderer_destroy(lr_renderer *r) {
     if (!r) return;
-    cudaSetDevice(r->ctx->device);
-    cudaStreamSynchronize(r->ctx->stream);
-    for (auto &ms : r->marks)
-        for (auto &[e, k] : ms) cudaEventDestroy(e);
-    for (auto e : r->mark_start)
-        if (e) cudaEventDestroy(e);
-    for (auto e : r->done_events) cudaEventDestroy(e);
-    if (r->exec) cudaGraphExecDestroy(r->exec);
-    if (r->graph) cudaGraphDestroy(r->graph);
-    if (r->block) cudaFree(r->block);
-    lr_gpu_scene_destroy(r->gs);
+    wave_destroy(&r->wave);
     delete r;
+}
+
+// ---- Batches ------------------------------------------------------------------------
+
+void lr_batch_settings_default(lr_batch_settings *s) {
+    if (!s) return;
+    *s = lr_batch_settings{};
+    s->pool = (uint32_t)kDefaultPool;
+    s->max_bounces = 12;
+    s->capacity = 256;
+    s->profile = 0;
+}
+
+int lr_batch_create(lr_context *ctx, const lr_batch_settings *settings, lr_batch **out) {
+    return guarded([&] {
+        if (!ctx || !settings || !out) fail(LR_INVALID, "a batch needs a context and settings");
+        *out = nullptr;
+        if (settings->max_bounces == 0 || settings->max_bounces > 253) fail(LR_INVALID, "a batch traces 1 to 253 bounces");
+        if (settings->capacity == 0 || settings->capacity > 65536) fail(LR_INVALID, "a batch holds 1 to 65536 members");
+        if (settings->pool == 0) fail(LR_INVALID, "a batch needs a pool of paths");
+        auto b = std::make_unique<lr_batch>();
+        try {
+            wave_create(&b->wave, ctx, settings->pool, settings->max_bounces + 1, settings->capacity, settings->profile);
+        } catch (...) {
+            wave_destroy(&b->wave);
+            throw;
+        }
+        *out = b.release();
+    });
+}
+
+int lr_batch_add(lr_batch *b, const lr_gpu_scene *gs, const lr_scene *scene, const lr_settings *settings,
+                 const lr_frame *frame, uint32_t *member) {
+    return guarded([&] {
+        if (!b || !gs || !scene || !settings || !member) fail(LR_INVALID, "a member needs a scene and settings");
+        lr_frame f;
+        if (frame) f = *frame;
+        else camera_of(scene, settings, f);
+        *member = member_add(&b->wave, gs, nullptr, scene, *settings, f);
+    });
+}
+
+int lr_batch_remove(lr_batch *b, uint32_t member) {
+    return guarded([&] {
+        if (!b) fail(LR_INVALID, "no batch");
+        MemberHost &mh = member_at(&b->wave, member);
+        mh.leaving = true;
+        collect(&b->wave);
+    });
+}
+
+int lr_batch_advance(lr_batch *b, int32_t *more) {
+    return guarded([&] {
+        if (!b || !more) fail(LR_INVALID, "no batch");
+        *more = wave_advance(&b->wave) ? 1 : 0;
+    });
+}
+
+int lr_batch_finish(lr_batch *b) {
+    return guarded([&] {
+        if (!b) fail(LR_INVALID, "no batch");
+        wave_finish(&b->wave);
+    });
+}
+
+int lr_batch_member_info(const lr_batch *b, uint32_t member, uint32_t *samples_done, uint32_t *samples_planned,
+                         uint32_t *samples) {
+    return guarded([&] {
+        if (!b) fail(LR_INVALID, "no batch");
+        const MemberHost &mh = member_at(const_cast<WaveHost *>(&b->wave), member);
+        if (samples_done) *samples_done = mh.done;
+        if (samples_planned) *samples_planned = mh.sample;
+        if (samples) *samples = mh.samples;
+    });
+}
+
+int lr_batch_set_samples(lr_batch *b, uint32_t member, uint32_t samples) {
+    return guarded([&] {
+        if (!b) fail(LR_INVALID, "no batch");
+        if (samples == 0) fail(LR_INVALID, "a render needs samples");
+        member_at(&b->wave, member).samples = samples;
+    });
+}
+
+int lr_batch_image(lr_batch *b, uint32_t member, void **device_rgba) {
+    return guarded([&] {
+        if (!b || !device_rgba) fail(LR_INVALID, "no batch");
+        *device_rgba = member_at(&b->wave, member).dev.image;
+    });
+}
+
+int lr_batch_read(lr_batch *b, uint32_t member, float *rgba, uint64_t count) {
+    return guarded([&] {
+        if (!b || !rgba) fail(LR_INVALID, "no batch");
+        member_read(&b->wave, member, rgba, count);
+    });
+}
+
+int lr_batch_passes(const lr_batch *b, uint64_t *recorded, uint64_t *finished) {
+    return guarded([&] {
+        if (!b) fail(LR_INVALID, "no batch");
+        if (recorded) *recorded = b->wave.recorded;
+        if (finished) *finished = b->wave.retired;
+    });
+}
+
+int lr_batch_kernel_times(lr_batch *b, double out[10]) {
+    return guarded([&] {
+        if (!b || !out) fail(LR_INVALID, "kernel times need ten numbers");
+        wave_kernel_times(&b->wave, out);
+    });
+}
+
+int lr_batch_stats(lr_batch *b, lr_render_stats *out) {
+    return guarded([&] {
+        if (!b || !out) fail(LR_INVALID, "no batch");
+        wave_stats(&b->wave, out);
+    });
+}
+
+void lr_batch_destroy(lr_batch *b) {
+    if (!b) return;
+    wave_destroy(&b->wave);
+    delete b;
 }
 
 }  // extern "C"

@@ -1,0 +1,150 @@
+"""Batches (lr_batch) through the C ABI: every member's image equals, bit for bit, the
+image a Renderer of its own makes of the same scene, frame and settings -- alone or in
+the mix, whatever the pool size, and with members joining and leaving between passes.
+Each path's arithmetic depends only on its member, pixel and sample, and a pixel takes
+its samples in order, so the tolerance is zero."""
+import numpy as np
+import pytest
+
+import luce_render_b200 as lr
+from luce_render_b200 import scenes, testscenes
+
+pytestmark = pytest.mark.gpu
+
+
+def _settings(width, height, samples, bounces, spectral, seed=1, material=None, background=(0.0, 0.0, 0.0)):
+    s = lr.RenderSettings.of(width, height, samples)
+    s.spectral = 1 if spectral else 0
+    s.max_bounces = bounces
+    s.light_tracing = 0.0
+    s.seed = seed
+    s.background = background
+    s.c.material = material if material is not None else lr.OpenPbr.lambert()
+    return s
+
+
+def _cases():
+    """(compiled scene, settings) pairs of uneven sizes, modes and depths."""
+    out = []
+    sc = lr.compile_scene(scenes.cornell_meshes(materials=True), [scenes.cornell_camera()],
+                          [scenes.cornell_light()], scenes.cornell_materials())
+    out.append((sc, _settings(48, 40, 4, 6, False, seed=3)))
+    sc = lr.compile_scene(scenes.furnace_meshes(4), [lr.camera((0.0, 0.0, 0.0))])
+    out.append((sc, _settings(32, 32, 3, 8, True, material=scenes.furnace_material(0.8, 1.0))))
+    meshes, cams, lights, mats = testscenes.emissive_quad_scene()
+    sc = lr.compile_scene(meshes, cams, lights, mats)
+    out.append((sc, _settings(24, 20, 5, 2, True, seed=7, material=lr.OpenPbr.lambert((0.5, 0.5, 0.5)))))
+    meshes, materials, lights, cam = scenes.scene_of_size(20_000, seed=11)
+    sc = lr.compile_scene(meshes, [cam], lights, materials)
+    out.append((sc, _settings(64, 36, 2, 6, False, seed=5, background=(0.1, 0.2, 0.3))))
+    meshes, cams, lights, mats = testscenes.colored_light_scene(kelvin=3200.0)
+    sc = lr.compile_scene(meshes, cams, lights, mats)
+    out.append((sc, _settings(16, 16, 6, 3, True, seed=9)))
+    return out
+
+
+def _alone(ctx, sc, settings):
+    r = lr.Renderer.create(ctx, sc, settings)
+    try:
+        r.finish()
+        assert r.samples_done() == settings.c.samples
+        return r.read()
+    finally:
+        r.destroy()
+
+
+@pytest.fixture(scope="module")
+def cases(ctx):
+    cs = _cases()
+    uploads = [lr.GpuScene.upload(ctx, sc) for sc, _ in cs]
+    alone = [_alone(ctx, sc, s) for sc, s in cs]
+    yield cs, uploads, alone
+    for gs in uploads:
+        gs.destroy()
+    for sc, _ in cs:
+        sc.close()
+
+
+def _bits(img):
+    return np.ascontiguousarray(img, np.float32).view(np.uint32)
+
+
+@pytest.mark.parametrize("pool", [1 << 21, 1500, 333])
+def test_members_equal_their_renderers(ctx, cases, pool):
+    # A pool larger than all films together (one pass a sample for everyone), one that
+    # splits the larger films over passes, and one smaller than every film but the last.
+    cs, uploads, alone = cases
+    b = lr.Batch(ctx, lr.BatchSettings.default(pool=pool, max_bounces=8, capacity=8))
+    try:
+        members = [b.add(gs, sc, s) for gs, (sc, s) in zip(uploads, cs)]
+        b.finish()
+        for m, (sc, s), want in zip(members, cs, alone):
+            assert b.samples_done(m) == s.c.samples
+            got = b.read(m)
+            assert np.array_equal(_bits(got), _bits(want)), m
+        st = b.stats()
+        total_paths = sum(s.c.width * s.c.height * s.c.samples for _, s in cs)
+        assert st.shaded == total_paths
+        if pool >= 1 << 21:
+            assert st.passes == max(s.c.samples for _, s in cs)
+    finally:
+        b.destroy()
+
+
+def test_members_join_and_leave(ctx, cases):
+    cs, uploads, alone = cases
+    b = lr.Batch(ctx, lr.BatchSettings.default(pool=700, max_bounces=8, capacity=3))
+    try:
+        first = b.add(uploads[0], *cs[0])
+        leaving = b.add(uploads[3], *cs[3])
+        for _ in range(5):
+            b.advance()
+        # A member joins while passes are in flight; another leaves part way.
+        late = b.add(uploads[1], *cs[1])
+        for _ in range(3):
+            b.advance()
+        b.remove(leaving)
+        with pytest.raises(lr.RenderError):
+            b.info(leaving)
+        # Its slot is taken again once its passes have finished.
+        again = b.add(uploads[4], *cs[4])
+        b.finish()
+        for m, i in ((first, 0), (late, 1), (again, 4)):
+            assert np.array_equal(_bits(b.read(m)), _bits(alone[i])), i
+    finally:
+        b.destroy()
+
+
+def test_more_samples_later(ctx, cases):
+    # set_samples after a finish continues each pixel's sample sequence.
+    cs, uploads, alone = cases
+    sc, s = cs[2]
+    fewer = _settings(24, 20, 2, 2, True, seed=7, material=lr.OpenPbr.lambert((0.5, 0.5, 0.5)))
+    b = lr.Batch(ctx, lr.BatchSettings.default(pool=100, max_bounces=4, capacity=2))
+    try:
+        m = b.add(uploads[2], sc, fewer)
+        b.finish()
+        assert b.info(m) == (2, 2, 2)
+        b.set_samples(m, s.c.samples)
+        b.finish()
+        assert b.samples_done(m) == s.c.samples
+        assert np.array_equal(_bits(b.read(m)), _bits(alone[2]))
+    finally:
+        b.destroy()
+
+
+def test_batch_limits(ctx, cases):
+    cs, uploads, _ = cases
+    b = lr.Batch(ctx, lr.BatchSettings.default(pool=4096, max_bounces=4, capacity=1))
+    try:
+        with pytest.raises(lr.RenderError) as e:
+            b.add(uploads[0], *cs[0])  # 6 bounces > 4
+        assert e.value.code == 401
+        b.add(uploads[2], *cs[2])
+        with pytest.raises(lr.RenderError) as e:
+            b.add(uploads[4], *cs[4])  # full
+        assert e.value.code == 401
+    finally:
+        b.destroy()
+    with pytest.raises(lr.RenderError):
+        lr.Batch(ctx, lr.BatchSettings.default(pool=0))
