@@ -332,7 +332,7 @@ void lr_renderer_destroy(lr_renderer *renderer);
  * settings makes, whatever else shares the batch. Members may join and leave between
  * passes. All calls on one batch from one host thread. */
 typedef struct {
-    uint32_t pool;        /* paths per pass (at most 4,194,304) */
+    uint32_t pool;        /* paths per pass (at most 8,388,608) */
     uint32_t max_bounces; /* the most bounces any member may ask for */
     uint32_t capacity;    /* the most members at once */
     int32_t profile;      /* as lr_settings.profile */
@@ -361,6 +361,17 @@ int lr_batch_set_samples(lr_batch *batch, uint32_t member, uint32_t samples);
 /* As lr_renderer_image / lr_renderer_read, for one member. */
 int lr_batch_image(lr_batch *batch, uint32_t member, void **device_rgba);
 int lr_batch_read(lr_batch *batch, uint32_t member, float *rgba, uint64_t float_count);
+/* The autotuner: times trial passes (which trace but change no film and move no member
+ * on) for each BVH width (2, 4, 8; a width every member falls back from is skipped)
+ * and pool fill (a quarter, half or all of the pool), on the members as they stand, and
+ * keeps the fastest for the passes that follow. Images do not change, only speed. */
+typedef struct {
+    uint32_t width;      /* the BVH width chosen */
+    uint32_t fill;       /* paths a pass */
+    double paths_per_ms; /* the chosen candidate's measured rate */
+    uint32_t candidates; /* candidates timed */
+} lr_batch_tuning;
+int lr_batch_tune(lr_batch *batch, lr_batch_tuning *out);
 int lr_batch_passes(const lr_batch *batch, uint64_t *recorded, uint64_t *finished);
 int lr_batch_kernel_times(lr_batch *batch, double out[10]);
 int lr_batch_stats(lr_batch *batch, lr_render_stats *out);

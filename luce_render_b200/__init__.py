@@ -187,6 +187,13 @@ class BatchSettings(C.Structure):
         return b
 
 
+class BatchTuning(C.Structure):
+    """lr_batch_tuning: the BVH width and paths a pass the autotuner chose, the chosen
+    candidate's measured rate and how many candidates it timed."""
+    _fields_ = [("width", C.c_uint32), ("fill", C.c_uint32), ("paths_per_ms", C.c_double),
+                ("candidates", C.c_uint32)]
+
+
 _vp, _i32, _u32, _u64, _sz = C.c_void_p, C.c_int32, C.c_uint32, C.c_uint64, C.c_size_t
 _SIGNATURES = {
     "lr_last_error": (C.c_char_p, []),
@@ -248,6 +255,7 @@ _SIGNATURES = {
     "lr_batch_set_samples": (C.c_int, [_vp, _u32, _u32]),
     "lr_batch_image": (C.c_int, [_vp, _u32, C.POINTER(_vp)]),
     "lr_batch_read": (C.c_int, [_vp, _u32, C.POINTER(C.c_float), _u64]),
+    "lr_batch_tune": (C.c_int, [_vp, C.POINTER(BatchTuning)]),
     "lr_batch_passes": (C.c_int, [_vp, C.POINTER(C.c_uint64), C.POINTER(C.c_uint64)]),
     "lr_batch_kernel_times": (C.c_int, [_vp, C.POINTER(C.c_double)]),
     "lr_batch_stats": (C.c_int, [_vp, C.POINTER(RenderStats)]),
@@ -795,6 +803,14 @@ class Batch:
 
     def set_samples(self, member: int, samples: int) -> None:
         _check(lib.lr_batch_set_samples(self.handle, member, samples))
+
+    def tune(self) -> dict:
+        """Autotune BVH width and paths a pass on the members as they stand (images do not
+        change)."""
+        t = BatchTuning()
+        _check(lib.lr_batch_tune(self.handle, C.byref(t)))
+        return {"width": int(t.width), "fill": int(t.fill), "paths_per_ms": float(t.paths_per_ms),
+                "candidates": int(t.candidates)}
 
     def passes(self):
         rec, fin = C.c_uint64(), C.c_uint64()

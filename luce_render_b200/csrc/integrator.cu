@@ -43,10 +43,10 @@ constexpr int kShadeBlock = 128;
 constexpr uint32_t kMaterialStride = 16;  // vec4 rows per material (openpbr.glsl:28)
 constexpr size_t kDefaultPool = 2097152;  // 2^21 paths (integrator.lucb:98)
 // A ray's tag: the path's pool index in the low bits, its segment in the high bits.
-constexpr uint32_t kPathBits = 22;
+constexpr uint32_t kPathBits = 23;
 constexpr uint32_t kPathMask = (1u << kPathBits) - 1u;
-constexpr uint32_t kMaxPool = 1u << kPathBits;             // 4,194,304 paths
-constexpr uint32_t kMaxSegments = 1u << (32 - kPathBits);  // 1,024 segments a pass
+constexpr uint32_t kMaxPool = 1u << kPathBits;             // 8,388,608 paths
+constexpr uint32_t kMaxSegments = 1u << (32 - kPathBits);  // 512 segments a pass
 
 // One member of a wave: everything its paths read, fixed while it is a member.
 struct Member {
@@ -73,8 +73,9 @@ struct Segment {
     uint32_t path_base, convert, reserved0, reserved1;
 };
 
+// `dry`: a trial pass (autotuning) that traces its segments but leaves films alone.
 struct PlanHeader {
-    uint32_t segments, paths, converts, reserved;
+    uint32_t segments, paths, converts, dry;
 };
 
 // A pass's plan: its segments, and the members whose images it brings up to date.
@@ -517,6 +518,7 @@ __global__ void __launch_bounds__(kShadeBlock) finish_kernel(Wave w) {
     const Plan *plan = w.plan;
     const uint32_t paths = plan->head.paths;
     const uint32_t stride = gridDim.x * blockDim.x;
+    if (plan->head.dry) return;
     for (uint32_t path = blockIdx.x * blockDim.x + threadIdx.x; path < paths; path += stride) {
         const Member &m = w.members[plan->seg[segment_of(plan, path)].member];
         const uint32_t pixel = w.path[path].x;
@@ -637,7 +639,6 @@ struct MemberHost {
     lr_gpu_scene *owned = nullptr;  // a renderer's own upload (null when borrowed)
     uint32_t samples = 0, sample = 0, next_pixel = 0, done = 0;
     uint32_t max_bounces = 0;
-    TraversalChoice traversal{2, 32};
     uint64_t last_pass = 0;  // the last pass (plus one) that traced it; 0: none
 };
 
@@ -673,6 +674,10 @@ struct WaveHost {
     std::deque<PassRecord> in_flight;
     double kernel_ms[10] = {0};
     uint32_t rotate = 0;  // the member the next plan starts from
+    // Tunables (lr_batch_tune): the BVH width asked of every member (0: the default) and
+    // the most paths a pass takes.
+    int width = 0;
+    uint32_t fill = 0;
 };
 
 namespace {
@@ -896,7 +901,6 @@ uint32_t member_add(WaveHost *h, const lr_gpu_scene *gs, lr_gpu_scene *owned, co
     mh.samples = settings.samples;
     mh.sample = mh.next_pixel = mh.done = 0;
     mh.max_bounces = settings.max_bounces;
-    mh.traversal = choose_traversal(gs->scene, 0);
     mh.last_pass = 0;
     return index;
 }
@@ -914,6 +918,9 @@ void collect(WaveHost *h) {
 }
 
 bool has_work(const MemberHost &mh) { return mh.used && !mh.leaving && mh.sample < mh.samples; }
+
+// Paths in the plan of the pass launched last.
+uint64_t h_plan_paths(WaveHost *h) { return h->h_plan[(h->recorded - 1) & 1]->head.paths; }
 
 // Retires the oldest pass in flight if it has finished (integrator.lucb:622-645).
 bool retire_one(WaveHost *h, bool wait) {
@@ -950,9 +957,11 @@ void settle(WaveHost *h) {
 }
 
 // Plans and launches one pass: each member with work left adds its next segment, in
-// turn from `rotate`, until the pool is full. A member takes one segment a pass at
-// most, so a pixel never gets two samples in one pass. Returns false with no work.
-bool launch_pass(WaveHost *h) {
+// turn from `rotate`, until the pass holds `fill` paths. A member takes one segment a
+// pass at most, so a pixel never gets two samples in one pass. A dry pass (autotuning)
+// plans the same way but moves no member on and leaves the films alone. Returns false
+// with no work.
+bool launch_pass(WaveHost *h, bool dry = false) {
     Plan *staging = h->h_plan[h->recorded & 1];
     Segment *seg = staging->seg;
     uint32_t n = 0, used = 0, converts = 0;
@@ -961,33 +970,37 @@ bool launch_pass(WaveHost *h) {
     PassRecord rec;
     rec.number = h->recorded;
     const uint32_t cap = h->capacity;
+    const uint32_t fill = h->fill ? std::min(h->fill, h->pool) : h->pool;
     uint32_t last = h->rotate;
-    for (uint32_t step = 0; step < cap && used < h->pool && n < kMaxSegments; step++) {
+    for (uint32_t step = 0; step < cap && used < fill && n < kMaxSegments; step++) {
         const uint32_t index = (h->rotate + step) % cap;
         MemberHost &mh = h->members[index];
         if (!has_work(mh)) continue;
         const uint64_t left = mh.dev.pixels - mh.next_pixel;
-        const uint32_t count = (uint32_t)std::min<uint64_t>(left, h->pool - used);
-        const bool ends = count == left;
+        const uint32_t count = (uint32_t)std::min<uint64_t>(left, fill - used);
+        const bool ends = count == left && !dry;
         seg[n] = Segment{index, mh.next_pixel, count, mh.sample, used, ends ? 1u : 0u, 0u, 0u};
         rec.members.push_back({index, ends});
         if (ends) staging->convert[converts++] = index;
         n++;
         used += count;
-        if (ends) {
-            mh.sample++;
-            mh.next_pixel = 0;
-        } else {
-            mh.next_pixel += count;
+        if (!dry) {
+            if (count == left) {
+                mh.sample++;
+                mh.next_pixel = 0;
+            } else {
+                mh.next_pixel += count;
+            }
         }
         mh.last_pass = h->recorded + 1;
-        if (width == 0) width = mh.traversal.width;
-        else if (width != mh.traversal.width) mixed = true;
-        stack = std::max(stack, mh.traversal.stack);
+        const TraversalChoice c = choose_traversal(mh.dev.scene, h->width);
+        if (width == 0) width = c.width;
+        else if (width != c.width) mixed = true;
+        stack = std::max(stack, c.stack);
         last = index;
     }
     if (n == 0) return false;
-    h->rotate = (last + 1) % cap;
+    if (!dry) h->rotate = (last + 1) % cap;
     // One traversal variant serves the pass: the members' common width with the deepest
     // stack among them, or the BVH2 when their widths differ.
     if (mixed) {
@@ -999,7 +1012,7 @@ bool launch_pass(WaveHost *h) {
         }
     }
     const int variant = width * 1000 + stack;
-    staging->head = PlanHeader{n, used, converts, 0u};
+    staging->head = PlanHeader{n, used, converts, dry ? 1u : 0u};
     cudaStream_t stream = h->ctx->stream;
     WaveHost::Exec &ex = exec_for(h, variant);
     // The header and convert list, then the segments in use.
@@ -1024,6 +1037,66 @@ bool wave_advance(WaveHost *h) {
     if (h->in_flight.size() >= 2) return true;
     if (launch_pass(h)) return true;
     return !h->in_flight.empty();
+}
+
+// Times dry passes of every candidate (BVH width, paths a pass) on the members as they
+// stand and keeps the fastest.
+void wave_tune(WaveHost *h, lr_batch_tuning *out) {
+    settle(h);
+    if (!std::any_of(h->members.begin(), h->members.end(), has_work))
+        fail(LR_INVALID, "tuning needs members with samples to come");
+    cudaStream_t stream = h->ctx->stream;
+    cudaEvent_t a, b;
+    LR_CUDA(cudaEventCreate(&a));
+    LR_CUDA(cudaEventCreate(&b));
+    double best = -1.0;
+    int best_width = 2;
+    uint32_t best_fill = h->pool, tried = 0;
+    std::vector<std::vector<int>> seen;
+    for (int width : {2, 4, 8}) {
+        // A width every member falls back from is a width already tried.
+        std::vector<int> got;
+        for (auto &mh : h->members)
+            if (has_work(mh)) got.push_back(choose_traversal(mh.dev.scene, width).width * 1000 +
+                                            choose_traversal(mh.dev.scene, width).stack);
+        if (std::find(seen.begin(), seen.end(), got) != seen.end()) continue;
+        seen.push_back(got);
+        for (uint32_t fill : {h->pool / 4, h->pool / 2, h->pool}) {
+            if (fill == 0) continue;
+            h->width = width;
+            h->fill = fill;
+            launch_pass(h, true);  // warm: builds the variant's graph
+            settle(h);
+            uint64_t paths = 0;
+            LR_CUDA(cudaEventRecord(a, stream));
+            for (int i = 0; i < 2; i++) {
+                launch_pass(h, true);
+                paths += h_plan_paths(h);
+            }
+            LR_CUDA(cudaEventRecord(b, stream));
+            LR_CUDA(cudaEventSynchronize(b));
+            settle(h);
+            float ms = 0.0f;
+            LR_CUDA(cudaEventElapsedTime(&ms, a, b));
+            const double rate = (double)paths / std::max(1e-3f, ms);
+            tried++;
+            if (rate > best) {
+                best = rate;
+                best_width = width;
+                best_fill = fill;
+            }
+        }
+    }
+    cudaEventDestroy(a);
+    cudaEventDestroy(b);
+    h->width = best_width;
+    h->fill = best_fill;
+    if (out) {
+        out->width = (uint32_t)best_width;
+        out->fill = best_fill;
+        out->paths_per_ms = best;
+        out->candidates = tried;
+    }
 }
 
 void wave_finish(WaveHost *h) {
@@ -1122,7 +1195,7 @@ void create(lr_context *ctx, const lr_scene *scene, const lr_settings &settings,
         wave_create(&r->wave, ctx, pool, settings.max_bounces + 1, 1, settings.profile);
         member_add(&r->wave, gs, gs, scene, settings, frame);
         // The graph for the scene's traversal variant, made now rather than at the first pass.
-        const TraversalChoice c = r->wave.members[0].traversal;
+        const TraversalChoice c = choose_traversal(gs->scene, 0);
         exec_for(&r->wave, c.width * 1000 + c.stack);
     } catch (...) {
         const bool owned = !r->wave.members.empty() && r->wave.members[0].used;
@@ -1353,6 +1426,13 @@ int lr_batch_read(lr_batch *b, uint32_t member, float *rgba, uint64_t count) {
     return guarded([&] {
         if (!b || !rgba) fail(LR_INVALID, "no batch");
         member_read(&b->wave, member, rgba, count);
+    });
+}
+
+int lr_batch_tune(lr_batch *b, lr_batch_tuning *out) {
+    return guarded([&] {
+        if (!b) fail(LR_INVALID, "no batch");
+        wave_tune(&b->wave, out);
     });
 }
 

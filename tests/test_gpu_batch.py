@@ -148,3 +148,24 @@ def test_batch_limits(ctx, cases):
         b.destroy()
     with pytest.raises(lr.RenderError):
         lr.Batch(ctx, lr.BatchSettings.default(pool=0))
+
+
+def test_tuning_changes_speed_not_images(ctx, cases):
+    cs, uploads, alone = cases
+    b = lr.Batch(ctx, lr.BatchSettings.default(pool=2048, max_bounces=8, capacity=8))
+    try:
+        members = [b.add(gs, sc, s) for gs, (sc, s) in zip(uploads, cs)]
+        for _ in range(3):
+            b.advance()
+        t = b.tune()
+        assert t["width"] in (2, 4, 8) and t["fill"] in (512, 1024, 2048)
+        assert t["candidates"] >= 3 and t["paths_per_ms"] > 0
+        st = b.stats()
+        b.finish()
+        for m, want in zip(members, alone):
+            assert np.array_equal(_bits(b.read(m)), _bits(want)), m
+        # Trial passes add no paths to the count of finished work.
+        assert b.stats().shaded == sum(s.c.width * s.c.height * s.c.samples for _, s in cs)
+        assert st.shaded <= b.stats().shaded
+    finally:
+        b.destroy()
