@@ -17,6 +17,7 @@ from __future__ import annotations
 
 import argparse
 import json
+import math
 import os
 import statistics
 import subprocess
@@ -41,6 +42,10 @@ def parse():
     p.add_argument("--warmup", type=int, default=5)
     p.add_argument("--impl", default="ours", choices=["ours", "reference"])
     p.add_argument("--rgb", action="store_true", help="the RGB build instead of the spectral one")
+    p.add_argument("--skip-batched", action="store_true", help="leave out the 64-scene batched comparison")
+    p.add_argument("--skip-served", action="store_true", help="leave out the served arrival stream")
+    p.add_argument("--served-seconds", type=float, default=10.0,
+                   help="length of the served arrival stream (the full workload is 60)")
     return p.parse_args()
 
 
@@ -199,6 +204,174 @@ class CpuReference:
         return total_rays / seconds / 1e6, seconds, total_rays
 
 
+BATCH_SPP, BATCH_BOUNCES, BATCH_POOL = 32, 6, 1 << 23
+
+
+def batch_cases(lr, scenes):
+    """The 64 scenes of the batched and served workloads with their plan entries."""
+    plan = scenes.batch_plan()
+    cases = []
+    for i, p in enumerate(plan):
+        meshes, materials, lights, cam = scenes.scene_of_size(p["triangles"], seed=0xBA7C4 + i)
+        cases.append((lr.compile_scene(meshes, [cam], lights, materials), p))
+    return cases
+
+
+def percentiles(values):
+    if not values:
+        return {"count": 0, "p50_ms": None, "p99_ms": None}
+    import numpy as np
+
+    v = np.asarray(values, np.float64) * 1e3
+    return {"count": len(values), "p50_ms": float(np.percentile(v, 50)), "p99_ms": float(np.percentile(v, 99)),
+            "max_ms": float(v.max())}
+
+
+def served(lr, scenes, dist, seconds: float):
+    """The served workload: a Poisson stream (200 requests/s, seed 0x5E4E) of 80% render
+    sessions (a scene of the batched workload at its film size, spp uniform in 16..256,
+    depth 6) and 20% probes (1k to 2M pixel rays, log-uniform, through the scene's
+    camera) into one Server (150 GB budget, 128 live sessions, pool 2^22). Latency is
+    the server's own host clock from submission: probes to their result in pinned host
+    memory, sessions to their first image and to completion."""
+    import numpy as np
+
+    cases = batch_cases(lr, scenes)
+    rng = np.random.default_rng(0x5E4E)
+    arrivals, t = [], 0.0
+    while True:
+        t += rng.exponential(1.0 / 200.0)
+        if t >= seconds:
+            break
+        if rng.random() < 0.2:
+            px = int(round(math.exp(rng.uniform(math.log(1000.0), math.log(2_000_000.0)))))
+            w = max(1, int(round(math.sqrt(px * 16.0 / 9.0))))
+            arrivals.append((t, "probe", int(rng.integers(len(cases))), w, max(1, px // w)))
+        else:
+            arrivals.append((t, "render", int(rng.integers(len(cases))), int(rng.integers(16, 257)), 0))
+    server = lr.Server(lr.ServerSettings.default(budget_bytes=150 * 10**9, capacity=128, pool=1 << 22,
+                                                 max_bounces=BATCH_BOUNCES))
+    ids = [server.add_scene(sc) for sc, _ in cases]
+    for sid in ids:  # the catalog starts resident, as a running service keeps it
+        server.preload(sid)
+    ring = [(lr.PinnedArray((2_000_000,), np.uint32), lr.PinnedArray((2_000_000,), np.float32)) for _ in range(32)]
+    submitted = []
+    dist.barrier()
+    start = time.perf_counter()
+    for k, (at, kind, scene, a, b) in enumerate(arrivals):
+        while time.perf_counter() - start < at:
+            time.sleep(min(2e-4, max(0.0, at - (time.perf_counter() - start))))
+        sc, p = cases[scene]
+        if kind == "probe":
+            faces, distances = ring[k % len(ring)]
+            frame = lr.ray_frame(sc.camera(), a, b)
+            submitted.append(("probe", server.submit_probe(ids[scene], frame, faces.array, distances.array)))
+        else:
+            s = lr.RenderSettings.of(p["side"], p["side"], a)
+            s.spectral = 1 if p["spectral"] else 0
+            s.max_bounces = BATCH_BOUNCES
+            s.light_tracing = 0.0
+            submitted.append(("render", server.submit_render(ids[scene], s)))
+    window = time.perf_counter() - start
+    stats_window = server.stats()
+    # Probes still queued finish; sessions are cut at the end of the stream.
+    for kind, rid in submitted:
+        if kind == "probe":
+            try:
+                server.wait(rid, 30.0)
+            except lr.RenderError:
+                pass
+    infos = [(kind, server.info(rid)) for kind, rid in submitted]
+    server.destroy()
+    for f, d in ring:
+        f.close()
+        d.close()
+    for sc, _ in cases:
+        sc.close()
+    probes = [i for k, i in infos if k == "probe"]
+    renders = [i for k, i in infos if k == "render"]
+    done_probes = [i["finished"] - i["submitted"] for i in probes if i["state"] == "done"]
+    first_images = [i["first"] - i["submitted"] for i in renders if i["first"] >= 0]
+    completed = [i["finished"] - i["submitted"] for i in renders if i["state"] == "done"]
+    demand = sum(i["pixels"] * i["samples"] for i in renders)
+    return {
+        "workload": ("Poisson arrivals at 200 requests/s (seed 0x5E4E): 80% render sessions of the batched "
+                     "workload's scenes at their film sizes, 16..256 spp, depth 6; 20% probes of 1k..2M pixel rays "
+                     "(log-uniform); budget 150 GB, 128 live sessions, pool 2^22, LRU eviction of idle scenes"),
+        "seconds": window, "requests": len(submitted),
+        "probe_latency": percentiles(done_probes),
+        "session_first_image": percentiles(first_images),
+        "session_completion": percentiles(completed),
+        "sessions": {"submitted": len(renders), "admitted": sum(1 for i in renders if i["admitted"] >= 0),
+                     "first_image": len(first_images), "done": len(completed)},
+        "probes": {"submitted": len(probes), "done": len(done_probes)},
+        "render_msamples_s": stats_window["pixel_samples"] / window / 1e6,
+        "probe_mrays_s": stats_window["probe_rays"] / window / 1e6,
+        "demand_msamples_s": demand / window / 1e6,
+        "uploads": stats_window["uploads"], "evictions": stats_window["evictions"],
+        "queued_at_end": stats_window["queued"], "live_at_end": stats_window["live"],
+        "timing": "host steady clock of the server, from submission; the stream is cut at its end",
+    }
+
+
+def batched(lr, scenes, ctx, dist):
+    """The batched workload: 64 scenes of the incoherent generator (triangles log-normal,
+    median 20k, clipped to [1k, 500k]; films 128^2..1024^2; half spectral), 32 spp, depth
+    6. Aggregate pixel-samples per second of the plain loop (one Renderer after another)
+    against one tuned Batch of all 64, device-timed on the context's stream, with every
+    image compared bit for bit (identical images have equal RMSE against any reference)."""
+    import numpy as np
+
+    cases = []
+    for sc, p in batch_cases(lr, scenes):
+        s = lr.RenderSettings.of(p["side"], p["side"], BATCH_SPP)
+        s.spectral = 1 if p["spectral"] else 0
+        s.max_bounces = BATCH_BOUNCES
+        s.light_tracing = 0.0
+        cases.append((sc, s))
+    samples = sum(s.c.width * s.c.height * BATCH_SPP for _, s in cases)
+    triangles = sum(sc.triangle_count() for sc, _ in cases)
+    renderers = [lr.Renderer.create(ctx, sc, s) for sc, s in cases]
+    dist.barrier()
+    ctx.synchronize()
+    ctx.timer_start()
+    for r in renderers:
+        r.finish()
+    loop_ms = dist.max(ctx.timer_stop())
+    alone = [r.read() for r in renderers]
+    for r in renderers:
+        r.destroy()
+    uploads = [lr.GpuScene.upload(ctx, sc) for sc, _ in cases]
+    b = lr.Batch(ctx, lr.BatchSettings.default(pool=BATCH_POOL, max_bounces=BATCH_BOUNCES, capacity=len(cases)))
+    members = [b.add(gs, sc, s) for gs, (sc, s) in zip(uploads, cases)]
+    tuning = b.tune()
+    dist.barrier()
+    ctx.synchronize()
+    ctx.timer_start()
+    b.finish()
+    batch_ms = dist.max(ctx.timer_stop())
+    identical = all(np.array_equal(b.read(m).view(np.uint32), img.view(np.uint32)) for m, img in zip(members, alone))
+    passes = b.stats().passes
+    b.destroy()
+    for gs in uploads:
+        gs.destroy()
+    for sc, _ in cases:
+        sc.close()
+    loop_rate = dist.sum(samples) / (loop_ms / 1e3) / 1e6
+    batch_rate = dist.sum(samples) / (batch_ms / 1e3) / 1e6
+    return {
+        "workload": ("64 scenes of the incoherent generator, triangles log-normal (median 20k, clipped to "
+                     f"[1k, 500k]; {triangles:,} in all), films "
+                     "128^2/256^2/512^2/1024^2, half spectral, 32 spp, depth 6, seed 0xBA7C4"),
+        "unit": "Msamples/s (pixel-samples, all scenes)",
+        "pixel_samples": samples,
+        "loop_ms": loop_ms, "batched_ms": batch_ms,
+        "loop_value": loop_rate, "batched_value": batch_rate, "speedup": loop_ms / batch_ms,
+        "identical_images": identical, "pool": BATCH_POOL, "passes": passes, "tuning": tuning,
+        "timing": "device (CUDA events on the context stream), renderers and batch members made beforehand",
+    }
+
+
 def main():
     args = parse()
     spectral = not args.rgb
@@ -298,6 +471,9 @@ def main():
     e2e_rays = dist.sum((e1.closest_rays - e0.closest_rays) + (e1.shadow_rays - e0.shadow_rays))
     e2e_value = e2e_rays / dist.max(e2e_s) / 1e6
 
+    batch_info = None if args.skip_batched else batched(lr, scenes, ctx, dist)
+    served_info = None if args.skip_served else served(lr, scenes, dist, args.served_seconds)
+
     cpu = None
     if dist.rank == 0 and dist.world == 1:
         from oracle import oracle
@@ -329,6 +505,8 @@ def main():
                     "d2h_bytes_per_step": WIDTH * HEIGHT * 16},
             "gpu_launches": K * (1 + 3 * (BOUNCES + 1) + 2),
             "clocks": clock_info,
+            "batched": batch_info,
+            "served": served_info,
         }
         print(json.dumps(line))
     ctx.close()

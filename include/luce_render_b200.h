@@ -46,6 +46,10 @@ typedef struct lr_context lr_context;
 
 /* gpu.Device.open (used at tests/gpu/main.lucb:18): a context on CUDA device `device`. */
 int lr_context_create(int device, lr_context **out);
+/* The same with a stream priority: 0 normal, 1 the device's highest (work queued on a
+ * high-priority stream starts ahead of normal work waiting for the GPU; a serving loop
+ * runs its probes there). */
+int lr_context_create_ex(int device, int priority, lr_context **out);
 void lr_context_destroy(lr_context *ctx);
 /* Wait for all work queued on the context's stream. */
 int lr_context_synchronize(lr_context *ctx);
@@ -342,8 +346,8 @@ typedef struct lr_batch lr_batch;
 /* pool 2^21, max_bounces 12, capacity 256, profile 0. */
 void lr_batch_settings_default(lr_batch_settings *out);
 int lr_batch_create(lr_context *ctx, const lr_batch_settings *settings, lr_batch **out);
-/* Adds `scene` (uploaded as `gpu_scene` through the batch's context; both stay the
- * caller's and must outlive the member) with `settings`, seen through `frame` or, when
+/* Adds `scene` (uploaded as `gpu_scene` to the batch's device; both stay the caller's
+ * and must outlive the member) with `settings`, seen through `frame` or, when
  * it is NULL, through the camera settings name. *member: its index. */
 int lr_batch_add(lr_batch *batch, const lr_gpu_scene *gpu_scene, const lr_scene *scene,
                  const lr_settings *settings, const lr_frame *frame, uint32_t *member);
@@ -354,6 +358,9 @@ int lr_batch_remove(lr_batch *batch, uint32_t member);
 int lr_batch_advance(lr_batch *batch, int32_t *more);
 /* Runs every remaining pass and waits. */
 int lr_batch_finish(lr_batch *batch);
+/* Waits for the oldest pass in flight, if any, and retires it; *in_flight: passes still
+ * in flight after. */
+int lr_batch_wait(lr_batch *batch, int32_t *in_flight);
 /* Samples finished, samples planned so far and samples asked for. Any may be NULL. */
 int lr_batch_member_info(const lr_batch *batch, uint32_t member, uint32_t *samples_done,
                          uint32_t *samples_planned, uint32_t *samples);
@@ -376,6 +383,79 @@ int lr_batch_passes(const lr_batch *batch, uint64_t *recorded, uint64_t *finishe
 int lr_batch_kernel_times(lr_batch *batch, double out[10]);
 int lr_batch_stats(lr_batch *batch, lr_render_stats *out);
 void lr_batch_destroy(lr_batch *batch);
+
+/* ---- Serving: sessions and probes as they arrive ----------------------------------
+ * No counterpart in the reference. A server owns a batch on one device and two host
+ * threads: a render thread that admits queued render sessions, in arrival order, while
+ * a live slot is free and the device memory budget holds the session's scene (uploaded
+ * on first use, kept resident, evicted least recently used when idle and room is
+ * needed) and its film, and advances every live session in shared passes; and a probe
+ * thread that runs probe queries on a high-priority stream (without device allocation
+ * up to LR_PROBE_STATIC_PIXELS pixels). Submitting never waits. A session's image is,
+ * bit for bit, what an lr_renderer of the same scene and settings makes; a probe's
+ * result is lr_probe's. Times are seconds on the host's steady clock since the server
+ * started. */
+typedef struct {
+    int32_t device;
+    uint64_t budget_bytes; /* device memory for resident scenes, live sessions and the pool */
+    uint32_t capacity;     /* live sessions at once (1 to 512) */
+    uint32_t pool;         /* paths a pass */
+    uint32_t max_bounces;  /* the most bounces a session may ask for */
+    int32_t probe_priority; /* 1: probes on the device's highest-priority stream */
+} lr_server_settings;
+typedef struct lr_server lr_server;
+
+#define LR_REQUEST_RENDER 0
+#define LR_REQUEST_PROBE 1
+#define LR_REQUEST_QUEUED 0
+#define LR_REQUEST_RUNNING 1
+#define LR_REQUEST_DONE 2
+#define LR_REQUEST_FAILED 3
+
+typedef struct {
+    int32_t kind, state, status;
+    uint32_t scene;
+    uint64_t pixels;
+    uint32_t samples, samples_done;
+    /* submitted; admitted (a live slot, or the probe thread took it); first image (the
+     * first sample of every pixel finished); finished. -1: not yet. */
+    double submitted, admitted, first, finished;
+} lr_request_info;
+
+typedef struct {
+    uint64_t sessions_done, probes_done, failed;
+    uint64_t pixel_samples; /* pixel-samples finished by render sessions */
+    uint64_t probe_rays;
+    uint64_t uploads, evictions;
+    uint64_t queued, live, scenes_resident;
+    uint64_t bytes_in_use;  /* resident scenes, live sessions and the pool */
+    double seconds;         /* since the server started */
+} lr_server_stats;
+
+/* device 0, budget 150 GB, capacity 128, pool 2^22, max_bounces 12, probe_priority 1. */
+void lr_server_settings_default(lr_server_settings *out);
+int lr_server_create(const lr_server_settings *settings, lr_server **out);
+/* Registers a compiled scene (the caller's; it must outlive the server). */
+int lr_server_add_scene(lr_server *server, const lr_scene *scene, uint32_t *scene_id);
+/* Uploads the scene now (on the caller's thread) rather than at its first request, if
+ * the budget has room (LR_LIMIT otherwise); it stays resident until evicted. */
+int lr_server_preload(lr_server *server, uint32_t scene_id);
+/* A progressive render of `settings.samples` samples through `frame` (NULL: the camera
+ * the settings name); when `rgba` is not NULL the finished image is copied there
+ * (width*height*4 floats). The session leaves the GPU when it finishes. */
+int lr_server_submit_render(lr_server *server, uint32_t scene_id, const lr_settings *settings,
+                            const lr_frame *frame, float *rgba, uint64_t *request);
+/* A probe (as lr_probe) into the caller's buffers, which must stay valid until it is
+ * finished; pinned host memory keeps the copy short. */
+int lr_server_submit_probe(lr_server *server, uint32_t scene_id, const lr_frame *frame,
+                           uint32_t flags, uint32_t *faces, float *distances, uint64_t *request);
+int lr_server_request_info(lr_server *server, uint64_t request, lr_request_info *out);
+/* Waits up to `timeout_seconds` for the request: LR_OK when it finished, LR_TIMEOUT, or
+ * the request's own failure. */
+int lr_server_wait(lr_server *server, uint64_t request, double timeout_seconds);
+int lr_server_stats_get(lr_server *server, lr_server_stats *out);
+/* Stops both threads (requests not finished end with LR_STOPPED) and frees everything. */
+void lr_server_destroy(lr_server *server);
 
 #if defined(__GNUC__)
 #pragma GCC visibility pop

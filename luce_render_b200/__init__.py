@@ -194,6 +194,35 @@ class BatchTuning(C.Structure):
                 ("candidates", C.c_uint32)]
 
 
+class ServerSettings(C.Structure):
+    """lr_server_settings."""
+    _fields_ = [("device", C.c_int32), ("budget_bytes", C.c_uint64), ("capacity", C.c_uint32),
+                ("pool", C.c_uint32), ("max_bounces", C.c_uint32), ("probe_priority", C.c_int32)]
+
+    @staticmethod
+    def default(**overrides) -> "ServerSettings":
+        s = ServerSettings()
+        lib.lr_server_settings_default(C.byref(s))
+        for key, value in overrides.items():
+            setattr(s, key, value)
+        return s
+
+
+class RequestInfo(C.Structure):
+    """lr_request_info."""
+    _fields_ = [("kind", C.c_int32), ("state", C.c_int32), ("status", C.c_int32), ("scene", C.c_uint32),
+                ("pixels", C.c_uint64), ("samples", C.c_uint32), ("samples_done", C.c_uint32),
+                ("submitted", C.c_double), ("admitted", C.c_double), ("first", C.c_double),
+                ("finished", C.c_double)]
+
+
+class ServerStats(C.Structure):
+    """lr_server_stats."""
+    _fields_ = [(n, C.c_uint64) for n in ("sessions_done", "probes_done", "failed", "pixel_samples", "probe_rays",
+                                          "uploads", "evictions", "queued", "live", "scenes_resident",
+                                          "bytes_in_use")] + [("seconds", C.c_double)]
+
+
 _vp, _i32, _u32, _u64, _sz = C.c_void_p, C.c_int32, C.c_uint32, C.c_uint64, C.c_size_t
 _SIGNATURES = {
     "lr_last_error": (C.c_char_p, []),
@@ -260,6 +289,20 @@ _SIGNATURES = {
     "lr_batch_kernel_times": (C.c_int, [_vp, C.POINTER(C.c_double)]),
     "lr_batch_stats": (C.c_int, [_vp, C.POINTER(RenderStats)]),
     "lr_batch_destroy": (None, [_vp]),
+    "lr_context_create_ex": (C.c_int, [C.c_int, C.c_int, C.POINTER(_vp)]),
+    "lr_batch_wait": (C.c_int, [_vp, C.POINTER(_i32)]),
+    "lr_server_settings_default": (None, [C.POINTER(ServerSettings)]),
+    "lr_server_create": (C.c_int, [C.POINTER(ServerSettings), C.POINTER(_vp)]),
+    "lr_server_add_scene": (C.c_int, [_vp, _vp, C.POINTER(C.c_uint32)]),
+    "lr_server_preload": (C.c_int, [_vp, _u32]),
+    "lr_server_submit_render": (C.c_int, [_vp, _u32, C.POINTER(Settings), C.POINTER(Frame), C.POINTER(C.c_float),
+                                          C.POINTER(C.c_uint64)]),
+    "lr_server_submit_probe": (C.c_int, [_vp, _u32, C.POINTER(Frame), _u32, C.POINTER(C.c_uint32),
+                                         C.POINTER(C.c_float), C.POINTER(C.c_uint64)]),
+    "lr_server_request_info": (C.c_int, [_vp, _u64, C.POINTER(RequestInfo)]),
+    "lr_server_wait": (C.c_int, [_vp, _u64, C.c_double]),
+    "lr_server_stats_get": (C.c_int, [_vp, C.POINTER(ServerStats)]),
+    "lr_server_destroy": (None, [_vp]),
 }
 
 for _name, (_res, _args) in _SIGNATURES.items():
@@ -848,6 +891,85 @@ class Batch:
         if self.handle:
             lib.lr_batch_destroy(self.handle)
             self.handle = None
+
+    close = destroy
+
+    def __del__(self):
+        try:
+            self.destroy()
+        except Exception:
+            pass
+
+
+REQUEST_STATES = {0: "queued", 1: "running", 2: "done", 3: "failed"}
+
+
+class Server:
+    """The serving loop (lr_server): render sessions and probe queries submitted at any
+    time, admitted by slots and memory budget, advanced together on one GPU."""
+
+    def __init__(self, settings: ServerSettings | None = None):
+        self.handle = None
+        self._keep = {}    # buffers and scenes the library holds pointers to
+        self._scenes = []
+        h = _vp()
+        _check(lib.lr_server_create(C.byref(settings or ServerSettings.default()), C.byref(h)))
+        self.handle = h
+
+    def add_scene(self, scene: CompiledScene) -> int:
+        sid = C.c_uint32()
+        _check(lib.lr_server_add_scene(self.handle, scene.handle, C.byref(sid)))
+        self._scenes.append(scene)
+        return int(sid.value)
+
+    def preload(self, scene_id: int) -> None:
+        _check(lib.lr_server_preload(self.handle, scene_id))
+
+    def submit_render(self, scene_id: int, settings: RenderSettings, frame: Frame | None = None,
+                      rgba: np.ndarray | None = None) -> int:
+        if rgba is not None and (rgba.dtype != np.float32 or not rgba.flags.c_contiguous):
+            raise RenderError(INVALID, "an image buffer is contiguous float32")
+        rid = C.c_uint64()
+        _check(lib.lr_server_submit_render(self.handle, scene_id, C.byref(settings.c),
+                                           C.byref(frame) if frame is not None else None,
+                                           _fptr(rgba) if rgba is not None else None, C.byref(rid)))
+        if rgba is not None:
+            self._keep[int(rid.value)] = (rgba,)
+        return int(rid.value)
+
+    def submit_probe(self, scene_id: int, frame: Frame, faces: np.ndarray, distances: np.ndarray,
+                     reference: bool = False) -> int:
+        n = int(frame.width) * int(frame.height)
+        if faces.dtype != np.uint32 or distances.dtype != np.float32 or faces.size < n or distances.size < n:
+            raise RenderError(INVALID, "a probe needs one result per pixel")
+        rid = C.c_uint64()
+        _check(lib.lr_server_submit_probe(self.handle, scene_id, C.byref(frame), TRACE_REFERENCE if reference else 0,
+                                          _uptr(faces), _fptr(distances), C.byref(rid)))
+        self._keep[int(rid.value)] = (faces, distances)
+        return int(rid.value)
+
+    def info(self, request: int) -> dict:
+        i = RequestInfo()
+        _check(lib.lr_server_request_info(self.handle, request, C.byref(i)))
+        return {"kind": "probe" if i.kind == 1 else "render", "state": REQUEST_STATES.get(i.state, "?"),
+                "status": int(i.status), "scene": int(i.scene), "pixels": int(i.pixels), "samples": int(i.samples),
+                "samples_done": int(i.samples_done), "submitted": i.submitted, "admitted": i.admitted,
+                "first": i.first, "finished": i.finished}
+
+    def wait(self, request: int, timeout: float = 600.0) -> None:
+        _check(lib.lr_server_wait(self.handle, request, float(timeout)))
+        self._keep.pop(request, None)
+
+    def stats(self) -> dict:
+        s = ServerStats()
+        _check(lib.lr_server_stats_get(self.handle, C.byref(s)))
+        return {name: getattr(s, name) for name, _ in ServerStats._fields_}
+
+    def destroy(self) -> None:
+        if self.handle:
+            lib.lr_server_destroy(self.handle)
+            self.handle = None
+            self._keep.clear()
 
     close = destroy
 

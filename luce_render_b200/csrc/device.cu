@@ -306,10 +306,13 @@ extern "C" {
 const char *lr_last_error(void) { return lr::g_last_error.c_str(); }
 const char *lr_version(void) { return "luce_render_b200 0.1 (sm_100a)"; }
 
-int lr_context_create(int device, lr_context **out) {
+int lr_context_create(int device, lr_context **out) { return lr_context_create_ex(device, 0, out); }
+
+int lr_context_create_ex(int device, int priority, lr_context **out) {
     return guarded([&] {
         if (!out) fail(LR_INVALID, "no place for the context");
         *out = nullptr;
+        if (priority != 0 && priority != 1) fail(LR_INVALID, "a context's priority is 0 (normal) or 1 (high)");
         int count = 0;
         LR_CUDA(cudaGetDeviceCount(&count));
         if (device < 0 || device >= count) fail(LR_INVALID, "no such CUDA device");
@@ -317,7 +320,9 @@ int lr_context_create(int device, lr_context **out) {
         auto ctx = std::make_unique<lr_context>();
         ctx->device = device;
         LR_CUDA(cudaDeviceGetAttribute(&ctx->sm_count, cudaDevAttrMultiProcessorCount, device));
-        LR_CUDA(cudaStreamCreateWithFlags(&ctx->stream, cudaStreamNonBlocking));
+        int least = 0, greatest = 0;
+        LR_CUDA(cudaDeviceGetStreamPriorityRange(&least, &greatest));
+        LR_CUDA(cudaStreamCreateWithPriority(&ctx->stream, cudaStreamNonBlocking, priority ? greatest : least));
         LR_CUDA(cudaEventCreate(&ctx->start));
         LR_CUDA(cudaEventCreate(&ctx->stop));
         // Status words at byte 0, traversal counts at byte 16.

@@ -25,6 +25,7 @@
 // the reference's bands; lr_batch is a wave of many members that come and go.
 #include <algorithm>
 #include <cstddef>
+#include <cstring>
 #include <deque>
 #include <map>
 #include <memory>
@@ -605,6 +606,35 @@ struct Layout {
     }
 };
 
+// Pinned host memory that stages uploads, so that they queue on a stream without
+// waiting for the work ahead of them; reused once its last copies have run.
+struct Staging {
+    char *ptr = nullptr;
+    size_t capacity = 0;
+    cudaEvent_t copied = nullptr;
+
+    char *take(size_t bytes) {
+        if (copied) LR_CUDA(cudaEventSynchronize(copied));
+        if (bytes > capacity) {
+            if (ptr) LR_CUDA(cudaFreeHost(ptr));
+            ptr = nullptr;
+            capacity = std::max<size_t>(bytes, 1u << 20);
+            LR_CUDA(cudaMallocHost((void **)&ptr, capacity));
+        }
+        return ptr;
+    }
+    void queued(cudaStream_t stream) {
+        if (!copied) LR_CUDA(cudaEventCreateWithFlags(&copied, cudaEventDisableTiming));
+        LR_CUDA(cudaEventRecord(copied, stream));
+    }
+    void release() {
+        if (copied) cudaEventSynchronize(copied);
+        if (ptr) cudaFreeHost(ptr);
+        if (copied) cudaEventDestroy(copied);
+        *this = Staging{};
+    }
+};
+
 // The Owen-scrambled Sobol sampler's byte tables (dimensions 1-3), set once per process
 // and device.
 void upload_sobol_tables(cudaStream_t stream) {
@@ -678,6 +708,7 @@ struct WaveHost {
     // the most paths a pass takes.
     int width = 0;
     uint32_t fill = 0;
+    Staging staging;  // member uploads
 };
 
 namespace {
@@ -828,7 +859,7 @@ uint32_t member_add(WaveHost *h, const lr_gpu_scene *gs, lr_gpu_scene *owned, co
     validate(settings, frame);
     if (settings.max_bounces + 1 > h->rounds)
         fail(LR_LIMIT, "this wave traces at most " + std::to_string(h->rounds - 1) + " bounces");
-    if (gs->ctx != h->ctx) fail(LR_INVALID, "the scene was uploaded through another context");
+    if (!gs->ctx || gs->ctx->device != h->ctx->device) fail(LR_INVALID, "the scene was uploaded to another device");
     uint32_t index = h->capacity;
     for (uint32_t i = 0; i < h->capacity; i++)
         if (!h->members[i].used) {
@@ -867,9 +898,26 @@ uint32_t member_add(WaveHost *h, const lr_gpu_scene *gs, lr_gpu_scene *owned, co
     const size_t p_film = lay.add(nullptr, pixels * 16);
     const size_t p_image = lay.add(nullptr, pixels * 16);
     MemberHost &mh = h->members[index];
-    size_t total = 0;
-    mh.block = lay.allocate(h->ctx->stream, total);
+    // Stream-ordered: the member's memory and data arrive ahead of the next pass without
+    // waiting for the passes in flight.
+    cudaStream_t stream = h->ctx->stream;
+    size_t total = 0, host_bytes = sizeof(Member);
+    for (auto &p : lay.parts) {
+        p.offset = total;
+        total += align256(std::max<size_t>(p.bytes, 64));
+        if (p.src) host_bytes += align256(p.bytes);
+    }
+    char *stage = h->staging.take(host_bytes);
+    LR_CUDA(cudaMallocAsync(&mh.block, total, stream));
     char *base = (char *)mh.block;
+    LR_CUDA(cudaMemsetAsync(base, 0, total, stream));
+    size_t at_stage = sizeof(Member);
+    for (auto &p : lay.parts) {
+        if (!p.src || !p.bytes) continue;
+        std::memcpy(stage + at_stage, p.src, p.bytes);
+        LR_CUDA(cudaMemcpyAsync(base + p.offset, stage + at_stage, p.bytes, cudaMemcpyHostToDevice, stream));
+        at_stage += align256(p.bytes);
+    }
     auto at = [&](size_t i) { return (void *)(base + lay.parts[i].offset); };
     Member &m = mh.dev;
     m = Member{};
@@ -893,8 +941,9 @@ uint32_t member_add(WaveHost *h, const lr_gpu_scene *gs, lr_gpu_scene *owned, co
     m.pixels = pixels;
     m.film = (float4 *)at(p_film);
     m.image = (float4 *)at(p_image);
-    LR_CUDA(cudaMemcpyAsync(h->d_members + index, &m, sizeof m, cudaMemcpyHostToDevice, h->ctx->stream));
-    LR_CUDA(cudaStreamSynchronize(h->ctx->stream));
+    std::memcpy(stage, &m, sizeof m);
+    LR_CUDA(cudaMemcpyAsync(h->d_members + index, stage, sizeof m, cudaMemcpyHostToDevice, stream));
+    h->staging.queued(stream);
     mh.used = true;
     mh.leaving = false;
     mh.owned = owned;
@@ -905,8 +954,8 @@ uint32_t member_add(WaveHost *h, const lr_gpu_scene *gs, lr_gpu_scene *owned, co
     return index;
 }
 
-void member_free(MemberHost &mh) {
-    if (mh.block) cudaFree(mh.block);
+void member_free(MemberHost &mh, cudaStream_t stream) {
+    if (mh.block) cudaFreeAsync(mh.block, stream);
     if (mh.owned) lr_gpu_scene_destroy(mh.owned);
     mh = MemberHost{};
 }
@@ -914,7 +963,7 @@ void member_free(MemberHost &mh) {
 // Frees members that asked to leave once no pass in flight traces them.
 void collect(WaveHost *h) {
     for (auto &mh : h->members)
-        if (mh.used && mh.leaving && mh.last_pass <= h->retired) member_free(mh);
+        if (mh.used && mh.leaving && mh.last_pass <= h->retired) member_free(mh, h->ctx->stream);
 }
 
 bool has_work(const MemberHost &mh) { return mh.used && !mh.leaving && mh.sample < mh.samples; }
@@ -1124,7 +1173,9 @@ void wave_destroy(WaveHost *h) {
         if (e.graph) cudaGraphDestroy(e.graph);
     }
     for (auto &mh : h->members)
-        if (mh.used) member_free(mh);
+        if (mh.used) member_free(mh, h->ctx->stream);
+    cudaStreamSynchronize(h->ctx->stream);
+    h->staging.release();
     for (auto p : h->h_plan)
         if (p) cudaFreeHost(p);
     if (h->block) cudaFree(h->block);
@@ -1393,6 +1444,14 @@ int lr_batch_finish(lr_batch *b) {
     return guarded([&] {
         if (!b) fail(LR_INVALID, "no batch");
         wave_finish(&b->wave);
+    });
+}
+
+int lr_batch_wait(lr_batch *b, int32_t *in_flight) {
+    return guarded([&] {
+        if (!b) fail(LR_INVALID, "no batch");
+        retire_one(&b->wave, true);
+        if (in_flight) *in_flight = (int32_t)b->wave.in_flight.size();
     });
 }
 

@@ -1,0 +1,46 @@
+"""Render cases shared by the batch and server tests: (compiled scene, settings) pairs of
+uneven sizes, spectral and RGB, depths 2 to 8, and the image a Renderer makes of each."""
+import luce_render_b200 as lr
+from luce_render_b200 import scenes, testscenes
+
+
+def settings(width, height, samples, bounces, spectral, seed=1, material=None, background=(0.0, 0.0, 0.0)):
+    s = lr.RenderSettings.of(width, height, samples)
+    s.spectral = 1 if spectral else 0
+    s.max_bounces = bounces
+    s.light_tracing = 0.0
+    s.seed = seed
+    s.background = background
+    s.c.material = material if material is not None else lr.OpenPbr.lambert()
+    return s
+
+
+def cases():
+    """(compiled scene, settings) pairs of uneven sizes, modes and depths."""
+    out = []
+    sc = lr.compile_scene(scenes.cornell_meshes(materials=True), [scenes.cornell_camera()],
+                          [scenes.cornell_light()], scenes.cornell_materials())
+    out.append((sc, settings(48, 40, 4, 6, False, seed=3)))
+    sc = lr.compile_scene(scenes.furnace_meshes(4), [lr.camera((0.0, 0.0, 0.0))])
+    out.append((sc, settings(32, 32, 3, 8, True, material=scenes.furnace_material(0.8, 1.0))))
+    meshes, cams, lights, mats = testscenes.emissive_quad_scene()
+    sc = lr.compile_scene(meshes, cams, lights, mats)
+    out.append((sc, settings(24, 20, 5, 2, True, seed=7, material=lr.OpenPbr.lambert((0.5, 0.5, 0.5)))))
+    meshes, materials, lights, cam = scenes.scene_of_size(20_000, seed=11)
+    sc = lr.compile_scene(meshes, [cam], lights, materials)
+    out.append((sc, settings(64, 36, 2, 6, False, seed=5, background=(0.1, 0.2, 0.3))))
+    meshes, cams, lights, mats = testscenes.colored_light_scene(kelvin=3200.0)
+    sc = lr.compile_scene(meshes, cams, lights, mats)
+    out.append((sc, settings(16, 16, 6, 3, True, seed=9)))
+    return out
+
+
+def alone(ctx, sc, s):
+    """The image a Renderer of its own makes."""
+    r = lr.Renderer.create(ctx, sc, s)
+    try:
+        r.finish()
+        assert r.samples_done() == s.c.samples
+        return r.read()
+    finally:
+        r.destroy()

@@ -7,57 +7,16 @@ import numpy as np
 import pytest
 
 import luce_render_b200 as lr
-from luce_render_b200 import scenes, testscenes
+import render_cases
 
 pytestmark = pytest.mark.gpu
 
 
-def _settings(width, height, samples, bounces, spectral, seed=1, material=None, background=(0.0, 0.0, 0.0)):
-    s = lr.RenderSettings.of(width, height, samples)
-    s.spectral = 1 if spectral else 0
-    s.max_bounces = bounces
-    s.light_tracing = 0.0
-    s.seed = seed
-    s.background = background
-    s.c.material = material if material is not None else lr.OpenPbr.lambert()
-    return s
-
-
-def _cases():
-    """(compiled scene, settings) pairs of uneven sizes, modes and depths."""
-    out = []
-    sc = lr.compile_scene(scenes.cornell_meshes(materials=True), [scenes.cornell_camera()],
-                          [scenes.cornell_light()], scenes.cornell_materials())
-    out.append((sc, _settings(48, 40, 4, 6, False, seed=3)))
-    sc = lr.compile_scene(scenes.furnace_meshes(4), [lr.camera((0.0, 0.0, 0.0))])
-    out.append((sc, _settings(32, 32, 3, 8, True, material=scenes.furnace_material(0.8, 1.0))))
-    meshes, cams, lights, mats = testscenes.emissive_quad_scene()
-    sc = lr.compile_scene(meshes, cams, lights, mats)
-    out.append((sc, _settings(24, 20, 5, 2, True, seed=7, material=lr.OpenPbr.lambert((0.5, 0.5, 0.5)))))
-    meshes, materials, lights, cam = scenes.scene_of_size(20_000, seed=11)
-    sc = lr.compile_scene(meshes, [cam], lights, materials)
-    out.append((sc, _settings(64, 36, 2, 6, False, seed=5, background=(0.1, 0.2, 0.3))))
-    meshes, cams, lights, mats = testscenes.colored_light_scene(kelvin=3200.0)
-    sc = lr.compile_scene(meshes, cams, lights, mats)
-    out.append((sc, _settings(16, 16, 6, 3, True, seed=9)))
-    return out
-
-
-def _alone(ctx, sc, settings):
-    r = lr.Renderer.create(ctx, sc, settings)
-    try:
-        r.finish()
-        assert r.samples_done() == settings.c.samples
-        return r.read()
-    finally:
-        r.destroy()
-
-
 @pytest.fixture(scope="module")
 def cases(ctx):
-    cs = _cases()
+    cs = render_cases.cases()
     uploads = [lr.GpuScene.upload(ctx, sc) for sc, _ in cs]
-    alone = [_alone(ctx, sc, s) for sc, s in cs]
+    alone = [render_cases.alone(ctx, sc, s) for sc, s in cs]
     yield cs, uploads, alone
     for gs in uploads:
         gs.destroy()
@@ -119,7 +78,7 @@ def test_more_samples_later(ctx, cases):
     # set_samples after a finish continues each pixel's sample sequence.
     cs, uploads, alone = cases
     sc, s = cs[2]
-    fewer = _settings(24, 20, 2, 2, True, seed=7, material=lr.OpenPbr.lambert((0.5, 0.5, 0.5)))
+    fewer = render_cases.settings(24, 20, 2, 2, True, seed=7, material=lr.OpenPbr.lambert((0.5, 0.5, 0.5)))
     b = lr.Batch(ctx, lr.BatchSettings.default(pool=100, max_bounces=4, capacity=2))
     try:
         m = b.add(uploads[2], sc, fewer)
