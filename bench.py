@@ -282,6 +282,14 @@ def served(lr, scenes, dist, seconds: float):
             except lr.RenderError:
                 pass
     infos = [(kind, server.info(rid)) for kind, rid in submitted]
+    failures = {}
+    for (kind, rid), (_, info) in zip(submitted, infos):
+        if info["state"] == "failed":
+            try:
+                server.wait(rid, 0.0)
+            except lr.RenderError as e:
+                key = f"{kind}: {e}"
+                failures[key] = failures.get(key, 0) + 1
     server.destroy()
     for f, d in ring:
         f.close()
@@ -308,6 +316,7 @@ def served(lr, scenes, dist, seconds: float):
         "render_msamples_s": stats_window["pixel_samples"] / window / 1e6,
         "probe_mrays_s": stats_window["probe_rays"] / window / 1e6,
         "demand_msamples_s": demand / window / 1e6,
+        "failures": failures,
         "uploads": stats_window["uploads"], "evictions": stats_window["evictions"],
         "queued_at_end": stats_window["queued"], "live_at_end": stats_window["live"],
         "timing": "host steady clock of the server, from submission; the stream is cut at its end",
@@ -399,26 +408,42 @@ def main():
     shadow_nodes = cs.shadow_nodes / max(1, cs.shadow_rays)
     shadow_tests = cs.shadow_tests / max(1, cs.shadow_rays)
 
-    # Device-timed region: per-kernel CUDA events on the renderer's stream.
+    # Kernel durations: a renderer that records CUDA events after every kernel (one pass
+    # at a time on one stream), for the roofline and the per-kernel shares.
     r = lr.Renderer.create(ctx, sc, settings_for(lr, W + K, spectral, profile=1))
     for _ in range(W):
         r.advance_one()
     r.wait()
-    s0, t0 = r.stats(), r.kernel_times()
+    p0, t0 = r.stats(), r.kernel_times()
+    for _ in range(K):
+        r.advance_one()
+    r.finish()
+    p1, t1 = r.stats(), r.kernel_times()
+    r.destroy()
+    kernel_ms = t1 - t0
+    profiled_closest = p1.closest_rays - p0.closest_rays
+
+    # Device-timed region: the renderer as it runs (passes taking turns on two streams),
+    # CUDA events on the context's stream joined after the last pass.
+    r = lr.Renderer.create(ctx, sc, settings_for(lr, W + K, spectral, profile=0))
+    for _ in range(W):
+        r.advance_one()
+    r.wait()
+    s0 = r.stats()
     dist.barrier()
     clocks = Clocks(dist.local)
     ctx.synchronize()
     ctx.timer_start()
     for _ in range(K):
         r.advance_one()
+    r.join()
     ms = ctx.timer_stop()
     clock_info = clocks.stop()
     r.finish()
-    s1, t1 = r.stats(), r.kernel_times()
+    s1 = r.stats()
     r.destroy()
     closest = s1.closest_rays - s0.closest_rays
     shadow = s1.shadow_rays - s0.shadow_rays
-    kernel_ms = t1 - t0
     slowest = dist.max(ms)
     rays_all = dist.sum(closest + shadow)
     value = rays_all / (slowest / 1e3) / 1e6
@@ -429,7 +454,7 @@ def main():
     peaks = measured_peaks()
     hbm = peaks.get("hbm_gbs")
     launches = K * (BOUNCES + 1)
-    closest_bytes = closest * (48.0 + 64.0 * closest_nodes + 48.0 * closest_tests)
+    closest_bytes = profiled_closest * (48.0 + 64.0 * closest_nodes + 48.0 * closest_tests)
     closest_s = kernel_ms[1] / 1e3
     achieved = closest_bytes / closest_s / 1e9 if closest_s > 0 else None
     traffic_per_ray = profile_traffic()
@@ -441,7 +466,7 @@ def main():
         "peak_source": "MEASURED_PEAKS.json hbm_gbs (of measured)" if hbm else "fallback 6.65 TB/s",
         "unit": "GB/s",
         "frac": (achieved / (hbm if hbm else 6650.0)) if achieved else None,
-        "traffic": (traffic_per_ray * closest / launches) if traffic_per_ray else None,
+        "traffic": (traffic_per_ray * profiled_closest / launches) if traffic_per_ray else None,
         "algorithmic_bytes_per_launch": closest_bytes / launches,
         "launch_ms": kernel_ms[1] / launches,
         "bytes_per_ray": 48.0 + 64.0 * closest_nodes + 48.0 * closest_tests,

@@ -291,7 +291,10 @@ int lr_renderer_create(lr_context *ctx, const lr_scene *scene, const lr_settings
 int lr_renderer_create_viewed(lr_context *ctx, const lr_scene *scene, const lr_settings *settings,
                               const lr_frame *frame, lr_renderer **out);
 /* Renderer.advance (integrator.lucb:649-693): queue the next pass (one sample of
- * one band) without waiting; *more is 1 while passes are running or to come. */
+ * one band) without waiting; *more is 1 while passes are running or to come. At most
+ * two passes are in flight; they take turns on two path pools and streams, so the
+ * second's first rounds overlap the first's last ones, and their film accumulation runs
+ * in order. */
 int lr_renderer_advance(lr_renderer *renderer, int32_t *more);
 /* Renderer.finish (integrator.lucb:724-729): run every remaining pass and wait. */
 int lr_renderer_finish(lr_renderer *renderer);
@@ -307,6 +310,10 @@ int lr_renderer_image(lr_renderer *renderer, void **device_rgba);
 /* Renderer.read (integrator.lucb:778-782): the image copied to `rgba` (4 floats a
  * pixel); waits for work in flight. */
 int lr_renderer_read(lr_renderer *renderer, float *rgba, uint64_t float_count);
+/* Orders the context's stream after every pass queued so far, without waiting: work
+ * the caller queues there afterwards (reading the device image, an event for timing)
+ * sees their results. Passes run on two streams, taking turns; see lr_renderer_advance. */
+int lr_renderer_join(lr_renderer *renderer);
 /* Renderer.set_samples (integrator.lucb:609-611). */
 int lr_renderer_set_samples(lr_renderer *renderer, uint32_t samples);
 /* Renderer.kernel_times (integrator.lucb:873-875): milliseconds per kernel kind
@@ -358,6 +365,8 @@ int lr_batch_remove(lr_batch *batch, uint32_t member);
 int lr_batch_advance(lr_batch *batch, int32_t *more);
 /* Runs every remaining pass and waits. */
 int lr_batch_finish(lr_batch *batch);
+/* As lr_renderer_join, for a batch. */
+int lr_batch_join(lr_batch *batch);
 /* Waits for the oldest pass in flight, if any, and retires it; *in_flight: passes still
  * in flight after. */
 int lr_batch_wait(lr_batch *batch, int32_t *in_flight);

@@ -270,6 +270,8 @@ _SIGNATURES = {
     "lr_renderer_image": (C.c_int, [_vp, C.POINTER(_vp)]),
     "lr_renderer_read": (C.c_int, [_vp, C.POINTER(C.c_float), _u64]),
     "lr_renderer_set_samples": (C.c_int, [_vp, _u32]),
+    "lr_renderer_join": (C.c_int, [_vp]),
+    "lr_batch_join": (C.c_int, [_vp]),
     "lr_renderer_kernel_times": (C.c_int, [_vp, C.POINTER(C.c_double)]),
     "lr_renderer_stats": (C.c_int, [_vp, C.POINTER(RenderStats)]),
     "lr_renderer_destroy": (None, [_vp]),
@@ -750,8 +752,13 @@ class Renderer:
             if not more:
                 return False
 
+    def join(self) -> None:
+        """Order the context's stream after the passes queued so far (no wait)."""
+        _check(lib.lr_renderer_join(self.handle))
+
     def wait(self) -> None:
         """Wait for the passes queued so far."""
+        self.join()
         self.ctx.synchronize()
 
     def read_into(self, out: np.ndarray) -> np.ndarray:

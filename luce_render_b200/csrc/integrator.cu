@@ -681,25 +681,43 @@ struct PassRecord {
     std::vector<std::pair<cudaEvent_t, int>> marks;  // profiling
 };
 
+struct Graph {
+    cudaGraph_t graph = nullptr;
+    cudaGraphExec_t exec = nullptr;
+};
+
+// One of a wave's two lanes: a path pool with its queues, counters and plan, and the
+// stream its passes run on. Consecutive passes take turns on the lanes, so a pass's
+// last, thinly populated rounds run while the next pass's first rounds fill the GPU;
+// only their film accumulation (finish and convert) is ordered, by an event chain, so
+// every pixel still takes its samples in order.
+struct Lane {
+    void *block = nullptr;
+    Wave w{};
+    Plan *d_plan = nullptr;
+    Plan *h_plan = nullptr;  // pinned staging of the plan
+    cudaStream_t stream = nullptr;
+    bool own_stream = false;
+    std::map<int, Graph> trace;  // camera and rounds, by variant: width * 1000 + stack
+    Graph finish;                // finish and convert
+    cudaEvent_t finished = nullptr;  // after its latest pass's convert
+    uint64_t members_seen = 0;       // the member uploads its stream has waited for
+};
+
 struct WaveHost {
     lr_context *ctx = nullptr;
     uint32_t pool = 0, rounds = 0, capacity = 0;
     int profile = 0;
-    void *block = nullptr;
-    Wave w{};
+    void *block = nullptr;  // the member table and stats, shared by the lanes
+    Lane lanes[2];
+    int lane_count = 2;     // 1 when profiling: kernel times are taken one pass at a time
     Member *d_members = nullptr;
-    Plan *d_plan = nullptr;
-    Plan *h_plan[2] = {nullptr, nullptr};  // pinned staging, by pass parity
+    unsigned long long *d_stats = nullptr;
     std::vector<MemberHost> members;
+    uint64_t member_uploads = 0;  // member records queued on the context's stream so far
     int grid_shade = 0;
-    struct Exec {
-        cudaGraph_t graph = nullptr;
-        cudaGraphExec_t exec = nullptr;
-        int grid_trace = 0;
-    };
-    std::map<int, Exec> execs;  // by variant: width * 1000 + stack
+    std::map<int, int> grid_trace;  // by variant
     uint64_t recorded = 0, retired = 0;
-    cudaEvent_t done_events[2] = {nullptr, nullptr};
     cudaEvent_t mark_start[2] = {nullptr, nullptr};
     std::deque<PassRecord> in_flight;
     double kernel_ms[10] = {0};
@@ -713,32 +731,40 @@ struct WaveHost {
 
 namespace {
 
-// Records one pass on `stream` with traversal variant (W, kStack). With `marks`, an
-// event follows each kernel (profiling); kCount instantiates the counting traversals.
+using Marks = std::vector<std::pair<cudaEvent_t, int>>;
+
+void mark(cudaStream_t stream, Marks *marks, int kind) {
+    if (!marks) return;
+    cudaEvent_t e;
+    LR_CUDA(cudaEventCreate(&e));
+    LR_CUDA(cudaEventRecord(e, stream));
+    marks->push_back({e, kind});
+}
+
+// Records a pass's tracing on `stream` with traversal variant (W, kStack): camera, then
+// (closest, shade, shadow) for every round. With `marks`, an event follows each kernel
+// (profiling); kCount instantiates the counting traversals.
 template <int W, int kStack, bool kCount>
-void record_pass(WaveHost *h, int grid_trace, cudaStream_t stream, std::vector<std::pair<cudaEvent_t, int>> *marks) {
-    const Wave &w = h->w;
-    auto mark = [&](int kind) {
-        if (!marks) return;
-        cudaEvent_t e;
-        LR_CUDA(cudaEventCreate(&e));
-        LR_CUDA(cudaEventRecord(e, stream));
-        marks->push_back({e, kind});
-    };
+void record_trace(const WaveHost *h, const Wave &w, int grid_trace, cudaStream_t stream, Marks *marks) {
     camera_kernel<<<h->grid_shade, kShadeBlock, 0, stream>>>(w);
-    mark(kCamera);
+    mark(stream, marks, kCamera);
     for (uint32_t round = 0; round < w.rounds; round++) {
         closest_kernel<W, kStack, kCount><<<grid_trace, kTraceBlock, 0, stream>>>(w, round);
-        mark(kClosest);
+        mark(stream, marks, kClosest);
         shade_kernel<<<h->grid_shade, kShadeBlock, 0, stream>>>(w, round);
-        mark(kSurface);
+        mark(stream, marks, kSurface);
         shadow_kernel<W, kStack, kCount><<<grid_trace, kTraceBlock, 0, stream>>>(w, round);
-        mark(kShadow);
+        mark(stream, marks, kShadow);
     }
+    LR_CUDA(cudaGetLastError());
+}
+
+// Records a pass's film accumulation: finish, then convert.
+void record_finish(const WaveHost *h, const Wave &w, cudaStream_t stream, Marks *marks) {
     finish_kernel<<<h->grid_shade, kShadeBlock, 0, stream>>>(w);
-    mark(kFinish);
+    mark(stream, marks, kFinish);
     convert_kernel<<<h->grid_shade, kShadeBlock, 0, stream>>>(w);
-    mark(kConvert);
+    mark(stream, marks, kConvert);
     LR_CUDA(cudaGetLastError());
 }
 
@@ -752,14 +778,22 @@ int trace_grid(int variant, int sms) {
     }
 }
 
-void record(WaveHost *h, int variant, int grid_trace, cudaStream_t stream,
-            std::vector<std::pair<cudaEvent_t, int>> *marks) {
+int grid_for(WaveHost *h, int variant) {
+    auto it = h->grid_trace.find(variant);
+    if (it != h->grid_trace.end()) return it->second;
+    const int g = trace_grid(variant, h->ctx->sm_count);
+    h->grid_trace[variant] = g;
+    return g;
+}
+
+void record_trace_any(WaveHost *h, const Wave &w, int variant, cudaStream_t stream, Marks *marks) {
     const bool count = h->profile == 2;
+    const int grid = grid_for(h, variant);
     switch (variant) {
 #define LR_CASE(wd, k)                                                                        \
     case wd * 1000 + k:                                                                       \
-        if (count) record_pass<wd, k, true>(h, grid_trace, stream, marks);                    \
-        else record_pass<wd, k, false>(h, grid_trace, stream, marks);                         \
+        if (count) record_trace<wd, k, true>(h, w, grid, stream, marks);                      \
+        else record_trace<wd, k, false>(h, w, grid, stream, marks);                           \
         break;
         LR_TRAVERSALS(LR_CASE)
 #undef LR_CASE
@@ -767,22 +801,32 @@ void record(WaveHost *h, int variant, int grid_trace, cudaStream_t stream,
     }
 }
 
-WaveHost::Exec &exec_for(WaveHost *h, int variant) {
-    auto it = h->execs.find(variant);
-    if (it != h->execs.end()) return it->second;
-    WaveHost::Exec e;
-    e.grid_trace = trace_grid(variant, h->ctx->sm_count);
-    if (!h->profile) {
-        // The pass as one graph, captured on a private stream.
-        cudaStream_t capture;
-        LR_CUDA(cudaStreamCreateWithFlags(&capture, cudaStreamNonBlocking));
-        LR_CUDA(cudaStreamBeginCapture(capture, cudaStreamCaptureModeThreadLocal));
-        record(h, variant, e.grid_trace, capture, nullptr);
-        LR_CUDA(cudaStreamEndCapture(capture, &e.graph));
-        LR_CUDA(cudaStreamDestroy(capture));
-        LR_CUDA(cudaGraphInstantiate(&e.exec, e.graph, 0));
-    }
-    return h->execs.emplace(variant, e).first->second;
+// Captures whatever `body` queues on a private stream as a graph.
+template <class Body>
+Graph capture(Body body) {
+    Graph g;
+    cudaStream_t stream;
+    LR_CUDA(cudaStreamCreateWithFlags(&stream, cudaStreamNonBlocking));
+    LR_CUDA(cudaStreamBeginCapture(stream, cudaStreamCaptureModeThreadLocal));
+    body(stream);
+    LR_CUDA(cudaStreamEndCapture(stream, &g.graph));
+    LR_CUDA(cudaStreamDestroy(stream));
+    LR_CUDA(cudaGraphInstantiate(&g.exec, g.graph, 0));
+    return g;
+}
+
+// The trace graph of `variant` on a lane, captured on first use.
+Graph &trace_graph(WaveHost *h, Lane &lane, int variant) {
+    auto it = lane.trace.find(variant);
+    if (it != lane.trace.end()) return it->second;
+    Graph g = capture([&](cudaStream_t s) { record_trace_any(h, lane.w, variant, s, nullptr); });
+    return lane.trace.emplace(variant, g).first->second;
+}
+
+void destroy_graph(Graph &g) {
+    if (g.exec) cudaGraphExecDestroy(g.exec);
+    if (g.graph) cudaGraphDestroy(g.graph);
+    g = Graph{};
 }
 
 void wave_create(WaveHost *h, lr_context *ctx, uint64_t pool, uint32_t rounds, uint32_t capacity, int profile) {
@@ -792,56 +836,80 @@ void wave_create(WaveHost *h, lr_context *ctx, uint64_t pool, uint32_t rounds, u
     h->rounds = rounds;
     h->capacity = capacity;
     h->profile = profile;
+    h->lane_count = profile ? 1 : 2;
     LR_CUDA(cudaSetDevice(ctx->device));
-    const uint64_t P = h->pool;
-    Layout L;
-    const size_t p_throughput = L.add(nullptr, P * 16), p_radiance = L.add(nullptr, P * 16);
-    const size_t p_lambda = L.add(nullptr, P * 16), p_vertex = L.add(nullptr, P * 16), p_path = L.add(nullptr, P * 16);
-    size_t p_ray[2][3];
-    for (int q = 0; q < 2; q++)
-        for (int j = 0; j < 3; j++) p_ray[q][j] = L.add(nullptr, P * 16);
-    const size_t p_shadow_o = L.add(nullptr, P * 16), p_shadow_d = L.add(nullptr, P * 16);
-    const size_t p_shadow_c = L.add(nullptr, P * 16);
-    const size_t p_counters = L.add(nullptr, (4 * (size_t)rounds + 2) * 4);
-    const size_t p_stats = L.add(nullptr, 8 * 8);
-    const size_t p_members = L.add(nullptr, (size_t)capacity * sizeof(Member));
-    const size_t p_plan = L.add(nullptr, sizeof(Plan));
-    size_t total = 0;
-    h->block = L.allocate(ctx->stream, total);
-    char *base = (char *)h->block;
-    auto at = [&](size_t i) { return (void *)(base + L.parts[i].offset); };
-    Wave &w = h->w;
-    w.pool = h->pool;
-    w.rounds = rounds;
-    w.throughput = (float4 *)at(p_throughput);
-    w.radiance = (float4 *)at(p_radiance);
-    w.lambda = (float4 *)at(p_lambda);
-    w.vertex = (float4 *)at(p_vertex);
-    w.path = (uint4 *)at(p_path);
-    for (int q = 0; q < 2; q++) {
-        w.ray_o[q] = (float4 *)at(p_ray[q][0]);
-        w.ray_d[q] = (float4 *)at(p_ray[q][1]);
-        w.hits[q] = (float4 *)at(p_ray[q][2]);
+    {
+        Layout L;
+        const size_t p_stats = L.add(nullptr, 8 * 8);
+        const size_t p_members = L.add(nullptr, (size_t)capacity * sizeof(Member));
+        size_t total = 0;
+        h->block = L.allocate(ctx->stream, total);
+        h->d_stats = (unsigned long long *)((char *)h->block + L.parts[p_stats].offset);
+        h->d_members = (Member *)((char *)h->block + L.parts[p_members].offset);
     }
-    w.shadow_o = (float4 *)at(p_shadow_o);
-    w.shadow_d = (float4 *)at(p_shadow_d);
-    w.shadow_c = (float4 *)at(p_shadow_c);
-    w.counters = (uint32_t *)at(p_counters);
-    w.stats = (unsigned long long *)at(p_stats);
-    w.status = ctx->status;
-    h->d_members = (Member *)at(p_members);
-    h->d_plan = (Plan *)at(p_plan);
-    w.members = h->d_members;
-    w.plan = h->d_plan;
-    for (auto &p : h->h_plan) LR_CUDA(cudaMallocHost((void **)&p, sizeof(Plan)));
+    const uint64_t P = h->pool;
+    for (int li = 0; li < h->lane_count; li++) {
+        Lane &lane = h->lanes[li];
+        Layout L;
+        const size_t p_throughput = L.add(nullptr, P * 16), p_radiance = L.add(nullptr, P * 16);
+        const size_t p_lambda = L.add(nullptr, P * 16), p_vertex = L.add(nullptr, P * 16);
+        const size_t p_path = L.add(nullptr, P * 16);
+        size_t p_ray[2][3];
+        for (int q = 0; q < 2; q++)
+            for (int j = 0; j < 3; j++) p_ray[q][j] = L.add(nullptr, P * 16);
+        const size_t p_shadow_o = L.add(nullptr, P * 16), p_shadow_d = L.add(nullptr, P * 16);
+        const size_t p_shadow_c = L.add(nullptr, P * 16);
+        const size_t p_counters = L.add(nullptr, (4 * (size_t)rounds + 2) * 4);
+        const size_t p_plan = L.add(nullptr, sizeof(Plan));
+        size_t total = 0;
+        lane.block = L.allocate(ctx->stream, total);
+        char *base = (char *)lane.block;
+        auto at = [&](size_t i) { return (void *)(base + L.parts[i].offset); };
+        Wave &w = lane.w;
+        w.pool = h->pool;
+        w.rounds = rounds;
+        w.throughput = (float4 *)at(p_throughput);
+        w.radiance = (float4 *)at(p_radiance);
+        w.lambda = (float4 *)at(p_lambda);
+        w.vertex = (float4 *)at(p_vertex);
+        w.path = (uint4 *)at(p_path);
+        for (int q = 0; q < 2; q++) {
+            w.ray_o[q] = (float4 *)at(p_ray[q][0]);
+            w.ray_d[q] = (float4 *)at(p_ray[q][1]);
+            w.hits[q] = (float4 *)at(p_ray[q][2]);
+        }
+        w.shadow_o = (float4 *)at(p_shadow_o);
+        w.shadow_d = (float4 *)at(p_shadow_d);
+        w.shadow_c = (float4 *)at(p_shadow_c);
+        w.counters = (uint32_t *)at(p_counters);
+        w.stats = h->d_stats;
+        w.status = ctx->status;
+        w.members = h->d_members;
+        lane.d_plan = (Plan *)at(p_plan);
+        w.plan = lane.d_plan;
+        LR_CUDA(cudaMallocHost((void **)&lane.h_plan, sizeof(Plan)));
+        if (li == 0) {
+            lane.stream = ctx->stream;
+        } else {
+            LR_CUDA(cudaStreamCreateWithFlags(&lane.stream, cudaStreamNonBlocking));
+            lane.own_stream = true;
+        }
+        LR_CUDA(cudaEventCreateWithFlags(&lane.finished, cudaEventDisableTiming));
+    }
     upload_sobol_tables(ctx->stream);
     LR_CUDA(cudaStreamSynchronize(ctx->stream));
     h->grid_shade = grid_of(shade_kernel, kShadeBlock, ctx->sm_count);
-    for (auto &e : h->done_events) LR_CUDA(cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
     if (profile)
         for (auto &e : h->mark_start) LR_CUDA(cudaEventCreate(&e));
+    else
+        for (int li = 0; li < h->lane_count; li++) {
+            Lane &lane = h->lanes[li];
+            lane.finish = capture([&](cudaStream_t s) { record_finish(h, lane.w, s, nullptr); });
+        }
     h->members.resize(capacity);
 }
+
+void settle(WaveHost *h);
 
 void validate(const lr_settings &s, const lr_frame &f) {
     if (f.width == 0 || f.height == 0 || f.width > 16384 || f.height > 16384)
@@ -860,12 +928,18 @@ uint32_t member_add(WaveHost *h, const lr_gpu_scene *gs, lr_gpu_scene *owned, co
     if (settings.max_bounces + 1 > h->rounds)
         fail(LR_LIMIT, "this wave traces at most " + std::to_string(h->rounds - 1) + " bounces");
     if (!gs->ctx || gs->ctx->device != h->ctx->device) fail(LR_INVALID, "the scene was uploaded to another device");
-    uint32_t index = h->capacity;
-    for (uint32_t i = 0; i < h->capacity; i++)
-        if (!h->members[i].used) {
-            index = i;
-            break;
-        }
+    auto free_slot = [&] {
+        for (uint32_t i = 0; i < h->capacity; i++)
+            if (!h->members[i].used) return i;
+        return h->capacity;
+    };
+    uint32_t index = free_slot();
+    if (index == h->capacity && std::any_of(h->members.begin(), h->members.end(),
+                                            [](const MemberHost &m) { return m.used && m.leaving; })) {
+        // A member that left holds its slot until its passes finish: wait for them.
+        settle(h);
+        index = free_slot();
+    }
     if (index == h->capacity) fail(LR_LIMIT, "the wave holds " + std::to_string(h->capacity) + " members");
     const Loaded L = load(*scene, settings);
     const uint64_t pixels = (uint64_t)frame.width * frame.height;
@@ -944,6 +1018,7 @@ uint32_t member_add(WaveHost *h, const lr_gpu_scene *gs, lr_gpu_scene *owned, co
     std::memcpy(stage, &m, sizeof m);
     LR_CUDA(cudaMemcpyAsync(h->d_members + index, stage, sizeof m, cudaMemcpyHostToDevice, stream));
     h->staging.queued(stream);
+    h->member_uploads++;
     mh.used = true;
     mh.leaving = false;
     mh.owned = owned;
@@ -968,14 +1043,16 @@ void collect(WaveHost *h) {
 
 bool has_work(const MemberHost &mh) { return mh.used && !mh.leaving && mh.sample < mh.samples; }
 
+Lane &lane_of(WaveHost *h, uint64_t pass) { return h->lanes[pass % (uint64_t)h->lane_count]; }
+
 // Paths in the plan of the pass launched last.
-uint64_t h_plan_paths(WaveHost *h) { return h->h_plan[(h->recorded - 1) & 1]->head.paths; }
+uint64_t h_plan_paths(WaveHost *h) { return lane_of(h, h->recorded - 1).h_plan->head.paths; }
 
 // Retires the oldest pass in flight if it has finished (integrator.lucb:622-645).
 bool retire_one(WaveHost *h, bool wait) {
     if (h->in_flight.empty()) return false;
     PassRecord &p = h->in_flight.front();
-    cudaEvent_t e = h->done_events[p.number & 1];
+    cudaEvent_t e = lane_of(h, p.number).finished;
     if (wait) {
         LR_CUDA(cudaEventSynchronize(e));
     } else {
@@ -1011,7 +1088,8 @@ void settle(WaveHost *h) {
 // plans the same way but moves no member on and leaves the films alone. Returns false
 // with no work.
 bool launch_pass(WaveHost *h, bool dry = false) {
-    Plan *staging = h->h_plan[h->recorded & 1];
+    Lane &lane = lane_of(h, h->recorded);
+    Plan *staging = lane.h_plan;
     Segment *seg = staging->seg;
     uint32_t n = 0, used = 0, converts = 0;
     int width = 0, stack = 32;
@@ -1062,21 +1140,38 @@ bool launch_pass(WaveHost *h, bool dry = false) {
     }
     const int variant = width * 1000 + stack;
     staging->head = PlanHeader{n, used, converts, dry ? 1u : 0u};
-    cudaStream_t stream = h->ctx->stream;
-    WaveHost::Exec &ex = exec_for(h, variant);
+    cudaStream_t stream = lane.stream;
+    // Member records queued on the context's stream reach this lane first.
+    if (stream != h->ctx->stream && lane.members_seen != h->member_uploads && h->staging.copied) {
+        LR_CUDA(cudaStreamWaitEvent(stream, h->staging.copied, 0));
+        lane.members_seen = h->member_uploads;
+    }
     // The header and convert list, then the segments in use.
-    LR_CUDA(cudaMemcpyAsync(h->d_plan, staging, offsetof(Plan, seg) + n * sizeof(Segment), cudaMemcpyHostToDevice,
+    LR_CUDA(cudaMemcpyAsync(lane.d_plan, staging, offsetof(Plan, seg) + n * sizeof(Segment), cudaMemcpyHostToDevice,
                             stream));
+    // Film accumulation waits for the previous pass's, which ran on the other lane.
+    Lane *before = rec.number > 0 && h->lane_count > 1 ? &lane_of(h, rec.number - 1) : nullptr;
     if (h->profile) {
         LR_CUDA(cudaEventRecord(h->mark_start[rec.number & 1], stream));
-        record(h, variant, ex.grid_trace, stream, &rec.marks);
+        record_trace_any(h, lane.w, variant, stream, &rec.marks);
+        if (before) LR_CUDA(cudaStreamWaitEvent(stream, before->finished, 0));
+        record_finish(h, lane.w, stream, &rec.marks);
     } else {
-        LR_CUDA(cudaGraphLaunch(ex.exec, stream));
+        LR_CUDA(cudaGraphLaunch(trace_graph(h, lane, variant).exec, stream));
+        if (before) LR_CUDA(cudaStreamWaitEvent(stream, before->finished, 0));
+        LR_CUDA(cudaGraphLaunch(lane.finish.exec, stream));
     }
-    LR_CUDA(cudaEventRecord(h->done_events[rec.number & 1], stream));
+    LR_CUDA(cudaEventRecord(lane.finished, stream));
     h->in_flight.push_back(std::move(rec));
     h->recorded++;
     return true;
+}
+
+// Orders the context's stream after every pass launched so far (their films and images).
+void join_lanes(WaveHost *h) {
+    if (h->recorded == 0) return;
+    Lane &last = lane_of(h, h->recorded - 1);
+    if (last.stream != h->ctx->stream) LR_CUDA(cudaStreamWaitEvent(h->ctx->stream, last.finished, 0));
 }
 
 // Renderer.advance (integrator.lucb:649-693): never waits; two passes in flight.
@@ -1122,6 +1217,7 @@ void wave_tune(WaveHost *h, lr_batch_tuning *out) {
                 launch_pass(h, true);
                 paths += h_plan_paths(h);
             }
+            join_lanes(h);
             LR_CUDA(cudaEventRecord(b, stream));
             LR_CUDA(cudaEventSynchronize(b));
             settle(h);
@@ -1161,30 +1257,34 @@ void wave_finish(WaveHost *h) {
 void wave_destroy(WaveHost *h) {
     if (!h->ctx) return;
     cudaSetDevice(h->ctx->device);
+    for (auto &lane : h->lanes)
+        if (lane.stream) cudaStreamSynchronize(lane.stream);
     cudaStreamSynchronize(h->ctx->stream);
     for (auto &p : h->in_flight)
         for (auto &[e, k] : p.marks) cudaEventDestroy(e);
     for (auto e : h->mark_start)
         if (e) cudaEventDestroy(e);
-    for (auto e : h->done_events)
-        if (e) cudaEventDestroy(e);
-    for (auto &[v, e] : h->execs) {
-        if (e.exec) cudaGraphExecDestroy(e.exec);
-        if (e.graph) cudaGraphDestroy(e.graph);
-    }
     for (auto &mh : h->members)
         if (mh.used) member_free(mh, h->ctx->stream);
     cudaStreamSynchronize(h->ctx->stream);
     h->staging.release();
-    for (auto p : h->h_plan)
-        if (p) cudaFreeHost(p);
+    for (auto &lane : h->lanes) {
+        for (auto &[v, g] : lane.trace) destroy_graph(g);
+        destroy_graph(lane.finish);
+        if (lane.finished) cudaEventDestroy(lane.finished);
+        if (lane.h_plan) cudaFreeHost(lane.h_plan);
+        if (lane.own_stream && lane.stream) cudaStreamDestroy(lane.stream);
+        if (lane.block) cudaFree(lane.block);
+        lane = Lane{};
+    }
     if (h->block) cudaFree(h->block);
 }
 
 void wave_stats(WaveHost *h, lr_render_stats *out) {
     settle(h);
     unsigned long long s[8];
-    LR_CUDA(cudaMemcpyAsync(s, h->w.stats, sizeof s, cudaMemcpyDeviceToHost, h->ctx->stream));
+    join_lanes(h);
+    LR_CUDA(cudaMemcpyAsync(s, h->d_stats, sizeof s, cudaMemcpyDeviceToHost, h->ctx->stream));
     LR_CUDA(cudaStreamSynchronize(h->ctx->stream));
     out->closest_rays = s[0];
     out->shadow_rays = s[1];
@@ -1211,6 +1311,7 @@ MemberHost &member_at(WaveHost *h, uint32_t member) {
 void member_read(WaveHost *h, uint32_t member, float *rgba, uint64_t count) {
     MemberHost &mh = member_at(h, member);
     if (count != mh.dev.pixels * 4) fail(LR_INVALID, "reading the image needs four floats a pixel");
+    join_lanes(h);
     LR_CUDA(cudaMemcpyAsync(rgba, mh.dev.image, count * 4, cudaMemcpyDeviceToHost, h->ctx->stream));
     LR_CUDA(cudaStreamSynchronize(h->ctx->stream));
 }
@@ -1245,9 +1346,10 @@ void create(lr_context *ctx, const lr_scene *scene, const lr_settings &settings,
     try {
         wave_create(&r->wave, ctx, pool, settings.max_bounces + 1, 1, settings.profile);
         member_add(&r->wave, gs, gs, scene, settings, frame);
-        // The graph for the scene's traversal variant, made now rather than at the first pass.
+        // The graphs for the scene's traversal variant, made now rather than at the first pass.
         const TraversalChoice c = choose_traversal(gs->scene, 0);
-        exec_for(&r->wave, c.width * 1000 + c.stack);
+        if (!settings.profile)
+            for (int li = 0; li < r->wave.lane_count; li++) trace_graph(&r->wave, r->wave.lanes[li], c.width * 1000 + c.stack);
     } catch (...) {
         const bool owned = !r->wave.members.empty() && r->wave.members[0].used;
         wave_destroy(&r->wave);
@@ -1356,6 +1458,13 @@ int lr_renderer_read(lr_renderer *r, float *rgba, uint64_t count) {
     });
 }
 
+int lr_renderer_join(lr_renderer *r) {
+    return guarded([&] {
+        if (!r) fail(LR_INVALID, "no renderer");
+        join_lanes(&r->wave);
+    });
+}
+
 int lr_renderer_set_samples(lr_renderer *r, uint32_t samples) {
     return guarded([&] {
         if (!r) fail(LR_INVALID, "no renderer");
@@ -1444,6 +1553,13 @@ int lr_batch_finish(lr_batch *b) {
     return guarded([&] {
         if (!b) fail(LR_INVALID, "no batch");
         wave_finish(&b->wave);
+    });
+}
+
+int lr_batch_join(lr_batch *b) {
+    return guarded([&] {
+        if (!b) fail(LR_INVALID, "no batch");
+        join_lanes(&b->wave);
     });
 }
 
