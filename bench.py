@@ -92,34 +92,56 @@ class Dist:
 
 
 class Clocks:
-    """nvidia-smi samples of SM clocks and throttle reasons during the timed region."""
+    """nvidia-smi samples of SM clocks and throttle reasons around the timed region: the
+    sampler runs from before the region (`ready` waits for its first sample) to after it
+    (`stop` waits for one sample past the end), every 100 ms."""
 
     FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
               "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
               "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
 
     def __init__(self, device: int):
-        self.device = device
-        self.proc = None
+        import threading
+
+        self.lines, self.proc = [], None
         try:
             self.proc = subprocess.Popen(
-                ["nvidia-smi", f"--query-gpu={self.FIELDS}", "--format=csv,noheader,nounits", "-lms", "200",
+                ["nvidia-smi", f"--query-gpu={self.FIELDS}", "--format=csv,noheader,nounits", "-lms", "100",
                  "-i", str(device)], stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
         except (FileNotFoundError, OSError):
             self.proc = None
+            return
+        self.reader = threading.Thread(target=self._read, daemon=True)
+        self.reader.start()
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.lines.append(line)
+
+    def _wait_for(self, count: int, seconds: float) -> None:
+        end = time.perf_counter() + seconds
+        while len(self.lines) < count and time.perf_counter() < end and self.proc.poll() is None:
+            time.sleep(0.01)
+
+    def ready(self) -> None:
+        if self.proc:
+            self._wait_for(1, 5.0)
+        self.first = len(self.lines)
 
     def stop(self) -> dict:
         if not self.proc:
             return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        self._wait_for(len(self.lines) + 1, 2.0)
         self.proc.terminate()
         try:
-            out, _ = self.proc.communicate(timeout=10)
+            self.proc.wait(timeout=10)
         except subprocess.TimeoutExpired:
             self.proc.kill()
-            out, _ = self.proc.communicate()
+        # The sample just before the region, the samples in it and the one just after.
+        lines = self.lines[max(0, getattr(self, "first", 1) - 1):]
         sm, mx, reasons = [], [], set()
         names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
-        for line in out.strip().splitlines():
+        for line in lines:
             parts = [x.strip() for x in line.split(",")]
             if len(parts) < 9:
                 continue
@@ -430,8 +452,9 @@ def main():
         r.advance_one()
     r.wait()
     s0 = r.stats()
-    dist.barrier()
     clocks = Clocks(dist.local)
+    clocks.ready()
+    dist.barrier()
     ctx.synchronize()
     ctx.timer_start()
     for _ in range(K):
