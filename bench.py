@@ -403,6 +403,27 @@ def batched(lr, scenes, ctx, dist):
     }
 
 
+def cpu_intersection(sc, scenes, oracle, cores: int) -> dict:
+    """The reference's CPU intersection on the 1M-triangle scene, on all host cores: its
+    f64 brute force (tests/gpu/main.lucb:82-119, every ray against every triangle) on a
+    seeded subset of 4,096 incoherent rays, and the restatement of trace_closest (BVH2)
+    on 262,144."""
+    a = sc.arrays()
+    rays = scenes.incoherent_rays(1 << 18, seed=5)
+    t0 = time.perf_counter()
+    oracle.nearest_f64(a["positions"], a["indices"], a["faces"], rays[:4096], threads=cores)
+    brute = time.perf_counter() - t0
+    t0 = time.perf_counter()
+    oracle.trace(a["nodes"], a["positions"], a["indices"], rays, threads=cores)
+    bvh = time.perf_counter() - t0
+    return {
+        "brute_force_f64": {"value": 4096 / brute / 1e6, "unit": "Mrays/s", "cores": cores,
+                            "sample": f"4,096 incoherent rays x {int(sc.triangle_count()):,} triangles, {brute:.1f} s"},
+        "bvh2_closest": {"value": len(rays) / bvh / 1e6, "unit": "Mrays/s", "cores": cores,
+                         "sample": f"{len(rays):,} incoherent rays, {bvh:.2f} s"},
+    }
+
+
 def main():
     args = parse()
     spectral = not args.rgb
@@ -533,6 +554,7 @@ def main():
                "sample": f"3 strips of {ref.pixels} pixels x 1 spp of the same frame ({rays} closest+shadow rays, "
                          f"{secs:.1f} s wall on {ref.cores} threads): the f64 restatement of the reference's "
                          f"estimator and BVH2 traversal"}
+        cpu.update(cpu_intersection(sc, scenes, oracle, ref.cores))
 
     if dist.rank == 0:
         line = {
