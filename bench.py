@@ -50,7 +50,8 @@ def parse():
 
 
 class Dist:
-    """torch.distributed plumbing for N > 1: barrier and max over ranks."""
+    """torch.distributed plumbing for N > 1: barrier, max and sum over ranks (NCCL on GPUs,
+    gloo on a host without one). No data crosses ranks: each renders its own replica."""
 
     def __init__(self, gpus: int):
         self.world = int(os.environ.get("WORLD_SIZE", "1"))
@@ -63,8 +64,12 @@ class Dist:
             import torch
             import torch.distributed as dist
 
-            torch.cuda.set_device(self.local)
-            dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300))
+            if torch.cuda.is_available():
+                torch.cuda.set_device(self.local)
+                backend, self.device = "nccl", f"cuda:{self.local}"
+            else:
+                backend, self.device = "gloo", "cpu"
+            dist.init_process_group(backend, timeout=datetime.timedelta(seconds=300))
             self.torch, self.dist = torch, dist
             self.pg = True
 
@@ -75,14 +80,14 @@ class Dist:
     def max(self, value: float) -> float:
         if not self.pg:
             return value
-        t = self.torch.tensor([value], dtype=self.torch.float64, device=f"cuda:{self.local}")
+        t = self.torch.tensor([value], dtype=self.torch.float64, device=self.device)
         self.dist.all_reduce(t, op=self.dist.ReduceOp.MAX)
         return float(t.item())
 
     def sum(self, value: float) -> float:
         if not self.pg:
             return value
-        t = self.torch.tensor([value], dtype=self.torch.float64, device=f"cuda:{self.local}")
+        t = self.torch.tensor([value], dtype=self.torch.float64, device=self.device)
         self.dist.all_reduce(t, op=self.dist.ReduceOp.SUM)
         return float(t.item())
 
@@ -239,6 +244,27 @@ def batch_cases(lr, scenes):
     return cases
 
 
+def arrival_stream(seconds: float, scenes: int, rate: float = 200.0, seed: int = 0x5E4E):
+    """The served workload's requests: (time, "probe", scene, width, height) for 20 %
+    (1k..2M pixel rays, log-uniform, 16:9) and (time, "render", scene, spp, 0) for 80 %
+    (spp uniform in 16..256), Poisson arrivals at `rate` a second."""
+    import numpy as np
+
+    rng = np.random.default_rng(seed)
+    arrivals, t = [], 0.0
+    while True:
+        t += rng.exponential(1.0 / rate)
+        if t >= seconds:
+            break
+        if rng.random() < 0.2:
+            px = int(round(math.exp(rng.uniform(math.log(1000.0), math.log(2_000_000.0)))))
+            w = max(1, int(round(math.sqrt(px * 16.0 / 9.0))))
+            arrivals.append((t, "probe", int(rng.integers(scenes)), w, max(1, px // w)))
+        else:
+            arrivals.append((t, "render", int(rng.integers(scenes)), int(rng.integers(16, 257)), 0))
+    return arrivals
+
+
 def percentiles(values):
     if not values:
         return {"count": 0, "p50_ms": None, "p99_ms": None}
@@ -259,18 +285,7 @@ def served(lr, scenes, dist, seconds: float):
     import numpy as np
 
     cases = batch_cases(lr, scenes)
-    rng = np.random.default_rng(0x5E4E)
-    arrivals, t = [], 0.0
-    while True:
-        t += rng.exponential(1.0 / 200.0)
-        if t >= seconds:
-            break
-        if rng.random() < 0.2:
-            px = int(round(math.exp(rng.uniform(math.log(1000.0), math.log(2_000_000.0)))))
-            w = max(1, int(round(math.sqrt(px * 16.0 / 9.0))))
-            arrivals.append((t, "probe", int(rng.integers(len(cases))), w, max(1, px // w)))
-        else:
-            arrivals.append((t, "render", int(rng.integers(len(cases))), int(rng.integers(16, 257)), 0))
+    arrivals = arrival_stream(seconds, len(cases))
     server = lr.Server(lr.ServerSettings.default(budget_bytes=150 * 10**9, capacity=128, pool=1 << 22,
                                                  max_bounces=BATCH_BOUNCES))
     ids = [server.add_scene(sc) for sc, _ in cases]
