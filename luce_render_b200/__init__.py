@@ -50,7 +50,7 @@ class RenderError(RuntimeError):
 def _load() -> C.CDLL:
     if not LIBRARY_PATH.exists():
         raise ImportError(
-            f"{LIBRARY_PATH} is missing: build it with `python -m luce_render_b200.build` "
+            f"{LIBRARY_PATH} is missing: build it with `python luce_render_b200/build.py` "
             "(nvcc for sm_100a). There is no CPU fallback.")
     return C.CDLL(str(LIBRARY_PATH))
 

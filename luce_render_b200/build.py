@@ -4,7 +4,7 @@ Every CUDA source is compiled for sm_100a only (``-gencode arch=compute_100a,cod
 host C++ goes through nvcc's host compiler. Objects land in ``_build/`` at the repository
 root and are rebuilt when a source or header is newer than its object.
 
-    python -m luce_render_b200.build          # or: python luce_render_b200/build.py
+    python luce_render_b200/build.py   (the package itself does not load before the library exists)
 """
 from __future__ import annotations
 
