@@ -339,12 +339,16 @@ def served(lr, scenes, dist, seconds: float):
     first_images = [i["first"] - i["submitted"] for i in renders if i["first"] >= 0]
     completed = [i["finished"] - i["submitted"] for i in renders if i["state"] == "done"]
     demand = sum(i["pixels"] * i["samples"] for i in renders)
+    slowest = sorted((i for i in probes if i["state"] == "done"), key=lambda i: i["finished"] - i["submitted"])[-3:]
     return {
         "workload": ("Poisson arrivals at 200 requests/s (seed 0x5E4E): 80% render sessions of the batched "
                      "workload's scenes at their film sizes, 16..256 spp, depth 6; 20% probes of 1k..2M pixel rays "
                      "(log-uniform); budget 150 GB, 128 live sessions, pool 2^22, LRU eviction of idle scenes"),
         "seconds": window, "requests": len(submitted),
         "probe_latency": percentiles(done_probes),
+        "slowest_probes": [{"pixels": i["pixels"], "submitted_s": i["submitted"],
+                            "wait_ms": (i["admitted"] - i["submitted"]) * 1e3,
+                            "latency_ms": (i["finished"] - i["submitted"]) * 1e3} for i in slowest],
         "session_first_image": percentiles(first_images),
         "session_completion": percentiles(completed),
         "sessions": {"submitted": len(renders), "admitted": sum(1 for i in renders if i["admitted"] >= 0),

@@ -378,14 +378,19 @@ int lr_batch_set_samples(lr_batch *batch, uint32_t member, uint32_t samples);
 int lr_batch_image(lr_batch *batch, uint32_t member, void **device_rgba);
 int lr_batch_read(lr_batch *batch, uint32_t member, float *rgba, uint64_t float_count);
 /* The autotuner: times trial passes (which trace but change no film and move no member
- * on) for each BVH width (2, 4, 8; a width every member falls back from is skipped)
- * and pool fill (a quarter, half or all of the pool), on the members as they stand, and
- * keeps the fastest for the passes that follow. Images do not change, only speed. */
+ * on) on the members as they stand. For each scene-size class present (under 16k
+ * triangles, under 128k, larger) it keeps the BVH width (2, 4, 8; a width all of the
+ * class's members fall back from is skipped) whose passes of that class alone run
+ * fastest; a pass then takes the width of the class holding most of its paths. Then it
+ * keeps the fastest pool fill (a quarter, half or all of the pool) for the mixed passes.
+ * Images do not change, only speed. */
 typedef struct {
-    uint32_t width;      /* the BVH width chosen */
-    uint32_t fill;       /* paths a pass */
-    double paths_per_ms; /* the chosen candidate's measured rate */
-    uint32_t candidates; /* candidates timed */
+    uint32_t width;            /* the widest BVH width chosen for any class */
+    uint32_t fill;             /* paths a pass */
+    double paths_per_ms;       /* the chosen fill's measured rate */
+    uint32_t candidates;       /* candidates timed */
+    uint32_t class_width[3];   /* the width chosen per size class (0: class absent) */
+    uint32_t class_members[3]; /* members with samples to come, per size class */
 } lr_batch_tuning;
 int lr_batch_tune(lr_batch *batch, lr_batch_tuning *out);
 int lr_batch_passes(const lr_batch *batch, uint64_t *recorded, uint64_t *finished);

@@ -191,7 +191,7 @@ class BatchTuning(C.Structure):
     """lr_batch_tuning: the BVH width and paths a pass the autotuner chose, the chosen
     candidate's measured rate and how many candidates it timed."""
     _fields_ = [("width", C.c_uint32), ("fill", C.c_uint32), ("paths_per_ms", C.c_double),
-                ("candidates", C.c_uint32)]
+                ("candidates", C.c_uint32), ("class_width", C.c_uint32 * 3), ("class_members", C.c_uint32 * 3)]
 
 
 class ServerSettings(C.Structure):
@@ -860,7 +860,8 @@ class Batch:
         t = BatchTuning()
         _check(lib.lr_batch_tune(self.handle, C.byref(t)))
         return {"width": int(t.width), "fill": int(t.fill), "paths_per_ms": float(t.paths_per_ms),
-                "candidates": int(t.candidates)}
+                "candidates": int(t.candidates), "class_width": list(t.class_width),
+                "class_members": list(t.class_members)}
 
     def passes(self):
         rec, fin = C.c_uint64(), C.c_uint64()

@@ -678,6 +678,11 @@ struct MemberHost {
 // The traversal variants a pass can take: (BVH width, stack entries).
 #define LR_TRAVERSALS(X) X(8, 32) X(8, 48) X(4, 32) X(4, 48) X(2, 32) X(2, 64) X(2, 96)
 
+// Scene-size classes the autotuner keeps a BVH width for: under 16k triangles, under
+// 128k, and larger.
+constexpr int kSizeClasses = 3;
+inline int size_class(uint64_t triangles) { return triangles < 16384 ? 0 : (triangles < 131072 ? 1 : 2); }
+
 struct PassRecord {
     uint64_t number;
     std::vector<std::pair<uint32_t, bool>> members;  // member, sample ended
@@ -725,9 +730,9 @@ struct WaveHost {
     std::deque<PassRecord> in_flight;
     double kernel_ms[10] = {0};
     uint32_t rotate = 0;  // the member the next plan starts from
-    // Tunables (lr_batch_tune): the BVH width asked of every member (0: the default) and
-    // the most paths a pass takes.
-    int width = 0;
+    // Tunables (lr_batch_tune): the BVH width asked for each scene-size class (0: the
+    // default) and the most paths a pass takes.
+    int class_width[kSizeClasses] = {0, 0, 0};
     uint32_t fill = 0;
     Staging staging;  // member uploads
 };
@@ -1088,15 +1093,14 @@ void settle(WaveHost *h) {
 // Plans and launches one pass: each member with work left adds its next segment, in
 // turn from `rotate`, until the pass holds `fill` paths. A member takes one segment a
 // pass at most, so a pixel never gets two samples in one pass. A dry pass (autotuning)
-// plans the same way but moves no member on and leaves the films alone. Returns false
-// with no work.
-bool launch_pass(WaveHost *h, bool dry = false) {
+// plans the same way, from the members of size class `only` when it is not -1, but
+// moves no member on and leaves the films alone. Returns false with no work.
+bool launch_pass(WaveHost *h, bool dry = false, int only = -1) {
     Lane &lane = lane_of(h, h->recorded);
     Plan *staging = lane.h_plan;
     Segment *seg = staging->seg;
     uint32_t n = 0, used = 0, converts = 0;
-    int width = 0, stack = 32;
-    bool mixed = false;
+    uint64_t class_paths[kSizeClasses] = {0, 0, 0};
     PassRecord rec;
     rec.number = h->recorded;
     const uint32_t cap = h->capacity;
@@ -1106,6 +1110,8 @@ bool launch_pass(WaveHost *h, bool dry = false) {
         const uint32_t index = (h->rotate + step) % cap;
         MemberHost &mh = h->members[index];
         if (!has_work(mh)) continue;
+        const int cls = size_class(mh.dev.scene.triangle_count);
+        if (only >= 0 && cls != only) continue;
         const uint64_t left = mh.dev.pixels - mh.next_pixel;
         const uint32_t count = (uint32_t)std::min<uint64_t>(left, fill - used);
         const bool ends = count == left && !dry;
@@ -1123,23 +1129,27 @@ bool launch_pass(WaveHost *h, bool dry = false) {
             }
         }
         mh.last_pass = h->recorded + 1;
-        const TraversalChoice c = choose_traversal(mh.dev.scene, h->width);
-        if (width == 0) width = c.width;
-        else if (width != c.width) mixed = true;
-        stack = std::max(stack, c.stack);
+        class_paths[cls] += count;
         last = index;
     }
     if (n == 0) return false;
     if (!dry) h->rotate = (last + 1) % cap;
-    // One traversal variant serves the pass: the members' common width with the deepest
-    // stack among them, or the BVH2 when their widths differ.
-    if (mixed) {
-        width = 2;
+    // One traversal variant serves the pass: the width tuned for the size class holding
+    // most of its paths, with the deepest stack among its members -- or the BVH2 when a
+    // member's stack bound does not fit that width.
+    const int dominant = (int)(std::max_element(class_paths, class_paths + kSizeClasses) - class_paths);
+    int width = choose_traversal(h->members[rec.members[0].first].dev.scene, h->class_width[dominant]).width;
+    int stack = 32;
+    for (int attempt = 0; attempt < 2; attempt++) {
+        bool fits = true;
         stack = 32;
         for (auto &[m, ended] : rec.members) {
-            const TraversalChoice c = choose_traversal(h->members[m].dev.scene, 2);
+            const TraversalChoice c = choose_traversal(h->members[m].dev.scene, width);
+            if (c.width != width) fits = false;
             stack = std::max(stack, c.stack);
         }
+        if (fits || width == 2) break;
+        width = 2;
     }
     const int variant = width * 1000 + stack;
     staging->head = PlanHeader{n, used, converts, dry ? 1u : 0u};
@@ -1186,64 +1196,91 @@ bool wave_advance(WaveHost *h) {
     return !h->in_flight.empty();
 }
 
-// Times dry passes of every candidate (BVH width, paths a pass) on the members as they
-// stand and keeps the fastest.
+// Times two dry passes from the current plan settings (members of size class `only`, or
+// all) and returns their paths a millisecond.
+double time_dry(WaveHost *h, int only, cudaEvent_t a, cudaEvent_t b) {
+    launch_pass(h, true, only);  // warm: builds the variant's graph
+    settle(h);
+    uint64_t paths = 0;
+    LR_CUDA(cudaEventRecord(a, h->ctx->stream));
+    for (int i = 0; i < 2; i++) {
+        if (!launch_pass(h, true, only)) break;
+        paths += h_plan_paths(h);
+    }
+    join_lanes(h);
+    LR_CUDA(cudaEventRecord(b, h->ctx->stream));
+    LR_CUDA(cudaEventSynchronize(b));
+    settle(h);
+    float ms = 0.0f;
+    LR_CUDA(cudaEventElapsedTime(&ms, a, b));
+    return (double)paths / std::max(1e-3f, ms);
+}
+
+// The autotuner, on dry passes over the members as they stand: for each scene-size class
+// present, the BVH width (2, 4, 8; a width all its members fall back from is skipped)
+// whose passes of that class alone run fastest; then, with those widths, the pool fill
+// (a quarter, half or all of the pool) of the mixed passes.
 void wave_tune(WaveHost *h, lr_batch_tuning *out) {
     settle(h);
     if (!std::any_of(h->members.begin(), h->members.end(), has_work))
         fail(LR_INVALID, "tuning needs members with samples to come");
-    cudaStream_t stream = h->ctx->stream;
+    if (out) *out = lr_batch_tuning{};
     cudaEvent_t a, b;
     LR_CUDA(cudaEventCreate(&a));
     LR_CUDA(cudaEventCreate(&b));
-    double best = -1.0;
-    int best_width = 2;
-    uint32_t best_fill = h->pool, tried = 0;
-    std::vector<std::vector<int>> seen;
-    for (int width : {2, 4, 8}) {
-        // A width every member falls back from is a width already tried.
-        std::vector<int> got;
+    uint32_t tried = 0;
+    h->fill = h->pool;
+    for (int cls = 0; cls < kSizeClasses; cls++) {
+        uint32_t members = 0;
         for (auto &mh : h->members)
-            if (has_work(mh)) got.push_back(choose_traversal(mh.dev.scene, width).width * 1000 +
-                                            choose_traversal(mh.dev.scene, width).stack);
-        if (std::find(seen.begin(), seen.end(), got) != seen.end()) continue;
-        seen.push_back(got);
-        for (uint32_t fill : {h->pool / 4, h->pool / 2, h->pool}) {
-            if (fill == 0) continue;
-            h->width = width;
-            h->fill = fill;
-            launch_pass(h, true);  // warm: builds the variant's graph
-            settle(h);
-            uint64_t paths = 0;
-            LR_CUDA(cudaEventRecord(a, stream));
-            for (int i = 0; i < 2; i++) {
-                launch_pass(h, true);
-                paths += h_plan_paths(h);
-            }
-            join_lanes(h);
-            LR_CUDA(cudaEventRecord(b, stream));
-            LR_CUDA(cudaEventSynchronize(b));
-            settle(h);
-            float ms = 0.0f;
-            LR_CUDA(cudaEventElapsedTime(&ms, a, b));
-            const double rate = (double)paths / std::max(1e-3f, ms);
+            if (has_work(mh) && size_class(mh.dev.scene.triangle_count) == cls) members++;
+        if (out) out->class_members[cls] = members;
+        if (!members) continue;
+        double best = -1.0;
+        int best_width = 2;
+        std::vector<std::vector<int>> seen;
+        for (int width : {2, 4, 8}) {
+            std::vector<int> got;
+            for (auto &mh : h->members)
+                if (has_work(mh) && size_class(mh.dev.scene.triangle_count) == cls) {
+                    const TraversalChoice c = choose_traversal(mh.dev.scene, width);
+                    got.push_back(c.width * 1000 + c.stack);
+                }
+            if (std::find(seen.begin(), seen.end(), got) != seen.end()) continue;
+            seen.push_back(got);
+            h->class_width[cls] = width;
+            const double rate = time_dry(h, cls, a, b);
             tried++;
             if (rate > best) {
                 best = rate;
                 best_width = width;
-                best_fill = fill;
             }
+        }
+        h->class_width[cls] = best_width;
+        if (out) out->class_width[cls] = (uint32_t)best_width;
+    }
+    double best = -1.0;
+    uint32_t best_fill = h->pool;
+    for (uint32_t fill : {h->pool / 4, h->pool / 2, h->pool}) {
+        if (fill == 0) continue;
+        h->fill = fill;
+        const double rate = time_dry(h, -1, a, b);
+        tried++;
+        if (rate > best) {
+            best = rate;
+            best_fill = fill;
         }
     }
     cudaEventDestroy(a);
     cudaEventDestroy(b);
-    h->width = best_width;
     h->fill = best_fill;
     if (out) {
-        out->width = (uint32_t)best_width;
         out->fill = best_fill;
         out->paths_per_ms = best;
         out->candidates = tried;
+        int widest = 0;
+        for (int cls = 0; cls < kSizeClasses; cls++) widest = std::max(widest, h->class_width[cls]);
+        out->width = (uint32_t)(widest ? widest : 2);
     }
 }
 

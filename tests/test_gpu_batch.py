@@ -118,7 +118,10 @@ def test_tuning_changes_speed_not_images(ctx, cases):
             b.advance()
         t = b.tune()
         assert t["width"] in (2, 4, 8) and t["fill"] in (512, 1024, 2048)
-        assert t["candidates"] >= 3 and t["paths_per_ms"] > 0
+        assert t["candidates"] >= 4 and t["paths_per_ms"] > 0
+        # The cases hold scenes under 16k triangles and one of about 20k.
+        assert t["class_members"][0] >= 1 and t["class_members"][1] == 1 and t["class_members"][2] == 0
+        assert all(w in (2, 4, 8) for w in t["class_width"][:2]) and t["class_width"][2] == 0
         st = b.stats()
         b.finish()
         for m, want in zip(members, alone):
