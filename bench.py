@@ -592,7 +592,7 @@ def main():
             "cpu_baseline": cpu,
             "e2e": {"value": e2e_value, "unit": "Mrays/s", "h2d_bytes_per_step": 0,
                     "d2h_bytes_per_step": WIDTH * HEIGHT * 16},
-            "gpu_launches": K * (1 + 3 * (BOUNCES + 1) + 2),
+            "gpu_launches": K * (1 + 3 * (BOUNCES + 1) + 3),
             "clocks": clock_info,
             "batched": batch_info,
             "served": served_info,

@@ -64,25 +64,46 @@ struct Member {
     uint32_t width, height;
     uint64_t pixels;
     float4 *film, *image;
+    // Light tracing (connect.glsl): light paths a sample (0: none), the band their
+    // sampler numbers follow, 1 / a pixel's area on the image plane at unit distance, and
+    // the splat accumulators (3 fixed-point words a pixel: kSplatScale units of the
+    // film's terms): the film's, and one per lane that a pass's connections land in until
+    // the pass's finish stage folds them into the film's, in pass order.
+    uint32_t light_paths, light_band;
+    float pixel_area_inv;
+    unsigned long long *splat;
+    unsigned long long *splat_lane[2];
 };
 
+// Splats add as 64-bit integers (units of 2^-32 of the film's terms), so their sum does
+// not depend on the order the connections arrive in.
+constexpr double kSplatScale = 4294967296.0;
+constexpr float kSplatLimit = 1e9f;
+
 // `count` pixels of member `member` from `first_pixel`, at sample `sample`, in pool
-// paths path_base .. path_base + count. `convert`: this segment ends the member's
-// sample, so its image is brought up to date after the pass.
+// paths path_base .. path_base + count -- or, of kind kLightSegment, `count` of the
+// sample's light paths from number `first_pixel`. `convert`: this segment ends the
+// member's sample, so its image is brought up to date after the pass.
+constexpr uint32_t kCameraSegment = 0, kLightSegment = 1;
 struct Segment {
     uint32_t member, first_pixel, count, sample;
-    uint32_t path_base, convert, reserved0, reserved1;
+    uint32_t path_base, convert, kind, reserved;
 };
 
 // `dry`: a trial pass (autotuning) that traces its segments but leaves films alone.
+// `camera_paths`: the pass's camera paths; `folds`: members whose light paths it traces.
 struct PlanHeader {
     uint32_t segments, paths, converts, dry;
+    uint32_t camera_paths, folds, reserved0, reserved1;
 };
 
-// A pass's plan: its segments, and the members whose images it brings up to date.
+// A pass's plan: its segments, the members whose images it brings up to date (and the
+// samples they will then hold), and the members whose splats it folds into their films.
 struct Plan {
     PlanHeader head;
     uint32_t convert[kMaxSegments];
+    uint32_t convert_samples[kMaxSegments];
+    uint32_t fold[kMaxSegments];
     Segment seg[kMaxSegments];
 };
 
@@ -91,9 +112,11 @@ struct Wave {
     const Member *members;
     const Plan *plan;
     uint32_t pool, rounds;
+    uint32_t lane;  // which of the wave's two lanes this is
     // path state, one slot per pool path
     float4 *throughput, *radiance, *lambda, *vertex;  // vertex: last scattering point, w survival scale
-    uint4 *path;                                      // pixel, bounces, previous normal, ray pdf bits
+    float4 *mis;                                      // light tracing's MIS state (connect.glsl)
+    uint4 *path;  // pixel (a light path's emitter), bounces, previous normal, ray pdf bits
     // ray queues (ping-pong by round) and their hits
     float4 *ray_o[2], *ray_d[2], *hits[2];
     float4 *shadow_o, *shadow_d, *shadow_c;
@@ -129,47 +152,10 @@ __device__ __forceinline__ const Member &member_of_tag(const Wave &w, uint32_t t
     return w.members[w.plan->seg[tag >> kPathBits].member];
 }
 
-// camera.comp:14-50: a jittered primary ray per pixel of every segment. Block 0 also
-// starts the pass's queue counters.
-__global__ void __launch_bounds__(kShadeBlock) camera_kernel(Wave w) {
-    const Plan *plan = w.plan;
-    const uint32_t paths = plan->head.paths;
-    if (blockIdx.x == 0) {
-        for (uint32_t i = threadIdx.x; i < 4 * w.rounds + 2; i += blockDim.x) w.counters[i] = i == 0 ? paths : 0u;
-    }
-    const uint32_t stride = gridDim.x * blockDim.x;
-    for (uint32_t path = blockIdx.x * blockDim.x + threadIdx.x; path < paths; path += stride) {
-        const uint32_t si = segment_of(plan, path);
-        const Segment &sg = plan->seg[si];
-        const Member &m = w.members[sg.member];
-        const uint32_t pixel = sg.first_pixel + (path - sg.path_base);
-        const uint32_t sample = sg.sample;
-        const uint32_t seed = m.k->seed;
-        const float3 position = make_float3(m.frame[0], m.frame[1], m.frame[2]);
-        const float3 corner = make_float3(m.frame[4], m.frame[5], m.frame[6]);
-        const float3 du = make_float3(m.frame[8], m.frame[9], m.frame[10]);
-        const float3 dv = make_float3(m.frame[12], m.frame[13], m.frame[14]);
-        const bool ortho = m.frame[3] > 0.5f;
-        const float4 u = sample4(seed, pixel, sample, kGroupCamera);
-        const float fx = (float)(pixel % m.width) + u.x, fy = (float)(pixel / m.width) + u.y;
-        const float3 film = corner + fx * du + fy * dv;
-        float3 origin = ortho ? position + film : position;
-        float3 direction = normalize(ortho ? cross(du, dv) : film);
-        if (!ortho && m.lens_radius > 0.0f) {
-            const float3 forward = make_float3(m.forward[0], m.forward[1], m.forward[2]);
-            const float3 focused = position + direction * (m.focus_distance / dot(direction, forward));
-            const float2 disk = concentric(make_float2(u.z, u.w));
-            origin = position + normalize(du) * (disk.x * m.lens_radius) + normalize(dv) * (disk.y * m.lens_radius);
-            direction = normalize(focused - origin);
-        }
-        w.path[path] = make_uint4(pixel, 0u, 0u, 0u);
-        w.throughput[path] = make_float4(1.0f, 1.0f, 1.0f, 1.0f);
-        w.radiance[path] = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
-        w.vertex[path] = make_float4(origin.x, origin.y, origin.z, 1.0f);
-        if (m.spectral) w.lambda[path] = sample_wavelengths(sample4(seed, pixel, sample, kGroupWavelength).x);
-        w.ray_o[0][path] = make_float4(origin.x, origin.y, origin.z, __uint_as_float(path | (si << kPathBits)));
-        w.ray_d[0][path] = make_float4(direction.x, direction.y, direction.z, kInfinity);
-    }
+// A light path's number among its sample's light paths.
+__device__ __forceinline__ uint32_t tag_light_index(const Wave &w, uint32_t tag) {
+    const Segment &sg = w.plan->seg[tag >> kPathBits];
+    return sg.first_pixel + ((tag & kPathMask) - sg.path_base);
 }
 
 // intersect_closest.comp:45-76: the nearest triangle, then the analytic lights
@@ -189,19 +175,25 @@ __global__ void __launch_bounds__(kTraceBlock) closest_kernel(Wave w, uint32_t r
     const uint32_t step = gridDim.x * blockDim.x;
     for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < count; i += step) {
         const float4 o = ray_o[i], d = ray_d[i];
-        const Member &m = member_of_tag(w, __float_as_uint(o.w));
-        const DeviceScene s = m.scene;
-        if (tr.start(s, Ray{xyz(o), 0.0f, xyz(d), d.w})) {
-            while (!tr.step(s, overflow, visits)) {
+        const uint32_t segment = __float_as_uint(o.w) >> kPathBits;
+        {
+            const DeviceScene s = w.members[w.plan->seg[segment].member].scene;
+            if (tr.start(s, Ray{xyz(o), 0.0f, xyz(d), d.w})) {
+                while (!tr.step(s, overflow, visits)) {
+                }
             }
         }
+        // The lights, read again past the traversal rather than held through it.
+        const Segment &sg = w.plan->seg[segment];
+        const Member &m = w.members[sg.member];
+        const bool flow = sg.kind == kLightSegment;  // light paths follow light
         uint32_t what = tr.h.slot >= 0 ? (uint32_t)tr.h.slot : kNone;
         float t = tr.h.t;
         const float4 *lights = m.lights;
         const uint32_t light_count = m.light_count;
         for (uint32_t light = 0; light < light_count; light++) {
             if (round == 0 && !light_visible(lights, light)) continue;
-            const float tl = intersect_light(lights, light, tr.r.o, tr.r.d, t);
+            const float tl = intersect_light(lights, light, tr.r.o, tr.r.d, t, flow);
             if (tl < t) {
                 t = tl;
                 what = kLightHit | light;
@@ -213,7 +205,9 @@ __global__ void __launch_bounds__(kTraceBlock) closest_kernel(Wave w, uint32_t r
     if (kCount) add_visits(&w.stats[4], visits);
 }
 
-// intersect_shadow.comp:51-92: unblocked light samples join their path's radiance.
+// intersect_shadow.comp:28-92: unblocked light samples join their path's radiance; a light
+// path's camera connection, unless a light the camera sees stands in it, splats its value
+// (in the film's terms) on its pixel in the lane's accumulator.
 template <int W, int kStack, bool kCount>
 __global__ void __launch_bounds__(kTraceBlock) shadow_kernel(Wave w, uint32_t round) {
     __shared__ int stack[TracerOf<W, true, kStack, kCount>::kInts * kTraceBlock];
@@ -225,14 +219,32 @@ __global__ void __launch_bounds__(kTraceBlock) shadow_kernel(Wave w, uint32_t ro
     for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < count; i += step) {
         const float4 o = w.shadow_o[i], d = w.shadow_d[i];
         const uint32_t tag = __float_as_uint(o.w);
-        const DeviceScene s = member_of_tag(w, tag).scene;
+        const Segment &sg = w.plan->seg[tag >> kPathBits];
+        const Member &m = w.members[sg.member];
+        const bool light_path = sg.kind == kLightSegment;
+        if (light_path) {
+            bool seen = false;
+            for (uint32_t light = 0; light < m.light_count && !seen; light++)
+                seen = light_visible(m.lights, light) && intersect_light(m.lights, light, xyz(o), xyz(d), d.w, true) < d.w;
+            if (seen) continue;
+        }
+        const DeviceScene s = m.scene;
         if (tr.start(s, Ray{xyz(o), 0.0f, xyz(d), d.w})) {
             while (!tr.step(s, overflow, visits)) {
             }
         }
-        if (tr.h.id < 0) {
+        if (tr.h.id >= 0) continue;
+        const float4 c = w.shadow_c[i];
+        if (!light_path) {
             const uint32_t path = tag & kPathMask;
-            w.radiance[path] = w.radiance[path] + w.shadow_c[i];
+            w.radiance[path] = w.radiance[path] + c;
+        } else if (!w.plan->head.dry && isfinite(c.x) && isfinite(c.y) && isfinite(c.z)) {
+            unsigned long long *at = m.splat_lane[w.lane] + (size_t)__float_as_uint(c.w) * 3;
+            const float v[3] = {c.x, c.y, c.z};
+            for (int k = 0; k < 3; k++) {
+                const float clamped_v = fminf(fmaxf(v[k], -kSplatLimit), kSplatLimit);
+                atomicAdd(at + k, (unsigned long long)llrint((double)clamped_v * kSplatScale));
+            }
         }
     }
     if (overflow) atomicAdd(&w.status[0], 1);
@@ -290,6 +302,301 @@ __device__ __forceinline__ bool sample_triangle(const Member &m, uint32_t slot, 
     return true;
 }
 
+// ---- Light tracing (shaders/connect.glsl, common.glsl:112-140) ---------------------------
+
+// camera_pdf (common.glsl:132-135): the camera's density of a ray along d, per unit of a
+// pixel's area on the image plane at unit distance.
+__device__ __forceinline__ float camera_pdf(const Member &m, float3 d) {
+    const float c = dot(d, make_float3(m.forward[0], m.forward[1], m.forward[2]));
+    return c > 0.0f ? m.pixel_area_inv / (c * c * c) : 0.0f;
+}
+
+// lens_point (common.glsl:125-130).
+__device__ __forceinline__ float3 lens_point(const Member &m, float2 u) {
+    const float3 position = make_float3(m.frame[0], m.frame[1], m.frame[2]);
+    if (m.lens_radius <= 0.0f) return position;
+    const float2 disk = concentric(u) * m.lens_radius;
+    return position + normalize(make_float3(m.frame[8], m.frame[9], m.frame[10])) * disk.x +
+           normalize(make_float3(m.frame[12], m.frame[13], m.frame[14])) * disk.y;
+}
+
+// camera_pixel (connect.glsl:30-45): the pixel the camera sees p through from `lens`, and
+// the unit direction and distance from there to p; false behind the camera or off image.
+__device__ __forceinline__ bool camera_pixel(const Member &m, float3 p, float3 lens, uint32_t &pixel, float3 &d,
+                                             float &distance) {
+    const float3 offset = p - lens;
+    distance = length(offset);
+    d = offset * (1.0f / fmaxf(distance, 1e-20f));
+    const float c = dot(d, make_float3(m.forward[0], m.forward[1], m.forward[2]));
+    if (c <= 1e-6f || distance <= 0.0f) return false;
+    const float3 position = make_float3(m.frame[0], m.frame[1], m.frame[2]);
+    const float3 corner = make_float3(m.frame[4], m.frame[5], m.frame[6]);
+    const float3 du = make_float3(m.frame[8], m.frame[9], m.frame[10]);
+    const float3 dv = make_float3(m.frame[12], m.frame[13], m.frame[14]);
+    const float focus = m.focus_distance;
+    const float3 film = (m.lens_radius > 0.0f ? (lens + d * (focus / c) - position) / focus : d / c) - corner;
+    const float x = dot(film, du) / dot(du, du), y = dot(film, dv) / dot(dv, dv);
+    if (!(x >= 0.0f && y >= 0.0f && x < (float)m.width && y < (float)m.height)) return false;
+    pixel = (uint32_t)y * m.width + (uint32_t)x;
+    return true;
+}
+
+__device__ __forceinline__ float node_energy(const TreeView &t, uint32_t node) {
+    return fmaxf(__ldg(&t.nodes[node * 3]).w, 0.0f);
+}
+
+// emitter_power_pdf (connect.glsl:68-83): an emitter's chance of starting a light path.
+__device__ __forceinline__ float emitter_power_pdf(const TreeView &t, uint32_t emitter) {
+    const uint4 record = __ldg(&t.records[emitter]);
+    const uint32_t trail = record.y, depth = record.z;
+    uint32_t node = 0;
+    float pdf = 1.0f;
+    for (uint32_t level = 0; level < depth; level++) {
+        const uint32_t link = __ldg(&t.links[node]).x;
+        const float left = node_energy(t, link), right = node_energy(t, link + 1u);
+        if (left + right <= 0.0f) return 0.0f;
+        const uint32_t bit = (trail >> level) & 1u;
+        pdf *= (bit == 0u ? left : right) / (left + right);
+        node = link + bit;
+    }
+    return pdf;
+}
+
+// emitter_by_power (connect.glsl:86-110).
+__device__ __forceinline__ bool emitter_by_power(const TreeView &t, float u, uint32_t &emitter, float &pdf) {
+    pdf = 1.0f;
+    emitter = 0;
+    if (t.node_count < 1) return false;
+    uint32_t node = 0;
+    for (uint32_t depth = 0; depth < 64u; depth++) {
+        const uint2 link = __ldg(&t.links[node]);
+        if ((link.y & kLeafNode) != 0u) {
+            emitter = link.x;
+            return pdf > 0.0f;
+        }
+        const float left = node_energy(t, link.x), right = node_energy(t, link.x + 1u);
+        if (left + right <= 0.0f) return false;
+        const float chance = left / (left + right);
+        if (u < chance) {
+            u = fminf(u / chance, 0.99999994f);
+            pdf *= chance;
+            node = link.x;
+        } else {
+            u = fminf((u - chance) / (1.0f - chance), 0.99999994f);
+            pdf *= 1.0f - chance;
+            node = link.x + 1u;
+        }
+    }
+    return false;
+}
+
+__device__ __forceinline__ bool emitter_is_triangle(const Member &m, uint32_t emitter) {
+    return (__ldg(&m.tree.records[emitter]).x & kEmitterTriangle) != 0u;
+}
+
+// emitter_area_pdf (connect.glsl:116-132). No light paths start from afar here: at the
+// Lambertian settings nothing casts caustics (loading.lucb:127-146).
+__device__ __forceinline__ float emitter_area_pdf(const Member &m, uint32_t emitter) {
+    const uint32_t code = __ldg(&m.tree.records[emitter]).x;
+    float area;
+    if (code & kEmitterTriangle) {
+        const uint32_t t = code & ~kEmitterTriangle;
+        const float3 a = position_of(m, m.scene.indices[t * 3]);
+        area = 0.5f * length(cross(position_of(m, m.scene.indices[t * 3 + 1]) - a, position_of(m, m.scene.indices[t * 3 + 2]) - a));
+    } else if (light_type(m.lights, code) == kLightSphere) {
+        const float r = light_at(m.lights, code, 1).w;
+        area = 4.0f * kPi * r * r;
+    } else {
+        area = light_at(m.lights, code, 3).w;
+    }
+    return area > 0.0f ? emitter_power_pdf(m.tree, emitter) / area : 0.0f;
+}
+
+__device__ __forceinline__ float emission_direction_pdf(const Member &m, uint32_t emitter, float c) {
+    return fabsf(c) / (emitter_is_triangle(m, emitter) ? 2.0f * kPi : kPi);
+}
+
+// camera_hit_ratio (connect.glsl:141-149): at a light the camera path's BSDF ray hit, the
+// light tracer's density over the camera's.
+__device__ __forceinline__ float camera_hit_ratio(const Member &m, float4 mis, uint32_t emitter, float cos_light,
+                                                  float distance, float bsdf_pdf) {
+    if (emitter == kNone || mis.y <= 0.0f || bsdf_pdf <= 0.0f) return 0.0f;
+    const float d2 = distance * distance;
+    const float at_vertex = emission_direction_pdf(m, emitter, cos_light) * mis.z / d2 / mis.y;
+    const float at_light = emitter_area_pdf(m, emitter) / (bsdf_pdf * fabsf(cos_light) / d2);
+    return mis.x * at_vertex * at_light;
+}
+
+// light_cos (lights.glsl:228-232).
+__device__ __forceinline__ float light_cos(const float4 *lights, uint32_t light, float3 o, float3 d, float t) {
+    const float4 row0 = light_at(lights, light, 0);
+    if ((uint32_t)row0.w == kLightSphere) return fmaxf(0.0f, -dot(d, normalize(o + d * t - xyz(row0))));
+    return fmaxf(0.0f, -dot(d, xyz(light_at(lights, light, 3))));
+}
+
+// light_sampler_pdf (connect.glsl:52-62) at the Lambertian settings: the pdf the light
+// sampler at a surface (shading normal n, geometric g, facing one side) gives `to` when
+// the light path arrived from `from` (both leaving the point).
+__device__ __forceinline__ float light_sampler_pdf(float p_diffuse, float3 n, float3 g, float3 from, float3 to) {
+    const bool same = dot(from, g) >= 0.0f;
+    const float3 nv = same ? n : -n, gv = same ? g : -g;
+    const float wo_z = dot(from, nv), wi_z = dot(to, nv);
+    if ((dot(to, gv) > 0.0f) != (wi_z > 0.0f)) return 0.0f;
+    if (wo_z <= 0.0f || wi_z <= 0.0f) return 0.0f;
+    return p_diffuse * wi_z / kPi;
+}
+
+// light_sample_ratio (light_paths.glsl:18-33): the light sample a camera path at p (the
+// surface seen from the camera's side: normal sn, geometric sg) would take toward the
+// light path's first point x0, over its BSDF pdf toward it.
+__device__ __forceinline__ float light_sample_ratio(const Member &m, const Constants &k, uint32_t emitter, float3 sn,
+                                                    float3 sg, float3 p, float3 x0, float bsdf_pdf) {
+    if (!(bsdf_pdf > 0.0f)) return 0.0f;
+    const float3 from = offset_origin(p, sg);
+    const float3 offset = x0 - from;
+    const float reach = length(offset);
+    const float3 d = offset / reach;
+    const float chance = (1.0f - k.p_distant) * tree_pdf(m.tree, emitter, from, sn);
+    const uint32_t code = __ldg(&m.tree.records[emitter]).x;
+    const float pdf = (code & kEmitterTriangle) ? triangle_hit_pdf(m, code & ~kEmitterTriangle, d, reach)
+                                                : light_hit_pdf(m.lights, code, from, d, reach);
+    return chance * pdf / bsdf_pdf;
+}
+
+// light_emit.comp:55-136 for an emitter of the light tree (no light paths start from afar
+// at the Lambertian settings): light path `path` of segment `sg`, its sampler number
+// 0x80000000 | (band + its index), from an emitter chosen by power, a point on it uniform
+// by area, a cosine-weighted direction (either side of an emissive triangle). A path
+// that cannot start gets a ray that reaches nothing.
+template <bool kSpectral>
+__device__ __forceinline__ void light_emit(const Wave &w, const Member &m, const Segment &sg, uint32_t si, uint32_t path) {
+    const uint32_t id = 0x80000000u | (m.light_band + sg.first_pixel + (path - sg.path_base));
+    const uint32_t seed = m.k->seed;
+    const float4 u_point = sample4(seed, id, sg.sample, kGroupCamera);
+    const float4 u_pick = sample4(seed, id, sg.sample, kGroupWavelength);
+    const float4 lambda = kSpectral ? sample_wavelengths(u_pick.x) : make_float4(0.0f, 0.0f, 0.0f, 0.0f);
+    const float tag = __uint_as_float(path | (si << kPathBits));
+    auto dead = [&] {
+        w.path[path] = make_uint4(kNone, 0u, 0u, 0u);
+        w.ray_o[0][path] = make_float4(0.0f, 0.0f, 0.0f, tag);
+        w.ray_d[0][path] = make_float4(0.0f, 0.0f, 1.0f, 0.0f);
+    };
+    uint32_t emitter;
+    float chance;
+    if (!emitter_by_power(m.tree, u_pick.y / fmaxf(1e-7f, 1.0f), emitter, chance)) return dead();
+    const uint32_t code = __ldg(&m.tree.records[emitter]).x;
+    float3 q, n;
+    float4 radiance;
+    float area;
+    bool two_sided = false;
+    if (code & kEmitterTriangle) {
+        const uint32_t t = code & ~kEmitterTriangle;
+        const float3 a = position_of(m, m.scene.indices[t * 3]);
+        const float3 b = position_of(m, m.scene.indices[t * 3 + 1]);
+        const float3 c = position_of(m, m.scene.indices[t * 3 + 2]);
+        const float r = sqrtf(u_point.x);
+        q = a * (1.0f - r) + b * (r * (1.0f - u_point.y)) + c * (r * u_point.y);
+        const float3 cross_ab = cross(b - a, c - a);
+        area = 0.5f * length(cross_ab);
+        n = cross_ab / fmaxf(2.0f * area, 1e-30f);
+        if (u_pick.z < 0.5f) n = -n;
+        two_sided = true;
+        const uint32_t material = __ldg(&m.scene.shading[t]).w;
+        radiance = spec_of<kSpectral>(material_at(m, material, 6), xyz(material_at(m, material, 7)), lambda);
+    } else {
+        const uint32_t type = light_type(m.lights, code);
+        const float4 row0 = light_at(m.lights, code, 0);
+        if (type == kLightSphere) {
+            const float r = light_at(m.lights, code, 1).w;
+            const float z = 1.0f - 2.0f * u_point.x;
+            const float sz = sqrtf(fmaxf(0.0f, 1.0f - z * z));
+            const float phi = 2.0f * kPi * u_point.y;
+            n = make_float3(sz * cosf(phi), sz * sinf(phi), z);
+            q = xyz(row0) + r * n;
+            area = 4.0f * kPi * r * r;
+        } else {
+            const float2 a = type == kLightRect ? make_float2(2.0f * u_point.x - 1.0f, 2.0f * u_point.y - 1.0f)
+                                                : concentric(make_float2(u_point.x, u_point.y));
+            q = xyz(row0) + a.x * xyz(light_at(m.lights, code, 1)) + a.y * xyz(light_at(m.lights, code, 2));
+            n = xyz(light_at(m.lights, code, 3));
+            area = light_at(m.lights, code, 3).w;
+        }
+        radiance = light_radiance<kSpectral>(m.lights, code, lambda);
+    }
+    if (area <= 0.0f) return dead();
+    const float2 disk = concentric(make_float2(u_point.z, u_point.w));
+    const float cos_n = sqrtf(fmaxf(0.0f, 1.0f - (disk.x * disk.x + disk.y * disk.y)));
+    if (cos_n <= 0.0f) return dead();
+    float3 t, b;
+    basis(n, t, b);
+    const float3 direction = normalize(t * disk.x + b * disk.y + n * cos_n);
+    const float point_pdf = chance / area;
+    const float direction_pdf = cos_n / (two_sided ? 2.0f * kPi : kPi);
+    const float4 throughput = radiance * (cos_n / (point_pdf * direction_pdf));
+    const float largest = spec_max<kSpectral>(throughput);
+    if (!(largest > 0.0f)) return dead();
+    const float3 origin = offset_origin(q, n);
+    w.path[path] = make_uint4(emitter, 0u, 0u, __float_as_uint(direction_pdf));
+    w.throughput[path] = throughput;
+    if (kSpectral) w.lambda[path] = lambda;
+    // Russian roulette weighs throughput relative to the start's.
+    w.vertex[path] = make_float4(q.x, q.y, q.z, 1.0f / largest);
+    w.mis[path] = make_float4(1.0f, point_pdf, cos_n, -1.0f);
+    w.ray_o[0][path] = make_float4(origin.x, origin.y, origin.z, tag);
+    w.ray_d[0][path] = make_float4(direction.x, direction.y, direction.z, kInfinity);
+}
+
+// camera.comp:14-50: a jittered primary ray per pixel of every camera segment; the light
+// paths of every light segment (light_emit.comp). Block 0 also
+// starts the pass's queue counters.
+__global__ void __launch_bounds__(kShadeBlock) camera_kernel(Wave w) {
+    const Plan *plan = w.plan;
+    const uint32_t paths = plan->head.paths;
+    if (blockIdx.x == 0) {
+        for (uint32_t i = threadIdx.x; i < 4 * w.rounds + 2; i += blockDim.x) w.counters[i] = i == 0 ? paths : 0u;
+    }
+    const uint32_t stride = gridDim.x * blockDim.x;
+    for (uint32_t path = blockIdx.x * blockDim.x + threadIdx.x; path < paths; path += stride) {
+        const uint32_t si = segment_of(plan, path);
+        const Segment &sg = plan->seg[si];
+        const Member &m = w.members[sg.member];
+        if (sg.kind == kLightSegment) {
+            if (m.spectral) light_emit<true>(w, m, sg, si, path);
+            else light_emit<false>(w, m, sg, si, path);
+            continue;
+        }
+        const uint32_t pixel = sg.first_pixel + (path - sg.path_base);
+        const uint32_t sample = sg.sample;
+        const uint32_t seed = m.k->seed;
+        const float3 position = make_float3(m.frame[0], m.frame[1], m.frame[2]);
+        const float3 corner = make_float3(m.frame[4], m.frame[5], m.frame[6]);
+        const float3 du = make_float3(m.frame[8], m.frame[9], m.frame[10]);
+        const float3 dv = make_float3(m.frame[12], m.frame[13], m.frame[14]);
+        const bool ortho = m.frame[3] > 0.5f;
+        const float4 u = sample4(seed, pixel, sample, kGroupCamera);
+        const float fx = (float)(pixel % m.width) + u.x, fy = (float)(pixel / m.width) + u.y;
+        const float3 film = corner + fx * du + fy * dv;
+        float3 origin = ortho ? position + film : position;
+        float3 direction = normalize(ortho ? cross(du, dv) : film);
+        if (!ortho && m.lens_radius > 0.0f) {
+            const float3 forward = make_float3(m.forward[0], m.forward[1], m.forward[2]);
+            const float3 focused = position + direction * (m.focus_distance / dot(direction, forward));
+            const float2 disk = concentric(make_float2(u.z, u.w));
+            origin = position + normalize(du) * (disk.x * m.lens_radius) + normalize(dv) * (disk.y * m.lens_radius);
+            direction = normalize(focused - origin);
+        }
+        w.path[path] = make_uint4(pixel, 0u, 0u, 0u);
+        w.throughput[path] = make_float4(1.0f, 1.0f, 1.0f, 1.0f);
+        w.radiance[path] = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
+        w.vertex[path] = make_float4(origin.x, origin.y, origin.z, 1.0f);
+        if (m.spectral) w.lambda[path] = sample_wavelengths(sample4(seed, pixel, sample, kGroupWavelength).x);
+        // Light tracing's MIS: the light paths a sample, and the camera's pdf (camera.comp:42).
+        if (m.light_paths) w.mis[path] = make_float4((float)m.light_paths, 0.0f, 0.0f, camera_pdf(m, direction));
+        w.ray_o[0][path] = make_float4(origin.x, origin.y, origin.z, __uint_as_float(path | (si << kPathBits)));
+        w.ray_d[0][path] = make_float4(direction.x, direction.y, direction.z, kInfinity);
+    }
+}
+
 struct ShadeOut {
     bool next = false, shadow = false;
     float4 o, d, so, sd, sc;
@@ -300,8 +607,9 @@ __device__ __forceinline__ float rgb_luminance(float3 c) {
 }
 
 // One queue entry: a miss (shade_miss.comp:12-51), a light hit or a surface hit
-// (shade_surface.comp:48-312 at the Lambertian settings).
-template <bool kSpectral>
+// (shade_surface.comp:48-312 at the Lambertian settings). kTracing: members of the pass
+// may trace light paths, so camera paths weigh their techniques against them.
+template <bool kSpectral, bool kTracing>
 __device__ __forceinline__ void shade_one(const Wave &w, const Member &m, uint32_t sample, uint32_t round, uint32_t i,
                                           float4 ro, ShadeOut &out) {
     const Constants &k = *m.k;
@@ -319,6 +627,8 @@ __device__ __forceinline__ void shade_one(const Wave &w, const Member &m, uint32
     const float t = hit.x;
     float4 radiance = w.radiance[path];
     const float4 *lights = m.lights;
+    const bool tracing = kTracing && m.light_paths != 0u;
+    const float4 mis = tracing ? w.mis[path] : make_float4(0.0f, 0.0f, 0.0f, 0.0f);
 
     if (what == kNone) {
         float4 r = spec_of<kSpectral>(k.background_fit, k.background_rgb, lambda);
@@ -355,7 +665,9 @@ __device__ __forceinline__ void shade_one(const Wave &w, const Member &m, uint32
             const uint32_t emitter = (uint32_t)light_at(lights, light, 6).w;
             const float reach = length(vertex - (origin + t * dir));
             const float chance = (1.0f - k.p_distant) * tree_pdf(m.tree, emitter, vertex, octahedral_decode(pu.z));
-            weight = mis_weight(light_hit_pdf(lights, light, vertex, dir, reach) * chance / ray_pdf, 0.0f);
+            const float traced =
+                tracing ? camera_hit_ratio(m, mis, emitter, light_cos(lights, light, vertex, dir, reach), reach, ray_pdf) : 0.0f;
+            weight = mis_weight(light_hit_pdf(lights, light, vertex, dir, reach) * chance / ray_pdf, traced);
         }
         w.radiance[path] = radiance + clamped<kSpectral>(throughput * light_radiance<kSpectral>(lights, light, lambda) * weight,
                                                           total, k.clamp_indirect);
@@ -372,6 +684,10 @@ __device__ __forceinline__ void shade_one(const Wave &w, const Member &m, uint32
     const uint32_t material = attributes.w;
     const float3 p = origin + t * dir;
     const float reach = length(vertex - p);
+    // The camera's density of this vertex (area), and what turns the light sampler's pdf
+    // here toward the last vertex into that vertex's density (shade_surface.comp:91-94).
+    const float density = (total == 0u ? mis.w : ray_pdf) * fabsf(dot(dir, geometric)) / (reach * reach);
+    const float back_reach = mis.z / (reach * reach);
 
     const float4 emission_row = material_at(m, material, 7);
     if (emission_row.w > 0.0f) {
@@ -379,7 +695,8 @@ __device__ __forceinline__ void shade_one(const Wave &w, const Member &m, uint32
         const uint32_t emitter = m.tree.triangle_map ? __ldg(&m.tree.triangle_map[slot]) : kNone;
         if (total > 0u && ray_pdf > 0.0f && emitter != kNone) {
             const float chance = (1.0f - k.p_distant) * tree_pdf(m.tree, emitter, vertex, octahedral_decode(pu.z));
-            weight = mis_weight(triangle_hit_pdf(m, slot, dir, reach) * chance / ray_pdf, 0.0f);
+            const float traced = tracing ? camera_hit_ratio(m, mis, emitter, fabsf(dot(dir, geometric)), reach, ray_pdf) : 0.0f;
+            weight = mis_weight(triangle_hit_pdf(m, slot, dir, reach) * chance / ray_pdf, traced);
         }
         radiance = radiance + clamped<kSpectral>(throughput * spec_of<kSpectral>(material_at(m, material, 6), xyz(emission_row), lambda) * weight,
                                                  total, k.clamp_indirect);
@@ -407,6 +724,7 @@ __device__ __forceinline__ void shade_one(const Wave &w, const Member &m, uint32
     float4 emitted = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
     float chance = 0.0f;
     bool sampled = false;
+    uint32_t nee_emitter = kNone;
     if (u_light.x < k.p_distant) {
         float share;
         const uint32_t light = pick_distant(lights, m.light_count, u_light.x / k.p_distant, share);
@@ -420,6 +738,7 @@ __device__ __forceinline__ void shade_one(const Wave &w, const Member &m, uint32
         float tree_chance;
         if (tree_sample(m.tree, (u_light.x - k.p_distant) / fmaxf(1e-7f, 1.0f - k.p_distant), from, normal, emitter, tree_chance)) {
             chance = (1.0f - k.p_distant) * tree_chance;
+            nee_emitter = emitter;
             const uint32_t code = __ldg(&m.tree.records[emitter]).x;
             if (code & kEmitterTriangle) {
                 sampled = sample_triangle<kSpectral>(m, code & ~kEmitterTriangle, p, make_float2(u_light.y, u_light.z), lambda, s, emitted);
@@ -437,7 +756,18 @@ __device__ __forceinline__ void shade_one(const Wave &w, const Member &m, uint32
             if (bsdf_pdf > 0.0f) {
                 const float4 f = eon(base, roughness, wi, wo);
                 const float light_pdf = s.pdf * chance;
-                const float weight = s.delta ? 1.0f : mis_weight(bsdf_pdf / light_pdf, 0.0f);
+                // The light tracer's density of this path over the camera path's BSDF ray
+                // reaching the same light point (shade_surface.comp:210-224).
+                float traced = 0.0f;
+                if (tracing && !s.delta && nee_emitter != kNone && density > 0.0f) {
+                    const float d2 = s.distance * s.distance;
+                    const float at_last =
+                        total == 0u ? 1.0f : light_sampler_pdf(p_diffuse, normal, geometric, s.direction, -dir) * back_reach / mis.y;
+                    const float at_vertex = emission_direction_pdf(m, nee_emitter, s.cos_light) * fabsf(side) / d2 / density;
+                    const float at_light = emitter_area_pdf(m, nee_emitter) / (bsdf_pdf * s.cos_light / d2);
+                    traced = mis.x * at_last * at_vertex * at_light;
+                }
+                const float weight = s.delta ? 1.0f : mis_weight(bsdf_pdf / light_pdf, traced * bsdf_pdf / light_pdf);
                 const float4 contribution = clamped<kSpectral>(throughput * f * emitted * (fabsf(wi.z) * (weight / light_pdf)),
                                                                total, k.clamp_indirect);
                 const float3 target = p + s.direction * s.distance;
@@ -475,6 +805,13 @@ __device__ __forceinline__ void shade_one(const Wave &w, const Member &m, uint32
         throughput = make_float4(throughput.x / survive, throughput.y / survive, throughput.z / survive, throughput.w / survive);
     }
     const float3 next = side > 0.0f ? from : offset_origin(p, -geometric);
+    if (tracing) {
+        // This vertex's factor of the light tracer's density, settled now that the light
+        // sampler's direction here is known (shade_surface.comp:304-307).
+        const float at_last =
+            total == 0u ? 1.0f : light_sampler_pdf(p_diffuse, normal, geometric, direction, -dir) * back_reach / mis.y;
+        w.mis[path] = make_float4(mis.x * at_last, density, fabsf(side), 0.0f);
+    }
     w.path[path] = make_uint4(pixel, next_bounces, octahedral_encode(normal), __float_as_uint(pdf));
     w.throughput[path] = throughput;
     w.vertex[path] = make_float4(next.x, next.y, next.z, survival_scale);
@@ -483,9 +820,149 @@ __device__ __forceinline__ void shade_one(const Wave &w, const Member &m, uint32
     out.d = make_float4(direction.x, direction.y, direction.z, kInfinity);
 }
 
+// A light path's hit (light_paths.glsl:35-189) at the Lambertian settings: a light ends
+// it; at a surface it connects to the camera -- a shadow ray carrying, in the film's
+// terms and MIS-weighted, what the camera would see of it to the pixel it projects to --
+// and scatters on by the BSDF as seen from where the light came, weighed by the BSDF as
+// the camera would evaluate it, with the shading-normal correction light paths need.
+template <bool kSpectral>
+__device__ __noinline__ void shade_light(const Wave &w, const Member &m, uint32_t sample, uint32_t round, uint32_t i,
+                                            float4 ro, ShadeOut &out) {
+    const Constants &k = *m.k;
+    const uint32_t q = round & 1u;
+    const float4 hit = w.hits[q][i];
+    const uint32_t what = __float_as_uint(hit.y);
+    if (what == kNone || (what & kLightHit)) return;
+    const float4 rd = w.ray_d[q][i];
+    const uint32_t tag = __float_as_uint(ro.w);
+    const uint32_t path = tag & kPathMask;
+    const uint4 pu = w.path[path];
+    const uint32_t emitter = pu.x, bounces = pu.y, total = bounces & 0xffu;
+    const float ray_pdf = __uint_as_float(pu.w);
+    const float3 origin = xyz(ro), dir = xyz(rd);
+    float4 throughput = w.throughput[path];
+    const float4 lambda = kSpectral ? w.lambda[path] : make_float4(0.0f, 0.0f, 0.0f, 0.0f);
+    const float4 vertex_row = w.vertex[path];
+    const float4 mis = w.mis[path];
+    const uint32_t id = 0x80000000u | (m.light_band + tag_light_index(w, tag));
+
+    const uint32_t slot = what;
+    const float3 p0 = position_of(m, m.scene.indices[slot * 3]);
+    float3 geometric = normalize(cross(position_of(m, m.scene.indices[slot * 3 + 1]) - p0,
+                                       position_of(m, m.scene.indices[slot * 3 + 2]) - p0));
+    if (dot(geometric, dir) > 0.0f) geometric = -geometric;
+    const uint4 attributes = __ldg(&m.scene.shading[slot]);
+    const uint32_t material = attributes.w;
+    const float3 p = origin + hit.x * dir;
+    if (total >= k.max_bounces) return;
+    const float hu = hit.z, hv = hit.w;
+    float3 normal = normalize(octahedral_decode(attributes.x) * (1.0f - hu - hv) + octahedral_decode(attributes.y) * hu +
+                              octahedral_decode(attributes.z) * hv);
+    if (dot(normal, geometric) < 0.0f) normal = -normal;
+    const float4 u_lens = sample4(k.seed, id, sample, group_light(total));
+    const float3 lens = lens_point(m, make_float2(u_lens.x, u_lens.y));
+    uint32_t pixel = 0;
+    float3 to_point;
+    float camera_distance;
+    const bool on_film = camera_pixel(m, p, lens, pixel, to_point, camera_distance);
+    const float4 base_rgb = material_at(m, material, 1);
+    const float4 base = spec_of<kSpectral>(material_at(m, material, 0), xyz(base_rgb), lambda) * base_rgb.w;
+    const float roughness = material_at(m, material, 10).y;
+    const float p_diffuse = fmaxf(rgb_luminance(xyz(base_rgb) * base_rgb.w), 0.0f) > 0.0f ? 1.0f : 0.0f;
+    const float3 toward_light = -dir;
+    const float3 x_last = xyz(vertex_row);
+    const float reach = length(x_last - p);
+    const float cos_in = fabsf(dot(dir, geometric));
+    const float density = ray_pdf * cos_in / (reach * reach);
+    const float back_reach = mis.z / (reach * reach);
+    const float cos_shading_in = dot(toward_light, normal);
+    if (cos_shading_in <= 0.0f || cos_in < 1e-6f) return;
+    const float shading_in = cos_shading_in / cos_in;
+    const float L = (float)m.light_paths;
+
+    if (on_film) {
+        const float3 to_camera = -to_point;
+        const float side = dot(to_camera, geometric);
+        const float3 sn = side > 0.0f ? normal : -normal, sg = side > 0.0f ? geometric : -geometric;
+        float3 st, sb;
+        basis(sn, st, sb);
+        const float3 wo = make_float3(dot(to_camera, st), dot(to_camera, sb), dot(to_camera, sn));
+        const float3 wi = make_float3(dot(toward_light, st), dot(toward_light, sb), dot(toward_light, sn));
+        if ((dot(toward_light, sg) > 0.0f) == (wi.z > 0.0f) && wo.z > 0.0f && wi.z > 0.0f) {
+            const float camera_bsdf_pdf = p_diffuse * wi.z / kPi;
+            const float4 f = eon(base, roughness, wi, wo);
+            const float camera_density = camera_pdf(m, to_point) * fabsf(side) / (camera_distance * camera_distance);
+            const float4 contribution = throughput * f * (shading_in * camera_density / L);
+            if (spec_max<kSpectral>(contribution) > 0.0f) {
+                // The camera techniques' densities over this one's.
+                const float last = mis.y > 0.0f ? camera_bsdf_pdf * back_reach / mis.y : 0.0f;
+                const float ratio = mis.x * last * camera_density / density;
+                const float sample_ratio =
+                    total == 0u ? light_sample_ratio(m, k, emitter, sn, sg, p, x_last, camera_bsdf_pdf) : fmaxf(mis.w, 0.0f);
+                const float weight = mis_weight(ratio / L, ratio * sample_ratio / L);
+                const float margin = 4e-4f * fmaxf(1.0f, fmaxf(fabsf(p.x), fmaxf(fabsf(p.y), fabsf(p.z))));
+                const float3 so = offset_origin(p, sg);
+                const float3 value = spec_to_film<kSpectral>(contribution * weight, lambda, k);
+                out.shadow = true;
+                out.so = make_float4(so.x, so.y, so.z, ro.w);
+                out.sd = make_float4(to_camera.x, to_camera.y, to_camera.z, fmaxf(0.0f, camera_distance - margin));
+                out.sc = make_float4(value.x, value.y, value.z, __uint_as_float(pixel));
+            }
+        }
+    }
+
+    // Scatter on, unless the next vertex would be past the bounce limit.
+    if (total + 1u >= k.max_bounces) return;
+    const float4 u = sample4(k.seed, id, sample, group_bsdf(total));
+    float3 tangent, bitangent;
+    basis(normal, tangent, bitangent);
+    const float wo_light_z = dot(toward_light, normal);
+    if (wo_light_z <= 0.0f || !(u.w < p_diffuse)) return;
+    const float2 disk = concentric(make_float2(u.x, u.y));
+    const float3 wl = make_float3(disk.x, disk.y, sqrtf(fmaxf(0.0f, 1.0f - (disk.x * disk.x + disk.y * disk.y))));
+    if (wl.z == 0.0f) return;
+    const float light_pdf = p_diffuse * wl.z / kPi;
+    if (!(light_pdf > 0.0f)) return;
+    const float3 direction = tangent * wl.x + bitangent * wl.y + normal * wl.z;
+    const float side = dot(direction, geometric);
+    if ((side > 0.0f) != (wl.z > 0.0f)) return;
+    const float3 sn = side > 0.0f ? normal : -normal, sg = side > 0.0f ? geometric : -geometric;
+    float3 st, sb;
+    basis(sn, st, sb);
+    const float3 wo = make_float3(dot(direction, st), dot(direction, sb), dot(direction, sn));
+    const float3 wi = make_float3(dot(toward_light, st), dot(toward_light, sb), dot(toward_light, sn));
+    if ((dot(toward_light, sg) > 0.0f) != (wi.z > 0.0f)) return;
+    const bool lobe = wo.z > 0.0f && wi.z > 0.0f;
+    const float camera_bsdf_pdf = lobe ? p_diffuse * wi.z / kPi : 0.0f;
+    const float4 f = lobe ? eon(base, roughness, wi, wo) : make_float4(0.0f, 0.0f, 0.0f, 0.0f);
+    const uint32_t next_bounces = next_bounce(bounces, 0u, k.limits);
+    if (next_bounces == kNone) return;
+    throughput = throughput * f * (shading_in * fabsf(side) / light_pdf);
+    const float survival_scale = vertex_row.w;
+    if (total + 1u >= 3u) {
+        const float survive = fminf(0.95f, spec_max<kSpectral>(throughput) * survival_scale);
+        if (u.z >= survive) return;
+        throughput = make_float4(throughput.x / survive, throughput.y / survive, throughput.z / survive, throughput.w / survive);
+    }
+    if (!(spec_max<kSpectral>(throughput) > 0.0f)) return;
+    const float last = mis.y > 0.0f ? camera_bsdf_pdf * back_reach / mis.y : 0.0f;
+    const float sample_ratio = total == 0u ? light_sample_ratio(m, k, emitter, sn, sg, p, x_last, camera_bsdf_pdf) : mis.w;
+    const float3 next = offset_origin(p, side > 0.0f ? geometric : -geometric);
+    w.path[path] = make_uint4(emitter, next_bounces, 0u, __float_as_uint(light_pdf));
+    w.throughput[path] = throughput;
+    w.vertex[path] = make_float4(p.x, p.y, p.z, survival_scale);
+    w.mis[path] = make_float4(mis.x * last, density, fabsf(side), sample_ratio);
+    out.next = true;
+    out.o = make_float4(next.x, next.y, next.z, ro.w);
+    out.d = make_float4(direction.x, direction.y, direction.z, kInfinity);
+}
+
 // 8 blocks an SM (64 registers): shade_one wants 128, which leaves 16 warps an SM to hide
 // its memory latency; capped, it spills a little and runs 17 % faster (1.21 -> 1.01 ms a
 // 1080p pass on the 1M-triangle scene; 48 registers: 0.99 ms with twice the spills).
+// kTracing: the pass holds light paths or camera paths that weigh against them; passes
+// without take the kernel without that code (it cost camera-only passes 16 %).
+template <bool kTracing>
 __global__ void __launch_bounds__(kShadeBlock, 8) shade_kernel(Wave w, uint32_t round) {
     const uint32_t count = w.counters[round];
     const uint32_t q = round & 1u, nq = q ^ 1u;
@@ -500,8 +977,14 @@ __global__ void __launch_bounds__(kShadeBlock, 8) shade_kernel(Wave w, uint32_t 
             const float4 ro = w.ray_o[q][i];
             const Segment &sg = w.plan->seg[__float_as_uint(ro.w) >> kPathBits];
             const Member &m = w.members[sg.member];
-            if (m.spectral) shade_one<true>(w, m, sg.sample, round, i, ro, out);
-            else shade_one<false>(w, m, sg.sample, round, i, ro, out);
+            if (kTracing && sg.kind == kLightSegment) {
+                if (m.spectral) shade_light<true>(w, m, sg.sample, round, i, ro, out);
+                else shade_light<false>(w, m, sg.sample, round, i, ro, out);
+            } else if (m.spectral) {
+                shade_one<true, kTracing>(w, m, sg.sample, round, i, ro, out);
+            } else {
+                shade_one<false, kTracing>(w, m, sg.sample, round, i, ro, out);
+            }
         }
         const uint32_t at = warp_push(next_counter, out.next);
         if (out.next) {
@@ -524,7 +1007,9 @@ __global__ void __launch_bounds__(kShadeBlock) finish_kernel(Wave w) {
     const uint32_t stride = gridDim.x * blockDim.x;
     if (plan->head.dry) return;
     for (uint32_t path = blockIdx.x * blockDim.x + threadIdx.x; path < paths; path += stride) {
-        const Member &m = w.members[plan->seg[segment_of(plan, path)].member];
+        const Segment &sg = plan->seg[segment_of(plan, path)];
+        if (sg.kind == kLightSegment) continue;  // light paths reach the film by splats
+        const Member &m = w.members[sg.member];
         const uint32_t pixel = w.path[path].x;
         float3 value = m.spectral ? spec_to_film<true>(w.radiance[path], w.lambda[path], *m.k)
                                   : spec_to_film<false>(w.radiance[path], make_float4(0, 0, 0, 0), *m.k);
@@ -540,13 +1025,35 @@ __global__ void __launch_bounds__(kShadeBlock) finish_kernel(Wave w) {
         }
         w.stats[0] += closest;
         w.stats[1] += shadow;
-        w.stats[2] += paths;
+        w.stats[2] += plan->head.camera_paths;
         w.stats[3] += 1;
     }
 }
 
-// film_convert.comp:36-53: the film's average into the rgba32f ACEScg image, for every
-// member whose sample ended in this pass.
+// The splats this lane's light paths left for the members traced in this pass, added into
+// their films' splat accumulators (in pass order: the finish stages run one after another)
+// and cleared for the lane's next pass.
+__global__ void __launch_bounds__(kShadeBlock) fold_kernel(Wave w) {
+    const Plan *plan = w.plan;
+    if (plan->head.dry) return;
+    const uint32_t folds = plan->head.folds;
+    const uint64_t stride = (uint64_t)gridDim.x * blockDim.x;
+    for (uint32_t f = 0; f < folds; f++) {
+        const Member &m = w.members[plan->fold[f]];
+        unsigned long long *lane = m.splat_lane[w.lane];
+        for (uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; i < m.pixels * 3; i += stride) {
+            const unsigned long long v = lane[i];
+            if (v) {
+                m.splat[i] += v;
+                lane[i] = 0ull;
+            }
+        }
+    }
+}
+
+// film_convert.comp:36-53: the film's average, and the light paths' splats over the
+// samples taken, into the rgba32f ACEScg image, for every member whose sample ended in
+// this pass.
 __global__ void __launch_bounds__(kShadeBlock) convert_kernel(Wave w) {
     const Plan *plan = w.plan;
     const uint32_t converts = plan->head.converts;
@@ -554,10 +1061,17 @@ __global__ void __launch_bounds__(kShadeBlock) convert_kernel(Wave w) {
     for (uint32_t c = 0; c < converts; c++) {
         const Member &m = w.members[plan->convert[c]];
         const Constants &k = *m.k;
+        const double per_sample = m.light_paths ? 1.0 / (kSplatScale * (double)plan->convert_samples[c]) : 0.0;
         for (uint64_t pixel = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; pixel < m.pixels; pixel += stride) {
             const float4 sum = m.film[pixel];
             const float wsum = fmaxf(sum.w, 1.0f);
             float3 value = make_float3(sum.x / wsum, sum.y / wsum, sum.z / wsum);
+            if (m.light_paths) {
+                const unsigned long long *sp = m.splat + pixel * 3;
+                value = value + make_float3((float)((double)(long long)sp[0] * per_sample),
+                                            (float)((double)(long long)sp[1] * per_sample),
+                                            (float)((double)(long long)sp[2] * per_sample));
+            }
             if (m.spectral)
                 value = make_float3(k.film[0] * value.x + k.film[1] * value.y + k.film[2] * value.z,
                                     k.film[3] * value.x + k.film[4] * value.y + k.film[5] * value.z,
@@ -671,6 +1185,7 @@ struct MemberHost {
     void *block = nullptr;
     lr_gpu_scene *owned = nullptr;  // a renderer's own upload (null when borrowed)
     uint32_t samples = 0, sample = 0, next_pixel = 0, done = 0;
+    uint32_t light_next = 0;  // light paths of the current sample planned so far
     uint32_t max_bounces = 0;
     uint64_t last_pass = 0;  // the last pass (plus one) that traced it; 0: none
 };
@@ -734,6 +1249,9 @@ struct WaveHost {
     // default) and the most paths a pass takes.
     int class_width[kSizeClasses] = {0, 0, 0};
     uint32_t fill = 0;
+    // The most camera paths a pass takes (0: as many as fit): a renderer's band, so that
+    // its passes are the reference's bands, light paths riding along in a sample's first.
+    uint32_t camera_cap = 0;
     Staging staging;  // member uploads
 };
 
@@ -753,13 +1271,14 @@ void mark(cudaStream_t stream, Marks *marks, int kind) {
 // (closest, shade, shadow) for every round. With `marks`, an event follows each kernel
 // (profiling); kCount instantiates the counting traversals.
 template <int W, int kStack, bool kCount>
-void record_trace(const WaveHost *h, const Wave &w, int grid_trace, cudaStream_t stream, Marks *marks) {
+void record_trace(const WaveHost *h, const Wave &w, int grid_trace, bool tracing, cudaStream_t stream, Marks *marks) {
     camera_kernel<<<h->grid_shade, kShadeBlock, 0, stream>>>(w);
     mark(stream, marks, kCamera);
     for (uint32_t round = 0; round < w.rounds; round++) {
         closest_kernel<W, kStack, kCount><<<grid_trace, kTraceBlock, 0, stream>>>(w, round);
         mark(stream, marks, kClosest);
-        shade_kernel<<<h->grid_shade, kShadeBlock, 0, stream>>>(w, round);
+        if (tracing) shade_kernel<true><<<h->grid_shade, kShadeBlock, 0, stream>>>(w, round);
+        else shade_kernel<false><<<h->grid_shade, kShadeBlock, 0, stream>>>(w, round);
         mark(stream, marks, kSurface);
         shadow_kernel<W, kStack, kCount><<<grid_trace, kTraceBlock, 0, stream>>>(w, round);
         mark(stream, marks, kShadow);
@@ -770,6 +1289,8 @@ void record_trace(const WaveHost *h, const Wave &w, int grid_trace, cudaStream_t
 // Records a pass's film accumulation: finish, then convert.
 void record_finish(const WaveHost *h, const Wave &w, cudaStream_t stream, Marks *marks) {
     finish_kernel<<<h->grid_shade, kShadeBlock, 0, stream>>>(w);
+    mark(stream, marks, kFinish);
+    fold_kernel<<<h->grid_shade, kShadeBlock, 0, stream>>>(w);
     mark(stream, marks, kFinish);
     convert_kernel<<<h->grid_shade, kShadeBlock, 0, stream>>>(w);
     mark(stream, marks, kConvert);
@@ -794,14 +1315,20 @@ int grid_for(WaveHost *h, int variant) {
     return g;
 }
 
+// A pass's variant: its traversal (BVH width * 1000 + stack entries), plus kTracingVariant
+// when it holds light tracing.
+constexpr int kTracingVariant = 100000;
+
 void record_trace_any(WaveHost *h, const Wave &w, int variant, cudaStream_t stream, Marks *marks) {
     const bool count = h->profile == 2;
-    const int grid = grid_for(h, variant);
-    switch (variant) {
+    const bool tracing = variant >= kTracingVariant;
+    const int traversal = variant % kTracingVariant;
+    const int grid = grid_for(h, traversal);
+    switch (traversal) {
 #define LR_CASE(wd, k)                                                                        \
     case wd * 1000 + k:                                                                       \
-        if (count) record_trace<wd, k, true>(h, w, grid, stream, marks);                      \
-        else record_trace<wd, k, false>(h, w, grid, stream, marks);                           \
+        if (count) record_trace<wd, k, true>(h, w, grid, tracing, stream, marks);             \
+        else record_trace<wd, k, false>(h, w, grid, tracing, stream, marks);                  \
         break;
         LR_TRAVERSALS(LR_CASE)
 #undef LR_CASE
@@ -861,7 +1388,7 @@ void wave_create(WaveHost *h, lr_context *ctx, uint64_t pool, uint32_t rounds, u
         Layout L;
         const size_t p_throughput = L.add(nullptr, P * 16), p_radiance = L.add(nullptr, P * 16);
         const size_t p_lambda = L.add(nullptr, P * 16), p_vertex = L.add(nullptr, P * 16);
-        const size_t p_path = L.add(nullptr, P * 16);
+        const size_t p_path = L.add(nullptr, P * 16), p_mis = L.add(nullptr, P * 16);
         size_t p_ray[2][3];
         for (int q = 0; q < 2; q++)
             for (int j = 0; j < 3; j++) p_ray[q][j] = L.add(nullptr, P * 16);
@@ -874,8 +1401,10 @@ void wave_create(WaveHost *h, lr_context *ctx, uint64_t pool, uint32_t rounds, u
         char *base = (char *)lane.block;
         auto at = [&](size_t i) { return (void *)(base + L.parts[i].offset); };
         Wave &w = lane.w;
+        w.lane = (uint32_t)li;
         w.pool = h->pool;
         w.rounds = rounds;
+        w.mis = (float4 *)at(p_mis);
         w.throughput = (float4 *)at(p_throughput);
         w.radiance = (float4 *)at(p_radiance);
         w.lambda = (float4 *)at(p_lambda);
@@ -906,7 +1435,7 @@ void wave_create(WaveHost *h, lr_context *ctx, uint64_t pool, uint32_t rounds, u
     }
     upload_sobol_tables(ctx->stream);
     LR_CUDA(cudaStreamSynchronize(ctx->stream));
-    h->grid_shade = grid_of(shade_kernel, kShadeBlock, ctx->sm_count);
+    h->grid_shade = grid_of(shade_kernel<false>, kShadeBlock, ctx->sm_count);
     if (profile)
         for (auto &e : h->mark_start) LR_CUDA(cudaEventCreate(&e));
     else
@@ -927,6 +1456,29 @@ void validate(const lr_settings &s, const lr_frame &f) {
     if (s.noise_threshold > 0.0) fail(LR_INVALID, "adaptive sampling is not part of this build (noise_threshold 0)");
     if (s.guiding) fail(LR_INVALID, "path guiding is not part of this build (guiding off)");
     if (s.max_bounces > 253) fail(LR_INVALID, "this build traces at most 253 bounces");
+}
+
+// Loaded.light_paths (loading.lucb:163-168): light tracing's share of a view's pixels (at
+// least one), at most a band's (the pool setting, or every pixel when fewer), and the band
+// their sampler numbers follow. None for an orthographic camera or a scene without
+// emitters of the light tree (loading.lucb:149): no light paths start from afar, since at
+// the Lambertian settings nothing casts caustics (loading.lucb:127-146).
+struct LightPaths {
+    uint32_t count = 0, band = 0;
+    double pixel_area_inv = 0.0;
+};
+
+LightPaths light_paths_of(const lr_settings &settings, const lr_frame &frame, uint64_t pixels, size_t emitters) {
+    LightPaths out;
+    const uint64_t pool = settings.pool ? settings.pool : kDefaultPool;
+    out.band = (uint32_t)std::min<uint64_t>(pool, pixels);
+    if (!(settings.light_tracing > 0.0) || frame.orthographic || emitters == 0) return out;
+    const double wanted = std::max(1.0, std::floor(settings.light_tracing * (double)pixels + 0.5));
+    out.count = (uint32_t)std::min<double>(wanted, (double)out.band);
+    const double du = std::sqrt(frame.du[0] * frame.du[0] + frame.du[1] * frame.du[1] + frame.du[2] * frame.du[2]);
+    const double dv = std::sqrt(frame.dv[0] * frame.dv[0] + frame.dv[1] * frame.dv[1] + frame.dv[2] * frame.dv[2]);
+    out.pixel_area_inv = du * dv > 0.0 ? 1.0 / (du * dv) : 0.0;
+    return out;
 }
 
 // Makes `scene` (uploaded as `gs`) seen through `frame` a member; returns its index.
@@ -951,6 +1503,7 @@ uint32_t member_add(WaveHost *h, const lr_gpu_scene *gs, lr_gpu_scene *owned, co
     if (index == h->capacity) fail(LR_LIMIT, "the wave holds " + std::to_string(h->capacity) + " members");
     const Loaded L = load(*scene, settings);
     const uint64_t pixels = (uint64_t)frame.width * frame.height;
+    const LightPaths traced = light_paths_of(settings, frame, pixels, L.tree.emitter_count);
     Constants k{};
     for (int i = 0; i < 9; i++) k.film[i] = (float)L.film.m[i];
     k.cmf_integrals[0] = (float)L.cmf_integrals.x;
@@ -979,6 +1532,9 @@ uint32_t member_add(WaveHost *h, const lr_gpu_scene *gs, lr_gpu_scene *owned, co
     const size_t p_constants = lay.add(&k, sizeof k);
     const size_t p_film = lay.add(nullptr, pixels * 16);
     const size_t p_image = lay.add(nullptr, pixels * 16);
+    const size_t splat_bytes = traced.count ? pixels * 24 : 0;
+    const size_t p_splat = lay.add(nullptr, splat_bytes);
+    const size_t p_splat_lane0 = lay.add(nullptr, splat_bytes), p_splat_lane1 = lay.add(nullptr, splat_bytes);
     MemberHost &mh = h->members[index];
     // Stream-ordered: the member's memory and data arrive ahead of the next pass without
     // waiting for the passes in flight.
@@ -1023,6 +1579,12 @@ uint32_t member_add(WaveHost *h, const lr_gpu_scene *gs, lr_gpu_scene *owned, co
     m.pixels = pixels;
     m.film = (float4 *)at(p_film);
     m.image = (float4 *)at(p_image);
+    m.light_paths = traced.count;
+    m.light_band = traced.band;
+    m.pixel_area_inv = (float)traced.pixel_area_inv;
+    m.splat = traced.count ? (unsigned long long *)at(p_splat) : nullptr;
+    m.splat_lane[0] = traced.count ? (unsigned long long *)at(p_splat_lane0) : nullptr;
+    m.splat_lane[1] = traced.count ? (unsigned long long *)at(p_splat_lane1) : nullptr;
     std::memcpy(stage, &m, sizeof m);
     LR_CUDA(cudaMemcpyAsync(h->d_members + index, stage, sizeof m, cudaMemcpyHostToDevice, stream));
     h->staging.queued(stream);
@@ -1031,7 +1593,7 @@ uint32_t member_add(WaveHost *h, const lr_gpu_scene *gs, lr_gpu_scene *owned, co
     mh.leaving = false;
     mh.owned = owned;
     mh.samples = settings.samples;
-    mh.sample = mh.next_pixel = mh.done = 0;
+    mh.sample = mh.next_pixel = mh.done = mh.light_next = 0;
     mh.max_bounces = settings.max_bounces;
     mh.last_pass = 0;
     return index;
@@ -1099,37 +1661,59 @@ bool launch_pass(WaveHost *h, bool dry = false, int only = -1) {
     Lane &lane = lane_of(h, h->recorded);
     Plan *staging = lane.h_plan;
     Segment *seg = staging->seg;
-    uint32_t n = 0, used = 0, converts = 0;
+    uint32_t n = 0, used = 0, converts = 0, camera_paths = 0, folds = 0;
     uint64_t class_paths[kSizeClasses] = {0, 0, 0};
     PassRecord rec;
     rec.number = h->recorded;
     const uint32_t cap = h->capacity;
     const uint32_t fill = h->fill ? std::min(h->fill, h->pool) : h->pool;
     uint32_t last = h->rotate;
-    for (uint32_t step = 0; step < cap && used < fill && n < kMaxSegments; step++) {
+    for (uint32_t step = 0; step < cap && used < fill && n + 2 <= kMaxSegments; step++) {
         const uint32_t index = (h->rotate + step) % cap;
         MemberHost &mh = h->members[index];
         if (!has_work(mh)) continue;
         const int cls = size_class(mh.dev.scene.triangle_count);
         if (only >= 0 && cls != only) continue;
+        // The light paths of the member's current sample come first, and its camera paths
+        // end the sample only in a pass that plans the last of them: the pass that ends a
+        // sample folds every splat of it before it converts the image.
+        const uint32_t lights = mh.dev.light_paths;
+        uint32_t light_next = mh.light_next;
+        if (light_next < lights) {
+            const uint32_t count = std::min(lights - light_next, fill - used);
+            seg[n++] = Segment{index, light_next, count, mh.sample, used, 0u, kLightSegment, 0u};
+            staging->fold[folds++] = index;
+            used += count;
+            light_next += count;
+            class_paths[cls] += count;
+        }
         const uint64_t left = mh.dev.pixels - mh.next_pixel;
-        const uint32_t count = (uint32_t)std::min<uint64_t>(left, fill - used);
-        const bool ends = count == left && !dry;
-        seg[n] = Segment{index, mh.next_pixel, count, mh.sample, used, ends ? 1u : 0u, 0u, 0u};
+        uint32_t count = (uint32_t)std::min<uint64_t>(left, fill - used);
+        if (h->camera_cap) count = std::min(count, h->camera_cap);
+        if (count == left && light_next < lights) count = (uint32_t)left - 1;
+        const bool ends = count > 0 && count == left && !dry;
         rec.members.push_back({index, ends});
-        if (ends) staging->convert[converts++] = index;
-        n++;
-        used += count;
+        if (count > 0) {
+            seg[n++] = Segment{index, mh.next_pixel, count, mh.sample, used, ends ? 1u : 0u, kCameraSegment, 0u};
+            if (ends) {
+                staging->convert[converts] = index;
+                staging->convert_samples[converts++] = mh.sample + 1;
+            }
+            used += count;
+            camera_paths += count;
+            class_paths[cls] += count;
+        }
         if (!dry) {
-            if (count == left) {
+            mh.light_next = light_next;
+            if (count > 0 && count == left) {
                 mh.sample++;
                 mh.next_pixel = 0;
+                mh.light_next = 0;
             } else {
                 mh.next_pixel += count;
             }
         }
         mh.last_pass = h->recorded + 1;
-        class_paths[cls] += count;
         last = index;
     }
     if (n == 0) return false;
@@ -1151,8 +1735,10 @@ bool launch_pass(WaveHost *h, bool dry = false, int only = -1) {
         if (fits || width == 2) break;
         width = 2;
     }
-    const int variant = width * 1000 + stack;
-    staging->head = PlanHeader{n, used, converts, dry ? 1u : 0u};
+    const bool tracing = std::any_of(rec.members.begin(), rec.members.end(),
+                                     [&](const std::pair<uint32_t, bool> &e) { return h->members[e.first].dev.light_paths != 0u; });
+    const int variant = width * 1000 + stack + (tracing ? kTracingVariant : 0);
+    staging->head = PlanHeader{n, used, converts, dry ? 1u : 0u, camera_paths, folds, 0u, 0u};
     cudaStream_t stream = lane.stream;
     // Member records queued on the context's stream reach this lane first.
     if (stream != h->ctx->stream && lane.members_seen != h->member_uploads && h->staging.copied) {
@@ -1378,18 +1964,25 @@ void create(lr_context *ctx, const lr_scene *scene, const lr_settings &settings,
     auto r = std::make_unique<lr_renderer>();
     LR_CUDA(cudaSetDevice(ctx->device));
     const uint64_t pixels = (uint64_t)frame.width * frame.height;
-    const uint64_t pool = std::min<uint64_t>(std::min<uint64_t>(settings.pool ? settings.pool : kDefaultPool, kMaxPool), pixels);
-    r->bands = (uint32_t)((pixels + pool - 1) / pool);
+    const uint64_t band = std::min<uint64_t>(std::min<uint64_t>(settings.pool ? settings.pool : kDefaultPool, kMaxPool), pixels);
+    r->bands = (uint32_t)((pixels + band - 1) / band);
+    // A pass holds a band and, in a sample's first, its light paths (integrator.lucb:419-423);
+    // room for them at most, until the scene says whether it has emitters.
+    const uint64_t most_lights = light_paths_of(settings, frame, pixels, 1).count;
     lr_gpu_scene *gs = nullptr;
     int status = lr_gpu_scene_upload(ctx, scene, &gs);
     if (status != LR_OK) fail(status, lr_last_error());
     try {
-        wave_create(&r->wave, ctx, pool, settings.max_bounces + 1, 1, settings.profile);
+        wave_create(&r->wave, ctx, band + most_lights, settings.max_bounces + 1, 1, settings.profile);
         member_add(&r->wave, gs, gs, scene, settings, frame);
+        r->wave.fill = (uint32_t)std::min<uint64_t>(band + r->wave.members[0].dev.light_paths, r->wave.pool);
+        r->wave.camera_cap = (uint32_t)band;
         // The graphs for the scene's traversal variant, made now rather than at the first pass.
         const TraversalChoice c = choose_traversal(gs->scene, 0);
         if (!settings.profile)
-            for (int li = 0; li < r->wave.lane_count; li++) trace_graph(&r->wave, r->wave.lanes[li], c.width * 1000 + c.stack);
+            for (int li = 0; li < r->wave.lane_count; li++)
+                trace_graph(&r->wave, r->wave.lanes[li],
+                            c.width * 1000 + c.stack + (r->wave.members[0].dev.light_paths ? kTracingVariant : 0));
     } catch (...) {
         const bool owned = !r->wave.members.empty() && r->wave.members[0].used;
         wave_destroy(&r->wave);

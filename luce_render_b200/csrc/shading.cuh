@@ -24,6 +24,8 @@ __device__ __forceinline__ float3 operator-(float3 a, float3 b) { return make_fl
 __device__ __forceinline__ float3 operator-(float3 a) { return make_float3(-a.x, -a.y, -a.z); }
 __device__ __forceinline__ float3 operator*(float3 a, float s) { return make_float3(a.x * s, a.y * s, a.z * s); }
 __device__ __forceinline__ float3 operator*(float s, float3 a) { return make_float3(a.x * s, a.y * s, a.z * s); }
+__device__ __forceinline__ float3 operator/(float3 a, float s) { return make_float3(a.x / s, a.y / s, a.z / s); }
+__device__ __forceinline__ float2 operator*(float2 a, float s) { return make_float2(a.x * s, a.y * s); }
 __device__ __forceinline__ float4 operator+(float4 a, float4 b) { return make_float4(a.x + b.x, a.y + b.y, a.z + b.z, a.w + b.w); }
 __device__ __forceinline__ float4 operator*(float4 a, float4 b) { return make_float4(a.x * b.x, a.y * b.y, a.z * b.z, a.w * b.w); }
 __device__ __forceinline__ float4 operator*(float4 a, float s) { return make_float4(a.x * s, a.y * s, a.z * s, a.w * s); }
@@ -365,8 +367,10 @@ __device__ __forceinline__ bool sample_light(const float4 *lights, uint32_t ligh
     return true;
 }
 
-// intersect_light (lights.glsl:239-259) for a camera path (light_flow false).
-__device__ __forceinline__ float intersect_light(const float4 *lights, uint32_t light, float3 o, float3 d, float t_max) {
+// intersect_light (lights.glsl:239-259). `flow`: the ray follows light (a light path), so a
+// flat light stops it only when crossed the way it shines.
+__device__ __forceinline__ float intersect_light(const float4 *lights, uint32_t light, float3 o, float3 d, float t_max,
+                                                 bool flow = false) {
     const float4 row0 = light_at(lights, light, 0);
     const uint32_t type = (uint32_t)row0.w;
     if (type == kLightSphere) {
@@ -377,7 +381,7 @@ __device__ __forceinline__ float intersect_light(const float4 *lights, uint32_t 
     const float3 u = xyz(light_at(lights, light, 1)), v = xyz(light_at(lights, light, 2)),
                  n = xyz(light_at(lights, light, 3));
     const float facing = dot(d, n);
-    if (facing >= 0.0f) return kInfinity;
+    if (flow ? facing <= 0.0f : facing >= 0.0f) return kInfinity;
     const float t = dot(xyz(row0) - o, n) / facing;
     if (t <= 0.0f || t >= t_max) return kInfinity;
     const float3 q = o + t * d - xyz(row0);

@@ -181,7 +181,7 @@ static spec light_radiance(const or_render_desc *r, uint32_t light, const double
 
 typedef struct {
     d3 direction;
-    double distance, pdf;
+    double distance, pdf, cos_light;
     int delta;
 } lsample;
 
@@ -222,6 +222,7 @@ static int sample_light(const or_render_desc *r, uint32_t light, d3 p, double u0
     const float *r0 = row(r, light, 0), *r1 = row(r, light, 1), *r2 = row(r, light, 2), *r3 = row(r, light, 3);
     uint32_t type = (uint32_t)r0[3];
     s->delta = 0;
+    s->cos_light = 1.0;
     if (type == 0 || type == 1) {
         double ax, ay;
         if (type == 0) ax = 2.0 * u0 - 1.0, ay = 2.0 * u1 - 1.0;
@@ -234,6 +235,7 @@ static int sample_light(const or_render_desc *r, uint32_t light, d3 p, double u0
         double cl = -dot(s->direction, rv(r3));
         if (cl <= 0.0 || r3[3] <= 0.0) return 0;
         s->pdf = d2 / (cl * r3[3]);
+        s->cos_light = cl;
         return 1;
     }
     if (type == 2) {
@@ -245,6 +247,7 @@ static int sample_light(const or_render_desc *r, uint32_t light, d3 p, double u0
         s->distance = sphere_hit(rv(r0), rad, p, s->direction);
         if (s->distance >= INF) return 0;
         s->pdf = 1.0 / (2.0 * PI * (1.0 - cos_max));
+        s->cos_light = fmax(0.0, -dot(s->direction, norm(sub(add(p, mul(s->direction, s->distance)), rv(r0)))));
         return 1;
     }
     d3 axis = neg(rv(r3));
@@ -261,7 +264,9 @@ static int sample_light(const or_render_desc *r, uint32_t light, d3 p, double u0
     return 1;
 }
 
-static double intersect_light(const or_render_desc *r, uint32_t light, d3 o, d3 d, double t_max) {
+/* intersect_light (lights.glsl:239-259); `flow`: the ray follows light (a light path), so
+ * a flat light stops it only when crossed the way it shines. */
+static double intersect_light(const or_render_desc *r, uint32_t light, d3 o, d3 d, double t_max, int flow) {
     const float *r0 = row(r, light, 0);
     uint32_t type = (uint32_t)r0[3];
     if (type == 2) {
@@ -271,7 +276,7 @@ static double intersect_light(const or_render_desc *r, uint32_t light, d3 o, d3 
     if (type >= 3) return INF;
     d3 u = rv(row(r, light, 1)), v = rv(row(r, light, 2)), n = rv(row(r, light, 3));
     double facing = dot(d, n);
-    if (facing >= 0.0) return INF;
+    if (flow ? facing <= 0.0 : facing >= 0.0) return INF;
     double t = dot(sub(rv(r0), o), n) / facing;
     if (t <= 0.0 || t >= t_max) return INF;
     d3 q = sub(add(o, mul(d, t)), rv(r0));
@@ -374,6 +379,143 @@ static double tree_pdf(const or_render_desc *r, uint32_t emitter, d3 p, d3 n) {
 }
 
 static const float *material(const or_render_desc *r, uint32_t m, int k) { return &r->materials[m * 64 + k * 4]; }
+
+/* ---- Light tracing (shaders/connect.glsl, common.glsl:112-140) ----------------------- */
+
+/* camera_pdf (common.glsl:132-135): per unit of a pixel's area at unit distance. */
+static double camera_pdf(const or_render_desc *r, d3 d) {
+    double c = dot(d, v3(r->forward[0], r->forward[1], r->forward[2]));
+    return c > 0.0 ? r->pixel_area_inv / (c * c * c) : 0.0;
+}
+
+/* lens_point (common.glsl:125-130). */
+static d3 lens_point(const or_render_desc *r, double u0, double u1) {
+    const float *f = r->frame;
+    d3 position = v3(f[0], f[1], f[2]);
+    if (r->lens_radius <= 0.0) return position;
+    double dx, dy;
+    concentric(u0, u1, &dx, &dy);
+    dx *= r->lens_radius;
+    dy *= r->lens_radius;
+    return add(add(position, mul(norm(v3(f[8], f[9], f[10])), dx)), mul(norm(v3(f[12], f[13], f[14])), dy));
+}
+
+/* camera_pixel (connect.glsl:30-45). */
+static int camera_pixel(const or_render_desc *r, d3 p, d3 lens, uint32_t *pixel, d3 *d_out, double *distance) {
+    const float *f = r->frame;
+    d3 offset = sub(p, lens);
+    *distance = len(offset);
+    d3 d = mul(offset, 1.0 / fmax(*distance, 1e-20));
+    *d_out = d;
+    double c = dot(d, v3(r->forward[0], r->forward[1], r->forward[2]));
+    if (c <= 1e-6 || *distance <= 0.0) return 0;
+    d3 position = v3(f[0], f[1], f[2]), corner = v3(f[4], f[5], f[6]), du = v3(f[8], f[9], f[10]), dv = v3(f[12], f[13], f[14]);
+    double focus = r->focus_distance;
+    d3 film = sub(r->lens_radius > 0.0 ? mul(sub(add(lens, mul(d, focus / c)), position), 1.0 / focus) : mul(d, 1.0 / c), corner);
+    double x = dot(film, du) / dot(du, du), y = dot(film, dv) / dot(dv, dv);
+    if (!(x >= 0.0 && y >= 0.0 && x < (double)r->width && y < (double)r->height)) return 0;
+    *pixel = (uint32_t)y * r->width + (uint32_t)x;
+    return 1;
+}
+
+static double node_energy(const or_render_desc *r, uint32_t node) { return fmax(r->tree_nodes[node * 12 + 3], 0.0); }
+
+/* emitter_power_pdf (connect.glsl:68-83). */
+static double emitter_power_pdf(const or_render_desc *r, uint32_t emitter) {
+    uint32_t trail = r->tree_records[emitter * 4 + 1], depth = r->tree_records[emitter * 4 + 2];
+    uint32_t node = 0;
+    double pdf = 1.0;
+    for (uint32_t level = 0; level < depth; level++) {
+        uint32_t link = r->tree_links[node * 2];
+        double left = node_energy(r, link), right = node_energy(r, link + 1);
+        if (left + right <= 0.0) return 0.0;
+        uint32_t bit = (trail >> level) & 1u;
+        pdf *= (bit == 0 ? left : right) / (left + right);
+        node = link + bit;
+    }
+    return pdf;
+}
+
+/* emitter_by_power (connect.glsl:86-110). */
+static int emitter_by_power(const or_render_desc *r, double u, uint32_t *emitter, double *pdf) {
+    *pdf = 1.0;
+    *emitter = 0;
+    if (r->tree_node_count < 1) return 0;
+    uint32_t node = 0;
+    for (int depth = 0; depth < 64; depth++) {
+        uint32_t link = r->tree_links[node * 2];
+        if (r->tree_links[node * 2 + 1] & 0x80000000u) {
+            *emitter = link;
+            return *pdf > 0.0;
+        }
+        double left = node_energy(r, link), right = node_energy(r, link + 1);
+        if (left + right <= 0.0) return 0;
+        double chance = left / (left + right);
+        if (u < chance) {
+            u = fmin(u / chance, 0.99999994);
+            *pdf *= chance;
+            node = link;
+        } else {
+            u = fmin((u - chance) / (1.0 - chance), 0.99999994);
+            *pdf *= 1.0 - chance;
+            node = link + 1;
+        }
+    }
+    return 0;
+}
+
+static int emitter_is_triangle(const or_render_desc *r, uint32_t emitter) {
+    return (r->tree_records[emitter * 4] & 0x80000000u) != 0;
+}
+
+/* emitter_area_pdf (connect.glsl:116-132); no light paths start from afar here. */
+static double emitter_area_pdf(const or_render_desc *r, uint32_t emitter) {
+    uint32_t code = r->tree_records[emitter * 4];
+    double area;
+    if (code & 0x80000000u) {
+        uint32_t t = code & 0x7fffffffu;
+        d3 a = point(r, r->indices[t * 3]);
+        area = 0.5 * len(cross(sub(point(r, r->indices[t * 3 + 1]), a), sub(point(r, r->indices[t * 3 + 2]), a)));
+    } else if (light_type(r, code) == 2) {
+        double rad = row(r, code, 1)[3];
+        area = 4.0 * PI * rad * rad;
+    } else {
+        area = row(r, code, 3)[3];
+    }
+    return area > 0.0 ? emitter_power_pdf(r, emitter) / area : 0.0;
+}
+
+static double emission_direction_pdf(const or_render_desc *r, uint32_t emitter, double c) {
+    return fabs(c) / (emitter_is_triangle(r, emitter) ? 2.0 * PI : PI);
+}
+
+/* camera_hit_ratio (connect.glsl:141-149). */
+static double camera_hit_ratio(const or_render_desc *r, const double mis[4], uint32_t emitter, double cos_light,
+                               double distance, double bsdf_pdf) {
+    if (emitter == NONE || mis[1] <= 0.0 || bsdf_pdf <= 0.0) return 0.0;
+    double d2 = distance * distance;
+    double at_vertex = emission_direction_pdf(r, emitter, cos_light) * mis[2] / d2 / mis[1];
+    double at_light = emitter_area_pdf(r, emitter) / (bsdf_pdf * fabs(cos_light) / d2);
+    return mis[0] * at_vertex * at_light;
+}
+
+/* light_cos (lights.glsl:228-232). */
+static double light_cos(const or_render_desc *r, uint32_t light, d3 o, d3 d, double t) {
+    const float *r0 = row(r, light, 0);
+    if ((uint32_t)r0[3] == 2) return fmax(0.0, -dot(d, norm(sub(add(o, mul(d, t)), rv(r0)))));
+    return fmax(0.0, -dot(d, rv(row(r, light, 3))));
+}
+
+/* light_sampler_pdf (connect.glsl:52-62) at the Lambertian settings: the surface (shading
+ * normal n, geometric g, facing one side) seen from `from`'s side, the cosine lobe. */
+static double light_sampler_pdf(double p_diffuse, d3 n, d3 g, d3 from, d3 to) {
+    int same = dot(from, g) >= 0.0;
+    d3 nv = same ? n : neg(n), gv = same ? g : neg(g);
+    double wo_z = dot(from, nv), wi_z = dot(to, nv);
+    if ((dot(to, gv) > 0.0) != (wi_z > 0.0)) return 0.0;
+    if (wo_z <= 0.0 || wi_z <= 0.0) return 0.0;
+    return p_diffuse * wi_z / PI;
+}
 
 static double mis_weight(double a, double b) {
     a = fmin(a, 1e18);
@@ -483,6 +625,10 @@ static void render_sample(const or_render_desc *r, uint32_t pixel, uint32_t samp
     uint32_t bounces = 0;
     d3 vertex = origin, prev_normal = v3(0, 0, 1);
     double survival = 1.0, ray_pdf = 0.0;
+    /* Light tracing's MIS state (common.glsl:136-143, camera.comp:42). */
+    const int tracing = r->light_paths > 0;
+    double mis[4] = {0, 0, 0, 0};
+    if (tracing) mis[0] = (double)r->light_paths, mis[3] = camera_pdf(r, dir);
     for (uint32_t round = 0; round <= r->max_bounces; round++) {
         uint32_t total = bounces & 0xffu;
         double t, hu = 0, hv = 0;
@@ -490,7 +636,7 @@ static void render_sample(const or_render_desc *r, uint32_t pixel, uint32_t samp
         rays[0]++;
         for (uint32_t l = 0; l < r->light_count; l++) {
             if (round == 0 && !light_visible(r, l)) continue;
-            double tl = intersect_light(r, l, origin, dir, t);
+            double tl = intersect_light(r, l, origin, dir, t, 0);
             if (tl < t) {
                 t = tl;
                 what = LIGHT_HIT | l;
@@ -525,7 +671,8 @@ static void render_sample(const or_render_desc *r, uint32_t pixel, uint32_t samp
                 uint32_t emitter = (uint32_t)row(r, l, 6)[3];
                 double reach = len(sub(vertex, add(origin, mul(dir, t))));
                 double chance = (1.0 - r->p_distant) * tree_pdf(r, emitter, vertex, prev_normal);
-                weight = mis_weight(light_hit_pdf(r, l, vertex, dir, reach) * chance / ray_pdf, 0.0);
+                double traced = tracing ? camera_hit_ratio(r, mis, emitter, light_cos(r, l, vertex, dir, reach), reach, ray_pdf) : 0.0;
+                weight = mis_weight(light_hit_pdf(r, l, vertex, dir, reach) * chance / ray_pdf, traced);
             }
             radiance = spec_add(radiance, clamped(r, spec_scale(spec_mul(throughput, light_radiance(r, l, lambda)), weight), total));
             break;
@@ -538,13 +685,18 @@ static void render_sample(const or_render_desc *r, uint32_t pixel, uint32_t samp
         uint32_t m = attr[3];
         d3 p = add(origin, mul(dir, t));
         double reach = len(sub(vertex, p));
+        /* The camera's density of this vertex, and what turns the light sampler's pdf here
+         * toward the last vertex into that vertex's density (shade_surface.comp:91-94). */
+        double density = (total == 0 ? mis[3] : ray_pdf) * fabs(dot(dir, geometric)) / (reach * reach);
+        double back_reach = mis[2] / (reach * reach);
         const float *em = material(r, m, 7);
         if (em[3] > 0.0f) {
             double weight = 1.0;
             uint32_t emitter = r->tree_records && slot < r->triangle_count ? r->tree_records[r->emitter_count * 4 + slot] : NONE;
             if (total > 0 && ray_pdf > 0.0 && emitter != NONE) {
                 double chance = (1.0 - r->p_distant) * tree_pdf(r, emitter, vertex, prev_normal);
-                weight = mis_weight(tri_hit_pdf(r, slot, dir, reach) * chance / ray_pdf, 0.0);
+                double traced = tracing ? camera_hit_ratio(r, mis, emitter, fabs(dot(dir, geometric)), reach, ray_pdf) : 0.0;
+                weight = mis_weight(tri_hit_pdf(r, slot, dir, reach) * chance / ray_pdf, traced);
             }
             radiance = spec_add(radiance, clamped(r, spec_scale(spec_mul(throughput, spec_of(r, material(r, m, 6), em, lambda)), weight), total));
         }
@@ -566,6 +718,7 @@ static void render_sample(const or_render_desc *r, uint32_t pixel, uint32_t samp
         spec emitted = spec_zero();
         double chance = 0.0;
         int sampled = 0;
+        uint32_t nee_emitter = NONE;
         if (ul[0] < r->p_distant) {
             double share;
             uint32_t l = pick_distant(r, ul[0] / r->p_distant, &share);
@@ -579,6 +732,7 @@ static void render_sample(const or_render_desc *r, uint32_t pixel, uint32_t samp
             double tc;
             if (tree_sample(r, (ul[0] - r->p_distant) / fmax(1e-7, 1.0 - r->p_distant), from, normal, &emitter, &tc)) {
                 chance = (1.0 - r->p_distant) * tc;
+                nee_emitter = emitter;
                 uint32_t code = r->tree_records[emitter * 4];
                 if (code & 0x80000000u) {
                     uint32_t ts = code & 0x7fffffffu;
@@ -595,6 +749,7 @@ static void render_sample(const or_render_desc *r, uint32_t pixel, uint32_t samp
                         double cl = fabs(dot(s.direction, cr)) / (2.0 * area);
                         if (cl > 0.0) {
                             s.pdf = d2 / (cl * area);
+                            s.cos_light = cl;
                             s.delta = 0;
                             uint32_t tm = r->shading[ts * 4 + 3];
                             emitted = spec_of(r, material(r, tm, 6), material(r, tm, 7), lambda);
@@ -615,7 +770,19 @@ static void render_sample(const or_render_desc *r, uint32_t pixel, uint32_t samp
                 if (bsdf_pdf > 0.0) {
                     spec fv = eon(base, rough, wi, wo);
                     double light_pdf = s.pdf * chance;
-                    double weight = s.delta ? 1.0 : mis_weight(bsdf_pdf / light_pdf, 0.0);
+                    /* The light tracer's density of this path over the camera's BSDF ray
+                     * reaching the same light point (shade_surface.comp:210-224). */
+                    double traced = 0.0;
+                    if (tracing && !s.delta && nee_emitter != NONE && density > 0.0) {
+                        double d2 = s.distance * s.distance;
+                        double at_last = total == 0 ? 1.0
+                                                    : light_sampler_pdf(p_diffuse, normal, geometric, s.direction, neg(dir)) *
+                                                          back_reach / mis[1];
+                        double at_vertex = emission_direction_pdf(r, nee_emitter, s.cos_light) * fabs(side) / d2 / density;
+                        double at_light = emitter_area_pdf(r, nee_emitter) / (bsdf_pdf * s.cos_light / d2);
+                        traced = mis[0] * at_last * at_vertex * at_light;
+                    }
+                    double weight = s.delta ? 1.0 : mis_weight(bsdf_pdf / light_pdf, traced * bsdf_pdf / light_pdf);
                     spec c = clamped(r, spec_scale(spec_mul(spec_mul(throughput, fv), emitted), fabs(wi.z) * (weight / light_pdf)), total);
                     d3 target = add(p, mul(s.direction, s.distance));
                     double margin = 4e-4 * fmax(1.0, fmax(fabs(target.x), fmax(fabs(target.y), fabs(target.z))));
@@ -651,6 +818,16 @@ static void render_sample(const or_render_desc *r, uint32_t pixel, uint32_t samp
             throughput = spec_scale(throughput, 1.0 / survive);
         }
         d3 next = side > 0.0 ? from : offset_origin(p, neg(geometric));
+        if (tracing) {
+            /* This vertex's factor of the light tracer's density, settled now that the light
+             * sampler's direction here is known (shade_surface.comp:304-307). */
+            double at_last = total == 0 ? 1.0
+                                        : light_sampler_pdf(p_diffuse, normal, geometric, direction, neg(dir)) * back_reach / mis[1];
+            mis[0] *= at_last;
+            mis[1] = density;
+            mis[2] = fabs(side);
+            mis[3] = 0.0;
+        }
         prev_normal = normal;
         origin = next;
         vertex = next;
@@ -665,6 +842,233 @@ static void render_sample(const or_render_desc *r, uint32_t pixel, uint32_t samp
         for (int i = 0; i < 3; i++) out[i] = r->film[i * 3] * value[0] + r->film[i * 3 + 1] * value[1] + r->film[i * 3 + 2] * value[2];
     } else {
         out[0] = value[0], out[1] = value[1], out[2] = value[2];
+    }
+}
+
+/* light_emit.comp:55-136 and light_paths.glsl:27-189 at the Lambertian settings: light
+ * path `index` of sample `sample` from an emitter of the light tree chosen by power (no
+ * light paths start from afar: Lambertian materials cast no caustics), each surface it
+ * reaches connected to the camera -- what gets through is added, in the film's terms, to
+ * `splat` (3 per pixel) -- and scattered on. */
+static void trace_light_path(const or_render_desc *r, uint32_t sample, uint32_t index, double *splat,
+                             uint64_t rays[2]) {
+    const uint32_t id = 0x80000000u | (r->light_band + index);
+    const double L = (double)r->light_paths;
+    double u_point[4], u_pick[4];
+    or_sample4(r->seed, id, sample, 0, u_point);
+    or_sample4(r->seed, id, sample, 1, u_pick);
+    double lambda[4] = {0, 0, 0, 0};
+    if (r->spectral) or_sample_wavelengths(u_pick[0], lambda);
+    uint32_t emitter;
+    double chance;
+    if (!emitter_by_power(r, u_pick[1] / fmax(1e-7, 1.0), &emitter, &chance)) return;
+    uint32_t code = r->tree_records[emitter * 4];
+    d3 q, n;
+    spec radiance;
+    double area;
+    int two_sided = 0;
+    if (code & 0x80000000u) {
+        uint32_t t = code & 0x7fffffffu;
+        d3 a = point(r, r->indices[t * 3]), b = point(r, r->indices[t * 3 + 1]), c = point(r, r->indices[t * 3 + 2]);
+        double rr = sqrt(u_point[0]);
+        q = add(add(mul(a, 1.0 - rr), mul(b, rr * (1.0 - u_point[1]))), mul(c, rr * u_point[1]));
+        d3 cr = cross(sub(b, a), sub(c, a));
+        area = 0.5 * len(cr);
+        n = mul(cr, 1.0 / fmax(2.0 * area, 1e-30));
+        if (u_pick[2] < 0.5) n = neg(n);
+        two_sided = 1;
+        uint32_t tm = r->shading[t * 4 + 3];
+        radiance = spec_of(r, material(r, tm, 6), material(r, tm, 7), lambda);
+    } else {
+        uint32_t type = light_type(r, code);
+        const float *r0 = row(r, code, 0);
+        if (type == 2) {
+            double rad = row(r, code, 1)[3];
+            double z = 1.0 - 2.0 * u_point[0], sz = sqrt(fmax(0.0, 1.0 - z * z)), phi = 2.0 * PI * u_point[1];
+            n = v3(sz * cos(phi), sz * sin(phi), z);
+            q = add(rv(r0), mul(n, rad));
+            area = 4.0 * PI * rad * rad;
+        } else {
+            double ax, ay;
+            if (type == 0) ax = 2.0 * u_point[0] - 1.0, ay = 2.0 * u_point[1] - 1.0;
+            else concentric(u_point[0], u_point[1], &ax, &ay);
+            q = add(add(rv(r0), mul(rv(row(r, code, 1)), ax)), mul(rv(row(r, code, 2)), ay));
+            n = rv(row(r, code, 3));
+            area = row(r, code, 3)[3];
+        }
+        radiance = light_radiance(r, code, lambda);
+    }
+    if (area <= 0.0) return;
+    double dx, dy;
+    concentric(u_point[2], u_point[3], &dx, &dy);
+    double cos_n = sqrt(fmax(0.0, 1.0 - (dx * dx + dy * dy)));
+    if (cos_n <= 0.0) return;
+    d3 tg, bt;
+    onb(n, &tg, &bt);
+    d3 dir = norm(add(add(mul(tg, dx), mul(bt, dy)), mul(n, cos_n)));
+    double point_pdf = chance / area;
+    double ray_pdf = cos_n / (two_sided ? 2.0 * PI : PI);
+    spec throughput = spec_scale(radiance, cos_n / (point_pdf * ray_pdf));
+    double largest = spec_max(r, throughput);
+    if (!(largest > 0.0)) return;
+    d3 origin = offset_origin(q, n), vertex = q;
+    double survival = 1.0 / largest;
+    double mis[4] = {1.0, point_pdf, cos_n, -1.0};
+    uint32_t bounces = 0;
+    for (uint32_t round = 0; round <= r->max_bounces; round++) {
+        uint32_t total = bounces & 0xffu;
+        double t, hu = 0, hv = 0;
+        uint32_t what = trace64(r, origin, dir, INF, 0, &t, &hu, &hv);
+        rays[0]++;
+        for (uint32_t l = 0; l < r->light_count; l++) {
+            if (total == 0 && !light_visible(r, l)) continue;
+            double tl = intersect_light(r, l, origin, dir, t, 1);
+            if (tl < t) {
+                t = tl;
+                what = LIGHT_HIT | l;
+            }
+        }
+        if (what == NONE || (what & LIGHT_HIT)) return;
+        uint32_t slot = what;
+        d3 p0 = point(r, r->indices[slot * 3]);
+        d3 geometric = norm(cross(sub(point(r, r->indices[slot * 3 + 1]), p0), sub(point(r, r->indices[slot * 3 + 2]), p0)));
+        if (dot(geometric, dir) > 0.0) geometric = neg(geometric);
+        const uint32_t *attr = &r->shading[slot * 4];
+        uint32_t m = attr[3];
+        d3 p = add(origin, mul(dir, t));
+        if (total >= r->max_bounces) return;
+        d3 normal = norm(add(add(mul(oct_decode(attr[0]), 1.0 - hu - hv), mul(oct_decode(attr[1]), hu)), mul(oct_decode(attr[2]), hv)));
+        if (dot(normal, geometric) < 0.0) normal = neg(normal);
+        double ul[4];
+        or_sample4(r->seed, id, sample, 2 + 3 * total, ul);
+        d3 lens = lens_point(r, ul[0], ul[1]);
+        uint32_t pixel = 0;
+        d3 to_point;
+        double camera_distance;
+        int on_film = camera_pixel(r, p, lens, &pixel, &to_point, &camera_distance);
+        const float *brgb = material(r, m, 1);
+        spec base = spec_scale(spec_of(r, material(r, m, 0), brgb, lambda), brgb[3]);
+        double rough = material(r, m, 10)[1];
+        double lum = (brgb[0] * 0.2722287168 + brgb[1] * 0.6740817658 + brgb[2] * 0.0536895174) * brgb[3];
+        double p_diffuse = fmax(lum, 0.0) > 0.0 ? 1.0 : 0.0;
+        d3 toward_light = neg(dir);
+        double reach = len(sub(vertex, p));
+        double cos_in = fabs(dot(dir, geometric));
+        double density = ray_pdf * cos_in / (reach * reach);
+        double back_reach = mis[2] / (reach * reach);
+        double cos_shading_in = dot(toward_light, normal);
+        if (cos_shading_in <= 0.0 || cos_in < 1e-6) return;
+        double shading_in = cos_shading_in / cos_in;
+        if (on_film) {
+            d3 to_camera = neg(to_point);
+            double side = dot(to_camera, geometric);
+            d3 sn = side > 0.0 ? normal : neg(normal), sg = side > 0.0 ? geometric : neg(geometric);
+            d3 st, sb;
+            onb(sn, &st, &sb);
+            d3 wo = v3(dot(to_camera, st), dot(to_camera, sb), dot(to_camera, sn));
+            d3 wi = v3(dot(toward_light, st), dot(toward_light, sb), dot(toward_light, sn));
+            if ((dot(toward_light, sg) > 0.0) == (wi.z > 0.0) && wo.z > 0.0 && wi.z > 0.0) {
+                double camera_bsdf_pdf = p_diffuse * wi.z / PI;
+                spec f = eon(base, rough, wi, wo);
+                double camera_density = camera_pdf(r, to_point) * fabs(side) / (camera_distance * camera_distance);
+                spec contribution = spec_scale(spec_mul(throughput, f), shading_in * camera_density / L);
+                if (spec_max(r, contribution) > 0.0) {
+                    double last = mis[1] > 0.0 ? camera_bsdf_pdf * back_reach / mis[1] : 0.0;
+                    double ratio = mis[0] * last * camera_density / density;
+                    double sample_ratio;
+                    if (total == 0) {
+                        sample_ratio = 0.0;
+                        if (camera_bsdf_pdf > 0.0) {
+                            d3 from = offset_origin(p, sg);
+                            d3 offset = sub(vertex, from);
+                            double rch = len(offset);
+                            d3 d = mul(offset, 1.0 / rch);
+                            double ch = (1.0 - r->p_distant) * tree_pdf(r, emitter, from, sn);
+                            double pdf = (code & 0x80000000u) ? tri_hit_pdf(r, code & 0x7fffffffu, d, rch)
+                                                               : light_hit_pdf(r, code, from, d, rch);
+                            sample_ratio = ch * pdf / camera_bsdf_pdf;
+                        }
+                    } else {
+                        sample_ratio = fmax(mis[3], 0.0);
+                    }
+                    double weight = mis_weight(ratio / L, ratio * sample_ratio / L);
+                    double margin = 4e-4 * fmax(1.0, fmax(fabs(p.x), fmax(fabs(p.y), fabs(p.z))));
+                    d3 so = offset_origin(p, sg);
+                    double sreach = fmax(0.0, camera_distance - margin);
+                    int blocked = 0;
+                    for (uint32_t l = 0; l < r->light_count && !blocked; l++)
+                        if (light_visible(r, l) && intersect_light(r, l, so, to_camera, sreach, 1) < sreach) blocked = 1;
+                    if (!blocked) {
+                        double tt, uu, vv;
+                        rays[1]++;
+                        if (trace64(r, so, to_camera, sreach, 1, &tt, &uu, &vv) == NONE) {
+                            double v[3];
+                            spec_to_film(r, spec_scale(contribution, weight), lambda, v);
+                            if (isfinite(v[0]) && isfinite(v[1]) && isfinite(v[2]))
+                                for (int k = 0; k < 3; k++) splat[pixel * 3 + k] += v[k];
+                        }
+                    }
+                }
+            }
+        }
+        if (total + 1 >= r->max_bounces) return;
+        double u[4];
+        or_sample4(r->seed, id, sample, 3 + 3 * total, u);
+        d3 tg2, bt2;
+        onb(normal, &tg2, &bt2);
+        d3 wo_light = v3(dot(toward_light, tg2), dot(toward_light, bt2), dot(toward_light, normal));
+        if (wo_light.z <= 0.0 || !(u[3] < p_diffuse)) return;
+        double ddx, ddy;
+        concentric(u[0], u[1], &ddx, &ddy);
+        d3 wl = v3(ddx, ddy, sqrt(fmax(0.0, 1.0 - (ddx * ddx + ddy * ddy))));
+        if (wl.z == 0.0) return;
+        double light_pdf = p_diffuse * wl.z / PI;
+        if (!(light_pdf > 0.0)) return;
+        d3 direction = add(add(mul(tg2, wl.x), mul(bt2, wl.y)), mul(normal, wl.z));
+        double side = dot(direction, geometric);
+        if ((side > 0.0) != (wl.z > 0.0)) return;
+        d3 sn = side > 0.0 ? normal : neg(normal), sg = side > 0.0 ? geometric : neg(geometric);
+        d3 st, sb;
+        onb(sn, &st, &sb);
+        d3 wo = v3(dot(direction, st), dot(direction, sb), dot(direction, sn));
+        d3 wi = v3(dot(toward_light, st), dot(toward_light, sb), dot(toward_light, sn));
+        if ((dot(toward_light, sg) > 0.0) != (wi.z > 0.0)) return;
+        double camera_bsdf_pdf = (wo.z > 0.0 && wi.z > 0.0) ? p_diffuse * wi.z / PI : 0.0;
+        spec f = (wo.z > 0.0 && wi.z > 0.0) ? eon(base, rough, wi, wo) : spec_zero();
+        uint32_t kind = ((bounces >> 8) & 0xffu) + 1u;
+        if ((double)kind > r->diffuse_limit || (bounces & 0xffu) >= 255u) return;
+        bounces = (bounces & ~(0xffu << 8)) + (kind << 8) + 1u;
+        throughput = spec_scale(spec_mul(throughput, f), shading_in * fabs(side) / light_pdf);
+        if (total + 1 >= 3) {
+            double survive = fmin(0.95, spec_max(r, throughput) * survival);
+            if (u[2] >= survive) return;
+            throughput = spec_scale(throughput, 1.0 / survive);
+        }
+        if (!(spec_max(r, throughput) > 0.0)) return;
+        double last = mis[1] > 0.0 ? camera_bsdf_pdf * back_reach / mis[1] : 0.0;
+        double sample_ratio;
+        if (total == 0) {
+            sample_ratio = 0.0;
+            if (camera_bsdf_pdf > 0.0) {
+                d3 from = offset_origin(p, sg);
+                d3 offset = sub(vertex, from);
+                double rch = len(offset);
+                d3 d = mul(offset, 1.0 / rch);
+                double ch = (1.0 - r->p_distant) * tree_pdf(r, emitter, from, sn);
+                double pdf = (code & 0x80000000u) ? tri_hit_pdf(r, code & 0x7fffffffu, d, rch) : light_hit_pdf(r, code, from, d, rch);
+                sample_ratio = ch * pdf / camera_bsdf_pdf;
+            }
+        } else {
+            sample_ratio = mis[3];
+        }
+        origin = offset_origin(p, side > 0.0 ? geometric : neg(geometric));
+        vertex = p;
+        dir = direction;
+        ray_pdf = light_pdf;
+        mis[0] *= last;
+        mis[1] = density;
+        mis[2] = fabs(side);
+        mis[3] = sample_ratio;
     }
 }
 
@@ -739,4 +1143,107 @@ void or_render_region(const or_render_desc *r, uint32_t samples, uint32_t sample
 
 void or_render(const or_render_desc *r, uint32_t samples, double *mean, double *var, int threads) {
     or_render_region(r, samples, 0, 0, (size_t)r->width * r->height, mean, var, NULL, threads);
+}
+
+/* ---- or_render_traced -------------------------------------------------------------- */
+
+typedef struct {
+    const or_render_desc *r;
+    uint32_t sample;
+    double *camera;             /* 3 per pixel */
+    double *splats;             /* 3 per pixel per worker */
+    size_t pixels;
+    size_t next_pixel, next_light;
+    uint64_t rays[2];
+    pthread_mutex_t lock;
+} traced_job;
+
+typedef struct {
+    traced_job *j;
+    int worker;
+} traced_arg;
+
+static void *traced_worker(void *arg) {
+    traced_arg *a = arg;
+    traced_job *j = a->j;
+    double *splat = j->splats + (size_t)a->worker * j->pixels * 3;
+    uint64_t rays[2] = {0, 0};
+    for (;;) {
+        pthread_mutex_lock(&j->lock);
+        size_t begin = j->next_pixel;
+        j->next_pixel = begin + 64 < j->pixels ? begin + 64 : j->pixels;
+        size_t end = j->next_pixel;
+        pthread_mutex_unlock(&j->lock);
+        if (begin >= end) break;
+        for (size_t at = begin; at < end; at++) render_sample(j->r, (uint32_t)at, j->sample, &j->camera[at * 3], rays);
+    }
+    for (;;) {
+        pthread_mutex_lock(&j->lock);
+        size_t begin = j->next_light;
+        j->next_light = begin + 64 < j->r->light_paths ? begin + 64 : j->r->light_paths;
+        size_t end = j->next_light;
+        pthread_mutex_unlock(&j->lock);
+        if (begin >= end) break;
+        for (size_t i = begin; i < end; i++) trace_light_path(j->r, j->sample, (uint32_t)i, splat, rays);
+    }
+    pthread_mutex_lock(&j->lock);
+    j->rays[0] += rays[0];
+    j->rays[1] += rays[1];
+    pthread_mutex_unlock(&j->lock);
+    return NULL;
+}
+
+void or_render_traced(const or_render_desc *r, uint32_t samples, uint32_t sample_first, double *mean, double *var,
+                      uint64_t rays[2], int threads) {
+    if (threads <= 0) threads = (int)sysconf(_SC_NPROCESSORS_ONLN);
+    if (threads > 256) threads = 256;
+    const size_t pixels = (size_t)r->width * r->height;
+    traced_job j;
+    j.r = r;
+    j.pixels = pixels;
+    j.camera = calloc(pixels * 3, sizeof(double));
+    j.splats = calloc(pixels * 3 * (size_t)threads, sizeof(double));
+    j.rays[0] = j.rays[1] = 0;
+    double *m2 = calloc(pixels * 3, sizeof(double));
+    for (size_t i = 0; i < pixels * 3; i++) mean[i] = 0.0;
+    pthread_mutex_init(&j.lock, NULL);
+    for (uint32_t s = 0; s < samples; s++) {
+        j.sample = sample_first + s;
+        j.next_pixel = j.next_light = 0;
+        for (size_t i = 0; i < pixels * 3 * (size_t)threads; i++) j.splats[i] = 0.0;
+        pthread_t ids[256];
+        traced_arg args[256];
+        for (int w = 0; w < threads; w++) {
+            args[w].j = &j;
+            args[w].worker = w;
+            pthread_create(&ids[w], NULL, traced_worker, &args[w]);
+        }
+        for (int w = 0; w < threads; w++) pthread_join(ids[w], NULL);
+        for (size_t px = 0; px < pixels; px++) {
+            double sp[3] = {0, 0, 0};
+            for (int w = 0; w < threads; w++)
+                for (int k = 0; k < 3; k++) sp[k] += j.splats[((size_t)w * pixels + px) * 3 + k];
+            double film_sp[3];
+            if (r->spectral) {
+                for (int k = 0; k < 3; k++) film_sp[k] = r->film[k * 3] * sp[0] + r->film[k * 3 + 1] * sp[1] + r->film[k * 3 + 2] * sp[2];
+            } else {
+                for (int k = 0; k < 3; k++) film_sp[k] = sp[k];
+            }
+            for (int k = 0; k < 3; k++) {
+                double v = j.camera[px * 3 + k] + film_sp[k];
+                double delta = v - mean[px * 3 + k];
+                mean[px * 3 + k] += delta / (double)(s + 1);
+                m2[px * 3 + k] += delta * (v - mean[px * 3 + k]);
+            }
+        }
+    }
+    for (size_t i = 0; i < pixels * 3; i++) var[i] = samples > 1 ? m2[i] / (double)(samples - 1) : 0.0;
+    pthread_mutex_destroy(&j.lock);
+    if (rays) {
+        rays[0] = j.rays[0];
+        rays[1] = j.rays[1];
+    }
+    free(m2);
+    free(j.camera);
+    free(j.splats);
 }

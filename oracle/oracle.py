@@ -6,6 +6,7 @@ checker and the CPU baseline; the product never does. Build with ``make -C oracl
 from __future__ import annotations
 
 import ctypes as C
+import math
 import os
 import subprocess
 from pathlib import Path
@@ -351,28 +352,65 @@ class RenderDesc(C.Structure):
                 ("cmf_integrals", C.c_double * 3), ("frame", C.c_float * 16), ("lens_radius", C.c_double),
                 ("focus_distance", C.c_double), ("forward", C.c_double * 3), ("width", C.c_uint32),
                 ("height", C.c_uint32), ("max_bounces", C.c_uint32), ("spectral", C.c_uint32), ("seed", C.c_uint32),
-                ("diffuse_limit", C.c_double), ("clamp", C.c_double)]
+                ("diffuse_limit", C.c_double), ("clamp", C.c_double), ("light_paths", C.c_uint32),
+                ("light_band", C.c_uint32), ("pixel_area_inv", C.c_double)]
 
 
 def render(arrays: dict, lights, library, frame, samples: int, max_bounces: int, spectral: bool, seed: int = 1,
-           background=(0.0, 0.0, 0.0), clamp: float = 0.0, diffuse_limit: float = 1024.0, threads: int = 0):
+           background=(0.0, 0.0, 0.0), clamp: float = 0.0, diffuse_limit: float = 1024.0, threads: int = 0,
+           light_tracing: float = 0.0, pool: int = 0):
     """The f64 estimator over a compiled scene's arrays (leaf order), the scene's lights
     (luce_render_b200.Light), the material library (default first, OrMaterial or
     luce_render_b200.OpenPbr) and a luce_render_b200.Frame. Returns (mean, variance),
-    each height x width x 3 (ACEScg)."""
-    job = RenderJob(arrays, lights, library, frame, max_bounces, spectral, seed, background, clamp, diffuse_limit)
+    each height x width x 3 (ACEScg); with light tracing, of each sample's image (camera
+    values plus that sample's light paths' splats)."""
+    job = RenderJob(arrays, lights, library, frame, max_bounces, spectral, seed, background, clamp, diffuse_limit,
+                    light_tracing, pool)
     n = frame.width * frame.height
-    mean, var, _ = job.region(samples, 0, 0, n, threads)
+    if job.light_paths:
+        mean, var, _ = job.traced(samples, 0, threads)
+    else:
+        mean, var, _ = job.region(samples, 0, 0, n, threads)
     return mean.reshape(frame.height, frame.width, 3), var.reshape(frame.height, frame.width, 3)
+
+
+def light_paths(light_tracing: float, pixels: int, pool: int, orthographic: bool, emitters: int):
+    """Loaded.light_paths (loading.lucb:163-168) and the band they follow: light tracing's
+    share of the pixels (at least one), at most a band's; none for an orthographic camera
+    or a scene without emitters (no light paths start from afar at the Lambertian
+    settings). Returns (light paths, band)."""
+    band = min(pool if pool > 0 else 2097152, pixels)
+    if light_tracing <= 0.0 or orthographic or emitters == 0:
+        return 0, band
+    wanted = max(1, int(math.floor(light_tracing * pixels + 0.5)))
+    return min(wanted, band), band
 
 
 class RenderJob:
     """A prepared f64 render: the loaded records built once, then any pixel range."""
 
     def __init__(self, arrays: dict, lights, library, frame, max_bounces: int, spectral: bool, seed: int = 1,
-                 background=(0.0, 0.0, 0.0), clamp: float = 0.0, diffuse_limit: float = 1024.0):
+                 background=(0.0, 0.0, 0.0), clamp: float = 0.0, diffuse_limit: float = 1024.0,
+                 light_tracing: float = 0.0, pool: int = 0):
         self.desc, self.keep = _render_desc(arrays, lights, library, frame, max_bounces, spectral, seed, background,
                                             clamp, diffuse_limit)
+        count, band = light_paths(light_tracing, frame.width * frame.height, pool, bool(frame.orthographic),
+                                  self.desc.emitter_count)
+        self.light_paths = count
+        self.desc.light_paths, self.desc.light_band = count, band
+        area = float(np.linalg.norm(np.array(frame.du)) * np.linalg.norm(np.array(frame.dv)))
+        self.desc.pixel_area_inv = 1.0 / area if area > 0.0 else 0.0
+        self.pixels = frame.width * frame.height
+
+    def traced(self, samples: int, sample_first: int = 0, threads: int = 0):
+        """All pixels with light tracing, samples [sample_first, + samples): (mean, var,
+        (closest rays, shadow rays)) of the per-sample images."""
+        mean = np.zeros(self.pixels * 3, np.float64)
+        var = np.zeros(self.pixels * 3, np.float64)
+        rays = (C.c_uint64 * 2)()
+        lib.or_render_traced(C.byref(self.desc), C.c_uint32(samples), C.c_uint32(sample_first), _p(mean, C.c_double),
+                             _p(var, C.c_double), rays, threads)
+        return mean.reshape(-1, 3), var.reshape(-1, 3), (int(rays[0]), int(rays[1]))
 
     def region(self, samples: int, sample_first: int, first: int, count: int, threads: int = 0):
         """Pixels [first, first + count), samples [sample_first, + samples): (mean, var,

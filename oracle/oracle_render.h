@@ -36,6 +36,11 @@ typedef struct {
     double lens_radius, focus_distance, forward[3];
     uint32_t width, height, max_bounces, spectral, seed;
     double diffuse_limit, clamp;
+    /* Light tracing (connect.glsl): light paths a sample (0: none), the band they follow
+     * (their sampler numbers are 0x80000000 | (band + i)), 1 / a pixel's area at unit
+     * distance. */
+    uint32_t light_paths, light_band;
+    double pixel_area_inv;
 } or_render_desc;
 
 void or_render(const or_render_desc *r, uint32_t samples, double *mean, double *var, int threads);
@@ -43,6 +48,12 @@ void or_render(const or_render_desc *r, uint32_t samples, double *mean, double *
  * samples); `rays` (may be NULL) counts the closest and shadow rays traced. */
 void or_render_region(const or_render_desc *r, uint32_t samples, uint32_t sample_first, size_t first, size_t count,
                       double *mean, double *var, uint64_t rays[2], int threads);
+
+/* With light tracing: per sample, every pixel's camera value plus the splats its light
+ * paths leave there; the mean and variance over samples [sample_first, + samples) of
+ * those images (ACEScg, 3 per pixel, all pixels). */
+void or_render_traced(const or_render_desc *r, uint32_t samples, uint32_t sample_first, double *mean, double *var,
+                      uint64_t rays[2], int threads);
 
 #ifdef __cplusplus
 }

@@ -1,5 +1,6 @@
 """Render cases shared by the batch and server tests: (compiled scene, settings) pairs of
-uneven sizes, spectral and RGB, depths 2 to 8, and the image a Renderer makes of each."""
+uneven sizes, spectral and RGB, depths 2 to 8, one with light tracing, and the image a
+Renderer makes of each."""
 import luce_render_b200 as lr
 from luce_render_b200 import scenes, testscenes
 
@@ -32,6 +33,12 @@ def cases():
     meshes, cams, lights, mats = testscenes.colored_light_scene(kelvin=3200.0)
     sc = lr.compile_scene(meshes, cams, lights, mats)
     out.append((sc, settings(16, 16, 6, 3, True, seed=9)))
+    # With light tracing: light paths share the pool and splat on the film.
+    sc = lr.compile_scene(scenes.cornell_meshes(materials=True), [scenes.cornell_camera()],
+                          [scenes.cornell_light()], scenes.cornell_materials())
+    traced = settings(40, 32, 3, 4, False, seed=13)
+    traced.light_tracing = 0.5
+    out.append((sc, traced))
     return out
 
 

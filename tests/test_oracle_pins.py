@@ -9,7 +9,7 @@ import numpy as np
 import pytest
 
 import luce_render_b200 as lr
-from luce_render_b200 import scenes
+from luce_render_b200 import scenes, testscenes
 from oracle import oracle as orc
 
 GOLDEN = Path(__file__).resolve().parent / "golden"
@@ -186,3 +186,30 @@ def test_light_tree_trails_and_energy():
         assert code & 0x80000000 and records[count * 4 + (code & 0x7FFFFFFF)] == index
         total += float(nodes[node][3])
     assert abs(float(nodes[0][3]) / total - 1.0) < 1e-4
+
+
+def test_oracle_light_tracing_is_unbiased():
+    # The three-technique estimator (connect.glsl) in f64: the area light's closed form
+    # within the reference's 2 % with light paths, and the Cornell box's image the same as
+    # camera paths alone within 3 sigma; the light paths contribute through their splats.
+
+    meshes, cams, lights, mats = testscenes.area_light_scene()
+    sc = lr.compile_scene(meshes, cams, lights, mats)
+    frame = lr.ray_frame(sc.camera(), 32, 32)
+    library = [lr.OpenPbr.lambert((0.5, 0.5, 0.5))] + list(mats)
+    mean, _ = orc.render(sc.arrays(), lights, library, frame, 128, 1, False, light_tracing=0.5)
+    assert abs(mean[14:18, 14:18, 1].mean() / testscenes.AREA_LIGHT_EXPECTED - 1.0) <= 0.02
+    job = orc.RenderJob(sc.arrays(), lights, library, frame, 1, False, light_tracing=0.5)
+    assert job.light_paths == 512
+    camera_part, _, _ = job.region(32, 0, 0, 32 * 32)
+    traced, _, _ = job.traced(32)
+    assert traced.sum() > camera_part.sum()  # splats add what the weights took away
+    sc = lr.compile_scene(scenes.cornell_meshes(True), [scenes.cornell_camera()], [scenes.cornell_light()],
+                          scenes.cornell_materials())
+    frame = lr.ray_frame(sc.camera(), 32, 32)
+    library = [lr.OpenPbr.lambert()] + scenes.cornell_materials()
+    a, va = orc.render(sc.arrays(), [scenes.cornell_light()], library, frame, 32, 5, True, light_tracing=0.5)
+    b, vb = orc.render(sc.arrays(), [scenes.cornell_light()], library, frame, 32, 5, True)
+    blocks = lambda x: x.reshape(4, 8, 4, 8, 3).mean((1, 3))
+    sem = np.sqrt((blocks(va) + blocks(vb)) / (64 * 32))
+    assert np.all(np.abs(blocks(a) - blocks(b)) <= 3.0 * sem + 1e-9)
