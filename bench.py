@@ -189,11 +189,11 @@ def build_scene(lr, scenes):
     return lr.compile_scene(meshes, [cam], lights, mats), lights, mats
 
 
-def settings_for(lr, samples: int, spectral: bool, profile: int = 0):
+def settings_for(lr, samples: int, spectral: bool, profile: int = 0, light_tracing: float = 0.0):
     s = lr.RenderSettings.of(WIDTH, HEIGHT, samples)
     s.max_bounces = BOUNCES
     s.spectral = 1 if spectral else 0
-    s.light_tracing = 0.0
+    s.light_tracing = light_tracing
     s.profile = profile
     s.c.material = lr.OpenPbr.lambert()
     return s
@@ -559,6 +559,30 @@ def main():
     e2e_rays = dist.sum((e1.closest_rays - e0.closest_rays) + (e1.shadow_rays - e0.shadow_rays))
     e2e_value = e2e_rays / dist.max(e2e_s) / 1e6
 
+    # The same workload with light tracing at the reference's default share (0.5): light
+    # paths and their camera connections count among the rays.
+    lt = lr.Renderer.create(ctx, sc, settings_for(lr, W + K, spectral, light_tracing=0.5))
+    for _ in range(W):
+        lt.advance_one()
+    lt.wait()
+    l0 = lt.stats()
+    dist.barrier()
+    ctx.synchronize()
+    ctx.timer_start()
+    for _ in range(K):
+        lt.advance_one()
+    lt.join()
+    lt_ms = dist.max(ctx.timer_stop())
+    lt.finish()
+    l1 = lt.stats()
+    lt.destroy()
+    lt_rays = dist.sum((l1.closest_rays - l0.closest_rays) + (l1.shadow_rays - l0.shadow_rays))
+    traced_info = {"light_tracing": 0.5, "value": lt_rays / (lt_ms / 1e3) / 1e6, "unit": "Mrays/s",
+                   "ms_per_step": lt_ms / K,
+                   "rays_per_step": lt_rays / K / dist.world,
+                   "note": "light paths (0.5 x the pixels a sample) from the scene's rect lights, their camera "
+                           "connections splatted; rays include the light paths' closest and connection rays"}
+
     batch_info = None if args.skip_batched else batched(lr, scenes, ctx, dist)
     served_info = None if args.skip_served else served(lr, scenes, dist, args.served_seconds)
 
@@ -594,6 +618,7 @@ def main():
                     "d2h_bytes_per_step": WIDTH * HEIGHT * 16},
             "gpu_launches": K * (1 + 3 * (BOUNCES + 1) + 3),
             "clocks": clock_info,
+            "light_traced": traced_info,
             "batched": batch_info,
             "served": served_info,
         }
