@@ -334,6 +334,14 @@ int lr_renderer_stats(lr_renderer *renderer, lr_render_stats *out);
 /* Renderer.destroy (integrator.lucb:887-900). */
 void lr_renderer_destroy(lr_renderer *renderer);
 
+/* (No counterpart in the reference, whose tables stay inside its kernels.) The albedo
+ * tables the glossy lobes' energy compensation reads (tables.comp:38-61,
+ * microfacet.glsl:67-84): LR_ALBEDO_TABLE_SIZE floats -- E_ggx[roughness][mu] (32 x 32),
+ * its average over mu (32), E_dielectric[z][roughness][mu] (16 x 32 x 32) -- made on the
+ * device once; copied to `out` (count at least LR_ALBEDO_TABLE_SIZE). */
+#define LR_ALBEDO_TABLE_SIZE 17440u
+int lr_albedo_tables(lr_context *ctx, float *out, size_t count);
+
 /* ---- Batches: many renders in one wavefront ------------------------------------------
  * No counterpart in the reference, which renders one scene per Renderer. A batch is a
  * pool of paths shared by its members (a member: an uploaded scene seen through one

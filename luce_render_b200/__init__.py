@@ -275,6 +275,7 @@ _SIGNATURES = {
     "lr_renderer_kernel_times": (C.c_int, [_vp, C.POINTER(C.c_double)]),
     "lr_renderer_stats": (C.c_int, [_vp, C.POINTER(RenderStats)]),
     "lr_renderer_destroy": (None, [_vp]),
+    "lr_albedo_tables": (C.c_int, [_vp, C.POINTER(C.c_float), _sz]),
     "lr_batch_settings_default": (None, [C.POINTER(BatchSettings)]),
     "lr_batch_create": (C.c_int, [_vp, C.POINTER(BatchSettings), C.POINTER(_vp)]),
     "lr_batch_add": (C.c_int, [_vp, _vp, _vp, C.POINTER(Settings), C.POINTER(Frame), C.POINTER(C.c_uint32)]),
@@ -638,6 +639,16 @@ def probe(ctx: Context, scene: GpuScene, frame: Frame, reference: bool = False):
 
 
 PROBE_STATIC_PIXELS = 1 << 21
+ALBEDO_TABLE_SIZE = 17440
+
+
+def albedo_tables(ctx: Context) -> np.ndarray:
+    """The albedo tables the glossy lobes read (E_ggx 32 x 32, its average over mu,
+    E_dielectric 16 x 32 x 32), as made on the device."""
+    out = np.empty(ALBEDO_TABLE_SIZE, np.float32)
+    _check(lib.lr_albedo_tables(ctx.handle, _fptr(out), out.size))
+    return out
+
 
 
 def probe_static(ctx: Context, scene: GpuScene, frame: Frame, reference: bool = False):

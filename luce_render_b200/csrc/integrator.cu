@@ -29,10 +29,12 @@
 #include <deque>
 #include <map>
 #include <memory>
+#include <mutex>
 #include <vector>
 
 #include "device.hpp"
 #include "loading.hpp"
+#include "openpbr.cuh"
 #include "shading.cuh"
 #include "traverse.cuh"
 
@@ -73,6 +75,9 @@ struct Member {
     float pixel_area_inv;
     unsigned long long *splat;
     unsigned long long *splat_lane[2];
+    // A material of the member's has a specular, metal, coat or transmission lobe: its
+    // surfaces take the layered OpenPBR shading (openpbr.cuh).
+    uint32_t glossy;
 };
 
 // Splats add as 64-bit integers (units of 2^-32 of the film's terms), so their sum does
@@ -597,6 +602,42 @@ __global__ void __launch_bounds__(kShadeBlock) camera_kernel(Wave w) {
     }
 }
 
+// One light sample at p (shade_surface.comp:167-197): a distant light by power, or an
+// emitter of the light tree by importance at `from` and `normal`. Returns the chance the
+// sample was taken with, 0 when none was; `emitter` is the tree's emitter (kNone for a
+// distant light).
+template <bool kSpectral>
+__device__ __forceinline__ float choose_light(const Member &m, const Constants &k, float4 u_light, float3 p, float3 from,
+                                              float3 normal, float4 lambda, LightSample &s, float4 &emitted,
+                                              uint32_t &emitter) {
+    const float4 *lights = m.lights;
+    emitted = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
+    emitter = kNone;
+    if (u_light.x < k.p_distant) {
+        float share;
+        const uint32_t light = pick_distant(lights, m.light_count, u_light.x / k.p_distant, share);
+        if (light != kNone && share > 0.0f && sample_light(lights, light, p, make_float2(u_light.y, u_light.z), s)) {
+            emitted = light_radiance<kSpectral>(lights, light, lambda);
+            return k.p_distant * share;
+        }
+        return 0.0f;
+    }
+    uint32_t chosen;
+    float tree_chance;
+    if (!tree_sample(m.tree, (u_light.x - k.p_distant) / fmaxf(1e-7f, 1.0f - k.p_distant), from, normal, chosen, tree_chance))
+        return 0.0f;
+    emitter = chosen;
+    const uint32_t code = __ldg(&m.tree.records[chosen]).x;
+    bool sampled;
+    if (code & kEmitterTriangle) {
+        sampled = sample_triangle<kSpectral>(m, code & ~kEmitterTriangle, p, make_float2(u_light.y, u_light.z), lambda, s, emitted);
+    } else {
+        sampled = sample_light(lights, code, p, make_float2(u_light.y, u_light.z), s);
+        if (sampled) emitted = light_radiance<kSpectral>(lights, code, lambda);
+    }
+    return sampled ? (1.0f - k.p_distant) * tree_chance : 0.0f;
+}
+
 struct ShadeOut {
     bool next = false, shadow = false;
     float4 o, d, so, sd, sc;
@@ -606,10 +647,145 @@ __device__ __forceinline__ float rgb_luminance(float3 c) {
     return c.x * 0.2722287168f + c.y * 0.6740817658f + c.z * 0.0536895174f;
 }
 
+// A surface hit of a member with glossy materials (shade_surface.comp:80-312, every
+// OpenPBR lobe): emission, then one light sample and one BSDF sample of the layered
+// surface, on either side of it when it transmits. Out of line, so that the Lambertian
+// members' shading keeps its registers, and compiled once whatever the pass's variant:
+// the compiler fuses multiply-adds by the code around them, so one body keeps a member's
+// image the same bits alone and in any mix.
+template <bool kSpectral>
+__device__ __noinline__ void shade_surface_glossy(const Wave &w, const Member &m, uint32_t sample, uint32_t round,
+                                                  uint32_t i, float4 ro, ShadeOut &out) {
+    const Constants &k = *m.k;
+    const uint32_t q = round & 1u;
+    const float4 rd = w.ray_d[q][i], hit = w.hits[q][i];
+    const uint32_t path = __float_as_uint(ro.w) & kPathMask;
+    const uint4 pu = w.path[path];
+    const uint32_t pixel = pu.x, bounces = pu.y, total = bounces & 0xffu;
+    const float ray_pdf = __uint_as_float(pu.w);
+    const float3 origin = xyz(ro), dir = xyz(rd);
+    float4 throughput = w.throughput[path];
+    const float4 lambda = kSpectral ? w.lambda[path] : make_float4(0.0f, 0.0f, 0.0f, 0.0f);
+    float4 radiance = w.radiance[path];
+    const bool tracing = m.light_paths != 0u;
+    const float4 mis = tracing ? w.mis[path] : make_float4(0.0f, 0.0f, 0.0f, 0.0f);
+    const float4 vertex_row = w.vertex[path];
+    const float3 vertex = xyz(vertex_row);
+
+    const uint32_t slot = __float_as_uint(hit.y);
+    const float3 p0 = position_of(m, m.scene.indices[slot * 3]);
+    float3 geometric = normalize(cross(position_of(m, m.scene.indices[slot * 3 + 1]) - p0,
+                                       position_of(m, m.scene.indices[slot * 3 + 2]) - p0));
+    // Faces wind counter-clockwise seen from outside: a ray along the normal is leaving.
+    const bool inside = dot(geometric, dir) > 0.0f;
+    if (inside) geometric = -geometric;
+    const uint4 attributes = __ldg(&m.scene.shading[slot]);
+    const uint32_t material = attributes.w;
+    const float3 p = origin + hit.x * dir;
+    const float reach = length(vertex - p);
+    const float density = (total == 0u ? mis.w : ray_pdf) * fabsf(dot(dir, geometric)) / (reach * reach);
+    const float back_reach = mis.z / (reach * reach);
+
+    const float4 emission_row = material_at(m, material, 7);
+    if (emission_row.w > 0.0f) {
+        float weight = 1.0f;
+        const uint32_t emitter = m.tree.triangle_map ? __ldg(&m.tree.triangle_map[slot]) : kNone;
+        if (total > 0u && ray_pdf > 0.0f && emitter != kNone) {
+            const float chance = (1.0f - k.p_distant) * tree_pdf(m.tree, emitter, vertex, octahedral_decode(pu.z));
+            const float traced = tracing ? camera_hit_ratio(m, mis, emitter, fabsf(dot(dir, geometric)), reach, ray_pdf) : 0.0f;
+            weight = mis_weight(triangle_hit_pdf(m, slot, dir, reach) * chance / ray_pdf, traced);
+        }
+        radiance = radiance + clamped<kSpectral>(throughput * spec_of<kSpectral>(material_at(m, material, 6), xyz(emission_row), lambda) * weight,
+                                                 total, k.clamp_indirect);
+    }
+    if (total >= k.max_bounces) {
+        w.radiance[path] = radiance;
+        return;
+    }
+    float3 normal = normalize(octahedral_decode(attributes.x) * (1.0f - hit.z - hit.w) + octahedral_decode(attributes.y) * hit.z +
+                              octahedral_decode(attributes.z) * hit.w);
+    if (dot(normal, geometric) < 0.0f) normal = -normal;
+    Surface surface = surface_at(normal, geometric, material, inside);
+    const float3 wo = to_local(surface, -dir);
+    prepare_surface<kSpectral>(surface, wo, lambda, m.materials);
+    const float3 from = offset_origin(p, geometric);
+
+    const float4 u_light = sample4(k.seed, pixel, sample, group_light(total));
+    LightSample s;
+    float4 emitted;
+    uint32_t nee_emitter;
+    const float chance = choose_light<kSpectral>(m, k, u_light, p, from, normal, lambda, s, emitted, nee_emitter);
+    if (chance > 0.0f) {
+        const float side = dot(s.direction, geometric);
+        const float3 wi = to_local(surface, s.direction);
+        if ((side > 0.0f) == (wi.z > 0.0f) && (side > 0.0f || surface.p_transmission > 0.0f)) {
+            float bsdf_pdf;
+            const float4 f = evaluate_surface(surface, wi, wo, bsdf_pdf);
+            if (bsdf_pdf > 0.0f) {
+                const float light_pdf = s.pdf * chance;
+                float traced = 0.0f;
+                if (tracing && !s.delta && nee_emitter != kNone && density > 0.0f) {
+                    const float d2 = s.distance * s.distance;
+                    const float at_last =
+                        total == 0u ? 1.0f : light_sampler_pdf(surface, s.direction, -dir, m.materials) * back_reach / mis.y;
+                    const float at_vertex = emission_direction_pdf(m, nee_emitter, s.cos_light) * fabsf(side) / d2 / density;
+                    const float at_light = emitter_area_pdf(m, nee_emitter) / (bsdf_pdf * s.cos_light / d2);
+                    traced = mis.x * at_last * at_vertex * at_light;
+                }
+                const float weight = s.delta ? 1.0f : mis_weight(bsdf_pdf / light_pdf, traced * bsdf_pdf / light_pdf);
+                const float4 contribution = clamped<kSpectral>(throughput * f * emitted * (fabsf(wi.z) * (weight / light_pdf)),
+                                                               total, k.clamp_indirect);
+                const float3 target = p + s.direction * s.distance;
+                const float margin = 4e-4f * fmaxf(1.0f, fmaxf(fabsf(target.x), fmaxf(fabsf(target.y), fabsf(target.z))));
+                const float shadow_reach = s.distance >= kInfinity ? kInfinity : fmaxf(0.0f, s.distance - margin);
+                const float3 so = offset_origin(p, side > 0.0f ? geometric : -geometric);
+                out.shadow = true;
+                out.so = make_float4(so.x, so.y, so.z, ro.w);
+                out.sd = make_float4(s.direction.x, s.direction.y, s.direction.z, shadow_reach);
+                out.sc = contribution;
+            }
+        }
+    }
+    w.radiance[path] = radiance;
+
+    // One BSDF sample (sample_surface with u.xyw: the lobe pick is u.w).
+    const float4 u = sample4(k.seed, pixel, sample, group_bsdf(total));
+    float3 wi;
+    float pdf, pdf_again;
+    uint32_t lobe;
+    if (!sample_direction(surface, wo, make_float3(u.x, u.y, u.w), wi, pdf, lobe)) return;
+    const float4 weight = evaluate_surface(surface, wi, wo, pdf_again) * (fabsf(wi.z) / pdf);
+    const float3 direction = to_world(surface, wi);
+    // A shading normal can send a ray to the wrong side of the true surface.
+    const float side = dot(direction, geometric);
+    if ((side > 0.0f) != (wi.z > 0.0f)) return;
+    const uint32_t next_bounces = next_bounce(bounces, lobe, k.limits);
+    if (next_bounces == kNone) return;
+    throughput = throughput * weight;
+    const float survival_scale = fminf(vertex_row.w, 1e6f);
+    if (total + 1u >= 3u) {
+        const float survive = fminf(0.95f, spec_max<kSpectral>(throughput) * survival_scale);
+        if (u.z >= survive) return;
+        throughput = make_float4(throughput.x / survive, throughput.y / survive, throughput.z / survive, throughput.w / survive);
+    }
+    const float3 next = side > 0.0f ? from : offset_origin(p, -geometric);
+    if (tracing) {
+        const float at_last =
+            total == 0u ? 1.0f : light_sampler_pdf(surface, direction, -dir, m.materials) * back_reach / mis.y;
+        w.mis[path] = make_float4(mis.x * at_last, density, fabsf(side), 0.0f);
+    }
+    w.path[path] = make_uint4(pixel, next_bounces, octahedral_encode(normal), __float_as_uint(pdf));
+    w.throughput[path] = throughput;
+    w.vertex[path] = make_float4(next.x, next.y, next.z, survival_scale);
+    out.next = true;
+    out.o = make_float4(next.x, next.y, next.z, ro.w);
+    out.d = make_float4(direction.x, direction.y, direction.z, kInfinity);
+}
+
 // One queue entry: a miss (shade_miss.comp:12-51), a light hit or a surface hit
 // (shade_surface.comp:48-312 at the Lambertian settings). kTracing: members of the pass
 // may trace light paths, so camera paths weigh their techniques against them.
-template <bool kSpectral, bool kTracing>
+template <bool kSpectral, bool kTracing, bool kGlossy>
 __device__ __forceinline__ void shade_one(const Wave &w, const Member &m, uint32_t sample, uint32_t round, uint32_t i,
                                           float4 ro, ShadeOut &out) {
     const Constants &k = *m.k;
@@ -675,6 +851,7 @@ __device__ __forceinline__ void shade_one(const Wave &w, const Member &m, uint32
     }
 
     // A surface.
+    if (kGlossy && m.glossy) return shade_surface_glossy<kSpectral>(w, m, sample, round, i, ro, out);
     const uint32_t slot = what;
     const float3 p0 = position_of(m, m.scene.indices[slot * 3]);
     float3 geometric = normalize(cross(position_of(m, m.scene.indices[slot * 3 + 1]) - p0,
@@ -957,13 +1134,146 @@ __device__ __noinline__ void shade_light(const Wave &w, const Member &m, uint32_
     out.d = make_float4(direction.x, direction.y, direction.z, kInfinity);
 }
 
+// A light path's hit on a member with glossy materials (light_paths.glsl:31-189, every
+// OpenPBR lobe): the surface read once on the side light arrives from; the camera
+// connection evaluates it as the camera would see it (oriented toward the camera, or read
+// again from the other side), the scattering samples light_lobes' choice and weighs the
+// direction by the BSDF as a camera arriving along it evaluates it.
+template <bool kSpectral>
+__device__ __noinline__ void shade_light_glossy(const Wave &w, const Member &m, uint32_t sample, uint32_t round, uint32_t i,
+                                                float4 ro, ShadeOut &out) {
+    const Constants &k = *m.k;
+    const uint32_t q = round & 1u;
+    const float4 hit = w.hits[q][i];
+    const uint32_t what = __float_as_uint(hit.y);
+    if (what == kNone || (what & kLightHit)) return;
+    const float4 rd = w.ray_d[q][i];
+    const uint32_t tag = __float_as_uint(ro.w);
+    const uint32_t path = tag & kPathMask;
+    const uint4 pu = w.path[path];
+    const uint32_t emitter = pu.x, bounces = pu.y, total = bounces & 0xffu;
+    const float ray_pdf = __uint_as_float(pu.w);
+    const float3 origin = xyz(ro), dir = xyz(rd);
+    float4 throughput = w.throughput[path];
+    const float4 lambda = kSpectral ? w.lambda[path] : make_float4(0.0f, 0.0f, 0.0f, 0.0f);
+    const float4 vertex_row = w.vertex[path];
+    const float4 mis = w.mis[path];
+    const uint32_t id = 0x80000000u | (m.light_band + tag_light_index(w, tag));
+
+    const uint32_t slot = what;
+    const float3 p0 = position_of(m, m.scene.indices[slot * 3]);
+    float3 geometric = normalize(cross(position_of(m, m.scene.indices[slot * 3 + 1]) - p0,
+                                       position_of(m, m.scene.indices[slot * 3 + 2]) - p0));
+    const bool back = dot(geometric, dir) > 0.0f;
+    if (back) geometric = -geometric;
+    const uint4 attributes = __ldg(&m.scene.shading[slot]);
+    const float3 p = origin + hit.x * dir;
+    if (total >= k.max_bounces) return;
+    float3 normal = normalize(octahedral_decode(attributes.x) * (1.0f - hit.z - hit.w) + octahedral_decode(attributes.y) * hit.z +
+                              octahedral_decode(attributes.z) * hit.w);
+    if (dot(normal, geometric) < 0.0f) normal = -normal;
+    const float4 u_lens = sample4(k.seed, id, sample, group_light(total));
+    const float3 lens = lens_point(m, make_float2(u_lens.x, u_lens.y));
+    uint32_t pixel = 0;
+    float3 to_point;
+    float camera_distance;
+    const bool on_film = camera_pixel(m, p, lens, pixel, to_point, camera_distance);
+    Surface lit = surface_at(normal, geometric, attributes.w, back);
+    const float3 toward_light = -dir;
+    read_material(lit, m.materials);
+    read_colors<kSpectral>(lit, m.materials, lambda);
+    const float3 x_last = xyz(vertex_row);
+    const float reach = length(x_last - p);
+    const float cos_in = fabsf(dot(dir, geometric));
+    const float density = ray_pdf * cos_in / (reach * reach);
+    const float back_reach = mis.z / (reach * reach);
+    const float cos_shading_in = dot(toward_light, normal);
+    if (cos_shading_in <= 0.0f || cos_in < 1e-6f) return;
+    const float shading_in = cos_shading_in / cos_in;
+    const float L = (float)m.light_paths;
+
+    if (on_film) {
+        const float3 to_camera = -to_point;
+        const float side = dot(to_camera, geometric);
+        Surface seen = side > 0.0f ? lit : turned(lit);
+        const float3 wo = to_local(seen, to_camera), wi = to_local(seen, toward_light);
+        if ((dot(toward_light, seen.geometric) > 0.0f) == (wi.z > 0.0f) && wo.z > 0.0f) {
+            if (side > 0.0f) orient_surface(seen, wo);
+            else prepare_surface<kSpectral>(seen, wo, lambda, m.materials);
+            float camera_bsdf_pdf;
+            const float4 f = evaluate_surface(seen, wi, wo, camera_bsdf_pdf);
+            const float camera_density = camera_pdf(m, to_point) * fabsf(side) / (camera_distance * camera_distance);
+            const float4 contribution = throughput * f * (shading_in * camera_density / L);
+            if (spec_max<kSpectral>(contribution) > 0.0f) {
+                const float last = mis.y > 0.0f ? camera_bsdf_pdf * back_reach / mis.y : 0.0f;
+                const float ratio = mis.x * last * camera_density / density;
+                const float sample_ratio = total == 0u ? light_sample_ratio(m, k, emitter, seen.normal, seen.geometric, p, x_last,
+                                                                            camera_bsdf_pdf)
+                                                       : fmaxf(mis.w, 0.0f);
+                const float weight = mis_weight(ratio / L, ratio * sample_ratio / L);
+                const float margin = 4e-4f * fmaxf(1.0f, fmaxf(fabsf(p.x), fmaxf(fabsf(p.y), fabsf(p.z))));
+                const float3 so = offset_origin(p, seen.geometric);
+                const float3 value = spec_to_film<kSpectral>(contribution * weight, lambda, k);
+                out.shadow = true;
+                out.so = make_float4(so.x, so.y, so.z, ro.w);
+                out.sd = make_float4(to_camera.x, to_camera.y, to_camera.z, fmaxf(0.0f, camera_distance - margin));
+                out.sc = make_float4(value.x, value.y, value.z, __uint_as_float(pixel));
+            }
+        }
+    }
+
+    // Scatter on, unless the next vertex would be past the bounce limit.
+    if (total + 1u >= k.max_bounces) return;
+    const float4 u = sample4(k.seed, id, sample, group_bsdf(total));
+    Surface choosing = lit;
+    light_lobes(choosing);
+    const float3 wo_light = to_local(lit, toward_light);
+    float3 wi_light;
+    float light_pdf;
+    uint32_t lobe;
+    if (!sample_direction(choosing, wo_light, make_float3(u.x, u.y, u.w), wi_light, light_pdf, lobe)) return;
+    const float3 direction = to_world(lit, wi_light);
+    const float side = dot(direction, geometric);
+    if ((side > 0.0f) != (wi_light.z > 0.0f)) return;
+    Surface seen = side > 0.0f ? lit : turned(lit);
+    const float3 wo = to_local(seen, direction), wi = to_local(seen, toward_light);
+    if ((dot(toward_light, seen.geometric) > 0.0f) != (wi.z > 0.0f)) return;
+    if (side > 0.0f) orient_surface(seen, wo);
+    else prepare_surface<kSpectral>(seen, wo, lambda, m.materials);
+    float camera_bsdf_pdf;
+    const float4 f = evaluate_surface(seen, wi, wo, camera_bsdf_pdf);
+    const uint32_t next_bounces = next_bounce(bounces, lobe, k.limits);
+    if (next_bounces == kNone) return;
+    throughput = throughput * f * (shading_in * fabsf(side) / light_pdf);
+    const float survival_scale = vertex_row.w;
+    if (total + 1u >= 3u) {
+        const float survive = fminf(0.95f, spec_max<kSpectral>(throughput) * survival_scale);
+        if (u.z >= survive) return;
+        throughput = make_float4(throughput.x / survive, throughput.y / survive, throughput.z / survive, throughput.w / survive);
+    }
+    if (!(spec_max<kSpectral>(throughput) > 0.0f)) return;
+    const float last = mis.y > 0.0f ? camera_bsdf_pdf * back_reach / mis.y : 0.0f;
+    const float sample_ratio =
+        total == 0u ? light_sample_ratio(m, k, emitter, seen.normal, seen.geometric, p, x_last, camera_bsdf_pdf) : mis.w;
+    const float3 next = offset_origin(p, side > 0.0f ? geometric : -geometric);
+    w.path[path] = make_uint4(emitter, next_bounces, 0u, __float_as_uint(light_pdf));
+    w.throughput[path] = throughput;
+    w.vertex[path] = make_float4(p.x, p.y, p.z, survival_scale);
+    w.mis[path] = make_float4(mis.x * last, density, fabsf(side), sample_ratio);
+    out.next = true;
+    out.o = make_float4(next.x, next.y, next.z, ro.w);
+    out.d = make_float4(direction.x, direction.y, direction.z, kInfinity);
+}
+
 // 8 blocks an SM (64 registers): shade_one wants 128, which leaves 16 warps an SM to hide
 // its memory latency; capped, it spills a little and runs 17 % faster (1.21 -> 1.01 ms a
 // 1080p pass on the 1M-triangle scene; 48 registers: 0.99 ms with twice the spills).
 // kTracing: the pass holds light paths or camera paths that weigh against them; passes
-// without take the kernel without that code (it cost camera-only passes 16 %).
-template <bool kTracing>
-__global__ void __launch_bounds__(kShadeBlock, 8) shade_kernel(Wave w, uint32_t round) {
+// without take the kernel without that code (it cost camera-only passes 16 %). kGlossy:
+// the pass holds a member with glossy materials, whose surfaces take the layered OpenPBR
+// shading (out of line, 4 blocks an SM for its registers); the rest shade as without it.
+template <bool kTracing, bool kGlossy>
+__global__ void __launch_bounds__(kShadeBlock, kGlossy ? 4 : 8) shade_kernel(Wave w, uint32_t round) {
     const uint32_t count = w.counters[round];
     const uint32_t q = round & 1u, nq = q ^ 1u;
     const uint32_t lane = threadIdx.x & 31u;
@@ -978,12 +1288,18 @@ __global__ void __launch_bounds__(kShadeBlock, 8) shade_kernel(Wave w, uint32_t 
             const Segment &sg = w.plan->seg[__float_as_uint(ro.w) >> kPathBits];
             const Member &m = w.members[sg.member];
             if (kTracing && sg.kind == kLightSegment) {
-                if (m.spectral) shade_light<true>(w, m, sg.sample, round, i, ro, out);
-                else shade_light<false>(w, m, sg.sample, round, i, ro, out);
+                if (kGlossy && m.glossy) {
+                    if (m.spectral) shade_light_glossy<true>(w, m, sg.sample, round, i, ro, out);
+                    else shade_light_glossy<false>(w, m, sg.sample, round, i, ro, out);
+                } else if (m.spectral) {
+                    shade_light<true>(w, m, sg.sample, round, i, ro, out);
+                } else {
+                    shade_light<false>(w, m, sg.sample, round, i, ro, out);
+                }
             } else if (m.spectral) {
-                shade_one<true, kTracing>(w, m, sg.sample, round, i, ro, out);
+                shade_one<true, kTracing, kGlossy>(w, m, sg.sample, round, i, ro, out);
             } else {
-                shade_one<false, kTracing>(w, m, sg.sample, round, i, ro, out);
+                shade_one<false, kTracing, kGlossy>(w, m, sg.sample, round, i, ro, out);
             }
         }
         const uint32_t at = warp_push(next_counter, out.next);
@@ -1238,7 +1554,7 @@ struct WaveHost {
     unsigned long long *d_stats = nullptr;
     std::vector<MemberHost> members;
     uint64_t member_uploads = 0;  // member records queued on the context's stream so far
-    int grid_shade = 0;
+    int grid_shade = 0, grid_shade_glossy = 0;
     std::map<int, int> grid_trace;  // by variant
     uint64_t recorded = 0, retired = 0;
     cudaEvent_t mark_start[2] = {nullptr, nullptr};
@@ -1271,14 +1587,21 @@ void mark(cudaStream_t stream, Marks *marks, int kind) {
 // (closest, shade, shadow) for every round. With `marks`, an event follows each kernel
 // (profiling); kCount instantiates the counting traversals.
 template <int W, int kStack, bool kCount>
-void record_trace(const WaveHost *h, const Wave &w, int grid_trace, bool tracing, cudaStream_t stream, Marks *marks) {
+void record_trace(const WaveHost *h, const Wave &w, int grid_trace, bool tracing, bool glossy, cudaStream_t stream,
+                  Marks *marks) {
     camera_kernel<<<h->grid_shade, kShadeBlock, 0, stream>>>(w);
     mark(stream, marks, kCamera);
     for (uint32_t round = 0; round < w.rounds; round++) {
         closest_kernel<W, kStack, kCount><<<grid_trace, kTraceBlock, 0, stream>>>(w, round);
         mark(stream, marks, kClosest);
-        if (tracing) shade_kernel<true><<<h->grid_shade, kShadeBlock, 0, stream>>>(w, round);
-        else shade_kernel<false><<<h->grid_shade, kShadeBlock, 0, stream>>>(w, round);
+        if (glossy) {
+            if (tracing) shade_kernel<true, true><<<h->grid_shade_glossy, kShadeBlock, 0, stream>>>(w, round);
+            else shade_kernel<false, true><<<h->grid_shade_glossy, kShadeBlock, 0, stream>>>(w, round);
+        } else if (tracing) {
+            shade_kernel<true, false><<<h->grid_shade, kShadeBlock, 0, stream>>>(w, round);
+        } else {
+            shade_kernel<false, false><<<h->grid_shade, kShadeBlock, 0, stream>>>(w, round);
+        }
         mark(stream, marks, kSurface);
         shadow_kernel<W, kStack, kCount><<<grid_trace, kTraceBlock, 0, stream>>>(w, round);
         mark(stream, marks, kShadow);
@@ -1316,19 +1639,20 @@ int grid_for(WaveHost *h, int variant) {
 }
 
 // A pass's variant: its traversal (BVH width * 1000 + stack entries), plus kTracingVariant
-// when it holds light tracing.
-constexpr int kTracingVariant = 100000;
+// when it holds light tracing and kGlossyVariant when it holds glossy materials.
+constexpr int kTracingVariant = 100000, kGlossyVariant = 200000;
 
 void record_trace_any(WaveHost *h, const Wave &w, int variant, cudaStream_t stream, Marks *marks) {
     const bool count = h->profile == 2;
-    const bool tracing = variant >= kTracingVariant;
+    const bool tracing = (variant / kTracingVariant) & 1;
+    const bool glossy = (variant / kTracingVariant) & 2;
     const int traversal = variant % kTracingVariant;
     const int grid = grid_for(h, traversal);
     switch (traversal) {
 #define LR_CASE(wd, k)                                                                        \
     case wd * 1000 + k:                                                                       \
-        if (count) record_trace<wd, k, true>(h, w, grid, tracing, stream, marks);             \
-        else record_trace<wd, k, false>(h, w, grid, tracing, stream, marks);                  \
+        if (count) record_trace<wd, k, true>(h, w, grid, tracing, glossy, stream, marks);     \
+        else record_trace<wd, k, false>(h, w, grid, tracing, glossy, stream, marks);          \
         break;
         LR_TRAVERSALS(LR_CASE)
 #undef LR_CASE
@@ -1362,6 +1686,22 @@ void destroy_graph(Graph &g) {
     if (g.exec) cudaGraphExecDestroy(g.exec);
     if (g.graph) cudaGraphDestroy(g.graph);
     g = Graph{};
+}
+
+// The albedo tables (tables.comp), made once a device on `stream` by its first wave; the
+// caller synchronizes the stream before any pass reads them.
+void make_albedo_tables(int device, cudaStream_t stream) {
+    static std::mutex lock;
+    static bool made[64] = {};
+    std::lock_guard<std::mutex> guard(lock);
+    if (device < 0 || device >= 64) fail(LR_INVALID, "no such CUDA device");
+    if (made[device]) return;
+    const uint32_t nodes = kTableMu * kTableRoughness * (1u + kTableEta);
+    albedo_table_kernel<<<(nodes + 63u) / 64u, 64, 0, stream>>>(0u);
+    albedo_table_kernel<<<1, 64, 0, stream>>>(1u);
+    LR_CUDA(cudaGetLastError());
+    LR_CUDA(cudaStreamSynchronize(stream));
+    made[device] = true;
 }
 
 void wave_create(WaveHost *h, lr_context *ctx, uint64_t pool, uint32_t rounds, uint32_t capacity, int profile) {
@@ -1434,8 +1774,10 @@ void wave_create(WaveHost *h, lr_context *ctx, uint64_t pool, uint32_t rounds, u
         LR_CUDA(cudaEventCreateWithFlags(&lane.finished, cudaEventDisableTiming));
     }
     upload_sobol_tables(ctx->stream);
+    make_albedo_tables(ctx->device, ctx->stream);
     LR_CUDA(cudaStreamSynchronize(ctx->stream));
-    h->grid_shade = grid_of(shade_kernel<false>, kShadeBlock, ctx->sm_count);
+    h->grid_shade = grid_of(shade_kernel<false, false>, kShadeBlock, ctx->sm_count);
+    h->grid_shade_glossy = grid_of(shade_kernel<false, true>, kShadeBlock, ctx->sm_count);
     if (profile)
         for (auto &e : h->mark_start) LR_CUDA(cudaEventCreate(&e));
     else
@@ -1585,6 +1927,7 @@ uint32_t member_add(WaveHost *h, const lr_gpu_scene *gs, lr_gpu_scene *owned, co
     m.splat = traced.count ? (unsigned long long *)at(p_splat) : nullptr;
     m.splat_lane[0] = traced.count ? (unsigned long long *)at(p_splat_lane0) : nullptr;
     m.splat_lane[1] = traced.count ? (unsigned long long *)at(p_splat_lane1) : nullptr;
+    m.glossy = L.glossy ? 1u : 0u;
     std::memcpy(stage, &m, sizeof m);
     LR_CUDA(cudaMemcpyAsync(h->d_members + index, stage, sizeof m, cudaMemcpyHostToDevice, stream));
     h->staging.queued(stream);
@@ -1737,7 +2080,9 @@ bool launch_pass(WaveHost *h, bool dry = false, int only = -1) {
     }
     const bool tracing = std::any_of(rec.members.begin(), rec.members.end(),
                                      [&](const std::pair<uint32_t, bool> &e) { return h->members[e.first].dev.light_paths != 0u; });
-    const int variant = width * 1000 + stack + (tracing ? kTracingVariant : 0);
+    const bool glossy = std::any_of(rec.members.begin(), rec.members.end(),
+                                    [&](const std::pair<uint32_t, bool> &e) { return h->members[e.first].dev.glossy != 0u; });
+    const int variant = width * 1000 + stack + (tracing ? kTracingVariant : 0) + (glossy ? kGlossyVariant : 0);
     staging->head = PlanHeader{n, used, converts, dry ? 1u : 0u, camera_paths, folds, 0u, 0u};
     cudaStream_t stream = lane.stream;
     // Member records queued on the context's stream reach this lane first.
@@ -1982,7 +2327,8 @@ void create(lr_context *ctx, const lr_scene *scene, const lr_settings &settings,
         if (!settings.profile)
             for (int li = 0; li < r->wave.lane_count; li++)
                 trace_graph(&r->wave, r->wave.lanes[li],
-                            c.width * 1000 + c.stack + (r->wave.members[0].dev.light_paths ? kTracingVariant : 0));
+                            c.width * 1000 + c.stack + (r->wave.members[0].dev.light_paths ? kTracingVariant : 0) +
+                                (r->wave.members[0].dev.glossy ? kGlossyVariant : 0));
     } catch (...) {
         const bool owned = !r->wave.members.empty() && r->wave.members[0].used;
         wave_destroy(&r->wave);
@@ -2103,6 +2449,17 @@ int lr_renderer_set_samples(lr_renderer *r, uint32_t samples) {
         if (!r) fail(LR_INVALID, "no renderer");
         if (samples == 0) fail(LR_INVALID, "a render needs samples");
         r->wave.members[0].samples = samples;
+    });
+}
+
+int lr_albedo_tables(lr_context *ctx, float *out, size_t count) {
+    return guarded([&] {
+        if (!ctx || !out) fail(LR_INVALID, "no context or buffer");
+        static_assert(kTableSize == LR_ALBEDO_TABLE_SIZE, "the table layout is the header's");
+        if (count < kTableSize) fail(LR_INVALID, "the tables hold " + std::to_string(kTableSize) + " floats");
+        LR_CUDA(cudaSetDevice(ctx->device));
+        make_albedo_tables(ctx->device, ctx->stream);
+        LR_CUDA(cudaMemcpyFromSymbol(out, g_albedo_tables, kTableSize * sizeof(float)));
     });
 }
 

@@ -305,18 +305,24 @@ void pack_material(const lr_openpbr &m, float program, std::vector<float> &out) 
     for (double v : rest) out.push_back((float)v);
 }
 
-// Scenes this build shades: Lambertian OpenPBR (EON diffuse with emission), opaque.
-void check_material(const lr_openpbr &m, size_t index) {
+// Materials this build shades: OpenPBR Surface's lobes (EON diffuse, GGX specular, F82
+// metal, coat, rough transmission, emission), opaque and, in the spectral build, without
+// dispersion.
+void check_material(const lr_openpbr &m, size_t index, bool spectral) {
     auto bad = [&](const char *what) {
-        fail(LR_INVALID, "material " + std::to_string(index) + ": " + what +
-                             " is not part of this build's Lambertian shading (set it to its neutral value)");
+        fail(LR_INVALID, "material " + std::to_string(index) + ": " + what + " is not part of this build's shading");
     };
-    if (m.specular_weight != 0.0) bad("specular_weight");
-    if (m.base_metalness != 0.0) bad("base_metalness");
-    if (m.transmission_weight != 0.0) bad("transmission_weight");
-    if (m.coat_weight != 0.0) bad("coat_weight");
-    if (m.geometry_opacity < 1.0) bad("geometry_opacity below 1");
+    if (m.geometry_opacity < 1.0) bad("geometry_opacity below 1 (cut-outs)");
+    if (spectral && m.transmission_weight > 0.0 && m.transmission_dispersion_scale > 0.0 &&
+        m.transmission_dispersion_abbe_number > 0.0)
+        bad("transmission dispersion");
     if (m.base_diffuse_roughness < 0.0 || m.base_diffuse_roughness > 1.0) bad("base_diffuse_roughness outside 0..1");
+}
+
+// Whether a material has a lobe besides EON diffuse (openpbr.glsl's HAS_COAT,
+// HAS_TRANSMISSION, HAS_METAL and a specular layer).
+bool is_glossy(const lr_openpbr &m) {
+    return m.specular_weight > 0.0 || m.base_metalness > 0.0 || m.transmission_weight > 0.0 || m.coat_weight > 0.0;
 }
 
 double scene_radius(const Scene &scene) {
@@ -332,7 +338,10 @@ Loaded load(const Scene &scene, const lr_settings &settings) {
     L.library.push_back(settings.material);
     for (const auto &m : scene.materials) L.library.push_back(m);
     for (size_t i = 0; i < L.library.size(); i++)
-        if (i >= scene.used.size() || scene.used[i]) check_material(L.library[i], i);
+        if (i >= scene.used.size() || scene.used[i]) {
+            check_material(L.library[i], i, settings.spectral != 0);
+            L.glossy = L.glossy || is_glossy(L.library[i]);
+        }
     L.radius = scene_radius(scene);
     L.lights = pack_lights(scene.lights, L.radius);
     L.tree = build_light_tree(scene, L.lights, L.library);

@@ -30,6 +30,7 @@ struct Loaded {
     LightTree tree;
     std::vector<float> materials;     // 64 floats per material
     double radius = 1.0, p_distant = 0.0;
+    bool glossy = false;              // a used material has more than EON diffuse
     double background_fit[4] = {0, 0, 0, 0};
     M3 film{};
     V3 cmf_integrals;

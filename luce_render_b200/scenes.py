@@ -287,3 +287,64 @@ def probe_test_scene():
     cams = [camera((0.5, 1.0, 6.0), (-0.15, 0.05, 0.0), focal_length=35.0, horizontal_aperture=36.0),
             camera((0.0, 0.0, 8.0), (-0.3, 0.2, 0.0), projection=1, focal_length=50.0, horizontal_aperture=60.0)]
     return meshes, cams
+
+
+# ---- glossy materials --------------------------------------------------------------------
+
+
+def openpbr(**fields) -> OpenPbr:
+    """OpenPbr.standard with the named fields set (colors as 3-tuples)."""
+    m = OpenPbr.standard()
+    for name, value in fields.items():
+        if isinstance(value, (tuple, list)):
+            getattr(m, name)[:] = list(value)
+        else:
+            setattr(m, name, value)
+    return m
+
+
+def glossy_cornell(ball_level: int = 3):
+    """The benchmark's layout: a Cornell box spanning x, z in [-1, 1] and y in [0, 2], open
+    toward +z (white floor, ceiling and back, red and green side walls, a 0.6 x 0.6 rect
+    light under the ceiling), holding a tall blue box under a clear coat, a smooth glass
+    ball, a rough gold ball, a small white cube and an orange rough plastic ball. Returns
+    (meshes, cameras, lights, materials); library materials 1..7 are white, red, green,
+    blue coat, glass, gold, orange."""
+    walls = [
+        (_quad((-1, 0, -1), (1, 0, -1), (1, 0, 1), (-1, 0, 1)), 1),    # floor, facing +y
+        (_quad((-1, 2, -1), (-1, 2, 1), (1, 2, 1), (1, 2, -1)), 1),    # ceiling, facing -y
+        (_quad((-1, 0, -1), (-1, 2, -1), (1, 2, -1), (1, 0, -1)), 1),  # back, facing +z
+        (_quad((-1, 0, -1), (-1, 0, 1), (-1, 2, 1), (-1, 2, -1)), 2),  # left (red), facing +x
+        (_quad((1, 0, -1), (1, 2, -1), (1, 2, 1), (1, 0, 1)), 3),      # right (green), facing -x
+    ]
+    meshes = [MeshData(p, t, faces=[0, 0], face_count=1, face_materials=[m]) for (p, t), m in walls]
+    for lo, hi, turn, at, material in [((-0.275, 0.0, -0.275), (0.275, 1.2, 0.275), 0.26, (-0.38, 0.0, -0.35), 4),
+                                       ((-0.175, 0.0, -0.175), (0.175, 0.35, 0.175), -0.3, (0.7, 0.0, 0.72), 1)]:
+        p, t, f = box_mesh(lo, hi)
+        meshes.append(MeshData(p, t, faces=f, face_count=6, face_materials=[material] * 6,
+                               transform=placement(at, (0.0, turn, 0.0))))
+    for radius, at, material in [(0.36, (0.3, 0.36, 0.05), 5), (0.26, (-0.5, 0.26, 0.5), 6),
+                                 (0.16, (0.0, 0.16, 0.62), 7)]:
+        p, t, n = icosphere(ball_level, radius)
+        meshes.append(MeshData(p, t, normals=n, faces=np.zeros(len(t), np.uint32), face_count=1,
+                               face_materials=[material], transform=placement(at)))
+    materials = [openpbr(base_color=(0.73, 0.73, 0.73), specular_weight=0.0),
+                 openpbr(base_color=(0.63, 0.065, 0.05), specular_weight=0.0),
+                 openpbr(base_color=(0.14, 0.45, 0.091), specular_weight=0.0),
+                 openpbr(base_color=(0.08, 0.16, 0.55), coat_weight=1.0, coat_roughness=0.05, specular_roughness=0.5),
+                 openpbr(transmission_weight=1.0, specular_roughness=0.0, base_color=(1.0, 1.0, 1.0)),
+                 openpbr(base_color=(1.0, 0.77, 0.34), base_metalness=1.0, specular_roughness=0.35),
+                 openpbr(base_color=(0.9, 0.35, 0.05), specular_roughness=0.45, base_diffuse_roughness=0.5)]
+    lights = [light(LIGHT_RECT, position=(0.0, 1.998, 0.0), rotation=(-0.5 * math.pi, 0.0, 0.0), intensity=15.0,
+                    width=0.6, height=0.6, normalize=False, visible=True)]
+    cams = [camera((0.0, 1.0, 3.9), (0.0, 0.0, 0.0), focal_length=18.0 / math.tan(math.radians(20.0)),
+                   horizontal_aperture=36.0)]
+    return meshes, cams, lights, materials
+
+
+def furnace_sphere(level: int = 4):
+    """A unit icosphere (smooth normals) at the origin and a camera at (0, 1, 4) looking at
+    its centre (50 mm on a 36 mm film), for furnaces under a uniform background."""
+    p, t, n = icosphere(level, 1.0)
+    cam = camera((0.0, 1.0, 4.0), (-math.atan2(1.0, 4.0), 0.0, 0.0), focal_length=50.0, horizontal_aperture=36.0)
+    return [MeshData(p, t, normals=n)], [cam]

@@ -16,34 +16,12 @@
 
 #include "oracle.h"
 #include "oracle_render.h"
+#include "oracle_vec.h"
+#include "oracle_openpbr.h"
 
-#define PI 3.14159265358979323846
 #define INF 3.0e38
 #define NONE 0xffffffffu
 #define LIGHT_HIT 0x80000000u
-
-typedef struct {
-    double x, y, z;
-} d3;
-
-static d3 v3(double x, double y, double z) { d3 r = {x, y, z}; return r; }
-static d3 add(d3 a, d3 b) { return v3(a.x + b.x, a.y + b.y, a.z + b.z); }
-static d3 sub(d3 a, d3 b) { return v3(a.x - b.x, a.y - b.y, a.z - b.z); }
-static d3 mul(d3 a, double s) { return v3(a.x * s, a.y * s, a.z * s); }
-static double dot(d3 a, d3 b) { return a.x * b.x + a.y * b.y + a.z * b.z; }
-static d3 cross(d3 a, d3 b) { return v3(a.y * b.z - a.z * b.y, a.z * b.x - a.x * b.z, a.x * b.y - a.y * b.x); }
-static double len(d3 a) { return sqrt(dot(a, a)); }
-static d3 norm(d3 a) { return mul(a, 1.0 / len(a)); }
-static d3 neg(d3 a) { return v3(-a.x, -a.y, -a.z); }
-
-typedef struct {
-    double s[4];
-} spec;
-
-static spec spec_scale(spec a, double k) { for (int i = 0; i < 4; i++) a.s[i] *= k; return a; }
-static spec spec_mul(spec a, spec b) { for (int i = 0; i < 4; i++) a.s[i] *= b.s[i]; return a; }
-static spec spec_add(spec a, spec b) { for (int i = 0; i < 4; i++) a.s[i] += b.s[i]; return a; }
-static spec spec_zero(void) { spec z = {{0, 0, 0, 0}}; return z; }
 
 /* ---- scene access ----------------------------------------------------------------- */
 
@@ -143,17 +121,7 @@ static uint32_t trace64(const or_render_desc *r, d3 o, d3 d, double tmax, int an
 /* ---- spectra and lights ---------------------------------------------------------------- */
 
 static spec spec_of(const or_render_desc *r, const float fit[4], const float rgb[3], const double lambda[4]) {
-    spec s;
-    if (!r->spectral) {
-        s.s[0] = rgb[0], s.s[1] = rgb[1], s.s[2] = rgb[2], s.s[3] = 0.0;
-        return s;
-    }
-    for (int i = 0; i < 4; i++) {
-        double x = (lambda[i] - 360.0) / (830.0 - 360.0);
-        double z = ((double)fit[0] * x + fit[1]) * x + fit[2];
-        s.s[i] = fit[3] * (0.5 + z / (2.0 * sqrt(1.0 + z * z)));
-    }
-    return s;
+    return spec_fit(r->spectral, fit, rgb, lambda);
 }
 
 static double spec_max(const or_render_desc *r, spec s) {
@@ -185,26 +153,11 @@ typedef struct {
     int delta;
 } lsample;
 
-static void onb(d3 n, d3 *t, d3 *b) {
-    double s = n.z >= 0.0 ? 1.0 : -1.0, a = -1.0 / (s + n.z), c = n.x * n.y * a;
-    *t = v3(1.0 + s * n.x * n.x * a, s * c, -s * n.x);
-    *b = v3(c, s + n.y * n.y * a, -n.y);
-}
-
 static d3 sample_cone(d3 axis, double cos_max, double u0, double u1) {
     double c = 1.0 - u0 * (1.0 - cos_max), s = sqrt(fmax(0.0, 1.0 - c * c)), phi = 2.0 * PI * u1;
     d3 t, b;
     onb(axis, &t, &b);
     return norm(add(add(mul(t, s * cos(phi)), mul(b, s * sin(phi))), mul(axis, c)));
-}
-
-static void concentric(double u0, double u1, double *x, double *y) {
-    double ox = 2.0 * u0 - 1.0, oy = 2.0 * u1 - 1.0, rr, th;
-    if (ox == 0.0 && oy == 0.0) { *x = *y = 0.0; return; }
-    if (fabs(ox) > fabs(oy)) { rr = ox; th = (PI / 4.0) * (oy / ox); }
-    else { rr = oy; th = (PI / 2.0) - (PI / 4.0) * (ox / oy); }
-    *x = rr * cos(th);
-    *y = rr * sin(th);
 }
 
 static double sphere_hit(d3 c, double radius, d3 o, d3 d) {
@@ -506,17 +459,6 @@ static double light_cos(const or_render_desc *r, uint32_t light, d3 o, d3 d, dou
     return fmax(0.0, -dot(d, rv(row(r, light, 3))));
 }
 
-/* light_sampler_pdf (connect.glsl:52-62) at the Lambertian settings: the surface (shading
- * normal n, geometric g, facing one side) seen from `from`'s side, the cosine lobe. */
-static double light_sampler_pdf(double p_diffuse, d3 n, d3 g, d3 from, d3 to) {
-    int same = dot(from, g) >= 0.0;
-    d3 nv = same ? n : neg(n), gv = same ? g : neg(g);
-    double wo_z = dot(from, nv), wi_z = dot(to, nv);
-    if ((dot(to, gv) > 0.0) != (wi_z > 0.0)) return 0.0;
-    if (wo_z <= 0.0 || wi_z <= 0.0) return 0.0;
-    return p_diffuse * wi_z / PI;
-}
-
 static double mis_weight(double a, double b) {
     a = fmin(a, 1e18);
     b = fmin(b, 1e18);
@@ -532,29 +474,6 @@ static spec clamped(const or_render_desc *r, spec c, uint32_t total) {
     if (total == 0 || r->clamp <= 0.0) return c;
     double m = spec_max(r, c);
     return m > r->clamp ? spec_scale(c, r->clamp / m) : c;
-}
-
-static double fon_albedo(double mu, double rr) {
-    double m = 1.0 - mu;
-    double g = m * (0.0571085289 + m * (0.491881867 + m * (-0.332181442 + m * 0.0714429953)));
-    return (1.0 + rr * g) / (1.0 + (0.5 - 2.0 / (3.0 * PI)) * rr);
-}
-
-static spec eon(spec rho, double rr, d3 wi, d3 wo) {
-    const double c1 = 0.5 - 2.0 / (3.0 * PI), c2 = 2.0 / 3.0 - 28.0 / (15.0 * PI);
-    double s = dot(wi, wo) - wi.z * wo.z;
-    double st = s > 0.0 ? s / fmax(wi.z, wo.z) : s;
-    double a = 1.0 / (1.0 + c1 * rr);
-    double eo = fon_albedo(wo.z, rr), ei = fon_albedo(wi.z, rr);
-    double avg = a * (1.0 + c2 * rr);
-    double k = fmax(1e-7, 1.0 - eo) * fmax(1e-7, 1.0 - ei) / (PI * fmax(1e-7, 1.0 - avg));
-    spec out;
-    for (int i = 0; i < 4; i++) {
-        double single = rho.s[i] * (a * (1.0 + rr * st) / PI);
-        double ms = rho.s[i] * rho.s[i] * avg / (1.0 - rho.s[i] * (1.0 - avg));
-        out.s[i] = single + ms * k;
-    }
-    return out;
 }
 
 static d3 oct_decode(uint32_t packed) {
@@ -680,7 +599,9 @@ static void render_sample(const or_render_desc *r, uint32_t pixel, uint32_t samp
         uint32_t slot = what;
         d3 p0 = point(r, r->indices[slot * 3]);
         d3 geometric = norm(cross(sub(point(r, r->indices[slot * 3 + 1]), p0), sub(point(r, r->indices[slot * 3 + 2]), p0)));
-        if (dot(geometric, dir) > 0.0) geometric = neg(geometric);
+        /* Faces wind counter-clockwise seen from outside: a ray along the normal leaves. */
+        int inside = dot(geometric, dir) > 0.0;
+        if (inside) geometric = neg(geometric);
         const uint32_t *attr = &r->shading[slot * 4];
         uint32_t m = attr[3];
         d3 p = add(origin, mul(dir, t));
@@ -703,14 +624,9 @@ static void render_sample(const or_render_desc *r, uint32_t pixel, uint32_t samp
         if (total >= r->max_bounces) break;
         d3 normal = norm(add(add(mul(oct_decode(attr[0]), 1.0 - hu - hv), mul(oct_decode(attr[1]), hu)), mul(oct_decode(attr[2]), hv)));
         if (dot(normal, geometric) < 0.0) normal = neg(normal);
-        d3 tg, bt;
-        onb(normal, &tg, &bt);
-        d3 wo = v3(-dot(dir, tg), -dot(dir, bt), -dot(dir, normal));
-        const float *brgb = material(r, m, 1);
-        spec base = spec_scale(spec_of(r, material(r, m, 0), brgb, lambda), brgb[3]);
-        double rough = material(r, m, 10)[1];
-        double lum = (brgb[0] * 0.2722287168 + brgb[1] * 0.6740817658 + brgb[2] * 0.0536895174) * brgb[3];
-        double p_diffuse = fmax(lum, 0.0) > 0.0 ? 1.0 : 0.0;
+        or_surface surface = or_surface_at(normal, geometric, m, inside);
+        d3 wo = or_to_local(&surface, neg(dir));
+        or_prepare_surface(&surface, wo, r->materials, (int)r->spectral, lambda);
         d3 from = offset_origin(p, geometric);
         double ul[4];
         or_sample4(r->seed, pixel, sample, 2 + 3 * total, ul);
@@ -764,11 +680,11 @@ static void render_sample(const or_render_desc *r, uint32_t pixel, uint32_t samp
         }
         if (sampled && chance > 0.0) {
             double side = dot(s.direction, geometric);
-            d3 wi = v3(dot(s.direction, tg), dot(s.direction, bt), dot(s.direction, normal));
-            if (side > 0.0 && wi.z > 0.0 && wo.z > 0.0) {
-                double bsdf_pdf = p_diffuse * wi.z / PI;
+            d3 wi = or_to_local(&surface, s.direction);
+            if ((side > 0.0) == (wi.z > 0.0) && (side > 0.0 || surface.p_transmission > 0.0)) {
+                double bsdf_pdf;
+                spec fv = or_evaluate_surface(&surface, wi, wo, &bsdf_pdf);
                 if (bsdf_pdf > 0.0) {
-                    spec fv = eon(base, rough, wi, wo);
                     double light_pdf = s.pdf * chance;
                     /* The light tracer's density of this path over the camera's BSDF ray
                      * reaching the same light point (shade_surface.comp:210-224). */
@@ -776,7 +692,7 @@ static void render_sample(const or_render_desc *r, uint32_t pixel, uint32_t samp
                     if (tracing && !s.delta && nee_emitter != NONE && density > 0.0) {
                         double d2 = s.distance * s.distance;
                         double at_last = total == 0 ? 1.0
-                                                    : light_sampler_pdf(p_diffuse, normal, geometric, s.direction, neg(dir)) *
+                                                    : or_light_sampler_pdf(&surface, r->materials, s.direction, neg(dir)) *
                                                           back_reach / mis[1];
                         double at_vertex = emission_direction_pdf(r, nee_emitter, s.cos_light) * fabs(side) / d2 / density;
                         double at_light = emitter_area_pdf(r, nee_emitter) / (bsdf_pdf * s.cos_light / d2);
@@ -789,27 +705,26 @@ static void render_sample(const or_render_desc *r, uint32_t pixel, uint32_t samp
                     double sreach = s.distance >= INF ? INF : fmax(0.0, s.distance - margin);
                     double tt, uu, vv;
                     rays[1]++;
-                    if (trace64(r, offset_origin(p, geometric), s.direction, sreach, 1, &tt, &uu, &vv) == NONE)
+                    if (trace64(r, offset_origin(p, side > 0.0 ? geometric : neg(geometric)), s.direction, sreach, 1, &tt,
+                                &uu, &vv) == NONE)
                         radiance = spec_add(radiance, c);
                 }
             }
         }
         double u[4];
         or_sample4(r->seed, pixel, sample, 3 + 3 * total, u);
-        if (wo.z <= 0.0 || !(u[3] < p_diffuse)) break;
-        double dx, dy;
-        concentric(u[0], u[1], &dx, &dy);
-        d3 wi = v3(dx, dy, sqrt(fmax(0.0, 1.0 - (dx * dx + dy * dy))));
-        if (wi.z == 0.0) break;
-        double pdf = p_diffuse * wi.z / PI;
-        if (!(pdf > 0.0)) break;
-        spec weight = spec_scale(eon(base, rough, wi, wo), fabs(wi.z) / pdf);
-        d3 direction = add(add(mul(tg, wi.x), mul(bt, wi.y)), mul(normal, wi.z));
+        d3 wi;
+        double pdf, pdf_again;
+        uint32_t lobe;
+        if (!or_sample_direction(&surface, wo, u[0], u[1], u[3], &wi, &pdf, &lobe)) break;
+        spec weight = spec_scale(or_evaluate_surface(&surface, wi, wo, &pdf_again), fabs(wi.z) / pdf);
+        d3 direction = or_to_world(&surface, wi);
+        /* A shading normal can send a ray to the wrong side of the true surface. */
         double side = dot(direction, geometric);
         if ((side > 0.0) != (wi.z > 0.0)) break;
-        uint32_t kind = ((bounces >> 8) & 0xffu) + 1u;
-        if ((double)kind > r->diffuse_limit || (bounces & 0xffu) >= 255u) break;
-        bounces = (bounces & ~(0xffu << 8)) + (kind << 8) + 1u;
+        uint32_t kind = ((bounces >> (8u * (lobe + 1u))) & 0xffu) + 1u;
+        if ((double)kind > r->limits[lobe] || (bounces & 0xffu) >= 255u) break;
+        bounces = (bounces & ~(0xffu << (8u * (lobe + 1u)))) + (kind << (8u * (lobe + 1u))) + 1u;
         throughput = spec_mul(throughput, weight);
         double scale = fmin(survival, 1e6);
         if (total + 1 >= 3) {
@@ -822,7 +737,7 @@ static void render_sample(const or_render_desc *r, uint32_t pixel, uint32_t samp
             /* This vertex's factor of the light tracer's density, settled now that the light
              * sampler's direction here is known (shade_surface.comp:304-307). */
             double at_last = total == 0 ? 1.0
-                                        : light_sampler_pdf(p_diffuse, normal, geometric, direction, neg(dir)) * back_reach / mis[1];
+                                        : or_light_sampler_pdf(&surface, r->materials, direction, neg(dir)) * back_reach / mis[1];
             mis[0] *= at_last;
             mis[1] = density;
             mis[2] = fabs(side);
@@ -843,6 +758,22 @@ static void render_sample(const or_render_desc *r, uint32_t pixel, uint32_t samp
     } else {
         out[0] = value[0], out[1] = value[1], out[2] = value[2];
     }
+}
+
+/* light_sample_ratio (light_paths.glsl:15-29): the light sample a camera path at p (the
+ * surface `s` faces its side) would take toward the light path's first point x0, over its
+ * BSDF pdf toward it. */
+static double light_sample_ratio(const or_render_desc *r, uint32_t emitter, const or_surface *s, d3 p, d3 x0,
+                                 double bsdf_pdf) {
+    if (!(bsdf_pdf > 0.0)) return 0.0;
+    d3 from = offset_origin(p, s->geometric);
+    d3 offset = sub(x0, from);
+    double reach = len(offset);
+    d3 d = mul(offset, 1.0 / reach);
+    double chance = (1.0 - r->p_distant) * tree_pdf(r, emitter, from, s->normal);
+    uint32_t code = r->tree_records[emitter * 4];
+    double pdf = (code & 0x80000000u) ? tri_hit_pdf(r, code & 0x7fffffffu, d, reach) : light_hit_pdf(r, code, from, d, reach);
+    return chance * pdf / bsdf_pdf;
 }
 
 /* light_emit.comp:55-136 and light_paths.glsl:27-189 at the Lambertian settings: light
@@ -932,7 +863,8 @@ static void trace_light_path(const or_render_desc *r, uint32_t sample, uint32_t 
         uint32_t slot = what;
         d3 p0 = point(r, r->indices[slot * 3]);
         d3 geometric = norm(cross(sub(point(r, r->indices[slot * 3 + 1]), p0), sub(point(r, r->indices[slot * 3 + 2]), p0)));
-        if (dot(geometric, dir) > 0.0) geometric = neg(geometric);
+        int back = dot(geometric, dir) > 0.0;
+        if (back) geometric = neg(geometric);
         const uint32_t *attr = &r->shading[slot * 4];
         uint32_t m = attr[3];
         d3 p = add(origin, mul(dir, t));
@@ -946,12 +878,12 @@ static void trace_light_path(const or_render_desc *r, uint32_t sample, uint32_t 
         d3 to_point;
         double camera_distance;
         int on_film = camera_pixel(r, p, lens, &pixel, &to_point, &camera_distance);
-        const float *brgb = material(r, m, 1);
-        spec base = spec_scale(spec_of(r, material(r, m, 0), brgb, lambda), brgb[3]);
-        double rough = material(r, m, 10)[1];
-        double lum = (brgb[0] * 0.2722287168 + brgb[1] * 0.6740817658 + brgb[2] * 0.0536895174) * brgb[3];
-        double p_diffuse = fmax(lum, 0.0) > 0.0 ? 1.0 : 0.0;
+        /* The surface on the side light arrives from, read once: seen from the camera or the
+         * next vertex on that side, it is only oriented (light_paths.glsl:93-96). */
+        or_surface lit = or_surface_at(normal, geometric, m, back);
         d3 toward_light = neg(dir);
+        or_read_material(&lit, r->materials);
+        or_read_colors(&lit, r->materials, (int)r->spectral, lambda);
         double reach = len(sub(vertex, p));
         double cos_in = fabs(dot(dir, geometric));
         double density = ray_pdf * cos_in / (reach * reach);
@@ -962,38 +894,23 @@ static void trace_light_path(const or_render_desc *r, uint32_t sample, uint32_t 
         if (on_film) {
             d3 to_camera = neg(to_point);
             double side = dot(to_camera, geometric);
-            d3 sn = side > 0.0 ? normal : neg(normal), sg = side > 0.0 ? geometric : neg(geometric);
-            d3 st, sb;
-            onb(sn, &st, &sb);
-            d3 wo = v3(dot(to_camera, st), dot(to_camera, sb), dot(to_camera, sn));
-            d3 wi = v3(dot(toward_light, st), dot(toward_light, sb), dot(toward_light, sn));
-            if ((dot(toward_light, sg) > 0.0) == (wi.z > 0.0) && wo.z > 0.0 && wi.z > 0.0) {
-                double camera_bsdf_pdf = p_diffuse * wi.z / PI;
-                spec f = eon(base, rough, wi, wo);
+            or_surface seen = side > 0.0 ? lit : or_turned(&lit);
+            d3 wo = or_to_local(&seen, to_camera), wi = or_to_local(&seen, toward_light);
+            if ((dot(toward_light, seen.geometric) > 0.0) == (wi.z > 0.0) && wo.z > 0.0) {
+                if (side > 0.0) or_orient_surface(&seen, wo);
+                else or_prepare_surface(&seen, wo, r->materials, (int)r->spectral, lambda);
+                double camera_bsdf_pdf;
+                spec f = or_evaluate_surface(&seen, wi, wo, &camera_bsdf_pdf);
                 double camera_density = camera_pdf(r, to_point) * fabs(side) / (camera_distance * camera_distance);
                 spec contribution = spec_scale(spec_mul(throughput, f), shading_in * camera_density / L);
                 if (spec_max(r, contribution) > 0.0) {
                     double last = mis[1] > 0.0 ? camera_bsdf_pdf * back_reach / mis[1] : 0.0;
                     double ratio = mis[0] * last * camera_density / density;
-                    double sample_ratio;
-                    if (total == 0) {
-                        sample_ratio = 0.0;
-                        if (camera_bsdf_pdf > 0.0) {
-                            d3 from = offset_origin(p, sg);
-                            d3 offset = sub(vertex, from);
-                            double rch = len(offset);
-                            d3 d = mul(offset, 1.0 / rch);
-                            double ch = (1.0 - r->p_distant) * tree_pdf(r, emitter, from, sn);
-                            double pdf = (code & 0x80000000u) ? tri_hit_pdf(r, code & 0x7fffffffu, d, rch)
-                                                               : light_hit_pdf(r, code, from, d, rch);
-                            sample_ratio = ch * pdf / camera_bsdf_pdf;
-                        }
-                    } else {
-                        sample_ratio = fmax(mis[3], 0.0);
-                    }
+                    double sample_ratio = total == 0 ? light_sample_ratio(r, emitter, &seen, p, vertex, camera_bsdf_pdf)
+                                                     : fmax(mis[3], 0.0);
                     double weight = mis_weight(ratio / L, ratio * sample_ratio / L);
                     double margin = 4e-4 * fmax(1.0, fmax(fabs(p.x), fmax(fabs(p.y), fabs(p.z))));
-                    d3 so = offset_origin(p, sg);
+                    d3 so = offset_origin(p, seen.geometric);
                     double sreach = fmax(0.0, camera_distance - margin);
                     int blocked = 0;
                     for (uint32_t l = 0; l < r->light_count && !blocked; l++)
@@ -1014,30 +931,27 @@ static void trace_light_path(const or_render_desc *r, uint32_t sample, uint32_t 
         if (total + 1 >= r->max_bounces) return;
         double u[4];
         or_sample4(r->seed, id, sample, 3 + 3 * total, u);
-        d3 tg2, bt2;
-        onb(normal, &tg2, &bt2);
-        d3 wo_light = v3(dot(toward_light, tg2), dot(toward_light, bt2), dot(toward_light, normal));
-        if (wo_light.z <= 0.0 || !(u[3] < p_diffuse)) return;
-        double ddx, ddy;
-        concentric(u[0], u[1], &ddx, &ddy);
-        d3 wl = v3(ddx, ddy, sqrt(fmax(0.0, 1.0 - (ddx * ddx + ddy * ddy))));
-        if (wl.z == 0.0) return;
-        double light_pdf = p_diffuse * wl.z / PI;
-        if (!(light_pdf > 0.0)) return;
-        d3 direction = add(add(mul(tg2, wl.x), mul(bt2, wl.y)), mul(normal, wl.z));
+        /* A direction by the lobe choice light paths sample with, weighed by the BSDF as a
+         * camera arriving along it evaluates it (light_paths.glsl:147-178). */
+        or_surface choosing = lit;
+        or_light_lobes(&choosing);
+        d3 wo_light = or_to_local(&lit, toward_light), wi_light;
+        double light_pdf;
+        uint32_t lobe;
+        if (!or_sample_direction(&choosing, wo_light, u[0], u[1], u[3], &wi_light, &light_pdf, &lobe)) return;
+        d3 direction = or_to_world(&lit, wi_light);
         double side = dot(direction, geometric);
-        if ((side > 0.0) != (wl.z > 0.0)) return;
-        d3 sn = side > 0.0 ? normal : neg(normal), sg = side > 0.0 ? geometric : neg(geometric);
-        d3 st, sb;
-        onb(sn, &st, &sb);
-        d3 wo = v3(dot(direction, st), dot(direction, sb), dot(direction, sn));
-        d3 wi = v3(dot(toward_light, st), dot(toward_light, sb), dot(toward_light, sn));
-        if ((dot(toward_light, sg) > 0.0) != (wi.z > 0.0)) return;
-        double camera_bsdf_pdf = (wo.z > 0.0 && wi.z > 0.0) ? p_diffuse * wi.z / PI : 0.0;
-        spec f = (wo.z > 0.0 && wi.z > 0.0) ? eon(base, rough, wi, wo) : spec_zero();
-        uint32_t kind = ((bounces >> 8) & 0xffu) + 1u;
-        if ((double)kind > r->diffuse_limit || (bounces & 0xffu) >= 255u) return;
-        bounces = (bounces & ~(0xffu << 8)) + (kind << 8) + 1u;
+        if ((side > 0.0) != (wi_light.z > 0.0)) return;
+        or_surface seen = side > 0.0 ? lit : or_turned(&lit);
+        d3 wo = or_to_local(&seen, direction), wi = or_to_local(&seen, toward_light);
+        if ((dot(toward_light, seen.geometric) > 0.0) != (wi.z > 0.0)) return;
+        if (side > 0.0) or_orient_surface(&seen, wo);
+        else or_prepare_surface(&seen, wo, r->materials, (int)r->spectral, lambda);
+        double camera_bsdf_pdf;
+        spec f = or_evaluate_surface(&seen, wi, wo, &camera_bsdf_pdf);
+        uint32_t kind = ((bounces >> (8u * (lobe + 1u))) & 0xffu) + 1u;
+        if ((double)kind > r->limits[lobe] || (bounces & 0xffu) >= 255u) return;
+        bounces = (bounces & ~(0xffu << (8u * (lobe + 1u)))) + (kind << (8u * (lobe + 1u))) + 1u;
         throughput = spec_scale(spec_mul(throughput, f), shading_in * fabs(side) / light_pdf);
         if (total + 1 >= 3) {
             double survive = fmin(0.95, spec_max(r, throughput) * survival);
@@ -1046,21 +960,7 @@ static void trace_light_path(const or_render_desc *r, uint32_t sample, uint32_t 
         }
         if (!(spec_max(r, throughput) > 0.0)) return;
         double last = mis[1] > 0.0 ? camera_bsdf_pdf * back_reach / mis[1] : 0.0;
-        double sample_ratio;
-        if (total == 0) {
-            sample_ratio = 0.0;
-            if (camera_bsdf_pdf > 0.0) {
-                d3 from = offset_origin(p, sg);
-                d3 offset = sub(vertex, from);
-                double rch = len(offset);
-                d3 d = mul(offset, 1.0 / rch);
-                double ch = (1.0 - r->p_distant) * tree_pdf(r, emitter, from, sn);
-                double pdf = (code & 0x80000000u) ? tri_hit_pdf(r, code & 0x7fffffffu, d, rch) : light_hit_pdf(r, code, from, d, rch);
-                sample_ratio = ch * pdf / camera_bsdf_pdf;
-            }
-        } else {
-            sample_ratio = mis[3];
-        }
+        double sample_ratio = total == 0 ? light_sample_ratio(r, emitter, &seen, p, vertex, camera_bsdf_pdf) : mis[3];
         origin = offset_origin(p, side > 0.0 ? geometric : neg(geometric));
         vertex = p;
         dir = direction;

@@ -89,6 +89,9 @@ lib.or_blackbody.argtypes = [C.c_double, C.c_double]
 lib.or_wavelength_pdf.restype = C.c_double
 lib.or_wavelength_pdf.argtypes = [C.c_double]
 lib.or_sample_wavelengths.argtypes = [C.c_double, C.POINTER(C.c_double)]
+lib.or_table_albedo.restype = C.c_double
+lib.or_table_albedo.argtypes = [C.c_double, C.c_double, C.c_double]
+lib.or_albedo_tables.restype = C.POINTER(C.c_double)
 lib.or_pack_lights.restype = C.c_size_t
 lib.or_pack_lights.argtypes = [C.POINTER(OrLight), C.c_size_t, C.c_double, C.POINTER(C.c_float),
                                C.POINTER(C.c_double)]
@@ -274,6 +277,22 @@ def octahedral_decode(packed: int) -> np.ndarray:
     return np.array(out[:])
 
 
+ALBEDO_TABLE_SIZE = 32 * 32 + 32 + 32 * 32 * 16
+
+
+def table_albedo(mu: float, roughness: float, eta: float) -> float:
+    """One node of the albedo tables (tables.comp:21-36): the mean of F G2 / G1 over a
+    32 x 32 grid of visible normals at view cosine mu; eta <= 0 for F = 1."""
+    return lib.or_table_albedo(mu, roughness, eta)
+
+
+def albedo_tables() -> np.ndarray:
+    """The whole table (E_ggx 32 x 32, its average over mu, E_dielectric 16 x 32 x 32),
+    laid out as the kernels read it (microfacet.glsl:67-74)."""
+    ptr = lib.or_albedo_tables()
+    return np.ctypeslib.as_array(ptr, shape=(ALBEDO_TABLE_SIZE,)).copy()
+
+
 def material_standard() -> OrMaterial:
     m = OrMaterial()
     lib.or_material_standard(C.byref(m))
@@ -352,19 +371,19 @@ class RenderDesc(C.Structure):
                 ("cmf_integrals", C.c_double * 3), ("frame", C.c_float * 16), ("lens_radius", C.c_double),
                 ("focus_distance", C.c_double), ("forward", C.c_double * 3), ("width", C.c_uint32),
                 ("height", C.c_uint32), ("max_bounces", C.c_uint32), ("spectral", C.c_uint32), ("seed", C.c_uint32),
-                ("diffuse_limit", C.c_double), ("clamp", C.c_double), ("light_paths", C.c_uint32),
+                ("limits", C.c_double * 3), ("clamp", C.c_double), ("light_paths", C.c_uint32),
                 ("light_band", C.c_uint32), ("pixel_area_inv", C.c_double)]
 
 
 def render(arrays: dict, lights, library, frame, samples: int, max_bounces: int, spectral: bool, seed: int = 1,
-           background=(0.0, 0.0, 0.0), clamp: float = 0.0, diffuse_limit: float = 1024.0, threads: int = 0,
+           background=(0.0, 0.0, 0.0), clamp: float = 0.0, limits=(1024.0, 1024.0, 1024.0), threads: int = 0,
            light_tracing: float = 0.0, pool: int = 0):
     """The f64 estimator over a compiled scene's arrays (leaf order), the scene's lights
     (luce_render_b200.Light), the material library (default first, OrMaterial or
     luce_render_b200.OpenPbr) and a luce_render_b200.Frame. Returns (mean, variance),
     each height x width x 3 (ACEScg); with light tracing, of each sample's image (camera
     values plus that sample's light paths' splats)."""
-    job = RenderJob(arrays, lights, library, frame, max_bounces, spectral, seed, background, clamp, diffuse_limit,
+    job = RenderJob(arrays, lights, library, frame, max_bounces, spectral, seed, background, clamp, limits,
                     light_tracing, pool)
     n = frame.width * frame.height
     if job.light_paths:
@@ -390,10 +409,10 @@ class RenderJob:
     """A prepared f64 render: the loaded records built once, then any pixel range."""
 
     def __init__(self, arrays: dict, lights, library, frame, max_bounces: int, spectral: bool, seed: int = 1,
-                 background=(0.0, 0.0, 0.0), clamp: float = 0.0, diffuse_limit: float = 1024.0,
+                 background=(0.0, 0.0, 0.0), clamp: float = 0.0, limits=(1024.0, 1024.0, 1024.0),
                  light_tracing: float = 0.0, pool: int = 0):
         self.desc, self.keep = _render_desc(arrays, lights, library, frame, max_bounces, spectral, seed, background,
-                                            clamp, diffuse_limit)
+                                            clamp, limits)
         count, band = light_paths(light_tracing, frame.width * frame.height, pool, bool(frame.orthographic),
                                   self.desc.emitter_count)
         self.light_paths = count
@@ -423,7 +442,7 @@ class RenderJob:
         return mean.reshape(-1, 3), var.reshape(-1, 3), (int(rays[0]), int(rays[1]))
 
 
-def _render_desc(arrays, lights, library, frame, max_bounces, spectral, seed, background, clamp, diffuse_limit):
+def _render_desc(arrays, lights, library, frame, max_bounces, spectral, seed, background, clamp, limits):
     positions = np.ascontiguousarray(arrays["positions"], np.float32).reshape(-1)
     indices = np.ascontiguousarray(arrays["indices"], np.uint32).reshape(-1)
     shading = np.ascontiguousarray(arrays["shading"], np.uint32).reshape(-1)
@@ -473,6 +492,6 @@ def _render_desc(arrays, lights, library, frame, max_bounces, spectral, seed, ba
     r.max_bounces = max_bounces
     r.spectral = 1 if spectral else 0
     r.seed = seed
-    r.diffuse_limit = diffuse_limit
+    r.limits[:] = [float(x) for x in limits]
     r.clamp = clamp
     return r, keep

@@ -35,7 +35,7 @@ typedef struct {
     float frame[16];
     double lens_radius, focus_distance, forward[3];
     uint32_t width, height, max_bounces, spectral, seed;
-    double diffuse_limit, clamp;
+    double limits[3], clamp; /* the most diffuse, glossy and transmission bounces */
     /* Light tracing (connect.glsl): light paths a sample (0: none), the band they follow
      * (their sampler numbers are 0x80000000 | (band + i)), 1 / a pixel's area at unit
      * distance. */

@@ -1,6 +1,6 @@
 """Render cases shared by the batch and server tests: (compiled scene, settings) pairs of
-uneven sizes, spectral and RGB, depths 2 to 8, one with light tracing, and the image a
-Renderer makes of each."""
+uneven sizes, spectral and RGB, depths 2 to 8, Lambertian and glossy, with and without
+light tracing, and the image a Renderer makes of each."""
 import luce_render_b200 as lr
 from luce_render_b200 import scenes, testscenes
 
@@ -39,6 +39,13 @@ def cases():
     traced = settings(40, 32, 3, 4, False, seed=13)
     traced.light_tracing = 0.5
     out.append((sc, traced))
+    # Glossy: coat, glass, gold and rough plastic, alone and with light tracing.
+    meshes, cams, lights, mats = scenes.glossy_cornell(2)
+    sc = lr.compile_scene(meshes, cams, lights, mats)
+    out.append((sc, settings(36, 28, 3, 6, False, seed=17)))
+    glossy_traced = settings(28, 24, 2, 5, True, seed=19)
+    glossy_traced.light_tracing = 0.5
+    out.append((sc, glossy_traced))
     return out
 
 
