@@ -414,7 +414,34 @@ __device__ __forceinline__ float emitter_area_pdf(const Member &m, uint32_t emit
     } else {
         area = light_at(m.lights, code, 3).w;
     }
-    return area > 0.0f ? emitter_power_pdf(m.tree, emitter) / area : 0.0f;
+    // Emitters of the tree share light paths with lights from afar.
+    const float finite = 1.0f - m.k->emit_share;
+    return area > 0.0f ? finite * emitter_power_pdf(m.tree, emitter) / area : 0.0f;
+}
+
+// ---- Light paths from afar (lights.glsl:283-308) ----------------------------------------
+
+// A light path's emitter code for one from distant light `light` (common.glsl:178).
+constexpr uint32_t kAfarEmitter = 0x40000000u;
+
+__device__ __forceinline__ bool emits_from_afar(const float4 *lights, uint32_t light) {
+    return light_type(lights, light) == kLightDistant && light_at(lights, light, 2).w < 1.0f - 1e-7f;
+}
+
+// The chance a light path leaves distant light `light` along -w (w toward the light).
+__device__ __forceinline__ float afar_emission_pdf(const Member &m, uint32_t light, float3 w) {
+    return m.k->emit_share * light_at(m.lights, light, 6).y *
+           light_hit_pdf(m.lights, light, make_float3(0.0f, 0.0f, 0.0f), w, kInfinity);
+}
+
+// The area density of a light path's first surface p (|cos| c there to w) past the disk
+// the path started on: zero outside the disk's shadow.
+__device__ __forceinline__ float afar_first_density(const Constants &k, float3 p, float3 w, float c) {
+    const float radius = k.emit_radius;
+    const float3 offset = p - k.emit_center;
+    const float3 across = offset - w * dot(offset, w);
+    if (dot(across, across) > radius * radius) return 0.0f;
+    return c / (kPi * radius * radius);
 }
 
 __device__ __forceinline__ float emission_direction_pdf(const Member &m, uint32_t emitter, float c) {
@@ -468,11 +495,25 @@ __device__ __forceinline__ float light_sample_ratio(const Member &m, const Const
     return chance * pdf / bsdf_pdf;
 }
 
-// light_emit.comp:55-136 for an emitter of the light tree (no light paths start from afar
-// at the Lambertian settings): light path `path` of segment `sg`, its sampler number
-// 0x80000000 | (band + its index), from an emitter chosen by power, a point on it uniform
-// by area, a cosine-weighted direction (either side of an emissive triangle). A path
-// that cannot start gets a ray that reaches nothing.
+// light_sample_ratio (light_paths.glsl:15-29) for any light path: one from afar (its
+// emitter code kAfarEmitter | light, arriving along -toward) takes the light sample a
+// camera path would toward that light's direction.
+__device__ __forceinline__ float light_sample_ratio(const Member &m, const Constants &k, uint32_t emitter, float3 sn,
+                                                    float3 sg, float3 p, float3 x0, float3 toward, float bsdf_pdf) {
+    if (!(bsdf_pdf > 0.0f)) return 0.0f;
+    if (emitter & kAfarEmitter) {
+        const uint32_t light = emitter & ~kAfarEmitter;
+        const float select = k.p_distant * light_at(m.lights, light, 6).y;
+        return select * light_hit_pdf(m.lights, light, offset_origin(p, sg), toward, kInfinity) / bsdf_pdf;
+    }
+    return light_sample_ratio(m, k, emitter, sn, sg, p, x0, bsdf_pdf);
+}
+
+// light_emit.comp:21-130: light path `path` of segment `sg`, its sampler number
+// 0x80000000 | (band + its index), from a distant light with a size (by its share of
+// light paths) on a disk facing it, or from an emitter of the light tree chosen by power,
+// a point on it uniform by area, a cosine-weighted direction (either side of an emissive
+// triangle). A path that cannot start gets a ray that reaches nothing.
 template <bool kSpectral>
 __device__ __forceinline__ void light_emit(const Wave &w, const Member &m, const Segment &sg, uint32_t si, uint32_t path) {
     const uint32_t id = 0x80000000u | (m.light_band + sg.first_pixel + (path - sg.path_base));
@@ -486,9 +527,40 @@ __device__ __forceinline__ void light_emit(const Wave &w, const Member &m, const
         w.ray_o[0][path] = make_float4(0.0f, 0.0f, 0.0f, tag);
         w.ray_d[0][path] = make_float4(0.0f, 0.0f, 1.0f, 0.0f);
     };
+    // From afar: a direction by the light's distribution, a point on the disk facing it
+    // about the casters' centre, toward the scene.
+    const float afar = m.k->emit_share;
+    if (u_pick.y < afar) {
+        float share;
+        const uint32_t light = pick_distant(m.lights, m.light_count, u_pick.y / afar, share);
+        if (light == kNone || share <= 0.0f || !emits_from_afar(m.lights, light)) return dead();
+        LightSample s;
+        if (!sample_light(m.lights, light, make_float3(0.0f, 0.0f, 0.0f), make_float2(u_point.x, u_point.y), s)) return dead();
+        const float3 toward = s.direction;
+        const float radius = m.k->emit_radius;
+        float3 t, b;
+        basis(toward, t, b);
+        const float2 disk = concentric(make_float2(u_point.z, u_point.w)) * radius;
+        const float3 start = m.k->emit_center + toward * (2.0f * radius) + t * disk.x + b * disk.y;
+        const float chance = afar * share * s.pdf;
+        const float4 carried = light_radiance<kSpectral>(m.lights, light, lambda) * (kPi * radius * radius / chance);
+        const float most = spec_max<kSpectral>(carried);
+        if (!(most > 0.0f)) return dead();
+        // The light "point" is a direction: its density is the chance, and the camera's
+        // density of it is its BSDF pdf alone (back_reach 1).
+        w.path[path] = make_uint4(kAfarEmitter | light, 0u, 0u, 0u);
+        w.throughput[path] = carried;
+        if (kSpectral) w.lambda[path] = lambda;
+        w.vertex[path] = make_float4(start.x, start.y, start.z, 1.0f / most);
+        w.mis[path] = make_float4(1.0f, chance, 1.0f, -1.0f);
+        w.ray_o[0][path] = make_float4(start.x, start.y, start.z, tag);
+        w.ray_d[0][path] = make_float4(-toward.x, -toward.y, -toward.z, kInfinity);
+        return;
+    }
     uint32_t emitter;
     float chance;
-    if (!emitter_by_power(m.tree, u_pick.y / fmaxf(1e-7f, 1.0f), emitter, chance)) return dead();
+    if (!emitter_by_power(m.tree, (u_pick.y - afar) / fmaxf(1e-7f, 1.0f - afar), emitter, chance)) return dead();
+    chance *= 1.0f - afar;
     const uint32_t code = __ldg(&m.tree.records[emitter]).x;
     float3 q, n;
     float4 radiance;
@@ -604,19 +676,21 @@ __global__ void __launch_bounds__(kShadeBlock) camera_kernel(Wave w) {
 
 // One light sample at p (shade_surface.comp:167-197): a distant light by power, or an
 // emitter of the light tree by importance at `from` and `normal`. Returns the chance the
-// sample was taken with, 0 when none was; `emitter` is the tree's emitter (kNone for a
-// distant light).
+// sample was taken with, 0 when none was; `emitter` is the tree's emitter and `afar` the
+// distant light (kNone for the other kind).
 template <bool kSpectral>
 __device__ __forceinline__ float choose_light(const Member &m, const Constants &k, float4 u_light, float3 p, float3 from,
                                               float3 normal, float4 lambda, LightSample &s, float4 &emitted,
-                                              uint32_t &emitter) {
+                                              uint32_t &emitter, uint32_t &afar) {
     const float4 *lights = m.lights;
     emitted = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
     emitter = kNone;
+    afar = kNone;
     if (u_light.x < k.p_distant) {
         float share;
         const uint32_t light = pick_distant(lights, m.light_count, u_light.x / k.p_distant, share);
         if (light != kNone && share > 0.0f && sample_light(lights, light, p, make_float2(u_light.y, u_light.z), s)) {
+            afar = light;
             emitted = light_radiance<kSpectral>(lights, light, lambda);
             return k.p_distant * share;
         }
@@ -647,15 +721,17 @@ __device__ __forceinline__ float rgb_luminance(float3 c) {
     return c.x * 0.2722287168f + c.y * 0.6740817658f + c.z * 0.0536895174f;
 }
 
-// A surface hit of a member with glossy materials (shade_surface.comp:80-312, every
-// OpenPBR lobe): emission, then one light sample and one BSDF sample of the layered
-// surface, on either side of it when it transmits. Out of line, so that the Lambertian
-// members' shading keeps its registers, and compiled once whatever the pass's variant:
-// the compiler fuses multiply-adds by the code around them, so one body keeps a member's
+// A queue entry of a member with glossy materials (shade_miss.comp:12-51,
+// shade_surface.comp:48-312, every OpenPBR lobe): a miss, a light hit, or a surface's
+// emission, one light sample and one BSDF sample of the layered surface, on either side
+// of it when it transmits; with light tracing, the techniques weigh against light paths
+// from the tree's emitters and from afar. Out of line, so that the Lambertian members'
+// shading keeps its registers, and compiled once whatever the pass's variant: the
+// compiler fuses multiply-adds by the code around them, so one body keeps a member's
 // image the same bits alone and in any mix.
 template <bool kSpectral>
-__device__ __noinline__ void shade_surface_glossy(const Wave &w, const Member &m, uint32_t sample, uint32_t round,
-                                                  uint32_t i, float4 ro, ShadeOut &out) {
+__device__ __noinline__ void shade_glossy(const Wave &w, const Member &m, uint32_t sample, uint32_t round, uint32_t i,
+                                          float4 ro, ShadeOut &out) {
     const Constants &k = *m.k;
     const uint32_t q = round & 1u;
     const float4 rd = w.ray_d[q][i], hit = w.hits[q][i];
@@ -671,8 +747,56 @@ __device__ __noinline__ void shade_surface_glossy(const Wave &w, const Member &m
     const float4 mis = tracing ? w.mis[path] : make_float4(0.0f, 0.0f, 0.0f, 0.0f);
     const float4 vertex_row = w.vertex[path];
     const float3 vertex = xyz(vertex_row);
+    const float4 *lights = m.lights;
+    const uint32_t what = __float_as_uint(hit.y);
 
-    const uint32_t slot = __float_as_uint(hit.y);
+    if (what == kNone) {
+        float4 r = spec_of<kSpectral>(k.background_fit, k.background_rgb, lambda);
+        for (uint32_t light = 0; light < m.light_count; light++) {
+            if (light_type(lights, light) < kLightDistant) continue;
+            const float cos_half = light_at(lights, light, 2).w;
+            if (cos_half >= 1.0f - 1e-7f || dot(dir, -xyz(light_at(lights, light, 3))) < cos_half) continue;
+            float weight = 1.0f;
+            if (total == 0u) {
+                if (!light_visible(lights, light)) continue;
+            } else if (ray_pdf > 0.0f) {
+                // With light tracing, paths from this light's disk weigh in too.
+                float traced = 0.0f;
+                if (tracing && emits_from_afar(lights, light) && mis.y > 0.0f)
+                    traced = mis.x * (afar_first_density(k, vertex, dir, mis.z) / mis.y) *
+                             (afar_emission_pdf(m, light, dir) / ray_pdf);
+                const float select = k.p_distant * light_at(lights, light, 6).y;
+                weight = mis_weight(light_hit_pdf(lights, light, make_float3(0.0f, 0.0f, 0.0f), dir, kInfinity) * select / ray_pdf,
+                                    traced);
+            }
+            r = r + light_radiance<kSpectral>(lights, light, lambda) * weight;
+        }
+        float4 contribution = throughput * r;
+        const float largest = spec_max<kSpectral>(contribution);
+        if (total > 0u && k.clamp_indirect > 0.0f && largest > k.clamp_indirect)
+            contribution = contribution * (k.clamp_indirect / largest);
+        w.radiance[path] = radiance + contribution;
+        return;
+    }
+    if (what & kLightHit) {
+        const uint32_t light = what & ~kLightHit;
+        float weight = 1.0f;
+        if (total == 0u) {
+            if (!light_visible(lights, light)) return;
+        } else if (ray_pdf > 0.0f) {
+            const uint32_t emitter = (uint32_t)light_at(lights, light, 6).w;
+            const float reach = length(vertex - (origin + hit.x * dir));
+            const float chance = (1.0f - k.p_distant) * tree_pdf(m.tree, emitter, vertex, octahedral_decode(pu.z));
+            const float traced =
+                tracing ? camera_hit_ratio(m, mis, emitter, light_cos(lights, light, vertex, dir, reach), reach, ray_pdf) : 0.0f;
+            weight = mis_weight(light_hit_pdf(lights, light, vertex, dir, reach) * chance / ray_pdf, traced);
+        }
+        w.radiance[path] = radiance + clamped<kSpectral>(throughput * light_radiance<kSpectral>(lights, light, lambda) * weight,
+                                                          total, k.clamp_indirect);
+        return;
+    }
+
+    const uint32_t slot = what;
     const float3 p0 = position_of(m, m.scene.indices[slot * 3]);
     float3 geometric = normalize(cross(position_of(m, m.scene.indices[slot * 3 + 1]) - p0,
                                        position_of(m, m.scene.indices[slot * 3 + 2]) - p0));
@@ -713,8 +837,8 @@ __device__ __noinline__ void shade_surface_glossy(const Wave &w, const Member &m
     const float4 u_light = sample4(k.seed, pixel, sample, group_light(total));
     LightSample s;
     float4 emitted;
-    uint32_t nee_emitter;
-    const float chance = choose_light<kSpectral>(m, k, u_light, p, from, normal, lambda, s, emitted, nee_emitter);
+    uint32_t nee_emitter, afar;
+    const float chance = choose_light<kSpectral>(m, k, u_light, p, from, normal, lambda, s, emitted, nee_emitter, afar);
     if (chance > 0.0f) {
         const float side = dot(s.direction, geometric);
         const float3 wi = to_local(surface, s.direction);
@@ -730,6 +854,13 @@ __device__ __noinline__ void shade_surface_glossy(const Wave &w, const Member &m
                         total == 0u ? 1.0f : light_sampler_pdf(surface, s.direction, -dir, m.materials) * back_reach / mis.y;
                     const float at_vertex = emission_direction_pdf(m, nee_emitter, s.cos_light) * fabsf(side) / d2 / density;
                     const float at_light = emitter_area_pdf(m, nee_emitter) / (bsdf_pdf * s.cos_light / d2);
+                    traced = mis.x * at_last * at_vertex * at_light;
+                }
+                if (tracing && afar != kNone && emits_from_afar(lights, afar) && density > 0.0f) {
+                    const float at_last =
+                        total == 0u ? 1.0f : light_sampler_pdf(surface, s.direction, -dir, m.materials) * back_reach / mis.y;
+                    const float at_vertex = afar_first_density(k, p, s.direction, fabsf(side)) / density;
+                    const float at_light = afar_emission_pdf(m, afar, s.direction) / bsdf_pdf;
                     traced = mis.x * at_last * at_vertex * at_light;
                 }
                 const float weight = s.delta ? 1.0f : mis_weight(bsdf_pdf / light_pdf, traced * bsdf_pdf / light_pdf);
@@ -788,6 +919,7 @@ __device__ __noinline__ void shade_surface_glossy(const Wave &w, const Member &m
 template <bool kSpectral, bool kTracing, bool kGlossy>
 __device__ __forceinline__ void shade_one(const Wave &w, const Member &m, uint32_t sample, uint32_t round, uint32_t i,
                                           float4 ro, ShadeOut &out) {
+    if (kGlossy && m.glossy) return shade_glossy<kSpectral>(w, m, sample, round, i, ro, out);
     const Constants &k = *m.k;
     const uint32_t q = round & 1u;
     const float4 rd = w.ray_d[q][i], hit = w.hits[q][i];
@@ -851,7 +983,6 @@ __device__ __forceinline__ void shade_one(const Wave &w, const Member &m, uint32
     }
 
     // A surface.
-    if (kGlossy && m.glossy) return shade_surface_glossy<kSpectral>(w, m, sample, round, i, ro, out);
     const uint32_t slot = what;
     const float3 p0 = position_of(m, m.scene.indices[slot * 3]);
     float3 geometric = normalize(cross(position_of(m, m.scene.indices[slot * 3 + 1]) - p0,
@@ -1185,8 +1316,15 @@ __device__ __noinline__ void shade_light_glossy(const Wave &w, const Member &m, 
     const float3 x_last = xyz(vertex_row);
     const float reach = length(x_last - p);
     const float cos_in = fabsf(dot(dir, geometric));
-    const float density = ray_pdf * cos_in / (reach * reach);
-    const float back_reach = mis.z / (reach * reach);
+    float density = ray_pdf * cos_in / (reach * reach);
+    float back_reach = mis.z / (reach * reach);
+    // The first surface of a path from afar: its density on the disk's shadow, and the
+    // light's "point" is a direction (no distance to convert).
+    if (total == 0u && (emitter & kAfarEmitter)) {
+        density = afar_first_density(k, p, -dir, cos_in);
+        back_reach = 1.0f;
+        if (!(density > 0.0f)) return;
+    }
     const float cos_shading_in = dot(toward_light, normal);
     if (cos_shading_in <= 0.0f || cos_in < 1e-6f) return;
     const float shading_in = cos_shading_in / cos_in;
@@ -1208,7 +1346,7 @@ __device__ __noinline__ void shade_light_glossy(const Wave &w, const Member &m, 
                 const float last = mis.y > 0.0f ? camera_bsdf_pdf * back_reach / mis.y : 0.0f;
                 const float ratio = mis.x * last * camera_density / density;
                 const float sample_ratio = total == 0u ? light_sample_ratio(m, k, emitter, seen.normal, seen.geometric, p, x_last,
-                                                                            camera_bsdf_pdf)
+                                                                            toward_light, camera_bsdf_pdf)
                                                        : fmaxf(mis.w, 0.0f);
                 const float weight = mis_weight(ratio / L, ratio * sample_ratio / L);
                 const float margin = 4e-4f * fmaxf(1.0f, fmaxf(fabsf(p.x), fmaxf(fabsf(p.y), fabsf(p.z))));
@@ -1254,7 +1392,8 @@ __device__ __noinline__ void shade_light_glossy(const Wave &w, const Member &m, 
     if (!(spec_max<kSpectral>(throughput) > 0.0f)) return;
     const float last = mis.y > 0.0f ? camera_bsdf_pdf * back_reach / mis.y : 0.0f;
     const float sample_ratio =
-        total == 0u ? light_sample_ratio(m, k, emitter, seen.normal, seen.geometric, p, x_last, camera_bsdf_pdf) : mis.w;
+        total == 0u ? light_sample_ratio(m, k, emitter, seen.normal, seen.geometric, p, x_last, toward_light, camera_bsdf_pdf)
+                    : mis.w;
     const float3 next = offset_origin(p, side > 0.0f ? geometric : -geometric);
     w.path[path] = make_uint4(emitter, next_bounces, 0u, __float_as_uint(light_pdf));
     w.throughput[path] = throughput;
@@ -1802,19 +1941,19 @@ void validate(const lr_settings &s, const lr_frame &f) {
 
 // Loaded.light_paths (loading.lucb:163-168): light tracing's share of a view's pixels (at
 // least one), at most a band's (the pool setting, or every pixel when fewer), and the band
-// their sampler numbers follow. None for an orthographic camera or a scene without
-// emitters of the light tree (loading.lucb:149): no light paths start from afar, since at
-// the Lambertian settings nothing casts caustics (loading.lucb:127-146).
+// their sampler numbers follow. None for an orthographic camera, or a scene with neither
+// emitters of the light tree nor light paths from afar (loading.lucb:149).
 struct LightPaths {
     uint32_t count = 0, band = 0;
     double pixel_area_inv = 0.0;
 };
 
-LightPaths light_paths_of(const lr_settings &settings, const lr_frame &frame, uint64_t pixels, size_t emitters) {
+LightPaths light_paths_of(const lr_settings &settings, const lr_frame &frame, uint64_t pixels, size_t emitters,
+                          bool afar) {
     LightPaths out;
     const uint64_t pool = settings.pool ? settings.pool : kDefaultPool;
     out.band = (uint32_t)std::min<uint64_t>(pool, pixels);
-    if (!(settings.light_tracing > 0.0) || frame.orthographic || emitters == 0) return out;
+    if (!(settings.light_tracing > 0.0) || frame.orthographic || (emitters == 0 && !afar)) return out;
     const double wanted = std::max(1.0, std::floor(settings.light_tracing * (double)pixels + 0.5));
     out.count = (uint32_t)std::min<double>(wanted, (double)out.band);
     const double du = std::sqrt(frame.du[0] * frame.du[0] + frame.du[1] * frame.du[1] + frame.du[2] * frame.du[2]);
@@ -1845,7 +1984,8 @@ uint32_t member_add(WaveHost *h, const lr_gpu_scene *gs, lr_gpu_scene *owned, co
     if (index == h->capacity) fail(LR_LIMIT, "the wave holds " + std::to_string(h->capacity) + " members");
     const Loaded L = load(*scene, settings);
     const uint64_t pixels = (uint64_t)frame.width * frame.height;
-    const LightPaths traced = light_paths_of(settings, frame, pixels, L.tree.emitter_count);
+    const double emit_share = frame.orthographic ? 0.0 : L.emit_share;
+    const LightPaths traced = light_paths_of(settings, frame, pixels, L.tree.emitter_count, emit_share > 0.0);
     Constants k{};
     for (int i = 0; i < 9; i++) k.film[i] = (float)L.film.m[i];
     k.cmf_integrals[0] = (float)L.cmf_integrals.x;
@@ -1863,6 +2003,9 @@ uint32_t member_add(WaveHost *h, const lr_gpu_scene *gs, lr_gpu_scene *owned, co
     k.light_count = (uint32_t)L.lights.count;
     k.tree_nodes = (uint32_t)L.tree.node_count;
     k.seed = settings.seed;
+    k.emit_share = (float)emit_share;
+    k.emit_radius = (float)L.emit_radius;
+    k.emit_center = make_float3((float)L.emit_center.x, (float)L.emit_center.y, (float)L.emit_center.z);
 
     Layout lay;
     const size_t p_lights = lay.add(L.lights.rows.data(), L.lights.rows.size() * 4);
@@ -2313,7 +2456,7 @@ void create(lr_context *ctx, const lr_scene *scene, const lr_settings &settings,
     r->bands = (uint32_t)((pixels + band - 1) / band);
     // A pass holds a band and, in a sample's first, its light paths (integrator.lucb:419-423);
     // room for them at most, until the scene says whether it has emitters.
-    const uint64_t most_lights = light_paths_of(settings, frame, pixels, 1).count;
+    const uint64_t most_lights = light_paths_of(settings, frame, pixels, 1, false).count;
     lr_gpu_scene *gs = nullptr;
     int status = lr_gpu_scene_upload(ctx, scene, &gs);
     if (status != LR_OK) fail(status, lr_last_error());

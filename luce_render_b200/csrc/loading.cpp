@@ -333,6 +333,41 @@ double scene_radius(const Scene &scene) {
     return std::max(1.0, 0.5 * d.length());
 }
 
+// casts_caustics (loading.lucb:215-219): it refracts, or reflects sharply enough (metal,
+// glossy specular or a clear coat) to focus light.
+bool casts_caustics(const lr_openpbr &m) {
+    if (m.transmission_weight > 0.0) return true;
+    if (m.base_metalness > 0.0 && m.specular_roughness < 0.3) return true;
+    if (m.coat_weight > 0.0 && m.coat_roughness < 0.3) return true;
+    return m.specular_weight > 0.0 && m.specular_roughness < 0.1;
+}
+
+namespace {
+
+// caster_bounds (loading.lucb:224-241): the sphere around the triangles that cast
+// caustics (centre, radius at least 1e-3), or false when none does.
+bool caster_bounds(const Scene &scene, const std::vector<lr_openpbr> &library, V3 &center, double &reach) {
+    V3 lo(1e30, 1e30, 1e30), hi(-1e30, -1e30, -1e30);
+    bool any = false;
+    for (size_t t = 0; t < scene.triangle_count(); t++) {
+        const size_t material = scene.shading[t * 4 + 3];
+        if (material >= library.size() || !casts_caustics(library[material])) continue;
+        for (int corner = 0; corner < 3; corner++) {
+            const size_t at = (size_t)scene.indices[t * 3 + corner] * 3;
+            const V3 point(scene.positions[at], scene.positions[at + 1], scene.positions[at + 2]);
+            lo = V3(std::min(lo.x, point.x), std::min(lo.y, point.y), std::min(lo.z, point.z));
+            hi = V3(std::max(hi.x, point.x), std::max(hi.y, point.y), std::max(hi.z, point.z));
+        }
+        any = true;
+    }
+    if (!any) return false;
+    center = (lo + hi) * 0.5;
+    reach = std::max(1e-3, 0.5 * (hi - lo).length());
+    return true;
+}
+
+}  // namespace
+
 Loaded load(const Scene &scene, const lr_settings &settings) {
     Loaded L;
     L.library.push_back(settings.material);
@@ -346,6 +381,24 @@ Loaded load(const Scene &scene, const lr_settings &settings) {
     L.lights = pack_lights(scene.lights, L.radius);
     L.tree = build_light_tree(scene, L.lights, L.library);
     for (size_t i = 0; i < L.library.size(); i++) pack_material(L.library[i], -1.0f, L.materials);
+    // Distant lights with a size start light paths too, on a disk around what casts
+    // caustics, sharing them with the tree's emitters by power (loading.lucb:127-146);
+    // looked for only when such a light would aim light paths at it. An orthographic
+    // view takes no light paths at all (the member drops the share).
+    bool sized = false;
+    for (size_t i = 0; i < L.lights.count; i++)
+        sized = sized || (L.lights.rows[i * 28 + 3] == 3.0f && L.lights.rows[i * 28 + 11] < 1.0f - 1e-7f);
+    if (sized && settings.light_tracing > 0.0) {
+        V3 center;
+        double reach = 1.0;
+        if (caster_bounds(scene, L.library, center, reach)) {
+            const double afar_power = L.lights.distant_power * (reach / L.radius) * (reach / L.radius);
+            const double both = afar_power + L.tree.energy;
+            L.emit_share = both > 0.0 ? afar_power / both : 0.0;
+            L.emit_radius = reach;
+            L.emit_center = center;
+        }
+    }
     const double total = L.lights.distant_power + L.tree.energy;
     L.p_distant = L.tree.emitter_count > 0 ? (total > 0.0 ? L.lights.distant_power / total : 0.0)
                                            : (L.lights.distant_power > 0.0 ? 1.0 : 0.0);

@@ -31,6 +31,11 @@ struct Loaded {
     std::vector<float> materials;     // 64 floats per material
     double radius = 1.0, p_distant = 0.0;
     bool glossy = false;              // a used material has more than EON diffuse
+    // Light paths from afar (lights.glsl:283-308): the chance a light path starts at a
+    // distant light with a size, and the disk it starts on (centre, radius) around what
+    // casts caustics; share 0 when none do.
+    double emit_share = 0.0, emit_radius = 1.0;
+    V3 emit_center;
     double background_fit[4] = {0, 0, 0, 0};
     M3 film{};
     V3 cmf_integrals;
@@ -41,5 +46,6 @@ LightTree build_light_tree(const Scene &scene, const LightRecords &lights, const
 void pack_material(const lr_openpbr &m, float program, std::vector<float> &out);
 double scene_radius(const Scene &scene);
 Loaded load(const Scene &scene, const lr_settings &settings);
+bool casts_caustics(const lr_openpbr &m);
 
 }  // namespace lr

@@ -235,6 +235,10 @@ struct Constants {
     uint32_t light_count;
     uint32_t tree_nodes;
     uint32_t seed;
+    // Light paths from afar (lights.glsl:287-288): their share of light paths, and the
+    // disk they start on, facing the light (radius, centre).
+    float emit_share, emit_radius;
+    float3 emit_center;
 };
 
 template <bool kSpectral>

@@ -348,3 +348,26 @@ def furnace_sphere(level: int = 4):
     p, t, n = icosphere(level, 1.0)
     cam = camera((0.0, 1.0, 4.0), (-math.atan2(1.0, 4.0), 0.0, 0.0), focal_length=50.0, horizontal_aperture=36.0)
     return [MeshData(p, t, normals=n)], [cam]
+
+
+def caustic_scene(sun_angle: float = 8.0, glass_roughness: float = 0.15):
+    """Light paths from afar: an 8 x 8 floor (32 triangles) under a sun of `sun_angle`
+    degrees and a dim sky, holding a glass ball (radius 0.5, the caustic caster), a gold
+    ball and a white cube; no emitters of the light tree, so every light path starts on
+    the disk facing the sun. Returns (meshes, cameras, lights, materials, background);
+    library materials 1..3 are the floor's white, glass and gold."""
+    p, t, f = grid(8.0, 4)
+    meshes = [MeshData(p, t, faces=f, face_count=int(f.max()) + 1, face_materials=[1] * (int(f.max()) + 1))]
+    for radius, at, material in [(0.5, (0.0, 0.5, 0.0), 2), (0.35, (-1.1, 0.35, -0.6), 3)]:
+        sp, st, sn = icosphere(3, radius)
+        meshes.append(MeshData(sp, st, normals=sn, faces=np.zeros(len(st), np.uint32), face_count=1,
+                               face_materials=[material], transform=placement(at)))
+    bp, bt, bf = box_mesh((-0.3, 0.0, -0.3), (0.3, 0.6, 0.3))
+    meshes.append(MeshData(bp, bt, faces=bf, face_count=6, face_materials=[1] * 6,
+                           transform=placement((1.2, 0.0, -0.8), (0.0, 0.4, 0.0))))
+    materials = [openpbr(base_color=(0.8, 0.8, 0.8), specular_weight=0.0),
+                 openpbr(transmission_weight=1.0, specular_roughness=glass_roughness, base_color=(1.0, 1.0, 1.0)),
+                 openpbr(base_color=(1.0, 0.77, 0.34), base_metalness=1.0, specular_roughness=0.25)]
+    lights = [light(LIGHT_DISTANT, rotation=(-0.75, 0.5, 0.0), intensity=3.0, angle=sun_angle)]
+    cams = [camera((0.0, 2.2, 4.0), (-math.atan2(1.8, 4.0), 0.0, 0.0), focal_length=35.0, horizontal_aperture=36.0)]
+    return meshes, cams, lights, materials, (0.05, 0.07, 0.1)

@@ -435,7 +435,27 @@ static double emitter_area_pdf(const or_render_desc *r, uint32_t emitter) {
     } else {
         area = row(r, code, 3)[3];
     }
-    return area > 0.0 ? emitter_power_pdf(r, emitter) / area : 0.0;
+    /* Emitters of the tree share light paths with lights from afar. */
+    return area > 0.0 ? (1.0 - r->emit_share) * emitter_power_pdf(r, emitter) / area : 0.0;
+}
+
+/* ---- light paths from afar (lights.glsl:283-308) --------------------------------------- */
+
+#define AFAR_EMITTER 0x40000000u
+
+static int emits_from_afar(const or_render_desc *r, uint32_t light) {
+    return light_type(r, light) == 3 && row(r, light, 2)[3] < 1.0f - 1e-7f;
+}
+
+static double afar_emission_pdf(const or_render_desc *r, uint32_t light, d3 w) {
+    return r->emit_share * row(r, light, 6)[1] * light_hit_pdf(r, light, v3(0, 0, 0), w, INF);
+}
+
+static double afar_first_density(const or_render_desc *r, d3 p, d3 w, double c) {
+    d3 offset = sub(p, v3(r->emit_center[0], r->emit_center[1], r->emit_center[2]));
+    d3 across = sub(offset, mul(w, dot(offset, w)));
+    if (dot(across, across) > r->emit_radius * r->emit_radius) return 0.0;
+    return c / (PI * r->emit_radius * r->emit_radius);
 }
 
 static double emission_direction_pdf(const or_render_desc *r, uint32_t emitter, double c) {
@@ -571,7 +591,11 @@ static void render_sample(const or_render_desc *r, uint32_t pixel, uint32_t samp
                 if (total == 0) {
                     if (!light_visible(r, l)) continue;
                 } else if (ray_pdf > 0.0) {
-                    weight = mis_weight(light_hit_pdf(r, l, v3(0, 0, 0), dir, INF) * (r->p_distant * row(r, l, 6)[1]) / ray_pdf, 0.0);
+                    /* With light tracing, paths from this light's disk weigh in too. */
+                    double traced = 0.0;
+                    if (tracing && emits_from_afar(r, l) && mis[1] > 0.0)
+                        traced = mis[0] * (afar_first_density(r, vertex, dir, mis[2]) / mis[1]) * (afar_emission_pdf(r, l, dir) / ray_pdf);
+                    weight = mis_weight(light_hit_pdf(r, l, v3(0, 0, 0), dir, INF) * (r->p_distant * row(r, l, 6)[1]) / ray_pdf, traced);
                 }
                 bg = spec_add(bg, spec_scale(light_radiance(r, l, lambda), weight));
             }
@@ -634,11 +658,12 @@ static void render_sample(const or_render_desc *r, uint32_t pixel, uint32_t samp
         spec emitted = spec_zero();
         double chance = 0.0;
         int sampled = 0;
-        uint32_t nee_emitter = NONE;
+        uint32_t nee_emitter = NONE, afar = NONE;
         if (ul[0] < r->p_distant) {
             double share;
             uint32_t l = pick_distant(r, ul[0] / r->p_distant, &share);
             if (l != NONE && share > 0.0 && sample_light(r, l, p, ul[1], ul[2], &s)) {
+                afar = l;
                 chance = r->p_distant * share;
                 emitted = light_radiance(r, l, lambda);
                 sampled = 1;
@@ -696,6 +721,14 @@ static void render_sample(const or_render_desc *r, uint32_t pixel, uint32_t samp
                                                           back_reach / mis[1];
                         double at_vertex = emission_direction_pdf(r, nee_emitter, s.cos_light) * fabs(side) / d2 / density;
                         double at_light = emitter_area_pdf(r, nee_emitter) / (bsdf_pdf * s.cos_light / d2);
+                        traced = mis[0] * at_last * at_vertex * at_light;
+                    }
+                    if (tracing && afar != NONE && emits_from_afar(r, afar) && density > 0.0) {
+                        double at_last = total == 0 ? 1.0
+                                                    : or_light_sampler_pdf(&surface, r->materials, s.direction, neg(dir)) *
+                                                          back_reach / mis[1];
+                        double at_vertex = afar_first_density(r, p, s.direction, fabs(side)) / density;
+                        double at_light = afar_emission_pdf(r, afar, s.direction) / bsdf_pdf;
                         traced = mis[0] * at_last * at_vertex * at_light;
                     }
                     double weight = s.delta ? 1.0 : mis_weight(bsdf_pdf / light_pdf, traced * bsdf_pdf / light_pdf);
@@ -764,9 +797,13 @@ static void render_sample(const or_render_desc *r, uint32_t pixel, uint32_t samp
  * surface `s` faces its side) would take toward the light path's first point x0, over its
  * BSDF pdf toward it. */
 static double light_sample_ratio(const or_render_desc *r, uint32_t emitter, const or_surface *s, d3 p, d3 x0,
-                                 double bsdf_pdf) {
+                                 d3 toward, double bsdf_pdf) {
     if (!(bsdf_pdf > 0.0)) return 0.0;
     d3 from = offset_origin(p, s->geometric);
+    if (emitter & AFAR_EMITTER) {
+        uint32_t l = emitter & ~AFAR_EMITTER;
+        return r->p_distant * row(r, l, 6)[1] * light_hit_pdf(r, l, from, toward, INF) / bsdf_pdf;
+    }
     d3 offset = sub(x0, from);
     double reach = len(offset);
     d3 d = mul(offset, 1.0 / reach);
@@ -790,61 +827,93 @@ static void trace_light_path(const or_render_desc *r, uint32_t sample, uint32_t 
     or_sample4(r->seed, id, sample, 1, u_pick);
     double lambda[4] = {0, 0, 0, 0};
     if (r->spectral) or_sample_wavelengths(u_pick[0], lambda);
-    uint32_t emitter;
-    double chance;
-    if (!emitter_by_power(r, u_pick[1] / fmax(1e-7, 1.0), &emitter, &chance)) return;
-    uint32_t code = r->tree_records[emitter * 4];
-    d3 q, n;
-    spec radiance;
-    double area;
-    int two_sided = 0;
-    if (code & 0x80000000u) {
-        uint32_t t = code & 0x7fffffffu;
-        d3 a = point(r, r->indices[t * 3]), b = point(r, r->indices[t * 3 + 1]), c = point(r, r->indices[t * 3 + 2]);
-        double rr = sqrt(u_point[0]);
-        q = add(add(mul(a, 1.0 - rr), mul(b, rr * (1.0 - u_point[1]))), mul(c, rr * u_point[1]));
-        d3 cr = cross(sub(b, a), sub(c, a));
-        area = 0.5 * len(cr);
-        n = mul(cr, 1.0 / fmax(2.0 * area, 1e-30));
-        if (u_pick[2] < 0.5) n = neg(n);
-        two_sided = 1;
-        uint32_t tm = r->shading[t * 4 + 3];
-        radiance = spec_of(r, material(r, tm, 6), material(r, tm, 7), lambda);
+    d3 origin, vertex, dir;
+    spec throughput;
+    double survival, ray_pdf, mis[4];
+    uint32_t emitter, code = 0;
+    double afar = r->emit_share;
+    if (u_pick[1] < afar) {
+        /* From afar: a direction by the light's distribution, a point on the disk facing it
+         * about the casters' centre, toward the scene (light_emit.comp:31-62). */
+        double share;
+        uint32_t l = pick_distant(r, u_pick[1] / afar, &share);
+        if (l == NONE || share <= 0.0 || !emits_from_afar(r, l)) return;
+        lsample s;
+        if (!sample_light(r, l, v3(0, 0, 0), u_point[0], u_point[1], &s)) return;
+        d3 w = s.direction, t, b;
+        double radius = r->emit_radius, dx, dy;
+        onb(w, &t, &b);
+        concentric(u_point[2], u_point[3], &dx, &dy);
+        d3 start = add(add(add(v3(r->emit_center[0], r->emit_center[1], r->emit_center[2]), mul(w, 2.0 * radius)),
+                           mul(t, dx * radius)), mul(b, dy * radius));
+        double chance = afar * share * s.pdf;
+        throughput = spec_scale(light_radiance(r, l, lambda), PI * radius * radius / chance);
+        double most = spec_max(r, throughput);
+        if (!(most > 0.0)) return;
+        /* The light "point" is a direction: its density is the chance, and the camera's
+         * density of it is its BSDF pdf alone (back_reach 1). */
+        emitter = AFAR_EMITTER | l;
+        origin = start, vertex = start, dir = neg(w);
+        survival = 1.0 / most;
+        ray_pdf = 0.0;
+        mis[0] = 1.0, mis[1] = chance, mis[2] = 1.0, mis[3] = -1.0;
     } else {
-        uint32_t type = light_type(r, code);
-        const float *r0 = row(r, code, 0);
-        if (type == 2) {
-            double rad = row(r, code, 1)[3];
-            double z = 1.0 - 2.0 * u_point[0], sz = sqrt(fmax(0.0, 1.0 - z * z)), phi = 2.0 * PI * u_point[1];
-            n = v3(sz * cos(phi), sz * sin(phi), z);
-            q = add(rv(r0), mul(n, rad));
-            area = 4.0 * PI * rad * rad;
+        double chance;
+        if (!emitter_by_power(r, (u_pick[1] - afar) / fmax(1e-7, 1.0 - afar), &emitter, &chance)) return;
+        chance *= 1.0 - afar;
+        code = r->tree_records[emitter * 4];
+        d3 q, n;
+        spec radiance;
+        double area;
+        int two_sided = 0;
+        if (code & 0x80000000u) {
+            uint32_t t = code & 0x7fffffffu;
+            d3 a = point(r, r->indices[t * 3]), b = point(r, r->indices[t * 3 + 1]), c = point(r, r->indices[t * 3 + 2]);
+            double rr = sqrt(u_point[0]);
+            q = add(add(mul(a, 1.0 - rr), mul(b, rr * (1.0 - u_point[1]))), mul(c, rr * u_point[1]));
+            d3 cr = cross(sub(b, a), sub(c, a));
+            area = 0.5 * len(cr);
+            n = mul(cr, 1.0 / fmax(2.0 * area, 1e-30));
+            if (u_pick[2] < 0.5) n = neg(n);
+            two_sided = 1;
+            uint32_t tm = r->shading[t * 4 + 3];
+            radiance = spec_of(r, material(r, tm, 6), material(r, tm, 7), lambda);
         } else {
-            double ax, ay;
-            if (type == 0) ax = 2.0 * u_point[0] - 1.0, ay = 2.0 * u_point[1] - 1.0;
-            else concentric(u_point[0], u_point[1], &ax, &ay);
-            q = add(add(rv(r0), mul(rv(row(r, code, 1)), ax)), mul(rv(row(r, code, 2)), ay));
-            n = rv(row(r, code, 3));
-            area = row(r, code, 3)[3];
+            uint32_t type = light_type(r, code);
+            const float *r0 = row(r, code, 0);
+            if (type == 2) {
+                double rad = row(r, code, 1)[3];
+                double z = 1.0 - 2.0 * u_point[0], sz = sqrt(fmax(0.0, 1.0 - z * z)), phi = 2.0 * PI * u_point[1];
+                n = v3(sz * cos(phi), sz * sin(phi), z);
+                q = add(rv(r0), mul(n, rad));
+                area = 4.0 * PI * rad * rad;
+            } else {
+                double ax, ay;
+                if (type == 0) ax = 2.0 * u_point[0] - 1.0, ay = 2.0 * u_point[1] - 1.0;
+                else concentric(u_point[0], u_point[1], &ax, &ay);
+                q = add(add(rv(r0), mul(rv(row(r, code, 1)), ax)), mul(rv(row(r, code, 2)), ay));
+                n = rv(row(r, code, 3));
+                area = row(r, code, 3)[3];
+            }
+            radiance = light_radiance(r, code, lambda);
         }
-        radiance = light_radiance(r, code, lambda);
+        if (area <= 0.0) return;
+        double dx, dy;
+        concentric(u_point[2], u_point[3], &dx, &dy);
+        double cos_n = sqrt(fmax(0.0, 1.0 - (dx * dx + dy * dy)));
+        if (cos_n <= 0.0) return;
+        d3 tg, bt;
+        onb(n, &tg, &bt);
+        dir = norm(add(add(mul(tg, dx), mul(bt, dy)), mul(n, cos_n)));
+        double point_pdf = chance / area;
+        ray_pdf = cos_n / (two_sided ? 2.0 * PI : PI);
+        throughput = spec_scale(radiance, cos_n / (point_pdf * ray_pdf));
+        double largest = spec_max(r, throughput);
+        if (!(largest > 0.0)) return;
+        origin = offset_origin(q, n), vertex = q;
+        survival = 1.0 / largest;
+        mis[0] = 1.0, mis[1] = point_pdf, mis[2] = cos_n, mis[3] = -1.0;
     }
-    if (area <= 0.0) return;
-    double dx, dy;
-    concentric(u_point[2], u_point[3], &dx, &dy);
-    double cos_n = sqrt(fmax(0.0, 1.0 - (dx * dx + dy * dy)));
-    if (cos_n <= 0.0) return;
-    d3 tg, bt;
-    onb(n, &tg, &bt);
-    d3 dir = norm(add(add(mul(tg, dx), mul(bt, dy)), mul(n, cos_n)));
-    double point_pdf = chance / area;
-    double ray_pdf = cos_n / (two_sided ? 2.0 * PI : PI);
-    spec throughput = spec_scale(radiance, cos_n / (point_pdf * ray_pdf));
-    double largest = spec_max(r, throughput);
-    if (!(largest > 0.0)) return;
-    d3 origin = offset_origin(q, n), vertex = q;
-    double survival = 1.0 / largest;
-    double mis[4] = {1.0, point_pdf, cos_n, -1.0};
     uint32_t bounces = 0;
     for (uint32_t round = 0; round <= r->max_bounces; round++) {
         uint32_t total = bounces & 0xffu;
@@ -888,6 +957,13 @@ static void trace_light_path(const or_render_desc *r, uint32_t sample, uint32_t 
         double cos_in = fabs(dot(dir, geometric));
         double density = ray_pdf * cos_in / (reach * reach);
         double back_reach = mis[2] / (reach * reach);
+        /* The first surface of a path from afar: its density on the disk's shadow, and the
+         * light's "point" is a direction (no distance to convert). */
+        if (total == 0 && (emitter & AFAR_EMITTER)) {
+            density = afar_first_density(r, p, neg(dir), cos_in);
+            back_reach = 1.0;
+            if (!(density > 0.0)) return;
+        }
         double cos_shading_in = dot(toward_light, normal);
         if (cos_shading_in <= 0.0 || cos_in < 1e-6) return;
         double shading_in = cos_shading_in / cos_in;
@@ -906,7 +982,7 @@ static void trace_light_path(const or_render_desc *r, uint32_t sample, uint32_t 
                 if (spec_max(r, contribution) > 0.0) {
                     double last = mis[1] > 0.0 ? camera_bsdf_pdf * back_reach / mis[1] : 0.0;
                     double ratio = mis[0] * last * camera_density / density;
-                    double sample_ratio = total == 0 ? light_sample_ratio(r, emitter, &seen, p, vertex, camera_bsdf_pdf)
+                    double sample_ratio = total == 0 ? light_sample_ratio(r, emitter, &seen, p, vertex, toward_light, camera_bsdf_pdf)
                                                      : fmax(mis[3], 0.0);
                     double weight = mis_weight(ratio / L, ratio * sample_ratio / L);
                     double margin = 4e-4 * fmax(1.0, fmax(fabs(p.x), fmax(fabs(p.y), fabs(p.z))));
@@ -960,7 +1036,7 @@ static void trace_light_path(const or_render_desc *r, uint32_t sample, uint32_t 
         }
         if (!(spec_max(r, throughput) > 0.0)) return;
         double last = mis[1] > 0.0 ? camera_bsdf_pdf * back_reach / mis[1] : 0.0;
-        double sample_ratio = total == 0 ? light_sample_ratio(r, emitter, &seen, p, vertex, camera_bsdf_pdf) : mis[3];
+        double sample_ratio = total == 0 ? light_sample_ratio(r, emitter, &seen, p, vertex, toward_light, camera_bsdf_pdf) : mis[3];
         origin = offset_origin(p, side > 0.0 ? geometric : neg(geometric));
         vertex = p;
         dir = direction;

@@ -372,7 +372,8 @@ class RenderDesc(C.Structure):
                 ("focus_distance", C.c_double), ("forward", C.c_double * 3), ("width", C.c_uint32),
                 ("height", C.c_uint32), ("max_bounces", C.c_uint32), ("spectral", C.c_uint32), ("seed", C.c_uint32),
                 ("limits", C.c_double * 3), ("clamp", C.c_double), ("light_paths", C.c_uint32),
-                ("light_band", C.c_uint32), ("pixel_area_inv", C.c_double)]
+                ("light_band", C.c_uint32), ("pixel_area_inv", C.c_double), ("emit_share", C.c_double),
+                ("emit_radius", C.c_double), ("emit_center", C.c_double * 3)]
 
 
 def render(arrays: dict, lights, library, frame, samples: int, max_bounces: int, spectral: bool, seed: int = 1,
@@ -393,13 +394,13 @@ def render(arrays: dict, lights, library, frame, samples: int, max_bounces: int,
     return mean.reshape(frame.height, frame.width, 3), var.reshape(frame.height, frame.width, 3)
 
 
-def light_paths(light_tracing: float, pixels: int, pool: int, orthographic: bool, emitters: int):
+def light_paths(light_tracing: float, pixels: int, pool: int, orthographic: bool, emitters: int, afar: bool = False):
     """Loaded.light_paths (loading.lucb:163-168) and the band they follow: light tracing's
     share of the pixels (at least one), at most a band's; none for an orthographic camera
-    or a scene without emitters (no light paths start from afar at the Lambertian
-    settings). Returns (light paths, band)."""
+    or a scene with neither emitters nor light paths from afar. Returns (light paths,
+    band)."""
     band = min(pool if pool > 0 else 2097152, pixels)
-    if light_tracing <= 0.0 or orthographic or emitters == 0:
+    if light_tracing <= 0.0 or orthographic or (emitters == 0 and not afar):
         return 0, band
     wanted = max(1, int(math.floor(light_tracing * pixels + 0.5)))
     return min(wanted, band), band
@@ -412,9 +413,9 @@ class RenderJob:
                  background=(0.0, 0.0, 0.0), clamp: float = 0.0, limits=(1024.0, 1024.0, 1024.0),
                  light_tracing: float = 0.0, pool: int = 0):
         self.desc, self.keep = _render_desc(arrays, lights, library, frame, max_bounces, spectral, seed, background,
-                                            clamp, limits)
+                                            clamp, limits, light_tracing)
         count, band = light_paths(light_tracing, frame.width * frame.height, pool, bool(frame.orthographic),
-                                  self.desc.emitter_count)
+                                  self.desc.emitter_count, self.desc.emit_share > 0.0)
         self.light_paths = count
         self.desc.light_paths, self.desc.light_band = count, band
         area = float(np.linalg.norm(np.array(frame.du)) * np.linalg.norm(np.array(frame.dv)))
@@ -442,7 +443,33 @@ class RenderJob:
         return mean.reshape(-1, 3), var.reshape(-1, 3), (int(rays[0]), int(rays[1]))
 
 
-def _render_desc(arrays, lights, library, frame, max_bounces, spectral, seed, background, clamp, limits):
+def casts_caustics(m) -> bool:
+    """casts_caustics (loading.lucb:215-219): it refracts, or reflects sharply enough."""
+    if m.transmission_weight > 0.0:
+        return True
+    if m.base_metalness > 0.0 and m.specular_roughness < 0.3:
+        return True
+    if m.coat_weight > 0.0 and m.coat_roughness < 0.3:
+        return True
+    return m.specular_weight > 0.0 and m.specular_roughness < 0.1
+
+
+def caster_bounds(positions, indices, shading, materials):
+    """caster_bounds (loading.lucb:224-241): (centre, radius) of the triangles whose
+    material casts caustics, or None."""
+    cast = np.array([casts_caustics(m) for m in materials], bool)
+    mat = np.asarray(shading, np.uint32).reshape(-1, 4)[:, 3]
+    chosen = (mat < len(materials)) & cast[np.minimum(mat, len(materials) - 1)]
+    if not chosen.any():
+        return None
+    corners = np.asarray(indices, np.uint32).reshape(-1, 3)[chosen].reshape(-1)
+    pts = np.asarray(positions, np.float32).reshape(-1, 3)[corners].astype(np.float64)
+    lo, hi = pts.min(0), pts.max(0)
+    return (lo + hi) * 0.5, max(1e-3, 0.5 * float(np.linalg.norm(hi - lo)))
+
+
+def _render_desc(arrays, lights, library, frame, max_bounces, spectral, seed, background, clamp, limits,
+                 light_tracing=0.0):
     positions = np.ascontiguousarray(arrays["positions"], np.float32).reshape(-1)
     indices = np.ascontiguousarray(arrays["indices"], np.uint32).reshape(-1)
     shading = np.ascontiguousarray(arrays["shading"], np.uint32).reshape(-1)
@@ -493,5 +520,18 @@ def _render_desc(arrays, lights, library, frame, max_bounces, spectral, seed, ba
     r.spectral = 1 if spectral else 0
     r.seed = seed
     r.limits[:] = [float(x) for x in limits]
+    # Light paths from afar (loading.lucb:127-146): distant lights with a size share light
+    # paths with the tree's emitters by power, on a disk around what casts caustics.
+    sized = any(row[3] == 3.0 and row[11] < np.float32(1.0) - np.float32(1e-7) for row in rows.reshape(-1, 28))
+    r.emit_share, r.emit_radius = 0.0, 1.0
+    if sized and light_tracing > 0.0 and not frame.orthographic:
+        found = caster_bounds(positions, indices, shading, mats)
+        if found is not None:
+            center, reach = found
+            afar_power = distant_power * (reach / radius) ** 2
+            both = afar_power + tree["energy"]
+            r.emit_share = afar_power / both if both > 0.0 else 0.0
+            r.emit_radius = reach
+            r.emit_center[:] = [float(x) for x in center]
     r.clamp = clamp
     return r, keep

@@ -41,6 +41,9 @@ typedef struct {
      * distance. */
     uint32_t light_paths, light_band;
     double pixel_area_inv;
+    /* Light paths from afar (lights.glsl:283-308): their share of light paths and the disk
+     * they start on, facing the light (radius, centre); share 0 for none. */
+    double emit_share, emit_radius, emit_center[3];
 } or_render_desc;
 
 void or_render(const or_render_desc *r, uint32_t samples, double *mean, double *var, int threads);

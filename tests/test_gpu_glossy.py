@@ -9,7 +9,8 @@ and out of transmissive objects (shaders/openpbr.glsl, microfacet.glsl, tables.c
   glass are white within the reference's 2 %.
 - The f64 oracle's restatement over the same samples, on the benchmark's layout (coat,
   glass, gold, rough plastic): 8x8-block means within 3 sigma, camera paths alone and with
-  light tracing, RGB and spectral.
+  light tracing, RGB and spectral; and a glass ball under a sun, its light paths starting
+  from afar (lights.glsl:283-308).
 """
 import math
 
@@ -134,3 +135,29 @@ def test_glossy_light_tracing_is_unbiased(ctx):
     assert np.all(np.abs(traced - camera) <= 4.0 * np.sqrt(se_traced ** 2 + se_camera ** 2) + 1e-6), (traced, camera)
     # Light paths carry the caustic with less noise than camera paths alone.
     assert se_traced.mean() < se_camera.mean()
+
+
+@pytest.mark.parametrize("spectral", [False, True])
+def test_gpu_matches_f64_oracle_light_paths_from_afar(ctx, spectral):
+    # A sun with a size and a glass ball: light paths start on the disk facing the sun,
+    # camera paths weigh their BSDF rays to the sun and their light samples against them.
+    meshes, cams, lights, mats, background = scenes.caustic_scene()
+    sc = lr.compile_scene(meshes, cams, lights, mats)
+    w, h, spp = 48, 32, 32
+    img = _render(ctx, sc, w, h, spp, 6, spectral, background=background, tracing=0.5)
+    frame = lr.ray_frame(sc.camera(), w, h)
+    job = orc.RenderJob(sc.arrays(), lights, [lr.OpenPbr.lambert()] + mats, frame, 6, spectral, background=background,
+                        light_tracing=0.5)
+    assert job.light_paths > 0 and job.desc.emitter_count == 0
+    mean, var, _ = job.traced(spp)
+    camera_part, _, _ = job.region(spp, 0, 0, w * h)
+    mean, var, camera_part = (x.reshape(h, w, 3) for x in (mean, var, camera_part))
+    gpu = img[..., :3].astype(np.float64)
+    g = _blocks(gpu, 8).mean((1, 3))
+    o = _blocks(mean, 8).mean((1, 3))
+    sem = np.sqrt(_blocks(var, 8).mean((1, 3)) / (64 * spp))
+    assert np.all(np.abs(g - o) <= 3.0 * sem + 1e-6), np.max(np.abs(g - o) / (sem + 1e-12))
+    relative = np.abs(gpu - mean) / np.maximum(np.abs(mean), 1e-3)
+    assert np.mean(relative < 1e-3) >= 0.95, np.mean(relative < 1e-3)
+    # The light paths from afar carry part of the image (the caustic under the ball).
+    assert (mean - camera_part).sum() / mean.sum() > 0.02

@@ -8,7 +8,8 @@
   roughness, a white base under a clear coat and a closed sphere of smooth glass, under a
   white sky, are white within 2 %.
 - Light tracing with glossy lobes leaves the image unbiased: the glossy Cornell box is the
-  same with and without light paths within 3 sigma.
+  same with and without light paths within 3 sigma, and so is a glass ball under a sun
+  whose light paths all start from afar (on the disk facing the sun).
 """
 import math
 
@@ -99,3 +100,27 @@ def test_oracle_glossy_light_tracing_is_unbiased():
     blocks = lambda x: x.reshape(4, 8, 4, 8, 3).mean((1, 3))
     sem = np.sqrt((blocks(va) + blocks(vb)) / (64 * 32))
     assert np.all(np.abs(blocks(a) - blocks(b)) <= 3.5 * sem + 1e-9), np.max(np.abs(blocks(a) - blocks(b)) / sem)
+
+
+def test_oracle_light_paths_from_afar():
+    # A sun with a size over a glass ball (loading.lucb:127-146): light paths start on the
+    # disk facing it (no emitters of the light tree here, so all of them), and the image is
+    # the camera paths' alone within 4 sigma.
+    meshes, cams, lights, mats, background = scenes.caustic_scene()
+    sc = lr.compile_scene(meshes, cams, lights, mats)
+    w, h = 48, 32
+    frame = lr.ray_frame(sc.camera(), w, h)
+    library = [lr.OpenPbr.lambert()] + mats
+    job = orc.RenderJob(sc.arrays(), lights, library, frame, 6, False, background=background, light_tracing=0.5)
+    assert job.light_paths == w * h // 2 and job.desc.emitter_count == 0 and job.desc.emit_share == 1.0
+    # The disk covers the casters: the glass ball of radius 0.5 at (0, 0.5, 0).
+    assert job.desc.emit_radius >= 0.5 * math.sqrt(3.0) - 1e-3
+    a, va = orc.render(sc.arrays(), lights, library, frame, 256, 6, False, background=background, light_tracing=0.5)
+    b, vb = orc.render(sc.arrays(), lights, library, frame, 256, 6, False, background=background)
+    blocks = lambda x: x.reshape(2, 16, 3, 16, 3).mean((1, 3))
+    sem = np.sqrt((blocks(va) + blocks(vb)) / (256 * 256))
+    assert np.all(np.abs(blocks(a) - blocks(b)) <= 4.0 * sem), np.max(np.abs(blocks(a) - blocks(b)) / sem)
+    # Without a caster nothing starts from afar: no emitters, so no light paths at all.
+    plain = [scenes.openpbr(base_color=(0.8, 0.8, 0.8), specular_weight=0.0)] * 3
+    job = orc.RenderJob(sc.arrays(), lights, [lr.OpenPbr.lambert()] + plain, frame, 6, False, light_tracing=0.5)
+    assert job.light_paths == 0 and job.desc.emit_share == 0.0
