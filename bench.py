@@ -44,6 +44,7 @@ def parse():
     p.add_argument("--rgb", action="store_true", help="the RGB build instead of the spectral one")
     p.add_argument("--skip-batched", action="store_true", help="leave out the 64-scene batched comparison")
     p.add_argument("--skip-served", action="store_true", help="leave out the served arrival stream")
+    p.add_argument("--skip-cornell", action="store_true", help="leave out the glossy Cornell benchmark lines")
     p.add_argument("--served-seconds", type=float, default=10.0,
                    help="length of the served arrival stream (the full workload is 60)")
     return p.parse_args()
@@ -422,6 +423,46 @@ def batched(lr, scenes, ctx, dist):
     }
 
 
+def cornell(lr, scenes, ctx, dist, samples: int = 16, warmup: int = 3) -> dict:
+    """The reference's Cornell benchmark configuration (tests/cornell/main.lucb: the box
+    with a clear-coated blue box, a smooth glass ball, a rough gold ball, a white cube and
+    an orange plastic ball; 12 bounces, camera at (0, 1, 3.9), 50.5 mm on a 36 mm film) at
+    512^2 and 1024^2, spectral and RGB, with light tracing at its default 0.5 and without:
+    ms a sample, timed with CUDA events on the context's stream around `samples` passes
+    after `warmup`. The reference publishes ms a sample for these configurations on an
+    M4 Max (Metal), which is not a B200 number: recorded beside, never divided by."""
+    meshes, cams, lights, mats = scenes.glossy_cornell(4)
+    cams = [lr.camera((0.0, 1.0, 3.9), (0.0, 0.0, 0.0), focal_length=50.5, horizontal_aperture=36.0)]
+    sc = lr.compile_scene(meshes, cams, lights, mats)
+    lines = []
+    for size, spectral, tracing in [(512, True, 0.5), (512, True, 0.0), (1024, True, 0.5), (1024, False, 0.5)]:
+        s = lr.RenderSettings.of(size, size, warmup + samples)
+        s.max_bounces = 12
+        s.spectral = 1 if spectral else 0
+        s.light_tracing = tracing
+        s.seed = 0
+        r = lr.Renderer.create(ctx, sc, s)
+        for _ in range(warmup):
+            r.advance_one()
+        r.wait()
+        s0 = r.stats()
+        dist.barrier()
+        ctx.synchronize()
+        ctx.timer_start()
+        for _ in range(samples):
+            r.advance_one()
+        r.join()
+        ms = dist.max(ctx.timer_stop())
+        r.finish()
+        s1 = r.stats()
+        r.destroy()
+        rays = (s1.closest_rays - s0.closest_rays) + (s1.shadow_rays - s0.shadow_rays)
+        lines.append({"size": size, "spectral": spectral, "light_tracing": tracing, "ms_per_sample": ms / samples,
+                      "mrays_s": rays / (ms / 1e3) / 1e6})
+    return {"triangles": int(sc.info.triangle_count), "max_bounces": 12, "samples": samples, "lines": lines,
+            "reference_m4_max_ms": {"1024 spectral": 8.1, "1024 rgb": 7.1, "512 path tracing only": 3.14}}
+
+
 def cpu_intersection(sc, scenes, oracle, cores: int) -> dict:
     """The reference's CPU intersection on the 1M-triangle scene, on all host cores: its
     f64 brute force (tests/gpu/main.lucb:82-119, every ray against every triangle) on a
@@ -583,6 +624,7 @@ def main():
                    "note": "light paths (0.5 x the pixels a sample) from the scene's rect lights, their camera "
                            "connections splatted; rays include the light paths' closest and connection rays"}
 
+    cornell_info = None if args.skip_cornell else cornell(lr, scenes, ctx, dist)
     batch_info = None if args.skip_batched else batched(lr, scenes, ctx, dist)
     served_info = None if args.skip_served else served(lr, scenes, dist, args.served_seconds)
 
@@ -619,6 +661,7 @@ def main():
             "gpu_launches": K * (1 + 3 * (BOUNCES + 1) + 3),
             "clocks": clock_info,
             "light_traced": traced_info,
+            "cornell": cornell_info,
             "batched": batch_info,
             "served": served_info,
         }

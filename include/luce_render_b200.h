@@ -110,9 +110,11 @@ typedef struct {
     int32_t normalize, visible;              /* UsdLux normalize; visible to the camera */
 } lr_light;
 
-/* OpenPBR Surface parameters (src/render/materials.lucb:17-53). This build shades the
- * Lambertian subset: specular_weight, base_metalness, transmission_weight and
- * coat_weight 0, geometry_opacity 1; base_diffuse_roughness is EON's. */
+/* OpenPBR Surface parameters (src/render/materials.lucb:17-53), shaded as
+ * shaders/openpbr.glsl does: EON diffuse, GGX specular, F82-tint metal, coat, rough
+ * transmission, emission. Not shaded: geometry_opacity below 1 (cut-outs) and, in the
+ * spectral build, transmission dispersion (rejected with 400); thin_walled is accepted
+ * and, as in the reference's kernels, changes nothing. */
 typedef struct {
     double base_weight, base_color[3], base_metalness, base_diffuse_roughness;
     double specular_weight, specular_color[3], specular_roughness, specular_roughness_anisotropy,

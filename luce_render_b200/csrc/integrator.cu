@@ -88,11 +88,12 @@ constexpr float kSplatLimit = 1e9f;
 // `count` pixels of member `member` from `first_pixel`, at sample `sample`, in pool
 // paths path_base .. path_base + count -- or, of kind kLightSegment, `count` of the
 // sample's light paths from number `first_pixel`. `convert`: this segment ends the
-// member's sample, so its image is brought up to date after the pass.
+// member's sample, so its image is brought up to date after the pass. `kind_base`: the
+// pass's paths of the segment's kind before it (its rays' place in the queues).
 constexpr uint32_t kCameraSegment = 0, kLightSegment = 1;
 struct Segment {
     uint32_t member, first_pixel, count, sample;
-    uint32_t path_base, convert, kind, reserved;
+    uint32_t path_base, convert, kind, kind_base;
 };
 
 // `dry`: a trial pass (autotuning) that traces its segments but leaves films alone.
@@ -125,11 +126,20 @@ struct Wave {
     // ray queues (ping-pong by round) and their hits
     float4 *ray_o[2], *ray_d[2], *hits[2];
     float4 *shadow_o, *shadow_d, *shadow_c;
-    // counters[r]: rays of round r; counters[rounds + 1 + r]: shadow rays of round r
+    // Ray queues hold camera paths' rays from the front and light paths' from the back
+    // (index pool - 1 - k), so that each kind shades in a launch of its own.
+    // counters[r]: camera paths' rays of round r; counters[rounds + 1 + r]: shadow rays of
+    // round r; counters[kLightCounters * rounds + 2 + r] (light_counter): light paths' rays.
     uint32_t *counters;
     unsigned long long *stats;  // closest rays, shadow rays, paths, passes, then traversal work
     int *status;
 };
+
+// Where the light paths' ray counts start in a wave's counters.
+constexpr uint32_t kLightCounters = 2;
+__device__ __forceinline__ uint32_t *light_counter(const Wave &w, uint32_t round) {
+    return &w.counters[kLightCounters * w.rounds + 2 + round];
+}
 
 __device__ __forceinline__ uint32_t warp_push(uint32_t *counter, bool want) {
     const unsigned mask = __ballot_sync(0xffffffffu, want);
@@ -171,14 +181,16 @@ template <int W, int kStack, bool kCount>
 __global__ void __launch_bounds__(kTraceBlock) closest_kernel(Wave w, uint32_t round) {
     __shared__ int stack[TracerOf<W, false, kStack, kCount>::kInts * kTraceBlock];
     const uint32_t q = round & 1u;
-    const uint32_t count = w.counters[round];
+    const uint32_t cameras = w.counters[round], count = cameras + *light_counter(w, round);
     bool overflow = false;
     Visits visits;
     const float4 *ray_o = w.ray_o[q], *ray_d = w.ray_d[q];
     float4 *hits = w.hits[q];
     typename TracerOf<W, false, kStack, kCount>::type tr(stack + threadIdx.x, kTraceBlock);
     const uint32_t step = gridDim.x * blockDim.x;
-    for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < count; i += step) {
+    for (uint32_t j = blockIdx.x * blockDim.x + threadIdx.x; j < count; j += step) {
+        // The camera paths' rays, then the light paths' from the queue's back.
+        const uint32_t i = j < cameras ? j : w.pool - 1u - (j - cameras);
         const float4 o = ray_o[i], d = ray_d[i];
         const uint32_t segment = __float_as_uint(o.w) >> kPathBits;
         {
@@ -399,8 +411,8 @@ __device__ __forceinline__ bool emitter_is_triangle(const Member &m, uint32_t em
     return (__ldg(&m.tree.records[emitter]).x & kEmitterTriangle) != 0u;
 }
 
-// emitter_area_pdf (connect.glsl:116-132). No light paths start from afar here: at the
-// Lambertian settings nothing casts caustics (loading.lucb:127-146).
+// emitter_area_pdf (connect.glsl:116-132): the area density light emission gives a point on
+// an emitter of the tree, the emitter's chance included.
 __device__ __forceinline__ float emitter_area_pdf(const Member &m, uint32_t emitter) {
     const uint32_t code = __ldg(&m.tree.records[emitter]).x;
     float area;
@@ -466,9 +478,10 @@ __device__ __forceinline__ float light_cos(const float4 *lights, uint32_t light,
     return fmaxf(0.0f, -dot(d, xyz(light_at(lights, light, 3))));
 }
 
-// light_sampler_pdf (connect.glsl:52-62) at the Lambertian settings: the pdf the light
-// sampler at a surface (shading normal n, geometric g, facing one side) gives `to` when
-// the light path arrived from `from` (both leaving the point).
+// light_sampler_pdf (connect.glsl:51-60) for a surface whose only lobe is diffuse (a
+// Lambertian member's): the pdf the light sampler at a surface (shading normal n,
+// geometric g, facing one side) gives `to` when the light path arrived from `from` (both
+// leaving the point). The layered surface's is in openpbr.cuh.
 __device__ __forceinline__ float light_sampler_pdf(float p_diffuse, float3 n, float3 g, float3 from, float3 to) {
     const bool same = dot(from, g) >= 0.0f;
     const float3 nv = same ? n : -n, gv = same ? g : -g;
@@ -515,7 +528,8 @@ __device__ __forceinline__ float light_sample_ratio(const Member &m, const Const
 // a point on it uniform by area, a cosine-weighted direction (either side of an emissive
 // triangle). A path that cannot start gets a ray that reaches nothing.
 template <bool kSpectral>
-__device__ __forceinline__ void light_emit(const Wave &w, const Member &m, const Segment &sg, uint32_t si, uint32_t path) {
+__device__ __forceinline__ void light_emit(const Wave &w, const Member &m, const Segment &sg, uint32_t si, uint32_t path,
+                                           uint32_t slot) {
     const uint32_t id = 0x80000000u | (m.light_band + sg.first_pixel + (path - sg.path_base));
     const uint32_t seed = m.k->seed;
     const float4 u_point = sample4(seed, id, sg.sample, kGroupCamera);
@@ -524,8 +538,8 @@ __device__ __forceinline__ void light_emit(const Wave &w, const Member &m, const
     const float tag = __uint_as_float(path | (si << kPathBits));
     auto dead = [&] {
         w.path[path] = make_uint4(kNone, 0u, 0u, 0u);
-        w.ray_o[0][path] = make_float4(0.0f, 0.0f, 0.0f, tag);
-        w.ray_d[0][path] = make_float4(0.0f, 0.0f, 1.0f, 0.0f);
+        w.ray_o[0][slot] = make_float4(0.0f, 0.0f, 0.0f, tag);
+        w.ray_d[0][slot] = make_float4(0.0f, 0.0f, 1.0f, 0.0f);
     };
     // From afar: a direction by the light's distribution, a point on the disk facing it
     // about the casters' centre, toward the scene.
@@ -553,8 +567,8 @@ __device__ __forceinline__ void light_emit(const Wave &w, const Member &m, const
         if (kSpectral) w.lambda[path] = lambda;
         w.vertex[path] = make_float4(start.x, start.y, start.z, 1.0f / most);
         w.mis[path] = make_float4(1.0f, chance, 1.0f, -1.0f);
-        w.ray_o[0][path] = make_float4(start.x, start.y, start.z, tag);
-        w.ray_d[0][path] = make_float4(-toward.x, -toward.y, -toward.z, kInfinity);
+        w.ray_o[0][slot] = make_float4(start.x, start.y, start.z, tag);
+        w.ray_d[0][slot] = make_float4(-toward.x, -toward.y, -toward.z, kInfinity);
         return;
     }
     uint32_t emitter;
@@ -619,8 +633,8 @@ __device__ __forceinline__ void light_emit(const Wave &w, const Member &m, const
     // Russian roulette weighs throughput relative to the start's.
     w.vertex[path] = make_float4(q.x, q.y, q.z, 1.0f / largest);
     w.mis[path] = make_float4(1.0f, point_pdf, cos_n, -1.0f);
-    w.ray_o[0][path] = make_float4(origin.x, origin.y, origin.z, tag);
-    w.ray_d[0][path] = make_float4(direction.x, direction.y, direction.z, kInfinity);
+    w.ray_o[0][slot] = make_float4(origin.x, origin.y, origin.z, tag);
+    w.ray_d[0][slot] = make_float4(direction.x, direction.y, direction.z, kInfinity);
 }
 
 // camera.comp:14-50: a jittered primary ray per pixel of every camera segment; the light
@@ -630,7 +644,9 @@ __global__ void __launch_bounds__(kShadeBlock) camera_kernel(Wave w) {
     const Plan *plan = w.plan;
     const uint32_t paths = plan->head.paths;
     if (blockIdx.x == 0) {
-        for (uint32_t i = threadIdx.x; i < 4 * w.rounds + 2; i += blockDim.x) w.counters[i] = i == 0 ? paths : 0u;
+        const uint32_t light_base = kLightCounters * w.rounds + 2;
+        for (uint32_t i = threadIdx.x; i < 4 * w.rounds + 2; i += blockDim.x)
+            w.counters[i] = i == 0 ? plan->head.camera_paths : (i == light_base ? paths - plan->head.camera_paths : 0u);
     }
     const uint32_t stride = gridDim.x * blockDim.x;
     for (uint32_t path = blockIdx.x * blockDim.x + threadIdx.x; path < paths; path += stride) {
@@ -638,10 +654,12 @@ __global__ void __launch_bounds__(kShadeBlock) camera_kernel(Wave w) {
         const Segment &sg = plan->seg[si];
         const Member &m = w.members[sg.member];
         if (sg.kind == kLightSegment) {
-            if (m.spectral) light_emit<true>(w, m, sg, si, path);
-            else light_emit<false>(w, m, sg, si, path);
+            const uint32_t slot = w.pool - 1u - (sg.kind_base + (path - sg.path_base));
+            if (m.spectral) light_emit<true>(w, m, sg, si, path, slot);
+            else light_emit<false>(w, m, sg, si, path, slot);
             continue;
         }
+        const uint32_t slot = sg.kind_base + (path - sg.path_base);
         const uint32_t pixel = sg.first_pixel + (path - sg.path_base);
         const uint32_t sample = sg.sample;
         const uint32_t seed = m.k->seed;
@@ -669,8 +687,8 @@ __global__ void __launch_bounds__(kShadeBlock) camera_kernel(Wave w) {
         if (m.spectral) w.lambda[path] = sample_wavelengths(sample4(seed, pixel, sample, kGroupWavelength).x);
         // Light tracing's MIS: the light paths a sample, and the camera's pdf (camera.comp:42).
         if (m.light_paths) w.mis[path] = make_float4((float)m.light_paths, 0.0f, 0.0f, camera_pdf(m, direction));
-        w.ray_o[0][path] = make_float4(origin.x, origin.y, origin.z, __uint_as_float(path | (si << kPathBits)));
-        w.ray_d[0][path] = make_float4(direction.x, direction.y, direction.z, kInfinity);
+        w.ray_o[0][slot] = make_float4(origin.x, origin.y, origin.z, __uint_as_float(path | (si << kPathBits)));
+        w.ray_d[0][slot] = make_float4(direction.x, direction.y, direction.z, kInfinity);
     }
 }
 
@@ -914,8 +932,11 @@ __device__ __noinline__ void shade_glossy(const Wave &w, const Member &m, uint32
 }
 
 // One queue entry: a miss (shade_miss.comp:12-51), a light hit or a surface hit
-// (shade_surface.comp:48-312 at the Lambertian settings). kTracing: members of the pass
-// may trace light paths, so camera paths weigh their techniques against them.
+// (shade_surface.comp:48-312) of a member whose materials are all EON diffuse (OpenPBR with
+// no specular, metal, coat or transmission lobe), where the layered surface reduces to
+// EON with p_diffuse 1. kTracing: members of the pass may trace light paths, so camera
+// paths weigh their techniques against them. kGlossy: members with glossy materials take
+// shade_glossy instead.
 template <bool kSpectral, bool kTracing, bool kGlossy>
 __device__ __forceinline__ void shade_one(const Wave &w, const Member &m, uint32_t sample, uint32_t round, uint32_t i,
                                           float4 ro, ShadeOut &out) {
@@ -1128,8 +1149,8 @@ __device__ __forceinline__ void shade_one(const Wave &w, const Member &m, uint32
     out.d = make_float4(direction.x, direction.y, direction.z, kInfinity);
 }
 
-// A light path's hit (light_paths.glsl:35-189) at the Lambertian settings: a light ends
-// it; at a surface it connects to the camera -- a shadow ray carrying, in the film's
+// A light path's hit (light_paths.glsl:31-189) on a member whose materials are all EON
+// diffuse: a light ends it; at a surface it connects to the camera -- a shadow ray carrying, in the film's
 // terms and MIS-weighted, what the camera would see of it to the pixel it projects to --
 // and scatters on by the BSDF as seen from where the light came, weighed by the BSDF as
 // the camera would evaluate it, with the shading-normal correction light paths need.
@@ -1409,24 +1430,29 @@ __device__ __noinline__ void shade_light_glossy(const Wave &w, const Member &m, 
 // 1080p pass on the 1M-triangle scene; 48 registers: 0.99 ms with twice the spills).
 // kTracing: the pass holds light paths or camera paths that weigh against them; passes
 // without take the kernel without that code (it cost camera-only passes 16 %). kGlossy:
-// the pass holds a member with glossy materials, whose surfaces take the layered OpenPBR
+// the pass holds a member with glossy materials, whose entries take the layered OpenPBR
 // shading (out of line, 4 blocks an SM for its registers); the rest shade as without it.
-template <bool kTracing, bool kGlossy>
+// kLight: the launch shades the light paths' rays (the queue's back) rather than the
+// camera paths' (its front). Camera and light paths shade in launches of their own: mixed
+// in one launch, their two large bodies fought over the instruction cache (the glossy box
+// with light tracing: 4.2 -> 1.8 ms of shading a 512^2 sample).
+template <bool kTracing, bool kGlossy, bool kLight>
 __global__ void __launch_bounds__(kShadeBlock, kGlossy ? 4 : 8) shade_kernel(Wave w, uint32_t round) {
-    const uint32_t count = w.counters[round];
+    const uint32_t count = kLight ? *light_counter(w, round) : w.counters[round];
     const uint32_t q = round & 1u, nq = q ^ 1u;
     const uint32_t lane = threadIdx.x & 31u;
     const uint32_t stride = gridDim.x * blockDim.x;
-    uint32_t *next_counter = &w.counters[round + 1];
+    uint32_t *next_counter = kLight ? light_counter(w, round + 1) : &w.counters[round + 1];
     uint32_t *shadow_counter = &w.counters[w.rounds + 1 + round];
     for (uint32_t base = blockIdx.x * blockDim.x + (threadIdx.x & ~31u); base < count; base += stride) {
-        const uint32_t i = base + lane;
+        const uint32_t k = base + lane;
+        const uint32_t i = kLight ? w.pool - 1u - k : k;
         ShadeOut out;
-        if (i < count) {
+        if (k < count) {
             const float4 ro = w.ray_o[q][i];
             const Segment &sg = w.plan->seg[__float_as_uint(ro.w) >> kPathBits];
             const Member &m = w.members[sg.member];
-            if (kTracing && sg.kind == kLightSegment) {
+            if (kLight) {
                 if (kGlossy && m.glossy) {
                     if (m.spectral) shade_light_glossy<true>(w, m, sg.sample, round, i, ro, out);
                     else shade_light_glossy<false>(w, m, sg.sample, round, i, ro, out);
@@ -1443,8 +1469,9 @@ __global__ void __launch_bounds__(kShadeBlock, kGlossy ? 4 : 8) shade_kernel(Wav
         }
         const uint32_t at = warp_push(next_counter, out.next);
         if (out.next) {
-            w.ray_o[nq][at] = out.o;
-            w.ray_d[nq][at] = out.d;
+            const uint32_t slot = kLight ? w.pool - 1u - at : at;
+            w.ray_o[nq][slot] = out.o;
+            w.ray_d[nq][slot] = out.d;
         }
         const uint32_t sat = warp_push(shadow_counter, out.shadow);
         if (out.shadow) {
@@ -1475,7 +1502,7 @@ __global__ void __launch_bounds__(kShadeBlock) finish_kernel(Wave w) {
     if (blockIdx.x == 0 && threadIdx.x == 0) {
         unsigned long long closest = 0, shadow = 0;
         for (uint32_t r = 0; r < w.rounds; r++) {
-            closest += w.counters[r];
+            closest += w.counters[r] + *light_counter(w, r);
             shadow += w.counters[w.rounds + 1 + r];
         }
         w.stats[0] += closest;
@@ -1734,12 +1761,17 @@ void record_trace(const WaveHost *h, const Wave &w, int grid_trace, bool tracing
         closest_kernel<W, kStack, kCount><<<grid_trace, kTraceBlock, 0, stream>>>(w, round);
         mark(stream, marks, kClosest);
         if (glossy) {
-            if (tracing) shade_kernel<true, true><<<h->grid_shade_glossy, kShadeBlock, 0, stream>>>(w, round);
-            else shade_kernel<false, true><<<h->grid_shade_glossy, kShadeBlock, 0, stream>>>(w, round);
+            if (tracing) {
+                shade_kernel<true, true, false><<<h->grid_shade_glossy, kShadeBlock, 0, stream>>>(w, round);
+                shade_kernel<true, true, true><<<h->grid_shade_glossy, kShadeBlock, 0, stream>>>(w, round);
+            } else {
+                shade_kernel<false, true, false><<<h->grid_shade_glossy, kShadeBlock, 0, stream>>>(w, round);
+            }
         } else if (tracing) {
-            shade_kernel<true, false><<<h->grid_shade, kShadeBlock, 0, stream>>>(w, round);
+            shade_kernel<true, false, false><<<h->grid_shade, kShadeBlock, 0, stream>>>(w, round);
+            shade_kernel<true, false, true><<<h->grid_shade, kShadeBlock, 0, stream>>>(w, round);
         } else {
-            shade_kernel<false, false><<<h->grid_shade, kShadeBlock, 0, stream>>>(w, round);
+            shade_kernel<false, false, false><<<h->grid_shade, kShadeBlock, 0, stream>>>(w, round);
         }
         mark(stream, marks, kSurface);
         shadow_kernel<W, kStack, kCount><<<grid_trace, kTraceBlock, 0, stream>>>(w, round);
@@ -1915,8 +1947,8 @@ void wave_create(WaveHost *h, lr_context *ctx, uint64_t pool, uint32_t rounds, u
     upload_sobol_tables(ctx->stream);
     make_albedo_tables(ctx->device, ctx->stream);
     LR_CUDA(cudaStreamSynchronize(ctx->stream));
-    h->grid_shade = grid_of(shade_kernel<false, false>, kShadeBlock, ctx->sm_count);
-    h->grid_shade_glossy = grid_of(shade_kernel<false, true>, kShadeBlock, ctx->sm_count);
+    h->grid_shade = grid_of(shade_kernel<false, false, false>, kShadeBlock, ctx->sm_count);
+    h->grid_shade_glossy = grid_of(shade_kernel<false, true, false>, kShadeBlock, ctx->sm_count);
     if (profile)
         for (auto &e : h->mark_start) LR_CUDA(cudaEventCreate(&e));
     else
@@ -2167,7 +2199,7 @@ bool launch_pass(WaveHost *h, bool dry = false, int only = -1) {
         uint32_t light_next = mh.light_next;
         if (light_next < lights) {
             const uint32_t count = std::min(lights - light_next, fill - used);
-            seg[n++] = Segment{index, light_next, count, mh.sample, used, 0u, kLightSegment, 0u};
+            seg[n++] = Segment{index, light_next, count, mh.sample, used, 0u, kLightSegment, used - camera_paths};
             staging->fold[folds++] = index;
             used += count;
             light_next += count;
@@ -2180,7 +2212,7 @@ bool launch_pass(WaveHost *h, bool dry = false, int only = -1) {
         const bool ends = count > 0 && count == left && !dry;
         rec.members.push_back({index, ends});
         if (count > 0) {
-            seg[n++] = Segment{index, mh.next_pixel, count, mh.sample, used, ends ? 1u : 0u, kCameraSegment, 0u};
+            seg[n++] = Segment{index, mh.next_pixel, count, mh.sample, used, ends ? 1u : 0u, kCameraSegment, camera_paths};
             if (ends) {
                 staging->convert[converts] = index;
                 staging->convert_samples[converts++] = mh.sample + 1;

@@ -1,8 +1,8 @@
 // Device math of the integrator's shading: the stateless Owen-scrambled Sobol sampler
 // (shaders/sampler.glsl:8-55), hero-wavelength spectra (spectrum.glsl:10-118), UsdLux
-// lights (lights.glsl:24-282), the light tree (lighttree.glsl:18-137), EON/Lambert
-// diffuse (openpbr.glsl:87-113, 460-547 at the Lambertian settings) and the path
-// helpers of common.glsl:103-276.
+// lights (lights.glsl:24-282), the light tree (lighttree.glsl:18-137), EON diffuse
+// (openpbr.glsl:87-113) and the path helpers of common.glsl:103-276. The layered OpenPBR
+// surface is in openpbr.cuh.
 #pragma once
 
 #include <cuda_runtime.h>
@@ -493,7 +493,7 @@ __device__ __forceinline__ float tree_pdf(const TreeView &t, uint32_t emitter, f
     return pdf;
 }
 
-// ---- EON diffuse at the Lambertian settings (openpbr.glsl:87-113) ---------------------
+// ---- EON diffuse (openpbr.glsl:87-113) -----------------------------------------------
 
 constexpr float kFonC1 = 0.5f - 2.0f / (3.0f * kPi);
 constexpr float kFonC2 = 2.0f / 3.0f - 28.0f / (15.0f * kPi);

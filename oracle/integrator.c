@@ -1,8 +1,8 @@
 /*
  * Oracle (test infrastructure): the reference's path-tracing estimator restated in f64,
  * one path at a time over the same Owen-scrambled Sobol samples the kernels draw:
- * camera.comp:14-50, intersect_closest.comp:45-76, shade_surface.comp:48-312 at the
- * Lambertian settings, shade_miss.comp:12-51, intersect_shadow.comp:51-92 (opaque),
+ * camera.comp:14-50, intersect_closest.comp:45-76, shade_surface.comp:48-312 with the
+ * OpenPBR surface of openpbr.c, shade_miss.comp:12-51, intersect_shadow.comp:51-92 (opaque),
  * finish.comp:13-39 and film_convert.comp:36-53, with the helpers of common.glsl,
  * spectrum.glsl, lights.glsl, lighttree.glsl and openpbr.glsl (EON, 87-113).
  * Traversal walks the same BVH nodes in f64 (box tests and Moller-Trumbore in f64).
@@ -813,11 +813,11 @@ static double light_sample_ratio(const or_render_desc *r, uint32_t emitter, cons
     return chance * pdf / bsdf_pdf;
 }
 
-/* light_emit.comp:55-136 and light_paths.glsl:27-189 at the Lambertian settings: light
- * path `index` of sample `sample` from an emitter of the light tree chosen by power (no
- * light paths start from afar: Lambertian materials cast no caustics), each surface it
- * reaches connected to the camera -- what gets through is added, in the film's terms, to
- * `splat` (3 per pixel) -- and scattered on. */
+/* light_emit.comp:21-130 and light_paths.glsl:31-189: light path `index` of sample
+ * `sample`, from a distant light with a size (by its share) on a disk facing it, or from
+ * an emitter of the light tree chosen by power; each surface it reaches connected to the
+ * camera -- what gets through is added, in the film's terms, to `splat` (3 per pixel) --
+ * and scattered on by light_lobes' choice. */
 static void trace_light_path(const or_render_desc *r, uint32_t sample, uint32_t index, double *splat,
                              uint64_t rays[2]) {
     const uint32_t id = 0x80000000u | (r->light_band + index);
