@@ -25,6 +25,12 @@ ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 COMMON = ["-O3", "-std=c++17", "-Xcompiler", "-fPIC", "-Xcompiler", "-fvisibility=hidden",
           "-I", str(ROOT / "include")]
 CUDA_FLAGS = ARCH + ["-lineinfo", "--expt-relaxed-constexpr", "-Xptxas", "-v"]
+# The integrator's shading divides and takes square roots at the reference's own
+# precision (Vulkan's GLSL allows 2.5 ulp for a division and computes sqrt from
+# inversesqrt), not as IEEE-exact software sequences; the traversal it includes decides
+# hits and distances with explicitly rounded intrinsics (__frcp_rn, __fmul_rn, ...), which
+# these flags do not touch, so hit ids and distances stay the exact ones.
+FILE_FLAGS = {"integrator.cu": ["-prec-div=false", "-prec-sqrt=false", "-ftz=true"]}
 
 
 def nvcc() -> str:
@@ -45,7 +51,7 @@ def headers() -> list[Path]:
 def _compile(src: Path, obj: Path) -> tuple[Path, str]:
     cmd = [nvcc(), *COMMON, "-c", str(src), "-o", str(obj)]
     if src.suffix == ".cu":
-        cmd[1:1] = CUDA_FLAGS
+        cmd[1:1] = CUDA_FLAGS + FILE_FLAGS.get(src.name, [])
     proc = subprocess.run(cmd, capture_output=True, text=True)
     if proc.returncode != 0:
         raise RuntimeError(f"compiling {src.name} failed:\n{' '.join(cmd)}\n{proc.stdout}\n{proc.stderr}")

@@ -1425,6 +1425,51 @@ __device__ __noinline__ void shade_light_glossy(const Wave &w, const Member &m, 
     out.d = make_float4(direction.x, direction.y, direction.z, kInfinity);
 }
 
+// Sorting keys of a shading tile: 0 for misses and light hits, 1 .. kSortBins - 2 for
+// surface hits by member and material, kSortBins - 1 past the queue's end.
+constexpr uint32_t kSortBins = 64;
+
+// A block's tile of queue entries [tile, tile + blockDim.x) ordered by key, counting-sort
+// style in shared memory; returns the tile position this thread shades. Every thread of
+// the block calls it.
+__device__ __forceinline__ uint32_t tile_order(const Wave &w, uint32_t q, uint32_t tile, uint32_t count, bool light,
+                                               uint32_t *bins, uint32_t *order) {
+    const uint32_t t = threadIdx.x, k = tile + t;
+    uint32_t key = kSortBins - 1u;
+    if (k < count) {
+        const uint32_t i = light ? w.pool - 1u - k : k;
+        const uint32_t what = __float_as_uint(w.hits[q][i].y);
+        if (what == kNone || (what & kLightHit)) {
+            key = 0u;
+        } else {
+            const uint32_t member = w.plan->seg[__float_as_uint(w.ray_o[q][i].w) >> kPathBits].member;
+            const uint32_t material = __ldg(&w.members[member].scene.shading[what]).w;
+            key = 1u + (material * 7u + member * 5u) % (kSortBins - 2u);
+        }
+    }
+    for (uint32_t b = t; b < kSortBins; b += blockDim.x) bins[b] = 0u;
+    __syncthreads();
+    const uint32_t rank = atomicAdd(&bins[key], 1u);
+    __syncthreads();
+    if (t < 32u) {  // exclusive scan of the bins, two a lane
+        const uint32_t a = bins[2u * t], b = bins[2u * t + 1u];
+        uint32_t sum = a + b;
+        for (uint32_t d = 1; d < 32u; d <<= 1) {
+            const uint32_t up = __shfl_up_sync(0xffffffffu, sum, d);
+            if (t >= d) sum += up;
+        }
+        const uint32_t before = sum - a - b;
+        bins[2u * t] = before;
+        bins[2u * t + 1u] = before + a;
+    }
+    __syncthreads();
+    order[bins[key] + rank] = t;
+    __syncthreads();
+    const uint32_t mine = order[t];
+    __syncthreads();  // the next tile rewrites the bins and the order
+    return mine;
+}
+
 // 8 blocks an SM (64 registers): shade_one wants 128, which leaves 16 warps an SM to hide
 // its memory latency; capped, it spills a little and runs 17 % faster (1.21 -> 1.01 ms a
 // 1080p pass on the 1M-triangle scene; 48 registers: 0.99 ms with twice the spills).
@@ -1440,12 +1485,11 @@ template <bool kTracing, bool kGlossy, bool kLight>
 __global__ void __launch_bounds__(kShadeBlock, kGlossy ? 4 : 8) shade_kernel(Wave w, uint32_t round) {
     const uint32_t count = kLight ? *light_counter(w, round) : w.counters[round];
     const uint32_t q = round & 1u, nq = q ^ 1u;
-    const uint32_t lane = threadIdx.x & 31u;
     const uint32_t stride = gridDim.x * blockDim.x;
     uint32_t *next_counter = kLight ? light_counter(w, round + 1) : &w.counters[round + 1];
     uint32_t *shadow_counter = &w.counters[w.rounds + 1 + round];
-    for (uint32_t base = blockIdx.x * blockDim.x + (threadIdx.x & ~31u); base < count; base += stride) {
-        const uint32_t k = base + lane;
+    // Shades queue entry k (all threads of the warp call it: the pushes are warp-wide).
+    auto shade = [&](uint32_t k) {
         const uint32_t i = kLight ? w.pool - 1u - k : k;
         ShadeOut out;
         if (k < count) {
@@ -1479,6 +1523,16 @@ __global__ void __launch_bounds__(kShadeBlock, kGlossy ? 4 : 8) shade_kernel(Wav
             w.shadow_d[sat] = out.sd;
             w.shadow_c[sat] = out.sc;
         }
+    };
+    if constexpr (kGlossy) {
+        // Layered surfaces branch by material: each block tile of the queue is ordered by
+        // what its entries shade before its warps take them, so a warp's lanes mostly
+        // follow one path through the lobes.
+        __shared__ uint32_t bins[kSortBins], order[kShadeBlock];
+        for (uint32_t tile = blockIdx.x * blockDim.x; tile < count; tile += stride)
+            shade(tile + tile_order(w, q, tile, count, kLight, bins, order));
+    } else {
+        for (uint32_t k = blockIdx.x * blockDim.x + threadIdx.x; k - (threadIdx.x & 31u) < count; k += stride) shade(k);
     }
 }
 
