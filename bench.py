@@ -45,6 +45,8 @@ def parse():
     p.add_argument("--skip-batched", action="store_true", help="leave out the 64-scene batched comparison")
     p.add_argument("--skip-served", action="store_true", help="leave out the served arrival stream")
     p.add_argument("--skip-cornell", action="store_true", help="leave out the glossy Cornell benchmark lines")
+    p.add_argument("--cornell-only", action="store_true",
+                   help="only the glossy Cornell benchmark lines (--steps samples each), one JSON line")
     p.add_argument("--served-seconds", type=float, default=10.0,
                    help="length of the served arrival stream (the full workload is 60)")
     return p.parse_args()
@@ -497,9 +499,16 @@ def main():
     from luce_render_b200 import scenes
 
     ctx = lr.Context(dist.local)
+    W, K = max(3, args.warmup), args.steps
+    if args.cornell_only:
+        info = cornell(lr, scenes, ctx, dist, samples=K, warmup=W)
+        if dist.rank == 0:
+            print(json.dumps({"cornell": info, "n_gpus": dist.world}))
+        ctx.close()
+        dist.close()
+        return
     sc, lights, mats = build_scene(lr, scenes)
     info = sc.info
-    W, K = max(3, args.warmup), args.steps
 
     # Work per ray, counted by the traversal kernels on one pass of the same workload.
     counter = lr.Renderer.create(ctx, sc, settings_for(lr, 1, spectral, profile=2))
@@ -581,19 +590,25 @@ def main():
         "kernel_share": kernel_ms[1] / max(1e-9, kernel_ms.sum()),
     }
 
-    # End to end through the public API: each step one pass and the image read back into
-    # pinned host memory (the pass takes no new input: the scene stays resident).
+    # End to end through the public API: each step one pass and its image read back into
+    # pinned host memory (the pass takes no new input: the scene stays resident). The reads
+    # are Renderer.read_async into two host buffers in turn, each copy running beside the
+    # next pass; the timed region ends when the last copy has landed.
     e2e_r = lr.Renderer.create(ctx, sc, settings_for(lr, W + K, spectral, profile=0))
-    host = lr.PinnedArray((HEIGHT, WIDTH, 4), np.float32)
-    for _ in range(W):
+    hosts = [lr.PinnedArray((HEIGHT, WIDTH, 4), np.float32) for _ in range(2)]
+    for step in range(W):
         e2e_r.advance_one()
-        e2e_r.read_into(host.array)
+        e2e_r.read_async(hosts[step % 2].array)
+    e2e_r.read_wait()
     e0 = e2e_r.stats()
     dist.barrier()
     start = time.perf_counter()
-    for _ in range(K):
+    for step in range(K):
         e2e_r.advance_one()
-        e2e_r.read_into(host.array)
+        if step >= 2:
+            e2e_r.read_wait()  # the buffer this read reuses is free again
+        e2e_r.read_async(hosts[step % 2].array)
+    e2e_r.read_wait()
     e2e_s = time.perf_counter() - start
     e1 = e2e_r.stats()
     e2e_r.destroy()

@@ -312,6 +312,14 @@ int lr_renderer_image(lr_renderer *renderer, void **device_rgba);
 /* Renderer.read (integrator.lucb:778-782): the image copied to `rgba` (4 floats a
  * pixel); waits for work in flight. */
 int lr_renderer_read(lr_renderer *renderer, float *rgba, uint64_t float_count);
+/* (No counterpart: the reference's read waits for the render.) Renderer.read without the
+ * wait: queues a copy of the image as the pass launched last leaves it into `rgba` (4
+ * floats a pixel; pinned host memory, e.g. lr_host_alloc_pinned, lets the copy run beside
+ * the passes launched after it) and returns at once. The buffer must stay untouched until
+ * lr_renderer_read_wait returns, which waits for every copy queued. Passes launched
+ * later never change a copy in flight. */
+int lr_renderer_read_async(lr_renderer *renderer, float *rgba, uint64_t count);
+int lr_renderer_read_wait(lr_renderer *renderer);
 /* Orders the context's stream after every pass queued so far, without waiting: work
  * the caller queues there afterwards (reading the device image, an event for timing)
  * sees their results. Passes run on two streams, taking turns; see lr_renderer_advance. */
@@ -387,6 +395,9 @@ int lr_batch_set_samples(lr_batch *batch, uint32_t member, uint32_t samples);
 /* As lr_renderer_image / lr_renderer_read, for one member. */
 int lr_batch_image(lr_batch *batch, uint32_t member, void **device_rgba);
 int lr_batch_read(lr_batch *batch, uint32_t member, float *rgba, uint64_t float_count);
+/* lr_renderer_read_async / _wait for a member of a batch. */
+int lr_batch_read_async(lr_batch *batch, uint32_t member, float *rgba, uint64_t count);
+int lr_batch_read_wait(lr_batch *batch);
 /* The autotuner: times trial passes (which trace but change no film and move no member
  * on) on the members as they stand. For each scene-size class present (under 16k
  * triangles, under 128k, larger) it keeps the BVH width (2, 4, 8; a width all of the

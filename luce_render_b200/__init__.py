@@ -271,6 +271,10 @@ _SIGNATURES = {
     "lr_renderer_read": (C.c_int, [_vp, C.POINTER(C.c_float), _u64]),
     "lr_renderer_set_samples": (C.c_int, [_vp, _u32]),
     "lr_renderer_join": (C.c_int, [_vp]),
+    "lr_renderer_read_async": (C.c_int, [_vp, C.POINTER(C.c_float), _u64]),
+    "lr_renderer_read_wait": (C.c_int, [_vp]),
+    "lr_batch_read_async": (C.c_int, [_vp, _u32, C.POINTER(C.c_float), _u64]),
+    "lr_batch_read_wait": (C.c_int, [_vp]),
     "lr_batch_join": (C.c_int, [_vp]),
     "lr_renderer_kernel_times": (C.c_int, [_vp, C.POINTER(C.c_double)]),
     "lr_renderer_stats": (C.c_int, [_vp, C.POINTER(RenderStats)]),
@@ -779,6 +783,18 @@ class Renderer:
         _check(lib.lr_renderer_read(self.handle, _fptr(out), out.size))
         return out
 
+    def read_async(self, out: np.ndarray) -> None:
+        """Queues a copy of the image as the pass launched last leaves it into `out` (float32,
+        height x width x 4; pinned, e.g. a PinnedArray's, for the copy to overlap the
+        passes after it) and returns at once; `out` is complete after read_wait()."""
+        if out.dtype != np.float32 or out.size != self.width * self.height * 4 or not out.flags.c_contiguous:
+            raise RenderError(INVALID, "reading the image needs four floats a pixel")
+        _check(lib.lr_renderer_read_async(self.handle, _fptr(out), out.size))
+
+    def read_wait(self) -> None:
+        """Waits for every copy read_async queued."""
+        _check(lib.lr_renderer_read_wait(self.handle))
+
     def image(self) -> int:
         """The device address of the rgba32f image."""
         p = _vp()
@@ -895,6 +911,15 @@ class Batch:
             raise RenderError(INVALID, "reading the image needs four floats a pixel")
         _check(lib.lr_batch_read(self.handle, member, _fptr(out), out.size))
         return out
+
+    def read_async(self, member: int, out: np.ndarray) -> None:
+        """Renderer.read_async for a member."""
+        if out.dtype != np.float32 or not out.flags.c_contiguous:
+            raise RenderError(INVALID, "reading the image needs four floats a pixel")
+        _check(lib.lr_batch_read_async(self.handle, member, _fptr(out), out.size))
+
+    def read_wait(self) -> None:
+        _check(lib.lr_batch_read_wait(self.handle))
 
     def kernel_times(self) -> np.ndarray:
         out = (C.c_double * 10)()

@@ -1761,6 +1761,7 @@ struct Lane {
     Graph finish;                // finish and convert
     cudaEvent_t finished = nullptr;  // after its latest pass's convert
     uint64_t members_seen = 0;       // the member uploads its stream has waited for
+    uint64_t reads_seen = 0;         // the image reads its film stage has waited for
 };
 
 struct WaveHost {
@@ -1789,6 +1790,12 @@ struct WaveHost {
     // its passes are the reference's bands, light paths riding along in a sample's first.
     uint32_t camera_cap = 0;
     Staging staging;  // member uploads
+    // Image reads that overlap the passes after them (member_read_async): copies on their
+    // own stream, each after the pass launched last; a film stage launched later waits
+    // for them before it rewrites an image.
+    cudaStream_t copy_stream = nullptr;
+    cudaEvent_t read_done = nullptr;
+    uint64_t reads = 0;
 };
 
 namespace {
@@ -2171,7 +2178,9 @@ uint32_t member_add(WaveHost *h, const lr_gpu_scene *gs, lr_gpu_scene *owned, co
     return index;
 }
 
-void member_free(MemberHost &mh, cudaStream_t stream) {
+void member_free(MemberHost &mh, cudaStream_t stream, cudaEvent_t reads = nullptr) {
+    // A read in flight may still copy from the member's image.
+    if (reads) cudaStreamWaitEvent(stream, reads, 0);
     if (mh.block) cudaFreeAsync(mh.block, stream);
     if (mh.owned) lr_gpu_scene_destroy(mh.owned);
     mh = MemberHost{};
@@ -2180,7 +2189,7 @@ void member_free(MemberHost &mh, cudaStream_t stream) {
 // Frees members that asked to leave once no pass in flight traces them.
 void collect(WaveHost *h) {
     for (auto &mh : h->members)
-        if (mh.used && mh.leaving && mh.last_pass <= h->retired) member_free(mh, h->ctx->stream);
+        if (mh.used && mh.leaving && mh.last_pass <= h->retired) member_free(mh, h->ctx->stream, h->read_done);
 }
 
 bool has_work(const MemberHost &mh) { return mh.used && !mh.leaving && mh.sample < mh.samples; }
@@ -2324,14 +2333,23 @@ bool launch_pass(WaveHost *h, bool dry = false, int only = -1) {
                             stream));
     // Film accumulation waits for the previous pass's, which ran on the other lane.
     Lane *before = rec.number > 0 && h->lane_count > 1 ? &lane_of(h, rec.number - 1) : nullptr;
+    // The film stage rewrites images: it waits for the reads queued since this lane's last.
+    auto after_reads = [&] {
+        if (lane.reads_seen != h->reads) {
+            LR_CUDA(cudaStreamWaitEvent(stream, h->read_done, 0));
+            lane.reads_seen = h->reads;
+        }
+    };
     if (h->profile) {
         LR_CUDA(cudaEventRecord(h->mark_start[rec.number & 1], stream));
         record_trace_any(h, lane.w, variant, stream, &rec.marks);
         if (before) LR_CUDA(cudaStreamWaitEvent(stream, before->finished, 0));
+        after_reads();
         record_finish(h, lane.w, stream, &rec.marks);
     } else {
         LR_CUDA(cudaGraphLaunch(trace_graph(h, lane, variant).exec, stream));
         if (before) LR_CUDA(cudaStreamWaitEvent(stream, before->finished, 0));
+        after_reads();
         LR_CUDA(cudaGraphLaunch(lane.finish.exec, stream));
     }
     LR_CUDA(cudaEventRecord(lane.finished, stream));
@@ -2464,10 +2482,13 @@ void wave_destroy(WaveHost *h) {
         for (auto &[e, k] : p.marks) cudaEventDestroy(e);
     for (auto e : h->mark_start)
         if (e) cudaEventDestroy(e);
+    if (h->copy_stream) cudaStreamSynchronize(h->copy_stream);
     for (auto &mh : h->members)
         if (mh.used) member_free(mh, h->ctx->stream);
     cudaStreamSynchronize(h->ctx->stream);
     h->staging.release();
+    if (h->read_done) cudaEventDestroy(h->read_done);
+    if (h->copy_stream) cudaStreamDestroy(h->copy_stream);
     for (auto &lane : h->lanes) {
         for (auto &[v, g] : lane.trace) destroy_graph(g);
         destroy_graph(lane.finish);
@@ -2514,6 +2535,32 @@ void member_read(WaveHost *h, uint32_t member, float *rgba, uint64_t count) {
     join_lanes(h);
     LR_CUDA(cudaMemcpyAsync(rgba, mh.dev.image, count * 4, cudaMemcpyDeviceToHost, h->ctx->stream));
     LR_CUDA(cudaStreamSynchronize(h->ctx->stream));
+}
+
+// Queues a copy of the member's image as the pass launched last leaves it into `rgba`
+// (pinned host memory, so that the copy runs beside the passes after it) and returns
+// without waiting; member_read_wait waits for every copy queued.
+void member_read_async(WaveHost *h, uint32_t member, float *rgba, uint64_t count) {
+    MemberHost &mh = member_at(h, member);
+    if (count != mh.dev.pixels * 4) fail(LR_INVALID, "reading the image needs four floats a pixel");
+    if (!h->copy_stream) {
+        LR_CUDA(cudaStreamCreateWithFlags(&h->copy_stream, cudaStreamNonBlocking));
+        LR_CUDA(cudaEventCreateWithFlags(&h->read_done, cudaEventDisableTiming));
+    }
+    // After the member's memory arrived (the context's stream) and the last pass launched.
+    cudaEvent_t ready;
+    LR_CUDA(cudaEventCreateWithFlags(&ready, cudaEventDisableTiming));
+    LR_CUDA(cudaEventRecord(ready, h->ctx->stream));
+    LR_CUDA(cudaStreamWaitEvent(h->copy_stream, ready, 0));
+    LR_CUDA(cudaEventDestroy(ready));
+    if (h->recorded > 0) LR_CUDA(cudaStreamWaitEvent(h->copy_stream, lane_of(h, h->recorded - 1).finished, 0));
+    LR_CUDA(cudaMemcpyAsync(rgba, mh.dev.image, count * 4, cudaMemcpyDeviceToHost, h->copy_stream));
+    LR_CUDA(cudaEventRecord(h->read_done, h->copy_stream));
+    h->reads++;
+}
+
+void member_read_wait(WaveHost *h) {
+    if (h->read_done) LR_CUDA(cudaEventSynchronize(h->read_done));
 }
 
 }  // namespace
@@ -2663,6 +2710,20 @@ int lr_renderer_read(lr_renderer *r, float *rgba, uint64_t count) {
     return guarded([&] {
         if (!r || !rgba) fail(LR_INVALID, "no renderer");
         member_read(&r->wave, 0, rgba, count);
+    });
+}
+
+int lr_renderer_read_async(lr_renderer *r, float *rgba, uint64_t count) {
+    return guarded([&] {
+        if (!r || !rgba) fail(LR_INVALID, "no renderer");
+        member_read_async(&r->wave, 0, rgba, count);
+    });
+}
+
+int lr_renderer_read_wait(lr_renderer *r) {
+    return guarded([&] {
+        if (!r) fail(LR_INVALID, "no renderer");
+        member_read_wait(&r->wave);
     });
 }
 
@@ -2820,6 +2881,20 @@ int lr_batch_read(lr_batch *b, uint32_t member, float *rgba, uint64_t count) {
     return guarded([&] {
         if (!b || !rgba) fail(LR_INVALID, "no batch");
         member_read(&b->wave, member, rgba, count);
+    });
+}
+
+int lr_batch_read_async(lr_batch *b, uint32_t member, float *rgba, uint64_t count) {
+    return guarded([&] {
+        if (!b || !rgba) fail(LR_INVALID, "no batch");
+        member_read_async(&b->wave, member, rgba, count);
+    });
+}
+
+int lr_batch_read_wait(lr_batch *b) {
+    return guarded([&] {
+        if (!b) fail(LR_INVALID, "no batch");
+        member_read_wait(&b->wave);
     });
 }
 

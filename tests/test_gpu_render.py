@@ -191,3 +191,35 @@ def test_renderer_api_progress_and_errors(ctx):
         bad = lr.RenderSettings.of(0, 10, 1)
         bad.c.material = lr.OpenPbr.lambert()
         lr.Renderer.create(ctx, sc, bad)
+
+
+def test_renderer_read_async_is_the_image_of_its_pass(ctx):
+    # A read queued after a pass holds that pass's image however many passes follow
+    # before it is waited for: the same bits as a render of that many samples.
+    sc = lr.compile_scene(scenes.cornell_meshes(True), [scenes.cornell_camera()], [scenes.cornell_light()],
+                          scenes.cornell_materials())
+    s = lr.RenderSettings.of(96, 64, 6)
+    s.max_bounces = 4
+    s.light_tracing = 0.0
+    s.c.material = lr.OpenPbr.lambert()
+    hosts = [lr.PinnedArray((64, 96, 4), np.float32) for _ in range(3)]
+    r = lr.Renderer.create(ctx, sc, s)
+    r.advance_one()
+    r.read_async(hosts[0].array)
+    r.advance_one()
+    r.advance_one()
+    r.read_async(hosts[1].array)
+    r.finish()
+    r.read_async(hosts[2].array)
+    r.read_wait()
+    final = r.read()
+    r.destroy()
+    for samples, got in ((1, hosts[0].array), (3, hosts[1].array), (6, hosts[2].array)):
+        s.samples = samples
+        want = lr.Renderer.create(ctx, sc, s)
+        want.finish()
+        assert np.array_equal(got, want.read()), samples
+        want.destroy()
+    assert np.array_equal(hosts[2].array, final)
+    for h in hosts:
+        h.close()
