@@ -50,6 +50,8 @@ constexpr uint32_t kPathBits = 23;
 constexpr uint32_t kPathMask = (1u << kPathBits) - 1u;
 constexpr uint32_t kMaxPool = 1u << kPathBits;             // 8,388,608 paths
 constexpr uint32_t kMaxSegments = 1u << (32 - kPathBits);  // 512 segments a pass
+// Rounds a pass traces beyond the bounces when the scene has cut-outs (loading.lucb:161).
+constexpr uint32_t kCutoutRounds = 8;
 
 // One member of a wave: everything its paths read, fixed while it is a member.
 struct Member {
@@ -78,7 +80,21 @@ struct Member {
     // A material of the member's has a specular, metal, coat or transmission lobe: its
     // surfaces take the layered OpenPBR shading (openpbr.cuh).
     uint32_t glossy;
+    // A material of the member's is a cut-out (geometry_opacity below 1), and the rounds
+    // its passes trace: its bounces + 1, + 8 for rays passing through cut-outs at the same
+    // bounce (integrator.lucb:806-808); a ray for a later round is not traced.
+    uint32_t cutouts, rounds;
 };
+
+// Cut-out opacity (shade_surface.comp:95-104): whether the ray passes through material
+// `material` at this hit, at random with probability 1 - opacity; the hit distance
+// decorrelates stacked layers. `u` is the path's opacity number for the bounce.
+__device__ __forceinline__ bool passes_through(const float4 *materials, uint32_t material, float t, float u) {
+    const float opacity = fminf(fmaxf(__ldg(&materials[material * 16u + 12u]).x, 0.0f), 1.0f);
+    if (!(opacity < 1.0f)) return false;
+    const float v = u + (float)hash_u32(__float_as_uint(t)) * (1.0f / 4294967296.0f);
+    return v - floorf(v) >= opacity;
+}
 
 // Splats add as 64-bit integers (units of 2^-32 of the film's terms), so their sum does
 // not depend on the order the connections arrive in.
@@ -225,7 +241,7 @@ __global__ void __launch_bounds__(kTraceBlock) closest_kernel(Wave w, uint32_t r
 // intersect_shadow.comp:28-92: unblocked light samples join their path's radiance; a light
 // path's camera connection, unless a light the camera sees stands in it, splats its value
 // (in the film's terms) on its pixel in the lane's accumulator.
-template <int W, int kStack, bool kCount>
+template <int W, int kStack, bool kCount, bool kCutouts>
 __global__ void __launch_bounds__(kTraceBlock) shadow_kernel(Wave w, uint32_t round) {
     __shared__ int stack[TracerOf<W, true, kStack, kCount>::kInts * kTraceBlock];
     const uint32_t count = w.counters[w.rounds + 1 + round];
@@ -246,12 +262,47 @@ __global__ void __launch_bounds__(kTraceBlock) shadow_kernel(Wave w, uint32_t ro
             if (seen) continue;
         }
         const DeviceScene s = m.scene;
-        if (tr.start(s, Ray{xyz(o), 0.0f, xyz(d), d.w})) {
-            while (!tr.step(s, overflow, visits)) {
+        float kept = 1.0f;
+        if (kCutouts && m.cutouts) {
+            // intersect_shadow.comp:70-91: on through the cut-outs it meets, keeping
+            // (1 - opacity) of the light at each; anything opaque blocks. Closest hits,
+            // on the same stack (a variant of its own: passes without cut-outs keep the
+            // leaner kernel).
+            typename TracerOf<W, false, kStack, kCount>::type walk(stack + threadIdx.x, kTraceBlock);
+            float3 from = xyz(o);
+            float remaining = d.w;
+            bool through = false;
+            for (int hop = 0; hop < 16 && kept > 0.0f; hop++) {
+                if (walk.start(s, Ray{from, 0.0f, xyz(d), remaining})) {
+                    while (!walk.step(s, overflow, visits)) {
+                    }
+                }
+                if (walk.h.slot < 0) {
+                    through = true;
+                    break;
+                }
+                const uint32_t material = __ldg(&s.shading[walk.h.slot]).w;
+                kept *= 1.0f - fminf(fmaxf(__ldg(&m.materials[material * 16u + 12u]).x, 0.0f), 1.0f);
+                if (kept < 1e-4f) kept = 0.0f;
+                const float3 p = from + xyz(d) * walk.h.t;
+                const float margin = 1e-4f * fmaxf(1.0f, fmaxf(fabsf(p.x), fmaxf(fabsf(p.y), fabsf(p.z))));
+                from = p + xyz(d) * margin;
+                remaining -= walk.h.t + margin;
+                if (remaining <= 0.0f) {
+                    through = kept > 0.0f;
+                    break;
+                }
             }
+            if (!through) continue;
+        } else {
+            if (tr.start(s, Ray{xyz(o), 0.0f, xyz(d), d.w})) {
+                while (!tr.step(s, overflow, visits)) {
+                }
+            }
+            if (tr.h.id >= 0) continue;
         }
-        if (tr.h.id >= 0) continue;
-        const float4 c = w.shadow_c[i];
+        float4 c = w.shadow_c[i];
+        if (kCutouts && m.cutouts) c = make_float4(c.x * kept, c.y * kept, c.z * kept, light_path ? c.w : c.w * kept);
         if (!light_path) {
             const uint32_t path = tag & kPathMask;
             w.radiance[path] = w.radiance[path] + c;
@@ -827,6 +878,14 @@ __device__ __noinline__ void shade_glossy(const Wave &w, const Member &m, uint32
     const float reach = length(vertex - p);
     const float density = (total == 0u ? mis.w : ray_pdf) * fabsf(dot(dir, geometric)) / (reach * reach);
     const float back_reach = mis.z / (reach * reach);
+    // A cut-out: pass straight through at the same bounce.
+    if (m.cutouts && passes_through(m.materials, material, hit.x, sample4(k.seed, pixel, sample, group_opacity(total)).x)) {
+        const float3 next = offset_origin(p, -geometric);
+        out.next = true;
+        out.o = make_float4(next.x, next.y, next.z, ro.w);
+        out.d = make_float4(dir.x, dir.y, dir.z, kInfinity);
+        return;
+    }
 
     const float4 emission_row = material_at(m, material, 7);
     if (emission_row.w > 0.0f) {
@@ -1017,6 +1076,14 @@ __device__ __forceinline__ void shade_one(const Wave &w, const Member &m, uint32
     // here toward the last vertex into that vertex's density (shade_surface.comp:91-94).
     const float density = (total == 0u ? mis.w : ray_pdf) * fabsf(dot(dir, geometric)) / (reach * reach);
     const float back_reach = mis.z / (reach * reach);
+    // A cut-out: pass straight through at the same bounce.
+    if (m.cutouts && passes_through(m.materials, material, hit.x, sample4(k.seed, pixel, sample, group_opacity(total)).x)) {
+        const float3 next = offset_origin(p, -geometric);
+        out.next = true;
+        out.o = make_float4(next.x, next.y, next.z, ro.w);
+        out.d = make_float4(dir.x, dir.y, dir.z, kInfinity);
+        return;
+    }
 
     const float4 emission_row = material_at(m, material, 7);
     if (emission_row.w > 0.0f) {
@@ -1183,6 +1250,14 @@ __device__ __noinline__ void shade_light(const Wave &w, const Member &m, uint32_
     const uint4 attributes = __ldg(&m.scene.shading[slot]);
     const uint32_t material = attributes.w;
     const float3 p = origin + hit.x * dir;
+    // A cut-out, as camera paths take it.
+    if (m.cutouts && passes_through(m.materials, attributes.w, hit.x, sample4(k.seed, id, sample, group_opacity(total)).x)) {
+        const float3 next = offset_origin(p, -geometric);
+        out.next = true;
+        out.o = make_float4(next.x, next.y, next.z, ro.w);
+        out.d = make_float4(dir.x, dir.y, dir.z, kInfinity);
+        return;
+    }
     if (total >= k.max_bounces) return;
     const float hu = hit.z, hv = hit.w;
     float3 normal = normalize(octahedral_decode(attributes.x) * (1.0f - hu - hv) + octahedral_decode(attributes.y) * hu +
@@ -1320,6 +1395,14 @@ __device__ __noinline__ void shade_light_glossy(const Wave &w, const Member &m, 
     if (back) geometric = -geometric;
     const uint4 attributes = __ldg(&m.scene.shading[slot]);
     const float3 p = origin + hit.x * dir;
+    // A cut-out, as camera paths take it.
+    if (m.cutouts && passes_through(m.materials, attributes.w, hit.x, sample4(k.seed, id, sample, group_opacity(total)).x)) {
+        const float3 next = offset_origin(p, -geometric);
+        out.next = true;
+        out.o = make_float4(next.x, next.y, next.z, ro.w);
+        out.d = make_float4(dir.x, dir.y, dir.z, kInfinity);
+        return;
+    }
     if (total >= k.max_bounces) return;
     float3 normal = normalize(octahedral_decode(attributes.x) * (1.0f - hit.z - hit.w) + octahedral_decode(attributes.y) * hit.z +
                               octahedral_decode(attributes.z) * hit.w);
@@ -1510,6 +1593,9 @@ __global__ void __launch_bounds__(kShadeBlock, kGlossy ? 4 : 8) shade_kernel(Wav
             } else {
                 shade_one<false, kTracing, kGlossy>(w, m, sg.sample, round, i, ro, out);
             }
+            // Past the member's last round (cut-outs passed at its last bounces) a ray is
+            // not traced, as the reference's pass loop ends there.
+            if (round + 1u >= m.rounds) out.next = false;
         }
         const uint32_t at = warp_push(next_counter, out.next);
         if (out.next) {
@@ -1814,8 +1900,8 @@ void mark(cudaStream_t stream, Marks *marks, int kind) {
 // (closest, shade, shadow) for every round. With `marks`, an event follows each kernel
 // (profiling); kCount instantiates the counting traversals.
 template <int W, int kStack, bool kCount>
-void record_trace(const WaveHost *h, const Wave &w, int grid_trace, bool tracing, bool glossy, cudaStream_t stream,
-                  Marks *marks) {
+void record_trace(const WaveHost *h, const Wave &w, int grid_trace, bool tracing, bool glossy, bool cutouts,
+                  cudaStream_t stream, Marks *marks) {
     camera_kernel<<<h->grid_shade, kShadeBlock, 0, stream>>>(w);
     mark(stream, marks, kCamera);
     for (uint32_t round = 0; round < w.rounds; round++) {
@@ -1835,7 +1921,8 @@ void record_trace(const WaveHost *h, const Wave &w, int grid_trace, bool tracing
             shade_kernel<false, false, false><<<h->grid_shade, kShadeBlock, 0, stream>>>(w, round);
         }
         mark(stream, marks, kSurface);
-        shadow_kernel<W, kStack, kCount><<<grid_trace, kTraceBlock, 0, stream>>>(w, round);
+        if (cutouts) shadow_kernel<W, kStack, kCount, true><<<grid_trace, kTraceBlock, 0, stream>>>(w, round);
+        else shadow_kernel<W, kStack, kCount, false><<<grid_trace, kTraceBlock, 0, stream>>>(w, round);
         mark(stream, marks, kShadow);
     }
     LR_CUDA(cudaGetLastError());
@@ -1871,20 +1958,22 @@ int grid_for(WaveHost *h, int variant) {
 }
 
 // A pass's variant: its traversal (BVH width * 1000 + stack entries), plus kTracingVariant
-// when it holds light tracing and kGlossyVariant when it holds glossy materials.
-constexpr int kTracingVariant = 100000, kGlossyVariant = 200000;
+// when it holds light tracing, kGlossyVariant when it holds glossy materials and
+// kCutoutVariant when it holds cut-outs.
+constexpr int kTracingVariant = 100000, kGlossyVariant = 200000, kCutoutVariant = 400000;
 
 void record_trace_any(WaveHost *h, const Wave &w, int variant, cudaStream_t stream, Marks *marks) {
     const bool count = h->profile == 2;
     const bool tracing = (variant / kTracingVariant) & 1;
     const bool glossy = (variant / kTracingVariant) & 2;
+    const bool cutouts = (variant / kTracingVariant) & 4;
     const int traversal = variant % kTracingVariant;
     const int grid = grid_for(h, traversal);
     switch (traversal) {
 #define LR_CASE(wd, k)                                                                        \
     case wd * 1000 + k:                                                                       \
-        if (count) record_trace<wd, k, true>(h, w, grid, tracing, glossy, stream, marks);     \
-        else record_trace<wd, k, false>(h, w, grid, tracing, glossy, stream, marks);          \
+        if (count) record_trace<wd, k, true>(h, w, grid, tracing, glossy, cutouts, stream, marks); \
+        else record_trace<wd, k, false>(h, w, grid, tracing, glossy, cutouts, stream, marks);      \
         break;
         LR_TRAVERSALS(LR_CASE)
 #undef LR_CASE
@@ -2059,8 +2148,11 @@ LightPaths light_paths_of(const lr_settings &settings, const lr_frame &frame, ui
 uint32_t member_add(WaveHost *h, const lr_gpu_scene *gs, lr_gpu_scene *owned, const lr_scene *scene,
                     const lr_settings &settings, const lr_frame &frame) {
     validate(settings, frame);
-    if (settings.max_bounces + 1 > h->rounds)
-        fail(LR_LIMIT, "this wave traces at most " + std::to_string(h->rounds - 1) + " bounces");
+    const uint32_t rounds = settings.max_bounces + 1 + (has_cutouts(*scene, settings) ? kCutoutRounds : 0);
+    if (rounds > h->rounds)
+        fail(LR_LIMIT, "this wave traces " + std::to_string(h->rounds) + " rounds a pass; the render needs " +
+                           std::to_string(rounds) + " (its bounces + 1, + " + std::to_string(kCutoutRounds) +
+                           " with cut-outs)");
     if (!gs->ctx || gs->ctx->device != h->ctx->device) fail(LR_INVALID, "the scene was uploaded to another device");
     auto free_slot = [&] {
         for (uint32_t i = 0; i < h->capacity; i++)
@@ -2164,6 +2256,8 @@ uint32_t member_add(WaveHost *h, const lr_gpu_scene *gs, lr_gpu_scene *owned, co
     m.splat_lane[0] = traced.count ? (unsigned long long *)at(p_splat_lane0) : nullptr;
     m.splat_lane[1] = traced.count ? (unsigned long long *)at(p_splat_lane1) : nullptr;
     m.glossy = L.glossy ? 1u : 0u;
+    m.cutouts = L.cutouts ? 1u : 0u;
+    m.rounds = rounds;
     std::memcpy(stage, &m, sizeof m);
     LR_CUDA(cudaMemcpyAsync(h->d_members + index, stage, sizeof m, cudaMemcpyHostToDevice, stream));
     h->staging.queued(stream);
@@ -2320,7 +2414,10 @@ bool launch_pass(WaveHost *h, bool dry = false, int only = -1) {
                                      [&](const std::pair<uint32_t, bool> &e) { return h->members[e.first].dev.light_paths != 0u; });
     const bool glossy = std::any_of(rec.members.begin(), rec.members.end(),
                                     [&](const std::pair<uint32_t, bool> &e) { return h->members[e.first].dev.glossy != 0u; });
-    const int variant = width * 1000 + stack + (tracing ? kTracingVariant : 0) + (glossy ? kGlossyVariant : 0);
+    const bool cutouts = std::any_of(rec.members.begin(), rec.members.end(),
+                                     [&](const std::pair<uint32_t, bool> &e) { return h->members[e.first].dev.cutouts != 0u; });
+    const int variant = width * 1000 + stack + (tracing ? kTracingVariant : 0) + (glossy ? kGlossyVariant : 0) +
+                        (cutouts ? kCutoutVariant : 0);
     staging->head = PlanHeader{n, used, converts, dry ? 1u : 0u, camera_paths, folds, 0u, 0u};
     cudaStream_t stream = lane.stream;
     // Member records queued on the context's stream reach this lane first.
@@ -2594,7 +2691,8 @@ void create(lr_context *ctx, const lr_scene *scene, const lr_settings &settings,
     int status = lr_gpu_scene_upload(ctx, scene, &gs);
     if (status != LR_OK) fail(status, lr_last_error());
     try {
-        wave_create(&r->wave, ctx, band + most_lights, settings.max_bounces + 1, 1, settings.profile);
+        const uint32_t rounds = settings.max_bounces + 1 + (has_cutouts(*scene, settings) ? kCutoutRounds : 0);
+        wave_create(&r->wave, ctx, band + most_lights, rounds, 1, settings.profile);
         member_add(&r->wave, gs, gs, scene, settings, frame);
         r->wave.fill = (uint32_t)std::min<uint64_t>(band + r->wave.members[0].dev.light_paths, r->wave.pool);
         r->wave.camera_cap = (uint32_t)band;
@@ -2604,7 +2702,8 @@ void create(lr_context *ctx, const lr_scene *scene, const lr_settings &settings,
             for (int li = 0; li < r->wave.lane_count; li++)
                 trace_graph(&r->wave, r->wave.lanes[li],
                             c.width * 1000 + c.stack + (r->wave.members[0].dev.light_paths ? kTracingVariant : 0) +
-                                (r->wave.members[0].dev.glossy ? kGlossyVariant : 0));
+                                (r->wave.members[0].dev.glossy ? kGlossyVariant : 0) +
+                                (r->wave.members[0].dev.cutouts ? kCutoutVariant : 0));
     } catch (...) {
         const bool owned = !r->wave.members.empty() && r->wave.members[0].used;
         wave_destroy(&r->wave);

@@ -306,17 +306,23 @@ void pack_material(const lr_openpbr &m, float program, std::vector<float> &out) 
 }
 
 // Materials this build shades: OpenPBR Surface's lobes (EON diffuse, GGX specular, F82
-// metal, coat, rough transmission, emission), opaque and, in the spectral build, without
+// metal, coat, rough transmission, emission), cut-outs and, in the spectral build, not
 // dispersion.
 void check_material(const lr_openpbr &m, size_t index, bool spectral) {
     auto bad = [&](const char *what) {
         fail(LR_INVALID, "material " + std::to_string(index) + ": " + what + " is not part of this build's shading");
     };
-    if (m.geometry_opacity < 1.0) bad("geometry_opacity below 1 (cut-outs)");
     if (spectral && m.transmission_weight > 0.0 && m.transmission_dispersion_scale > 0.0 &&
         m.transmission_dispersion_abbe_number > 0.0)
         bad("transmission dispersion");
     if (m.base_diffuse_roughness < 0.0 || m.base_diffuse_roughness > 1.0) bad("base_diffuse_roughness outside 0..1");
+}
+
+bool has_cutouts(const Scene &scene, const lr_settings &settings) {
+    if (settings.material.geometry_opacity < 1.0 && (scene.used.empty() || scene.used[0])) return true;
+    for (size_t i = 0; i < scene.materials.size(); i++)
+        if (scene.materials[i].geometry_opacity < 1.0 && (i + 1 >= scene.used.size() || scene.used[i + 1])) return true;
+    return false;
 }
 
 // Whether a material has a lobe besides EON diffuse (openpbr.glsl's HAS_COAT,
@@ -376,6 +382,7 @@ Loaded load(const Scene &scene, const lr_settings &settings) {
         if (i >= scene.used.size() || scene.used[i]) {
             check_material(L.library[i], i, settings.spectral != 0);
             L.glossy = L.glossy || is_glossy(L.library[i]);
+            L.cutouts = L.cutouts || L.library[i].geometry_opacity < 1.0;
         }
     L.radius = scene_radius(scene);
     L.lights = pack_lights(scene.lights, L.radius);

@@ -31,6 +31,7 @@ struct Loaded {
     std::vector<float> materials;     // 64 floats per material
     double radius = 1.0, p_distant = 0.0;
     bool glossy = false;              // a used material has more than EON diffuse
+    bool cutouts = false;             // a used material has geometry_opacity below 1
     // Light paths from afar (lights.glsl:283-308): the chance a light path starts at a
     // distant light with a size, and the disk it starts on (centre, radius) around what
     // casts caustics; share 0 when none do.
@@ -47,5 +48,8 @@ void pack_material(const lr_openpbr &m, float program, std::vector<float> &out);
 double scene_radius(const Scene &scene);
 Loaded load(const Scene &scene, const lr_settings &settings);
 bool casts_caustics(const lr_openpbr &m);
+// Whether a material the scene uses (the settings' default included) is a cut-out: its
+// passes trace 8 rounds more (loading.lucb:121-124, 161).
+bool has_cutouts(const Scene &scene, const lr_settings &settings);
 
 }  // namespace lr

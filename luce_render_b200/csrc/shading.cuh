@@ -89,6 +89,7 @@ __device__ __forceinline__ float4 sample4(uint32_t seed, uint32_t pixel, uint32_
 constexpr uint32_t kGroupCamera = 0, kGroupWavelength = 1;
 __device__ __forceinline__ uint32_t group_light(uint32_t b) { return 2u + 3u * b; }
 __device__ __forceinline__ uint32_t group_bsdf(uint32_t b) { return 3u + 3u * b; }
+__device__ __forceinline__ uint32_t group_opacity(uint32_t b) { return 4u + 3u * b; }
 
 // ---- common.glsl ---------------------------------------------------------------------
 

@@ -58,3 +58,42 @@ def colored_light_scene(color=(1.0, 0.4, 0.1), kelvin: float = 0.0):
     lamp = light(LIGHT_RECT, position=(0.0, 2.0, 0.0), rotation=(-0.5 * math.pi, 0.0, 0.0), color=color,
                  intensity=10.0, temperature=kelvin, width=2.0, height=2.0, normalize=True, visible=False)
     return [_floor()], [cam], [lamp], []
+
+
+def cutout_sphere_scene():
+    """integrator.lucb:170-192: a sphere emitting 3 nits at opacity one half, in the dark,
+    seen from (0, 1, 4) through 100 mm: half the rays stop at its front and see 3, a
+    quarter pass to its back face and see 3 there, so it shows 2.25. The sphere is this
+    package's icosphere (level 4); its material is the default, so the settings carry it
+    (cutout_material)."""
+    from .scenes import icosphere
+    p, t, n = icosphere(4, 1.0)
+    cam = camera((0.0, 1.0, 4.0), (-math.atan2(1.0, 4.0), 0.0, 0.0), focal_length=100.0, horizontal_aperture=36.0)
+    return [MeshData(p, t, normals=n)], [cam], [], []
+
+
+CUTOUT_SPHERE_EXPECTED = 2.25
+
+
+def cutout_material(opacity: float = 0.5, emission: float = 3.0) -> OpenPbr:
+    m = OpenPbr.lambert((0.0, 0.0, 0.0), emission=emission)
+    m.geometry_opacity = opacity
+    return m
+
+
+def veil_scene(opacity: float):
+    """integrator.lucb:292-333: the area light's floor under a 3 x 3 veil at height 0.5
+    (opacity `opacity`, base weight 0, library material 1), seen from below the veil at
+    (0, 0.3, 3): at opacity one half the floor under the light gets exactly half of what it
+    gets through a fully transparent veil (shadow rays walk through cut-outs keeping
+    1 - opacity, BSDF rays pass at random, MIS weighs both)."""
+    p, t, f = grid(3.0, 1)
+    veil = OpenPbr.lambert((0.8, 0.8, 0.8))
+    veil.base_weight = 0.0
+    veil.geometry_opacity = opacity
+    sheet = MeshData(p, t, faces=f, face_count=1, face_materials=[1], transform=placement((0.0, 0.5, 0.0)))
+    pitch = -math.atan2(0.3, 3.0)
+    cam = camera((0.0, 0.3, 3.0), (pitch, 0.0, 0.0), focal_length=200.0, horizontal_aperture=36.0)
+    lamp = light(LIGHT_RECT, position=(0.0, 1.0, 0.0), rotation=(-0.5 * math.pi, 0.0, 0.0), intensity=4.0,
+                 width=1.0, height=1.0, normalize=False, visible=False)
+    return [_floor(), sheet], [cam], [lamp], [veil]

@@ -534,6 +534,39 @@ static void spec_to_film(const or_render_desc *r, spec rad, const double lambda[
     for (int k = 0; k < 3; k++) out[k] = sum[k] * 0.25 / r->cmf_integrals[k];
 }
 
+/* Cut-out opacity (shade_surface.comp:95-104): whether a ray passes through material `m`
+ * at a hit at distance t (f32, as the kernels hold it), with the path's opacity number u. */
+static int passes_through(const or_render_desc *r, uint32_t m, float t, double u) {
+    double opacity = fmin(fmax(material(r, m, 12)[0], 0.0), 1.0);
+    if (!(opacity < 1.0)) return 0;
+    uint32_t bits;
+    memcpy(&bits, &t, 4);
+    double v = u + (double)or_hash_u32(bits) * (1.0 / 4294967296.0);
+    return v - floor(v) >= opacity;
+}
+
+/* intersect_shadow.comp:58-91: what of a shadow ray's light arrives: 1 unblocked, 0 when
+ * something opaque stands in it; through cut-outs (scenes with any), (1 - opacity) of it
+ * at each, walked with closest hits. */
+static double shadow_kept(const or_render_desc *r, d3 o, d3 d, double reach) {
+    double tt, uu, vv;
+    if (!r->through) return trace64(r, o, d, reach, 1, &tt, &uu, &vv) == NONE ? 1.0 : 0.0;
+    d3 from = o;
+    double remaining = reach, kept = 1.0;
+    for (int hop = 0; hop < 16; hop++) {
+        uint32_t slot = trace64(r, from, d, remaining, 0, &tt, &uu, &vv);
+        if (slot == NONE) return kept;
+        kept *= 1.0 - fmin(fmax(material(r, r->shading[slot * 4 + 3], 12)[0], 0.0), 1.0);
+        if (kept < 1e-4) return 0.0;
+        d3 p = add(from, mul(d, tt));
+        double margin = 1e-4 * fmax(1.0, fmax(fabs(p.x), fmax(fabs(p.y), fabs(p.z))));
+        from = add(p, mul(d, margin));
+        remaining -= tt + margin;
+        if (remaining <= 0.0) return kept;
+    }
+    return 0.0;
+}
+
 /* One sample of one pixel: its ACEScg value. */
 static void render_sample(const or_render_desc *r, uint32_t pixel, uint32_t sample, double out[3], uint64_t rays[2]) {
     const float *f = r->frame;
@@ -568,7 +601,7 @@ static void render_sample(const or_render_desc *r, uint32_t pixel, uint32_t samp
     const int tracing = r->light_paths > 0;
     double mis[4] = {0, 0, 0, 0};
     if (tracing) mis[0] = (double)r->light_paths, mis[3] = camera_pdf(r, dir);
-    for (uint32_t round = 0; round <= r->max_bounces; round++) {
+    for (uint32_t round = 0; round < r->max_bounces + 1 + r->through; round++) {
         uint32_t total = bounces & 0xffu;
         double t, hu = 0, hv = 0;
         uint32_t what = trace64(r, origin, dir, INF, 0, &t, &hu, &hv);
@@ -634,6 +667,15 @@ static void render_sample(const or_render_desc *r, uint32_t pixel, uint32_t samp
          * toward the last vertex into that vertex's density (shade_surface.comp:91-94). */
         double density = (total == 0 ? mis[3] : ray_pdf) * fabs(dot(dir, geometric)) / (reach * reach);
         double back_reach = mis[2] / (reach * reach);
+        if (r->through) {
+            /* A cut-out: pass straight through at the same bounce. */
+            double uo[4];
+            or_sample4(r->seed, pixel, sample, 4 + 3 * total, uo);
+            if (passes_through(r, m, (float)t, uo[0])) {
+                origin = offset_origin(p, neg(geometric));
+                continue;
+            }
+        }
         const float *em = material(r, m, 7);
         if (em[3] > 0.0f) {
             double weight = 1.0;
@@ -736,11 +778,9 @@ static void render_sample(const or_render_desc *r, uint32_t pixel, uint32_t samp
                     d3 target = add(p, mul(s.direction, s.distance));
                     double margin = 4e-4 * fmax(1.0, fmax(fabs(target.x), fmax(fabs(target.y), fabs(target.z))));
                     double sreach = s.distance >= INF ? INF : fmax(0.0, s.distance - margin);
-                    double tt, uu, vv;
                     rays[1]++;
-                    if (trace64(r, offset_origin(p, side > 0.0 ? geometric : neg(geometric)), s.direction, sreach, 1, &tt,
-                                &uu, &vv) == NONE)
-                        radiance = spec_add(radiance, c);
+                    double kept = shadow_kept(r, offset_origin(p, side > 0.0 ? geometric : neg(geometric)), s.direction, sreach);
+                    if (kept > 0.0) radiance = spec_add(radiance, spec_scale(c, kept));
                 }
             }
         }
@@ -915,7 +955,7 @@ static void trace_light_path(const or_render_desc *r, uint32_t sample, uint32_t 
         mis[0] = 1.0, mis[1] = point_pdf, mis[2] = cos_n, mis[3] = -1.0;
     }
     uint32_t bounces = 0;
-    for (uint32_t round = 0; round <= r->max_bounces; round++) {
+    for (uint32_t round = 0; round < r->max_bounces + 1 + r->through; round++) {
         uint32_t total = bounces & 0xffu;
         double t, hu = 0, hv = 0;
         uint32_t what = trace64(r, origin, dir, INF, 0, &t, &hu, &hv);
@@ -937,6 +977,14 @@ static void trace_light_path(const or_render_desc *r, uint32_t sample, uint32_t 
         const uint32_t *attr = &r->shading[slot * 4];
         uint32_t m = attr[3];
         d3 p = add(origin, mul(dir, t));
+        if (r->through) {
+            double uo[4];
+            or_sample4(r->seed, id, sample, 4 + 3 * total, uo);
+            if (passes_through(r, m, (float)t, uo[0])) {
+                origin = offset_origin(p, neg(geometric));
+                continue;
+            }
+        }
         if (total >= r->max_bounces) return;
         d3 normal = norm(add(add(mul(oct_decode(attr[0]), 1.0 - hu - hv), mul(oct_decode(attr[1]), hu)), mul(oct_decode(attr[2]), hv)));
         if (dot(normal, geometric) < 0.0) normal = neg(normal);
@@ -992,11 +1040,11 @@ static void trace_light_path(const or_render_desc *r, uint32_t sample, uint32_t 
                     for (uint32_t l = 0; l < r->light_count && !blocked; l++)
                         if (light_visible(r, l) && intersect_light(r, l, so, to_camera, sreach, 1) < sreach) blocked = 1;
                     if (!blocked) {
-                        double tt, uu, vv;
                         rays[1]++;
-                        if (trace64(r, so, to_camera, sreach, 1, &tt, &uu, &vv) == NONE) {
+                        double kept = shadow_kept(r, so, to_camera, sreach);
+                        if (kept > 0.0) {
                             double v[3];
-                            spec_to_film(r, spec_scale(contribution, weight), lambda, v);
+                            spec_to_film(r, spec_scale(contribution, weight * kept), lambda, v);
                             if (isfinite(v[0]) && isfinite(v[1]) && isfinite(v[2]))
                                 for (int k = 0; k < 3; k++) splat[pixel * 3 + k] += v[k];
                         }

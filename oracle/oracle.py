@@ -373,7 +373,7 @@ class RenderDesc(C.Structure):
                 ("height", C.c_uint32), ("max_bounces", C.c_uint32), ("spectral", C.c_uint32), ("seed", C.c_uint32),
                 ("limits", C.c_double * 3), ("clamp", C.c_double), ("light_paths", C.c_uint32),
                 ("light_band", C.c_uint32), ("pixel_area_inv", C.c_double), ("emit_share", C.c_double),
-                ("emit_radius", C.c_double), ("emit_center", C.c_double * 3)]
+                ("emit_radius", C.c_double), ("emit_center", C.c_double * 3), ("through", C.c_uint32)]
 
 
 def render(arrays: dict, lights, library, frame, samples: int, max_bounces: int, spectral: bool, seed: int = 1,
@@ -520,6 +520,10 @@ def _render_desc(arrays, lights, library, frame, max_bounces, spectral, seed, ba
     r.spectral = 1 if spectral else 0
     r.seed = seed
     r.limits[:] = [float(x) for x in limits]
+    # Cut-outs (loading.lucb:121-124, 161): 8 rounds more when a material the triangles
+    # use has geometry_opacity below 1.
+    used = set(int(x) for x in np.asarray(shading, np.uint32).reshape(-1, 4)[:, 3]) if T else set()
+    r.through = 8 if any(i < len(mats) and mats[i].geometry_opacity < 1.0 for i in used) else 0
     # Light paths from afar (loading.lucb:127-146): distant lights with a size share light
     # paths with the tree's emitters by power, on a disk around what casts caustics.
     sized = any(row[3] == 3.0 and row[11] < np.float32(1.0) - np.float32(1e-7) for row in rows.reshape(-1, 28))

@@ -44,6 +44,9 @@ typedef struct {
     /* Light paths from afar (lights.glsl:283-308): their share of light paths and the disk
      * they start on, facing the light (radius, centre); share 0 for none. */
     double emit_share, emit_radius, emit_center[3];
+    /* Rounds beyond the bounces for rays passing through cut-outs (8 when a material the
+     * triangles use has geometry_opacity below 1, else 0). */
+    uint32_t through;
 } or_render_desc;
 
 void or_render(const or_render_desc *r, uint32_t samples, double *mean, double *var, int threads);

@@ -1,6 +1,6 @@
 """Render cases shared by the batch and server tests: (compiled scene, settings) pairs of
-uneven sizes, spectral and RGB, depths 2 to 8, Lambertian and glossy, with and without
-light tracing, and the image a Renderer makes of each."""
+uneven sizes, spectral and RGB, depths 2 to 8, Lambertian, glossy and cut-out, with and
+without light tracing, and the image a Renderer makes of each."""
 import luce_render_b200 as lr
 from luce_render_b200 import scenes, testscenes
 
@@ -46,6 +46,10 @@ def cases():
     glossy_traced = settings(28, 24, 2, 5, True, seed=19)
     glossy_traced.light_tracing = 0.5
     out.append((sc, glossy_traced))
+    # Cut-outs: 8 rounds more than the bounces, shadow rays walking through the veil.
+    meshes, cams, lights, mats = testscenes.veil_scene(0.5)
+    sc = lr.compile_scene(meshes, cams, lights, mats)
+    out.append((sc, settings(24, 24, 4, 2, False, seed=23, material=lr.OpenPbr.lambert((0.5, 0.5, 0.5)))))
     return out
 
 

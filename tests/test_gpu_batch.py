@@ -33,7 +33,8 @@ def test_members_equal_their_renderers(ctx, cases, pool):
     # A pool larger than all films together (one pass a sample for everyone), one that
     # splits the larger films over passes, and one smaller than every film but the last.
     cs, uploads, alone = cases
-    b = lr.Batch(ctx, lr.BatchSettings.default(pool=pool, max_bounces=8, capacity=8))
+    # 12 bounces of room: 11 rounds for the cut-out case (2 bounces + 1 + 8).
+    b = lr.Batch(ctx, lr.BatchSettings.default(pool=pool, max_bounces=12, capacity=16))
     try:
         members = [b.add(gs, sc, s) for gs, (sc, s) in zip(uploads, cs)]
         b.finish()
@@ -111,7 +112,7 @@ def test_batch_limits(ctx, cases):
 
 def test_tuning_changes_speed_not_images(ctx, cases):
     cs, uploads, alone = cases
-    b = lr.Batch(ctx, lr.BatchSettings.default(pool=2048, max_bounces=8, capacity=8))
+    b = lr.Batch(ctx, lr.BatchSettings.default(pool=2048, max_bounces=12, capacity=16))
     try:
         members = [b.add(gs, sc, s) for gs, (sc, s) in zip(uploads, cs)]
         for _ in range(3):

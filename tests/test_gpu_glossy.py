@@ -18,7 +18,7 @@ import numpy as np
 import pytest
 
 import luce_render_b200 as lr
-from luce_render_b200 import scenes
+from luce_render_b200 import scenes, testscenes
 from oracle import oracle as orc
 
 pytestmark = pytest.mark.gpu
@@ -161,3 +161,39 @@ def test_gpu_matches_f64_oracle_light_paths_from_afar(ctx, spectral):
     assert np.mean(relative < 1e-3) >= 0.95, np.mean(relative < 1e-3)
     # The light paths from afar carry part of the image (the caustic under the ball).
     assert (mean - camera_part).sum() / mean.sum() > 0.02
+
+
+@pytest.mark.parametrize("spectral", [False, True])
+def test_cutouts(ctx, spectral):
+    # integrator.lucb:170-192: the half-transparent emitting sphere in the dark shows 2.25
+    # (the reference's tolerance 0.05).
+    meshes, cams, lights, mats = testscenes.cutout_sphere_scene()
+    sc = lr.compile_scene(meshes, cams, lights, mats)
+    img = _render(ctx, sc, 32, 32, 256, 8, spectral, material=testscenes.cutout_material())
+    center = img[12:20, 12:20, 1].mean()
+    assert abs(center - testscenes.CUTOUT_SPHERE_EXPECTED) <= 0.05, center
+    # integrator.lucb:292-333: a veil at opacity one half passes half the light (0.015).
+    means = []
+    for opacity in (0.5, 0.0):
+        meshes, cams, lights, mats = testscenes.veil_scene(opacity)
+        sc = lr.compile_scene(meshes, cams, lights, mats)
+        img = _render(ctx, sc, 32, 32, 256, 1, spectral, material=lr.OpenPbr.lambert((0.5, 0.5, 0.5)))
+        means.append(img[14:18, 14:18, 1].mean())
+    assert abs(means[0] / means[1] - 0.5) <= 0.015, means
+
+
+def test_cutouts_match_f64_oracle(ctx):
+    # The veil over the floor at depth 3 (rays pass through at the same bounce, shadow rays
+    # walk through), with light tracing: 8x8-block means within 3 sigma of the oracle's.
+    meshes, cams, lights, mats = testscenes.veil_scene(0.5)
+    sc = lr.compile_scene(meshes, cams, lights, mats)
+    w, h, spp = 48, 32, 32
+    base = lr.OpenPbr.lambert((0.5, 0.5, 0.5))
+    for tracing in (0.0, 0.5):
+        img = _render(ctx, sc, w, h, spp, 3, False, material=base, tracing=tracing)
+        frame = lr.ray_frame(sc.camera(), w, h)
+        mean, var = orc.render(sc.arrays(), lights, [base] + mats, frame, spp, 3, False, light_tracing=tracing)
+        g = _blocks(img[..., :3].astype(np.float64), 8).mean((1, 3))
+        o = _blocks(mean, 8).mean((1, 3))
+        sem = np.sqrt(_blocks(var, 8).mean((1, 3)) / (64 * spp))
+        assert np.all(np.abs(g - o) <= 3.0 * sem + 1e-6), (tracing, np.max(np.abs(g - o) / (sem + 1e-12)))

@@ -155,11 +155,12 @@ def test_renderer_api_progress_and_errors(ctx):
     # Camera paths alone: light paths' sampler numbers follow the band, so an image with
     # light tracing depends on the pool size (as the reference's does).
     s.light_tracing = 0.0
-    cutout = lr.OpenPbr.lambert()
-    cutout.geometry_opacity = 0.5
-    s.c.material = cutout
+    dispersive = lr.OpenPbr.lambert()
+    dispersive.transmission_weight = 1.0
+    dispersive.transmission_dispersion_scale = 1.0
+    s.c.material = dispersive
     with pytest.raises(lr.RenderError) as e:
-        lr.Renderer.create(ctx, sc, s)  # cut-outs are not part of this build
+        lr.Renderer.create(ctx, sc, s)  # spectral dispersion is not part of this build
     assert e.value.code == 400
     s.c.material = lr.OpenPbr.lambert()
     s.pool = 1000  # bands of 1,000 paths: 4 passes a sample

@@ -39,7 +39,7 @@ def test_results_same_alone_and_in_the_mix(ctx):
     biggest_scene = max(_upload_estimate(sc) for sc, _ in cs)
     biggest_session = max(s.c.width * s.c.height * 32 + (1 << 20) for _, s in cs)
     budget = wave + biggest_scene + biggest_session
-    server = lr.Server(lr.ServerSettings.default(budget_bytes=budget, capacity=2, pool=pool, max_bounces=8))
+    server = lr.Server(lr.ServerSettings.default(budget_bytes=budget, capacity=2, pool=pool, max_bounces=12))
     try:
         ids = [server.add_scene(sc) for sc, _ in cs]
         renders, probes = [], []

@@ -17,7 +17,7 @@ import numpy as np
 import pytest
 
 import luce_render_b200 as lr
-from luce_render_b200 import scenes
+from luce_render_b200 import scenes, testscenes
 from oracle import oracle as orc
 
 
@@ -124,3 +124,22 @@ def test_oracle_light_paths_from_afar():
     plain = [scenes.openpbr(base_color=(0.8, 0.8, 0.8), specular_weight=0.0)] * 3
     job = orc.RenderJob(sc.arrays(), lights, [lr.OpenPbr.lambert()] + plain, frame, 6, False, light_tracing=0.5)
     assert job.light_paths == 0 and job.desc.emit_share == 0.0
+
+
+def test_oracle_cutouts():
+    # integrator.lucb:170-192: the half-transparent emitting sphere shows 2.25.
+    meshes, cams, lights, mats = testscenes.cutout_sphere_scene()
+    sc = lr.compile_scene(meshes, cams, lights, mats)
+    frame = lr.ray_frame(sc.camera(), 32, 32)
+    mean, var = orc.render(sc.arrays(), lights, [testscenes.cutout_material()], frame, 64, 8, False)
+    center = mean[12:20, 12:20, 1].mean()
+    assert abs(center - testscenes.CUTOUT_SPHERE_EXPECTED) <= 0.05, center
+    # integrator.lucb:292-333: a veil at opacity one half passes half the light.
+    means = []
+    for opacity in (0.5, 0.0):
+        meshes, cams, lights, mats = testscenes.veil_scene(opacity)
+        sc = lr.compile_scene(meshes, cams, lights, mats)
+        frame = lr.ray_frame(sc.camera(), 32, 32)
+        mean, _ = orc.render(sc.arrays(), lights, [lr.OpenPbr.lambert((0.5, 0.5, 0.5))] + mats, frame, 128, 1, False)
+        means.append(mean[14:18, 14:18, 1].mean())
+    assert abs(means[0] / means[1] - 0.5) <= 0.015, means
