@@ -112,9 +112,9 @@ typedef struct {
 
 /* OpenPBR Surface parameters (src/render/materials.lucb:17-53), shaded as
  * shaders/openpbr.glsl does: EON diffuse, GGX specular, F82-tint metal, coat, rough
- * transmission, emission. Not shaded: geometry_opacity below 1 (cut-outs) and, in the
- * spectral build, transmission dispersion (rejected with 400); thin_walled is accepted
- * and, as in the reference's kernels, changes nothing. */
+ * transmission with dispersion (spectral build), emission, cut-out opacity.
+ * base_diffuse_roughness outside 0..1 is rejected with 400; thin_walled is accepted and,
+ * as in the reference's kernels, changes nothing. */
 typedef struct {
     double base_weight, base_color[3], base_metalness, base_diffuse_roughness;
     double specular_weight, specular_color[3], specular_roughness, specular_roughness_anisotropy,

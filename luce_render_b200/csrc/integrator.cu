@@ -810,7 +810,7 @@ __device__ __noinline__ void shade_glossy(const Wave &w, const Member &m, uint32
     const float ray_pdf = __uint_as_float(pu.w);
     const float3 origin = xyz(ro), dir = xyz(rd);
     float4 throughput = w.throughput[path];
-    const float4 lambda = kSpectral ? w.lambda[path] : make_float4(0.0f, 0.0f, 0.0f, 0.0f);
+    float4 lambda = kSpectral ? w.lambda[path] : make_float4(0.0f, 0.0f, 0.0f, 0.0f);
     float4 radiance = w.radiance[path];
     const bool tracing = m.light_paths != 0u;
     const float4 mis = tracing ? w.mis[path] : make_float4(0.0f, 0.0f, 0.0f, 0.0f);
@@ -886,6 +886,15 @@ __device__ __noinline__ void shade_glossy(const Wave &w, const Member &m, uint32
         out.d = make_float4(dir.x, dir.y, dir.z, kInfinity);
         return;
     }
+    // A dispersive material ends the secondary wavelengths (openpbr.glsl:182-194): the
+    // hero carries the sample, and dispersive indices are taken at it from then on.
+    if (kSpectral && material_at(m, material, 12).w != 0.0f && lambda.y >= 0.0f) {
+        throughput = make_float4(throughput.x * 4.0f, 0.0f, 0.0f, 0.0f);
+        radiance = make_float4(radiance.x * 4.0f, 0.0f, 0.0f, 0.0f);
+        lambda = make_float4(lambda.x, -lambda.y, -lambda.z, -lambda.w);
+        w.lambda[path] = lambda;
+    }
+    const float hero = kSpectral && lambda.y < 0.0f ? lambda.x : 0.0f;
 
     const float4 emission_row = material_at(m, material, 7);
     if (emission_row.w > 0.0f) {
@@ -928,14 +937,14 @@ __device__ __noinline__ void shade_glossy(const Wave &w, const Member &m, uint32
                 if (tracing && !s.delta && nee_emitter != kNone && density > 0.0f) {
                     const float d2 = s.distance * s.distance;
                     const float at_last =
-                        total == 0u ? 1.0f : light_sampler_pdf(surface, s.direction, -dir, m.materials) * back_reach / mis.y;
+                        total == 0u ? 1.0f : light_sampler_pdf(surface, s.direction, -dir, m.materials, hero) * back_reach / mis.y;
                     const float at_vertex = emission_direction_pdf(m, nee_emitter, s.cos_light) * fabsf(side) / d2 / density;
                     const float at_light = emitter_area_pdf(m, nee_emitter) / (bsdf_pdf * s.cos_light / d2);
                     traced = mis.x * at_last * at_vertex * at_light;
                 }
                 if (tracing && afar != kNone && emits_from_afar(lights, afar) && density > 0.0f) {
                     const float at_last =
-                        total == 0u ? 1.0f : light_sampler_pdf(surface, s.direction, -dir, m.materials) * back_reach / mis.y;
+                        total == 0u ? 1.0f : light_sampler_pdf(surface, s.direction, -dir, m.materials, hero) * back_reach / mis.y;
                     const float at_vertex = afar_first_density(k, p, s.direction, fabsf(side)) / density;
                     const float at_light = afar_emission_pdf(m, afar, s.direction) / bsdf_pdf;
                     traced = mis.x * at_last * at_vertex * at_light;
@@ -979,7 +988,7 @@ __device__ __noinline__ void shade_glossy(const Wave &w, const Member &m, uint32
     const float3 next = side > 0.0f ? from : offset_origin(p, -geometric);
     if (tracing) {
         const float at_last =
-            total == 0u ? 1.0f : light_sampler_pdf(surface, direction, -dir, m.materials) * back_reach / mis.y;
+            total == 0u ? 1.0f : light_sampler_pdf(surface, direction, -dir, m.materials, hero) * back_reach / mis.y;
         w.mis[path] = make_float4(mis.x * at_last, density, fabsf(side), 0.0f);
     }
     w.path[path] = make_uint4(pixel, next_bounces, octahedral_encode(normal), __float_as_uint(pdf));
@@ -1382,7 +1391,7 @@ __device__ __noinline__ void shade_light_glossy(const Wave &w, const Member &m, 
     const float ray_pdf = __uint_as_float(pu.w);
     const float3 origin = xyz(ro), dir = xyz(rd);
     float4 throughput = w.throughput[path];
-    const float4 lambda = kSpectral ? w.lambda[path] : make_float4(0.0f, 0.0f, 0.0f, 0.0f);
+    float4 lambda = kSpectral ? w.lambda[path] : make_float4(0.0f, 0.0f, 0.0f, 0.0f);
     const float4 vertex_row = w.vertex[path];
     const float4 mis = w.mis[path];
     const uint32_t id = 0x80000000u | (m.light_band + tag_light_index(w, tag));
@@ -1404,6 +1413,12 @@ __device__ __noinline__ void shade_light_glossy(const Wave &w, const Member &m, 
         return;
     }
     if (total >= k.max_bounces) return;
+    // Dispersion ends the secondary wavelengths, as on camera paths.
+    if (kSpectral && material_at(m, attributes.w, 12).w != 0.0f && lambda.y >= 0.0f) {
+        throughput = make_float4(throughput.x * 4.0f, 0.0f, 0.0f, 0.0f);
+        lambda = make_float4(lambda.x, -lambda.y, -lambda.z, -lambda.w);
+        w.lambda[path] = lambda;
+    }
     float3 normal = normalize(octahedral_decode(attributes.x) * (1.0f - hit.z - hit.w) + octahedral_decode(attributes.y) * hit.z +
                               octahedral_decode(attributes.z) * hit.w);
     if (dot(normal, geometric) < 0.0f) normal = -normal;
@@ -1415,7 +1430,7 @@ __device__ __noinline__ void shade_light_glossy(const Wave &w, const Member &m, 
     const bool on_film = camera_pixel(m, p, lens, pixel, to_point, camera_distance);
     Surface lit = surface_at(normal, geometric, attributes.w, back);
     const float3 toward_light = -dir;
-    read_material(lit, m.materials);
+    read_material(lit, m.materials, kSpectral && lambda.y < 0.0f ? lambda.x : 0.0f);
     read_colors<kSpectral>(lit, m.materials, lambda);
     const float3 x_last = xyz(vertex_row);
     const float reach = length(x_last - p);

@@ -306,15 +306,11 @@ void pack_material(const lr_openpbr &m, float program, std::vector<float> &out) 
 }
 
 // Materials this build shades: OpenPBR Surface's lobes (EON diffuse, GGX specular, F82
-// metal, coat, rough transmission, emission), cut-outs and, in the spectral build, not
-// dispersion.
+// metal, coat, rough transmission with dispersion, emission) and cut-outs.
 void check_material(const lr_openpbr &m, size_t index, bool spectral) {
     auto bad = [&](const char *what) {
         fail(LR_INVALID, "material " + std::to_string(index) + ": " + what + " is not part of this build's shading");
     };
-    if (spectral && m.transmission_weight > 0.0 && m.transmission_dispersion_scale > 0.0 &&
-        m.transmission_dispersion_abbe_number > 0.0)
-        bad("transmission dispersion");
     if (m.base_diffuse_roughness < 0.0 || m.base_diffuse_roughness > 1.0) bad("base_diffuse_roughness outside 0..1");
 }
 

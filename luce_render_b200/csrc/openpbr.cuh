@@ -231,8 +231,15 @@ __device__ __forceinline__ float rgb_luma(float3 c) {
     return c.x * 0.2722287168f + c.y * 0.6740817658f + c.z * 0.0536895174f;
 }
 
-// read_material (openpbr.glsl:264-320) without node graphs or dispersion.
-__device__ __forceinline__ void read_material(Surface &s, const float4 *materials) {
+// Cauchy's index at `lambda` nm through `ior` at 587.6 nm (openpbr.glsl:177-180).
+__device__ __forceinline__ float dispersed_ior(float ior, float b, float lambda) {
+    return ior + b * (1.0f / (lambda * lambda) - 1.0f / (587.6f * 587.6f));
+}
+
+// read_material (openpbr.glsl:264-320) without node graphs. `hero`: the path's hero
+// wavelength once a dispersive hit has ended the others (0 before), at which a
+// dispersive material's index is taken.
+__device__ __forceinline__ void read_material(Surface &s, const float4 *materials, float hero = 0.0f) {
     const float4 *row = materials + (size_t)s.material * 16u;
     const float4 base_rgb = __ldg(&row[1]), specular_rgb = __ldg(&row[3]), coat_rgb = __ldg(&row[5]);
     const float4 transmission_rgb = __ldg(&row[9]), scalars = __ldg(&row[10]), indices = __ldg(&row[11]);
@@ -253,7 +260,8 @@ __device__ __forceinline__ void read_material(Surface &s, const float4 *material
     const float c4 = s.coat_roughness * s.coat_roughness * s.coat_roughness * s.coat_roughness;
     s.roughness = mixf(roughness, fminf(1.0f, powf(r4 + 2.0f * c4, 0.25f)), s.coat);
     s.alpha = ggx_alpha(s.roughness, fminf(fmaxf(scalars.w, 0.0f), 1.0f));
-    const float eta = fmaxf(indices.x, 1.0001f);
+    float eta = fmaxf(indices.x, 1.0001f);
+    if (geometry.w != 0.0f && hero > 0.0f) eta = fmaxf(dispersed_ior(eta, geometry.w, hero), 1.0001f);
     float relative = eta / s.coat_eta;
     if (relative < 1.0f) relative = 1.0f / relative;
     s.ior = fmaxf(mixf(eta, relative, s.coat), 1.0001f);
@@ -341,7 +349,7 @@ __device__ __forceinline__ void read_colors(Surface &s, const float4 *materials,
 
 template <bool kSpectral>
 __device__ __forceinline__ void prepare_surface(Surface &s, float3 wo, float4 lambda, const float4 *materials) {
-    read_material(s, materials);
+    read_material(s, materials, kSpectral && lambda.y < 0.0f ? lambda.x : 0.0f);
     orient_lobes(s, wo);
     read_colors<kSpectral>(s, materials, lambda);
     update_substrate(s);
@@ -469,12 +477,13 @@ __device__ __forceinline__ bool sample_direction(const Surface &s, float3 wo, fl
 // when the light path arrived from `from` (world, unit, both leaving the point): the
 // surface (read) seen from `from`'s side, choosing lobes by light_lobes; zero where the
 // sampler would reject `to`.
-__device__ __forceinline__ float light_sampler_pdf(const Surface &s, float3 from, float3 to, const float4 *materials) {
+__device__ __forceinline__ float light_sampler_pdf(const Surface &s, float3 from, float3 to, const float4 *materials,
+                                                  float hero) {
     const bool same = dot(from, s.geometric) >= 0.0f;
     Surface v = same ? s : turned(s);
     const float3 wo = to_local(v, from), wi = to_local(v, to);
     if ((dot(to, v.geometric) > 0.0f) != (wi.z > 0.0f)) return 0.0f;
-    if (!same) read_material(v, materials);
+    if (!same) read_material(v, materials, hero);
     light_lobes(v);
     return surface_pdf(v, wi, wo);
 }

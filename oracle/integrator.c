@@ -676,6 +676,14 @@ static void render_sample(const or_render_desc *r, uint32_t pixel, uint32_t samp
                 continue;
             }
         }
+        /* A dispersive material ends the secondary wavelengths; the hero carries the sample
+         * (openpbr.glsl:182-194). */
+        if (r->spectral && material(r, m, 12)[3] != 0.0f && lambda[1] >= 0.0) {
+            throughput.s[0] *= 4.0, throughput.s[1] = throughput.s[2] = throughput.s[3] = 0.0;
+            radiance.s[0] *= 4.0, radiance.s[1] = radiance.s[2] = radiance.s[3] = 0.0;
+            lambda[1] = -lambda[1], lambda[2] = -lambda[2], lambda[3] = -lambda[3];
+        }
+        const double hero = r->spectral && lambda[1] < 0.0 ? lambda[0] : 0.0;
         const float *em = material(r, m, 7);
         if (em[3] > 0.0f) {
             double weight = 1.0;
@@ -759,7 +767,7 @@ static void render_sample(const or_render_desc *r, uint32_t pixel, uint32_t samp
                     if (tracing && !s.delta && nee_emitter != NONE && density > 0.0) {
                         double d2 = s.distance * s.distance;
                         double at_last = total == 0 ? 1.0
-                                                    : or_light_sampler_pdf(&surface, r->materials, s.direction, neg(dir)) *
+                                                    : or_light_sampler_pdf(&surface, r->materials, s.direction, neg(dir), hero) *
                                                           back_reach / mis[1];
                         double at_vertex = emission_direction_pdf(r, nee_emitter, s.cos_light) * fabs(side) / d2 / density;
                         double at_light = emitter_area_pdf(r, nee_emitter) / (bsdf_pdf * s.cos_light / d2);
@@ -767,7 +775,7 @@ static void render_sample(const or_render_desc *r, uint32_t pixel, uint32_t samp
                     }
                     if (tracing && afar != NONE && emits_from_afar(r, afar) && density > 0.0) {
                         double at_last = total == 0 ? 1.0
-                                                    : or_light_sampler_pdf(&surface, r->materials, s.direction, neg(dir)) *
+                                                    : or_light_sampler_pdf(&surface, r->materials, s.direction, neg(dir), hero) *
                                                           back_reach / mis[1];
                         double at_vertex = afar_first_density(r, p, s.direction, fabs(side)) / density;
                         double at_light = afar_emission_pdf(r, afar, s.direction) / bsdf_pdf;
@@ -810,7 +818,7 @@ static void render_sample(const or_render_desc *r, uint32_t pixel, uint32_t samp
             /* This vertex's factor of the light tracer's density, settled now that the light
              * sampler's direction here is known (shade_surface.comp:304-307). */
             double at_last = total == 0 ? 1.0
-                                        : or_light_sampler_pdf(&surface, r->materials, direction, neg(dir)) * back_reach / mis[1];
+                                        : or_light_sampler_pdf(&surface, r->materials, direction, neg(dir), hero) * back_reach / mis[1];
             mis[0] *= at_last;
             mis[1] = density;
             mis[2] = fabs(side);
@@ -986,6 +994,11 @@ static void trace_light_path(const or_render_desc *r, uint32_t sample, uint32_t 
             }
         }
         if (total >= r->max_bounces) return;
+        /* Dispersion ends the secondary wavelengths, as on camera paths. */
+        if (r->spectral && material(r, m, 12)[3] != 0.0f && lambda[1] >= 0.0) {
+            throughput.s[0] *= 4.0, throughput.s[1] = throughput.s[2] = throughput.s[3] = 0.0;
+            lambda[1] = -lambda[1], lambda[2] = -lambda[2], lambda[3] = -lambda[3];
+        }
         d3 normal = norm(add(add(mul(oct_decode(attr[0]), 1.0 - hu - hv), mul(oct_decode(attr[1]), hu)), mul(oct_decode(attr[2]), hv)));
         if (dot(normal, geometric) < 0.0) normal = neg(normal);
         double ul[4];
@@ -999,7 +1012,7 @@ static void trace_light_path(const or_render_desc *r, uint32_t sample, uint32_t 
          * next vertex on that side, it is only oriented (light_paths.glsl:93-96). */
         or_surface lit = or_surface_at(normal, geometric, m, back);
         d3 toward_light = neg(dir);
-        or_read_material(&lit, r->materials);
+        or_read_material(&lit, r->materials, r->spectral && lambda[1] < 0.0 ? lambda[0] : 0.0);
         or_read_colors(&lit, r->materials, (int)r->spectral, lambda);
         double reach = len(sub(vertex, p));
         double cos_in = fabs(dot(dir, geometric));

@@ -224,7 +224,7 @@ or_surface or_surface_at(d3 normal, d3 geometric, uint32_t material, int back) {
 
 or_surface or_turned(const or_surface *s) { return or_surface_at(neg(s->normal), neg(s->geometric), s->material, !s->back); }
 
-void or_read_material(or_surface *s, const float *materials) {
+void or_read_material(or_surface *s, const float *materials, double hero) {
     const float *base_rgb = mrow(materials, s->material, 1), *specular_rgb = mrow(materials, s->material, 3);
     const float *coat_rgb = mrow(materials, s->material, 5), *transmission_rgb = mrow(materials, s->material, 9);
     const float *scalars = mrow(materials, s->material, 10), *indices = mrow(materials, s->material, 11);
@@ -246,6 +246,9 @@ void or_read_material(or_surface *s, const float *materials) {
     s->roughness = mixd(roughness, fmin(1.0, pow(r4 + 2.0 * c4, 0.25)), s->coat);
     ggx_alpha(s->roughness, clampd(scalars[3], 0.0, 1.0), s->alpha);
     double eta = fmax(indices[0], 1.0001);
+    /* Cauchy's index at the hero wavelength once dispersion split the path (openpbr.glsl:177-180, 309). */
+    if (geometry[3] != 0.0f && hero > 0.0)
+        eta = fmax(eta + geometry[3] * (1.0 / (hero * hero) - 1.0 / (587.6 * 587.6)), 1.0001);
     double relative = eta / s->coat_eta;
     if (relative < 1.0) relative = 1.0 / relative;
     s->ior = fmax(mixd(eta, relative, s->coat), 1.0001);
@@ -327,7 +330,7 @@ void or_read_colors(or_surface *s, const float *materials, int spectral, const d
 }
 
 void or_prepare_surface(or_surface *s, d3 wo, const float *materials, int spectral, const double lambda[4]) {
-    or_read_material(s, materials);
+    or_read_material(s, materials, spectral && lambda[1] < 0.0 ? lambda[0] : 0.0);
     or_orient_lobes(s, wo);
     or_read_colors(s, materials, spectral, lambda);
     or_update_substrate(s);
@@ -443,12 +446,12 @@ int or_sample_direction(const or_surface *s, d3 wo, double u0, double u1, double
     return *pdf > 0.0;
 }
 
-double or_light_sampler_pdf(const or_surface *s, const float *materials, d3 from, d3 to) {
+double or_light_sampler_pdf(const or_surface *s, const float *materials, d3 from, d3 to, double hero) {
     int same = dot(from, s->geometric) >= 0.0;
     or_surface v = same ? *s : or_turned(s);
     d3 wo = or_to_local(&v, from), wi = or_to_local(&v, to);
     if ((dot(to, v.geometric) > 0.0) != (wi.z > 0.0)) return 0.0;
-    if (!same) or_read_material(&v, materials);
+    if (!same) or_read_material(&v, materials, hero);
     or_light_lobes(&v);
     return or_surface_pdf(&v, wi, wo);
 }

@@ -37,7 +37,7 @@ or_surface or_surface_at(d3 normal, d3 geometric, uint32_t material, int back);
 or_surface or_turned(const or_surface *s);
 d3 or_to_local(const or_surface *s, d3 v);
 d3 or_to_world(const or_surface *s, d3 v);
-void or_read_material(or_surface *s, const float *materials);
+void or_read_material(or_surface *s, const float *materials, double hero);
 void or_orient_lobes(or_surface *s, d3 wo);
 void or_update_substrate(or_surface *s);
 void or_read_colors(or_surface *s, const float *materials, int spectral, const double lambda[4]);
@@ -48,7 +48,8 @@ double or_surface_pdf(const or_surface *s, d3 wi, d3 wo);
 spec or_evaluate_surface(const or_surface *s, d3 wi, d3 wo, double *pdf);
 int or_sample_direction(const or_surface *s, d3 wo, double u0, double u1, double pick, d3 *wi, double *pdf,
                         uint32_t *lobe);
-/* connect.glsl:51-60: the pdf the light sampler gives `to` when light arrived from `from`. */
-double or_light_sampler_pdf(const or_surface *s, const float *materials, d3 from, d3 to);
+/* connect.glsl:51-60: the pdf the light sampler gives `to` when light arrived from `from`;
+ * `hero`: the path's hero wavelength after a dispersive hit (0 before). */
+double or_light_sampler_pdf(const or_surface *s, const float *materials, d3 from, d3 to, double hero);
 
 #endif

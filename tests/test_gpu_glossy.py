@@ -197,3 +197,30 @@ def test_cutouts_match_f64_oracle(ctx):
         o = _blocks(mean, 8).mean((1, 3))
         sem = np.sqrt(_blocks(var, 8).mean((1, 3)) / (64 * spp))
         assert np.all(np.abs(g - o) <= 3.0 * sem + 1e-6), (tracing, np.max(np.abs(g - o) / (sem + 1e-12)))
+
+
+def test_dispersion(ctx):
+    # integrator.lucb:135-167 (kind 3, 1,024 samples): dispersive glass under a white sky
+    # stays white within 2 %; and over the benchmark's box, against the oracle's image.
+    m = scenes.openpbr(base_color=(1.0, 1.0, 1.0), transmission_weight=1.0, specular_roughness=0.0,
+                       transmission_dispersion_scale=1.0, transmission_dispersion_abbe_number=10.0)
+    meshes, cams = scenes.furnace_sphere(4)
+    sc = lr.compile_scene(meshes, cams)
+    img = _render(ctx, sc, 64, 48, 1024, 64, True, material=m, background=(1.0, 1.0, 1.0))
+    center = img[16:32, 24:40, :3].reshape(-1, 3).mean(0)
+    assert abs(center[1] - 1.0) <= 0.02, center
+    meshes, cams, lights, mats = scenes.glossy_cornell(2)
+    mats = list(mats)
+    mats[4] = m  # the glass ball disperses
+    sc = lr.compile_scene(meshes, cams, lights, mats)
+    w = h = 48
+    spp = 32
+    for tracing in (0.0, 0.5):
+        img = _render(ctx, sc, w, h, spp, 6, True, tracing=tracing)
+        frame = lr.ray_frame(sc.camera(), w, h)
+        mean, var = orc.render(sc.arrays(), lights, [lr.OpenPbr.lambert()] + mats, frame, spp, 6, True,
+                               light_tracing=tracing)
+        g = _blocks(img[..., :3].astype(np.float64), 8).mean((1, 3))
+        o = _blocks(mean, 8).mean((1, 3))
+        sem = np.sqrt(_blocks(var, 8).mean((1, 3)) / (64 * spp))
+        assert np.all(np.abs(g - o) <= 3.0 * sem + 1e-6), (tracing, np.max(np.abs(g - o) / (sem + 1e-12)))

@@ -143,3 +143,13 @@ def test_oracle_cutouts():
         mean, _ = orc.render(sc.arrays(), lights, [lr.OpenPbr.lambert((0.5, 0.5, 0.5))] + mats, frame, 128, 1, False)
         means.append(mean[14:18, 14:18, 1].mean())
     assert abs(means[0] / means[1] - 0.5) <= 0.015, means
+
+
+def test_oracle_dispersive_glass_furnace():
+    # integrator.lucb:135-167 (kind 3): a closed sphere of smooth dispersive glass under a
+    # white sky is white: its wavelengths split at the first hit and the hero carries the
+    # sample (openpbr.glsl:182-194).
+    m = scenes.openpbr(base_color=(1.0, 1.0, 1.0), transmission_weight=1.0, specular_roughness=0.0,
+                       transmission_dispersion_scale=1.0, transmission_dispersion_abbe_number=10.0)
+    center, sem = _furnace(m, True, samples=256)
+    assert abs(center[1] - 1.0) <= 0.02 + 3.0 * sem, (center, sem)
