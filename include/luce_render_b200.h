@@ -326,6 +326,36 @@ int lr_renderer_read_wait(lr_renderer *renderer);
 int lr_renderer_join(lr_renderer *renderer);
 /* Renderer.set_samples (integrator.lucb:609-611). */
 int lr_renderer_set_samples(lr_renderer *renderer, uint32_t samples);
+/* Renderer.restart (integrator.lucb:455-466): start over through `frame` (a moved camera, a
+ * resized view; the projection kept). The film clears before the next pass; passes in
+ * flight finish uncounted and never show (a new generation); the display keeps the last
+ * whole image until the new view's first whole sample replaces it. Waits for nothing
+ * unless the view outgrows the renderer's buffers (then the passes in flight are waited
+ * for and the buffers made again, a quarter larger each way). */
+int lr_renderer_restart(lr_renderer *renderer, const lr_frame *frame);
+/* Renderer.reload (integrator.lucb:483-541): the same geometry with other lights,
+ * materials or settings (the size and pool kept): `scene` must hold the renderer's points
+ * and triangles (400 otherwise); the triangles' normals and materials are uploaded again
+ * when they changed. The film starts over, through `frame` (NULL: the current view). */
+int lr_renderer_reload(lr_renderer *renderer, const lr_scene *scene, const lr_settings *settings,
+                       const lr_frame *frame);
+/* Renderer.replace_scene (integrator.lucb:543-574): new geometry in the same renderer (the
+ * pool and BVH choice kept, 400 otherwise); the display keeps the last image until the new
+ * scene's first whole sample; the old upload is released once the passes that read it
+ * have finished. */
+int lr_renderer_replace_scene(lr_renderer *renderer, const lr_scene *scene, const lr_settings *settings,
+                              const lr_frame *frame);
+/* Renderer.display (integrator.lucb:741-746): the render ready to show, rgba16f (4 halves a
+ * pixel, row by row at the shown view's width): exposed, in linear Rec.709, through the
+ * view; always one whole image of one view (no pass in flight writes it). */
+int lr_renderer_display(lr_renderer *renderer, void **device_rgba16f);
+/* Renderer.shown_size (integrator.lucb:748-751): the size of the image in the display,
+ * (0, 0) before the first whole sample. */
+int lr_renderer_shown_size(lr_renderer *renderer, uint32_t out[2]);
+/* Renderer.set_display (integrator.lucb:753-757): `exposure` stops through `view` (0
+ * standard: clipped; 1 Khronos PBR Neutral tone mapping); the next pass, or a conversion
+ * of its own once every sample is taken, applies it. */
+int lr_renderer_set_display(lr_renderer *renderer, double exposure, int view);
 /* Renderer.kernel_times (integrator.lucb:873-875): milliseconds per kernel kind
  * over finished passes with settings.profile on, in the order camera, intersect
  * closest, shade surface, shade miss, intersect shadow, light emission, finish,

@@ -272,6 +272,12 @@ _SIGNATURES = {
     "lr_renderer_set_samples": (C.c_int, [_vp, _u32]),
     "lr_renderer_join": (C.c_int, [_vp]),
     "lr_renderer_read_async": (C.c_int, [_vp, C.POINTER(C.c_float), _u64]),
+    "lr_renderer_restart": (C.c_int, [_vp, C.POINTER(Frame)]),
+    "lr_renderer_reload": (C.c_int, [_vp, _vp, C.POINTER(Settings), C.POINTER(Frame)]),
+    "lr_renderer_replace_scene": (C.c_int, [_vp, _vp, C.POINTER(Settings), C.POINTER(Frame)]),
+    "lr_renderer_display": (C.c_int, [_vp, C.POINTER(_vp)]),
+    "lr_renderer_shown_size": (C.c_int, [_vp, C.POINTER(C.c_uint32)]),
+    "lr_renderer_set_display": (C.c_int, [_vp, C.c_double, C.c_int]),
     "lr_renderer_read_wait": (C.c_int, [_vp]),
     "lr_batch_read_async": (C.c_int, [_vp, _u32, C.POINTER(C.c_float), _u64]),
     "lr_batch_read_wait": (C.c_int, [_vp]),
@@ -794,6 +800,46 @@ class Renderer:
     def read_wait(self) -> None:
         """Waits for every copy read_async queued."""
         _check(lib.lr_renderer_read_wait(self.handle))
+
+    def restart(self, frame: Frame) -> None:
+        """Renderer.restart (integrator.lucb:463): start over through `frame`."""
+        _check(lib.lr_renderer_restart(self.handle, C.byref(frame)))
+        self.width, self.height = int(frame.width), int(frame.height)
+
+    def reload(self, scene: "CompiledScene", settings: "RenderSettings", frame: Frame | None = None) -> None:
+        """Renderer.reload (integrator.lucb:491): the same geometry, other lights,
+        materials or settings."""
+        _check(lib.lr_renderer_reload(self.handle, scene.handle, C.byref(settings.c),
+                                      C.byref(frame) if frame is not None else None))
+        if frame is not None:
+            self.width, self.height = int(frame.width), int(frame.height)
+
+    def replace_scene(self, scene: "CompiledScene", settings: "RenderSettings", frame: Frame) -> None:
+        """Renderer.replace_scene (integrator.lucb:543): new geometry."""
+        _check(lib.lr_renderer_replace_scene(self.handle, scene.handle, C.byref(settings.c), C.byref(frame)))
+        self.width, self.height = int(frame.width), int(frame.height)
+
+    def display(self) -> int:
+        """The device address of the rgba16f display image."""
+        p = _vp()
+        _check(lib.lr_renderer_display(self.handle, C.byref(p)))
+        return p.value or 0
+
+    def shown_size(self) -> tuple[int, int]:
+        out = (C.c_uint32 * 2)()
+        _check(lib.lr_renderer_shown_size(self.handle, out))
+        return int(out[0]), int(out[1])
+
+    def read_display(self) -> np.ndarray:
+        """The display image copied to the host (float16, shown height x width x 4)."""
+        w, h = self.shown_size()
+        out = np.zeros((h, w, 4), np.float16)
+        if w and h:
+            _check(lib.lr_memcpy_dtoh(self.ctx.handle, out.ctypes.data_as(_vp), C.c_void_p(self.display()), out.nbytes))
+        return out
+
+    def set_display(self, exposure: float = 0.0, view: int = 0) -> None:
+        _check(lib.lr_renderer_set_display(self.handle, exposure, view))
 
     def image(self) -> int:
         """The device address of the rgba32f image."""

@@ -34,6 +34,8 @@
 
 #include "device.hpp"
 #include "loading.hpp"
+#include <cuda_fp16.h>
+
 #include "openpbr.cuh"
 #include "shading.cuh"
 #include "traverse.cuh"
@@ -119,10 +121,20 @@ struct PlanHeader {
     uint32_t camera_paths, folds, reserved0, reserved1;
 };
 
+// A renderer's display image for the pass (film_convert.comp:50-52): where the pass that
+// ends a sample writes the image ready to show (rgba16f, or none), its exposure scale and
+// view (0 clipped, 1 PBR Neutral tone mapping).
+struct PlanDisplay {
+    unsigned long long image;
+    float scale;
+    uint32_t view, reserved0, reserved1;
+};
+
 // A pass's plan: its segments, the members whose images it brings up to date (and the
 // samples they will then hold), and the members whose splats it folds into their films.
 struct Plan {
     PlanHeader head;
+    PlanDisplay display;  // for the first member converted (a renderer's own)
     uint32_t convert[kMaxSegments];
     uint32_t convert_samples[kMaxSegments];
     uint32_t fold[kMaxSegments];
@@ -1691,6 +1703,22 @@ __global__ void __launch_bounds__(kShadeBlock) fold_kernel(Wave w) {
 // film_convert.comp:36-53: the film's average, and the light paths' splats over the
 // samples taken, into the rgba32f ACEScg image, for every member whose sample ended in
 // this pass.
+// Khronos PBR Neutral tone mapping (film_convert.comp:20-34): linear below 0.76, with
+// hue-preserving compression above.
+__device__ __forceinline__ float3 pbr_neutral(float3 c) {
+    const float start = 0.8f - 0.04f, desaturation = 0.15f;
+    const float x = fminf(c.x, fminf(c.y, c.z));
+    const float offset = x < 0.08f ? x - 6.25f * x * x : 0.04f;
+    c = make_float3(c.x - offset, c.y - offset, c.z - offset);
+    const float peak = fmaxf(c.x, fmaxf(c.y, c.z));
+    if (peak < start) return c;
+    const float d = 1.0f - start;
+    const float new_peak = 1.0f - d * d / (peak + d - start);
+    c = c * (new_peak / peak);
+    const float g = 1.0f - 1.0f / (desaturation * (peak - new_peak) + 1.0f);
+    return make_float3(c.x * (1.0f - g) + new_peak * g, c.y * (1.0f - g) + new_peak * g, c.z * (1.0f - g) + new_peak * g);
+}
+
 __global__ void __launch_bounds__(kShadeBlock) convert_kernel(Wave w) {
     const Plan *plan = w.plan;
     const uint32_t converts = plan->head.converts;
@@ -1714,6 +1742,19 @@ __global__ void __launch_bounds__(kShadeBlock) convert_kernel(Wave w) {
                                     k.film[3] * value.x + k.film[4] * value.y + k.film[5] * value.z,
                                     k.film[6] * value.x + k.film[7] * value.y + k.film[8] * value.z);
             m.image[pixel] = make_float4(value.x, value.y, value.z, 1.0f);
+            if (c == 0 && plan->display.image) {
+                // Exposed, in linear Rec.709 (ACEScg Bradford-adapted to D65), through the view.
+                const float e = plan->display.scale;
+                float3 shown = make_float3(fmaxf(0.0f, e * (1.70505f * value.x - 0.62179f * value.y - 0.08326f * value.z)),
+                                           fmaxf(0.0f, e * (-0.13026f * value.x + 1.14080f * value.y - 0.01055f * value.z)),
+                                           fmaxf(0.0f, e * (-0.02400f * value.x - 0.12897f * value.y + 1.15297f * value.z)));
+                if (plan->display.view == 1u) shown = pbr_neutral(shown);
+                __half *out = (__half *)plan->display.image + pixel * 4;
+                out[0] = __float2half_rn(fminf(shown.x, 1.0f));
+                out[1] = __float2half_rn(fminf(shown.y, 1.0f));
+                out[2] = __float2half_rn(fminf(shown.z, 1.0f));
+                out[3] = __float2half_rn(1.0f);
+            }
         }
     }
 }
@@ -1819,12 +1860,21 @@ void upload_sobol_tables(cudaStream_t stream) {
 struct MemberHost {
     bool used = false, leaving = false;
     Member dev{};
-    void *block = nullptr;
+    void *block = nullptr;  // loaded records: lights, light tree, materials, constants
+    void *view = nullptr;   // the view's memory: film, image, splat accumulators
+    uint64_t view_pixels = 0;  // pixels the view memory holds
+    bool view_traced = false;  // it holds splat accumulators
     lr_gpu_scene *owned = nullptr;  // a renderer's own upload (null when borrowed)
     uint32_t samples = 0, sample = 0, next_pixel = 0, done = 0;
     uint32_t light_next = 0;  // light paths of the current sample planned so far
     uint32_t max_bounces = 0;
     uint64_t last_pass = 0;  // the last pass (plus one) that traced it; 0: none
+    // Restarts so far (integrator.lucb:572-582): passes of an older generation finish
+    // uncounted; and what a restart needs again without reloading.
+    uint32_t generation = 0;
+    lr_settings settings{};
+    size_t emitters = 0;
+    double emit_share = 0.0;
 };
 
 // The traversal variants a pass can take: (BVH width, stack entries).
@@ -1838,7 +1888,10 @@ inline int size_class(uint64_t triangles) { return triangles < 16384 ? 0 : (tria
 struct PassRecord {
     uint64_t number;
     std::vector<std::pair<uint32_t, bool>> members;  // member, sample ended
+    std::vector<uint32_t> generations;               // each member's generation at launch
     std::vector<std::pair<cudaEvent_t, int>> marks;  // profiling
+    int display_slot = -1;                           // the display image it writes
+    uint32_t width = 0, height = 0;                  // the view it shows
 };
 
 struct Graph {
@@ -1897,6 +1950,20 @@ struct WaveHost {
     cudaStream_t copy_stream = nullptr;
     cudaEvent_t read_done = nullptr;
     uint64_t reads = 0;
+    // A renderer's display images (integrator.lucb:695-713): three rgba16f images of
+    // `display_pixels`, the one shown (`front`, -1 none yet) and its size; a pass that ends
+    // a sample writes one that is neither shown nor written by a pass in flight, and it
+    // is shown once that pass retires in the current generation.
+    void *display_block = nullptr;
+    uint64_t display_pixels = 0;
+    int front = -1;
+    uint32_t shown_width = 0, shown_height = 0;
+    float display_scale = 1.0f;  // exp2(exposure)
+    uint32_t display_view = 0;
+    bool display_stale = false;  // set_display since the last conversion
+    // Scenes a reload or replacement let go, destroyed once the passes launched before
+    // (the number) have retired.
+    std::vector<std::pair<uint64_t, lr_gpu_scene *>> retiring_scenes;
 };
 
 namespace {
@@ -2040,24 +2107,10 @@ void make_albedo_tables(int device, cudaStream_t stream) {
     made[device] = true;
 }
 
-void wave_create(WaveHost *h, lr_context *ctx, uint64_t pool, uint32_t rounds, uint32_t capacity, int profile) {
-    if (pool == 0 || rounds == 0 || capacity == 0) fail(LR_INVALID, "a wave needs paths, rounds and members");
-    h->ctx = ctx;
-    h->pool = (uint32_t)std::min<uint64_t>(pool, kMaxPool);
-    h->rounds = rounds;
-    h->capacity = capacity;
-    h->profile = profile;
-    h->lane_count = profile ? 1 : 2;
-    LR_CUDA(cudaSetDevice(ctx->device));
-    {
-        Layout L;
-        const size_t p_stats = L.add(nullptr, 8 * 8);
-        const size_t p_members = L.add(nullptr, (size_t)capacity * sizeof(Member));
-        size_t total = 0;
-        h->block = L.allocate(ctx->stream, total);
-        h->d_stats = (unsigned long long *)((char *)h->block + L.parts[p_stats].offset);
-        h->d_members = (Member *)((char *)h->block + L.parts[p_members].offset);
-    }
+// Each lane's path state, ray queues, counters and plan, for the wave's pool and rounds.
+void lanes_create(WaveHost *h) {
+    lr_context *ctx = h->ctx;
+    const uint32_t rounds = h->rounds;
     const uint64_t P = h->pool;
     for (int li = 0; li < h->lane_count; li++) {
         Lane &lane = h->lanes[li];
@@ -2109,6 +2162,35 @@ void wave_create(WaveHost *h, lr_context *ctx, uint64_t pool, uint32_t rounds, u
         }
         LR_CUDA(cudaEventCreateWithFlags(&lane.finished, cudaEventDisableTiming));
     }
+}
+
+// Each lane's film stage as a graph (finish, fold, convert).
+void lanes_capture(WaveHost *h) {
+    for (int li = 0; li < h->lane_count; li++) {
+        Lane &lane = h->lanes[li];
+        lane.finish = capture([&](cudaStream_t s) { record_finish(h, lane.w, s, nullptr); });
+    }
+}
+
+void wave_create(WaveHost *h, lr_context *ctx, uint64_t pool, uint32_t rounds, uint32_t capacity, int profile) {
+    if (pool == 0 || rounds == 0 || capacity == 0) fail(LR_INVALID, "a wave needs paths, rounds and members");
+    h->ctx = ctx;
+    h->pool = (uint32_t)std::min<uint64_t>(pool, kMaxPool);
+    h->rounds = rounds;
+    h->capacity = capacity;
+    h->profile = profile;
+    h->lane_count = profile ? 1 : 2;
+    LR_CUDA(cudaSetDevice(ctx->device));
+    {
+        Layout L;
+        const size_t p_stats = L.add(nullptr, 8 * 8);
+        const size_t p_members = L.add(nullptr, (size_t)capacity * sizeof(Member));
+        size_t total = 0;
+        h->block = L.allocate(ctx->stream, total);
+        h->d_stats = (unsigned long long *)((char *)h->block + L.parts[p_stats].offset);
+        h->d_members = (Member *)((char *)h->block + L.parts[p_members].offset);
+    }
+    lanes_create(h);
     upload_sobol_tables(ctx->stream);
     make_albedo_tables(ctx->device, ctx->stream);
     LR_CUDA(cudaStreamSynchronize(ctx->stream));
@@ -2117,10 +2199,7 @@ void wave_create(WaveHost *h, lr_context *ctx, uint64_t pool, uint32_t rounds, u
     if (profile)
         for (auto &e : h->mark_start) LR_CUDA(cudaEventCreate(&e));
     else
-        for (int li = 0; li < h->lane_count; li++) {
-            Lane &lane = h->lanes[li];
-            lane.finish = capture([&](cudaStream_t s) { record_finish(h, lane.w, s, nullptr); });
-        }
+        lanes_capture(h);
     h->members.resize(capacity);
 }
 
@@ -2159,34 +2238,49 @@ LightPaths light_paths_of(const lr_settings &settings, const lr_frame &frame, ui
     return out;
 }
 
-// Makes `scene` (uploaded as `gs`) seen through `frame` a member; returns its index.
-uint32_t member_add(WaveHost *h, const lr_gpu_scene *gs, lr_gpu_scene *owned, const lr_scene *scene,
-                    const lr_settings &settings, const lr_frame &frame) {
-    validate(settings, frame);
-    const uint32_t rounds = settings.max_bounces + 1 + (has_cutouts(*scene, settings) ? kCutoutRounds : 0);
-    if (rounds > h->rounds)
-        fail(LR_LIMIT, "this wave traces " + std::to_string(h->rounds) + " rounds a pass; the render needs " +
-                           std::to_string(rounds) + " (its bounces + 1, + " + std::to_string(kCutoutRounds) +
-                           " with cut-outs)");
-    if (!gs->ctx || gs->ctx->device != h->ctx->device) fail(LR_INVALID, "the scene was uploaded to another device");
-    auto free_slot = [&] {
-        for (uint32_t i = 0; i < h->capacity; i++)
-            if (!h->members[i].used) return i;
-        return h->capacity;
-    };
-    uint32_t index = free_slot();
-    if (index == h->capacity && std::any_of(h->members.begin(), h->members.end(),
-                                            [](const MemberHost &m) { return m.used && m.leaving; })) {
-        // A member that left holds its slot until its passes finish: wait for them.
-        settle(h);
-        index = free_slot();
+// Gives `lay`'s parts their offsets (256-byte aligned); returns the block's size.
+size_t lay_out(Layout &lay) {
+    size_t total = 0;
+    for (auto &p : lay.parts) {
+        p.offset = total;
+        total += align256(std::max<size_t>(p.bytes, 64));
     }
-    if (index == h->capacity) fail(LR_LIMIT, "the wave holds " + std::to_string(h->capacity) + " members");
-    const Loaded L = load(*scene, settings);
-    const uint64_t pixels = (uint64_t)frame.width * frame.height;
-    const double emit_share = frame.orthographic ? 0.0 : L.emit_share;
-    const LightPaths traced = light_paths_of(settings, frame, pixels, L.tree.emitter_count, emit_share > 0.0);
+    return total;
+}
+
+// Lays out `lay` as one zeroed stream-ordered block on `stream` and copies the parts
+// that have a source through the pinned `stage`, from `stage_at` on.
+void *place(Layout &lay, cudaStream_t stream, char *stage, size_t &stage_at) {
+    const size_t total = lay_out(lay);
+    void *block = nullptr;
+    LR_CUDA(cudaMallocAsync(&block, total, stream));
+    char *base = (char *)block;
+    LR_CUDA(cudaMemsetAsync(base, 0, total, stream));
+    for (auto &p : lay.parts) {
+        if (!p.src || !p.bytes) continue;
+        std::memcpy(stage + stage_at, p.src, p.bytes);
+        LR_CUDA(cudaMemcpyAsync(base + p.offset, stage + stage_at, p.bytes, cudaMemcpyHostToDevice, stream));
+        stage_at += align256(p.bytes);
+    }
+    return block;
+}
+
+size_t staged_bytes(const Layout &lay) {
+    size_t bytes = 0;
+    for (const auto &p : lay.parts)
+        if (p.src) bytes += align256(p.bytes);
+    return bytes;
+}
+
+// A member's loaded records (lights, light tree, materials, constants) from `L`.
+struct LoadedRecords {
     Constants k{};
+    Layout lay;
+    size_t lights = 0, nodes = 0, links = 0, records = 0, map = 0, materials = 0, constants = 0;
+};
+
+void loaded_records(const Loaded &L, const lr_settings &settings, double emit_share, LoadedRecords &r) {
+    Constants &k = r.k;
     for (int i = 0; i < 9; i++) k.film[i] = (float)L.film.m[i];
     k.cmf_integrals[0] = (float)L.cmf_integrals.x;
     k.cmf_integrals[1] = (float)L.cmf_integrals.y;
@@ -2206,73 +2300,121 @@ uint32_t member_add(WaveHost *h, const lr_gpu_scene *gs, lr_gpu_scene *owned, co
     k.emit_share = (float)emit_share;
     k.emit_radius = (float)L.emit_radius;
     k.emit_center = make_float3((float)L.emit_center.x, (float)L.emit_center.y, (float)L.emit_center.z);
+    r.lights = r.lay.add(L.lights.rows.data(), L.lights.rows.size() * 4);
+    r.nodes = r.lay.add(L.tree.nodes.data(), L.tree.nodes.size() * 4);
+    r.links = r.lay.add(L.tree.links.data(), L.tree.links.size() * 4);
+    r.records = r.lay.add(L.tree.records.data(), L.tree.records.size() * 4);
+    r.map = r.lay.add(L.tree.triangle_map.data(), L.tree.triangle_map.size() * 4);
+    r.materials = r.lay.add(L.materials.data(), L.materials.size() * 4);
+    r.constants = r.lay.add(&k, sizeof k);
+}
 
-    Layout lay;
-    const size_t p_lights = lay.add(L.lights.rows.data(), L.lights.rows.size() * 4);
-    const size_t p_tree_nodes = lay.add(L.tree.nodes.data(), L.tree.nodes.size() * 4);
-    const size_t p_tree_links = lay.add(L.tree.links.data(), L.tree.links.size() * 4);
-    const size_t p_tree_records = lay.add(L.tree.records.data(), L.tree.records.size() * 4);
-    const size_t p_tree_map = lay.add(L.tree.triangle_map.data(), L.tree.triangle_map.size() * 4);
-    const size_t p_materials = lay.add(L.materials.data(), L.materials.size() * 4);
-    const size_t p_constants = lay.add(&k, sizeof k);
-    const size_t p_film = lay.add(nullptr, pixels * 16);
-    const size_t p_image = lay.add(nullptr, pixels * 16);
-    const size_t splat_bytes = traced.count ? pixels * 24 : 0;
-    const size_t p_splat = lay.add(nullptr, splat_bytes);
-    const size_t p_splat_lane0 = lay.add(nullptr, splat_bytes), p_splat_lane1 = lay.add(nullptr, splat_bytes);
-    MemberHost &mh = h->members[index];
-    // Stream-ordered: the member's memory and data arrive ahead of the next pass without
-    // waiting for the passes in flight.
-    cudaStream_t stream = h->ctx->stream;
-    size_t total = 0, host_bytes = sizeof(Member);
-    for (auto &p : lay.parts) {
-        p.offset = total;
-        total += align256(std::max<size_t>(p.bytes, 64));
-        if (p.src) host_bytes += align256(p.bytes);
-    }
-    char *stage = h->staging.take(host_bytes);
-    LR_CUDA(cudaMallocAsync(&mh.block, total, stream));
-    char *base = (char *)mh.block;
-    LR_CUDA(cudaMemsetAsync(base, 0, total, stream));
-    size_t at_stage = sizeof(Member);
-    for (auto &p : lay.parts) {
-        if (!p.src || !p.bytes) continue;
-        std::memcpy(stage + at_stage, p.src, p.bytes);
-        LR_CUDA(cudaMemcpyAsync(base + p.offset, stage + at_stage, p.bytes, cudaMemcpyHostToDevice, stream));
-        at_stage += align256(p.bytes);
-    }
-    auto at = [&](size_t i) { return (void *)(base + lay.parts[i].offset); };
-    Member &m = mh.dev;
-    m = Member{};
-    m.scene = gs->scene;
-    m.lights = (const float4 *)at(p_lights);
+// Points `m` at its loaded records in `block`.
+void set_loaded(Member &m, const LoadedRecords &r, const Loaded &L, void *block, const lr_settings &settings,
+                uint32_t rounds) {
+    auto at = [&](size_t i) { return (void *)((char *)block + r.lay.parts[i].offset); };
+    m.lights = (const float4 *)at(r.lights);
     m.light_count = (uint32_t)L.lights.count;
     m.spectral = settings.spectral ? 1u : 0u;
-    m.tree.nodes = (const float4 *)at(p_tree_nodes);
-    m.tree.links = (const uint2 *)at(p_tree_links);
-    m.tree.records = (const uint4 *)at(p_tree_records);
-    m.tree.triangle_map = L.tree.triangle_map.empty() ? nullptr : (const uint32_t *)at(p_tree_map);
+    m.tree.nodes = (const float4 *)at(r.nodes);
+    m.tree.links = (const uint2 *)at(r.links);
+    m.tree.records = (const uint4 *)at(r.records);
+    m.tree.triangle_map = L.tree.triangle_map.empty() ? nullptr : (const uint32_t *)at(r.map);
     m.tree.node_count = (uint32_t)L.tree.node_count;
-    m.materials = (const float4 *)at(p_materials);
-    m.k = (const Constants *)at(p_constants);
+    m.materials = (const float4 *)at(r.materials);
+    m.k = (const Constants *)at(r.constants);
+    m.glossy = L.glossy ? 1u : 0u;
+    m.cutouts = L.cutouts ? 1u : 0u;
+    m.rounds = rounds;
+}
+
+// The view's memory for `pixels`: film, image and, for light tracing, the splat
+// accumulators (the film's and one per lane).
+Layout view_layout(uint64_t pixels, bool traced, size_t parts[5]) {
+    Layout lay;
+    parts[0] = lay.add(nullptr, pixels * 16);
+    parts[1] = lay.add(nullptr, pixels * 16);
+    const size_t splat_bytes = traced ? pixels * 24 : 0;
+    for (int i = 2; i < 5; i++) parts[i] = lay.add(nullptr, splat_bytes);
+    return lay;
+}
+
+void set_view_memory(Member &m, const Layout &lay, const size_t parts[5], void *view, bool traced) {
+    auto at = [&](size_t i) { return (void *)((char *)view + lay.parts[i].offset); };
+    m.film = (float4 *)at(parts[0]);
+    m.image = (float4 *)at(parts[1]);
+    m.splat = traced ? (unsigned long long *)at(parts[2]) : nullptr;
+    m.splat_lane[0] = traced ? (unsigned long long *)at(parts[3]) : nullptr;
+    m.splat_lane[1] = traced ? (unsigned long long *)at(parts[4]) : nullptr;
+}
+
+// The view `m` renders: its frame, size and light paths.
+void set_view(Member &m, const lr_frame &frame, const LightPaths &traced) {
     pack_frame(frame, m.frame);
     m.lens_radius = (float)frame.lens_radius;
     m.focus_distance = (float)frame.focus_distance;
     for (int i = 0; i < 3; i++) m.forward[i] = (float)frame.forward[i];
     m.width = frame.width;
     m.height = frame.height;
-    m.pixels = pixels;
-    m.film = (float4 *)at(p_film);
-    m.image = (float4 *)at(p_image);
+    m.pixels = (uint64_t)frame.width * frame.height;
     m.light_paths = traced.count;
     m.light_band = traced.band;
     m.pixel_area_inv = (float)traced.pixel_area_inv;
-    m.splat = traced.count ? (unsigned long long *)at(p_splat) : nullptr;
-    m.splat_lane[0] = traced.count ? (unsigned long long *)at(p_splat_lane0) : nullptr;
-    m.splat_lane[1] = traced.count ? (unsigned long long *)at(p_splat_lane1) : nullptr;
-    m.glossy = L.glossy ? 1u : 0u;
-    m.cutouts = L.cutouts ? 1u : 0u;
-    m.rounds = rounds;
+}
+
+uint32_t rounds_of(const lr_scene &scene, const lr_settings &settings) {
+    return settings.max_bounces + 1 + (has_cutouts(scene, settings) ? kCutoutRounds : 0);
+}
+
+void check_rounds(const WaveHost *h, uint32_t rounds) {
+    if (rounds > h->rounds)
+        fail(LR_LIMIT, "this wave traces " + std::to_string(h->rounds) + " rounds a pass; the render needs " +
+                           std::to_string(rounds) + " (its bounces + 1, + " + std::to_string(kCutoutRounds) +
+                           " with cut-outs)");
+}
+
+// Makes `scene` (uploaded as `gs`) seen through `frame` a member; returns its index.
+uint32_t member_add(WaveHost *h, const lr_gpu_scene *gs, lr_gpu_scene *owned, const lr_scene *scene,
+                    const lr_settings &settings, const lr_frame &frame) {
+    validate(settings, frame);
+    const uint32_t rounds = rounds_of(*scene, settings);
+    check_rounds(h, rounds);
+    if (!gs->ctx || gs->ctx->device != h->ctx->device) fail(LR_INVALID, "the scene was uploaded to another device");
+    auto free_slot = [&] {
+        for (uint32_t i = 0; i < h->capacity; i++)
+            if (!h->members[i].used) return i;
+        return h->capacity;
+    };
+    uint32_t index = free_slot();
+    if (index == h->capacity && std::any_of(h->members.begin(), h->members.end(),
+                                            [](const MemberHost &m) { return m.used && m.leaving; })) {
+        // A member that left holds its slot until its passes finish: wait for them.
+        settle(h);
+        index = free_slot();
+    }
+    if (index == h->capacity) fail(LR_LIMIT, "the wave holds " + std::to_string(h->capacity) + " members");
+    const Loaded L = load(*scene, settings);
+    const uint64_t pixels = (uint64_t)frame.width * frame.height;
+    const double emit_share = frame.orthographic ? 0.0 : L.emit_share;
+    const LightPaths traced = light_paths_of(settings, frame, pixels, L.tree.emitter_count, emit_share > 0.0);
+    LoadedRecords records;
+    loaded_records(L, settings, emit_share, records);
+    size_t view_parts[5];
+    Layout view = view_layout(pixels, traced.count > 0, view_parts);
+    MemberHost &mh = h->members[index];
+    // Stream-ordered: the member's memory and data arrive ahead of the next pass without
+    // waiting for the passes in flight.
+    cudaStream_t stream = h->ctx->stream;
+    char *stage = h->staging.take(sizeof(Member) + staged_bytes(records.lay) + staged_bytes(view));
+    size_t stage_at = sizeof(Member);
+    mh.block = place(records.lay, stream, stage, stage_at);
+    mh.view = place(view, stream, stage, stage_at);
+    Member &m = mh.dev;
+    m = Member{};
+    m.scene = gs->scene;
+    set_loaded(m, records, L, mh.block, settings, rounds);
+    set_view_memory(m, view, view_parts, mh.view, traced.count > 0);
+    set_view(m, frame, traced);
     std::memcpy(stage, &m, sizeof m);
     LR_CUDA(cudaMemcpyAsync(h->d_members + index, stage, sizeof m, cudaMemcpyHostToDevice, stream));
     h->staging.queued(stream);
@@ -2284,13 +2426,117 @@ uint32_t member_add(WaveHost *h, const lr_gpu_scene *gs, lr_gpu_scene *owned, co
     mh.sample = mh.next_pixel = mh.done = mh.light_next = 0;
     mh.max_bounces = settings.max_bounces;
     mh.last_pass = 0;
+    mh.view_pixels = pixels;
+    mh.view_traced = traced.count > 0;
+    mh.settings = settings;
+    mh.emitters = L.tree.emitter_count;
+    mh.emit_share = L.emit_share;
     return index;
+}
+
+MemberHost &member_at(WaveHost *h, uint32_t member);
+
+// Orders the context's stream after every pass launched so far: what it does next (frees,
+// record uploads, clears) does not overtake them.
+void after_passes(WaveHost *h) {
+    if (h->recorded == 0) return;
+    for (int li = 0; li < h->lane_count; li++) {
+        Lane &lane = h->lanes[li];
+        if (lane.stream != h->ctx->stream) LR_CUDA(cudaStreamWaitEvent(h->ctx->stream, lane.finished, 0));
+    }
+}
+
+// A view memory a restarted or reloaded view can grow into: a quarter more pixels each
+// way than asked (integrator.lucb:478-482), so that a window resized a few pixels at a
+// time makes it again seldom.
+uint64_t roomy_pixels(const lr_frame &frame) {
+    const uint64_t w = frame.width + frame.width / 4, h = frame.height + frame.height / 4;
+    return w * h;
+}
+
+// Renderer.restart / reload / replace_scene (integrator.lucb:463-582) for member `index`:
+// the view through `frame`, and when `scene` is given its records loaded again from it
+// and `settings` (the geometry `gs`, its upload when `owned`). Passes in flight finish
+// uncounted (a new generation), the film starts over, and nothing waits for the device:
+// the member's new records, its cleared or new memory and the release of the old follow
+// the passes launched so far on the context's stream.
+void member_renew(WaveHost *h, uint32_t index, const lr_frame &frame, const lr_scene *scene, const lr_settings *settings,
+                  const lr_gpu_scene *gs, lr_gpu_scene *owned) {
+    MemberHost &mh = member_at(h, index);
+    const lr_settings &chosen = settings ? *settings : mh.settings;
+    validate(chosen, frame);
+    cudaStream_t stream = h->ctx->stream;
+    std::unique_ptr<Loaded> L;
+    LoadedRecords records;
+    uint32_t rounds = mh.dev.rounds;
+    size_t emitters = mh.emitters;
+    double emit_share = mh.emit_share;
+    if (scene) {
+        rounds = rounds_of(*scene, chosen);
+        check_rounds(h, rounds);
+        L = std::make_unique<Loaded>(load(*scene, chosen));
+        emitters = L->tree.emitter_count;
+        emit_share = L->emit_share;
+        loaded_records(*L, chosen, frame.orthographic ? 0.0 : emit_share, records);
+    }
+    const uint64_t pixels = (uint64_t)frame.width * frame.height;
+    const LightPaths traced = light_paths_of(chosen, frame, pixels, emitters, !frame.orthographic && emit_share > 0.0);
+    const bool new_view = pixels > mh.view_pixels || (traced.count > 0 && !mh.view_traced);
+    size_t view_parts[5];
+    const uint64_t capacity = new_view ? roomy_pixels(frame) : mh.view_pixels;
+    const bool view_traced = new_view ? traced.count > 0 : mh.view_traced;
+    Layout view = view_layout(capacity, view_traced, view_parts);
+    lay_out(view);
+    char *stage = h->staging.take(sizeof(Member) + (scene ? staged_bytes(records.lay) : 0));
+    size_t stage_at = sizeof(Member);
+    after_passes(h);
+    Member m = mh.dev;
+    if (scene) {
+        void *block = place(records.lay, stream, stage, stage_at);
+        LR_CUDA(cudaFreeAsync(mh.block, stream));
+        mh.block = block;
+        m.scene = gs->scene;
+        set_loaded(m, records, *L, block, chosen, rounds);
+    }
+    if (new_view) {
+        if (h->read_done) LR_CUDA(cudaStreamWaitEvent(stream, h->read_done, 0));
+        void *fresh = place(view, stream, stage, stage_at);
+        LR_CUDA(cudaFreeAsync(mh.view, stream));
+        mh.view = fresh;
+        mh.view_pixels = capacity;
+        mh.view_traced = view_traced;
+    } else {
+        // The film starts over; the image keeps the last one until a sample replaces it.
+        LR_CUDA(cudaMemsetAsync((char *)mh.view + view.parts[view_parts[0]].offset, 0, pixels * 16, stream));
+        if (view_traced)
+            LR_CUDA(cudaMemsetAsync((char *)mh.view + view.parts[view_parts[2]].offset, 0, pixels * 24, stream));
+    }
+    set_view_memory(m, view, view_parts, mh.view, view_traced);
+    set_view(m, frame, traced);
+    if (!traced.count) m.splat = m.splat_lane[0] = m.splat_lane[1] = nullptr;
+    mh.dev = m;
+    std::memcpy(stage, &m, sizeof m);
+    LR_CUDA(cudaMemcpyAsync(h->d_members + index, stage, sizeof m, cudaMemcpyHostToDevice, stream));
+    h->staging.queued(stream);
+    h->member_uploads++;
+    if (owned && owned != mh.owned) {
+        if (mh.owned) h->retiring_scenes.push_back({h->recorded, mh.owned});
+        mh.owned = owned;
+    }
+    mh.generation++;
+    mh.sample = mh.next_pixel = mh.done = mh.light_next = 0;
+    mh.settings = chosen;
+    mh.samples = chosen.samples;
+    mh.max_bounces = chosen.max_bounces;
+    mh.emitters = emitters;
+    mh.emit_share = emit_share;
 }
 
 void member_free(MemberHost &mh, cudaStream_t stream, cudaEvent_t reads = nullptr) {
     // A read in flight may still copy from the member's image.
     if (reads) cudaStreamWaitEvent(stream, reads, 0);
     if (mh.block) cudaFreeAsync(mh.block, stream);
+    if (mh.view) cudaFreeAsync(mh.view, stream);
     if (mh.owned) lr_gpu_scene_destroy(mh.owned);
     mh = MemberHost{};
 }
@@ -2330,16 +2576,53 @@ bool retire_one(WaveHost *h, bool wait) {
         }
         for (auto &[ev, kind] : p.marks) cudaEventDestroy(ev);
     }
-    for (auto &[m, ended] : p.members)
+    bool current = true;
+    for (size_t i = 0; i < p.members.size(); i++) {
+        const auto &[m, ended] = p.members[i];
+        if (h->members[m].generation != p.generations[i]) {
+            current = false;  // launched before a restart: counts for nothing
+            continue;
+        }
         if (ended) h->members[m].done++;
+    }
+    if (p.display_slot >= 0 && current) {
+        h->front = p.display_slot;
+        h->shown_width = p.width;
+        h->shown_height = p.height;
+    }
     h->retired = p.number + 1;
     h->in_flight.pop_front();
     collect(h);
+    for (size_t i = 0; i < h->retiring_scenes.size();) {
+        if (h->retiring_scenes[i].first <= h->retired) {
+            lr_gpu_scene_destroy(h->retiring_scenes[i].second);
+            h->retiring_scenes.erase(h->retiring_scenes.begin() + (long)i);
+        } else {
+            i++;
+        }
+    }
     return true;
 }
 
 void settle(WaveHost *h) {
     while (!h->in_flight.empty()) retire_one(h, true);
+}
+
+// A renderer's display image `slot`.
+void *display_image(WaveHost *h, int slot) {
+    return (char *)h->display_block + (size_t)slot * align256(h->display_pixels * 8);
+}
+
+// A display image neither shown nor written by a pass in flight (of three, with at most
+// two passes in flight, one is always free).
+int free_display_slot(WaveHost *h) {
+    for (int slot = 0; slot < 3; slot++) {
+        if (slot == h->front) continue;
+        bool busy = false;
+        for (const PassRecord &p : h->in_flight) busy = busy || p.display_slot == slot;
+        if (!busy) return slot;
+    }
+    return h->front;
 }
 
 // Plans and launches one pass: each member with work left adds its next segment, in
@@ -2383,6 +2666,7 @@ bool launch_pass(WaveHost *h, bool dry = false, int only = -1) {
         if (count == left && light_next < lights) count = (uint32_t)left - 1;
         const bool ends = count > 0 && count == left && !dry;
         rec.members.push_back({index, ends});
+        rec.generations.push_back(mh.generation);
         if (count > 0) {
             seg[n++] = Segment{index, mh.next_pixel, count, mh.sample, used, ends ? 1u : 0u, kCameraSegment, camera_paths};
             if (ends) {
@@ -2434,6 +2718,15 @@ bool launch_pass(WaveHost *h, bool dry = false, int only = -1) {
     const int variant = width * 1000 + stack + (tracing ? kTracingVariant : 0) + (glossy ? kGlossyVariant : 0) +
                         (cutouts ? kCutoutVariant : 0);
     staging->head = PlanHeader{n, used, converts, dry ? 1u : 0u, camera_paths, folds, 0u, 0u};
+    staging->display = PlanDisplay{0ull, h->display_scale, h->display_view, 0u, 0u};
+    if (h->display_block && converts > 0) {
+        rec.display_slot = free_display_slot(h);
+        staging->display.image = (unsigned long long)display_image(h, rec.display_slot);
+        const MemberHost &shown = h->members[staging->convert[0]];
+        rec.width = shown.dev.width;
+        rec.height = shown.dev.height;
+        h->display_stale = false;
+    }
     cudaStream_t stream = lane.stream;
     // Member records queued on the context's stream reach this lane first.
     if (stream != h->ctx->stream && lane.members_seen != h->member_uploads && h->staging.copied) {
@@ -2478,11 +2771,57 @@ void join_lanes(WaveHost *h) {
 }
 
 // Renderer.advance (integrator.lucb:649-693): never waits; two passes in flight.
+// A film stage alone for a renderer whose display settings changed after its last sample
+// (integrator.lucb:663-675): its image and a display image converted again.
+void launch_convert(WaveHost *h) {
+    Lane &lane = lane_of(h, h->recorded);
+    Plan *staging = lane.h_plan;
+    MemberHost &mh = h->members[0];
+    PassRecord rec;
+    rec.number = h->recorded;
+    rec.members.push_back({0u, false});
+    rec.generations.push_back(mh.generation);
+    staging->head = PlanHeader{0u, 0u, 1u, 0u, 0u, 0u, 0u, 0u};
+    staging->convert[0] = 0u;
+    staging->convert_samples[0] = mh.sample;
+    rec.display_slot = free_display_slot(h);
+    staging->display = PlanDisplay{(unsigned long long)display_image(h, rec.display_slot), h->display_scale,
+                                   h->display_view, 0u, 0u};
+    rec.width = mh.dev.width;
+    rec.height = mh.dev.height;
+    h->display_stale = false;
+    cudaStream_t stream = lane.stream;
+    if (stream != h->ctx->stream && lane.members_seen != h->member_uploads && h->staging.copied) {
+        LR_CUDA(cudaStreamWaitEvent(stream, h->staging.copied, 0));
+        lane.members_seen = h->member_uploads;
+    }
+    LR_CUDA(cudaMemcpyAsync(lane.d_plan, staging, offsetof(Plan, seg), cudaMemcpyHostToDevice, stream));
+    Lane *before = rec.number > 0 && h->lane_count > 1 ? &lane_of(h, rec.number - 1) : nullptr;
+    if (before) LR_CUDA(cudaStreamWaitEvent(stream, before->finished, 0));
+    if (lane.reads_seen != h->reads) {
+        LR_CUDA(cudaStreamWaitEvent(stream, h->read_done, 0));
+        lane.reads_seen = h->reads;
+    }
+    if (h->profile) {
+        LR_CUDA(cudaEventRecord(h->mark_start[rec.number & 1], stream));
+        record_finish(h, lane.w, stream, &rec.marks);
+    } else {
+        LR_CUDA(cudaGraphLaunch(lane.finish.exec, stream));
+    }
+    LR_CUDA(cudaEventRecord(lane.finished, stream));
+    h->recorded++;
+    h->in_flight.push_back(std::move(rec));
+}
+
 bool wave_advance(WaveHost *h) {
     while (retire_one(h, false)) {
     }
     if (h->in_flight.size() >= 2) return true;
     if (launch_pass(h)) return true;
+    if (h->display_block && h->display_stale && h->members[0].used) {
+        launch_convert(h);
+        return true;
+    }
     return !h->in_flight.empty();
 }
 
@@ -2584,6 +2923,33 @@ void wave_finish(WaveHost *h) {
     check_status(h->ctx);
 }
 
+void lanes_destroy(WaveHost *h) {
+    for (auto &lane : h->lanes) {
+        for (auto &[v, g] : lane.trace) destroy_graph(g);
+        destroy_graph(lane.finish);
+        if (lane.finished) cudaEventDestroy(lane.finished);
+        if (lane.h_plan) cudaFreeHost(lane.h_plan);
+        if (lane.own_stream && lane.stream) cudaStreamDestroy(lane.stream);
+        if (lane.block) cudaFree(lane.block);
+        lane = Lane{};
+    }
+}
+
+// The wave's lanes made again for `pool` paths and `rounds` rounds, after the passes in
+// flight; its members stay.
+void wave_resize(WaveHost *h, uint64_t pool, uint32_t rounds) {
+    settle(h);
+    for (auto &lane : h->lanes)
+        if (lane.stream) LR_CUDA(cudaStreamSynchronize(lane.stream));
+    LR_CUDA(cudaStreamSynchronize(h->ctx->stream));
+    lanes_destroy(h);
+    h->pool = (uint32_t)std::min<uint64_t>(pool, kMaxPool);
+    h->rounds = rounds;
+    lanes_create(h);
+    LR_CUDA(cudaStreamSynchronize(h->ctx->stream));
+    if (!h->profile) lanes_capture(h);
+}
+
 void wave_destroy(WaveHost *h) {
     if (!h->ctx) return;
     cudaSetDevice(h->ctx->device);
@@ -2601,15 +2967,11 @@ void wave_destroy(WaveHost *h) {
     h->staging.release();
     if (h->read_done) cudaEventDestroy(h->read_done);
     if (h->copy_stream) cudaStreamDestroy(h->copy_stream);
-    for (auto &lane : h->lanes) {
-        for (auto &[v, g] : lane.trace) destroy_graph(g);
-        destroy_graph(lane.finish);
-        if (lane.finished) cudaEventDestroy(lane.finished);
-        if (lane.h_plan) cudaFreeHost(lane.h_plan);
-        if (lane.own_stream && lane.stream) cudaStreamDestroy(lane.stream);
-        if (lane.block) cudaFree(lane.block);
-        lane = Lane{};
-    }
+    for (auto &[pass, gs] : h->retiring_scenes) lr_gpu_scene_destroy(gs);
+    h->retiring_scenes.clear();
+    if (h->display_block) cudaFree(h->display_block);
+    h->display_block = nullptr;
+    lanes_destroy(h);
     if (h->block) cudaFree(h->block);
 }
 
@@ -2683,6 +3045,14 @@ using namespace lr;
 struct lr_renderer {
     WaveHost wave;
     uint32_t bands = 1;
+    // The view it renders, and what a reload compares a scene with: a hash of the
+    // geometry (points and triangles, leaf order) and the triangles' shading as uploaded
+    // (normals and materials), staged for a reload's upload through `shading_stage`.
+    lr_frame frame{};
+    uint64_t geometry = 0;
+    std::vector<uint32_t> shading;
+    uint32_t *shading_stage = nullptr;
+    cudaEvent_t shading_copied = nullptr;
 };
 
 struct lr_batch {
@@ -2691,6 +3061,70 @@ struct lr_batch {
 
 namespace lr {
 namespace {
+
+// FNV-1a over a scene's geometry: its points and triangles in leaf order (same_geometry,
+// scene.lucb:168-181, asks the same of the geometry sets a compile starts from).
+uint64_t geometry_hash(const lr_scene &scene) {
+    uint64_t key = 14695981039346656037ull;
+    auto mix = [&](const void *data, size_t bytes) {
+        const unsigned char *p = (const unsigned char *)data;
+        for (size_t i = 0; i < bytes; i++) key = (key ^ p[i]) * 1099511628211ull;
+    };
+    const uint64_t counts[2] = {scene.point_count(), scene.triangle_count()};
+    mix(counts, sizeof counts);
+    mix(scene.positions.data(), scene.positions.size() * sizeof(float));
+    mix(scene.indices.data(), scene.indices.size() * sizeof(uint32_t));
+    return key;
+}
+
+// A renderer's three display images, for views of up to `pixels` (made again, none shown,
+// when a view outgrows them).
+void display_images(WaveHost *h, uint64_t pixels) {
+    if (h->display_block && pixels <= h->display_pixels) return;
+    if (h->display_block) {
+        settle(h);
+        LR_CUDA(cudaStreamSynchronize(h->ctx->stream));
+        LR_CUDA(cudaFree(h->display_block));
+        h->display_block = nullptr;
+    }
+    h->display_pixels = pixels;
+    LR_CUDA(cudaMalloc(&h->display_block, 3 * align256(pixels * 8)));
+    LR_CUDA(cudaMemsetAsync(h->display_block, 0, 3 * align256(pixels * 8), h->ctx->stream));
+    h->front = -1;
+    h->shown_width = h->shown_height = 0;
+}
+
+// The band a renderer's passes take for `pixels` (integrator.lucb:419-423).
+uint64_t band_of(const lr_settings &settings, uint64_t pixels) {
+    return std::min<uint64_t>(std::min<uint64_t>(settings.pool ? settings.pool : kDefaultPool, kMaxPool), pixels);
+}
+
+// Renderer.restart / reload / replace_scene: the member renewed through `frame`, its
+// bands and pass fill set for the new view. A view or scene that needs a larger path pool
+// or more rounds than the renderer's wave has waits for the passes in flight and makes
+// the wave again.
+void renderer_renew(lr_renderer *r, const lr_frame &frame, const lr_scene *scene, const lr_settings *settings,
+                    lr_gpu_scene *gs) {
+    WaveHost *h = &r->wave;
+    MemberHost &mh = member_at(h, 0);
+    const lr_settings &chosen = settings ? *settings : mh.settings;
+    validate(chosen, frame);
+    if ((bool)frame.orthographic != (mh.dev.frame[3] > 0.5f)) fail(LR_INVALID, "a restart keeps the view's projection");
+    const uint64_t pixels = (uint64_t)frame.width * frame.height;
+    const uint64_t band = band_of(chosen, pixels);
+    const uint64_t most_lights = light_paths_of(chosen, frame, pixels, 1, false).count;
+    const uint32_t rounds = scene ? rounds_of(*scene, chosen) : mh.dev.rounds;
+    // A view or scene that needs a larger path pool or more rounds than the wave has makes
+    // the lanes again after the passes in flight (the reference makes its view's buffers
+    // again in the same case).
+    if (band + most_lights > h->pool || rounds > h->rounds)
+        wave_resize(h, std::max<uint64_t>(band + most_lights, h->pool), std::max(rounds, h->rounds));
+    member_renew(h, 0, frame, scene, settings, gs, gs);
+    r->bands = (uint32_t)((pixels + band - 1) / band);
+    h->fill = (uint32_t)std::min<uint64_t>(band + h->members[0].dev.light_paths, h->pool);
+    h->camera_cap = (uint32_t)band;
+    display_images(h, pixels);
+}
 
 void create(lr_context *ctx, const lr_scene *scene, const lr_settings &settings, const lr_frame &frame, lr_renderer **out) {
     validate(settings, frame);
@@ -2711,6 +3145,10 @@ void create(lr_context *ctx, const lr_scene *scene, const lr_settings &settings,
         member_add(&r->wave, gs, gs, scene, settings, frame);
         r->wave.fill = (uint32_t)std::min<uint64_t>(band + r->wave.members[0].dev.light_paths, r->wave.pool);
         r->wave.camera_cap = (uint32_t)band;
+        display_images(&r->wave, pixels);
+        r->frame = frame;
+        r->geometry = geometry_hash(*scene);
+        r->shading = scene->shading;
         // The graphs for the scene's traversal variant, made now rather than at the first pass.
         const TraversalChoice c = choose_traversal(gs->scene, 0);
         if (!settings.profile)
@@ -2820,6 +3258,104 @@ int lr_renderer_image(lr_renderer *r, void **device_rgba) {
     });
 }
 
+int lr_renderer_restart(lr_renderer *r, const lr_frame *frame) {
+    return guarded([&] {
+        if (!r || !frame) fail(LR_INVALID, "restart needs a renderer and a frame");
+        LR_CUDA(cudaSetDevice(r->wave.ctx->device));
+        renderer_renew(r, *frame, nullptr, nullptr, nullptr);
+        r->frame = *frame;
+    });
+}
+
+int lr_renderer_reload(lr_renderer *r, const lr_scene *scene, const lr_settings *settings, const lr_frame *frame) {
+    return guarded([&] {
+        if (!r || !scene || !settings) fail(LR_INVALID, "reload needs a renderer, a scene and settings");
+        LR_CUDA(cudaSetDevice(r->wave.ctx->device));
+        if (geometry_hash(*scene) != r->geometry) fail(LR_INVALID, "a reload keeps the scene's geometry");
+        WaveHost *h = &r->wave;
+        MemberHost &mh = member_at(h, 0);
+        const lr_frame f = frame ? *frame : r->frame;
+        lr_settings chosen = *settings;
+        chosen.width = f.width;
+        chosen.height = f.height;
+        chosen.pool = mh.settings.pool;
+        chosen.software_bvh = mh.settings.software_bvh;
+        if (scene->shading != r->shading) {
+            // The triangles' normals and materials again, into the upload, after the passes in
+            // flight (the reference uploads the per-triangle shading again).
+            const size_t bytes = scene->shading.size() * sizeof(uint32_t);
+            if (r->shading_copied) LR_CUDA(cudaEventSynchronize(r->shading_copied));
+            else LR_CUDA(cudaEventCreateWithFlags(&r->shading_copied, cudaEventDisableTiming));
+            if (!r->shading_stage) LR_CUDA(cudaMallocHost((void **)&r->shading_stage, std::max<size_t>(bytes, 16)));
+            std::memcpy(r->shading_stage, scene->shading.data(), bytes);
+            after_passes(h);
+            LR_CUDA(cudaMemcpyAsync((void *)mh.dev.scene.shading, r->shading_stage, bytes, cudaMemcpyHostToDevice,
+                                    h->ctx->stream));
+            LR_CUDA(cudaEventRecord(r->shading_copied, h->ctx->stream));
+            r->shading = scene->shading;
+        }
+        renderer_renew(r, f, scene, &chosen, mh.owned);
+        r->frame = f;
+    });
+}
+
+int lr_renderer_replace_scene(lr_renderer *r, const lr_scene *scene, const lr_settings *settings, const lr_frame *frame) {
+    return guarded([&] {
+        if (!r || !scene || !settings || !frame) fail(LR_INVALID, "replace_scene needs a renderer, a scene, settings and a frame");
+        WaveHost *h = &r->wave;
+        MemberHost &mh = member_at(h, 0);
+        if (settings->pool != mh.settings.pool || settings->software_bvh != mh.settings.software_bvh)
+            fail(LR_INVALID, "a scene replaced keeps the pool and BVH choice");
+        LR_CUDA(cudaSetDevice(h->ctx->device));
+        lr_settings chosen = *settings;
+        chosen.width = frame->width;
+        chosen.height = frame->height;
+        lr_gpu_scene *gs = nullptr;
+        const int status = lr_gpu_scene_upload(h->ctx, scene, &gs);
+        if (status != LR_OK) fail(status, lr_last_error());
+        try {
+            renderer_renew(r, *frame, scene, &chosen, gs);
+        } catch (...) {
+            if (member_at(h, 0).owned != gs) lr_gpu_scene_destroy(gs);
+            throw;
+        }
+        r->frame = *frame;
+        r->geometry = geometry_hash(*scene);
+        r->shading = scene->shading;
+    });
+}
+
+int lr_renderer_display(lr_renderer *r, void **device_rgba16f) {
+    return guarded([&] {
+        if (!r || !device_rgba16f) fail(LR_INVALID, "no renderer");
+        WaveHost *h = &r->wave;
+        while (retire_one(h, false)) {
+        }
+        *device_rgba16f = display_image(h, h->front >= 0 ? h->front : 0);
+    });
+}
+
+int lr_renderer_shown_size(lr_renderer *r, uint32_t out[2]) {
+    return guarded([&] {
+        if (!r || !out) fail(LR_INVALID, "no renderer");
+        WaveHost *h = &r->wave;
+        while (retire_one(h, false)) {
+        }
+        out[0] = h->front >= 0 ? h->shown_width : 0u;
+        out[1] = h->front >= 0 ? h->shown_height : 0u;
+    });
+}
+
+int lr_renderer_set_display(lr_renderer *r, double exposure, int view) {
+    return guarded([&] {
+        if (!r) fail(LR_INVALID, "no renderer");
+        if (view != 0 && view != 1) fail(LR_INVALID, "a display view is 0 (standard) or 1 (neutral)");
+        r->wave.display_scale = (float)std::exp2(exposure);
+        r->wave.display_view = (uint32_t)view;
+        r->wave.display_stale = true;
+    });
+}
+
 int lr_renderer_read(lr_renderer *r, float *rgba, uint64_t count) {
     return guarded([&] {
         if (!r || !rgba) fail(LR_INVALID, "no renderer");
@@ -2884,6 +3420,8 @@ int lr_renderer_stats(lr_renderer *r, lr_render_stats *out) {
 void lr_renderer_destroy(lr_renderer *r) {
     if (!r) return;
     wave_destroy(&r->wave);
+    if (r->shading_copied) cudaEventDestroy(r->shading_copied);
+    if (r->shading_stage) cudaFreeHost(r->shading_stage);
     delete r;
 }
 
