@@ -356,6 +356,10 @@ int lr_renderer_shown_size(lr_renderer *renderer, uint32_t out[2]);
  * standard: clipped; 1 Khronos PBR Neutral tone mapping); the next pass, or a conversion
  * of its own once every sample is taken, applies it. */
 int lr_renderer_set_display(lr_renderer *renderer, double exposure, int view);
+/* Renderer.converged_pixels (integrator.lucb:759-768): how many pixels adaptive sampling
+ * (settings.noise_threshold > 0, checked every 4 samples from adaptive_minimum on) has
+ * stopped; waits for work in flight. */
+int lr_renderer_converged_pixels(lr_renderer *renderer, uint64_t *out);
 /* Renderer.kernel_times (integrator.lucb:873-875): milliseconds per kernel kind
  * over finished passes with settings.profile on, in the order camera, intersect
  * closest, shade surface, shade miss, intersect shadow, light emission, finish,

@@ -278,6 +278,7 @@ _SIGNATURES = {
     "lr_renderer_display": (C.c_int, [_vp, C.POINTER(_vp)]),
     "lr_renderer_shown_size": (C.c_int, [_vp, C.POINTER(C.c_uint32)]),
     "lr_renderer_set_display": (C.c_int, [_vp, C.c_double, C.c_int]),
+    "lr_renderer_converged_pixels": (C.c_int, [_vp, C.POINTER(C.c_uint64)]),
     "lr_renderer_read_wait": (C.c_int, [_vp]),
     "lr_batch_read_async": (C.c_int, [_vp, _u32, C.POINTER(C.c_float), _u64]),
     "lr_batch_read_wait": (C.c_int, [_vp]),
@@ -840,6 +841,12 @@ class Renderer:
 
     def set_display(self, exposure: float = 0.0, view: int = 0) -> None:
         _check(lib.lr_renderer_set_display(self.handle, exposure, view))
+
+    def converged_pixels(self) -> int:
+        """Renderer.converged_pixels: pixels adaptive sampling has stopped."""
+        out = C.c_uint64()
+        _check(lib.lr_renderer_converged_pixels(self.handle, C.byref(out)))
+        return int(out.value)
 
     def image(self) -> int:
         """The device address of the rgba32f image."""

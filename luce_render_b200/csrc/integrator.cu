@@ -86,6 +86,10 @@ struct Member {
     // its passes trace: its bounces + 1, + 8 for rays passing through cut-outs at the same
     // bounce (integrator.lucb:806-808); a ray for a later round is not traced.
     uint32_t cutouts, rounds;
+    // Adaptive sampling (adaptive.comp, finish.comp:22-23): the second estimate (odd
+    // samples, twice; w: converged) and the convergence verdicts, or null when off.
+    float4 *half;
+    float *scratch;
 };
 
 // Cut-out opacity (shade_surface.comp:95-104): whether the ray passes through material
@@ -118,7 +122,7 @@ struct Segment {
 // `camera_paths`: the pass's camera paths; `folds`: members whose light paths it traces.
 struct PlanHeader {
     uint32_t segments, paths, converts, dry;
-    uint32_t camera_paths, folds, reserved0, reserved1;
+    uint32_t camera_paths, folds, adapts, reserved;
 };
 
 // A renderer's display image for the pass (film_convert.comp:50-52): where the pass that
@@ -138,6 +142,7 @@ struct Plan {
     uint32_t convert[kMaxSegments];
     uint32_t convert_samples[kMaxSegments];
     uint32_t fold[kMaxSegments];
+    uint32_t adapt[kMaxSegments];  // members whose convergence the pass checks
     Segment seg[kMaxSegments];
 };
 
@@ -724,6 +729,14 @@ __global__ void __launch_bounds__(kShadeBlock) camera_kernel(Wave w) {
         }
         const uint32_t slot = sg.kind_base + (path - sg.path_base);
         const uint32_t pixel = sg.first_pixel + (path - sg.path_base);
+        if (m.half && m.half[pixel].w > 0.5f) {
+            // Converged (adaptive sampling): the pixel starts no path (camera.comp:18-21);
+            // its ray reaches nothing and its shading ends at once.
+            w.path[path] = make_uint4(kNone, 0u, 0u, 0u);
+            w.ray_o[0][slot] = make_float4(0.0f, 0.0f, 0.0f, __uint_as_float(path | (si << kPathBits)));
+            w.ray_d[0][slot] = make_float4(0.0f, 0.0f, 1.0f, 0.0f);
+            continue;
+        }
         const uint32_t sample = sg.sample;
         const uint32_t seed = m.k->seed;
         const float3 position = make_float3(m.frame[0], m.frame[1], m.frame[2]);
@@ -819,6 +832,7 @@ __device__ __noinline__ void shade_glossy(const Wave &w, const Member &m, uint32
     const uint32_t path = __float_as_uint(ro.w) & kPathMask;
     const uint4 pu = w.path[path];
     const uint32_t pixel = pu.x, bounces = pu.y, total = bounces & 0xffu;
+    if (pixel == kNone) return;  // a converged pixel's (adaptive sampling)
     const float ray_pdf = __uint_as_float(pu.w);
     const float3 origin = xyz(ro), dir = xyz(rd);
     float4 throughput = w.throughput[path];
@@ -1028,6 +1042,7 @@ __device__ __forceinline__ void shade_one(const Wave &w, const Member &m, uint32
     const uint32_t path = tag & kPathMask;
     uint4 pu = w.path[path];
     const uint32_t pixel = pu.x, bounces = pu.y, total = bounces & 0xffu;
+    if (pixel == kNone) return;  // a converged pixel's (adaptive sampling)
     const float ray_pdf = __uint_as_float(pu.w);
     const float3 origin = xyz(ro), dir = xyz(rd);
     float4 throughput = w.throughput[path];
@@ -1660,11 +1675,17 @@ __global__ void __launch_bounds__(kShadeBlock) finish_kernel(Wave w) {
         if (sg.kind == kLightSegment) continue;  // light paths reach the film by splats
         const Member &m = w.members[sg.member];
         const uint32_t pixel = w.path[path].x;
+        if (pixel == kNone) continue;  // converged: no sample taken
         float3 value = m.spectral ? spec_to_film<true>(w.radiance[path], w.lambda[path], *m.k)
                                   : spec_to_film<false>(w.radiance[path], make_float4(0, 0, 0, 0), *m.k);
         if (!isfinite(value.x) || !isfinite(value.y) || !isfinite(value.z)) value = make_float3(0.0f, 0.0f, 0.0f);
         const float4 f = m.film[pixel];
         m.film[pixel] = make_float4(f.x + value.x, f.y + value.y, f.z + value.z, f.w + 1.0f);
+        // Adaptive sampling's second estimate: every other sample, twice.
+        if (m.half && (sg.sample & 1u)) {
+            const float4 hs = m.half[pixel];
+            m.half[pixel] = make_float4(hs.x + 2.0f * value.x, hs.y + 2.0f * value.y, hs.z + 2.0f * value.z, hs.w);
+        }
     }
     if (blockIdx.x == 0 && threadIdx.x == 0) {
         unsigned long long closest = 0, shadow = 0;
@@ -1676,6 +1697,42 @@ __global__ void __launch_bounds__(kShadeBlock) finish_kernel(Wave w) {
         w.stats[1] += shadow;
         w.stats[2] += plan->head.camera_paths;
         w.stats[3] += 1;
+    }
+}
+
+// adaptive.comp (after Dammertz et al. and Cycles' film_adaptive_sampling), for the members
+// the pass checks: phase 0 judges each pixel by how far its full and half estimates differ
+// against the square root of its brightness; phase 1 marks a pixel converged (the half
+// estimate's w) when its whole 3 x 3 neighbourhood is, so noise at a converged pixel's
+// edge keeps it sampling.
+__global__ void __launch_bounds__(kShadeBlock) adaptive_kernel(Wave w, uint32_t phase) {
+    const Plan *plan = w.plan;
+    if (plan->head.dry) return;
+    const uint64_t stride = (uint64_t)gridDim.x * blockDim.x;
+    for (uint32_t a = 0; a < plan->head.adapts; a++) {
+        const Member &m = w.members[plan->adapt[a]];
+        const float threshold = m.k->noise_threshold;
+        for (uint64_t pixel = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; pixel < m.pixels; pixel += stride) {
+            if (phase == 0u) {
+                const float4 sum = m.film[pixel], half_sum = m.half[pixel];
+                const float scale = 1.0f / fmaxf(sum.w, 1.0f);
+                const float difference =
+                    (fabsf(sum.x - half_sum.x) + fabsf(sum.y - half_sum.y) + fabsf(sum.z - half_sum.z)) * scale;
+                const float brightness = fmaxf(0.0f, (sum.x + sum.y + sum.z) * scale);
+                const float error = difference / (0.0001f + sqrtf(brightness));
+                m.scratch[pixel] = error < threshold ? 1.0f : 0.0f;
+                continue;
+            }
+            const int x = (int)(pixel % m.width), y = (int)(pixel / m.width);
+            float converged = 1.0f;
+            for (int dy = -1; dy <= 1; dy++)
+                for (int dx = -1; dx <= 1; dx++) {
+                    const int nx = x + dx, ny = y + dy;
+                    if (nx < 0 || ny < 0 || nx >= (int)m.width || ny >= (int)m.height) continue;
+                    converged = fminf(converged, m.scratch[(uint64_t)ny * m.width + nx]);
+                }
+            m.half[pixel].w = converged;
+        }
     }
 }
 
@@ -1864,6 +1921,7 @@ struct MemberHost {
     void *view = nullptr;   // the view's memory: film, image, splat accumulators
     uint64_t view_pixels = 0;  // pixels the view memory holds
     bool view_traced = false;  // it holds splat accumulators
+    bool view_adaptive = false;  // it holds the half estimate and verdicts
     lr_gpu_scene *owned = nullptr;  // a renderer's own upload (null when borrowed)
     uint32_t samples = 0, sample = 0, next_pixel = 0, done = 0;
     uint32_t light_next = 0;  // light paths of the current sample planned so far
@@ -2016,6 +2074,9 @@ void record_finish(const WaveHost *h, const Wave &w, cudaStream_t stream, Marks 
     mark(stream, marks, kFinish);
     fold_kernel<<<h->grid_shade, kShadeBlock, 0, stream>>>(w);
     mark(stream, marks, kFinish);
+    adaptive_kernel<<<h->grid_shade, kShadeBlock, 0, stream>>>(w, 0u);
+    adaptive_kernel<<<h->grid_shade, kShadeBlock, 0, stream>>>(w, 1u);
+    mark(stream, marks, kAdaptive);
     convert_kernel<<<h->grid_shade, kShadeBlock, 0, stream>>>(w);
     mark(stream, marks, kConvert);
     LR_CUDA(cudaGetLastError());
@@ -2210,7 +2271,6 @@ void validate(const lr_settings &s, const lr_frame &f) {
         fail(LR_INVALID, "an image is 1 to 16384 pixels on a side");
     if (s.samples == 0 || s.max_bounces == 0 || s.max_bounces > 1024)
         fail(LR_INVALID, "a render needs samples and 1 to 1024 bounces");
-    if (s.noise_threshold > 0.0) fail(LR_INVALID, "adaptive sampling is not part of this build (noise_threshold 0)");
     if (s.guiding) fail(LR_INVALID, "path guiding is not part of this build (guiding off)");
     if (s.max_bounces > 253) fail(LR_INVALID, "this build traces at most 253 bounces");
 }
@@ -2300,6 +2360,7 @@ void loaded_records(const Loaded &L, const lr_settings &settings, double emit_sh
     k.emit_share = (float)emit_share;
     k.emit_radius = (float)L.emit_radius;
     k.emit_center = make_float3((float)L.emit_center.x, (float)L.emit_center.y, (float)L.emit_center.z);
+    k.noise_threshold = (float)std::max(0.0, settings.noise_threshold);
     r.lights = r.lay.add(L.lights.rows.data(), L.lights.rows.size() * 4);
     r.nodes = r.lay.add(L.tree.nodes.data(), L.tree.nodes.size() * 4);
     r.links = r.lay.add(L.tree.links.data(), L.tree.links.size() * 4);
@@ -2329,23 +2390,30 @@ void set_loaded(Member &m, const LoadedRecords &r, const Loaded &L, void *block,
 }
 
 // The view's memory for `pixels`: film, image and, for light tracing, the splat
-// accumulators (the film's and one per lane).
-Layout view_layout(uint64_t pixels, bool traced, size_t parts[5]) {
+// accumulators (the film's and one per lane); for adaptive sampling, the half estimate
+// and the verdicts.
+constexpr int kViewParts = 7;
+Layout view_layout(uint64_t pixels, bool traced, bool adaptive, size_t parts[kViewParts]) {
     Layout lay;
     parts[0] = lay.add(nullptr, pixels * 16);
     parts[1] = lay.add(nullptr, pixels * 16);
     const size_t splat_bytes = traced ? pixels * 24 : 0;
     for (int i = 2; i < 5; i++) parts[i] = lay.add(nullptr, splat_bytes);
+    parts[5] = lay.add(nullptr, adaptive ? pixels * 16 : 0);
+    parts[6] = lay.add(nullptr, adaptive ? pixels * 4 : 0);
     return lay;
 }
 
-void set_view_memory(Member &m, const Layout &lay, const size_t parts[5], void *view, bool traced) {
+void set_view_memory(Member &m, const Layout &lay, const size_t parts[kViewParts], void *view, bool traced,
+                     bool adaptive) {
     auto at = [&](size_t i) { return (void *)((char *)view + lay.parts[i].offset); };
     m.film = (float4 *)at(parts[0]);
     m.image = (float4 *)at(parts[1]);
     m.splat = traced ? (unsigned long long *)at(parts[2]) : nullptr;
     m.splat_lane[0] = traced ? (unsigned long long *)at(parts[3]) : nullptr;
     m.splat_lane[1] = traced ? (unsigned long long *)at(parts[4]) : nullptr;
+    m.half = adaptive ? (float4 *)at(parts[5]) : nullptr;
+    m.scratch = adaptive ? (float *)at(parts[6]) : nullptr;
 }
 
 // The view `m` renders: its frame, size and light paths.
@@ -2399,8 +2467,9 @@ uint32_t member_add(WaveHost *h, const lr_gpu_scene *gs, lr_gpu_scene *owned, co
     const LightPaths traced = light_paths_of(settings, frame, pixels, L.tree.emitter_count, emit_share > 0.0);
     LoadedRecords records;
     loaded_records(L, settings, emit_share, records);
-    size_t view_parts[5];
-    Layout view = view_layout(pixels, traced.count > 0, view_parts);
+    const bool adaptive = settings.noise_threshold > 0.0;
+    size_t view_parts[kViewParts];
+    Layout view = view_layout(pixels, traced.count > 0, adaptive, view_parts);
     MemberHost &mh = h->members[index];
     // Stream-ordered: the member's memory and data arrive ahead of the next pass without
     // waiting for the passes in flight.
@@ -2413,7 +2482,7 @@ uint32_t member_add(WaveHost *h, const lr_gpu_scene *gs, lr_gpu_scene *owned, co
     m = Member{};
     m.scene = gs->scene;
     set_loaded(m, records, L, mh.block, settings, rounds);
-    set_view_memory(m, view, view_parts, mh.view, traced.count > 0);
+    set_view_memory(m, view, view_parts, mh.view, traced.count > 0, adaptive);
     set_view(m, frame, traced);
     std::memcpy(stage, &m, sizeof m);
     LR_CUDA(cudaMemcpyAsync(h->d_members + index, stage, sizeof m, cudaMemcpyHostToDevice, stream));
@@ -2428,6 +2497,7 @@ uint32_t member_add(WaveHost *h, const lr_gpu_scene *gs, lr_gpu_scene *owned, co
     mh.last_pass = 0;
     mh.view_pixels = pixels;
     mh.view_traced = traced.count > 0;
+    mh.view_adaptive = adaptive;
     mh.settings = settings;
     mh.emitters = L.tree.emitter_count;
     mh.emit_share = L.emit_share;
@@ -2481,11 +2551,13 @@ void member_renew(WaveHost *h, uint32_t index, const lr_frame &frame, const lr_s
     }
     const uint64_t pixels = (uint64_t)frame.width * frame.height;
     const LightPaths traced = light_paths_of(chosen, frame, pixels, emitters, !frame.orthographic && emit_share > 0.0);
-    const bool new_view = pixels > mh.view_pixels || (traced.count > 0 && !mh.view_traced);
-    size_t view_parts[5];
+    const bool adaptive = chosen.noise_threshold > 0.0;
+    const bool new_view = pixels > mh.view_pixels || (traced.count > 0 && !mh.view_traced) || (adaptive && !mh.view_adaptive);
+    size_t view_parts[kViewParts];
     const uint64_t capacity = new_view ? roomy_pixels(frame) : mh.view_pixels;
     const bool view_traced = new_view ? traced.count > 0 : mh.view_traced;
-    Layout view = view_layout(capacity, view_traced, view_parts);
+    const bool view_adaptive = new_view ? adaptive : mh.view_adaptive;
+    Layout view = view_layout(capacity, view_traced, view_adaptive, view_parts);
     lay_out(view);
     char *stage = h->staging.take(sizeof(Member) + (scene ? staged_bytes(records.lay) : 0));
     size_t stage_at = sizeof(Member);
@@ -2505,15 +2577,19 @@ void member_renew(WaveHost *h, uint32_t index, const lr_frame &frame, const lr_s
         mh.view = fresh;
         mh.view_pixels = capacity;
         mh.view_traced = view_traced;
+        mh.view_adaptive = view_adaptive;
     } else {
         // The film starts over; the image keeps the last one until a sample replaces it.
         LR_CUDA(cudaMemsetAsync((char *)mh.view + view.parts[view_parts[0]].offset, 0, pixels * 16, stream));
         if (view_traced)
             LR_CUDA(cudaMemsetAsync((char *)mh.view + view.parts[view_parts[2]].offset, 0, pixels * 24, stream));
+        if (view_adaptive)
+            LR_CUDA(cudaMemsetAsync((char *)mh.view + view.parts[view_parts[5]].offset, 0, pixels * 16, stream));
     }
-    set_view_memory(m, view, view_parts, mh.view, view_traced);
+    set_view_memory(m, view, view_parts, mh.view, view_traced, view_adaptive);
     set_view(m, frame, traced);
     if (!traced.count) m.splat = m.splat_lane[0] = m.splat_lane[1] = nullptr;
+    if (!adaptive) m.half = nullptr, m.scratch = nullptr;
     mh.dev = m;
     std::memcpy(stage, &m, sizeof m);
     LR_CUDA(cudaMemcpyAsync(h->d_members + index, stage, sizeof m, cudaMemcpyHostToDevice, stream));
@@ -2634,7 +2710,7 @@ bool launch_pass(WaveHost *h, bool dry = false, int only = -1) {
     Lane &lane = lane_of(h, h->recorded);
     Plan *staging = lane.h_plan;
     Segment *seg = staging->seg;
-    uint32_t n = 0, used = 0, converts = 0, camera_paths = 0, folds = 0;
+    uint32_t n = 0, used = 0, converts = 0, camera_paths = 0, folds = 0, adapts = 0;
     uint64_t class_paths[kSizeClasses] = {0, 0, 0};
     PassRecord rec;
     rec.number = h->recorded;
@@ -2672,6 +2748,10 @@ bool launch_pass(WaveHost *h, bool dry = false, int only = -1) {
             if (ends) {
                 staging->convert[converts] = index;
                 staging->convert_samples[converts++] = mh.sample + 1;
+                // After every 4th sample past the minimum, check which pixels converged
+                // (integrator.lucb:819-826).
+                const uint32_t taken = mh.sample + 1;
+                if (mh.dev.half && taken >= mh.settings.adaptive_minimum && taken % 4u == 0u) staging->adapt[adapts++] = index;
             }
             used += count;
             camera_paths += count;
@@ -2717,7 +2797,7 @@ bool launch_pass(WaveHost *h, bool dry = false, int only = -1) {
                                      [&](const std::pair<uint32_t, bool> &e) { return h->members[e.first].dev.cutouts != 0u; });
     const int variant = width * 1000 + stack + (tracing ? kTracingVariant : 0) + (glossy ? kGlossyVariant : 0) +
                         (cutouts ? kCutoutVariant : 0);
-    staging->head = PlanHeader{n, used, converts, dry ? 1u : 0u, camera_paths, folds, 0u, 0u};
+    staging->head = PlanHeader{n, used, converts, dry ? 1u : 0u, camera_paths, folds, adapts, 0u};
     staging->display = PlanDisplay{0ull, h->display_scale, h->display_view, 0u, 0u};
     if (h->display_block && converts > 0) {
         rec.display_slot = free_display_slot(h);
@@ -3343,6 +3423,22 @@ int lr_renderer_shown_size(lr_renderer *r, uint32_t out[2]) {
         }
         out[0] = h->front >= 0 ? h->shown_width : 0u;
         out[1] = h->front >= 0 ? h->shown_height : 0u;
+    });
+}
+
+int lr_renderer_converged_pixels(lr_renderer *r, uint64_t *out) {
+    return guarded([&] {
+        if (!r || !out) fail(LR_INVALID, "no renderer");
+        WaveHost *h = &r->wave;
+        MemberHost &mh = member_at(h, 0);
+        *out = 0;
+        if (!mh.dev.half) return;
+        std::vector<float4> half(mh.dev.pixels);
+        join_lanes(h);
+        LR_CUDA(cudaMemcpyAsync(half.data(), mh.dev.half, half.size() * sizeof(float4), cudaMemcpyDeviceToHost,
+                                h->ctx->stream));
+        LR_CUDA(cudaStreamSynchronize(h->ctx->stream));
+        for (const float4 &v : half) *out += v.w > 0.5f ? 1u : 0u;
     });
 }
 

@@ -240,6 +240,7 @@ struct Constants {
     // disk they start on, facing the light (radius, centre).
     float emit_share, emit_radius;
     float3 emit_center;
+    float noise_threshold;  // adaptive sampling's (0: off)
 };
 
 template <bool kSpectral>

@@ -46,6 +46,13 @@ def cases():
     glossy_traced = settings(28, 24, 2, 5, True, seed=19)
     glossy_traced.light_tracing = 0.5
     out.append((sc, glossy_traced))
+    # Adaptive sampling: checks after samples 4 and 8 stop converged pixels.
+    meshes, cams, lights, mats = testscenes.area_light_scene()
+    sc = lr.compile_scene(meshes, cams, lights, mats)
+    adaptive = settings(32, 24, 8, 2, False, seed=29, material=lr.OpenPbr.lambert((0.5, 0.5, 0.5)))
+    adaptive.noise_threshold = 0.05
+    adaptive.adaptive_minimum = 4
+    out.append((sc, adaptive))
     # Cut-outs: 8 rounds more than the bounces, shadow rays walking through the veil.
     meshes, cams, lights, mats = testscenes.veil_scene(0.5)
     sc = lr.compile_scene(meshes, cams, lights, mats)

@@ -223,3 +223,33 @@ def test_renderer_read_async_is_the_image_of_its_pass(ctx):
     assert np.array_equal(hosts[2].array, final)
     for h in hosts:
         h.close()
+
+
+def test_adaptive_sampling(ctx):
+    # tests/gpu/integrator.lucb:334-358: a sphere under an area light, half the frame empty
+    # sky: with adaptive sampling the image is the same within 1 % (it stops sampling only
+    # where the image is clean) and at least a third of the pixels stop early.
+    sp, st, sn = scenes.icosphere(4, 1.0)
+    cam = lr.camera((1.5, 1.0, 5.0), (-math.atan2(1.0, math.hypot(1.5, 5.0)), math.atan2(1.5, 5.0), 0.0),
+                    focal_length=35.0, horizontal_aperture=36.0)
+    key = lr.light(lr.LIGHT_RECT, position=(1.0, 4.0, 1.0), rotation=(-1.2, 0.3, 0.0), intensity=20.0, width=2.0,
+                   height=2.0, normalize=True, visible=False)
+    sc = lr.compile_scene([lr.MeshData(sp, st, normals=sn)], [cam], [key])
+    sums, stopped, images = [], 0, []
+    for threshold in (0.01, 0.0):
+        s = lr.RenderSettings.of(64, 48, 64)
+        s.spectral = 0
+        s.noise_threshold = threshold
+        r = lr.Renderer.create(ctx, sc, s)
+        r.finish()
+        img = r.read()
+        images.append(img)
+        sums.append(img[..., 1].astype(np.float64).sum())
+        if threshold > 0.0:
+            stopped = r.converged_pixels()
+        r.destroy()
+    assert abs(sums[0] / sums[1] - 1.0) <= 0.01, sums
+    assert stopped >= 64 * 48 // 3, stopped
+    # The sky (nothing hit) converges at the first check and stays black.
+    sky = images[1][..., :3].sum(-1) == 0.0
+    assert sky.sum() > 0 and np.all(images[0][sky][:, :3] == 0.0)
