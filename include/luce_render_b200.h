@@ -101,6 +101,7 @@ typedef struct {
 #define LR_LIGHT_DISK 1
 #define LR_LIGHT_SPHERE 2
 #define LR_LIGHT_DISTANT 3
+#define LR_LIGHT_DOME 4
 typedef struct {
     double matrix[12];  /* columns x, y, z (the light shines down its -Z), translation */
     int32_t shape;      /* LR_LIGHT_* */
@@ -108,6 +109,14 @@ typedef struct {
     double intensity, exposure, temperature; /* temperature in kelvin, 0: none */
     double width, height, radius, angle;     /* rect size, disk/sphere radius, distant angle (deg) */
     int32_t normalize, visible;              /* UsdLux normalize; visible to the camera */
+    /* A dome's lat-long image (the pixels environment.lucb:102-156 reads from the dome's
+     * OpenEXR file, which this ABI takes decoded): linear Rec.709 RGB, 3 floats a pixel,
+     * image_width x image_height, rows from the top; its centre looks down the dome's -Z,
+     * its top is +Y. NULL: the dome shines its colour evenly. As in the reference
+     * (loading.lucb:55-61), only the first dome with an image lights by it. The compiled
+     * scene keeps a copy. Ignored for other shapes. */
+    const float *image;
+    uint32_t image_width, image_height;
 } lr_light;
 
 /* OpenPBR Surface parameters (src/render/materials.lucb:17-53), shaded as

@@ -35,7 +35,7 @@ LIBRARY_PATH = _HERE / "libluce_render_b200.so"
 
 INVALID, LIMIT, STOPPED, DEVICE, TIMEOUT = 400, 401, 402, 500, 504
 TRACE_ANY, TRACE_REFERENCE, TRACE_COUNT = 1, 2, 4
-LIGHT_RECT, LIGHT_DISK, LIGHT_SPHERE, LIGHT_DISTANT = 0, 1, 2, 3
+LIGHT_RECT, LIGHT_DISK, LIGHT_SPHERE, LIGHT_DISTANT, LIGHT_DOME = 0, 1, 2, 3, 4
 
 
 class RenderError(RuntimeError):
@@ -77,7 +77,8 @@ class Light(C.Structure):
     _fields_ = [("matrix", C.c_double * 12), ("shape", C.c_int32), ("color", C.c_double * 3),
                 ("intensity", C.c_double), ("exposure", C.c_double), ("temperature", C.c_double),
                 ("width", C.c_double), ("height", C.c_double), ("radius", C.c_double), ("angle", C.c_double),
-                ("normalize", C.c_int32), ("visible", C.c_int32)]
+                ("normalize", C.c_int32), ("visible", C.c_int32), ("image", C.POINTER(C.c_float)),
+                ("image_width", C.c_uint32), ("image_height", C.c_uint32)]
 
 
 class OpenPbr(C.Structure):
@@ -499,7 +500,9 @@ def camera(position, rotation=(0.0, 0.0, 0.0), projection: int = 0, focal_length
 def light(shape: int, position=(0.0, 0.0, 0.0), rotation=(0.0, 0.0, 0.0), color=(1.0, 1.0, 1.0),
           intensity: float = 1.0, exposure: float = 0.0, temperature: float = 0.0, width: float = 1.0,
           height: float = 1.0, radius: float = 0.5, angle: float = 0.0, normalize: bool = False,
-          visible: bool = True, matrix=None) -> Light:
+          visible: bool = True, matrix=None, image=None) -> Light:
+    """A UsdLux light. `image`, for a dome: its lat-long image as linear Rec.709 RGB,
+    height x width x 3 (rows from the top), kept alive with the light."""
     l = Light()
     l.matrix = _matrix12(matrix if matrix is not None else placement(position, rotation))
     l.shape = shape
@@ -508,6 +511,13 @@ def light(shape: int, position=(0.0, 0.0, 0.0), rotation=(0.0, 0.0, 0.0), color=
     l.width, l.height, l.radius, l.angle = width, height, radius, angle
     l.normalize = 1 if normalize else 0
     l.visible = 1 if visible else 0
+    if image is not None:
+        pixels = np.ascontiguousarray(image, np.float32)
+        if pixels.ndim != 3 or pixels.shape[2] != 3:
+            raise ValueError("a dome's image is height x width x 3")
+        l.keep_image = pixels
+        l.image = pixels.ctypes.data_as(C.POINTER(C.c_float))
+        l.image_height, l.image_width = pixels.shape[0], pixels.shape[1]
     return l
 
 

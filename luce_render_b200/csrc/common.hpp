@@ -78,6 +78,7 @@ M3 acescg_to_xyz_e();   // ACEScg -> XYZ under E
 V3 cmf_integrals();     // each CIE channel's sum over 360..830 nm at 1 nm
 void fit_spectrum(const V3 &rgb, double out[4]);
 V3 blackbody_xyz(double kelvin);
+M3 basis_weights();     // ACEScg -> weights of a dome texel's three basis spectra
 uint32_t octahedral(const V3 &n);
 
 // sampler.cpp: the 128 Sobol direction numbers (4 dimensions x 32 bits).
@@ -92,7 +93,8 @@ struct Scene {
     std::vector<lr_bvh_node> nodes;      // binned-SAH BVH2
     std::vector<uint32_t> order;         // source triangle at each leaf slot
     std::vector<lr_camera> cameras;
-    std::vector<lr_light> lights;
+    std::vector<lr_light> lights;        // image pointers cleared: the pixels are in light_images
+    std::vector<std::vector<float>> light_images;  // per light: a dome's RGB pixels (else empty)
     std::vector<lr_openpbr> materials;   // the library (material k+1 of the triangles)
     std::vector<uint8_t> used;           // which materials (0: default) triangles use
     uint32_t face_count = 0;

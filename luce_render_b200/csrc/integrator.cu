@@ -501,14 +501,15 @@ __device__ __forceinline__ float emitter_area_pdf(const Member &m, uint32_t emit
 
 // ---- Light paths from afar (lights.glsl:283-308) ----------------------------------------
 
-// A light path's emitter code for one from distant light `light` (common.glsl:178).
+// A light path's emitter code for one from dome or distant light `light` (common.glsl:176-178).
 constexpr uint32_t kAfarEmitter = 0x40000000u;
 
 __device__ __forceinline__ bool emits_from_afar(const float4 *lights, uint32_t light) {
-    return light_type(lights, light) == kLightDistant && light_at(lights, light, 2).w < 1.0f - 1e-7f;
+    const uint32_t type = light_type(lights, light);
+    return type == kLightDome || (type == kLightDistant && light_at(lights, light, 2).w < 1.0f - 1e-7f);
 }
 
-// The chance a light path leaves distant light `light` along -w (w toward the light).
+// The chance a light path leaves dome or distant light `light` along -w (w toward the light).
 __device__ __forceinline__ float afar_emission_pdf(const Member &m, uint32_t light, float3 w) {
     return m.k->emit_share * light_at(m.lights, light, 6).y *
            light_hit_pdf(m.lights, light, make_float3(0.0f, 0.0f, 0.0f), w, kInfinity);
@@ -591,7 +592,7 @@ __device__ __forceinline__ float light_sample_ratio(const Member &m, const Const
 }
 
 // light_emit.comp:21-130: light path `path` of segment `sg`, its sampler number
-// 0x80000000 | (band + its index), from a distant light with a size (by its share of
+// 0x80000000 | (band + its index), from a dome or a distant light with a size (by its share of
 // light paths) on a disk facing it, or from an emitter of the light tree chosen by power,
 // a point on it uniform by area, a cosine-weighted direction (either side of an emissive
 // triangle). A path that cannot start gets a ray that reaches nothing.
@@ -625,7 +626,10 @@ __device__ __forceinline__ void light_emit(const Wave &w, const Member &m, const
         const float2 disk = concentric(make_float2(u_point.z, u_point.w)) * radius;
         const float3 start = m.k->emit_center + toward * (2.0f * radius) + t * disk.x + b * disk.y;
         const float chance = afar * share * s.pdf;
-        const float4 carried = light_radiance<kSpectral>(m.lights, light, lambda) * (kPi * radius * radius / chance);
+        const float4 emitted = light_type(m.lights, light) == kLightDome
+                                   ? dome_radiance<kSpectral>(m.lights, light, toward, lambda)
+                                   : light_radiance<kSpectral>(m.lights, light, lambda);
+        const float4 carried = emitted * (kPi * radius * radius / chance);
         const float most = spec_max<kSpectral>(carried);
         if (!(most > 0.0f)) return dead();
         // The light "point" is a direction: its density is the chance, and the camera's
@@ -785,7 +789,8 @@ __device__ __forceinline__ float choose_light(const Member &m, const Constants &
         const uint32_t light = pick_distant(lights, m.light_count, u_light.x / k.p_distant, share);
         if (light != kNone && share > 0.0f && sample_light(lights, light, p, make_float2(u_light.y, u_light.z), s)) {
             afar = light;
-            emitted = light_radiance<kSpectral>(lights, light, lambda);
+            emitted = light_type(lights, light) == kLightDome ? dome_radiance<kSpectral>(lights, light, s.direction, lambda)
+                                                              : light_radiance<kSpectral>(lights, light, lambda);
             return k.p_distant * share;
         }
         return 0.0f;
@@ -848,9 +853,12 @@ __device__ __noinline__ void shade_glossy(const Wave &w, const Member &m, uint32
     if (what == kNone) {
         float4 r = spec_of<kSpectral>(k.background_fit, k.background_rgb, lambda);
         for (uint32_t light = 0; light < m.light_count; light++) {
-            if (light_type(lights, light) < kLightDistant) continue;
-            const float cos_half = light_at(lights, light, 2).w;
-            if (cos_half >= 1.0f - 1e-7f || dot(dir, -xyz(light_at(lights, light, 3))) < cos_half) continue;
+            const uint32_t type = light_type(lights, light);
+            if (type < kLightDistant) continue;
+            if (type == kLightDistant) {
+                const float cos_half = light_at(lights, light, 2).w;
+                if (cos_half >= 1.0f - 1e-7f || dot(dir, -xyz(light_at(lights, light, 3))) < cos_half) continue;
+            }
             float weight = 1.0f;
             if (total == 0u) {
                 if (!light_visible(lights, light)) continue;
@@ -864,7 +872,9 @@ __device__ __noinline__ void shade_glossy(const Wave &w, const Member &m, uint32
                 weight = mis_weight(light_hit_pdf(lights, light, make_float3(0.0f, 0.0f, 0.0f), dir, kInfinity) * select / ray_pdf,
                                     traced);
             }
-            r = r + light_radiance<kSpectral>(lights, light, lambda) * weight;
+            r = r + (type == kLightDome ? dome_radiance<kSpectral>(lights, light, dir, lambda)
+                                        : light_radiance<kSpectral>(lights, light, lambda)) *
+                        weight;
         }
         float4 contribution = throughput * r;
         const float largest = spec_max<kSpectral>(contribution);
@@ -1059,8 +1069,10 @@ __device__ __forceinline__ void shade_one(const Wave &w, const Member &m, uint32
         for (uint32_t light = 0; light < m.light_count; light++) {
             const uint32_t type = light_type(lights, light);
             if (type < kLightDistant) continue;
-            const float cos_half = light_at(lights, light, 2).w;
-            if (cos_half >= 1.0f - 1e-7f || dot(dir, -xyz(light_at(lights, light, 3))) < cos_half) continue;
+            if (type == kLightDistant) {
+                const float cos_half = light_at(lights, light, 2).w;
+                if (cos_half >= 1.0f - 1e-7f || dot(dir, -xyz(light_at(lights, light, 3))) < cos_half) continue;
+            }
             float weight = 1.0f;
             if (total == 0u) {
                 if (!light_visible(lights, light)) continue;
@@ -1069,7 +1081,9 @@ __device__ __forceinline__ void shade_one(const Wave &w, const Member &m, uint32
                 weight = mis_weight(light_hit_pdf(lights, light, make_float3(0.0f, 0.0f, 0.0f), dir, kInfinity) *
                                         select / ray_pdf, 0.0f);
             }
-            r = r + light_radiance<kSpectral>(lights, light, lambda) * weight;
+            r = r + (type == kLightDome ? dome_radiance<kSpectral>(lights, light, dir, lambda)
+                                        : light_radiance<kSpectral>(lights, light, lambda)) *
+                        weight;
         }
         float4 contribution = throughput * r;
         const float largest = spec_max<kSpectral>(contribution);
@@ -1162,7 +1176,8 @@ __device__ __forceinline__ void shade_one(const Wave &w, const Member &m, uint32
         const uint32_t light = pick_distant(lights, m.light_count, u_light.x / k.p_distant, share);
         if (light != kNone && share > 0.0f && sample_light(lights, light, p, make_float2(u_light.y, u_light.z), s)) {
             chance = k.p_distant * share;
-            emitted = light_radiance<kSpectral>(lights, light, lambda);
+            emitted = light_type(lights, light) == kLightDome ? dome_radiance<kSpectral>(lights, light, s.direction, lambda)
+                                                              : light_radiance<kSpectral>(lights, light, lambda);
             sampled = true;
         }
     } else {

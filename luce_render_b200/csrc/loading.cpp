@@ -5,6 +5,7 @@
 #include "loading.hpp"
 
 #include <algorithm>
+#include <cstring>
 #include <numeric>
 
 namespace lr {
@@ -80,11 +81,71 @@ void select_kth(const std::vector<Emitter> &e, uint32_t *order, size_t length, s
 
 }  // namespace
 
-LightRecords pack_lights(const std::vector<lr_light> &lights, double radius) {
+Environment environment_of(const std::vector<float> &pixels, uint32_t width, uint32_t height, bool spectral) {
+    // Linear Rec.709 (sRGB primaries, D65) to ACEScg, Bradford-adapted (environment.lucb:21-25).
+    static const M3 kRec709ToAcescg{{0.613097, 0.339523, 0.047379, 0.070194, 0.916354, 0.013452, 0.020616, 0.109570,
+                                     0.869815}};
+    const M3 basis = basis_weights();
+    Environment e;
+    e.width = width;
+    e.height = height;
+    e.texels.reserve((size_t)width * height * 4);
+    e.cdf.reserve((size_t)width * height + height);
+    std::vector<double> rows(height);
+    double luminance_sum = 0.0, solid_angle = 0.0;
+    for (uint32_t y = 0; y < height; y++) {
+        const double sin_theta = std::sin(kPi * ((double)y + 0.5) / (double)height);
+        double row = 0.0;
+        const size_t start = e.cdf.size();
+        for (uint32_t x = 0; x < width; x++) {
+            const float *p = &pixels[((size_t)y * width + x) * 3];
+            const V3 raw = kRec709ToAcescg.apply(V3(p[0], p[1], p[2]));
+            const V3 rgb(std::max(0.0, raw.x), std::max(0.0, raw.y), std::max(0.0, raw.z));
+            const double lum = luminance(rgb);
+            const double weight = lum * sin_theta;
+            // The spectral build keeps each texel as its basis spectra's weights, the
+            // 3 x 3 product spec_of_texel (spectrum.glsl:67-80) makes, done once here.
+            const V3 stored = spectral ? basis.apply(rgb) : rgb;
+            for (double value : {stored.x, stored.y, stored.z, weight}) e.texels.push_back((float)value);
+            row += weight;
+            e.cdf.push_back((float)row);
+            luminance_sum += lum * sin_theta;
+            solid_angle += sin_theta;
+        }
+        // Each row's cumulative weights end at 1 (uniform across an empty row).
+        for (uint32_t x = 0; x < width; x++)
+            e.cdf[start + x] = (float)(row > 0.0 ? (double)e.cdf[start + x] / row : (double)(x + 1) / (double)width);
+        rows[y] = row;
+    }
+    double total = 0.0;
+    for (double row : rows) total += row;
+    double running = 0.0;
+    for (uint32_t y = 0; y < height; y++) {
+        running += rows[y];
+        e.cdf.push_back((float)(total > 0.0 ? running / total : (double)(y + 1) / (double)height));
+    }
+    e.total = total;
+    e.average = solid_angle > 0.0 ? luminance_sum / solid_angle : 0.0;
+    return e;
+}
+
+LightRecords pack_lights(const std::vector<lr_light> &lights, const std::vector<std::vector<float>> &images,
+                         double radius, bool spectral) {
     LightRecords out;
     const M3 to_acescg = film_matrix();
     std::vector<double> powers;
-    for (const lr_light &light : lights) {
+    // The first dome with an image lights by it (loading.lucb:55-61).
+    Environment environment;
+    int32_t textured = -1;
+    for (size_t i = 0; i < lights.size(); i++)
+        if (lights[i].shape == LR_LIGHT_DOME && i < images.size() && !images[i].empty()) {
+            environment = environment_of(images[i], lights[i].image_width, lights[i].image_height, spectral);
+            textured = (int32_t)i;
+            break;
+        }
+    int32_t textured_record = -1;
+    for (size_t index = 0; index < lights.size(); index++) {
+        const lr_light &light = lights[index];
         const double *m = light.matrix;
         V3 position(m[9], m[10], m[11]);
         V3 mz(-m[6], -m[7], -m[8]);
@@ -107,6 +168,12 @@ LightRecords pack_lights(const std::vector<lr_light> &lights, double radius) {
             double det = V3(m[0], m[1], m[2]).dot(V3(m[3], m[4], m[5]).cross(V3(m[6], m[7], m[8])));
             size = light.radius * std::cbrt(std::fabs(det));
             area = 4.0 * kPi * size * size;
+        } else if (light.shape == LR_LIGHT_DOME) {
+            kind = 4.0;
+            u = unit(V3(m[0], m[1], m[2]), "a dome's x axis");
+            v = unit(V3(m[3], m[4], m[5]), "a dome's y axis");
+            // Rows 1-3 are the dome's axes (X, Y, Z): world to its frame.
+            emits = unit(V3(m[6], m[7], m[8]), "a dome's z axis");
         } else {
             kind = 3.0;
             cos_half = std::cos(0.5 * light.angle * kPi / 180.0);
@@ -134,6 +201,15 @@ LightRecords pack_lights(const std::vector<lr_light> &lights, double radius) {
         if (kind == 3.0)
             power = std::max(0.0, luminance(rgb)) * (cos_half < 1.0 - 1e-7 ? 2.0 * kPi * (1.0 - cos_half) : 1.0) * kPi *
                     radius * radius;
+        // A dome's power: what a sphere of its mean radiance pours into the scene's disk.
+        if (kind == 4.0) {
+            double mean = 1.0;
+            if ((int32_t)index == textured) {
+                mean = environment.average;
+                textured_record = (int32_t)powers.size();
+            }
+            power = std::max(0.0, luminance(rgb)) * mean * kPi * kPi * radius * radius;
+        }
         powers.push_back(power);
         const double rows[28] = {position.x, position.y, position.z, kind,   u.x,    u.y,    u.z,    size,
                                  v.x,        v.y,        v.z,        cos_half, emits.x, emits.y, emits.z, area,
@@ -163,6 +239,33 @@ LightRecords pack_lights(const std::vector<lr_light> &lights, double radius) {
         row6[2] = (float)running;
     }
     out.distant_power = total;
+    // The textured dome's texels (a float4 each), then its cumulative weights, after the
+    // records. The reference keeps where they start in two constant rows (K_DOME,
+    // K_DOME_CDF); here the dome's own record holds them, in slots a dome leaves unused:
+    // row 0 x the weights' sum, rows 1-3 w the texels' first float4, the width and the
+    // height, row 6 w the cumulative weights' first float (the integers as their bits).
+    if (textured_record >= 0) {
+        float *record = &out.rows[(size_t)textured_record * 28];
+        auto bits = [](size_t v) {
+            const uint32_t u = (uint32_t)v;
+            float f;
+            std::memcpy(&f, &u, 4);
+            return f;
+        };
+        const size_t texel_base = out.rows.size() / 4;
+        out.rows.insert(out.rows.end(), environment.texels.begin(), environment.texels.end());
+        const size_t cdf_base = out.rows.size();
+        out.rows.insert(out.rows.end(), environment.cdf.begin(), environment.cdf.end());
+        while (out.rows.size() % 4 != 0) out.rows.push_back(0.0f);
+        if (out.rows.size() >= ((size_t)1 << 32)) fail(LR_LIMIT, "a dome's image does not fit the light records");
+        record[0] = (float)environment.total;
+        record[1] = record[2] = 0.0f;
+        record[7] = bits(texel_base);
+        record[11] = bits(environment.width);
+        record[15] = bits(environment.height);
+        record[27] = bits(cdf_base);
+        out.dome = textured_record;
+    }
     return out;
 }
 
@@ -381,16 +484,17 @@ Loaded load(const Scene &scene, const lr_settings &settings) {
             L.cutouts = L.cutouts || L.library[i].geometry_opacity < 1.0;
         }
     L.radius = scene_radius(scene);
-    L.lights = pack_lights(scene.lights, L.radius);
+    L.lights = pack_lights(scene.lights, scene.light_images, L.radius, settings.spectral != 0);
     L.tree = build_light_tree(scene, L.lights, L.library);
     for (size_t i = 0; i < L.library.size(); i++) pack_material(L.library[i], -1.0f, L.materials);
-    // Distant lights with a size start light paths too, on a disk around what casts
-    // caustics, sharing them with the tree's emitters by power (loading.lucb:127-146);
+    // Domes and distant lights with a size start light paths too, on a disk around what
+    // casts caustics, sharing them with the tree's emitters by power (loading.lucb:127-146);
     // looked for only when such a light would aim light paths at it. An orthographic
     // view takes no light paths at all (the member drops the share).
     bool sized = false;
     for (size_t i = 0; i < L.lights.count; i++)
-        sized = sized || (L.lights.rows[i * 28 + 3] == 3.0f && L.lights.rows[i * 28 + 11] < 1.0f - 1e-7f);
+        sized = sized || L.lights.rows[i * 28 + 3] == 4.0f ||
+                (L.lights.rows[i * 28 + 3] == 3.0f && L.lights.rows[i * 28 + 11] < 1.0f - 1e-7f);
     if (sized && settings.light_tracing > 0.0) {
         V3 center;
         double reach = 1.0;

@@ -7,11 +7,23 @@
 
 namespace lr {
 
-// Light records: 7 vec4 (28 floats) per light, as shaders/lights.glsl:1-22 lays them out.
+// Light records: 7 vec4 (28 floats) per light, as shaders/lights.glsl:1-22 lays them out,
+// then the textured dome's texels and cumulative weights (pack_lights says where).
 struct LightRecords {
     std::vector<float> rows;
     size_t count = 0;
-    double distant_power = 0.0;
+    double distant_power = 0.0;  // distant lights' and domes' power
+    int32_t dome = -1;           // the light whose image the records hold (-1: none)
+};
+
+// A dome's image sampled by importance (environment.lucb:60-156): per texel its colour
+// (ACEScg, or in the spectral build its three basis spectra's weights) and its weight
+// (luminance x sin theta); each row's cumulative weights, then the rows'; their sum and
+// the mean luminance over the sphere.
+struct Environment {
+    uint32_t width = 0, height = 0;
+    std::vector<float> texels, cdf;
+    double total = 0.0, average = 0.0;
 };
 
 // The light tree (light_tree.lucb:16-20): 12 floats per node (lo, energy; hi, cos theta_o;
@@ -42,7 +54,9 @@ struct Loaded {
     V3 cmf_integrals;
 };
 
-LightRecords pack_lights(const std::vector<lr_light> &lights, double radius);
+Environment environment_of(const std::vector<float> &pixels, uint32_t width, uint32_t height, bool spectral);
+LightRecords pack_lights(const std::vector<lr_light> &lights, const std::vector<std::vector<float>> &images,
+                         double radius, bool spectral);
 LightTree build_light_tree(const Scene &scene, const LightRecords &lights, const std::vector<lr_openpbr> &library);
 void pack_material(const lr_openpbr &m, float program, std::vector<float> &out);
 double scene_radius(const Scene &scene);

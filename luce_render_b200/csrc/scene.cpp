@@ -216,10 +216,19 @@ int lr_scene_compile(const lr_mesh *meshes, size_t mesh_count, const lr_camera *
         for (size_t i = 0; i < mesh_count; i++) add_mesh(*scene, meshes[i], face_base, material_count);
         scene->face_count = face_base;
         scene->cameras.assign(cameras, cameras + camera_count);
-        for (size_t i = 0; i < light_count; i++)
-            if (lights[i].shape < 0 || lights[i].shape > 3)
-                fail(LR_INVALID, "a light is rect, disk, sphere or distant");
+        scene->light_images.resize(light_count);
+        for (size_t i = 0; i < light_count; i++) {
+            const lr_light &l = lights[i];
+            if (l.shape < 0 || l.shape > LR_LIGHT_DOME) fail(LR_INVALID, "a light is rect, disk, sphere, distant or dome");
+            if (l.shape != LR_LIGHT_DOME || !l.image) continue;
+            // A dome's image (environment.lucb:102-156; the reference caps images at 2^26 pixels).
+            const uint64_t pixels = (uint64_t)l.image_width * l.image_height;
+            if (pixels == 0) fail(LR_INVALID, "a dome's image has no pixels");
+            if (pixels > (1ull << 26)) fail(LR_LIMIT, "a dome's image is larger than 67,108,864 pixels");
+            scene->light_images[i].assign(l.image, l.image + pixels * 3);
+        }
         scene->lights.assign(lights, lights + light_count);
+        for (lr_light &l : scene->lights) l.image = nullptr;
         build_bvh(*scene);
         *out = scene.release();
     });

@@ -260,7 +260,7 @@ __device__ __forceinline__ float3 spec_to_film(float4 radiance, float4 lambda, c
 // ---- lights.glsl ---------------------------------------------------------------------
 
 constexpr uint32_t kLightStride = 7;
-constexpr uint32_t kLightRect = 0, kLightDisk = 1, kLightSphere = 2, kLightDistant = 3;
+constexpr uint32_t kLightRect = 0, kLightDisk = 1, kLightSphere = 2, kLightDistant = 3, kLightDome = 4;
 
 struct LightSample {
     float3 direction;
@@ -290,6 +290,100 @@ __device__ __forceinline__ float4 light_radiance(const float4 *lights, uint32_t 
         radiance.w *= blackbody(lambda.w, kelvin);
     }
     return radiance;
+}
+
+// ---- Dome lights (lights.glsl:89-174): a lat-long image around the scene, its centre
+// down the dome's -Z, its top +Y; a dome with no image (or not the one image the records
+// hold) shines its colour evenly.
+
+// Where the records keep the textured dome's image (loading.cpp's pack_lights): its
+// texels (colour or basis weights, and the sampling weight), cumulative weights (each
+// row's, then the rows'), size and weights' sum.
+struct DomeImage {
+    const float4 *texels;
+    const float *cdf;
+    uint32_t width, height;
+    float total;
+};
+
+__device__ __forceinline__ bool dome_image(const float4 *lights, uint32_t light, DomeImage &image) {
+    const uint32_t base = __float_as_uint(light_at(lights, light, 1).w);
+    if (base == 0u) return false;
+    image.texels = lights + base;
+    image.width = __float_as_uint(light_at(lights, light, 2).w);
+    image.height = __float_as_uint(light_at(lights, light, 3).w);
+    image.cdf = reinterpret_cast<const float *>(lights) + __float_as_uint(light_at(lights, light, 6).w);
+    image.total = light_at(lights, light, 0).x;
+    return true;
+}
+
+// dome_texel (lights.glsl:99-110): the texel world direction d falls in, and sin theta there.
+__device__ __forceinline__ uint32_t dome_texel(const float4 *lights, uint32_t light, const DomeImage &image, float3 d,
+                                               float &sin_theta) {
+    const float3 l = make_float3(dot(d, xyz(light_at(lights, light, 1))), dot(d, xyz(light_at(lights, light, 2))),
+                                 dot(d, xyz(light_at(lights, light, 3))));
+    const float u = 0.5f + atan2f(l.x, -l.z) * (0.5f / kPi);
+    const float v = acosf(fminf(fmaxf(l.y, -1.0f), 1.0f)) / kPi;
+    sin_theta = sqrtf(fmaxf(0.0f, 1.0f - l.y * l.y));
+    const uint32_t x = min((uint32_t)(u * (float)image.width), image.width - 1u);
+    const uint32_t y = min((uint32_t)(v * (float)image.height), image.height - 1u);
+    return y * image.width + x;
+}
+
+// spec_of_texel (spectrum.glsl:61-80): the spectral build's texel holds the weights of
+// three smooth spectra that sum to the flat one (blue, green, red); the RGB build's its
+// ACEScg as it is.
+template <bool kSpectral>
+__device__ __forceinline__ float4 spec_of_texel(float3 texel, float4 lambda) {
+    if (!kSpectral) return make_float4(texel.x, texel.y, texel.z, 0.0f);
+    const float l[4] = {lambda.x, lambda.y, lambda.z, lambda.w};
+    float out[4];
+#pragma unroll
+    for (int i = 0; i < 4; i++) {
+        const float blue = 1.0f - 1.0f / (1.0f + expf(-(l[i] - 490.0f) / 12.0f));
+        const float red = 1.0f / (1.0f + expf(-(l[i] - 595.0f) / 12.0f));
+        out[i] = texel.x * blue + texel.y * (1.0f - blue - red) + texel.z * red;
+    }
+    return make_float4(out[0], out[1], out[2], out[3]);
+}
+
+// dome_radiance (lights.glsl:112-118): the dome's radiance toward -d (d toward the dome).
+template <bool kSpectral>
+__device__ __forceinline__ float4 dome_radiance(const float4 *lights, uint32_t light, float3 d, float4 lambda) {
+    const float4 radiance = light_radiance<kSpectral>(lights, light, lambda);
+    DomeImage image;
+    if (!dome_image(lights, light, image)) return radiance;
+    float sin_theta;
+    const float4 texel = __ldg(&image.texels[dome_texel(lights, light, image, d, sin_theta)]);
+    return radiance * spec_of_texel<kSpectral>(xyz(texel), lambda);
+}
+
+// dome_pdf (lights.glsl:120-129): the solid-angle pdf of sampling direction d (the
+// selection's chance not included): a texel's weight over the sum, spread over its solid
+// angle.
+__device__ __forceinline__ float dome_pdf(const float4 *lights, uint32_t light, float3 d) {
+    DomeImage image;
+    if (!dome_image(lights, light, image)) return 1.0f / (4.0f * kPi);
+    float sin_theta;
+    const uint32_t texel = dome_texel(lights, light, image, d, sin_theta);
+    if (sin_theta <= 0.0f) return 0.0f;
+    const float weight = __ldg(&image.texels[texel]).w;
+    return weight / image.total * (float)image.width * (float)image.height / (2.0f * kPi * kPi * sin_theta);
+}
+
+// dome_search (lights.glsl:136-150): the first of `count` cumulative weights from `first`
+// that passes u, and u's place within it (0..1).
+__device__ __forceinline__ uint32_t dome_search(const float *cdf, uint32_t first, uint32_t count, float u, float &within) {
+    uint32_t low = 0u, high = count - 1u;
+    while (low < high) {
+        const uint32_t middle = (low + high) / 2u;
+        if (__ldg(&cdf[first + middle]) > u) high = middle;
+        else low = middle + 1u;
+    }
+    const float below = low > 0u ? __ldg(&cdf[first + low - 1u]) : 0.0f;
+    const float above = __ldg(&cdf[first + low]);
+    within = above > below ? fminf(fmaxf((u - below) / (above - below), 0.0f), 0.99999994f) : 0.5f;
+    return low;
 }
 
 __device__ __forceinline__ uint32_t pick_distant(const float4 *lights, uint32_t count, float u, float &pdf) {
@@ -327,10 +421,37 @@ __device__ __forceinline__ float sphere_hit(float3 center, float radius, float3 
     return t > 0.0f ? t : kInfinity;
 }
 
+// sample_dome (lights.glsl:152-174): a direction by the image's weights (rows, then the
+// chosen row's texels), or uniform over the sphere for a dome without an image.
+__device__ __forceinline__ bool sample_dome(const float4 *lights, uint32_t light, float2 u, LightSample &s) {
+    s.distance = kInfinity;
+    s.delta = false;
+    s.cos_light = 1.0f;
+    float3 l;
+    DomeImage image;
+    if (!dome_image(lights, light, image)) {
+        const float z = 1.0f - 2.0f * u.x;
+        const float r = sqrtf(fmaxf(0.0f, 1.0f - z * z));
+        l = make_float3(r * cosf(2.0f * kPi * u.y), z, r * sinf(2.0f * kPi * u.y));
+    } else {
+        float fy, fx;
+        const uint32_t y = dome_search(image.cdf, image.width * image.height, image.height, u.y, fy);
+        const uint32_t x = dome_search(image.cdf, y * image.width, image.width, u.x, fx);
+        const float theta = kPi * ((float)y + fy) / (float)image.height;
+        const float phi = 2.0f * kPi * (((float)x + fx) / (float)image.width - 0.5f);
+        l = make_float3(sinf(theta) * sinf(phi), cosf(theta), -sinf(theta) * cosf(phi));
+    }
+    s.direction = normalize(xyz(light_at(lights, light, 1)) * l.x + xyz(light_at(lights, light, 2)) * l.y +
+                            xyz(light_at(lights, light, 3)) * l.z);
+    s.pdf = dome_pdf(lights, light, s.direction);
+    return s.pdf > 0.0f;
+}
+
 __device__ __forceinline__ bool sample_light(const float4 *lights, uint32_t light, float3 p, float2 u, LightSample &s) {
     const float4 row0 = light_at(lights, light, 0), row1 = light_at(lights, light, 1), row2 = light_at(lights, light, 2),
                  row3 = light_at(lights, light, 3);
     const uint32_t type = (uint32_t)row0.w;
+    if (type == kLightDome) return sample_dome(lights, light, u, s);
     s.delta = false;
     s.cos_light = 1.0f;
     if (type == kLightRect || type == kLightDisk) {
@@ -407,6 +528,7 @@ __device__ __forceinline__ float light_hit_pdf(const float4 *lights, uint32_t li
         return 1.0f / (2.0f * kPi * fmaxf(1e-12f, 1.0f - cos_max));
     }
     if (type == kLightDistant) return 1.0f / (2.0f * kPi * fmaxf(1e-12f, 1.0f - light_at(lights, light, 2).w));
+    if (type == kLightDome) return dome_pdf(lights, light, d);
     const float4 row3 = light_at(lights, light, 3);
     const float cos_light = fmaxf(1e-12f, -dot(d, xyz(row3)));
     return t * t / (cos_light * row3.w);

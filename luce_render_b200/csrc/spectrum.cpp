@@ -134,6 +134,31 @@ V3 blackbody_xyz(double kelvin) {
     return {sum.x / integrals.x, sum.y / integrals.y, sum.z / integrals.z};
 }
 
+// The three smooth spectra a dome's texel is made of (environment.lucb:27-35): blue below
+// ~490 nm, red above ~595 nm, green between; they sum to the flat spectrum.
+V3 basis_spectra(double lambda) {
+    const double blue = 1.0 - 1.0 / (1.0 + std::exp(-(lambda - 490.0) / 12.0));
+    const double red = 1.0 / (1.0 + std::exp(-(lambda - 595.0) / 12.0));
+    return {blue, 1.0 - blue - red, red};
+}
+
+// basis_weights (environment.lucb:37-58): ACEScg -> the basis spectra's weights, the
+// inverse of the matrix whose columns are the basis spectra's colours through the film.
+M3 basis_weights() {
+    const V3 integrals = cmf_integrals();
+    V3 columns[3];
+    for (double lambda = kLambdaMin; lambda <= kLambdaMax; lambda += 1.0) {
+        const V3 b = basis_spectra(lambda), matching = cmf(lambda);
+        for (int k = 0; k < 3; k++) columns[k] = columns[k] + matching * b[k];
+    }
+    const M3 film = film_matrix();
+    V3 rgb[3];
+    for (int k = 0; k < 3; k++)
+        rgb[k] = film.apply({columns[k].x / integrals.x, columns[k].y / integrals.y, columns[k].z / integrals.z});
+    const M3 colors{{rgb[0].x, rgb[1].x, rgb[2].x, rgb[0].y, rgb[1].y, rgb[2].y, rgb[0].z, rgb[1].z, rgb[2].z}};
+    return inv(colors);
+}
+
 uint32_t octahedral(const V3 &n) {
     double length = std::fabs(n.x) + std::fabs(n.y) + std::fabs(n.z);
     if (length <= 0.0) return octahedral({0.0, 1.0, 0.0});

@@ -1,14 +1,14 @@
 """Scenes of the reference's closed-form integrator checks (tests/gpu/integrator.lucb),
 rebuilt from this package's own primitives: a 20 x 20 floor of 8 divisions under a
-1 x 1 light at height 1, seen from the side; the same light as an emissive quad; and a
-coloured (or blackbody) 2 x 2 light over a white floor."""
+1 x 1 light at height 1, seen from the side; the same light as an emissive quad; a
+coloured (or blackbody) 2 x 2 light over a white floor; cut-outs; and dome lights."""
 from __future__ import annotations
 
 import math
 
 import numpy as np
 
-from . import (LIGHT_RECT, MeshData, OpenPbr, camera, light, placement)
+from . import (LIGHT_DOME, LIGHT_RECT, MeshData, OpenPbr, camera, light, placement)
 from .scenes import grid
 
 
@@ -97,3 +97,47 @@ def veil_scene(opacity: float):
     lamp = light(LIGHT_RECT, position=(0.0, 1.0, 0.0), rotation=(-0.5 * math.pi, 0.0, 0.0), intensity=4.0,
                  width=1.0, height=1.0, normalize=False, visible=False)
     return [_floor(), sheet], [cam], [lamp], [veil]
+
+
+# ---- dome lights (integrator.lucb:495-582) -----------------------------------------------
+
+
+def dome_furnace_scene(level: int = 4):
+    """integrator.lucb:495-518: a white sphere under a white dome with no image (intensity
+    1, visible, turned about +Y): the furnace again, lit by the dome's light samples and BSDF
+    hits under MIS instead of the background. The sphere is this package's icosphere; its
+    material is the settings' default."""
+    from .scenes import furnace_sphere
+    meshes, cams = furnace_sphere(level)
+    sky = light(LIGHT_DOME, rotation=(0.3, 1.0, 0.0), intensity=1.0, visible=True)
+    return meshes, cams, [sky], []
+
+
+def sun_sky(width: int = 64, height: int = 32):
+    """integrator.lucb:520-549: a dim grey sky (0.5) with a 2 x 2-texel sun 400 times
+    brighter, as linear Rec.709 (height x width x 3), and the irradiance a floor facing +Y
+    receives from it (cos theta integrated over each texel in 8 x 8 pieces)."""
+    sky = np.full((height, width, 3), 0.5, np.float32)
+    sky[8:10, 40:42] = 200.0
+    irradiance = 0.0
+    for y in range(height):
+        for sy in range(8):
+            theta = math.pi * (y + (sy + 0.5) / 8.0) / height
+            c = math.cos(theta)
+            if c <= 0.0:
+                continue
+            row = float(sky[y, :, 1].astype(np.float64).sum())
+            irradiance += row * c * math.sin(theta) * (math.pi / height / 8.0) * (2.0 * math.pi / width)
+    return sky, irradiance
+
+
+def dome_sun_scene():
+    """integrator.lucb:551-582: a 20 x 20 floor under the sun sky's dome (+Y up), seen
+    straight down from height 4 (50 mm on a 36 mm film): with one bounce, what the floor
+    reflects straight up is albedo / pi x the image's irradiance, which needs the image
+    sampled by importance (the sun is 1/512 of the texels). Returns (meshes, cameras,
+    lights, materials, irradiance)."""
+    sky, irradiance = sun_sky()
+    cam = camera((0.0, 4.0, 0.0), (-0.5 * math.pi, 0.0, 0.0), focal_length=50.0, horizontal_aperture=36.0)
+    dome = light(LIGHT_DOME, intensity=1.0, visible=False, image=sky)
+    return [_floor()], [cam], [dome], [], irradiance

@@ -153,6 +153,129 @@ typedef struct {
     int delta;
 } lsample;
 
+/* ---- dome lights (lights.glsl:89-174, environment.lucb) --------------------------------- */
+
+typedef struct {
+    const float *texels, *cdf;
+    uint32_t width, height;
+    double total;
+} dome_img;
+
+static uint32_t bits_of(float f) {
+    uint32_t u;
+    memcpy(&u, &f, 4);
+    return u;
+}
+
+/* The textured dome's image, where its record says the light rows hold it. */
+static int dome_image(const or_render_desc *r, uint32_t light, dome_img *img) {
+    uint32_t base = bits_of(row(r, light, 1)[3]);
+    if (base == 0) return 0;
+    img->texels = &r->light_rows[(size_t)base * 4];
+    img->width = bits_of(row(r, light, 2)[3]);
+    img->height = bits_of(row(r, light, 3)[3]);
+    img->cdf = &r->light_rows[bits_of(row(r, light, 6)[3])];
+    img->total = row(r, light, 0)[0];
+    return 1;
+}
+
+/* dome_texel (lights.glsl:99-110). */
+static uint32_t dome_texel(const or_render_desc *r, uint32_t light, const dome_img *img, d3 d, double *sin_theta) {
+    d3 l = v3(dot(d, rv(row(r, light, 1))), dot(d, rv(row(r, light, 2))), dot(d, rv(row(r, light, 3))));
+    double u = 0.5 + atan2(l.x, -l.z) * (0.5 / PI);
+    double v = acos(fmin(fmax(l.y, -1.0), 1.0)) / PI;
+    *sin_theta = sqrt(fmax(0.0, 1.0 - l.y * l.y));
+    uint32_t x = (uint32_t)(u * (double)img->width), y = (uint32_t)(v * (double)img->height);
+    if (x > img->width - 1) x = img->width - 1;
+    if (y > img->height - 1) y = img->height - 1;
+    return y * img->width + x;
+}
+
+static double basis_matrix[9];
+static pthread_once_t basis_once = PTHREAD_ONCE_INIT;
+static void basis_init(void) { or_basis_weights(basis_matrix); }
+
+/* spec_of_texel (spectrum.glsl:61-80): ACEScg through the basis spectra, or as it is. */
+static spec spec_of_texel(const or_render_desc *r, const float *texel, const double lambda[4]) {
+    spec s = spec_zero();
+    if (!r->spectral) {
+        for (int i = 0; i < 3; i++) s.s[i] = texel[i];
+        return s;
+    }
+    pthread_once(&basis_once, basis_init);
+    double w[3];
+    for (int i = 0; i < 3; i++)
+        w[i] = basis_matrix[i * 3] * texel[0] + basis_matrix[i * 3 + 1] * texel[1] + basis_matrix[i * 3 + 2] * texel[2];
+    for (int i = 0; i < 4; i++) {
+        double b[3];
+        or_basis_spectra(lambda[i], b);
+        s.s[i] = w[0] * b[0] + w[1] * b[1] + w[2] * b[2];
+    }
+    return s;
+}
+
+/* dome_radiance (lights.glsl:112-118): toward -d, d toward the dome. */
+static spec dome_radiance(const or_render_desc *r, uint32_t light, d3 d, const double lambda[4]) {
+    spec radiance = light_radiance(r, light, lambda);
+    dome_img img;
+    if (!dome_image(r, light, &img)) return radiance;
+    double sin_theta;
+    uint32_t texel = dome_texel(r, light, &img, d, &sin_theta);
+    return spec_mul(radiance, spec_of_texel(r, &img.texels[(size_t)texel * 4], lambda));
+}
+
+/* dome_pdf (lights.glsl:120-129). */
+static double dome_pdf(const or_render_desc *r, uint32_t light, d3 d) {
+    dome_img img;
+    if (!dome_image(r, light, &img)) return 1.0 / (4.0 * PI);
+    double sin_theta;
+    uint32_t texel = dome_texel(r, light, &img, d, &sin_theta);
+    if (sin_theta <= 0.0) return 0.0;
+    double weight = img.texels[(size_t)texel * 4 + 3];
+    return weight / img.total * (double)img.width * (double)img.height / (2.0 * PI * PI * sin_theta);
+}
+
+/* dome_search (lights.glsl:136-150). */
+static uint32_t dome_search(const float *cdf, uint32_t first, uint32_t count, double u, double *within) {
+    uint32_t low = 0, high = count - 1;
+    while (low < high) {
+        uint32_t middle = (low + high) / 2;
+        if (cdf[first + middle] > u) high = middle;
+        else low = middle + 1;
+    }
+    double below = low > 0 ? cdf[first + low - 1] : 0.0, above = cdf[first + low];
+    *within = above > below ? fmin(fmax((u - below) / (above - below), 0.0), 0.99999994) : 0.5;
+    return low;
+}
+
+/* sample_dome (lights.glsl:152-174). */
+static int sample_dome(const or_render_desc *r, uint32_t light, double u0, double u1, lsample *s) {
+    s->distance = INF;
+    s->delta = 0;
+    s->cos_light = 1.0;
+    d3 l;
+    dome_img img;
+    if (!dome_image(r, light, &img)) {
+        double z = 1.0 - 2.0 * u0, rr = sqrt(fmax(0.0, 1.0 - z * z));
+        l = v3(rr * cos(2.0 * PI * u1), z, rr * sin(2.0 * PI * u1));
+    } else {
+        double fy, fx;
+        uint32_t y = dome_search(img.cdf, img.width * img.height, img.height, u1, &fy);
+        uint32_t x = dome_search(img.cdf, y * img.width, img.width, u0, &fx);
+        double theta = PI * ((double)y + fy) / (double)img.height;
+        double phi = 2.0 * PI * (((double)x + fx) / (double)img.width - 0.5);
+        l = v3(sin(theta) * sin(phi), cos(theta), -sin(theta) * cos(phi));
+    }
+    s->direction = norm(add(add(mul(rv(row(r, light, 1)), l.x), mul(rv(row(r, light, 2)), l.y)), mul(rv(row(r, light, 3)), l.z)));
+    s->pdf = dome_pdf(r, light, s->direction);
+    return s->pdf > 0.0;
+}
+
+/* The radiance a dome or distant light sends toward -d. */
+static spec far_radiance(const or_render_desc *r, uint32_t light, d3 d, const double lambda[4]) {
+    return light_type(r, light) == 4 ? dome_radiance(r, light, d, lambda) : light_radiance(r, light, lambda);
+}
+
 static d3 sample_cone(d3 axis, double cos_max, double u0, double u1) {
     double c = 1.0 - u0 * (1.0 - cos_max), s = sqrt(fmax(0.0, 1.0 - c * c)), phi = 2.0 * PI * u1;
     d3 t, b;
@@ -174,6 +297,7 @@ static double sphere_hit(d3 c, double radius, d3 o, d3 d) {
 static int sample_light(const or_render_desc *r, uint32_t light, d3 p, double u0, double u1, lsample *s) {
     const float *r0 = row(r, light, 0), *r1 = row(r, light, 1), *r2 = row(r, light, 2), *r3 = row(r, light, 3);
     uint32_t type = (uint32_t)r0[3];
+    if (type == 4) return sample_dome(r, light, u0, u1, s);
     s->delta = 0;
     s->cos_light = 1.0;
     if (type == 0 || type == 1) {
@@ -248,6 +372,7 @@ static double light_hit_pdf(const or_render_desc *r, uint32_t light, d3 o, d3 d,
         return 1.0 / (2.0 * PI * fmax(1e-12, 1.0 - cos_max));
     }
     if (type == 3) return 1.0 / (2.0 * PI * fmax(1e-12, 1.0 - row(r, light, 2)[3]));
+    if (type == 4) return dome_pdf(r, light, d);
     const float *r3 = row(r, light, 3);
     double cl = fmax(1e-12, -dot(d, rv(r3)));
     return t * t / (cl * r3[3]);
@@ -444,7 +569,8 @@ static double emitter_area_pdf(const or_render_desc *r, uint32_t emitter) {
 #define AFAR_EMITTER 0x40000000u
 
 static int emits_from_afar(const or_render_desc *r, uint32_t light) {
-    return light_type(r, light) == 3 && row(r, light, 2)[3] < 1.0f - 1e-7f;
+    uint32_t type = light_type(r, light);
+    return type == 4 || (type == 3 && row(r, light, 2)[3] < 1.0f - 1e-7f);
 }
 
 static double afar_emission_pdf(const or_render_desc *r, uint32_t light, d3 w) {
@@ -618,8 +744,10 @@ static void render_sample(const or_render_desc *r, uint32_t pixel, uint32_t samp
             spec bg = spec_of(r, r->background_fit, r->background_rgb, lambda);
             for (uint32_t l = 0; l < r->light_count; l++) {
                 if (light_type(r, l) < 3) continue;
-                double cos_half = row(r, l, 2)[3];
-                if (cos_half >= 1.0 - 1e-7 || dot(dir, neg(rv(row(r, l, 3)))) < cos_half) continue;
+                if (light_type(r, l) == 3) {
+                    double cos_half = row(r, l, 2)[3];
+                    if (cos_half >= 1.0 - 1e-7 || dot(dir, neg(rv(row(r, l, 3)))) < cos_half) continue;
+                }
                 double weight = 1.0;
                 if (total == 0) {
                     if (!light_visible(r, l)) continue;
@@ -630,7 +758,7 @@ static void render_sample(const or_render_desc *r, uint32_t pixel, uint32_t samp
                         traced = mis[0] * (afar_first_density(r, vertex, dir, mis[2]) / mis[1]) * (afar_emission_pdf(r, l, dir) / ray_pdf);
                     weight = mis_weight(light_hit_pdf(r, l, v3(0, 0, 0), dir, INF) * (r->p_distant * row(r, l, 6)[1]) / ray_pdf, traced);
                 }
-                bg = spec_add(bg, spec_scale(light_radiance(r, l, lambda), weight));
+                bg = spec_add(bg, spec_scale(far_radiance(r, l, dir, lambda), weight));
             }
             spec c = spec_mul(throughput, bg);
             double m = spec_max(r, c);
@@ -715,7 +843,7 @@ static void render_sample(const or_render_desc *r, uint32_t pixel, uint32_t samp
             if (l != NONE && share > 0.0 && sample_light(r, l, p, ul[1], ul[2], &s)) {
                 afar = l;
                 chance = r->p_distant * share;
-                emitted = light_radiance(r, l, lambda);
+                emitted = far_radiance(r, l, s.direction, lambda);
                 sampled = 1;
             }
         } else {
@@ -895,7 +1023,7 @@ static void trace_light_path(const or_render_desc *r, uint32_t sample, uint32_t 
         d3 start = add(add(add(v3(r->emit_center[0], r->emit_center[1], r->emit_center[2]), mul(w, 2.0 * radius)),
                            mul(t, dx * radius)), mul(b, dy * radius));
         double chance = afar * share * s.pdf;
-        throughput = spec_scale(light_radiance(r, l, lambda), PI * radius * radius / chance);
+        throughput = spec_scale(far_radiance(r, l, w, lambda), PI * radius * radius / chance);
         double most = spec_max(r, throughput);
         if (!(most > 0.0)) return;
         /* The light "point" is a direction: its density is the chance, and the camera's

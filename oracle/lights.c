@@ -76,13 +76,92 @@ void or_pack_material(const or_material *m, float program, float out[64]) {
     for (int k = 0; k < 24; k++) out[at++] = (float)rest[k];
 }
 
-/* pack_lights (lights.lucb:29-131); domes are not part of this path. */
+/* The first dome with an image (loading.lucb:55-61), or -1. */
+static long textured_dome(const or_light *lights, size_t count) {
+    for (size_t i = 0; i < count; i++)
+        if (lights[i].shape == 4 && lights[i].image && lights[i].image_width > 0 && lights[i].image_height > 0)
+            return (long)i;
+    return -1;
+}
+
+size_t or_pack_lights_size(const or_light *lights, size_t count) {
+    size_t floats = count * 28;
+    long dome = textured_dome(lights, count);
+    if (dome >= 0) {
+        size_t texels = (size_t)lights[dome].image_width * lights[dome].image_height;
+        floats += texels * 4 + texels + lights[dome].image_height + 3;
+    }
+    return floats;
+}
+
+static float float_bits(size_t v) {
+    uint32_t u = (uint32_t)v;
+    float f;
+    memcpy(&f, &u, 4);
+    return f;
+}
+
+/* environment_of (environment.lucb:118-156) into `texels` (4 floats each) and `cdf`
+ * (width*height + height floats); *total the weights' sum, *average the mean luminance. */
+static void environment_of(const or_light *light, float *texels, float *cdf, double *total, double *average) {
+    static const double to_acescg[9] = {0.613097, 0.339523, 0.047379, 0.070194, 0.916354, 0.013452,
+                                        0.020616, 0.109570, 0.869815};
+    const uint32_t width = light->image_width, height = light->image_height;
+    double *rows = malloc(sizeof(double) * height);
+    double luminance_sum = 0.0, solid_angle = 0.0;
+    size_t at_cdf = 0, at_texel = 0;
+    for (uint32_t y = 0; y < height; y++) {
+        double sin_theta = sin(PI * ((double)y + 0.5) / (double)height);
+        double row = 0.0;
+        size_t start = at_cdf;
+        for (uint32_t x = 0; x < width; x++) {
+            const float *p = &light->image[((size_t)y * width + x) * 3];
+            double source[3] = {p[0], p[1], p[2]}, rgb[3];
+            for (int i = 0; i < 3; i++)
+                rgb[i] = fmax(0.0, to_acescg[i * 3] * source[0] + to_acescg[i * 3 + 1] * source[1] +
+                                       to_acescg[i * 3 + 2] * source[2]);
+            double lum = luminance(rgb), weight = lum * sin_theta;
+            texels[at_texel++] = (float)rgb[0];
+            texels[at_texel++] = (float)rgb[1];
+            texels[at_texel++] = (float)rgb[2];
+            texels[at_texel++] = (float)weight;
+            row += weight;
+            cdf[at_cdf++] = (float)row;
+            luminance_sum += lum * sin_theta;
+            solid_angle += sin_theta;
+        }
+        for (uint32_t x = 0; x < width; x++)
+            cdf[start + x] = (float)(row > 0.0 ? (double)cdf[start + x] / row : (double)(x + 1) / (double)width);
+        rows[y] = row;
+    }
+    double sum = 0.0, running = 0.0;
+    for (uint32_t y = 0; y < height; y++) sum += rows[y];
+    for (uint32_t y = 0; y < height; y++) {
+        running += rows[y];
+        cdf[at_cdf++] = (float)(sum > 0.0 ? running / sum : (double)(y + 1) / (double)height);
+    }
+    free(rows);
+    *total = sum;
+    *average = solid_angle > 0.0 ? luminance_sum / solid_angle : 0.0;
+}
+
+/* pack_lights (lights.lucb:29-131). */
 size_t or_pack_lights(const or_light *lights, size_t count, double radius, float *out,
                       double *distant_power) {
     double film[9];
     or_film_matrix(film);
     double *powers = malloc(sizeof(double) * (count + 1));
     size_t n = 0;
+    long dome = textured_dome(lights, count);
+    long dome_record = -1;
+    double dome_total = 0.0, dome_average = 0.0;
+    float *texels = NULL, *cdf = NULL;
+    if (dome >= 0) {
+        size_t pixels = (size_t)lights[dome].image_width * lights[dome].image_height;
+        texels = malloc(sizeof(float) * pixels * 4);
+        cdf = malloc(sizeof(float) * (pixels + lights[dome].image_height));
+        environment_of(&lights[dome], texels, cdf, &dome_total, &dome_average);
+    }
     for (size_t index = 0; index < count; index++) {
         const or_light *light = &lights[index];
         const double *m = light->matrix;
@@ -114,6 +193,15 @@ size_t or_pack_lights(const or_light *lights, size_t count, double radius, float
                          m[6] * (m[1] * m[5] - m[2] * m[4]);
             size = light->radius * cbrt(fabs(det));
             area = 4.0 * PI * size * size;
+        } else if (light->shape == 4) {
+            /* Rows 1-3 are the dome's axes (X, Y, Z): world to its frame. */
+            kind = 4.0;
+            double lx = vlen(&m[0]), ly = vlen(&m[3]), lz = vlen(&m[6]);
+            for (int k = 0; k < 3; k++) {
+                u[k] = m[k] / lx;
+                v[k] = m[3 + k] / ly;
+                emits[k] = m[6 + k] / lz;
+            }
         } else {
             kind = 3.0;
             cos_half = cos(0.5 * light->angle * PI / 180.0);
@@ -142,6 +230,15 @@ size_t or_pack_lights(const or_light *lights, size_t count, double radius, float
         if (kind == 3.0)
             power = fmax(0.0, luminance(rgb)) * (cos_half < 1.0 - 1e-7 ? 2.0 * PI * (1.0 - cos_half) : 1.0) *
                     PI * radius * radius;
+        if (kind == 4.0) {
+            /* What a sphere of its mean radiance pours into the scene's disk. */
+            double mean = 1.0;
+            if ((long)index == dome) {
+                mean = dome_average;
+                dome_record = (long)n;
+            }
+            power = fmax(0.0, luminance(rgb)) * mean * PI * PI * radius * radius;
+        }
         powers[n] = power;
         double rows[28] = {position[0], position[1], position[2], kind, u[0], u[1], u[2], size,
                            v[0], v[1], v[2], cos_half, emits[0], emits[1], emits[2], area,
@@ -172,6 +269,27 @@ size_t or_pack_lights(const or_light *lights, size_t count, double radius, float
         row6[2] = (float)running;
     }
     free(powers);
+    if (dome_record >= 0) {
+        const uint32_t width = lights[dome].image_width, height = lights[dome].image_height;
+        const size_t pixels = (size_t)width * height;
+        size_t at = n * 28;
+        const size_t texel_base = at / 4;
+        memcpy(&out[at], texels, sizeof(float) * pixels * 4);
+        at += pixels * 4;
+        const size_t cdf_base = at;
+        memcpy(&out[at], cdf, sizeof(float) * (pixels + height));
+        at += pixels + height;
+        while (at % 4 != 0) out[at++] = 0.0f;
+        float *record = &out[dome_record * 28];
+        record[0] = (float)dome_total;
+        record[1] = record[2] = 0.0f;
+        record[7] = float_bits(texel_base);
+        record[11] = float_bits(width);
+        record[15] = float_bits(height);
+        record[27] = float_bits(cdf_base);
+    }
+    free(texels);
+    free(cdf);
     if (distant_power) *distant_power = total;
     return n;
 }

@@ -164,11 +164,13 @@ void or_octahedral_decode(uint32_t packed, double out[3]);
 
 typedef struct {
     double matrix[12]; /* columns x, y, z, translation */
-    int shape;         /* 0 rect, 1 disk, 2 sphere, 3 distant */
+    int shape;         /* 0 rect, 1 disk, 2 sphere, 3 distant, 4 dome */
     double color[3];
     double intensity, exposure, temperature;
     double width, height, radius, angle;
     int normalize, visible;
+    const float *image; /* a dome's linear Rec.709 RGB, 3 floats a pixel, rows from the top */
+    uint32_t image_width, image_height;
 } or_light;
 
 typedef struct {
@@ -187,10 +189,18 @@ typedef struct {
 void or_material_standard(or_material *m);
 /* pack_material (materials.lucb:105-119): 64 floats. */
 void or_pack_material(const or_material *m, float program, float out[64]);
-/* pack_lights (lights.lucb:29-131): 28 floats per light into `out` (count*28).
- * Returns the light count; *distant_power the distant lights' power. */
+/* pack_lights (lights.lucb:29-131): 28 floats per light into `out`, then the textured
+ * dome's image as environment_of (environment.lucb:118-156) makes it: its texels (ACEScg
+ * and weight, 4 floats each) and cumulative weights (each row's, then the rows'), padded
+ * to a multiple of 4 floats; the dome's record holds where (row 0 x the weights' sum;
+ * rows 1, 2, 3 w the texels' first float4, the width, the height; row 6 w the cumulative
+ * weights' first float; the integers as their bits). `out` holds or_pack_lights_size
+ * floats. Returns the light count; *distant_power the distant lights' and domes' power. */
+size_t or_pack_lights_size(const or_light *lights, size_t count);
 size_t or_pack_lights(const or_light *lights, size_t count, double radius, float *out,
                       double *distant_power);
+void or_basis_spectra(double lambda, double out[3]);
+void or_basis_weights(double out[9]);
 
 typedef struct {
     float *nodes;      /* 12 floats per node */

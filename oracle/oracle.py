@@ -49,7 +49,8 @@ class OrLight(C.Structure):
     _fields_ = [("matrix", C.c_double * 12), ("shape", C.c_int), ("color", C.c_double * 3),
                 ("intensity", C.c_double), ("exposure", C.c_double), ("temperature", C.c_double),
                 ("width", C.c_double), ("height", C.c_double), ("radius", C.c_double), ("angle", C.c_double),
-                ("normalize", C.c_int), ("visible", C.c_int)]
+                ("normalize", C.c_int), ("visible", C.c_int), ("image", C.POINTER(C.c_float)),
+                ("image_width", C.c_uint32), ("image_height", C.c_uint32)]
 
 
 class OrMaterial(C.Structure):
@@ -93,6 +94,8 @@ lib.or_table_albedo.restype = C.c_double
 lib.or_table_albedo.argtypes = [C.c_double, C.c_double, C.c_double]
 lib.or_albedo_tables.restype = C.POINTER(C.c_double)
 lib.or_pack_lights.restype = C.c_size_t
+lib.or_pack_lights_size.restype = C.c_size_t
+lib.or_pack_lights_size.argtypes = [C.POINTER(OrLight), C.c_size_t]
 lib.or_pack_lights.argtypes = [C.POINTER(OrLight), C.c_size_t, C.c_double, C.POINTER(C.c_float),
                                C.POINTER(C.c_double)]
 lib.or_ray_frame.argtypes = [C.POINTER(C.c_double), C.c_int, C.c_double, C.c_double, C.c_double, C.c_double,
@@ -328,11 +331,16 @@ def light_from(l) -> OrLight:
     return o
 
 
-def pack_lights(lights, radius: float):
+def pack_lights(lights, radius: float, with_image: bool = False):
+    """pack_lights (lights.lucb:29-131): (records n x 28, distant and dome power); with
+    `with_image`, the flat rows with the textured dome's texels and cumulative weights
+    after the records, and the light count: (rows, power, n)."""
     arr = (OrLight * max(1, len(lights)))(*[light_from(l) for l in lights])
-    out = np.zeros(max(1, len(lights)) * 28, np.float32)
+    out = np.zeros(max(28, lib.or_pack_lights_size(arr, len(lights))), np.float32)
     power = C.c_double()
     n = lib.or_pack_lights(arr, len(lights), radius, _p(out, _f), C.byref(power))
+    if with_image:
+        return out, power.value, n
     return out[: n * 28].reshape(-1, 28).copy(), power.value
 
 
@@ -480,7 +488,8 @@ def _render_desc(arrays, lights, library, frame, max_bounces, spectral, seed, ba
     if T and root["lo"][0] <= root["hi"][0]:
         d = (root["hi"].astype(np.float64) - root["lo"].astype(np.float64))
         radius = max(1.0, 0.5 * float(np.sqrt((d * d).sum())))
-    rows, distant_power = pack_lights(list(lights), radius)
+    flat_rows, distant_power, light_count = pack_lights(list(lights), radius, with_image=True)
+    rows = flat_rows[: light_count * 28].reshape(-1, 28)
     mats = [m if isinstance(m, OrMaterial) else material_from(m) for m in library]
     tree = light_tree(positions, indices, shading, rows, mats)
     total = distant_power + tree["energy"]
@@ -489,7 +498,7 @@ def _render_desc(arrays, lights, library, frame, max_bounces, spectral, seed, ba
     else:
         p_distant = 1.0 if distant_power > 0 else 0.0
     material_rows = np.concatenate([pack_material(m) for m in mats]).astype(np.float32)
-    rows = np.ascontiguousarray(rows.reshape(-1), np.float32)
+    rows = np.ascontiguousarray(flat_rows, np.float32)
     tnodes = np.ascontiguousarray(tree["nodes"].reshape(-1), np.float32)
     tlinks = np.ascontiguousarray(tree["links"].reshape(-1), np.uint32)
     trec = np.ascontiguousarray(tree["records"], np.uint32)
@@ -499,7 +508,7 @@ def _render_desc(arrays, lights, library, frame, max_bounces, spectral, seed, ba
     r.triangle_count = T
     r.nodes = nodes.ctypes.data_as(C.c_void_p)
     r.light_rows = _p(rows, _f)
-    r.light_count = len(rows) // 28
+    r.light_count = light_count
     r.tree_nodes = _p(tnodes, _f) if len(tnodes) else None
     r.tree_links = _p(tlinks, _u) if len(tlinks) else None
     r.tree_records = _p(trec, _u) if len(trec) else None
@@ -524,9 +533,11 @@ def _render_desc(arrays, lights, library, frame, max_bounces, spectral, seed, ba
     # use has geometry_opacity below 1.
     used = set(int(x) for x in np.asarray(shading, np.uint32).reshape(-1, 4)[:, 3]) if T else set()
     r.through = 8 if any(i < len(mats) and mats[i].geometry_opacity < 1.0 for i in used) else 0
-    # Light paths from afar (loading.lucb:127-146): distant lights with a size share light
-    # paths with the tree's emitters by power, on a disk around what casts caustics.
-    sized = any(row[3] == 3.0 and row[11] < np.float32(1.0) - np.float32(1e-7) for row in rows.reshape(-1, 28))
+    # Light paths from afar (loading.lucb:127-146): domes and distant lights with a size
+    # share light paths with the tree's emitters by power, on a disk around what casts
+    # caustics.
+    sized = any(row[3] == 4.0 or (row[3] == 3.0 and row[11] < np.float32(1.0) - np.float32(1e-7))
+                for row in flat_rows[: light_count * 28].reshape(-1, 28))
     r.emit_share, r.emit_radius = 0.0, 1.0
     if sized and light_tracing > 0.0 and not frame.orthographic:
         found = caster_bounds(positions, indices, shading, mats)

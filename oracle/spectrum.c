@@ -112,6 +112,38 @@ void or_cmf_integrals(double out[3]) {
     memcpy(out, sum, sizeof sum);
 }
 
+/* basis_spectra (environment.lucb:27-35): blue, green, red at lambda nm. */
+void or_basis_spectra(double lambda, double out[3]) {
+    double blue = 1.0 - 1.0 / (1.0 + exp(-(lambda - 490.0) / 12.0));
+    double red = 1.0 / (1.0 + exp(-(lambda - 595.0) / 12.0));
+    out[0] = blue;
+    out[1] = 1.0 - blue - red;
+    out[2] = red;
+}
+
+/* basis_weights (environment.lucb:37-58): ACEScg to the basis spectra's weights, the
+ * inverse of their colours through the film. */
+void or_basis_weights(double out[9]) {
+    double integrals[3], columns[3][3] = {{0}}, b[3], c[3];
+    or_cmf_integrals(integrals);
+    for (double lambda = LAMBDA_MIN; lambda <= LAMBDA_MAX; lambda += 1.0) {
+        or_basis_spectra(lambda, b);
+        or_cmf(lambda, c);
+        for (int k = 0; k < 3; k++)
+            for (int i = 0; i < 3; i++) columns[k][i] += c[i] * b[k];
+    }
+    mat3 film;
+    or_film_matrix(film.m);
+    double rgb[3][3];
+    for (int k = 0; k < 3; k++) {
+        double xyz[3] = {columns[k][0] / integrals[0], columns[k][1] / integrals[1], columns[k][2] / integrals[2]};
+        apply(&film, xyz, rgb[k]);
+    }
+    mat3 colors = {{rgb[0][0], rgb[1][0], rgb[2][0], rgb[0][1], rgb[1][1], rgb[2][1], rgb[0][2], rgb[1][2], rgb[2][2]}};
+    mat3 w = inverse(&colors);
+    memcpy(out, w.m, sizeof w.m);
+}
+
 static double sigmoid(double z) { return 0.5 + z / (2.0 * sqrt(1.0 + z * z)); }
 
 enum { FIT_SAMPLES = 95 };

@@ -1,6 +1,7 @@
 """Render cases shared by the batch and server tests: (compiled scene, settings) pairs of
-uneven sizes, spectral and RGB, depths 2 to 8, Lambertian, glossy and cut-out, with and
-without light tracing, and the image a Renderer makes of each."""
+uneven sizes, spectral and RGB, depths 2 to 8, Lambertian, glossy and cut-out, lit by
+rect, distant, emissive and dome lights, with and without light tracing, and the image a
+Renderer makes of each."""
 import luce_render_b200 as lr
 from luce_render_b200 import scenes, testscenes
 
@@ -57,6 +58,14 @@ def cases():
     meshes, cams, lights, mats = testscenes.veil_scene(0.5)
     sc = lr.compile_scene(meshes, cams, lights, mats)
     out.append((sc, settings(24, 24, 4, 2, False, seed=23, material=lr.OpenPbr.lambert((0.5, 0.5, 0.5)))))
+    # A dome light with an image over glossy objects, with light paths from afar.
+    meshes, cams, lights, mats, background = scenes.caustic_scene()
+    sky, _ = testscenes.sun_sky()
+    dome = lr.light(lr.LIGHT_DOME, rotation=(0.0, 0.7, 0.0), intensity=0.5, image=sky)
+    sc = lr.compile_scene(meshes, cams, [dome], mats)
+    domed = settings(32, 24, 3, 5, True, seed=31, background=background)
+    domed.light_tracing = 0.5
+    out.append((sc, domed))
     return out
 
 
