@@ -159,6 +159,14 @@ int lr_scene_compile(const lr_mesh *meshes, size_t mesh_count, const lr_camera *
                      const lr_openpbr *materials, size_t material_count, lr_scene **out);
 /* CompiledScene.close (scene.lucb:87-98). */
 void lr_scene_free(lr_scene *scene);
+/* (No counterpart: the reference compiles a moved mesh again, rebuilding its BVH2,
+ * bvh.lucb:66-82.) Moves a compiled scene's points to `positions` (3 floats a point, world
+ * space, in the scene's point order: the meshes' points in the order they were passed)
+ * with the triangles kept, and refits the BVH2 in place: every node's box again from its
+ * triangles or children, the topology and leaf order unchanged; triangles compiled
+ * without authored normals get their new flat normals. What lr_gpu_scene_refit does on
+ * the device, on the host. */
+int lr_scene_move_points(lr_scene *scene, const float *positions, uint64_t point_count);
 
 typedef struct {
     uint64_t point_count, triangle_count, node_count;
@@ -205,6 +213,21 @@ typedef struct lr_gpu_scene lr_gpu_scene;
 int lr_gpu_scene_upload(lr_context *ctx, const lr_scene *scene, lr_gpu_scene **out);
 /* GpuScene.destroy (device.lucb:108-121). */
 void lr_gpu_scene_destroy(lr_gpu_scene *scene);
+
+/* (No counterpart: the reference rebuilds its BVH2 on the host when geometry changes,
+ * bvh.lucb:66-82.) Moves an uploaded scene's points to `positions` (3 floats a point, in
+ * the compiled scene's point order; host memory, or device memory of the scene's device
+ * with LR_REFIT_DEVICE, e.g. a simulation's output) and refits it on the device: the
+ * triangle records, flat normals, and the BVH2's boxes bottom-up in one launch, then the
+ * watertight path's widened boxes and the 4- and 8-wide collapses' boxes; topology and leaf
+ * order are kept, so traversal stays exact but slows as the tree fits the moved points
+ * worse. The boxes equal lr_scene_move_points' bit for bit. Runs on `ctx`'s stream and
+ * waits. Work that reads the scene must not be in flight: ray queries queued earlier on
+ * other streams, or a batch member's passes (a batch member keeps the root box it joined
+ * with: remove it, refit, add it again; lr_renderer_refit does this for a renderer). */
+#define LR_REFIT_DEVICE 1u
+int lr_gpu_scene_refit(lr_context *ctx, lr_gpu_scene *scene, const void *positions, uint64_t point_count,
+                       uint32_t flags);
 
 /* What a scene holds on the device (no reference counterpart: the wide BVHs are this
  * build's): bytes, the BVH2's depth, the 4- and 8-wide collapses' node counts and
@@ -354,6 +377,15 @@ int lr_renderer_reload(lr_renderer *renderer, const lr_scene *scene, const lr_se
  * have finished. */
 int lr_renderer_replace_scene(lr_renderer *renderer, const lr_scene *scene, const lr_settings *settings,
                               const lr_frame *frame);
+/* (No counterpart: the reference's replace_scene uploads geometry rebuilt on the host,
+ * integrator.lucb:543-574.) The renderer's geometry with its points moved: `scene` is the
+ * renderer's compiled scene after lr_scene_move_points (the same triangles, 400
+ * otherwise). The renderer's upload is refit on the device after the passes in flight
+ * (they finish uncounted, a new generation), the lights, light tree and materials are
+ * loaded again from `scene`, and the film starts over through `frame` (NULL: the current
+ * view); the display keeps the last whole image until the first new one. Waits for the
+ * passes in flight. */
+int lr_renderer_refit(lr_renderer *renderer, const lr_scene *scene, const lr_frame *frame);
 /* Renderer.display (integrator.lucb:741-746): the render ready to show, rgba16f (4 halves a
  * pixel, row by row at the shown view's width): exposed, in linear Rec.709, through the
  * view; always one whole image of one view (no pass in flight writes it). */

@@ -36,6 +36,7 @@ LIBRARY_PATH = _HERE / "libluce_render_b200.so"
 INVALID, LIMIT, STOPPED, DEVICE, TIMEOUT = 400, 401, 402, 500, 504
 TRACE_ANY, TRACE_REFERENCE, TRACE_COUNT = 1, 2, 4
 LIGHT_RECT, LIGHT_DISK, LIGHT_SPHERE, LIGHT_DISTANT, LIGHT_DOME = 0, 1, 2, 3, 4
+REFIT_DEVICE = 1
 
 
 class RenderError(RuntimeError):
@@ -254,6 +255,9 @@ _SIGNATURES = {
     "lr_scene_camera": (C.c_int, [_vp, _i32, C.POINTER(Camera)]),
     "lr_gpu_scene_upload": (C.c_int, [_vp, _vp, C.POINTER(_vp)]),
     "lr_gpu_scene_destroy": (None, [_vp]),
+    "lr_scene_move_points": (C.c_int, [_vp, C.POINTER(C.c_float), _u64]),
+    "lr_gpu_scene_refit": (C.c_int, [_vp, _vp, _vp, _u64, _u32]),
+    "lr_renderer_refit": (C.c_int, [_vp, _vp, C.POINTER(Frame)]),
     "lr_gpu_scene_info_get": (C.c_int, [_vp, C.POINTER(GpuSceneInfo)]),
     "lr_probe": (C.c_int, [_vp, _vp, C.POINTER(Frame), _u32, C.POINTER(C.c_uint32), C.POINTER(C.c_float)]),
     "lr_probe_static": (C.c_int, [_vp, _vp, C.POINTER(Frame), _u32, C.POINTER(C.c_uint32),
@@ -567,6 +571,12 @@ class CompiledScene:
         _check(lib.lr_scene_camera(self.handle, index, C.byref(c)))
         return c
 
+    def move_points(self, positions) -> None:
+        """Moves the compiled points (point_count x 3, world space, the scene's point
+        order) with the triangles kept, and refits the BVH2 and flat normals in place."""
+        p = np.ascontiguousarray(positions, np.float32).reshape(-1)
+        _check(lib.lr_scene_move_points(self.handle, p.ctypes.data_as(C.POINTER(C.c_float)), C.c_uint64(len(p) // 3)))
+
     def close(self) -> None:
         if self.handle:
             lib.lr_scene_free(self.handle)
@@ -634,6 +644,17 @@ class GpuScene:
             self.handle = None
 
     close = destroy
+
+    def refit(self, ctx: "Context", positions, device: bool = False) -> None:
+        """Moves the uploaded points and refits the scene's BVHs on the device: `positions`
+        a host array (point_count x 3), or with `device` the address of device memory and
+        the point count as a (pointer, count) pair."""
+        if device:
+            ptr, count = positions
+            _check(lib.lr_gpu_scene_refit(ctx.handle, self.handle, C.c_void_p(ptr), C.c_uint64(count), REFIT_DEVICE))
+            return
+        p = np.ascontiguousarray(positions, np.float32).reshape(-1)
+        _check(lib.lr_gpu_scene_refit(ctx.handle, self.handle, p.ctypes.data_as(C.c_void_p), C.c_uint64(len(p) // 3), 0))
 
     @property
     def info(self) -> GpuSceneInfo:
@@ -829,6 +850,13 @@ class Renderer:
         """Renderer.replace_scene (integrator.lucb:543): new geometry."""
         _check(lib.lr_renderer_replace_scene(self.handle, scene.handle, C.byref(settings.c), C.byref(frame)))
         self.width, self.height = int(frame.width), int(frame.height)
+
+    def refit(self, scene: "CompiledScene", frame: Frame | None = None) -> None:
+        """The renderer's geometry with its points moved (`scene` after move_points): its
+        upload refit on the device, its lights loaded again, the film started over."""
+        _check(lib.lr_renderer_refit(self.handle, scene.handle, C.byref(frame) if frame is not None else None))
+        if frame is not None:
+            self.width, self.height = int(frame.width), int(frame.height)
 
     def display(self) -> int:
         """The device address of the rgba16f display image."""

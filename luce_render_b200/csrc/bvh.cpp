@@ -268,15 +268,18 @@ void build_bvh(Scene &scene) {
     // reorder (bvh.lucb:198-217)
     scene.order = b.order;
     std::vector<uint32_t> indices(count * 3), faces(count), shading(count * 4);
+    std::vector<uint8_t> flat(count);
     for (size_t at = 0; at < count; at++) {
         size_t s = scene.order[at];
         for (int k = 0; k < 3; k++) indices[at * 3 + k] = scene.indices[s * 3 + k];
         for (int k = 0; k < 4; k++) shading[at * 4 + k] = scene.shading[s * 4 + k];
         faces[at] = scene.faces[s];
+        flat[at] = scene.flat[s];
     }
     scene.indices.swap(indices);
     scene.faces.swap(faces);
     scene.shading.swap(shading);
+    scene.flat.swap(flat);
     scene.bvh_depth = bvh_depth(nodes);
 }
 

@@ -80,6 +80,9 @@ void fit_spectrum(const V3 &rgb, double out[4]);
 V3 blackbody_xyz(double kelvin);
 M3 basis_weights();     // ACEScg -> weights of a dome texel's three basis spectra
 uint32_t octahedral(const V3 &n);
+// The flat shading normal a compile gives a triangle without authored normals: its own
+// geometric normal (b - a) x (c - a), octahedrally encoded.
+uint32_t flat_normal(const float *a, const float *b, const float *c);
 
 // sampler.cpp: the 128 Sobol direction numbers (4 dimensions x 32 bits).
 const uint32_t *sobol_table();
@@ -90,6 +93,7 @@ struct Scene {
     std::vector<uint32_t> indices;       // 3 per triangle, leaf order
     std::vector<uint32_t> faces;         // polygon per triangle, leaf order
     std::vector<uint32_t> shading;       // 3 octahedral normals + material, leaf order
+    std::vector<uint8_t> flat;           // 1 where the normals are the triangle's own (no authored ones)
     std::vector<lr_bvh_node> nodes;      // binned-SAH BVH2
     std::vector<uint32_t> order;         // source triangle at each leaf slot
     std::vector<lr_camera> cameras;
@@ -106,6 +110,8 @@ struct Scene {
 // bvh.cpp: the binned-SAH build of bvh.lucb:66-217, reordering the scene's triangles
 // into leaf order.
 void build_bvh(Scene &scene);
+// Moves the scene's points (same triangles) and refits its BVH2 and flat normals (scene.cpp).
+void move_points(Scene &scene, const float *positions);
 uint32_t bvh_depth(const std::vector<lr_bvh_node> &nodes);
 
 // camera.cpp

@@ -216,6 +216,8 @@ struct HostLayout {
     int root = 0;
     float root_lo[3], root_hi[3];
     float delta = 0.0f;
+    // For refits: per interior entry its parent slot; per BVH2 node the slot holding its box.
+    std::vector<uint32_t> parents, slot_of_node;
 };
 
 int leaf_link(const lr_bvh_node &n) {
@@ -243,8 +245,15 @@ void build_layout(const lr::Scene &scene, HostLayout &L) {
     auto link = [&](uint32_t c) { return nodes[c].count == 0 ? entry[c] : leaf_link(nodes[c]); };
     L.entries.resize((size_t)interior * 4);
     L.ref_entries.resize((size_t)interior * 4);
+    L.parents.assign((size_t)interior, 0xffffffffu);
+    L.slot_of_node.assign(nodes.size(), kRefitRoot);
     for (size_t n = 0; n < nodes.size(); n++) {
         if (entry[n] < 0) continue;
+        for (uint32_t side = 0; side < 2; side++) {
+            const uint32_t c = nodes[n].first + side;
+            L.slot_of_node[c] = (uint32_t)entry[n] << 1 | side;
+            if (entry[c] >= 0) L.parents[(size_t)entry[c]] = (uint32_t)entry[n] << 1 | side;
+        }
         const lr_bvh_node &a = nodes[nodes[n].first], &b = nodes[nodes[n].first + 1];
         const float d = L.delta;
         float4 *e = &L.entries[(size_t)entry[n] * 4];
@@ -437,6 +446,13 @@ int lr_gpu_scene_upload(lr_context *ctx, const lr_scene *scene, lr_gpu_scene **o
         const WideBvh w4 = build_wide(scene->nodes, 4, L.delta, widen_down, widen_up, leaf_link);
         const WideBvh w8 = build_wide(scene->nodes, 8, L.delta, widen_down, widen_up, leaf_link);
         const size_t T = scene->triangle_count(), P = scene->point_count();
+        // The wide nodes' child slots as refit sources: the BVH2 slot (or root) of each box.
+        std::vector<uint32_t> sources4(w4.sources.size()), sources8(w8.sources.size());
+        for (auto [from, to] : {std::pair{&w4.sources, &sources4}, std::pair{&w8.sources, &sources8}})
+            for (size_t i = 0; i < from->size(); i++)
+                (*to)[i] = (*from)[i] == 0xffffffffu ? 0xffffffffu : L.slot_of_node[(*from)[i]];
+        const float root_box[8] = {L.root_lo[0], L.root_lo[1], L.root_lo[2], 0.0f,
+                                   L.root_hi[0], L.root_hi[1], L.root_hi[2], 0.0f};
         // One allocation, arrays at 256-byte offsets; empty arrays still get room.
         struct Part {
             const void *src;
@@ -454,6 +470,12 @@ int lr_gpu_scene_upload(lr_context *ctx, const lr_scene *scene, lr_gpu_scene **o
             {L.shading.data(), T * sizeof(uint4), 0},
             {w4.nodes.data(), w4.nodes.size() * sizeof(float), 0},
             {w8.nodes.data(), w8.nodes.size() * sizeof(float), 0},
+            {L.parents.data(), L.parents.size() * sizeof(uint32_t), 0},
+            {nullptr, L.parents.size() * sizeof(uint32_t), 0},  // climb counters
+            {sources4.data(), sources4.size() * sizeof(uint32_t), 0},
+            {sources8.data(), sources8.size() * sizeof(uint32_t), 0},
+            {scene->flat.data(), scene->flat.size(), 0},
+            {root_box, sizeof root_box, 0},
         };
         size_t total = 0;
         for (auto &p : parts) {
@@ -467,7 +489,8 @@ int lr_gpu_scene_upload(lr_context *ctx, const lr_scene *scene, lr_gpu_scene **o
         char *base = (char *)gs->allocation;
         LR_CUDA(cudaMemsetAsync(base, 0, total, ctx->stream));
         for (auto &p : parts)
-            if (p.bytes) LR_CUDA(cudaMemcpyAsync(base + p.offset, p.src, p.bytes, cudaMemcpyHostToDevice, ctx->stream));
+            if (p.bytes && p.src)
+                LR_CUDA(cudaMemcpyAsync(base + p.offset, p.src, p.bytes, cudaMemcpyHostToDevice, ctx->stream));
         LR_CUDA(cudaStreamSynchronize(ctx->stream));
         DeviceScene &s = gs->scene;
         s.bvh.entries = (const float4 *)(base + parts[0].offset);
@@ -482,6 +505,13 @@ int lr_gpu_scene_upload(lr_context *ctx, const lr_scene *scene, lr_gpu_scene **o
         s.wide8 = DeviceWide{(const float4 *)(base + parts[9].offset), T ? 8 : 0, w8.max_stack};
         gs->wide4_nodes = w4.node_count;
         gs->wide8_nodes = w8.node_count;
+        gs->parents = (uint32_t *)(base + parts[10].offset);
+        gs->counters = (uint32_t *)(base + parts[11].offset);
+        gs->wide4_sources = (uint32_t *)(base + parts[12].offset);
+        gs->wide8_sources = (uint32_t *)(base + parts[13].offset);
+        gs->flat = (uint8_t *)(base + parts[14].offset);
+        gs->root_box = (float *)(base + parts[15].offset);
+        gs->topology = topology_hash(*scene);
         for (DeviceBvh *b : {&s.bvh, &s.ref_bvh}) {
             b->root = L.root;
             b->empty = T == 0 ? 1 : 0;

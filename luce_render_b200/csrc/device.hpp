@@ -78,7 +78,24 @@ struct lr_gpu_scene {
     void *allocation = nullptr;  // one device block holds every array
     size_t bytes = 0;
     size_t wide4_nodes = 0, wide8_nodes = 0;
+    // What a refit (refit.cu) reads besides the traversal arrays: per interior entry its
+    // parent (entry << 1 | side; 0xffffffff the root) and a climb counter; per wide child
+    // slot the BVH2 box it holds (entry << 1 | side; kRefitRoot the root's; 0xffffffff
+    // none); per leaf slot whether its normals are its own flat one; the exact root box.
+    uint32_t *parents = nullptr, *counters = nullptr, *wide4_sources = nullptr, *wide8_sources = nullptr;
+    uint8_t *flat = nullptr;
+    float *root_box = nullptr;
+    uint64_t topology = 0;  // a hash of the triangles (leaf order) a refit must keep
 };
+
+namespace lr {
+constexpr uint32_t kRefitRoot = 0xfffffffeu;
+// refit.cu: with the uploaded scene's points already moved (its `positions` array),
+// refits its triangle records, flat normals and every BVH's boxes on `stream`; waits.
+void refit_scene(lr_gpu_scene *gs, cudaStream_t stream);
+// FNV-1a over a scene's triangle count and leaf-order indices.
+uint64_t topology_hash(const Scene &scene);
+}  // namespace lr
 
 namespace lr {
 // The traversal the watertight path uses for a scene: BVH width 2, 4 or 8 and stack

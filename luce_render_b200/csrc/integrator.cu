@@ -3420,6 +3420,31 @@ int lr_renderer_replace_scene(lr_renderer *r, const lr_scene *scene, const lr_se
     });
 }
 
+int lr_renderer_refit(lr_renderer *r, const lr_scene *scene, const lr_frame *frame) {
+    return guarded([&] {
+        if (!r || !scene) fail(LR_INVALID, "a refit needs a renderer and its scene with the points moved");
+        WaveHost *h = &r->wave;
+        MemberHost &mh = member_at(h, 0);
+        lr_gpu_scene *gs = mh.owned;
+        if (!gs || topology_hash(*scene) != gs->topology) fail(LR_INVALID, "a refit keeps the renderer's triangles");
+        LR_CUDA(cudaSetDevice(h->ctx->device));
+        const lr_frame f = frame ? *frame : r->frame;
+        lr_settings chosen = mh.settings;
+        chosen.width = f.width;
+        chosen.height = f.height;
+        // The passes in flight read the geometry: the new points and the refit follow them.
+        after_passes(h);
+        if (scene->point_count())
+            LR_CUDA(cudaMemcpyAsync(const_cast<float *>(gs->scene.positions), scene->positions.data(),
+                                    scene->positions.size() * sizeof(float), cudaMemcpyHostToDevice, h->ctx->stream));
+        refit_scene(gs, h->ctx->stream);
+        renderer_renew(r, f, scene, &chosen, gs);
+        r->frame = f;
+        r->geometry = geometry_hash(*scene);
+        r->shading = scene->shading;
+    });
+}
+
 int lr_renderer_display(lr_renderer *r, void **device_rgba16f) {
     return guarded([&] {
         if (!r || !device_rgba16f) fail(LR_INVALID, "no renderer");

@@ -1,0 +1,293 @@
+// Refitting an uploaded scene on the device after its points move (the triangles, their
+// leaf order and the BVH topology kept): a deforming mesh, or points a simulation writes
+// straight into device memory, traced again without a host rebuild or a re-upload.
+//
+// The reference rebuilds its BVH2 on the host for every geometry change (bvh.lucb:66-82,
+// called from compile_scene); this keeps the reference's tree and recomputes its boxes:
+//   1. every leaf slot's triangle record (3 float4) from the moved points, and the flat
+//      shading normal of triangles that had no authored normals;
+//   2. the BVH2's exact boxes bottom-up in one launch: a thread per interior entry writes
+//      its leaf children's boxes, then climbs -- at each entry the second child to finish
+//      (an atomic count of finished children) unions both boxes into its parent's slot, the
+//      first stops -- so every box is written once, after both of its children, with no
+//      thread waiting on another;
+//   3. the watertight path's widened boxes from the exact ones, with the widening taken
+//      again from the new root box (2^-16 of the scene's scale, one more float step);
+//   4. the 4- and 8-wide collapses' child boxes, copied from the BVH2 slots they came from.
+// With the points unchanged a refit leaves every array bit for bit as the upload made it,
+// and the boxes equal the host refit (lr_scene_move_points) of the same move exactly: boxes
+// are minima and maxima of the same floats, and the widening is the same float arithmetic.
+#include <algorithm>
+#include <cmath>
+#include <cstring>
+
+#include "device.hpp"
+
+namespace lr {
+namespace {
+
+struct Box {
+    float lo[3], hi[3];
+};
+
+// Entry e's child `side` box in the traversal layout: side 0 in float4 0 (x, y) and the
+// first half of float4 2 (z); side 1 in float4 1 and the second half of float4 2. Reads and
+// writes go through L2 (other threads' boxes are read after an atomic, never from L1).
+__device__ __forceinline__ Box read_side(const float4 *entries, uint32_t e, uint32_t side) {
+    const float4 xy = __ldcg(&entries[(size_t)e * 4 + side]);
+    const float2 z = __ldcg(reinterpret_cast<const float2 *>(&entries[(size_t)e * 4 + 2]) + side);
+    return Box{{xy.x, xy.z, z.x}, {xy.y, xy.w, z.y}};
+}
+
+__device__ __forceinline__ void write_side(float4 *entries, uint32_t e, uint32_t side, const Box &b) {
+    __stcg(&entries[(size_t)e * 4 + side], make_float4(b.lo[0], b.hi[0], b.lo[1], b.hi[1]));
+    __stcg(reinterpret_cast<float2 *>(&entries[(size_t)e * 4 + 2]) + side, make_float2(b.lo[2], b.hi[2]));
+}
+
+__device__ __forceinline__ Box leaf_box(const float4 *tris, int link) {
+    const uint32_t code = (uint32_t)(-1 - link);
+    const uint32_t first = code >> kLeafShift, count = (code & ((1u << kLeafShift) - 1u)) + 1u;
+    Box b{{INFINITY, INFINITY, INFINITY}, {-INFINITY, -INFINITY, -INFINITY}};
+    for (uint32_t t = first; t < first + count; t++)
+        for (uint32_t c = 0; c < 3; c++) {
+            const float4 v = tris[(size_t)t * 3 + c];
+            b.lo[0] = fminf(b.lo[0], v.x);
+            b.lo[1] = fminf(b.lo[1], v.y);
+            b.lo[2] = fminf(b.lo[2], v.z);
+            b.hi[0] = fmaxf(b.hi[0], v.x);
+            b.hi[1] = fmaxf(b.hi[1], v.y);
+            b.hi[2] = fmaxf(b.hi[2], v.z);
+        }
+    return b;
+}
+
+__device__ __forceinline__ Box join(const Box &a, const Box &b) {
+    return Box{{fminf(a.lo[0], b.lo[0]), fminf(a.lo[1], b.lo[1]), fminf(a.lo[2], b.lo[2])},
+               {fmaxf(a.hi[0], b.hi[0]), fmaxf(a.hi[1], b.hi[1]), fmaxf(a.hi[2], b.hi[2])}};
+}
+
+// The host's widen_down / widen_up (device.cu): `delta` outward, then one more float step.
+__device__ __forceinline__ float widen_lo(float v, float delta) { return nextafterf(v - delta, -INFINITY); }
+__device__ __forceinline__ float widen_hi(float v, float delta) { return nextafterf(v + delta, INFINITY); }
+
+__global__ void tris_kernel(uint64_t count, const float *positions, const uint32_t *indices, float4 *tris) {
+    for (uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; i < count * 3; i += (uint64_t)gridDim.x * blockDim.x) {
+        const uint32_t point = indices[i];
+        const float w = tris[i].w;  // the first corner's w holds the source triangle id
+        tris[i] = make_float4(positions[(size_t)point * 3], positions[(size_t)point * 3 + 1],
+                              positions[(size_t)point * 3 + 2], w);
+    }
+}
+
+// octahedral (scene.cpp, scene.lucb:400-412) of (b - a) x (c - a), in f64 with every
+// operation rounded as the host's (no fused multiply-adds), so the codes are the host's.
+__device__ uint32_t flat_code(const float *pa, const float *pb, const float *pc) {
+    const double e1[3] = {__dsub_rn(pb[0], pa[0]), __dsub_rn(pb[1], pa[1]), __dsub_rn(pb[2], pa[2])};
+    const double e2[3] = {__dsub_rn(pc[0], pa[0]), __dsub_rn(pc[1], pa[1]), __dsub_rn(pc[2], pa[2])};
+    const double n[3] = {__dsub_rn(__dmul_rn(e1[1], e2[2]), __dmul_rn(e1[2], e2[1])),
+                         __dsub_rn(__dmul_rn(e1[2], e2[0]), __dmul_rn(e1[0], e2[2])),
+                         __dsub_rn(__dmul_rn(e1[0], e2[1]), __dmul_rn(e1[1], e2[0]))};
+    const double length = __dadd_rn(__dadd_rn(fabs(n[0]), fabs(n[1])), fabs(n[2]));
+    double x = 0.0, y = 1.0;  // a degenerate triangle's normal: +Y (octahedral of (0, 1, 0))
+    if (length > 0.0) {
+        x = __ddiv_rn(n[0], length);
+        y = __ddiv_rn(n[1], length);
+        if (n[2] < 0.0) {
+            const double fx = __dmul_rn(__dsub_rn(1.0, fabs(y)), x >= 0.0 ? 1.0 : -1.0);
+            const double fy = __dmul_rn(__dsub_rn(1.0, fabs(x)), y >= 0.0 ? 1.0 : -1.0);
+            x = fx;
+            y = fy;
+        }
+    }
+    const long long qx = (long long)round(__dmul_rn(fmin(fmax(x, -1.0), 1.0), 32767.0));
+    const long long qy = (long long)round(__dmul_rn(fmin(fmax(y, -1.0), 1.0), 32767.0));
+    return (uint32_t)(qx & 0xffff) | ((uint32_t)(qy & 0xffff) << 16);
+}
+
+__global__ void flat_kernel(uint64_t count, const float *positions, const uint32_t *indices, const uint8_t *flat,
+                            uint4 *shading) {
+    for (uint64_t t = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; t < count; t += (uint64_t)gridDim.x * blockDim.x) {
+        if (!flat[t]) continue;
+        const uint32_t code = flat_code(&positions[(size_t)indices[t * 3] * 3], &positions[(size_t)indices[t * 3 + 1] * 3],
+                                        &positions[(size_t)indices[t * 3 + 2] * 3]);
+        const uint4 s = shading[t];
+        shading[t] = make_uint4(code, code, code, s.w);
+    }
+}
+
+// Step 2. `levels` bounds a climb (the BVH2's depth + 1), so a damaged parent table can
+// only end a climb early, never loop.
+__global__ void climb_kernel(uint32_t entries, const float4 *tris, float4 *exact, const uint32_t *parents,
+                             uint32_t *counters, float *root_box, uint32_t levels) {
+    const uint32_t e = blockIdx.x * blockDim.x + threadIdx.x;
+    if (e >= entries) return;
+    const float4 links = exact[(size_t)e * 4 + 3];
+    const int link[2] = {__float_as_int(links.x), __float_as_int(links.y)};
+    uint32_t leaves = 0;
+    for (uint32_t side = 0; side < 2; side++)
+        if (link[side] < 0) {
+            write_side(exact, e, side, leaf_box(tris, link[side]));
+            leaves++;
+        }
+    if (leaves == 0) return;
+    __threadfence();
+    if (atomicAdd(&counters[e], leaves) + leaves != 2u) return;
+    uint32_t at = e;
+    for (uint32_t level = 0; level < levels; level++) {
+        __threadfence();
+        const Box box = join(read_side(exact, at, 0), read_side(exact, at, 1));
+        const uint32_t up = parents[at];
+        if (up == 0xffffffffu) {
+            for (int k = 0; k < 3; k++) {
+                __stcg(&root_box[k], box.lo[k]);
+                __stcg(&root_box[4 + k], box.hi[k]);
+            }
+            return;
+        }
+        write_side(exact, up >> 1, up & 1u, box);
+        __threadfence();
+        if (atomicAdd(&counters[up >> 1], 1u) == 0u) return;  // the sibling is still on its way
+        at = up >> 1;
+    }
+}
+
+// A scene whose root is a leaf (at most 16 triangles): its box.
+__global__ void leaf_root_kernel(const float4 *tris, int root, float *root_box) {
+    if (threadIdx.x != 0 || blockIdx.x != 0) return;
+    const Box b = leaf_box(tris, root);
+    for (int k = 0; k < 3; k++) {
+        root_box[k] = b.lo[k];
+        root_box[4 + k] = b.hi[k];
+    }
+}
+
+// Step 3: the float4s 0..2 of every entry hold (lo, hi, lo, hi) pairs.
+__global__ void widen_kernel(uint64_t count, const float4 *exact, float4 *widened, float delta) {
+    for (uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; i < count; i += (uint64_t)gridDim.x * blockDim.x) {
+        const uint64_t e = i / 3, k = i % 3;
+        const float4 v = exact[e * 4 + k];
+        widened[e * 4 + k] = make_float4(widen_lo(v.x, delta), widen_hi(v.y, delta), widen_lo(v.z, delta),
+                                         widen_hi(v.w, delta));
+    }
+}
+
+// Step 4: wide node n's child slot i from the BVH2 slot (or the root) it was collapsed from;
+// empty slots keep their inverted boxes.
+__global__ void wide_kernel(uint64_t slots, int width, const uint32_t *sources, const float4 *exact,
+                            const float *root_box, float delta, float4 *nodes) {
+    const int per_node = width == 4 ? 7 : 14, planes = width / 4;
+    for (uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; i < slots; i += (uint64_t)gridDim.x * blockDim.x) {
+        const uint32_t source = sources[i];
+        if (source == 0xffffffffu) continue;
+        Box b;
+        if (source == kRefitRoot) {
+            for (int k = 0; k < 3; k++) {
+                b.lo[k] = root_box[k];
+                b.hi[k] = root_box[4 + k];
+            }
+        } else {
+            b = read_side(exact, source >> 1, source & 1u);
+        }
+        const uint64_t n = i / width;
+        const int slot = (int)(i % width);
+        float *base = reinterpret_cast<float *>(nodes + n * per_node);
+        for (int k = 0; k < 3; k++) {
+            base[((2 * k) * planes) * 4 + slot] = widen_lo(b.lo[k], delta);
+            base[((2 * k + 1) * planes) * 4 + slot] = widen_hi(b.hi[k], delta);
+        }
+    }
+}
+
+unsigned grid_for(uint64_t items, int sm_count) {
+    const uint64_t blocks = (items + 255) / 256;
+    return (unsigned)std::max<uint64_t>(1, std::min<uint64_t>(blocks, (uint64_t)sm_count * 8));
+}
+
+float host_widen_down(float v, float delta) { return std::nextafter(v - delta, -INFINITY); }
+float host_widen_up(float v, float delta) { return std::nextafter(v + delta, INFINITY); }
+
+}  // namespace
+
+uint64_t topology_hash(const Scene &scene) {
+    uint64_t key = 14695981039346656037ull;
+    auto mix = [&](const void *data, size_t bytes) {
+        const unsigned char *p = (const unsigned char *)data;
+        for (size_t i = 0; i < bytes; i++) key = (key ^ p[i]) * 1099511628211ull;
+    };
+    const uint64_t counts[2] = {scene.point_count(), scene.triangle_count()};
+    mix(counts, sizeof counts);
+    mix(scene.indices.data(), scene.indices.size() * sizeof(uint32_t));
+    return key;
+}
+
+void refit_scene(lr_gpu_scene *gs, cudaStream_t stream) {
+    DeviceScene &s = gs->scene;
+    const uint64_t T = s.triangle_count;
+    if (T == 0) return;
+    const int sms = gs->ctx->sm_count;
+    float4 *tris = const_cast<float4 *>(s.tris);
+    float4 *exact = const_cast<float4 *>(s.ref_bvh.entries);
+    float4 *widened = const_cast<float4 *>(s.bvh.entries);
+    tris_kernel<<<grid_for(T * 3, sms), 256, 0, stream>>>(T, s.positions, s.indices, tris);
+    flat_kernel<<<grid_for(T, sms), 256, 0, stream>>>(T, s.positions, s.indices, gs->flat, const_cast<uint4 *>(s.shading));
+    const uint64_t E = s.entry_count;
+    if (E > 0) {
+        LR_CUDA(cudaMemsetAsync(gs->counters, 0, E * sizeof(uint32_t), stream));
+        climb_kernel<<<(unsigned)((E + 127) / 128), 128, 0, stream>>>((uint32_t)E, tris, exact, gs->parents, gs->counters,
+                                                                       gs->root_box, s.depth + 2);
+    } else {
+        leaf_root_kernel<<<1, 32, 0, stream>>>(tris, s.bvh.root, gs->root_box);
+    }
+    LR_CUDA(cudaGetLastError());
+    float root[8];
+    LR_CUDA(cudaMemcpyAsync(root, gs->root_box, sizeof root, cudaMemcpyDeviceToHost, stream));
+    LR_CUDA(cudaStreamSynchronize(stream));
+    // The widening as the upload takes it (device.cu's build_layout), from the new root box.
+    double scale = 1.0;
+    for (int k = 0; k < 3; k++) {
+        scale = std::max(scale, (double)std::fabs(root[k]));
+        scale = std::max(scale, (double)std::fabs(root[4 + k]));
+        scale = std::max(scale, (double)(root[4 + k] - root[k]));
+    }
+    const float delta = (float)std::ldexp(scale, -16);
+    for (int k = 0; k < 3; k++) {
+        s.ref_bvh.root_lo[k] = root[k];
+        s.ref_bvh.root_hi[k] = root[4 + k];
+        s.bvh.root_lo[k] = host_widen_down(root[k], delta);
+        s.bvh.root_hi[k] = host_widen_up(root[4 + k], delta);
+    }
+    if (E > 0) widen_kernel<<<grid_for(E * 3, sms), 256, 0, stream>>>(E * 3, exact, widened, delta);
+    if (s.wide4.width)
+        wide_kernel<<<grid_for(gs->wide4_nodes * 4, sms), 256, 0, stream>>>(
+            gs->wide4_nodes * 4, 4, gs->wide4_sources, exact, gs->root_box, delta, const_cast<float4 *>(s.wide4.nodes));
+    if (s.wide8.width)
+        wide_kernel<<<grid_for(gs->wide8_nodes * 8, sms), 256, 0, stream>>>(
+            gs->wide8_nodes * 8, 8, gs->wide8_sources, exact, gs->root_box, delta, const_cast<float4 *>(s.wide8.nodes));
+    LR_CUDA(cudaGetLastError());
+    LR_CUDA(cudaStreamSynchronize(stream));
+}
+
+}  // namespace lr
+
+using namespace lr;
+
+extern "C" {
+
+int lr_gpu_scene_refit(lr_context *ctx, lr_gpu_scene *gs, const void *positions, uint64_t point_count, uint32_t flags) {
+    return guarded([&] {
+        if (!ctx || !gs || (point_count && !positions)) fail(LR_INVALID, "a refit needs a context, a scene and its points");
+        if (ctx->device != gs->ctx->device) fail(LR_INVALID, "a refit runs on the scene's device");
+        if (flags & ~LR_REFIT_DEVICE) fail(LR_INVALID, "unknown refit flags");
+        if (point_count != gs->scene.point_count) fail(LR_INVALID, "a refit keeps the scene's point count");
+        LR_CUDA(cudaSetDevice(ctx->device));
+        float *dst = const_cast<float *>(gs->scene.positions);
+        const size_t bytes = point_count * 3 * sizeof(float);
+        if (bytes && dst != positions)
+            LR_CUDA(cudaMemcpyAsync(dst, positions, bytes,
+                                    (flags & LR_REFIT_DEVICE) ? cudaMemcpyDeviceToDevice : cudaMemcpyHostToDevice,
+                                    ctx->stream));
+        refit_scene(gs, ctx->stream);
+    });
+}
+
+}  // extern "C"

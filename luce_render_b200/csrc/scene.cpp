@@ -87,12 +87,11 @@ void add_mesh(Scene &scene, const lr_mesh &mesh, uint32_t &face_base, size_t lib
         } else {
             // No authored normals: the triangle's own (flat) normal, in world space.
             const float *p = scene.positions.data();
-            V3 a(p[(base + corner[0]) * 3], p[(base + corner[0]) * 3 + 1], p[(base + corner[0]) * 3 + 2]);
-            V3 b(p[(base + corner[1]) * 3], p[(base + corner[1]) * 3 + 1], p[(base + corner[1]) * 3 + 2]);
-            V3 c(p[(base + corner[2]) * 3], p[(base + corner[2]) * 3 + 1], p[(base + corner[2]) * 3 + 2]);
-            uint32_t flat = octahedral((b - a).cross(c - a));
+            const uint32_t flat =
+                flat_normal(&p[(base + corner[0]) * 3], &p[(base + corner[1]) * 3], &p[(base + corner[2]) * 3]);
             encoded[0] = encoded[1] = encoded[2] = flat;
         }
+        scene.flat.push_back(mesh.normals ? 0 : 1);
         scene.shading.push_back(encoded[0]);
         scene.shading.push_back(encoded[1]);
         scene.shading.push_back(encoded[2]);
@@ -103,6 +102,52 @@ void add_mesh(Scene &scene, const lr_mesh &mesh, uint32_t &face_base, size_t lib
 }
 
 }  // namespace
+
+uint32_t flat_normal(const float *a, const float *b, const float *c) {
+    const V3 pa(a[0], a[1], a[2]), pb(b[0], b[1], b[2]), pc(c[0], c[1], c[2]);
+    return octahedral((pb - pa).cross(pc - pa));
+}
+
+// Moves the points and refits the BVH2 in place: every node's box again from its
+// triangles (a leaf) or its children (an interior node; children follow their parent in
+// the numbering, so one pass from the last node back reaches every child first), the
+// topology and leaf order kept.
+void move_points(Scene &scene, const float *positions) {
+    std::copy(positions, positions + scene.positions.size(), scene.positions.begin());
+    const float *p = scene.positions.data();
+    const size_t T = scene.triangle_count();
+    for (size_t t = 0; t < T; t++) {
+        if (!scene.flat[t]) continue;
+        const uint32_t n = flat_normal(&p[(size_t)scene.indices[t * 3] * 3], &p[(size_t)scene.indices[t * 3 + 1] * 3],
+                                       &p[(size_t)scene.indices[t * 3 + 2] * 3]);
+        scene.shading[t * 4] = scene.shading[t * 4 + 1] = scene.shading[t * 4 + 2] = n;
+    }
+    if (T == 0) return;
+    for (size_t n = scene.nodes.size(); n-- > 0;) {
+        lr_bvh_node &node = scene.nodes[n];
+        float lo[3] = {INFINITY, INFINITY, INFINITY}, hi[3] = {-INFINITY, -INFINITY, -INFINITY};
+        if (node.count > 0) {
+            for (uint32_t t = node.first; t < node.first + node.count; t++)
+                for (int c = 0; c < 3; c++) {
+                    const float *v = &p[(size_t)scene.indices[(size_t)t * 3 + c] * 3];
+                    for (int k = 0; k < 3; k++) {
+                        lo[k] = std::min(lo[k], v[k]);
+                        hi[k] = std::max(hi[k], v[k]);
+                    }
+                }
+        } else {
+            for (uint32_t c = node.first; c < node.first + 2; c++)
+                for (int k = 0; k < 3; k++) {
+                    lo[k] = std::min(lo[k], scene.nodes[c].lo[k]);
+                    hi[k] = std::max(hi[k], scene.nodes[c].hi[k]);
+                }
+        }
+        for (int k = 0; k < 3; k++) {
+            node.lo[k] = lo[k];
+            node.hi[k] = hi[k];
+        }
+    }
+}
 
 // ray_frame (camera.lucb:57-76)
 void camera_frame(const lr_camera &camera, uint32_t width, uint32_t height, lr_frame &out) {
@@ -235,6 +280,16 @@ int lr_scene_compile(const lr_mesh *meshes, size_t mesh_count, const lr_camera *
 }
 
 void lr_scene_free(lr_scene *scene) { delete scene; }
+
+int lr_scene_move_points(lr_scene *scene, const float *positions, uint64_t point_count) {
+    return guarded([&] {
+        if (!scene || (point_count && !positions)) fail(LR_INVALID, "moving points needs a scene and its points");
+        if (point_count != scene->point_count()) fail(LR_INVALID, "a move keeps the scene's point count");
+        for (uint64_t i = 0; i < point_count * 3; i++)
+            if (!std::isfinite(positions[i])) fail(LR_INVALID, "a moved point is not finite");
+        move_points(*scene, positions);
+    });
+}
 
 int lr_scene_info_get(const lr_scene *scene, lr_scene_info *out) {
     return guarded([&] {

@@ -88,6 +88,7 @@ WideBvh build_wide(const std::vector<lr_bvh_node> &nodes, int width, float delta
     const size_t count = children_of.size();
     w.node_count = count;
     w.nodes.assign(count * per_node * 4, 0.0f);
+    w.sources.assign(count * width, 0xffffffffu);
     std::vector<uint32_t> index_of_bvh2(nodes.size(), 0xffffffffu);
     for (const Job &j : queue) index_of_bvh2[j.bvh2] = j.wide;
     // The wide root stands for BVH2 node 0 even when it is a leaf.
@@ -100,6 +101,7 @@ WideBvh build_wide(const std::vector<lr_bvh_node> &nodes, int width, float delta
             float lo[3] = {INFINITY, INFINITY, INFINITY}, hi[3] = {-INFINITY, -INFINITY, -INFINITY};
             int link = 0;
             if (slot < (int)list.size()) {
+                w.sources[n * width + slot] = list[slot];
                 const lr_bvh_node &c = nodes[list[slot]];
                 for (int k = 0; k < 3; k++) {
                     lo[k] = widen_down(c.lo[k], delta);

@@ -13,6 +13,9 @@ struct WideBvh {
     size_t node_count = 0;
     std::vector<float> nodes;  // node_count * floats_per_node float4s
     uint32_t max_stack = 0;    // the most stack entries a traversal can hold
+    // Per node and child slot, the BVH2 node whose box the slot holds (0xffffffff: an
+    // empty slot), so a refit can copy the boxes again.
+    std::vector<uint32_t> sources;
 };
 
 // Collapses the BVH2 `nodes` into a `width`-wide BVH (4 or 8). Child boxes are widened by
