@@ -45,6 +45,8 @@ def parse():
     p.add_argument("--skip-batched", action="store_true", help="leave out the 64-scene batched comparison")
     p.add_argument("--skip-served", action="store_true", help="leave out the served arrival stream")
     p.add_argument("--skip-cornell", action="store_true", help="leave out the glossy Cornell benchmark lines")
+    p.add_argument("--skip-refit", action="store_true", help="leave out the moved-geometry refit line")
+    p.add_argument("--refit-only", action="store_true", help="only the moved-geometry refit line (for profiling)")
     p.add_argument("--cornell-only", action="store_true",
                    help="only the glossy Cornell benchmark lines (--steps samples each), one JSON line")
     p.add_argument("--served-seconds", type=float, default=10.0,
@@ -465,6 +467,65 @@ def cornell(lr, scenes, ctx, dist, samples: int = 16, warmup: int = 3) -> dict:
             "reference_m4_max_ms": {"1024 spectral": 8.1, "1024 rgb": 7.1, "512 path tracing only": 3.14}}
 
 
+def refit(lr, scenes, ctx, dist, repeats: int = 10) -> dict:
+    """Moved geometry on the 1,048,576-triangle scene: the device refit with the points
+    already in device memory (a simulation's output), against the reference's route for
+    moved geometry -- a host compile of the moved mesh (its binned-SAH rebuild) and an
+    upload. Two poses alternate, so every refit moves every point."""
+    import numpy as np
+
+    meshes, mats, lights, cam = scenes.incoherent_scene()
+    sc = lr.compile_scene(meshes, [cam], lights, mats)
+    gs = lr.GpuScene.upload(ctx, sc)
+    a = sc.arrays()
+    base = a["positions"].astype(np.float64)
+    poses = [(base + amount * np.sin(0.7 * base[:, [1, 2, 0]])).astype(np.float32) for amount in (0.05, 0.1)]
+    buffers = []
+    for pose in poses:
+        buffers.append(ctx.alloc(pose.nbytes))
+        ctx.upload(buffers[-1], pose)
+    points, triangles = len(base), len(a["indices"])
+    for k in range(3):
+        gs.refit(ctx, (buffers[k % 2], points), device=True)
+    times = []
+    for k in range(repeats):
+        ctx.synchronize()
+        ctx.timer_start()
+        gs.refit(ctx, (buffers[k % 2], points), device=True)
+        times.append(ctx.timer_stop())
+    refit_ms = dist.max(statistics.median(times))
+    info = gs.info
+    entries = (int(sc.info.node_count) - 1) // 2
+    # Bytes a refit must move at least once: the points and indices read, the triangle
+    # records written, both copies of the BVH2's boxes and the wide nodes' boxes written.
+    algorithmic = (12 * points + 12 * triangles + 48 * triangles + 96 * entries + 96 * int(info.wide4_nodes) +
+                   192 * int(info.wide8_nodes))
+    for b in buffers:
+        ctx.free(b)
+    gs.destroy()
+    # The reference's route: compile the moved mesh again (BVH2 rebuilt on the host) and upload it.
+    moved = lr.MeshData(poses[1], a["indices"][np.argsort(a["order"])])
+    start = time.perf_counter()
+    rebuilt = lr.compile_scene([moved], [cam], lights, mats)
+    compile_s = time.perf_counter() - start
+    start = time.perf_counter()
+    gs2 = lr.GpuScene.upload(ctx, rebuilt)
+    upload_s = time.perf_counter() - start
+    gs2.destroy()
+    rebuilt.close()
+    sc.close()
+    hbm = measured_peaks().get("hbm_gbs") or 6650.0
+    achieved = algorithmic / (refit_ms / 1e3) / 1e9
+    return {"workload": "every point of the 1,048,576-triangle scene moved (two poses alternating), points in "
+                        "device memory; BVH2, 4- and 8-wide boxes, triangle records refit",
+            "triangles": triangles, "points": points, "device_refit_ms": refit_ms,
+            "algorithmic_bytes": algorithmic, "achieved_gbs": achieved, "hbm_frac": achieved / hbm,
+            "host_compile_ms": compile_s * 1e3, "host_upload_ms": upload_s * 1e3,
+            "speedup_vs_host_rebuild": (compile_s + upload_s) * 1e3 / refit_ms,
+            "timing": "device refit: CUDA events on the context's stream around the call (it waits for the new "
+                      "root box between launches), median of 10; host rebuild: wall clock"}
+
+
 def cpu_intersection(sc, scenes, oracle, cores: int) -> dict:
     """The reference's CPU intersection on the 1M-triangle scene, on all host cores: its
     f64 brute force (tests/gpu/main.lucb:82-119, every ray against every triangle) on a
@@ -500,10 +561,10 @@ def main():
 
     ctx = lr.Context(dist.local)
     W, K = max(3, args.warmup), args.steps
-    if args.cornell_only:
-        info = cornell(lr, scenes, ctx, dist, samples=K, warmup=W)
+    if args.cornell_only or args.refit_only:
+        info = cornell(lr, scenes, ctx, dist, samples=K, warmup=W) if args.cornell_only else refit(lr, scenes, ctx, dist)
         if dist.rank == 0:
-            print(json.dumps({"cornell": info, "n_gpus": dist.world}))
+            print(json.dumps({"cornell" if args.cornell_only else "refit": info, "n_gpus": dist.world}))
         ctx.close()
         dist.close()
         return
@@ -642,6 +703,7 @@ def main():
     cornell_info = None if args.skip_cornell else cornell(lr, scenes, ctx, dist)
     batch_info = None if args.skip_batched else batched(lr, scenes, ctx, dist)
     served_info = None if args.skip_served else served(lr, scenes, dist, args.served_seconds)
+    refit_info = None if args.skip_refit else refit(lr, scenes, ctx, dist)
 
     cpu = None
     if dist.rank == 0 and dist.world == 1:
@@ -679,6 +741,7 @@ def main():
             "cornell": cornell_info,
             "batched": batch_info,
             "served": served_info,
+            "refit": refit_info,
         }
         print(json.dumps(line))
     ctx.close()

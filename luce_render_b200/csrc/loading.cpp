@@ -245,7 +245,6 @@ LightRecords pack_lights(const std::vector<lr_light> &lights, const std::vector<
     // row 0 x the weights' sum, rows 1-3 w the texels' first float4, the width and the
     // height, row 6 w the cumulative weights' first float (the integers as their bits).
     if (textured_record >= 0) {
-        float *record = &out.rows[(size_t)textured_record * 28];
         auto bits = [](size_t v) {
             const uint32_t u = (uint32_t)v;
             float f;
@@ -258,6 +257,7 @@ LightRecords pack_lights(const std::vector<lr_light> &lights, const std::vector<
         out.rows.insert(out.rows.end(), environment.cdf.begin(), environment.cdf.end());
         while (out.rows.size() % 4 != 0) out.rows.push_back(0.0f);
         if (out.rows.size() >= ((size_t)1 << 32)) fail(LR_LIMIT, "a dome's image does not fit the light records");
+        float *record = &out.rows[(size_t)textured_record * 28];  // after the inserts, which may move the rows
         record[0] = (float)environment.total;
         record[1] = record[2] = 0.0f;
         record[7] = bits(texel_base);

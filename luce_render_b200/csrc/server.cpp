@@ -36,6 +36,7 @@ struct SceneSlot {
     uint64_t last_use = 0;       // a tick of the server's clock of uses (LRU)
     int users = 0;               // live sessions and running probes
     bool loading = false;
+    uint64_t image_bytes = 0;    // what each session's light records add for a dome's image
 };
 
 struct Request {
@@ -91,7 +92,18 @@ void check(int status) {
     if (status != LR_OK) fail(status, lr_last_error());
 }
 
-uint64_t session_bytes(const Request &r) { return r.pixels * 32 + (1u << 20); }
+// A session's film and image, its records, and a dome's image in its light records
+// (per texel a float4 and a cumulative weight).
+uint64_t session_bytes(const Request &r, uint64_t image_bytes) { return r.pixels * 32 + (1u << 20) + image_bytes; }
+
+uint64_t dome_image_bytes(const lr_scene *scene) {
+    for (size_t i = 0; i < scene->lights.size(); i++)
+        if (scene->lights[i].shape == LR_LIGHT_DOME && !scene->light_images[i].empty()) {
+            const uint64_t pixels = scene->light_images[i].size() / 3;
+            return pixels * 20 + (uint64_t)scene->lights[i].image_height * 4 + 64;
+        }
+    return 0;
+}
 
 // The budget left for scenes and sessions once the pool is paid for.
 uint64_t available(const lr_server *s) {
@@ -318,6 +330,7 @@ uint64_t submit(lr_server *s, Request &&r, bool probe) {
     std::lock_guard<std::mutex> lk(s->mu);
     if (s->stopping) fail(LR_STOPPED, "the server is stopping");
     if (r.scene >= s->scenes.size()) fail(LR_INVALID, "no such scene");
+    if (!probe) r.bytes = session_bytes(r, s->scenes[r.scene].image_bytes);
     r.submitted = seconds_since(s->t0);
     const uint64_t id = s->requests.size();
     s->requests.push_back(std::move(r));
@@ -393,6 +406,7 @@ int lr_server_add_scene(lr_server *s, const lr_scene *scene, uint32_t *scene_id)
         std::lock_guard<std::mutex> lk(s->mu);
         SceneSlot slot;
         slot.scene = scene;
+        slot.image_bytes = dome_image_bytes(scene);
         s->scenes.push_back(slot);
         *scene_id = (uint32_t)(s->scenes.size() - 1);
     });
@@ -426,7 +440,6 @@ int lr_server_submit_render(lr_server *s, uint32_t scene_id, const lr_settings *
         r.pixels = w * h;
         r.samples = settings->samples;
         r.rgba = rgba;
-        r.bytes = session_bytes(r);
         *request = submit(s, std::move(r), false);
     });
 }

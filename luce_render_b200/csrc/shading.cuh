@@ -348,8 +348,10 @@ __device__ __forceinline__ float4 spec_of_texel(float3 texel, float4 lambda) {
 }
 
 // dome_radiance (lights.glsl:112-118): the dome's radiance toward -d (d toward the dome).
+// The dome functions are out of line: only scenes with a dome call them, and inlined
+// into every light loop they would crowd the shading kernels' instruction cache.
 template <bool kSpectral>
-__device__ __forceinline__ float4 dome_radiance(const float4 *lights, uint32_t light, float3 d, float4 lambda) {
+__device__ __noinline__ float4 dome_radiance(const float4 *lights, uint32_t light, float3 d, float4 lambda) {
     const float4 radiance = light_radiance<kSpectral>(lights, light, lambda);
     DomeImage image;
     if (!dome_image(lights, light, image)) return radiance;
@@ -361,7 +363,7 @@ __device__ __forceinline__ float4 dome_radiance(const float4 *lights, uint32_t l
 // dome_pdf (lights.glsl:120-129): the solid-angle pdf of sampling direction d (the
 // selection's chance not included): a texel's weight over the sum, spread over its solid
 // angle.
-__device__ __forceinline__ float dome_pdf(const float4 *lights, uint32_t light, float3 d) {
+__device__ __noinline__ float dome_pdf(const float4 *lights, uint32_t light, float3 d) {
     DomeImage image;
     if (!dome_image(lights, light, image)) return 1.0f / (4.0f * kPi);
     float sin_theta;
@@ -423,7 +425,7 @@ __device__ __forceinline__ float sphere_hit(float3 center, float radius, float3 
 
 // sample_dome (lights.glsl:152-174): a direction by the image's weights (rows, then the
 // chosen row's texels), or uniform over the sphere for a dome without an image.
-__device__ __forceinline__ bool sample_dome(const float4 *lights, uint32_t light, float2 u, LightSample &s) {
+__device__ __noinline__ bool sample_dome(const float4 *lights, uint32_t light, float2 u, LightSample &s) {
     s.distance = kInfinity;
     s.delta = false;
     s.cos_light = 1.0f;
