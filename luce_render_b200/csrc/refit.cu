@@ -44,19 +44,22 @@ __device__ __forceinline__ void write_side(float4 *entries, uint32_t e, uint32_t
     __stcg(reinterpret_cast<float2 *>(&entries[(size_t)e * 4 + 2]) + side, make_float2(b.lo[2], b.hi[2]));
 }
 
-__device__ __forceinline__ Box leaf_box(const float4 *tris, int link) {
+// A leaf's box from its triangles' corners: 12 bytes of indices a triangle and the points
+// (which stay in L2), not the 48-byte triangle records.
+__device__ __forceinline__ Box leaf_box(const float *positions, const uint32_t *indices, int link) {
     const uint32_t code = (uint32_t)(-1 - link);
     const uint32_t first = code >> kLeafShift, count = (code & ((1u << kLeafShift) - 1u)) + 1u;
     Box b{{INFINITY, INFINITY, INFINITY}, {-INFINITY, -INFINITY, -INFINITY}};
     for (uint32_t t = first; t < first + count; t++)
         for (uint32_t c = 0; c < 3; c++) {
-            const float4 v = tris[(size_t)t * 3 + c];
-            b.lo[0] = fminf(b.lo[0], v.x);
-            b.lo[1] = fminf(b.lo[1], v.y);
-            b.lo[2] = fminf(b.lo[2], v.z);
-            b.hi[0] = fmaxf(b.hi[0], v.x);
-            b.hi[1] = fmaxf(b.hi[1], v.y);
-            b.hi[2] = fmaxf(b.hi[2], v.z);
+            const float *v = &positions[(size_t)__ldg(&indices[(size_t)t * 3 + c]) * 3];
+            const float x = __ldg(v), y = __ldg(v + 1), z = __ldg(v + 2);
+            b.lo[0] = fminf(b.lo[0], x);
+            b.lo[1] = fminf(b.lo[1], y);
+            b.lo[2] = fminf(b.lo[2], z);
+            b.hi[0] = fmaxf(b.hi[0], x);
+            b.hi[1] = fmaxf(b.hi[1], y);
+            b.hi[2] = fmaxf(b.hi[2], z);
         }
     return b;
 }
@@ -70,10 +73,14 @@ __device__ __forceinline__ Box join(const Box &a, const Box &b) {
 __device__ __forceinline__ float widen_lo(float v, float delta) { return nextafterf(v - delta, -INFINITY); }
 __device__ __forceinline__ float widen_hi(float v, float delta) { return nextafterf(v + delta, INFINITY); }
 
-__global__ void tris_kernel(uint64_t count, const float *positions, const uint32_t *indices, float4 *tris) {
+// The first corner's w holds the source triangle id (the upload's layout), taken from the
+// 4-byte ids rather than by reading the old record back.
+__global__ void tris_kernel(uint64_t count, const float *positions, const uint32_t *indices, const uint32_t *ids,
+                            float4 *tris) {
     for (uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; i < count * 3; i += (uint64_t)gridDim.x * blockDim.x) {
         const uint32_t point = indices[i];
-        const float w = tris[i].w;  // the first corner's w holds the source triangle id
+        const uint64_t t = i / 3;
+        const float w = i - t * 3 == 0 ? __uint_as_float(ids[t]) : 0.0f;
         tris[i] = make_float4(positions[(size_t)point * 3], positions[(size_t)point * 3 + 1],
                               positions[(size_t)point * 3 + 2], w);
     }
@@ -117,8 +124,8 @@ __global__ void flat_kernel(uint64_t count, const float *positions, const uint32
 
 // Step 2. `levels` bounds a climb (the BVH2's depth + 1), so a damaged parent table can
 // only end a climb early, never loop.
-__global__ void climb_kernel(uint32_t entries, const float4 *tris, float4 *exact, const uint32_t *parents,
-                             uint32_t *counters, float *root_box, uint32_t levels) {
+__global__ void climb_kernel(uint32_t entries, const float *positions, const uint32_t *indices, float4 *exact,
+                             const uint32_t *parents, uint32_t *counters, float *root_box, uint32_t levels) {
     const uint32_t e = blockIdx.x * blockDim.x + threadIdx.x;
     if (e >= entries) return;
     const float4 links = exact[(size_t)e * 4 + 3];
@@ -126,7 +133,7 @@ __global__ void climb_kernel(uint32_t entries, const float4 *tris, float4 *exact
     uint32_t leaves = 0;
     for (uint32_t side = 0; side < 2; side++)
         if (link[side] < 0) {
-            write_side(exact, e, side, leaf_box(tris, link[side]));
+            write_side(exact, e, side, leaf_box(positions, indices, link[side]));
             leaves++;
         }
     if (leaves == 0) return;
@@ -152,9 +159,9 @@ __global__ void climb_kernel(uint32_t entries, const float4 *tris, float4 *exact
 }
 
 // A scene whose root is a leaf (at most 16 triangles): its box.
-__global__ void leaf_root_kernel(const float4 *tris, int root, float *root_box) {
+__global__ void leaf_root_kernel(const float *positions, const uint32_t *indices, int root, float *root_box) {
     if (threadIdx.x != 0 || blockIdx.x != 0) return;
-    const Box b = leaf_box(tris, root);
+    const Box b = leaf_box(positions, indices, root);
     for (int k = 0; k < 3; k++) {
         root_box[k] = b.lo[k];
         root_box[4 + k] = b.hi[k];
@@ -228,15 +235,16 @@ void refit_scene(lr_gpu_scene *gs, cudaStream_t stream) {
     float4 *tris = const_cast<float4 *>(s.tris);
     float4 *exact = const_cast<float4 *>(s.ref_bvh.entries);
     float4 *widened = const_cast<float4 *>(s.bvh.entries);
-    tris_kernel<<<grid_for(T * 3, sms), 256, 0, stream>>>(T, s.positions, s.indices, tris);
+    tris_kernel<<<grid_for(T * 3, sms), 256, 0, stream>>>(T, s.positions, s.indices, s.ids, tris);
     flat_kernel<<<grid_for(T, sms), 256, 0, stream>>>(T, s.positions, s.indices, gs->flat, const_cast<uint4 *>(s.shading));
     const uint64_t E = s.entry_count;
     if (E > 0) {
         LR_CUDA(cudaMemsetAsync(gs->counters, 0, E * sizeof(uint32_t), stream));
-        climb_kernel<<<(unsigned)((E + 127) / 128), 128, 0, stream>>>((uint32_t)E, tris, exact, gs->parents, gs->counters,
-                                                                       gs->root_box, s.depth + 2);
+        climb_kernel<<<(unsigned)((E + 127) / 128), 128, 0, stream>>>((uint32_t)E, s.positions, s.indices, exact,
+                                                                       gs->parents, gs->counters, gs->root_box,
+                                                                       s.depth + 2);
     } else {
-        leaf_root_kernel<<<1, 32, 0, stream>>>(tris, s.bvh.root, gs->root_box);
+        leaf_root_kernel<<<1, 32, 0, stream>>>(s.positions, s.indices, s.bvh.root, gs->root_box);
     }
     LR_CUDA(cudaGetLastError());
     float root[8];
