@@ -223,8 +223,10 @@ void lr_gpu_scene_destroy(lr_gpu_scene *scene);
  * order are kept, so traversal stays exact but slows as the tree fits the moved points
  * worse. The boxes equal lr_scene_move_points' bit for bit. Runs on `ctx`'s stream and
  * waits. Work that reads the scene must not be in flight: ray queries queued earlier on
- * other streams, or a batch member's passes (a batch member keeps the root box it joined
- * with: remove it, refit, add it again; lr_renderer_refit does this for a renderer). */
+ * other streams, or the passes of a batch with members tracing it (lr_batch_wait first).
+ * Such members trace the moved geometry from their next pass on; their lights and light
+ * tree stay as they were loaded (remove and add a member to load them again). A renderer
+ * refits its own upload through lr_renderer_refit. */
 #define LR_REFIT_DEVICE 1u
 int lr_gpu_scene_refit(lr_context *ctx, lr_gpu_scene *scene, const void *positions, uint64_t point_count,
                        uint32_t flags);

@@ -86,6 +86,7 @@ struct lr_gpu_scene {
     uint8_t *flat = nullptr;
     float *root_box = nullptr;
     uint64_t topology = 0;  // a hash of the triangles (leaf order) a refit must keep
+    uint64_t refits = 0;    // refits so far: batch members borrowing the scene follow them
 };
 
 namespace lr {

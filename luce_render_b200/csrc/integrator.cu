@@ -1938,6 +1938,10 @@ struct MemberHost {
     bool view_traced = false;  // it holds splat accumulators
     bool view_adaptive = false;  // it holds the half estimate and verdicts
     lr_gpu_scene *owned = nullptr;  // a renderer's own upload (null when borrowed)
+    // The upload the member traces and the refits of it its record has seen: a refit
+    // (refit.cu) moves the root box, which the record holds by value.
+    const lr_gpu_scene *source = nullptr;
+    uint64_t source_refits = 0;
     uint32_t samples = 0, sample = 0, next_pixel = 0, done = 0;
     uint32_t light_next = 0;  // light paths of the current sample planned so far
     uint32_t max_bounces = 0;
@@ -2496,6 +2500,8 @@ uint32_t member_add(WaveHost *h, const lr_gpu_scene *gs, lr_gpu_scene *owned, co
     Member &m = mh.dev;
     m = Member{};
     m.scene = gs->scene;
+    mh.source = gs;
+    mh.source_refits = gs->refits;
     set_loaded(m, records, L, mh.block, settings, rounds);
     set_view_memory(m, view, view_parts, mh.view, traced.count > 0, adaptive);
     set_view(m, frame, traced);
@@ -2583,6 +2589,8 @@ void member_renew(WaveHost *h, uint32_t index, const lr_frame &frame, const lr_s
         LR_CUDA(cudaFreeAsync(mh.block, stream));
         mh.block = block;
         m.scene = gs->scene;
+        mh.source = gs;
+        mh.source_refits = gs->refits;
         set_loaded(m, records, *L, block, chosen, rounds);
     }
     if (new_view) {
@@ -2721,7 +2729,28 @@ int free_display_slot(WaveHost *h) {
 // pass at most, so a pixel never gets two samples in one pass. A dry pass (autotuning)
 // plans the same way, from the members of size class `only` when it is not -1, but
 // moves no member on and leaves the films alone. Returns false with no work.
+// Members whose upload was refit since their record was made take its new scene record
+// (root boxes) ahead of the next pass, stream-ordered like any member upload. Their
+// loaded records (light tree, scene radius) stay as they were loaded: still an unbiased
+// estimator, as each pdf comes from the same records that sample it.
+void follow_refits(WaveHost *h) {
+    for (size_t i = 0; i < h->members.size(); i++) {
+        MemberHost &mh = h->members[i];
+        if (!mh.used || !mh.source || mh.source->refits == mh.source_refits) continue;
+        mh.dev.scene = mh.source->scene;
+        mh.source_refits = mh.source->refits;
+        const size_t at = (size_t)((const char *)&mh.dev.scene - (const char *)&mh.dev);
+        char *stage = h->staging.take(sizeof(DeviceScene));
+        std::memcpy(stage, &mh.dev.scene, sizeof(DeviceScene));
+        LR_CUDA(cudaMemcpyAsync((char *)(h->d_members + i) + at, stage, sizeof(DeviceScene), cudaMemcpyHostToDevice,
+                                h->ctx->stream));
+        h->staging.queued(h->ctx->stream);
+        h->member_uploads++;
+    }
+}
+
 bool launch_pass(WaveHost *h, bool dry = false, int only = -1) {
+    follow_refits(h);
     Lane &lane = lane_of(h, h->recorded);
     Plan *staging = lane.h_plan;
     Segment *seg = staging->seg;

@@ -273,6 +273,7 @@ void refit_scene(lr_gpu_scene *gs, cudaStream_t stream) {
             gs->wide8_nodes * 8, 8, gs->wide8_sources, exact, gs->root_box, delta, const_cast<float4 *>(s.wide8.nodes));
     LR_CUDA(cudaGetLastError());
     LR_CUDA(cudaStreamSynchronize(stream));
+    gs->refits++;
 }
 
 }  // namespace lr

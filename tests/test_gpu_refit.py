@@ -176,3 +176,35 @@ def test_renderer_refit_equals_fresh_renderer(ctx, spectral):
     finally:
         fresh.destroy()
     assert np.array_equal(_bits(got), _bits(want))
+
+
+def test_batch_member_follows_a_refit(ctx):
+    # A batch member borrowing an upload that is refit before its passes traces the moved
+    # geometry: the Cornell box grown by a fifth (past its old root box) renders, bit for
+    # bit, what a renderer made from the moved scene renders. Its loaded records do not
+    # depend on the points here (a rect light, no light paths).
+    sc = lr.compile_scene(scenes.cornell_meshes(materials=True), [scenes.cornell_camera()],
+                          [scenes.cornell_light()], scenes.cornell_materials())
+    s = lr.RenderSettings.of(40, 32, 3)
+    s.max_bounces = 4
+    s.light_tracing = 0.0
+    s.seed = 11
+    gs = lr.GpuScene.upload(ctx, sc)
+    b = lr.Batch(ctx, lr.BatchSettings.default(pool=1 << 16, max_bounces=8, capacity=2))
+    try:
+        m = b.add(gs, sc, s)
+        moved = (sc.arrays()["positions"] * np.float32(1.2)).astype(np.float32)
+        sc.move_points(moved)
+        gs.refit(ctx, moved)
+        b.finish()
+        got = b.read(m)
+    finally:
+        b.destroy()
+        gs.destroy()
+    fresh = lr.Renderer.create(ctx, sc, s)
+    try:
+        fresh.finish()
+        want = fresh.read()
+    finally:
+        fresh.destroy()
+    assert np.array_equal(_bits(got), _bits(want))
