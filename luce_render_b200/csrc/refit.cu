@@ -122,8 +122,18 @@ __global__ void flat_kernel(uint64_t count, const float *positions, const uint32
     }
 }
 
+// An atomic add with release and acquire semantics at device scope: the box stores before
+// it are visible to the thread whose add comes after, and that thread's loads after its add
+// see them (one atom.acq_rel in place of a full __threadfence on each side).
+__device__ __forceinline__ uint32_t add_acq_rel(uint32_t *counter, uint32_t value) {
+    uint32_t old;
+    asm volatile("atom.acq_rel.gpu.global.add.u32 %0, [%1], %2;" : "=r"(old) : "l"(counter), "r"(value) : "memory");
+    return old;
+}
+
 // Step 2. `levels` bounds a climb (the BVH2's depth + 1), so a damaged parent table can
-// only end a climb early, never loop.
+// only end a climb early, never loop. The next parent link is fetched before the atomic
+// (the table is read-only), so it is not on the climb's chain of dependent latencies.
 __global__ void climb_kernel(uint32_t entries, const float *positions, const uint32_t *indices, float4 *exact,
                              const uint32_t *parents, uint32_t *counters, float *root_box, uint32_t levels) {
     const uint32_t e = blockIdx.x * blockDim.x + threadIdx.x;
@@ -137,13 +147,11 @@ __global__ void climb_kernel(uint32_t entries, const float *positions, const uin
             leaves++;
         }
     if (leaves == 0) return;
-    __threadfence();
-    if (atomicAdd(&counters[e], leaves) + leaves != 2u) return;
+    uint32_t up = __ldg(&parents[e]);
+    if (add_acq_rel(&counters[e], leaves) + leaves != 2u) return;
     uint32_t at = e;
     for (uint32_t level = 0; level < levels; level++) {
-        __threadfence();
         const Box box = join(read_side(exact, at, 0), read_side(exact, at, 1));
-        const uint32_t up = parents[at];
         if (up == 0xffffffffu) {
             for (int k = 0; k < 3; k++) {
                 __stcg(&root_box[k], box.lo[k]);
@@ -151,10 +159,12 @@ __global__ void climb_kernel(uint32_t entries, const float *positions, const uin
             }
             return;
         }
-        write_side(exact, up >> 1, up & 1u, box);
-        __threadfence();
-        if (atomicAdd(&counters[up >> 1], 1u) == 0u) return;  // the sibling is still on its way
-        at = up >> 1;
+        const uint32_t parent = up >> 1;
+        const uint32_t next = __ldg(&parents[parent]);
+        write_side(exact, parent, up & 1u, box);
+        if (add_acq_rel(&counters[parent], 1u) == 0u) return;  // the sibling is still on its way
+        at = parent;
+        up = next;
     }
 }
 
