@@ -301,10 +301,9 @@ int lr_gpu_scene_refit(lr_context *ctx, lr_gpu_scene *gs, const void *positions,
         LR_CUDA(cudaSetDevice(ctx->device));
         float *dst = const_cast<float *>(gs->scene.positions);
         const size_t bytes = point_count * 3 * sizeof(float);
-        if (bytes && dst != positions)
-            LR_CUDA(cudaMemcpyAsync(dst, positions, bytes,
-                                    (flags & LR_REFIT_DEVICE) ? cudaMemcpyDeviceToDevice : cudaMemcpyHostToDevice,
-                                    ctx->stream));
+        // The copy's direction follows the pointer (unified addressing), so a pointer given
+        // with the wrong flag is still copied from where it lives rather than misread.
+        if (bytes && dst != positions) LR_CUDA(cudaMemcpyAsync(dst, positions, bytes, cudaMemcpyDefault, ctx->stream));
         refit_scene(gs, ctx->stream);
     });
 }
