@@ -91,3 +91,40 @@ def test_gpu_matches_f64_oracle_dome(ctx, spectral):
     assert np.all(np.abs(g - o) <= 3.0 * sem + 1e-6), np.max(np.abs(g - o) / (sem + 1e-12))
     relative = np.abs(gpu - mean) / np.maximum(np.abs(mean), 1e-3)
     assert np.mean(relative < 1e-3) >= 0.95, np.mean(relative < 1e-3)
+
+
+def test_reload_with_another_dome_image(ctx):
+    # Renderer.reload with the same geometry under another sky (the sun moved, a brighter
+    # dome), passes in flight: the image equals a renderer made for the new sky, bit for bit.
+    meshes, cams, _, mats, background = scenes.caustic_scene()
+    sky, _ = testscenes.sun_sky()
+    moved_sun = np.full_like(sky, 0.5)
+    moved_sun[4:6, 10:12] = 300.0
+    s = lr.RenderSettings.of(32, 24, 6)
+    s.spectral = 1
+    s.max_bounces = 4
+    s.light_tracing = 0.5
+    s.background = background
+    s.c.material = lr.OpenPbr.lambert()
+
+    def compiled(image, intensity):
+        dome = lr.light(lr.LIGHT_DOME, rotation=(0.0, 0.7, 0.0), intensity=intensity, image=image)
+        return lr.compile_scene(meshes, cams, [dome], mats)
+
+    first, second = compiled(sky, 0.5), compiled(moved_sun, 0.8)
+    r = lr.Renderer.create(ctx, first, s)
+    try:
+        r.advance()
+        r.advance()
+        r.reload(second, s)
+        r.finish()
+        got = r.read()
+    finally:
+        r.destroy()
+    fresh = lr.Renderer.create(ctx, second, s)
+    try:
+        fresh.finish()
+        want = fresh.read()
+    finally:
+        fresh.destroy()
+    assert np.array_equal(got.view(np.uint32), want.view(np.uint32))
