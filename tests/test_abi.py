@@ -73,3 +73,20 @@ def test_empty_scene_and_bad_light():
     bad = lr.light(9)
     with pytest.raises(lr.RenderError):
         lr.compile_scene([], lights=[bad])
+
+
+def test_dome_image_checks():
+    # A dome's image is height x width x 3 (the harness checks the shape); an image with
+    # no pixels is refused by the compile; the compiled scene keeps its own copy.
+    with pytest.raises(ValueError):
+        lr.light(lr.LIGHT_DOME, image=np.zeros((4, 4), np.float32))
+    empty = lr.light(lr.LIGHT_DOME, image=np.zeros((2, 3, 3), np.float32))
+    empty.image_width = 0
+    with pytest.raises(lr.RenderError) as e:
+        lr.compile_scene([], lights=[empty])
+    assert e.value.code == 400
+    sky = np.ones((2, 4, 3), np.float32)
+    dome = lr.light(lr.LIGHT_DOME, image=sky)
+    sc = lr.compile_scene([], lights=[dome])
+    sky[:] = np.nan  # the caller's buffer may change or go once the compile returns
+    assert sc.info.light_count == 1
