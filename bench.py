@@ -735,7 +735,9 @@ def main():
             "cpu_baseline": cpu,
             "e2e": {"value": e2e_value, "unit": "Mrays/s", "h2d_bytes_per_step": 0,
                     "d2h_bytes_per_step": WIDTH * HEIGHT * 16},
-            "gpu_launches": K * (1 + 3 * (BOUNCES + 1) + 3),
+            # a pass: camera; closest, shade and shadow each round; finish, fold, the two
+            # adaptive phases and convert (the launch list in profiles/ counts the same)
+            "gpu_launches": K * (1 + 3 * (BOUNCES + 1) + 5),
             "clocks": clock_info,
             "light_traced": traced_info,
             "cornell": cornell_info,

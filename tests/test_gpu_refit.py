@@ -208,3 +208,14 @@ def test_batch_member_follows_a_refit(ctx):
     finally:
         fresh.destroy()
     assert np.array_equal(_bits(got), _bits(want))
+
+
+def test_refit_empty_scene(ctx):
+    sc = lr.compile_scene([])
+    gs = lr.GpuScene.upload(ctx, sc)
+    try:
+        gs.refit(ctx, np.zeros((0, 3), np.float32))
+        hits = lr.trace_rays(ctx, gs, scenes.random_rays(64))
+        assert np.all(lr.hit_ids(hits) == -1)
+    finally:
+        gs.destroy()

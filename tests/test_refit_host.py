@@ -95,3 +95,9 @@ def test_move_points_rejects_other_counts():
     bad[0, 0] = np.nan
     with pytest.raises(lr.RenderError):
         sc.move_points(bad)
+
+
+def test_move_points_of_an_empty_scene():
+    sc = lr.compile_scene([])
+    sc.move_points(np.zeros((0, 3), np.float32))
+    assert sc.triangle_count() == 0 and len(sc.arrays()["nodes"]) == 1
