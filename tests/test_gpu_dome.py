@@ -6,9 +6,9 @@ sampled by importance (rows, then the row's texels), or a uniform colour without
   white sphere under a white dome, white within 1 % over the frame and 2 % on the sphere)
   and the dome sun (a grey floor under a sky whose sun is 1/512 of its texels reflects
   albedo / pi x the image's irradiance within 2 %), spectral and RGB.
-- The f64 oracle over the same samples on a glossy scene under the sun sky's dome, with
-  light tracing (light paths from afar start on the disk facing the dome): 8x8-block means
-  within 3 sigma and most pixels within f32 rounding.
+- The f64 oracle over the same samples on a glossy scene under the sun sky's dome, or a dome
+  of one colour, with light tracing (light paths from afar start on the disk facing the
+  dome): 8x8-block means within 3 sigma and most pixels within f32 rounding.
 """
 import math
 
@@ -68,11 +68,13 @@ def _blocks(x, b):
     return x[: h // b * b, : w // b * b].reshape(h // b, b, w // b, b, -1)
 
 
-@pytest.mark.parametrize("spectral", [False, True])
-def test_gpu_matches_f64_oracle_dome(ctx, spectral):
+@pytest.mark.parametrize("spectral,textured", [(False, True), (True, True), (True, False)])
+def test_gpu_matches_f64_oracle_dome(ctx, spectral, textured):
+    # The sun sky's dome, or a dome of one colour (sampled uniformly over the sphere).
     meshes, cams, lights, mats, background = scenes.caustic_scene()
     sky, _ = testscenes.sun_sky()
-    lights = [lr.light(lr.LIGHT_DOME, rotation=(0.0, 0.7, 0.0), intensity=0.5, image=sky)]
+    lights = [lr.light(lr.LIGHT_DOME, rotation=(0.0, 0.7, 0.0), intensity=0.5, image=sky if textured else None,
+                       color=(1.0, 0.9, 0.7))]
     sc = lr.compile_scene(meshes, cams, lights, mats)
     w, h, spp, bounces = 48, 32, 32, 6
     library = [lr.OpenPbr.lambert()] + mats

@@ -84,13 +84,15 @@ def test_oracle_dome_sun(spectral):
     assert abs(mean[..., 1].mean() / expected - 1.0) < 0.02, (mean[..., 1].mean(), expected)
 
 
-def test_oracle_dome_light_paths_are_unbiased():
-    # Light paths from afar start on the disk facing the dome (its image by importance);
-    # with and without them, the image of glossy objects under the sun sky has the same mean.
+@pytest.mark.parametrize("textured", [True, False])
+def test_oracle_dome_light_paths_are_unbiased(textured):
+    # Light paths from afar start on the disk facing the dome (its image by importance, or
+    # uniform over the sphere for a dome of one colour); with and without them, the image of
+    # glossy objects under the dome has the same mean.
     from luce_render_b200 import scenes
     meshes, cams, _, mats, background = scenes.caustic_scene()
     sky, _ = testscenes.sun_sky()
-    lights = [lr.light(lr.LIGHT_DOME, rotation=(0.0, 0.7, 0.0), intensity=0.5, image=sky)]
+    lights = [lr.light(lr.LIGHT_DOME, rotation=(0.0, 0.7, 0.0), intensity=0.5, image=sky if textured else None)]
     sc = lr.compile_scene(meshes, cams, lights, mats)
     w, h, spp = 32, 24, 64
     frame = lr.ray_frame(sc.camera(), w, h)
