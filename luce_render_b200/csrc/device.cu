@@ -512,6 +512,7 @@ int lr_gpu_scene_upload(lr_context *ctx, const lr_scene *scene, lr_gpu_scene **o
         gs->flat = (uint8_t *)(base + parts[14].offset);
         gs->root_box = (float *)(base + parts[15].offset);
         gs->topology = topology_hash(*scene);
+        gs->any_flat = std::any_of(scene->flat.begin(), scene->flat.end(), [](uint8_t f) { return f != 0; });
         for (DeviceBvh *b : {&s.bvh, &s.ref_bvh}) {
             b->root = L.root;
             b->empty = T == 0 ? 1 : 0;

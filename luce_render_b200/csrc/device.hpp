@@ -87,6 +87,7 @@ struct lr_gpu_scene {
     float *root_box = nullptr;
     uint64_t topology = 0;  // a hash of the triangles (leaf order) a refit must keep
     uint64_t refits = 0;    // refits so far: batch members borrowing the scene follow them
+    bool any_flat = false;  // some triangle's normals are its own flat one
 };
 
 namespace lr {

@@ -246,7 +246,9 @@ void refit_scene(lr_gpu_scene *gs, cudaStream_t stream) {
     float4 *exact = const_cast<float4 *>(s.ref_bvh.entries);
     float4 *widened = const_cast<float4 *>(s.bvh.entries);
     tris_kernel<<<grid_for(T * 3, sms), 256, 0, stream>>>(T, s.positions, s.indices, s.ids, tris);
-    flat_kernel<<<grid_for(T, sms), 256, 0, stream>>>(T, s.positions, s.indices, gs->flat, const_cast<uint4 *>(s.shading));
+    if (gs->any_flat)
+        flat_kernel<<<grid_for(T, sms), 256, 0, stream>>>(T, s.positions, s.indices, gs->flat,
+                                                         const_cast<uint4 *>(s.shading));
     const uint64_t E = s.entry_count;
     if (E > 0) {
         LR_CUDA(cudaMemsetAsync(gs->counters, 0, E * sizeof(uint32_t), stream));
