@@ -157,6 +157,15 @@ typedef struct lr_scene lr_scene;
 int lr_scene_compile(const lr_mesh *meshes, size_t mesh_count, const lr_camera *cameras,
                      size_t camera_count, const lr_light *lights, size_t light_count,
                      const lr_openpbr *materials, size_t material_count, lr_scene **out);
+/* compile_scene(..., trees = false) (scene.lucb:111-129): with LR_COMPILE_NO_TREES the
+ * host builds no BVH2 and the triangles stay in the meshes' order (order is the identity);
+ * such a scene is for lr_gpu_scene_build, which builds its tree on the device. flags 0 is
+ * lr_scene_compile. */
+#define LR_COMPILE_NO_TREES 1u
+int lr_scene_compile_ex(const lr_mesh *meshes, size_t mesh_count, const lr_camera *cameras,
+                        size_t camera_count, const lr_light *lights, size_t light_count,
+                        const lr_openpbr *materials, size_t material_count, uint32_t flags,
+                        lr_scene **out);
 /* CompiledScene.close (scene.lucb:87-98). */
 void lr_scene_free(lr_scene *scene);
 /* (No counterpart: the reference compiles a moved mesh again, rebuilding its BVH2,
@@ -211,6 +220,14 @@ typedef struct lr_gpu_scene lr_gpu_scene;
 /* GpuScene.upload (device.lucb:41): the scene's traversal and shading buffers in HBM.
  * The scene may be freed afterwards. */
 int lr_gpu_scene_upload(lr_context *ctx, const lr_scene *scene, lr_gpu_scene **out);
+/* GpuScene.upload(accelerate = true) (device.lucb:41-89), where a ray-tracing device builds
+ * its own acceleration structure: uploads the scene's triangles and builds a linear BVH2 on
+ * the device (Morton codes of the centroids, a radix sort, the Karras hierarchy, boxes by
+ * the refit climb), ignoring any host tree; a scene compiled with LR_COMPILE_NO_TREES skips
+ * the host build entirely. Probes and ray queries on it (the BVH2 path only) return the same
+ * exact closest hits as an upload; renders (lr_batch_add) refuse it, since its leaf order
+ * is its own. Runs on ctx's stream and waits; LR_LIMIT past 2^27 triangles or 94 levels. */
+int lr_gpu_scene_build(lr_context *ctx, const lr_scene *scene, lr_gpu_scene **out);
 /* GpuScene.destroy (device.lucb:108-121). */
 void lr_gpu_scene_destroy(lr_gpu_scene *scene);
 

@@ -37,6 +37,7 @@ INVALID, LIMIT, STOPPED, DEVICE, TIMEOUT = 400, 401, 402, 500, 504
 TRACE_ANY, TRACE_REFERENCE, TRACE_COUNT = 1, 2, 4
 LIGHT_RECT, LIGHT_DISK, LIGHT_SPHERE, LIGHT_DISTANT, LIGHT_DOME = 0, 1, 2, 3, 4
 REFIT_DEVICE = 1
+COMPILE_NO_TREES = 1
 
 
 class RenderError(RuntimeError):
@@ -245,6 +246,8 @@ _SIGNATURES = {
     "lr_openpbr_standard": (None, [C.POINTER(OpenPbr)]),
     "lr_scene_compile": (C.c_int, [C.POINTER(Mesh), _sz, C.POINTER(Camera), _sz, C.POINTER(Light), _sz,
                                    C.POINTER(OpenPbr), _sz, C.POINTER(_vp)]),
+    "lr_scene_compile_ex": (C.c_int, [C.POINTER(Mesh), _sz, C.POINTER(Camera), _sz, C.POINTER(Light), _sz,
+                                      C.POINTER(OpenPbr), _sz, _u32, C.POINTER(_vp)]),
     "lr_scene_free": (None, [_vp]),
     "lr_scene_info_get": (C.c_int, [_vp, C.POINTER(SceneInfo)]),
     "lr_scene_arrays": (C.c_int, [_vp] + [C.POINTER(_vp)] * 6),
@@ -254,6 +257,7 @@ _SIGNATURES = {
     "lr_frame_pack": (C.c_int, [C.POINTER(Frame), C.POINTER(C.c_float)]),
     "lr_scene_camera": (C.c_int, [_vp, _i32, C.POINTER(Camera)]),
     "lr_gpu_scene_upload": (C.c_int, [_vp, _vp, C.POINTER(_vp)]),
+    "lr_gpu_scene_build": (C.c_int, [_vp, _vp, C.POINTER(_vp)]),
     "lr_gpu_scene_destroy": (None, [_vp]),
     "lr_scene_move_points": (C.c_int, [_vp, C.POINTER(C.c_float), _u64]),
     "lr_gpu_scene_refit": (C.c_int, [_vp, _vp, _vp, _u64, _u32]),
@@ -596,15 +600,16 @@ class CompiledScene:
 
 
 def compile_scene(meshes: Sequence[MeshData], cameras: Sequence[Camera] = (), lights: Sequence[Light] = (),
-                  materials: Sequence[OpenPbr] = ()) -> CompiledScene:
-    """render.compile_scene (scene.lucb:111-129)."""
+                  materials: Sequence[OpenPbr] = (), trees: bool = True) -> CompiledScene:
+    """render.compile_scene (scene.lucb:111-129). Without `trees` the host builds no BVH2 and
+    the triangles keep the meshes' order: such a scene is for GpuScene.build."""
     cm = (Mesh * max(1, len(meshes)))(*[m.to_c() for m in meshes])
     cc = (Camera * max(1, len(cameras)))(*cameras)
     cl = (Light * max(1, len(lights)))(*lights)
     cmat = (OpenPbr * max(1, len(materials)))(*materials)
     handle = _vp()
-    _check(lib.lr_scene_compile(cm, len(meshes), cc, len(cameras), cl, len(lights), cmat, len(materials),
-                                C.byref(handle)))
+    _check(lib.lr_scene_compile_ex(cm, len(meshes), cc, len(cameras), cl, len(lights), cmat, len(materials),
+                                   0 if trees else COMPILE_NO_TREES, C.byref(handle)))
     return CompiledScene(handle)
 
 
@@ -636,6 +641,14 @@ class GpuScene:
     def upload(ctx: Context, scene: CompiledScene) -> "GpuScene":
         handle = _vp()
         _check(lib.lr_gpu_scene_upload(ctx.handle, scene.handle, C.byref(handle)))
+        return GpuScene(handle, ctx)
+
+    @staticmethod
+    def build(ctx: Context, scene: CompiledScene) -> "GpuScene":
+        """GpuScene.upload(accelerate = true) (device.lucb:41-89): the scene's triangles with a
+        linear BVH2 built on the device (lr_gpu_scene_build). Probes and ray queries only."""
+        handle = _vp()
+        _check(lib.lr_gpu_scene_build(ctx.handle, scene.handle, C.byref(handle)))
         return GpuScene(handle, ctx)
 
     def destroy(self) -> None:

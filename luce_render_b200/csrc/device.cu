@@ -125,8 +125,9 @@ TraversalChoice choose_traversal(const DeviceScene &s, int requested) {
         }
     }
     auto wide_stack = [](uint32_t bound) { return bound + 1 <= 32 ? 32 : (bound + 1 <= 48 ? 48 : 0); };
-    if (requested == 8 && wide_stack(s.wide8.max_stack)) return {8, wide_stack(s.wide8.max_stack)};
-    if (requested >= 4 && wide_stack(s.wide4.max_stack)) return {4, wide_stack(s.wide4.max_stack)};
+    // A scene built on the device has no wide collapses (null nodes).
+    if (requested == 8 && s.wide8.nodes && wide_stack(s.wide8.max_stack)) return {8, wide_stack(s.wide8.max_stack)};
+    if (requested >= 4 && s.wide4.nodes && wide_stack(s.wide4.max_stack)) return {4, wide_stack(s.wide4.max_stack)};
     return {2, stack_for(s.depth)};
 }
 

@@ -88,6 +88,9 @@ struct lr_gpu_scene {
     uint64_t topology = 0;  // a hash of the triangles (leaf order) a refit must keep
     uint64_t refits = 0;    // refits so far: batch members borrowing the scene follow them
     bool any_flat = false;  // some triangle's normals are its own flat one
+    // Built on the device (build.cu): a linear BVH in its own leaf order, no wide collapses;
+    // its leaf order is not the compiled scene's, so renders do not take it.
+    bool device_built = false;
 };
 
 namespace lr {

@@ -3623,6 +3623,8 @@ int lr_batch_add(lr_batch *b, const lr_gpu_scene *gs, const lr_scene *scene, con
                  const lr_frame *frame, uint32_t *member) {
     return guarded([&] {
         if (!b || !gs || !scene || !settings || !member) fail(LR_INVALID, "a member needs a scene and settings");
+        if (gs->device_built)
+            fail(LR_INVALID, "a member renders an upload of its compiled scene (lr_gpu_scene_upload), not a device build");
         lr_frame f;
         if (frame) f = *frame;
         else camera_of(scene, settings, f);

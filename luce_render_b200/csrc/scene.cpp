@@ -248,7 +248,15 @@ void lr_openpbr_standard(lr_openpbr *m) {
 int lr_scene_compile(const lr_mesh *meshes, size_t mesh_count, const lr_camera *cameras,
                      size_t camera_count, const lr_light *lights, size_t light_count,
                      const lr_openpbr *materials, size_t material_count, lr_scene **out) {
+    return lr_scene_compile_ex(meshes, mesh_count, cameras, camera_count, lights, light_count, materials,
+                               material_count, 0u, out);
+}
+
+int lr_scene_compile_ex(const lr_mesh *meshes, size_t mesh_count, const lr_camera *cameras,
+                        size_t camera_count, const lr_light *lights, size_t light_count,
+                        const lr_openpbr *materials, size_t material_count, uint32_t flags, lr_scene **out) {
     return guarded([&] {
+        if (flags & ~LR_COMPILE_NO_TREES) fail(LR_INVALID, "unknown compile flags");
         if (!out) fail(LR_INVALID, "compile_scene needs somewhere to put the scene");
         *out = nullptr;
         if ((mesh_count && !meshes) || (camera_count && !cameras) || (light_count && !lights) ||
@@ -274,7 +282,16 @@ int lr_scene_compile(const lr_mesh *meshes, size_t mesh_count, const lr_camera *
         }
         scene->lights.assign(lights, lights + light_count);
         for (lr_light &l : scene->lights) l.image = nullptr;
-        build_bvh(*scene);
+        if (flags & LR_COMPILE_NO_TREES) {
+            // Without trees (scene.lucb:127-128): the triangles in the meshes' order.
+            if (scene->triangle_count() > 0x7fffffffull) fail(LR_LIMIT, "a scene holds at most 2^31 triangles");
+            scene->nodes.clear();
+            scene->order.resize(scene->triangle_count());
+            for (size_t t = 0; t < scene->order.size(); t++) scene->order[t] = (uint32_t)t;
+            scene->bvh_depth = 0;
+        } else {
+            build_bvh(*scene);
+        }
         *out = scene.release();
     });
 }
