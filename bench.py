@@ -513,6 +513,7 @@ def refit(lr, scenes, ctx, dist, repeats: int = 10) -> dict:
     upload_s = time.perf_counter() - start
     gs2.destroy()
     rebuilt.close()
+    build_info = device_build(lr, scenes, ctx, dist, sc, meshes, cam, lights, mats)
     sc.close()
     hbm = measured_peaks().get("hbm_gbs") or 6650.0
     achieved = algorithmic / (refit_ms / 1e3) / 1e9
@@ -523,7 +524,58 @@ def refit(lr, scenes, ctx, dist, repeats: int = 10) -> dict:
             "host_compile_ms": compile_s * 1e3, "host_upload_ms": upload_s * 1e3,
             "speedup_vs_host_rebuild": (compile_s + upload_s) * 1e3 / refit_ms,
             "timing": "device refit: CUDA events on the context's stream around the call (it waits for the new "
-                      "root box between launches), median of 10; host rebuild: wall clock"}
+                      "root box between launches), median of 10; host rebuild: wall clock",
+            "device_build": build_info}
+
+
+def device_build(lr, scenes, ctx, dist, sc, meshes, cam, lights, mats, repeats: int = 5) -> dict:
+    """The 1,048,576-triangle scene's BVH2 built on the device (lr_gpu_scene_build on a tree-less
+    compile) against the host's binned-SAH compile and upload, and the closest-hit rate of both
+    trees on the same 2^22 incoherent rays resident in device memory."""
+    start = time.perf_counter()
+    flat = lr.compile_scene(meshes, [cam], lights, mats, trees=False)
+    flat_compile_s = time.perf_counter() - start
+    start = time.perf_counter()
+    full = lr.compile_scene(meshes, [cam], lights, mats)
+    sah_compile_s = time.perf_counter() - start
+    uploaded = lr.GpuScene.upload(ctx, full)
+    for _ in range(2):
+        lr.GpuScene.build(ctx, flat).destroy()
+    times = []
+    for _ in range(repeats):
+        ctx.synchronize()
+        ctx.timer_start()
+        built = lr.GpuScene.build(ctx, flat)
+        times.append(ctx.timer_stop())
+        built.destroy()
+    build_ms = dist.max(statistics.median(times))
+    built = lr.GpuScene.build(ctx, flat)
+    rays = scenes.incoherent_rays(1 << 22, seed=9)
+    d_rays, d_hits = ctx.alloc(rays.nbytes), ctx.alloc(len(rays) * 16)
+    ctx.upload(d_rays, rays)
+    rates = {}
+    for name, gs in (("device_built", built), ("host_sah", uploaded)):
+        for _ in range(3):
+            lr._check(lr.lib.lr_trace_rays_device(ctx.handle, gs.handle, d_rays, len(rays), d_hits, 0))
+        ms = []
+        for _ in range(5):
+            ctx.synchronize()
+            ctx.timer_start()
+            lr._check(lr.lib.lr_trace_rays_device(ctx.handle, gs.handle, d_rays, len(rays), d_hits, 0))
+            ms.append(ctx.timer_stop())
+        rates[name] = len(rays) / (dist.max(statistics.median(ms)) / 1e3) / 1e6
+    ctx.free(d_rays)
+    ctx.free(d_hits)
+    built.destroy()
+    uploaded.destroy()
+    full.close()
+    flat.close()
+    return {"device_build_ms": build_ms, "tree_less_compile_ms": flat_compile_s * 1e3,
+            "host_sah_compile_ms": sah_compile_s * 1e3,
+            "closest_mrays_device_built": rates["device_built"], "closest_mrays_host_sah": rates["host_sah"],
+            "timing": "device build: CUDA events around lr_gpu_scene_build (its copies of the triangles "
+                      "included), median of 5; closest: 2^22 incoherent rays in device memory, CUDA events, "
+                      "median of 5; compiles: wall clock"}
 
 
 def cpu_intersection(sc, scenes, oracle, cores: int) -> dict:
