@@ -435,6 +435,17 @@ typedef struct {
     uint64_t closest_nodes, closest_tests, shadow_nodes, shadow_tests;
 } lr_render_stats;
 int lr_renderer_stats(lr_renderer *renderer, lr_render_stats *out);
+/* (No counterpart in the reference: a test hook.) With settings.profile = 3 every pass
+ * records the rays its traversal kernels traced, round by round; this copies the last
+ * pass's records of round `round` -- the closest-hit queue, or with `shadow` the shadow
+ * queue -- after waiting for work in flight. 12 floats a ray: origin and the path's tag
+ * bits, direction and reach (t_max; the query's t_min is 0), then the triangle
+ * traversal's answer: closest (t, source triangle id as int32 bits or -1, u, v), before
+ * the analytic lights are tested; shadow (1 blocked, 0 clear, -1 not traced by the
+ * any-hit query, 0, 0). *count: the rays of that round; `out` may be NULL to ask for it,
+ * else it holds at least 12 * count floats (`capacity`, in floats). */
+int lr_renderer_recorded_rays(lr_renderer *renderer, uint32_t round, int32_t shadow, float *out,
+                              uint64_t capacity, uint64_t *count);
 /* Renderer.destroy (integrator.lucb:887-900). */
 void lr_renderer_destroy(lr_renderer *renderer);
 

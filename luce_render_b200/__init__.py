@@ -294,6 +294,8 @@ _SIGNATURES = {
     "lr_batch_join": (C.c_int, [_vp]),
     "lr_renderer_kernel_times": (C.c_int, [_vp, C.POINTER(C.c_double)]),
     "lr_renderer_stats": (C.c_int, [_vp, C.POINTER(RenderStats)]),
+    "lr_renderer_recorded_rays": (C.c_int, [_vp, _u32, C.c_int32, C.POINTER(C.c_float), _u64,
+                                            C.POINTER(C.c_uint64)]),
     "lr_renderer_destroy": (None, [_vp]),
     "lr_albedo_tables": (C.c_int, [_vp, C.POINTER(C.c_float), _sz]),
     "lr_batch_settings_default": (None, [C.POINTER(BatchSettings)]),
@@ -922,6 +924,19 @@ class Renderer:
         s = RenderStats()
         _check(lib.lr_renderer_stats(self.handle, C.byref(s)))
         return s
+
+    def recorded_rays(self, round_: int, shadow: bool = False) -> tuple[np.ndarray, np.ndarray]:
+        """The last pass's rays of round `round_` (settings.profile = 3) as the ray
+        queries take them -- (n, 8) float32: origin, t_min 0, direction, t_max -- and the
+        traversal's answers, (n, 4): closest (t, id bits, u, v) or shadow (1 blocked, 0
+        clear, -1 not traced by the any-hit query)."""
+        n = C.c_uint64()
+        _check(lib.lr_renderer_recorded_rays(self.handle, round_, int(shadow), None, 0, C.byref(n)))
+        out = np.empty((n.value, 12), np.float32)
+        _check(lib.lr_renderer_recorded_rays(self.handle, round_, int(shadow), _fptr(out), out.size, C.byref(n)))
+        rays = out[:, :8].copy()
+        rays[:, 3] = 0.0  # the origin's w holds the path's tag; the queries start at t 0
+        return rays, out[:, 8:].copy()
 
     def destroy(self) -> None:
         if self.handle:

@@ -27,9 +27,11 @@ COMMON = ["-O3", "-std=c++17", "-Xcompiler", "-fPIC", "-Xcompiler", "-fvisibilit
 CUDA_FLAGS = ARCH + ["-lineinfo", "--expt-relaxed-constexpr", "-Xptxas", "-v"]
 # The integrator's shading divides and takes square roots at the reference's own
 # precision (Vulkan's GLSL allows 2.5 ulp for a division and computes sqrt from
-# inversesqrt), not as IEEE-exact software sequences; the traversal it includes decides
-# hits and distances with explicitly rounded intrinsics (__frcp_rn, __fmul_rn, ...), which
-# these flags do not touch, so hit ids and distances stay the exact ones.
+# inversesqrt), not as IEEE-exact software sequences. Its traversal kernels live in
+# trace.cu, which takes no such flag: -ftz would also flush the denormal results of the
+# explicitly rounded intrinsics (__fmul_rn, __fsub_rn, ...) the watertight test decides
+# hits with, so the integrator's hits would no longer be the ray queries' and the brute
+# force's.
 FILE_FLAGS = {"integrator.cu": ["-prec-div=false", "-prec-sqrt=false", "-ftz=true"]}
 
 

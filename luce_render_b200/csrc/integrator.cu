@@ -39,58 +39,10 @@
 #include "openpbr.cuh"
 #include "shading.cuh"
 #include "traverse.cuh"
+#include "wave.cuh"
 
 namespace lr {
 namespace {
-
-constexpr int kTraceBlock = 128;
-constexpr int kShadeBlock = 128;
-constexpr uint32_t kMaterialStride = 16;  // vec4 rows per material (openpbr.glsl:28)
-constexpr size_t kDefaultPool = 2097152;  // 2^21 paths (integrator.lucb:98)
-// A ray's tag: the path's pool index in the low bits, its segment in the high bits.
-constexpr uint32_t kPathBits = 23;
-constexpr uint32_t kPathMask = (1u << kPathBits) - 1u;
-constexpr uint32_t kMaxPool = 1u << kPathBits;             // 8,388,608 paths
-constexpr uint32_t kMaxSegments = 1u << (32 - kPathBits);  // 512 segments a pass
-// Rounds a pass traces beyond the bounces when the scene has cut-outs (loading.lucb:161).
-constexpr uint32_t kCutoutRounds = 8;
-
-// One member of a wave: everything its paths read, fixed while it is a member.
-struct Member {
-    DeviceScene scene;
-    const float4 *lights;
-    uint32_t light_count;
-    uint32_t spectral;
-    TreeView tree;
-    const float4 *materials;
-    const Constants *k;
-    float frame[16];
-    float lens_radius, focus_distance;
-    float forward[3];
-    uint32_t width, height;
-    uint64_t pixels;
-    float4 *film, *image;
-    // Light tracing (connect.glsl): light paths a sample (0: none), the band their
-    // sampler numbers follow, 1 / a pixel's area on the image plane at unit distance, and
-    // the splat accumulators (3 fixed-point words a pixel: kSplatScale units of the
-    // film's terms): the film's, and one per lane that a pass's connections land in until
-    // the pass's finish stage folds them into the film's, in pass order.
-    uint32_t light_paths, light_band;
-    float pixel_area_inv;
-    unsigned long long *splat;
-    unsigned long long *splat_lane[2];
-    // A material of the member's has a specular, metal, coat or transmission lobe: its
-    // surfaces take the layered OpenPBR shading (openpbr.cuh).
-    uint32_t glossy;
-    // A material of the member's is a cut-out (geometry_opacity below 1), and the rounds
-    // its passes trace: its bounces + 1, + 8 for rays passing through cut-outs at the same
-    // bounce (integrator.lucb:806-808); a ray for a later round is not traced.
-    uint32_t cutouts, rounds;
-    // Adaptive sampling (adaptive.comp, finish.comp:22-23): the second estimate (odd
-    // samples, twice; w: converged) and the convergence verdicts, or null when off.
-    float4 *half;
-    float *scratch;
-};
 
 // Cut-out opacity (shade_surface.comp:95-104): whether the ray passes through material
 // `material` at this hit, at random with probability 1 - opacity; the hit distance
@@ -102,239 +54,7 @@ __device__ __forceinline__ bool passes_through(const float4 *materials, uint32_t
     return v - floorf(v) >= opacity;
 }
 
-// Splats add as 64-bit integers (units of 2^-32 of the film's terms), so their sum does
-// not depend on the order the connections arrive in.
-constexpr double kSplatScale = 4294967296.0;
-constexpr float kSplatLimit = 1e9f;
 
-// `count` pixels of member `member` from `first_pixel`, at sample `sample`, in pool
-// paths path_base .. path_base + count -- or, of kind kLightSegment, `count` of the
-// sample's light paths from number `first_pixel`. `convert`: this segment ends the
-// member's sample, so its image is brought up to date after the pass. `kind_base`: the
-// pass's paths of the segment's kind before it (its rays' place in the queues).
-constexpr uint32_t kCameraSegment = 0, kLightSegment = 1;
-struct Segment {
-    uint32_t member, first_pixel, count, sample;
-    uint32_t path_base, convert, kind, kind_base;
-};
-
-// `dry`: a trial pass (autotuning) that traces its segments but leaves films alone.
-// `camera_paths`: the pass's camera paths; `folds`: members whose light paths it traces.
-struct PlanHeader {
-    uint32_t segments, paths, converts, dry;
-    uint32_t camera_paths, folds, adapts, reserved;
-};
-
-// A renderer's display image for the pass (film_convert.comp:50-52): where the pass that
-// ends a sample writes the image ready to show (rgba16f, or none), its exposure scale and
-// view (0 clipped, 1 PBR Neutral tone mapping).
-struct PlanDisplay {
-    unsigned long long image;
-    float scale;
-    uint32_t view, reserved0, reserved1;
-};
-
-// A pass's plan: its segments, the members whose images it brings up to date (and the
-// samples they will then hold), and the members whose splats it folds into their films.
-struct Plan {
-    PlanHeader head;
-    PlanDisplay display;  // for the first member converted (a renderer's own)
-    uint32_t convert[kMaxSegments];
-    uint32_t convert_samples[kMaxSegments];
-    uint32_t fold[kMaxSegments];
-    uint32_t adapt[kMaxSegments];  // members whose convergence the pass checks
-    Segment seg[kMaxSegments];
-};
-
-// What a pass's kernels read besides the members: passed by value, fixed for the wave.
-struct Wave {
-    const Member *members;
-    const Plan *plan;
-    uint32_t pool, rounds;
-    uint32_t lane;  // which of the wave's two lanes this is
-    // path state, one slot per pool path
-    float4 *throughput, *radiance, *lambda, *vertex;  // vertex: last scattering point, w survival scale
-    float4 *mis;                                      // light tracing's MIS state (connect.glsl)
-    uint4 *path;  // pixel (a light path's emitter), bounces, previous normal, ray pdf bits
-    // ray queues (ping-pong by round) and their hits
-    float4 *ray_o[2], *ray_d[2], *hits[2];
-    float4 *shadow_o, *shadow_d, *shadow_c;
-    // Ray queues hold camera paths' rays from the front and light paths' from the back
-    // (index pool - 1 - k), so that each kind shades in a launch of its own.
-    // counters[r]: camera paths' rays of round r; counters[rounds + 1 + r]: shadow rays of
-    // round r; counters[kLightCounters * rounds + 2 + r] (light_counter): light paths' rays.
-    uint32_t *counters;
-    unsigned long long *stats;  // closest rays, shadow rays, paths, passes, then traversal work
-    int *status;
-};
-
-// Where the light paths' ray counts start in a wave's counters.
-constexpr uint32_t kLightCounters = 2;
-__device__ __forceinline__ uint32_t *light_counter(const Wave &w, uint32_t round) {
-    return &w.counters[kLightCounters * w.rounds + 2 + round];
-}
-
-__device__ __forceinline__ uint32_t warp_push(uint32_t *counter, bool want) {
-    const unsigned mask = __ballot_sync(0xffffffffu, want);
-    if (mask == 0u) return 0u;
-    const int lane = threadIdx.x & 31;
-    const int leader = __ffs(mask) - 1;
-    uint32_t base = 0;
-    if (lane == leader) base = atomicAdd(counter, (uint32_t)__popc(mask));
-    base = __shfl_sync(0xffffffffu, base, leader);
-    return base + (uint32_t)__popc(mask & ((1u << lane) - 1u));
-}
-
-// The segment holding pool path `path` (segments lie end to end from path 0).
-__device__ __forceinline__ uint32_t segment_of(const Plan *plan, uint32_t path) {
-    uint32_t lo = 0, hi = plan->head.segments;
-    while (hi - lo > 1u) {
-        const uint32_t mid = (lo + hi) >> 1;
-        if (plan->seg[mid].path_base <= path) lo = mid;
-        else hi = mid;
-    }
-    return lo;
-}
-
-__device__ __forceinline__ const Member &member_of_tag(const Wave &w, uint32_t tag) {
-    return w.members[w.plan->seg[tag >> kPathBits].member];
-}
-
-// A light path's number among its sample's light paths.
-__device__ __forceinline__ uint32_t tag_light_index(const Wave &w, uint32_t tag) {
-    const Segment &sg = w.plan->seg[tag >> kPathBits];
-    return sg.first_pixel + ((tag & kPathMask) - sg.path_base);
-}
-
-// intersect_closest.comp:45-76: the nearest triangle, then the analytic lights
-// before it (camera rays skip lights invisible to the camera). The grid-stride walk
-// hands each warp 32 neighbouring queue entries at a time (neighbouring primary rays,
-// or rays a shading warp pushed together), which keeps its lanes on similar nodes.
-template <int W, int kStack, bool kCount>
-__global__ void __launch_bounds__(kTraceBlock) closest_kernel(Wave w, uint32_t round) {
-    __shared__ int stack[TracerOf<W, false, kStack, kCount>::kInts * kTraceBlock];
-    const uint32_t q = round & 1u;
-    const uint32_t cameras = w.counters[round], count = cameras + *light_counter(w, round);
-    bool overflow = false;
-    Visits visits;
-    const float4 *ray_o = w.ray_o[q], *ray_d = w.ray_d[q];
-    float4 *hits = w.hits[q];
-    typename TracerOf<W, false, kStack, kCount>::type tr(stack + threadIdx.x, kTraceBlock);
-    const uint32_t step = gridDim.x * blockDim.x;
-    for (uint32_t j = blockIdx.x * blockDim.x + threadIdx.x; j < count; j += step) {
-        // The camera paths' rays, then the light paths' from the queue's back.
-        const uint32_t i = j < cameras ? j : w.pool - 1u - (j - cameras);
-        const float4 o = ray_o[i], d = ray_d[i];
-        const uint32_t segment = __float_as_uint(o.w) >> kPathBits;
-        {
-            const DeviceScene s = w.members[w.plan->seg[segment].member].scene;
-            if (tr.start(s, Ray{xyz(o), 0.0f, xyz(d), d.w})) {
-                while (!tr.step(s, overflow, visits)) {
-                }
-            }
-        }
-        // The lights, read again past the traversal rather than held through it.
-        const Segment &sg = w.plan->seg[segment];
-        const Member &m = w.members[sg.member];
-        const bool flow = sg.kind == kLightSegment;  // light paths follow light
-        uint32_t what = tr.h.slot >= 0 ? (uint32_t)tr.h.slot : kNone;
-        float t = tr.h.t;
-        const float4 *lights = m.lights;
-        const uint32_t light_count = m.light_count;
-        for (uint32_t light = 0; light < light_count; light++) {
-            if (round == 0 && !light_visible(lights, light)) continue;
-            const float tl = intersect_light(lights, light, tr.r.o, tr.r.d, t, flow);
-            if (tl < t) {
-                t = tl;
-                what = kLightHit | light;
-            }
-        }
-        hits[i] = make_float4(t, __uint_as_float(what), tr.h.u, tr.h.v);
-    }
-    if (overflow) atomicAdd(&w.status[0], 1);
-    if (kCount) add_visits(&w.stats[4], visits);
-}
-
-// intersect_shadow.comp:28-92: unblocked light samples join their path's radiance; a light
-// path's camera connection, unless a light the camera sees stands in it, splats its value
-// (in the film's terms) on its pixel in the lane's accumulator.
-template <int W, int kStack, bool kCount, bool kCutouts>
-__global__ void __launch_bounds__(kTraceBlock) shadow_kernel(Wave w, uint32_t round) {
-    __shared__ int stack[TracerOf<W, true, kStack, kCount>::kInts * kTraceBlock];
-    const uint32_t count = w.counters[w.rounds + 1 + round];
-    bool overflow = false;
-    Visits visits;
-    typename TracerOf<W, true, kStack, kCount>::type tr(stack + threadIdx.x, kTraceBlock);
-    const uint32_t step = gridDim.x * blockDim.x;
-    for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < count; i += step) {
-        const float4 o = w.shadow_o[i], d = w.shadow_d[i];
-        const uint32_t tag = __float_as_uint(o.w);
-        const Segment &sg = w.plan->seg[tag >> kPathBits];
-        const Member &m = w.members[sg.member];
-        const bool light_path = sg.kind == kLightSegment;
-        if (light_path) {
-            bool seen = false;
-            for (uint32_t light = 0; light < m.light_count && !seen; light++)
-                seen = light_visible(m.lights, light) && intersect_light(m.lights, light, xyz(o), xyz(d), d.w, true) < d.w;
-            if (seen) continue;
-        }
-        const DeviceScene s = m.scene;
-        float kept = 1.0f;
-        if (kCutouts && m.cutouts) {
-            // intersect_shadow.comp:70-91: on through the cut-outs it meets, keeping
-            // (1 - opacity) of the light at each; anything opaque blocks. Closest hits,
-            // on the same stack (a variant of its own: passes without cut-outs keep the
-            // leaner kernel).
-            typename TracerOf<W, false, kStack, kCount>::type walk(stack + threadIdx.x, kTraceBlock);
-            float3 from = xyz(o);
-            float remaining = d.w;
-            bool through = false;
-            for (int hop = 0; hop < 16 && kept > 0.0f; hop++) {
-                if (walk.start(s, Ray{from, 0.0f, xyz(d), remaining})) {
-                    while (!walk.step(s, overflow, visits)) {
-                    }
-                }
-                if (walk.h.slot < 0) {
-                    through = true;
-                    break;
-                }
-                const uint32_t material = __ldg(&s.shading[walk.h.slot]).w;
-                kept *= 1.0f - fminf(fmaxf(__ldg(&m.materials[material * 16u + 12u]).x, 0.0f), 1.0f);
-                if (kept < 1e-4f) kept = 0.0f;
-                const float3 p = from + xyz(d) * walk.h.t;
-                const float margin = 1e-4f * fmaxf(1.0f, fmaxf(fabsf(p.x), fmaxf(fabsf(p.y), fabsf(p.z))));
-                from = p + xyz(d) * margin;
-                remaining -= walk.h.t + margin;
-                if (remaining <= 0.0f) {
-                    through = kept > 0.0f;
-                    break;
-                }
-            }
-            if (!through) continue;
-        } else {
-            if (tr.start(s, Ray{xyz(o), 0.0f, xyz(d), d.w})) {
-                while (!tr.step(s, overflow, visits)) {
-                }
-            }
-            if (tr.h.id >= 0) continue;
-        }
-        float4 c = w.shadow_c[i];
-        if (kCutouts && m.cutouts) c = make_float4(c.x * kept, c.y * kept, c.z * kept, light_path ? c.w : c.w * kept);
-        if (!light_path) {
-            const uint32_t path = tag & kPathMask;
-            w.radiance[path] = w.radiance[path] + c;
-        } else if (!w.plan->head.dry && isfinite(c.x) && isfinite(c.y) && isfinite(c.z)) {
-            unsigned long long *at = m.splat_lane[w.lane] + (size_t)__float_as_uint(c.w) * 3;
-            const float v[3] = {c.x, c.y, c.z};
-            for (int k = 0; k < 3; k++) {
-                const float clamped_v = fminf(fmaxf(v[k], -kSplatLimit), kSplatLimit);
-                atomicAdd(at + k, (unsigned long long)llrint((double)clamped_v * kSplatScale));
-            }
-        }
-    }
-    if (overflow) atomicAdd(&w.status[0], 1);
-    if (kCount) add_visits(&w.stats[6], visits);
-}
 
 template <bool kSpectral>
 __device__ __forceinline__ float4 clamped(float4 c, uint32_t total, float clamp_value) {
@@ -1954,8 +1674,6 @@ struct MemberHost {
     double emit_share = 0.0;
 };
 
-// The traversal variants a pass can take: (BVH width, stack entries).
-#define LR_TRAVERSALS(X) X(8, 32) X(8, 48) X(4, 32) X(4, 48) X(2, 32) X(2, 64) X(2, 96)
 
 // Scene-size classes the autotuner keeps a BVH width for: under 16k triangles, under
 // 128k, and larger.
@@ -2064,7 +1782,7 @@ void record_trace(const WaveHost *h, const Wave &w, int grid_trace, bool tracing
     camera_kernel<<<h->grid_shade, kShadeBlock, 0, stream>>>(w);
     mark(stream, marks, kCamera);
     for (uint32_t round = 0; round < w.rounds; round++) {
-        closest_kernel<W, kStack, kCount><<<grid_trace, kTraceBlock, 0, stream>>>(w, round);
+        launch_closest(W, kStack, kCount, grid_trace, stream, w, round);
         mark(stream, marks, kClosest);
         if (glossy) {
             if (tracing) {
@@ -2080,8 +1798,7 @@ void record_trace(const WaveHost *h, const Wave &w, int grid_trace, bool tracing
             shade_kernel<false, false, false><<<h->grid_shade, kShadeBlock, 0, stream>>>(w, round);
         }
         mark(stream, marks, kSurface);
-        if (cutouts) shadow_kernel<W, kStack, kCount, true><<<grid_trace, kTraceBlock, 0, stream>>>(w, round);
-        else shadow_kernel<W, kStack, kCount, false><<<grid_trace, kTraceBlock, 0, stream>>>(w, round);
+        launch_shadow(W, kStack, kCount, cutouts, grid_trace, stream, w, round);
         mark(stream, marks, kShadow);
     }
     LR_CUDA(cudaGetLastError());
@@ -2101,15 +1818,7 @@ void record_finish(const WaveHost *h, const Wave &w, cudaStream_t stream, Marks 
     LR_CUDA(cudaGetLastError());
 }
 
-int trace_grid(int variant, int sms) {
-    switch (variant) {
-#define LR_CASE(wd, k) \
-    case wd * 1000 + k: return grid_of(closest_kernel<wd, k, false>, kTraceBlock, sms);
-        LR_TRAVERSALS(LR_CASE)
-#undef LR_CASE
-        default: fail(LR_LIMIT, "no traversal variant for this scene");
-    }
-}
+int trace_grid(int variant, int sms) { return closest_grid(variant / 1000, variant % 1000, sms); }
 
 int grid_for(WaveHost *h, int variant) {
     auto it = h->grid_trace.find(variant);
@@ -2205,6 +1914,11 @@ void lanes_create(WaveHost *h) {
         const size_t p_shadow_c = L.add(nullptr, P * 16);
         const size_t p_counters = L.add(nullptr, (4 * (size_t)rounds + 2) * 4);
         const size_t p_plan = L.add(nullptr, sizeof(Plan));
+        // Ray records (settings.profile = 3): three float4 per queue entry and round, for
+        // the closest-hit and the shadow queue.
+        const bool recording = h->profile == kProfileRecord;
+        const size_t record_bytes = recording ? (size_t)rounds * P * 48 : 0;
+        const size_t p_rec_closest = L.add(nullptr, record_bytes), p_rec_shadow = L.add(nullptr, record_bytes);
         size_t total = 0;
         lane.block = L.allocate(ctx->stream, total);
         char *base = (char *)lane.block;
@@ -2232,6 +1946,8 @@ void lanes_create(WaveHost *h) {
         w.status = ctx->status;
         w.members = h->d_members;
         lane.d_plan = (Plan *)at(p_plan);
+        w.record_closest = recording ? (float4 *)at(p_rec_closest) : nullptr;
+        w.record_shadow = recording ? (float4 *)at(p_rec_shadow) : nullptr;
         w.plan = lane.d_plan;
         LR_CUDA(cudaMallocHost((void **)&lane.h_plan, sizeof(Plan)));
         if (li == 0) {
@@ -3099,6 +2815,34 @@ void wave_destroy(WaveHost *h) {
     if (h->block) cudaFree(h->block);
 }
 
+// The last pass's ray records of round `round` (settings.profile = kProfileRecord): the
+// camera paths' rays, then the light paths', of the closest-hit queue, or the shadow
+// queue; 12 floats a ray (origin + tag, direction + reach, the traversal's answer).
+uint64_t wave_records(WaveHost *h, uint32_t round, bool shadow, float *out, uint64_t capacity) {
+    if (h->profile != kProfileRecord) fail(LR_INVALID, "ray records need settings.profile = 3");
+    if (round >= h->rounds) fail(LR_INVALID, "no such round");
+    settle(h);
+    join_lanes(h);
+    const Lane &lane = h->lanes[0];
+    std::vector<uint32_t> counters(4 * (size_t)h->rounds + 2);
+    LR_CUDA(cudaMemcpyAsync(counters.data(), lane.w.counters, counters.size() * 4, cudaMemcpyDeviceToHost,
+                            h->ctx->stream));
+    LR_CUDA(cudaStreamSynchronize(h->ctx->stream));
+    const uint64_t front = shadow ? counters[h->rounds + 1 + round] : counters[round];
+    const uint64_t back = shadow ? 0 : counters[kLightCounters * h->rounds + 2 + round];
+    const uint64_t total = front + back;
+    if (!out) return total;
+    if (capacity < total * 12) fail(LR_LIMIT, "the output holds fewer rays than the round traced");
+    const float4 *rec = (shadow ? lane.w.record_shadow : lane.w.record_closest) + (size_t)round * h->pool * 3;
+    if (front) LR_CUDA(cudaMemcpyAsync(out, rec, front * 48, cudaMemcpyDeviceToHost, h->ctx->stream));
+    // Light paths' rays fill the queue from its back: entry pool - 1 - k holds ray k.
+    if (back)
+        LR_CUDA(cudaMemcpyAsync(out + front * 12, rec + (h->pool - back) * 3, back * 48, cudaMemcpyDeviceToHost,
+                                h->ctx->stream));
+    LR_CUDA(cudaStreamSynchronize(h->ctx->stream));
+    return total;
+}
+
 void wave_stats(WaveHost *h, lr_render_stats *out) {
     settle(h);
     unsigned long long s[8];
@@ -3572,6 +3316,14 @@ int lr_renderer_kernel_times(lr_renderer *r, double out[10]) {
     return guarded([&] {
         if (!r || !out) fail(LR_INVALID, "kernel times need ten numbers");
         wave_kernel_times(&r->wave, out);
+    });
+}
+
+int lr_renderer_recorded_rays(lr_renderer *r, uint32_t round, int32_t shadow, float *out, uint64_t capacity,
+                              uint64_t *count) {
+    return guarded([&] {
+        if (!r || !count) fail(LR_INVALID, "no renderer");
+        *count = wave_records(&r->wave, round, shadow != 0, out, capacity);
     });
 }
 

@@ -43,7 +43,7 @@ __device__ __forceinline__ float3 xyz(float4 a) { return make_float3(a.x, a.y, a
 // is the XOR of the direction numbers of the set bits of byte value v at byte position b,
 // so a 32-bit index costs four lookups (XOR is associative: the same value as the
 // bit-by-bit sum of sampler.glsl:32-37). Dimension 0 is van der Corput, a bit reversal.
-__device__ uint32_t g_sobol_bytes[3 * 4 * 256];
+static __device__ uint32_t g_sobol_bytes[3 * 4 * 256];
 
 __device__ __forceinline__ uint32_t hash_u32(uint32_t x) {
     x ^= x >> 16;
@@ -363,7 +363,7 @@ __device__ __noinline__ float4 dome_radiance(const float4 *lights, uint32_t ligh
 // dome_pdf (lights.glsl:120-129): the solid-angle pdf of sampling direction d (the
 // selection's chance not included): a texel's weight over the sum, spread over its solid
 // angle.
-__device__ __noinline__ float dome_pdf(const float4 *lights, uint32_t light, float3 d) {
+static __device__ __noinline__ float dome_pdf(const float4 *lights, uint32_t light, float3 d) {
     DomeImage image;
     if (!dome_image(lights, light, image)) return 1.0f / (4.0f * kPi);
     float sin_theta;
@@ -425,7 +425,7 @@ __device__ __forceinline__ float sphere_hit(float3 center, float radius, float3 
 
 // sample_dome (lights.glsl:152-174): a direction by the image's weights (rows, then the
 // chosen row's texels), or uniform over the sphere for a dome without an image.
-__device__ __noinline__ bool sample_dome(const float4 *lights, uint32_t light, float2 u, LightSample &s) {
+static __device__ __noinline__ bool sample_dome(const float4 *lights, uint32_t light, float2 u, LightSample &s) {
     s.distance = kInfinity;
     s.delta = false;
     s.cos_light = 1.0f;

@@ -1,0 +1,209 @@
+// The integrator's traversal kernels: intersect_closest.comp and intersect_shadow.comp of
+// the reference, over the wave's ray queues (wave.cuh).
+//
+// This translation unit is compiled at IEEE single precision -- denormals kept, division
+// and square root correctly rounded -- so the watertight triangle test here decides every
+// hit exactly as the ray queries of device.cu (lr_trace_rays, lr_probe) do, and as the FP32
+// brute force of the oracle does: an edge function that is a denormal stays a nonzero
+// number of its sign instead of turning "outside" into "on the edge". The shading kernels
+// (integrator.cu) take approximate division and flush denormals; nothing here depends on
+// them.
+#include "device.hpp"
+#include "shading.cuh"
+#include "traverse.cuh"
+#include "wave.cuh"
+
+namespace lr {
+namespace {
+
+// intersect_closest.comp:45-76: the nearest triangle, then the analytic lights
+// before it (camera rays skip lights invisible to the camera). The grid-stride walk
+// hands each warp 32 neighbouring queue entries at a time (neighbouring primary rays,
+// or rays a shading warp pushed together), which keeps its lanes on similar nodes.
+template <int W, int kStack, bool kCount>
+__global__ void __launch_bounds__(kTraceBlock) closest_kernel(Wave w, uint32_t round) {
+    __shared__ int stack[TracerOf<W, false, kStack, kCount>::kInts * kTraceBlock];
+    const uint32_t q = round & 1u;
+    const uint32_t cameras = w.counters[round], count = cameras + *light_counter(w, round);
+    bool overflow = false;
+    Visits visits;
+    const float4 *ray_o = w.ray_o[q], *ray_d = w.ray_d[q];
+    float4 *hits = w.hits[q];
+    typename TracerOf<W, false, kStack, kCount>::type tr(stack + threadIdx.x, kTraceBlock);
+    const uint32_t step = gridDim.x * blockDim.x;
+    for (uint32_t j = blockIdx.x * blockDim.x + threadIdx.x; j < count; j += step) {
+        // The camera paths' rays, then the light paths' from the queue's back.
+        const uint32_t i = j < cameras ? j : w.pool - 1u - (j - cameras);
+        const float4 o = ray_o[i], d = ray_d[i];
+        const uint32_t segment = __float_as_uint(o.w) >> kPathBits;
+        {
+            const DeviceScene s = w.members[w.plan->seg[segment].member].scene;
+            if (tr.start(s, Ray{xyz(o), 0.0f, xyz(d), d.w})) {
+                while (!tr.step(s, overflow, visits)) {
+                }
+            }
+        }
+        if (w.record_closest) {
+            float4 *rec = w.record_closest + ((size_t)round * w.pool + i) * 3u;
+            rec[0] = o;
+            rec[1] = d;
+            rec[2] = make_float4(tr.h.t, __int_as_float(tr.h.id), tr.h.u, tr.h.v);
+        }
+        // The lights, read again past the traversal rather than held through it.
+        const Segment &sg = w.plan->seg[segment];
+        const Member &m = w.members[sg.member];
+        const bool flow = sg.kind == kLightSegment;  // light paths follow light
+        uint32_t what = tr.h.slot >= 0 ? (uint32_t)tr.h.slot : kNone;
+        float t = tr.h.t;
+        const float4 *lights = m.lights;
+        const uint32_t light_count = m.light_count;
+        for (uint32_t light = 0; light < light_count; light++) {
+            if (round == 0 && !light_visible(lights, light)) continue;
+            const float tl = intersect_light(lights, light, tr.r.o, tr.r.d, t, flow);
+            if (tl < t) {
+                t = tl;
+                what = kLightHit | light;
+            }
+        }
+        hits[i] = make_float4(t, __uint_as_float(what), tr.h.u, tr.h.v);
+    }
+    if (overflow) atomicAdd(&w.status[0], 1);
+    if (kCount) add_visits(&w.stats[4], visits);
+}
+
+// intersect_shadow.comp:28-92: unblocked light samples join their path's radiance; a light
+// path's camera connection, unless a light the camera sees stands in it, splats its value
+// (in the film's terms) on its pixel in the lane's accumulator.
+template <int W, int kStack, bool kCount, bool kCutouts>
+__global__ void __launch_bounds__(kTraceBlock) shadow_kernel(Wave w, uint32_t round) {
+    __shared__ int stack[TracerOf<W, true, kStack, kCount>::kInts * kTraceBlock];
+    const uint32_t count = w.counters[w.rounds + 1 + round];
+    bool overflow = false;
+    Visits visits;
+    typename TracerOf<W, true, kStack, kCount>::type tr(stack + threadIdx.x, kTraceBlock);
+    const uint32_t step = gridDim.x * blockDim.x;
+    for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < count; i += step) {
+        const float4 o = w.shadow_o[i], d = w.shadow_d[i];
+        const uint32_t tag = __float_as_uint(o.w);
+        float4 *rec = w.record_shadow ? w.record_shadow + ((size_t)round * w.pool + i) * 3u : nullptr;
+        if (rec) {
+            // -1: not traced by the any-hit query (a light the camera sees stands in the
+            // connection, or the walk through cut-outs decides it).
+            rec[0] = o;
+            rec[1] = d;
+            rec[2] = make_float4(-1.0f, 0.0f, 0.0f, 0.0f);
+        }
+        const Segment &sg = w.plan->seg[tag >> kPathBits];
+        const Member &m = w.members[sg.member];
+        const bool light_path = sg.kind == kLightSegment;
+        if (light_path) {
+            bool seen = false;
+            for (uint32_t light = 0; light < m.light_count && !seen; light++)
+                seen = light_visible(m.lights, light) && intersect_light(m.lights, light, xyz(o), xyz(d), d.w, true) < d.w;
+            if (seen) continue;
+        }
+        const DeviceScene s = m.scene;
+        float kept = 1.0f;
+        if (kCutouts && m.cutouts) {
+            // intersect_shadow.comp:70-91: on through the cut-outs it meets, keeping
+            // (1 - opacity) of the light at each; anything opaque blocks. Closest hits,
+            // on the same stack (a variant of its own: passes without cut-outs keep the
+            // leaner kernel).
+            typename TracerOf<W, false, kStack, kCount>::type walk(stack + threadIdx.x, kTraceBlock);
+            float3 from = xyz(o);
+            float remaining = d.w;
+            bool through = false;
+            for (int hop = 0; hop < 16 && kept > 0.0f; hop++) {
+                if (walk.start(s, Ray{from, 0.0f, xyz(d), remaining})) {
+                    while (!walk.step(s, overflow, visits)) {
+                    }
+                }
+                if (walk.h.slot < 0) {
+                    through = true;
+                    break;
+                }
+                const uint32_t material = __ldg(&s.shading[walk.h.slot]).w;
+                kept *= 1.0f - fminf(fmaxf(__ldg(&m.materials[material * 16u + 12u]).x, 0.0f), 1.0f);
+                if (kept < 1e-4f) kept = 0.0f;
+                const float3 p = from + xyz(d) * walk.h.t;
+                const float margin = 1e-4f * fmaxf(1.0f, fmaxf(fabsf(p.x), fmaxf(fabsf(p.y), fabsf(p.z))));
+                from = p + xyz(d) * margin;
+                remaining -= walk.h.t + margin;
+                if (remaining <= 0.0f) {
+                    through = kept > 0.0f;
+                    break;
+                }
+            }
+            if (!through) continue;
+        } else {
+            if (tr.start(s, Ray{xyz(o), 0.0f, xyz(d), d.w})) {
+                while (!tr.step(s, overflow, visits)) {
+                }
+            }
+            if (rec) rec[2] = make_float4(tr.h.id >= 0 ? 1.0f : 0.0f, 0.0f, 0.0f, 0.0f);
+            if (tr.h.id >= 0) continue;
+        }
+        float4 c = w.shadow_c[i];
+        if (kCutouts && m.cutouts) c = make_float4(c.x * kept, c.y * kept, c.z * kept, light_path ? c.w : c.w * kept);
+        if (!light_path) {
+            const uint32_t path = tag & kPathMask;
+            w.radiance[path] = w.radiance[path] + c;
+        } else if (!w.plan->head.dry && isfinite(c.x) && isfinite(c.y) && isfinite(c.z)) {
+            unsigned long long *at = m.splat_lane[w.lane] + (size_t)__float_as_uint(c.w) * 3;
+            const float v[3] = {c.x, c.y, c.z};
+            for (int k = 0; k < 3; k++) {
+                const float clamped_v = fminf(fmaxf(v[k], -kSplatLimit), kSplatLimit);
+                atomicAdd(at + k, (unsigned long long)llrint((double)clamped_v * kSplatScale));
+            }
+        }
+    }
+    if (overflow) atomicAdd(&w.status[0], 1);
+    if (kCount) add_visits(&w.stats[6], visits);
+}
+
+}  // namespace
+
+void launch_closest(int width, int stack, bool count, int grid, cudaStream_t stream, const Wave &w, uint32_t round) {
+    switch (width * 1000 + stack) {
+#define LR_CASE(wd, k)                                                                           \
+    case wd * 1000 + k:                                                                          \
+        if (count) closest_kernel<wd, k, true><<<grid, kTraceBlock, 0, stream>>>(w, round);       \
+        else closest_kernel<wd, k, false><<<grid, kTraceBlock, 0, stream>>>(w, round);           \
+        return;
+        LR_TRAVERSALS(LR_CASE)
+#undef LR_CASE
+        default: fail(LR_LIMIT, "no traversal variant for this scene");
+    }
+}
+
+void launch_shadow(int width, int stack, bool count, bool cutouts, int grid, cudaStream_t stream, const Wave &w,
+                   uint32_t round) {
+    switch (width * 1000 + stack) {
+#define LR_CASE(wd, k)                                                                                  \
+    case wd * 1000 + k:                                                                                 \
+        if (count && cutouts) shadow_kernel<wd, k, true, true><<<grid, kTraceBlock, 0, stream>>>(w, round);    \
+        else if (count) shadow_kernel<wd, k, true, false><<<grid, kTraceBlock, 0, stream>>>(w, round);         \
+        else if (cutouts) shadow_kernel<wd, k, false, true><<<grid, kTraceBlock, 0, stream>>>(w, round);       \
+        else shadow_kernel<wd, k, false, false><<<grid, kTraceBlock, 0, stream>>>(w, round);                   \
+        return;
+        LR_TRAVERSALS(LR_CASE)
+#undef LR_CASE
+        default: fail(LR_LIMIT, "no traversal variant for this scene");
+    }
+}
+
+int closest_grid(int width, int stack, int sm_count) {
+    int per_sm = 0;
+    switch (width * 1000 + stack) {
+#define LR_CASE(wd, k)                                                                                       \
+    case wd * 1000 + k:                                                                                      \
+        LR_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, closest_kernel<wd, k, false>, kTraceBlock, 0)); \
+        break;
+        LR_TRAVERSALS(LR_CASE)
+#undef LR_CASE
+        default: fail(LR_LIMIT, "no traversal variant for this scene");
+    }
+    return (per_sm > 0 ? per_sm : 1) * sm_count;
+}
+
+}  // namespace lr
