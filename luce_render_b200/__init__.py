@@ -49,15 +49,50 @@ class RenderError(RuntimeError):
         self.message = message
 
 
-def _load() -> C.CDLL:
-    if not LIBRARY_PATH.exists():
-        raise ImportError(
-            f"{LIBRARY_PATH} is missing: build it with `python luce_render_b200/build.py` "
+def _missing() -> str:
+    return (f"{LIBRARY_PATH} is missing: build it with `python luce_render_b200/build.py` "
             "(nvcc for sm_100a). There is no CPU fallback.")
-    return C.CDLL(str(LIBRARY_PATH))
 
 
-lib = _load()
+if not LIBRARY_PATH.exists():
+    raise ImportError(_missing())
+
+
+class _Library:
+    """The C-ABI library, mapped into the process at the first call through it.
+
+    Describing a workload -- MeshData, camera(), light(), OpenPbr and the scene
+    generators of :mod:`luce_render_b200.scenes` -- calls nothing in it, so a process
+    that only builds inputs (the benchmark's CPU reference arm) never maps it. Every
+    compile, upload, trace and render goes through it; there is no CPU fallback: the
+    package refuses to import without the library, and a library that fails to load
+    raises at that first call."""
+
+    def __init__(self):
+        self._dll = None
+
+    def _open(self) -> C.CDLL:
+        if self._dll is None:
+            if not LIBRARY_PATH.exists():
+                raise ImportError(_missing())
+            dll = C.CDLL(str(LIBRARY_PATH))
+            for name, (res, args) in _SIGNATURES.items():
+                fn = getattr(dll, name, None)
+                if fn is not None:
+                    fn.restype = res
+                    fn.argtypes = args
+            self._dll = dll
+        return self._dll
+
+    def __getattr__(self, name: str):
+        if name.startswith("__"):
+            raise AttributeError(name)
+        fn = getattr(self._open(), name)
+        setattr(self, name, fn)  # later calls skip this lookup
+        return fn
+
+
+lib = _Library()
 
 
 # ---- structures (include/luce_render_b200.h) ------------------------------------------
@@ -98,9 +133,18 @@ class OpenPbr(C.Structure):
 
     @staticmethod
     def standard() -> "OpenPbr":
-        """OpenPbr.standard (materials.lucb:46-53)."""
+        """OpenPbr.standard (materials.lucb:46-53): the values lr_openpbr_standard sets,
+        filled here so that describing a material maps no library (a CPU test holds the
+        two equal)."""
         m = OpenPbr()
-        lib.lr_openpbr_standard(C.byref(m))
+        m.base_weight = 1.0
+        m.base_color[:] = [0.8, 0.8, 0.8]
+        for name in ("specular_color", "transmission_color", "coat_color", "emission_color"):
+            getattr(m, name)[:] = [1.0, 1.0, 1.0]
+        m.specular_weight, m.specular_roughness, m.specular_ior = 1.0, 0.3, 1.5
+        m.coat_ior, m.coat_darkening = 1.6, 1.0
+        m.geometry_opacity = 1.0
+        m.transmission_dispersion_abbe_number = 20.0
         return m
 
     @staticmethod
@@ -329,14 +373,6 @@ _SIGNATURES = {
     "lr_server_stats_get": (C.c_int, [_vp, C.POINTER(ServerStats)]),
     "lr_server_destroy": (None, [_vp]),
 }
-
-for _name, (_res, _args) in _SIGNATURES.items():
-    _fn = getattr(lib, _name, None)
-    if _fn is None:
-        continue
-    _fn.restype = _res
-    _fn.argtypes = _args
-
 
 def exported_symbols() -> list[str]:
     """The entry points this harness binds (every one the header declares)."""

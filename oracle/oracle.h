@@ -50,6 +50,33 @@ void or_reorder(const uint32_t *order, size_t count, uint32_t *indices, uint32_t
 /* The deepest leaf's depth (root = 0). */
 uint32_t or_bvh_depth(const or_node *nodes, size_t node_count);
 
+/* ---- Scene compile (src/render/scene.lucb) ---------------------------------- */
+
+/* A mesh as the boundary takes it: points, triangles, a polygon per triangle (NULL: its
+ * own), per-point or per-corner normals (NULL: the triangle's own), a material per
+ * polygon (library index + 1; NULL or unknown: 0) and a 12-double placement (columns x,
+ * y, z, translation; all zero: identity). */
+typedef struct {
+    const float *positions;
+    uint64_t point_count;
+    const uint32_t *indices;
+    uint64_t triangle_count;
+    const uint32_t *faces;
+    uint32_t face_count;
+    const float *normals;
+    int normals_per_corner;
+    const uint32_t *face_materials;
+    double transform[12];
+} or_mesh;
+
+/* compile_scene (scene.lucb:111-129, add_mesh 253-294, shading_normals 364-398) and
+ * build_bvh + reorder: world-space points (3 floats each), then indices (3), shading
+ * (3 octahedral normals + material) and polygons per triangle in leaf order, the BVH
+ * (2 * max(T, 1) nodes) and the leaf order. Returns 0, or -1 for a triangle naming a
+ * point or polygon its mesh lacks. */
+int or_compile_meshes(const or_mesh *meshes, size_t mesh_count, size_t library, float *positions, uint32_t *indices,
+                      uint32_t *shading, uint32_t *faces, or_node *nodes, uint32_t *order, size_t *node_count);
+
 /* ---- Traversal (shaders/bvh.glsl) ------------------------------------------- */
 
 typedef struct {

@@ -44,6 +44,18 @@ class OrFrame(C.Structure):
                 ("width", C.c_uint32), ("height", C.c_uint32), ("lens_radius", C.c_double),
                 ("focus_distance", C.c_double)]
 
+    def pack(self) -> np.ndarray:
+        """RayFrame.pack (camera.lucb:41-47): the 16 floats the kernels read."""
+        return frame_pack(self)
+
+
+class OrMesh(C.Structure):
+    _fields_ = [("positions", C.POINTER(C.c_float)), ("point_count", C.c_uint64),
+                ("indices", C.POINTER(C.c_uint32)), ("triangle_count", C.c_uint64),
+                ("faces", C.POINTER(C.c_uint32)), ("face_count", C.c_uint32),
+                ("normals", C.POINTER(C.c_float)), ("normals_per_corner", C.c_int),
+                ("face_materials", C.POINTER(C.c_uint32)), ("transform", C.c_double * 12)]
+
 
 class OrLight(C.Structure):
     _fields_ = [("matrix", C.c_double * 12), ("shape", C.c_int), ("color", C.c_double * 3),
@@ -79,6 +91,7 @@ def _p(a, ctype):
 
 _f, _u, _d = C.c_float, C.c_uint32, C.c_double
 lib.or_build_bvh.restype = C.c_size_t
+lib.or_compile_meshes.restype = C.c_int
 lib.or_bvh_depth.restype = C.c_uint32
 lib.or_hash_u32.restype = C.c_uint32
 lib.or_hash_combine.restype = C.c_uint32
@@ -114,6 +127,58 @@ def build_bvh(positions: np.ndarray, indices: np.ndarray):
     n = lib.or_build_bvh(_p(positions, _f), _p(indices, _u), C.c_size_t(T), nodes.ctypes.data_as(C.c_void_p),
                          _p(order, _u))
     return nodes[:n].copy(), order[:T].copy()
+
+
+def compile_meshes(meshes, library: int) -> dict:
+    """compile_scene (scene.lucb:111-129, 253-294, 364-398) with its BVH, over meshes with
+    the boundary's fields (positions, indices, faces, face_count, normals,
+    normals_per_corner, face_materials, transform; luce_render_b200.MeshData has them):
+    the arrays a compiled scene holds -- positions, then indices, shading, faces in leaf
+    order, nodes, order."""
+    keep = []
+
+    def arr(a, dtype, cols):
+        if a is None:
+            return None
+        a = np.ascontiguousarray(a, dtype).reshape(-1, cols) if cols else np.ascontiguousarray(a, dtype)
+        keep.append(a)
+        return a
+
+    descs = (OrMesh * max(1, len(meshes)))()
+    points = triangles = 0
+    for d, m in zip(descs, meshes):
+        pos, tri = arr(m.positions, np.float32, 3), arr(m.indices, np.uint32, 3)
+        d.positions, d.point_count = _p(pos, _f), len(pos)
+        d.indices, d.triangle_count = _p(tri, _u), len(tri)
+        faces = arr(m.faces, np.uint32, 0)
+        if faces is not None:
+            d.faces = _p(faces, _u)
+        d.face_count = int(m.face_count)
+        normals = arr(m.normals, np.float32, 3)
+        if normals is not None:
+            d.normals = _p(normals, _f)
+            d.normals_per_corner = 1 if m.normals_per_corner else 0
+        mats = arr(m.face_materials, np.uint32, 0)
+        if mats is not None:
+            d.face_materials = _p(mats, _u)
+        if m.transform is not None:
+            d.transform[:] = [float(v) for v in np.asarray(m.transform, np.float64).reshape(-1)]
+        points += len(pos)
+        triangles += len(tri)
+    positions = np.zeros((points, 3), np.float32)
+    indices = np.zeros((triangles, 3), np.uint32)
+    shading = np.zeros((triangles, 4), np.uint32)
+    faces = np.zeros(triangles, np.uint32)
+    nodes = np.zeros(2 * max(triangles, 1), NODE_DTYPE)
+    order = np.zeros(max(triangles, 1), np.uint32)
+    count = C.c_size_t()
+    status = lib.or_compile_meshes(descs, len(meshes), C.c_size_t(library), _p(positions, _f), _p(indices, _u),
+                                   _p(shading, _u), _p(faces, _u), nodes.ctypes.data_as(C.c_void_p), _p(order, _u),
+                                   C.byref(count))
+    if status != 0:
+        raise ValueError("a triangle names a point or polygon its mesh lacks")
+    return {"positions": positions, "indices": indices, "shading": shading, "faces": faces,
+            "nodes": nodes[: count.value].copy(), "order": order[:triangles].copy()}
 
 
 def bvh_depth(nodes: np.ndarray) -> int:

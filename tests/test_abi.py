@@ -90,3 +90,25 @@ def test_dome_image_checks():
     sc = lr.compile_scene([], lights=[dome])
     sky[:] = np.nan  # the caller's buffer may change or go once the compile returns
     assert sc.info.light_count == 1
+
+
+def test_standard_material_is_the_libraries():
+    # OpenPbr.standard fills materials.lucb:46-53's values in Python (describing a scene
+    # maps no library); lr_openpbr_standard is the ABI's own copy of them.
+    import ctypes as C
+    ours = lr.OpenPbr.standard()
+    theirs = lr.OpenPbr()
+    lr.lib.lr_openpbr_standard(C.byref(theirs))
+    assert bytes(ours) == bytes(theirs)
+
+
+def test_describing_a_workload_maps_no_library():
+    # The scene generators and descriptions run without the C library (the benchmark's
+    # CPU reference arm builds its workload this way and maps only the oracle).
+    import subprocess
+    import sys
+    code = ("import luce_render_b200 as lr; from luce_render_b200 import scenes; "
+            "scenes.incoherent_scene(spheres=2, tori=2); scenes.cornell_meshes(True); scenes.cornell_materials(); "
+            "assert lr.lib._dll is None; "
+            "assert 'libluce_render_b200' not in open('/proc/self/maps').read()")
+    subprocess.run([sys.executable, "-c", code], check=True, cwd=str(ROOT))

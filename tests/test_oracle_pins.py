@@ -248,3 +248,48 @@ def test_bvh_equals_oracle_build_node_for_node(which):
         assert np.array_equal(order, a["order"])
     finally:
         sc.close()
+
+
+def _compiled_equal(meshes, library, cams=(), lights=(), mats=()):
+    sc = lr.compile_scene(meshes, cams, lights, mats)
+    try:
+        a = sc.arrays()
+        o = orc.compile_meshes(meshes, library)
+        for key in ("positions", "indices", "shading", "faces", "order"):
+            assert np.array_equal(np.asarray(a[key]).reshape(-1).view(np.uint32),
+                                  np.asarray(o[key]).reshape(-1).view(np.uint32)), key
+        assert np.array_equal(a["nodes"].view(np.uint8), o["nodes"].view(np.uint8))
+    finally:
+        sc.close()
+
+
+@pytest.mark.parametrize("which", ["cornell", "icosphere", "million"])
+def test_scene_compile_equals_oracle_compile(which):
+    # csrc/scene.cpp (placement, polygons, octahedral normals, materials, BVH, leaf order)
+    # against the oracle's restatement of scene.lucb's compile_scene, bit for bit.
+    if which == "cornell":
+        mats = scenes.cornell_materials()
+        _compiled_equal(scenes.cornell_meshes(True), len(mats), [scenes.cornell_camera()], [scenes.cornell_light()],
+                        mats)
+    elif which == "icosphere":
+        _compiled_equal(scenes.furnace_meshes(5), 0)
+    else:
+        meshes, mats, lights, cam = scenes.incoherent_scene()
+        _compiled_equal(meshes, len(mats), [cam], lights, mats)
+
+
+def test_scene_compile_edge_cases_equal_oracle():
+    # Per-corner normals, polygons of two triangles, a mirroring placement (the normals'
+    # cofactors take the determinant's sign), a singular one, unknown materials (-> 0).
+    p, t, f = scenes.cube(2.0)
+    rng = np.random.default_rng(3)
+    corner_normals = rng.normal(size=(len(t) * 3, 3)).astype(np.float32)
+    mirror = lr.placement((1.0, 2.0, 3.0), (0.3, 0.2, 0.1), (-1.0, 2.0, 0.5))
+    flat = np.zeros(12)
+    flat[0], flat[4], flat[9] = 1.0, 1.0, 4.0  # z axis zero: singular
+    meshes = [lr.MeshData(p, t, faces=f, face_count=6, face_materials=[0, 1, 2, 3, 9, 1]),
+              lr.MeshData(p, t, normals=corner_normals, normals_per_corner=True, transform=mirror),
+              lr.MeshData(p, t, normals=p, faces=f, face_count=6, transform=flat),
+              lr.MeshData(p, t, transform=mirror)]
+    mats = [lr.OpenPbr.lambert(), lr.OpenPbr.lambert((0.2, 0.3, 0.4)), lr.OpenPbr.lambert((0.9, 0.1, 0.1))]
+    _compiled_equal(meshes, len(mats), mats=mats)
