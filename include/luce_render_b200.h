@@ -292,11 +292,20 @@ int lr_probe(lr_context *ctx, const lr_gpu_scene *scene, const lr_frame *frame, 
  * holds the GPU at its memory budget. Larger frames are refused with LR_LIMIT. The
  * first call on a device does set-up (looks up the array's address, which may load the
  * module), so make it before any stream capture. All calls on one device share the
- * array: calls that overlap in time, from any thread or context on that device, race;
- * each call waits for its result, so calls made one after another are safe. */
+ * array, and two calls whose kernels overlapped on the GPU would race on it; so a call
+ * holds a per-device lock of this library from its launch until its results are on the
+ * host (on a failure too), and calls from several threads or contexts of one process
+ * take turns. The array's address is kept for the process: do not use the library
+ * across a cudaDeviceReset. */
 #define LR_PROBE_STATIC_PIXELS 2097152u
 int lr_probe_static(lr_context *ctx, const lr_gpu_scene *scene, const lr_frame *frame,
                     uint32_t flags, uint32_t *faces, float *distances);
+/* (No counterpart in the reference: a diagnostic.) The context's device memory: out[0]
+ * free and out[1] total bytes (cudaMemGetInfo), out[2] the bytes the device's default
+ * stream-ordered pool has handed out now, out[3] the most it has handed out at once since
+ * the last reset; `reset_high` nonzero resets that high-water mark to the current use
+ * first. lr_probe, lr_trace_rays and batch members allocate from that pool. */
+int lr_context_memory(lr_context *ctx, int32_t reset_high, uint64_t out[4]);
 
 /* Ray queries, the ray-list form of the probe. A ray is 8 floats (origin xyz, tmin,
  * direction xyz, tmax; hits have tmin < t < tmax); a hit is 4 words (t, triangle id as
@@ -531,7 +540,11 @@ void lr_batch_destroy(lr_batch *batch);
  * on first use, kept resident, evicted least recently used when idle and room is
  * needed) and its film, and advances every live session in shared passes; and a probe
  * thread that runs probe queries on a high-priority stream (without device allocation
- * up to LR_PROBE_STATIC_PIXELS pixels). Submitting never waits. A session's image is,
+ * up to LR_PROBE_STATIC_PIXELS pixels: through lr_probe_static, whose one array a device
+ * shares with every other lr_probe_static call of the process -- other servers' probe
+ * threads included -- the calls taking turns on the library's per-device lock; its
+ * 16 MiB count against budget_bytes, and lr_server_create does its set-up before the
+ * threads start). Submitting never waits. A session's image is,
  * bit for bit, what an lr_renderer of the same scene and settings makes; a probe's
  * result is lr_probe's. Times are seconds on the host's steady clock since the server
  * started. */

@@ -338,6 +338,7 @@ _SIGNATURES = {
     "lr_batch_join": (C.c_int, [_vp]),
     "lr_renderer_kernel_times": (C.c_int, [_vp, C.POINTER(C.c_double)]),
     "lr_renderer_stats": (C.c_int, [_vp, C.POINTER(RenderStats)]),
+    "lr_context_memory": (C.c_int, [_vp, C.c_int32, C.POINTER(C.c_uint64)]),
     "lr_renderer_recorded_rays": (C.c_int, [_vp, _u32, C.c_int32, C.POINTER(C.c_float), _u64,
                                             C.POINTER(C.c_uint64)]),
     "lr_renderer_destroy": (None, [_vp]),
@@ -449,6 +450,14 @@ class Context:
 
     def memset(self, dst: int, value: int, nbytes: int) -> None:
         _check(lib.lr_memset_device(self.handle, dst, value, nbytes))
+
+    def memory(self, reset_high: bool = False) -> dict:
+        """The device's memory: free and total bytes, and the default stream-ordered
+        pool's bytes in use now and at most since the last reset (`reset_high` resets
+        that mark to the current use first)."""
+        out = (C.c_uint64 * 4)()
+        _check(lib.lr_context_memory(self.handle, 1 if reset_high else 0, out))
+        return {"free": out[0], "total": out[1], "pool_used": out[2], "pool_high": out[3]}
 
     def timer_start(self) -> None:
         _check(lib.lr_timer_start(self.handle))

@@ -597,22 +597,37 @@ namespace {
 constexpr int kScratchDevices = 64;
 std::mutex g_scratch_mutex;
 void *g_scratch_of[kScratchDevices] = {};
+// One lock a device, held by a call from its launch until its results are on the host:
+// calls from several host threads of this process take turns on the array.
+std::mutex g_scratch_in_use[kScratchDevices];
 
-// The address of g_probe_scratch on `device`, looked up once per device with that
-// device current (the first lookup may load the module there).
-void *probe_scratch(int device) {
+}  // namespace
+
+namespace lr {
+
+// The address of g_probe_scratch on `device`, looked up once per device with that device
+// current (the first lookup may load the module there). The address stays valid while
+// the process keeps the device's primary context: the library is not to be used across a
+// cudaDeviceReset.
+void *probe_static_setup(int device) {
     if (device < 0 || device >= kScratchDevices) fail(LR_LIMIT, "lr_probe_static serves devices 0 to 63");
     std::lock_guard<std::mutex> lock(g_scratch_mutex);
     if (!g_scratch_of[device]) {
+        int current = -1;
+        LR_CUDA(cudaGetDevice(&current));
+        if (current != device) LR_CUDA(cudaSetDevice(device));
         void *address = nullptr;
-        LR_CUDA(cudaGetSymbolAddress(&address, g_probe_scratch));
+        const cudaError_t looked = cudaGetSymbolAddress(&address, g_probe_scratch);
+        if (current != device && current >= 0) cudaSetDevice(current);
+        if (looked != cudaSuccess)
+            fail(LR_DEVICE, std::string("cudaGetSymbolAddress(g_probe_scratch): ") + cudaGetErrorString(looked));
         if (!address) fail(LR_DEVICE, "no address for the static probe scratch");
         g_scratch_of[device] = address;
     }
     return g_scratch_of[device];
 }
 
-}  // namespace
+}  // namespace lr
 
 extern "C" {
 
@@ -629,22 +644,55 @@ int lr_probe_static(lr_context *ctx, const lr_gpu_scene *gs, const lr_frame *fra
         ProbeFrame f;
         pack_frame(*frame, f.b);
         LR_CUDA(cudaSetDevice(ctx->device));
-        char *scratch = (char *)probe_scratch(ctx->device);
+        char *scratch = (char *)probe_static_setup(ctx->device);
+        std::lock_guard<std::mutex> turn(g_scratch_in_use[ctx->device]);
         // The kernel writes every pixel's face and distance, so nothing in the scratch has
         // to start at zero; the status words it may raise are the context's, kept at zero.
         uint32_t *d_faces = (uint32_t *)scratch;
         float *d_ts = (float *)(scratch + (size_t)LR_PROBE_STATIC_PIXELS * 4);
-        if (flags & LR_TRACE_REFERENCE)
-            dispatch_probe<true>(gs, f, count, d_faces, d_ts, ctx->status, ctx->stream);
-        else
-            dispatch_probe<false>(gs, f, count, d_faces, d_ts, ctx->status, ctx->stream);
-        LR_CUDA(cudaGetLastError());
-        LR_CUDA(cudaMemcpyAsync(faces, d_faces, count * 4, cudaMemcpyDeviceToHost, ctx->stream));
-        LR_CUDA(cudaMemcpyAsync(distances, d_ts, count * 4, cudaMemcpyDeviceToHost, ctx->stream));
-        LR_CUDA(cudaStreamSynchronize(ctx->stream));
+        try {
+            if (flags & LR_TRACE_REFERENCE)
+                dispatch_probe<true>(gs, f, count, d_faces, d_ts, ctx->status, ctx->stream);
+            else
+                dispatch_probe<false>(gs, f, count, d_faces, d_ts, ctx->status, ctx->stream);
+            LR_CUDA(cudaGetLastError());
+            LR_CUDA(cudaMemcpyAsync(faces, d_faces, count * 4, cudaMemcpyDeviceToHost, ctx->stream));
+            LR_CUDA(cudaMemcpyAsync(distances, d_ts, count * 4, cudaMemcpyDeviceToHost, ctx->stream));
+            LR_CUDA(cudaStreamSynchronize(ctx->stream));
+        } catch (...) {
+            // Whatever was queued finishes before the array is handed to the next call.
+            cudaStreamSynchronize(ctx->stream);
+            throw;
+        }
         check_status(ctx);
     });
 }
+
+int lr_context_memory(lr_context *ctx, int32_t reset_high, uint64_t out[4]) {
+    return guarded([&] {
+        if (!ctx || !out) fail(LR_INVALID, "memory figures need a context and four words");
+        LR_CUDA(cudaSetDevice(ctx->device));
+        size_t free_bytes = 0, total_bytes = 0;
+        LR_CUDA(cudaMemGetInfo(&free_bytes, &total_bytes));
+        cudaMemPool_t pool;
+        LR_CUDA(cudaDeviceGetDefaultMemPool(&pool, ctx->device));
+        if (reset_high) {
+            unsigned long long zero = 0;
+            LR_CUDA(cudaMemPoolSetAttribute(pool, cudaMemPoolAttrUsedMemHigh, &zero));
+        }
+        unsigned long long used = 0, high = 0;
+        LR_CUDA(cudaMemPoolGetAttribute(pool, cudaMemPoolAttrUsedMemCurrent, &used));
+        LR_CUDA(cudaMemPoolGetAttribute(pool, cudaMemPoolAttrUsedMemHigh, &high));
+        out[0] = free_bytes;
+        out[1] = total_bytes;
+        out[2] = used;
+        out[3] = high;
+    });
+}
+
+}  // extern "C"
+
+extern "C" {
 
 static void trace_device(lr_context *ctx, const lr_gpu_scene *gs, const void *rays, uint64_t n, void *hits,
                          uint32_t flags) {

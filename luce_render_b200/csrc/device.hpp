@@ -70,6 +70,9 @@ struct lr_context {
 namespace lr {
 // Reads and clears the context's status words; fails when one is set.
 void check_status(lr_context *ctx);
+// lr_probe_static's set-up on `device` (the device address of its static array, looked up
+// once per device, which may load the module there); returns the address.
+void *probe_static_setup(int device);
 }  // namespace lr
 
 struct lr_gpu_scene {

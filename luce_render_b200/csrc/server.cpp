@@ -24,6 +24,7 @@
 #include <vector>
 
 #include "common.hpp"
+#include "device.hpp"
 
 namespace {
 
@@ -383,8 +384,13 @@ int lr_server_create(const lr_server_settings *settings, lr_server **out) {
             bs.max_bounces = settings->max_bounces;
             bs.capacity = settings->capacity;
             check(lr_batch_create(s->ctx, &bs, &s->batch));
-            // The wave's own memory: 15 float4 arrays of pool entries, and small parts.
-            s->wave_bytes = (uint64_t)std::min<uint32_t>(settings->pool, 1u << 23) * 16 * 15 + (1u << 20);
+            // The wave's own memory: 15 float4 arrays of pool entries, and small parts; and
+            // the static probe array (lr_probe_static), which the device holds from the
+            // module's load on. Its set-up runs here, before the threads start, so a first
+            // probe does not load the module after the scenes have filled the budget.
+            lr::probe_static_setup(settings->device);
+            s->wave_bytes = (uint64_t)std::min<uint32_t>(settings->pool, 1u << 23) * 16 * 15 + (1u << 20) +
+                            (uint64_t)LR_PROBE_STATIC_PIXELS * 8;
             if (s->wave_bytes >= settings->budget_bytes) fail(LR_LIMIT, "the pool alone exceeds the memory budget");
         } catch (...) {
             if (s->batch) lr_batch_destroy(s->batch);

@@ -74,3 +74,28 @@ def test_static_probe_refuses_frames_beyond_its_scratch(ctx):
     finally:
         gs.destroy()
         sc.close()
+
+
+def test_static_probe_allocates_nothing(ctx):
+    # What the entry point exists for: after its first call on the device (its set-up,
+    # which may load the module and so reserve the static array), calls take nothing from
+    # the device -- its free bytes stay the same and the stream-ordered pool hands out
+    # nothing -- while lr_probe, on the same frame, does draw its 16 MiB of scratch from
+    # that pool (the measurement sees an allocation when there is one).
+    sc = lr.compile_scene(scenes.cornell_meshes())
+    gs = lr.GpuScene.upload(ctx, sc)
+    try:
+        frame = scenes.cornell_frame(2048, 1024)
+        first = lr.probe_static(ctx, gs, frame)
+        before = ctx.memory(reset_high=True)
+        for _ in range(3):
+            assert _same(lr.probe_static(ctx, gs, frame), first)
+        after = ctx.memory()
+        assert after["free"] == before["free"], (before, after)
+        assert after["pool_used"] == before["pool_used"] and after["pool_high"] <= before["pool_used"], (before, after)
+        lr.probe(ctx, gs, frame)
+        control = ctx.memory()
+        assert control["pool_high"] >= before["pool_used"] + 2048 * 1024 * 8, (before, control)
+    finally:
+        gs.destroy()
+        sc.close()
