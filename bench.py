@@ -306,14 +306,14 @@ def served(lr, scenes, dist, seconds: float):
     """The served workload: a Poisson stream (200 requests/s, seed 0x5E4E) of 80% render
     sessions (a scene of the batched workload at its film size, spp uniform in 16..256,
     depth 6) and 20% probes (1k to 2M pixel rays, log-uniform, through the scene's
-    camera) into one Server (150 GB budget, 128 live sessions, pool 2^22). Latency is
+    camera) into one Server (150 GB budget, 256 live sessions, pool 2^23). Latency is
     the server's own host clock from submission: probes to their result in pinned host
     memory, sessions to their first image and to completion."""
     import numpy as np
 
     cases = batch_cases(lr, scenes)
     arrivals = arrival_stream(seconds, len(cases))
-    server = lr.Server(lr.ServerSettings.default(budget_bytes=150 * 10**9, capacity=128, pool=1 << 22,
+    server = lr.Server(lr.ServerSettings.default(budget_bytes=150 * 10**9, capacity=256, pool=1 << 23,
                                                  max_bounces=BATCH_BOUNCES))
     ids = [server.add_scene(sc) for sc, _ in cases]
     for sid in ids:  # the catalog starts resident, as a running service keeps it
@@ -370,7 +370,7 @@ def served(lr, scenes, dist, seconds: float):
     return {
         "workload": ("Poisson arrivals at 200 requests/s (seed 0x5E4E): 80% render sessions of the batched "
                      "workload's scenes at their film sizes, 16..256 spp, depth 6; 20% probes of 1k..2M pixel rays "
-                     "(log-uniform); budget 150 GB, 128 live sessions, pool 2^22, LRU eviction of idle scenes"),
+                     "(log-uniform); budget 150 GB, 256 live sessions, pool 2^23, LRU eviction of idle scenes"),
         "seconds": window, "requests": len(submitted),
         "probe_latency": percentiles(done_probes),
         "slowest_probes": [{"pixels": i["pixels"], "submitted_s": i["submitted"],
@@ -600,6 +600,42 @@ def device_build(lr, scenes, ctx, dist, sc, meshes, cam, lights, mats, repeats: 
                       "median of 5; compiles: wall clock"}
 
 
+def overhead(lr, scenes, ctx, dist) -> dict:
+    """Launch overhead (the analogue of the reference's tests/gpu/overhead.lucb:9-39):
+    chains of 10, 100 and 400 dependent empty launches, one by one and as one CUDA graph,
+    microseconds a launch on the device and on the host's clock; and the fixed cost of a
+    pass -- a renderer of an 8 x 8 film of the Cornell box at depth 6, whose passes hold
+    64 paths, so nearly all of a pass's time is its launches and their tails -- in ms a
+    pass, device-timed over 200 passes after 20."""
+    chains = {}
+    for count in (10, 100, 400):
+        for graph in (False, True):
+            device_us, host_us = ctx.launch_overhead(count, graph)
+            chains[f"{count}_{'graph' if graph else 'stream'}"] = {"device_us": device_us, "host_us": host_us}
+    sc = lr.compile_scene(scenes.cornell_meshes(True), [scenes.cornell_camera()], [scenes.cornell_light()],
+                          scenes.cornell_materials())
+    s = lr.RenderSettings.of(8, 8, 220)
+    s.max_bounces = BOUNCES
+    s.light_tracing = 0.0
+    r = lr.Renderer.create(ctx, sc, s)
+    for _ in range(20):
+        r.advance_one()
+    r.wait()
+    dist.barrier()
+    ctx.synchronize()
+    ctx.timer_start()
+    for _ in range(200):
+        r.advance_one()
+    r.join()
+    ms = dist.max(ctx.timer_stop())
+    r.destroy()
+    sc.close()
+    return {"launch_chains": chains, "empty_pass_ms": ms / 200.0,
+            "kernels_per_pass": 1 + 3 * (BOUNCES + 1) + 5,
+            "timing": "chains: best of 5, CUDA events and the host clock; passes: CUDA events on the context "
+                      "stream over 200 passes of 64 paths (two lanes, graphs)"}
+
+
 def cpu_intersection(arrays, scenes, oracle, cores: int) -> dict:
     """The reference's CPU intersection on the 1M-triangle scene, on all host cores: its
     f64 brute force (tests/gpu/main.lucb:82-119, every ray against every triangle) on a
@@ -783,6 +819,7 @@ def main():
     batch_info = None if args.skip_batched else batched(lr, scenes, ctx, dist)
     served_info = None if args.skip_served else served(lr, scenes, dist, args.served_seconds)
     refit_info = None if args.skip_refit else refit(lr, scenes, ctx, dist)
+    overhead_info = overhead(lr, scenes, ctx, dist)
 
     cpu = None
     if dist.rank == 0 and dist.world == 1:
@@ -820,6 +857,7 @@ def main():
             "batched": batch_info,
             "served": served_info,
             "refit": refit_info,
+            "overhead": overhead_info,
         }
         print(json.dumps(line))
     ctx.close()

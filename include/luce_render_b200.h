@@ -300,6 +300,12 @@ int lr_probe(lr_context *ctx, const lr_gpu_scene *scene, const lr_frame *frame, 
 #define LR_PROBE_STATIC_PIXELS 2097152u
 int lr_probe_static(lr_context *ctx, const lr_gpu_scene *scene, const lr_frame *frame,
                     uint32_t flags, uint32_t *faces, float *distances);
+/* (A diagnostic; the analogue of the reference's tests/gpu/overhead.lucb:9-39, which
+ * times chains of dependent empty dispatches.) `count` dependent launches of an empty
+ * kernel on the context's stream -- one after another, or with `graph` nonzero as one
+ * captured CUDA graph -- best of five: out[0] microseconds a launch on the device (CUDA
+ * events), out[1] microseconds a launch on the host's clock (launch calls and wait). */
+int lr_launch_overhead(lr_context *ctx, uint32_t count, int32_t graph, double out[2]);
 /* (No counterpart in the reference: a diagnostic.) The context's device memory: out[0]
  * free and out[1] total bytes (cudaMemGetInfo), out[2] the bytes the device's default
  * stream-ordered pool has handed out now, out[3] the most it has handed out at once since
@@ -515,17 +521,24 @@ int lr_batch_read_wait(lr_batch *batch);
 /* The autotuner: times trial passes (which trace but change no film and move no member
  * on) on the members as they stand. For each scene-size class present (under 16k
  * triangles, under 128k, larger) it keeps the BVH width (2, 4, 8; a width all of the
- * class's members fall back from is skipped) whose passes of that class alone run
- * fastest; a pass then takes the width of the class holding most of its paths. Then it
- * keeps the fastest pool fill (a quarter, half or all of the pool) for the mixed passes.
+ * class's members fall back from is skipped), the traversal stack depth (each depth the
+ * width's kernels offer that holds the members' bound) and the traversal kernels' block
+ * size (64, 128, 256 threads) whose passes of that class alone run fastest; a pass then
+ * takes the choices of the class holding most of its paths. Then it keeps the fastest
+ * pool fill (a quarter, half or all of the pool) for the mixed passes, and the fastest
+ * interval at which the shade kernels group outgoing rays by direction octant (never,
+ * every round, every second round; the queues are compacted every round regardless).
  * Images do not change, only speed. */
 typedef struct {
     uint32_t width;            /* the widest BVH width chosen for any class */
     uint32_t fill;             /* paths a pass */
-    double paths_per_ms;       /* the chosen fill's measured rate */
+    double paths_per_ms;       /* the chosen candidate's measured rate */
     uint32_t candidates;       /* candidates timed */
     uint32_t class_width[3];   /* the width chosen per size class (0: class absent) */
     uint32_t class_members[3]; /* members with samples to come, per size class */
+    uint32_t class_stack[3];   /* traversal stack entries chosen per size class */
+    uint32_t class_block[3];   /* traversal kernels' threads a block chosen per size class */
+    uint32_t bin_interval;     /* rounds between sorts of outgoing rays by octant (0: none) */
 } lr_batch_tuning;
 int lr_batch_tune(lr_batch *batch, lr_batch_tuning *out);
 int lr_batch_passes(const lr_batch *batch, uint64_t *recorded, uint64_t *finished);

@@ -238,7 +238,8 @@ class BatchTuning(C.Structure):
     """lr_batch_tuning: the BVH width and paths a pass the autotuner chose, the chosen
     candidate's measured rate and how many candidates it timed."""
     _fields_ = [("width", C.c_uint32), ("fill", C.c_uint32), ("paths_per_ms", C.c_double),
-                ("candidates", C.c_uint32), ("class_width", C.c_uint32 * 3), ("class_members", C.c_uint32 * 3)]
+                ("candidates", C.c_uint32), ("class_width", C.c_uint32 * 3), ("class_members", C.c_uint32 * 3),
+                ("class_stack", C.c_uint32 * 3), ("class_block", C.c_uint32 * 3), ("bin_interval", C.c_uint32)]
 
 
 class ServerSettings(C.Structure):
@@ -339,6 +340,7 @@ _SIGNATURES = {
     "lr_renderer_kernel_times": (C.c_int, [_vp, C.POINTER(C.c_double)]),
     "lr_renderer_stats": (C.c_int, [_vp, C.POINTER(RenderStats)]),
     "lr_context_memory": (C.c_int, [_vp, C.c_int32, C.POINTER(C.c_uint64)]),
+    "lr_launch_overhead": (C.c_int, [_vp, _u32, C.c_int32, C.POINTER(C.c_double)]),
     "lr_renderer_recorded_rays": (C.c_int, [_vp, _u32, C.c_int32, C.POINTER(C.c_float), _u64,
                                             C.POINTER(C.c_uint64)]),
     "lr_renderer_destroy": (None, [_vp]),
@@ -458,6 +460,13 @@ class Context:
         out = (C.c_uint64 * 4)()
         _check(lib.lr_context_memory(self.handle, 1 if reset_high else 0, out))
         return {"free": out[0], "total": out[1], "pool_used": out[2], "pool_high": out[3]}
+
+    def launch_overhead(self, count: int, graph: bool) -> tuple[float, float]:
+        """Microseconds a launch of `count` dependent empty launches costs (direct, or
+        one CUDA graph): on the device, and on the host's clock."""
+        out = (C.c_double * 2)()
+        _check(lib.lr_launch_overhead(self.handle, count, 1 if graph else 0, out))
+        return out[0], out[1]
 
     def timer_start(self) -> None:
         _check(lib.lr_timer_start(self.handle))
@@ -1046,13 +1055,15 @@ class Batch:
         _check(lib.lr_batch_set_samples(self.handle, member, samples))
 
     def tune(self) -> dict:
-        """Autotune BVH width and paths a pass on the members as they stand (images do not
-        change)."""
+        """Autotune, per scene-size class, BVH width, traversal stack depth and threads a
+        block, then paths a pass and the interval of octant sorts of outgoing rays, on the
+        members as they stand (images do not change)."""
         t = BatchTuning()
         _check(lib.lr_batch_tune(self.handle, C.byref(t)))
         return {"width": int(t.width), "fill": int(t.fill), "paths_per_ms": float(t.paths_per_ms),
                 "candidates": int(t.candidates), "class_width": list(t.class_width),
-                "class_members": list(t.class_members)}
+                "class_members": list(t.class_members), "class_stack": list(t.class_stack),
+                "class_block": list(t.class_block), "bin_interval": int(t.bin_interval)}
 
     def passes(self):
         rec, fin = C.c_uint64(), C.c_uint64()

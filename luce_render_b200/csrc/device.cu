@@ -1,6 +1,7 @@
 // The context, the scene in HBM (GpuScene.upload, src/render/device.lucb:41-89), the
 // primary-ray probe (device.lucb:138-160, shaders/probe.comp) and ray-list queries.
 #include <algorithm>
+#include <chrono>
 #include <cmath>
 #include <cstring>
 #include <memory>
@@ -100,6 +101,11 @@ __global__ void __launch_bounds__(kBlock) trace_resident_kernel(DeviceScene s, c
     trace_strided<W, kAny, kStack, kCount>(s, n, stack + threadIdx.x, kBlock, load, store, overflow, visits);
     note_overflow(status, overflow);
     if (kCount) add_visits(counts, visits);
+}
+
+// Does nothing (the sink is never written): launch-overhead measurements.
+__global__ void idle_kernel(int *sink) {
+    if (sink && threadIdx.x == 1023u) *sink = 0;
 }
 
 int stack_for(uint32_t depth) {
@@ -433,6 +439,51 @@ int lr_timer_stop(lr_context *ctx, float *ms) {
         LR_CUDA(cudaEventRecord(ctx->stop, ctx->stream));
         LR_CUDA(cudaEventSynchronize(ctx->stop));
         LR_CUDA(cudaEventElapsedTime(ms, ctx->start, ctx->stop));
+    });
+}
+
+int lr_launch_overhead(lr_context *ctx, uint32_t count, int32_t graph, double out[2]) {
+    return guarded([&] {
+        if (!ctx || !out || count == 0 || count > 100000) fail(LR_INVALID, "1 to 100000 launches, two results");
+        LR_CUDA(cudaSetDevice(ctx->device));
+        cudaGraph_t g = nullptr;
+        cudaGraphExec_t exec = nullptr;
+        auto chain = [&](cudaStream_t s) {
+            for (uint32_t i = 0; i < count; i++) idle_kernel<<<1, 32, 0, s>>>(nullptr);
+        };
+        if (graph) {
+            cudaStream_t s;
+            LR_CUDA(cudaStreamCreateWithFlags(&s, cudaStreamNonBlocking));
+            LR_CUDA(cudaStreamBeginCapture(s, cudaStreamCaptureModeThreadLocal));
+            chain(s);
+            LR_CUDA(cudaStreamEndCapture(s, &g));
+            LR_CUDA(cudaStreamDestroy(s));
+            LR_CUDA(cudaGraphInstantiate(&exec, g, 0));
+        }
+        auto run = [&] {
+            if (graph) LR_CUDA(cudaGraphLaunch(exec, ctx->stream));
+            else chain(ctx->stream);
+        };
+        run();  // warm: module load, first launch
+        LR_CUDA(cudaStreamSynchronize(ctx->stream));
+        double best_device = 1e30, best_host = 1e30;
+        for (int round = 0; round < 5; round++) {
+            const auto t0 = std::chrono::steady_clock::now();
+            LR_CUDA(cudaEventRecord(ctx->start, ctx->stream));
+            run();
+            LR_CUDA(cudaEventRecord(ctx->stop, ctx->stream));
+            LR_CUDA(cudaEventSynchronize(ctx->stop));
+            const double host = std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t0).count();
+            float ms = 0.0f;
+            LR_CUDA(cudaEventElapsedTime(&ms, ctx->start, ctx->stop));
+            best_device = std::min(best_device, (double)ms);
+            best_host = std::min(best_host, host);
+        }
+        if (exec) cudaGraphExecDestroy(exec);
+        if (g) cudaGraphDestroy(g);
+        LR_CUDA(cudaGetLastError());
+        out[0] = best_device * 1e3 / count;
+        out[1] = best_host * 1e3 / count;
     });
 }
 

@@ -36,7 +36,7 @@
 #include "loading.hpp"
 #include <cuda_fp16.h>
 
-#include "openpbr.cuh"
+#include "paths.cuh"
 #include "shading.cuh"
 #include "traverse.cuh"
 #include "wave.cuh"
@@ -44,394 +44,9 @@
 namespace lr {
 namespace {
 
-// Cut-out opacity (shade_surface.comp:95-104): whether the ray passes through material
-// `material` at this hit, at random with probability 1 - opacity; the hit distance
-// decorrelates stacked layers. `u` is the path's opacity number for the bounce.
-__device__ __forceinline__ bool passes_through(const float4 *materials, uint32_t material, float t, float u) {
-    const float opacity = fminf(fmaxf(__ldg(&materials[material * 16u + 12u]).x, 0.0f), 1.0f);
-    if (!(opacity < 1.0f)) return false;
-    const float v = u + (float)hash_u32(__float_as_uint(t)) * (1.0f / 4294967296.0f);
-    return v - floorf(v) >= opacity;
-}
-
-
-
-template <bool kSpectral>
-__device__ __forceinline__ float4 clamped(float4 c, uint32_t total, float clamp_value) {
-    if (total == 0u || clamp_value <= 0.0f) return c;
-    const float largest = spec_max<kSpectral>(c);
-    return largest > clamp_value ? c * (clamp_value / largest) : c;
-}
-
-__device__ __forceinline__ float4 material_at(const Member &m, uint32_t material, uint32_t row) {
-    return __ldg(&m.materials[material * kMaterialStride + row]);
-}
-
-__device__ __forceinline__ float3 position_of(const Member &m, uint32_t index) {
-    return make_float3(__ldg(&m.scene.positions[index * 3]), __ldg(&m.scene.positions[index * 3 + 1]),
-                       __ldg(&m.scene.positions[index * 3 + 2]));
-}
-
-// triangle_hit_pdf (lighttree.glsl:131-137)
-__device__ __forceinline__ float triangle_hit_pdf(const Member &m, uint32_t slot, float3 d, float t) {
-    const float3 a = position_of(m, m.scene.indices[slot * 3]);
-    const float3 cr = cross(position_of(m, m.scene.indices[slot * 3 + 1]) - a, position_of(m, m.scene.indices[slot * 3 + 2]) - a);
-    const float area = 0.5f * length(cr);
-    const float cos_light = fabsf(dot(d, cr)) / fmaxf(1e-20f, 2.0f * area);
-    return t * t / fmaxf(1e-20f, cos_light * area);
-}
-
-// sample_triangle (lighttree.glsl:107-128)
-template <bool kSpectral>
-__device__ __forceinline__ bool sample_triangle(const Member &m, uint32_t slot, float3 p, float2 u, float4 lambda,
-                                                LightSample &s, float4 &radiance) {
-    const float3 a = position_of(m, m.scene.indices[slot * 3]);
-    const float3 b = position_of(m, m.scene.indices[slot * 3 + 1]);
-    const float3 c = position_of(m, m.scene.indices[slot * 3 + 2]);
-    const float r = sqrtf(u.x);
-    const float3 q = a * (1.0f - r) + b * (r * (1.0f - u.y)) + c * (r * u.y);
-    const float3 cr = cross(b - a, c - a);
-    const float area = 0.5f * length(cr);
-    const float3 d = q - p;
-    const float d2 = dot(d, d);
-    if (area <= 0.0f || d2 <= 0.0f) return false;
-    s.distance = sqrtf(d2);
-    s.direction = d * (1.0f / s.distance);
-    const float cos_light = fabsf(dot(s.direction, cr)) / (2.0f * area);
-    if (cos_light <= 0.0f) return false;
-    s.pdf = d2 / (cos_light * area);
-    s.cos_light = cos_light;
-    s.delta = false;
-    const uint32_t material = __ldg(&m.scene.shading[slot]).w;
-    radiance = spec_of<kSpectral>(material_at(m, material, 6), xyz(material_at(m, material, 7)), lambda);
-    return true;
-}
-
-// ---- Light tracing (shaders/connect.glsl, common.glsl:112-140) ---------------------------
-
-// camera_pdf (common.glsl:132-135): the camera's density of a ray along d, per unit of a
-// pixel's area on the image plane at unit distance.
-__device__ __forceinline__ float camera_pdf(const Member &m, float3 d) {
-    const float c = dot(d, make_float3(m.forward[0], m.forward[1], m.forward[2]));
-    return c > 0.0f ? m.pixel_area_inv / (c * c * c) : 0.0f;
-}
-
-// lens_point (common.glsl:125-130).
-__device__ __forceinline__ float3 lens_point(const Member &m, float2 u) {
-    const float3 position = make_float3(m.frame[0], m.frame[1], m.frame[2]);
-    if (m.lens_radius <= 0.0f) return position;
-    const float2 disk = concentric(u) * m.lens_radius;
-    return position + normalize(make_float3(m.frame[8], m.frame[9], m.frame[10])) * disk.x +
-           normalize(make_float3(m.frame[12], m.frame[13], m.frame[14])) * disk.y;
-}
-
-// camera_pixel (connect.glsl:30-45): the pixel the camera sees p through from `lens`, and
-// the unit direction and distance from there to p; false behind the camera or off image.
-__device__ __forceinline__ bool camera_pixel(const Member &m, float3 p, float3 lens, uint32_t &pixel, float3 &d,
-                                             float &distance) {
-    const float3 offset = p - lens;
-    distance = length(offset);
-    d = offset * (1.0f / fmaxf(distance, 1e-20f));
-    const float c = dot(d, make_float3(m.forward[0], m.forward[1], m.forward[2]));
-    if (c <= 1e-6f || distance <= 0.0f) return false;
-    const float3 position = make_float3(m.frame[0], m.frame[1], m.frame[2]);
-    const float3 corner = make_float3(m.frame[4], m.frame[5], m.frame[6]);
-    const float3 du = make_float3(m.frame[8], m.frame[9], m.frame[10]);
-    const float3 dv = make_float3(m.frame[12], m.frame[13], m.frame[14]);
-    const float focus = m.focus_distance;
-    const float3 film = (m.lens_radius > 0.0f ? (lens + d * (focus / c) - position) / focus : d / c) - corner;
-    const float x = dot(film, du) / dot(du, du), y = dot(film, dv) / dot(dv, dv);
-    if (!(x >= 0.0f && y >= 0.0f && x < (float)m.width && y < (float)m.height)) return false;
-    pixel = (uint32_t)y * m.width + (uint32_t)x;
-    return true;
-}
-
-__device__ __forceinline__ float node_energy(const TreeView &t, uint32_t node) {
-    return fmaxf(__ldg(&t.nodes[node * 3]).w, 0.0f);
-}
-
-// emitter_power_pdf (connect.glsl:68-83): an emitter's chance of starting a light path.
-__device__ __forceinline__ float emitter_power_pdf(const TreeView &t, uint32_t emitter) {
-    const uint4 record = __ldg(&t.records[emitter]);
-    const uint32_t trail = record.y, depth = record.z;
-    uint32_t node = 0;
-    float pdf = 1.0f;
-    for (uint32_t level = 0; level < depth; level++) {
-        const uint32_t link = __ldg(&t.links[node]).x;
-        const float left = node_energy(t, link), right = node_energy(t, link + 1u);
-        if (left + right <= 0.0f) return 0.0f;
-        const uint32_t bit = (trail >> level) & 1u;
-        pdf *= (bit == 0u ? left : right) / (left + right);
-        node = link + bit;
-    }
-    return pdf;
-}
-
-// emitter_by_power (connect.glsl:86-110).
-__device__ __forceinline__ bool emitter_by_power(const TreeView &t, float u, uint32_t &emitter, float &pdf) {
-    pdf = 1.0f;
-    emitter = 0;
-    if (t.node_count < 1) return false;
-    uint32_t node = 0;
-    for (uint32_t depth = 0; depth < 64u; depth++) {
-        const uint2 link = __ldg(&t.links[node]);
-        if ((link.y & kLeafNode) != 0u) {
-            emitter = link.x;
-            return pdf > 0.0f;
-        }
-        const float left = node_energy(t, link.x), right = node_energy(t, link.x + 1u);
-        if (left + right <= 0.0f) return false;
-        const float chance = left / (left + right);
-        if (u < chance) {
-            u = fminf(u / chance, 0.99999994f);
-            pdf *= chance;
-            node = link.x;
-        } else {
-            u = fminf((u - chance) / (1.0f - chance), 0.99999994f);
-            pdf *= 1.0f - chance;
-            node = link.x + 1u;
-        }
-    }
-    return false;
-}
-
-__device__ __forceinline__ bool emitter_is_triangle(const Member &m, uint32_t emitter) {
-    return (__ldg(&m.tree.records[emitter]).x & kEmitterTriangle) != 0u;
-}
-
-// emitter_area_pdf (connect.glsl:116-132): the area density light emission gives a point on
-// an emitter of the tree, the emitter's chance included.
-__device__ __forceinline__ float emitter_area_pdf(const Member &m, uint32_t emitter) {
-    const uint32_t code = __ldg(&m.tree.records[emitter]).x;
-    float area;
-    if (code & kEmitterTriangle) {
-        const uint32_t t = code & ~kEmitterTriangle;
-        const float3 a = position_of(m, m.scene.indices[t * 3]);
-        area = 0.5f * length(cross(position_of(m, m.scene.indices[t * 3 + 1]) - a, position_of(m, m.scene.indices[t * 3 + 2]) - a));
-    } else if (light_type(m.lights, code) == kLightSphere) {
-        const float r = light_at(m.lights, code, 1).w;
-        area = 4.0f * kPi * r * r;
-    } else {
-        area = light_at(m.lights, code, 3).w;
-    }
-    // Emitters of the tree share light paths with lights from afar.
-    const float finite = 1.0f - m.k->emit_share;
-    return area > 0.0f ? finite * emitter_power_pdf(m.tree, emitter) / area : 0.0f;
-}
-
-// ---- Light paths from afar (lights.glsl:283-308) ----------------------------------------
-
-// A light path's emitter code for one from dome or distant light `light` (common.glsl:176-178).
-constexpr uint32_t kAfarEmitter = 0x40000000u;
-
-__device__ __forceinline__ bool emits_from_afar(const float4 *lights, uint32_t light) {
-    const uint32_t type = light_type(lights, light);
-    return type == kLightDome || (type == kLightDistant && light_at(lights, light, 2).w < 1.0f - 1e-7f);
-}
-
-// The chance a light path leaves dome or distant light `light` along -w (w toward the light).
-__device__ __forceinline__ float afar_emission_pdf(const Member &m, uint32_t light, float3 w) {
-    return m.k->emit_share * light_at(m.lights, light, 6).y *
-           light_hit_pdf(m.lights, light, make_float3(0.0f, 0.0f, 0.0f), w, kInfinity);
-}
-
-// The area density of a light path's first surface p (|cos| c there to w) past the disk
-// the path started on: zero outside the disk's shadow.
-__device__ __forceinline__ float afar_first_density(const Constants &k, float3 p, float3 w, float c) {
-    const float radius = k.emit_radius;
-    const float3 offset = p - k.emit_center;
-    const float3 across = offset - w * dot(offset, w);
-    if (dot(across, across) > radius * radius) return 0.0f;
-    return c / (kPi * radius * radius);
-}
-
-__device__ __forceinline__ float emission_direction_pdf(const Member &m, uint32_t emitter, float c) {
-    return fabsf(c) / (emitter_is_triangle(m, emitter) ? 2.0f * kPi : kPi);
-}
-
-// camera_hit_ratio (connect.glsl:141-149): at a light the camera path's BSDF ray hit, the
-// light tracer's density over the camera's.
-__device__ __forceinline__ float camera_hit_ratio(const Member &m, float4 mis, uint32_t emitter, float cos_light,
-                                                  float distance, float bsdf_pdf) {
-    if (emitter == kNone || mis.y <= 0.0f || bsdf_pdf <= 0.0f) return 0.0f;
-    const float d2 = distance * distance;
-    const float at_vertex = emission_direction_pdf(m, emitter, cos_light) * mis.z / d2 / mis.y;
-    const float at_light = emitter_area_pdf(m, emitter) / (bsdf_pdf * fabsf(cos_light) / d2);
-    return mis.x * at_vertex * at_light;
-}
-
-// light_cos (lights.glsl:228-232).
-__device__ __forceinline__ float light_cos(const float4 *lights, uint32_t light, float3 o, float3 d, float t) {
-    const float4 row0 = light_at(lights, light, 0);
-    if ((uint32_t)row0.w == kLightSphere) return fmaxf(0.0f, -dot(d, normalize(o + d * t - xyz(row0))));
-    return fmaxf(0.0f, -dot(d, xyz(light_at(lights, light, 3))));
-}
-
-// light_sampler_pdf (connect.glsl:51-60) for a surface whose only lobe is diffuse (a
-// Lambertian member's): the pdf the light sampler at a surface (shading normal n,
-// geometric g, facing one side) gives `to` when the light path arrived from `from` (both
-// leaving the point). The layered surface's is in openpbr.cuh.
-__device__ __forceinline__ float light_sampler_pdf(float p_diffuse, float3 n, float3 g, float3 from, float3 to) {
-    const bool same = dot(from, g) >= 0.0f;
-    const float3 nv = same ? n : -n, gv = same ? g : -g;
-    const float wo_z = dot(from, nv), wi_z = dot(to, nv);
-    if ((dot(to, gv) > 0.0f) != (wi_z > 0.0f)) return 0.0f;
-    if (wo_z <= 0.0f || wi_z <= 0.0f) return 0.0f;
-    return p_diffuse * wi_z / kPi;
-}
-
-// light_sample_ratio (light_paths.glsl:18-33): the light sample a camera path at p (the
-// surface seen from the camera's side: normal sn, geometric sg) would take toward the
-// light path's first point x0, over its BSDF pdf toward it.
-__device__ __forceinline__ float light_sample_ratio(const Member &m, const Constants &k, uint32_t emitter, float3 sn,
-                                                    float3 sg, float3 p, float3 x0, float bsdf_pdf) {
-    if (!(bsdf_pdf > 0.0f)) return 0.0f;
-    const float3 from = offset_origin(p, sg);
-    const float3 offset = x0 - from;
-    const float reach = length(offset);
-    const float3 d = offset / reach;
-    const float chance = (1.0f - k.p_distant) * tree_pdf(m.tree, emitter, from, sn);
-    const uint32_t code = __ldg(&m.tree.records[emitter]).x;
-    const float pdf = (code & kEmitterTriangle) ? triangle_hit_pdf(m, code & ~kEmitterTriangle, d, reach)
-                                                : light_hit_pdf(m.lights, code, from, d, reach);
-    return chance * pdf / bsdf_pdf;
-}
-
-// light_sample_ratio (light_paths.glsl:15-29) for any light path: one from afar (its
-// emitter code kAfarEmitter | light, arriving along -toward) takes the light sample a
-// camera path would toward that light's direction.
-__device__ __forceinline__ float light_sample_ratio(const Member &m, const Constants &k, uint32_t emitter, float3 sn,
-                                                    float3 sg, float3 p, float3 x0, float3 toward, float bsdf_pdf) {
-    if (!(bsdf_pdf > 0.0f)) return 0.0f;
-    if (emitter & kAfarEmitter) {
-        const uint32_t light = emitter & ~kAfarEmitter;
-        const float select = k.p_distant * light_at(m.lights, light, 6).y;
-        return select * light_hit_pdf(m.lights, light, offset_origin(p, sg), toward, kInfinity) / bsdf_pdf;
-    }
-    return light_sample_ratio(m, k, emitter, sn, sg, p, x0, bsdf_pdf);
-}
-
-// light_emit.comp:21-130: light path `path` of segment `sg`, its sampler number
-// 0x80000000 | (band + its index), from a dome or a distant light with a size (by its share of
-// light paths) on a disk facing it, or from an emitter of the light tree chosen by power,
-// a point on it uniform by area, a cosine-weighted direction (either side of an emissive
-// triangle). A path that cannot start gets a ray that reaches nothing.
-template <bool kSpectral>
-__device__ __forceinline__ void light_emit(const Wave &w, const Member &m, const Segment &sg, uint32_t si, uint32_t path,
-                                           uint32_t slot) {
-    const uint32_t id = 0x80000000u | (m.light_band + sg.first_pixel + (path - sg.path_base));
-    const uint32_t seed = m.k->seed;
-    const float4 u_point = sample4(seed, id, sg.sample, kGroupCamera);
-    const float4 u_pick = sample4(seed, id, sg.sample, kGroupWavelength);
-    const float4 lambda = kSpectral ? sample_wavelengths(u_pick.x) : make_float4(0.0f, 0.0f, 0.0f, 0.0f);
-    const float tag = __uint_as_float(path | (si << kPathBits));
-    auto dead = [&] {
-        w.path[path] = make_uint4(kNone, 0u, 0u, 0u);
-        w.ray_o[0][slot] = make_float4(0.0f, 0.0f, 0.0f, tag);
-        w.ray_d[0][slot] = make_float4(0.0f, 0.0f, 1.0f, 0.0f);
-    };
-    // From afar: a direction by the light's distribution, a point on the disk facing it
-    // about the casters' centre, toward the scene.
-    const float afar = m.k->emit_share;
-    if (u_pick.y < afar) {
-        float share;
-        const uint32_t light = pick_distant(m.lights, m.light_count, u_pick.y / afar, share);
-        if (light == kNone || share <= 0.0f || !emits_from_afar(m.lights, light)) return dead();
-        LightSample s;
-        if (!sample_light(m.lights, light, make_float3(0.0f, 0.0f, 0.0f), make_float2(u_point.x, u_point.y), s)) return dead();
-        const float3 toward = s.direction;
-        const float radius = m.k->emit_radius;
-        float3 t, b;
-        basis(toward, t, b);
-        const float2 disk = concentric(make_float2(u_point.z, u_point.w)) * radius;
-        const float3 start = m.k->emit_center + toward * (2.0f * radius) + t * disk.x + b * disk.y;
-        const float chance = afar * share * s.pdf;
-        const float4 emitted = light_type(m.lights, light) == kLightDome
-                                   ? dome_radiance<kSpectral>(m.lights, light, toward, lambda)
-                                   : light_radiance<kSpectral>(m.lights, light, lambda);
-        const float4 carried = emitted * (kPi * radius * radius / chance);
-        const float most = spec_max<kSpectral>(carried);
-        if (!(most > 0.0f)) return dead();
-        // The light "point" is a direction: its density is the chance, and the camera's
-        // density of it is its BSDF pdf alone (back_reach 1).
-        w.path[path] = make_uint4(kAfarEmitter | light, 0u, 0u, 0u);
-        w.throughput[path] = carried;
-        if (kSpectral) w.lambda[path] = lambda;
-        w.vertex[path] = make_float4(start.x, start.y, start.z, 1.0f / most);
-        w.mis[path] = make_float4(1.0f, chance, 1.0f, -1.0f);
-        w.ray_o[0][slot] = make_float4(start.x, start.y, start.z, tag);
-        w.ray_d[0][slot] = make_float4(-toward.x, -toward.y, -toward.z, kInfinity);
-        return;
-    }
-    uint32_t emitter;
-    float chance;
-    if (!emitter_by_power(m.tree, (u_pick.y - afar) / fmaxf(1e-7f, 1.0f - afar), emitter, chance)) return dead();
-    chance *= 1.0f - afar;
-    const uint32_t code = __ldg(&m.tree.records[emitter]).x;
-    float3 q, n;
-    float4 radiance;
-    float area;
-    bool two_sided = false;
-    if (code & kEmitterTriangle) {
-        const uint32_t t = code & ~kEmitterTriangle;
-        const float3 a = position_of(m, m.scene.indices[t * 3]);
-        const float3 b = position_of(m, m.scene.indices[t * 3 + 1]);
-        const float3 c = position_of(m, m.scene.indices[t * 3 + 2]);
-        const float r = sqrtf(u_point.x);
-        q = a * (1.0f - r) + b * (r * (1.0f - u_point.y)) + c * (r * u_point.y);
-        const float3 cross_ab = cross(b - a, c - a);
-        area = 0.5f * length(cross_ab);
-        n = cross_ab / fmaxf(2.0f * area, 1e-30f);
-        if (u_pick.z < 0.5f) n = -n;
-        two_sided = true;
-        const uint32_t material = __ldg(&m.scene.shading[t]).w;
-        radiance = spec_of<kSpectral>(material_at(m, material, 6), xyz(material_at(m, material, 7)), lambda);
-    } else {
-        const uint32_t type = light_type(m.lights, code);
-        const float4 row0 = light_at(m.lights, code, 0);
-        if (type == kLightSphere) {
-            const float r = light_at(m.lights, code, 1).w;
-            const float z = 1.0f - 2.0f * u_point.x;
-            const float sz = sqrtf(fmaxf(0.0f, 1.0f - z * z));
-            const float phi = 2.0f * kPi * u_point.y;
-            n = make_float3(sz * cosf(phi), sz * sinf(phi), z);
-            q = xyz(row0) + r * n;
-            area = 4.0f * kPi * r * r;
-        } else {
-            const float2 a = type == kLightRect ? make_float2(2.0f * u_point.x - 1.0f, 2.0f * u_point.y - 1.0f)
-                                                : concentric(make_float2(u_point.x, u_point.y));
-            q = xyz(row0) + a.x * xyz(light_at(m.lights, code, 1)) + a.y * xyz(light_at(m.lights, code, 2));
-            n = xyz(light_at(m.lights, code, 3));
-            area = light_at(m.lights, code, 3).w;
-        }
-        radiance = light_radiance<kSpectral>(m.lights, code, lambda);
-    }
-    if (area <= 0.0f) return dead();
-    const float2 disk = concentric(make_float2(u_point.z, u_point.w));
-    const float cos_n = sqrtf(fmaxf(0.0f, 1.0f - (disk.x * disk.x + disk.y * disk.y)));
-    if (cos_n <= 0.0f) return dead();
-    float3 t, b;
-    basis(n, t, b);
-    const float3 direction = normalize(t * disk.x + b * disk.y + n * cos_n);
-    const float point_pdf = chance / area;
-    const float direction_pdf = cos_n / (two_sided ? 2.0f * kPi : kPi);
-    const float4 throughput = radiance * (cos_n / (point_pdf * direction_pdf));
-    const float largest = spec_max<kSpectral>(throughput);
-    if (!(largest > 0.0f)) return dead();
-    const float3 origin = offset_origin(q, n);
-    w.path[path] = make_uint4(emitter, 0u, 0u, __float_as_uint(direction_pdf));
-    w.throughput[path] = throughput;
-    if (kSpectral) w.lambda[path] = lambda;
-    // Russian roulette weighs throughput relative to the start's.
-    w.vertex[path] = make_float4(q.x, q.y, q.z, 1.0f / largest);
-    w.mis[path] = make_float4(1.0f, point_pdf, cos_n, -1.0f);
-    w.ray_o[0][slot] = make_float4(origin.x, origin.y, origin.z, tag);
-    w.ray_d[0][slot] = make_float4(direction.x, direction.y, direction.z, kInfinity);
-}
-
-// camera.comp:14-50: a jittered primary ray per pixel of every camera segment; the light
-// paths of every light segment (light_emit.comp). Block 0 also
-// starts the pass's queue counters.
+// camera.comp:14-50 and light_emit.comp:21-130: every camera segment's paths start a
+// jittered primary ray, every light segment's a light path. Block 0 also starts the
+// pass's queue counters.
 __global__ void __launch_bounds__(kShadeBlock) camera_kernel(Wave w) {
     const Plan *plan = w.plan;
     const uint32_t paths = plan->head.paths;
@@ -447,842 +62,60 @@ __global__ void __launch_bounds__(kShadeBlock) camera_kernel(Wave w) {
         const Member &m = w.members[sg.member];
         if (sg.kind == kLightSegment) {
             const uint32_t slot = w.pool - 1u - (sg.kind_base + (path - sg.path_base));
-            if (m.spectral) light_emit<true>(w, m, sg, si, path, slot);
-            else light_emit<false>(w, m, sg, si, path, slot);
-            continue;
+            if (m.spectral) start_light_path<true>(w, m, sg, si, path, slot);
+            else start_light_path<false>(w, m, sg, si, path, slot);
+        } else {
+            start_camera_path(w, m, sg, si, path, sg.kind_base + (path - sg.path_base));
         }
-        const uint32_t slot = sg.kind_base + (path - sg.path_base);
-        const uint32_t pixel = sg.first_pixel + (path - sg.path_base);
-        if (m.half && m.half[pixel].w > 0.5f) {
-            // Converged (adaptive sampling): the pixel starts no path (camera.comp:18-21);
-            // its ray reaches nothing and its shading ends at once.
-            w.path[path] = make_uint4(kNone, 0u, 0u, 0u);
-            w.ray_o[0][slot] = make_float4(0.0f, 0.0f, 0.0f, __uint_as_float(path | (si << kPathBits)));
-            w.ray_d[0][slot] = make_float4(0.0f, 0.0f, 1.0f, 0.0f);
-            continue;
-        }
-        const uint32_t sample = sg.sample;
-        const uint32_t seed = m.k->seed;
-        const float3 position = make_float3(m.frame[0], m.frame[1], m.frame[2]);
-        const float3 corner = make_float3(m.frame[4], m.frame[5], m.frame[6]);
-        const float3 du = make_float3(m.frame[8], m.frame[9], m.frame[10]);
-        const float3 dv = make_float3(m.frame[12], m.frame[13], m.frame[14]);
-        const bool ortho = m.frame[3] > 0.5f;
-        const float4 u = sample4(seed, pixel, sample, kGroupCamera);
-        const float fx = (float)(pixel % m.width) + u.x, fy = (float)(pixel / m.width) + u.y;
-        const float3 film = corner + fx * du + fy * dv;
-        float3 origin = ortho ? position + film : position;
-        float3 direction = normalize(ortho ? cross(du, dv) : film);
-        if (!ortho && m.lens_radius > 0.0f) {
-            const float3 forward = make_float3(m.forward[0], m.forward[1], m.forward[2]);
-            const float3 focused = position + direction * (m.focus_distance / dot(direction, forward));
-            const float2 disk = concentric(make_float2(u.z, u.w));
-            origin = position + normalize(du) * (disk.x * m.lens_radius) + normalize(dv) * (disk.y * m.lens_radius);
-            direction = normalize(focused - origin);
-        }
-        w.path[path] = make_uint4(pixel, 0u, 0u, 0u);
-        w.throughput[path] = make_float4(1.0f, 1.0f, 1.0f, 1.0f);
-        w.radiance[path] = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
-        w.vertex[path] = make_float4(origin.x, origin.y, origin.z, 1.0f);
-        if (m.spectral) w.lambda[path] = sample_wavelengths(sample4(seed, pixel, sample, kGroupWavelength).x);
-        // Light tracing's MIS: the light paths a sample, and the camera's pdf (camera.comp:42).
-        if (m.light_paths) w.mis[path] = make_float4((float)m.light_paths, 0.0f, 0.0f, camera_pdf(m, direction));
-        w.ray_o[0][slot] = make_float4(origin.x, origin.y, origin.z, __uint_as_float(path | (si << kPathBits)));
-        w.ray_d[0][slot] = make_float4(direction.x, direction.y, direction.z, kInfinity);
     }
 }
 
-// One light sample at p (shade_surface.comp:167-197): a distant light by power, or an
-// emitter of the light tree by importance at `from` and `normal`. Returns the chance the
-// sample was taken with, 0 when none was; `emitter` is the tree's emitter and `afar` the
-// distant light (kNone for the other kind).
+// The bodies every pass variant shares, compiled once per spectral mode (out of line):
+// the compiler fuses multiply-adds by the code around a body, so one body keeps a
+// member's image the same bits alone and in any mix of members. All-diffuse camera paths
+// take the lean body inlined instead (its registers decide the kernel's occupancy).
 template <bool kSpectral>
-__device__ __forceinline__ float choose_light(const Member &m, const Constants &k, float4 u_light, float3 p, float3 from,
-                                              float3 normal, float4 lambda, LightSample &s, float4 &emitted,
-                                              uint32_t &emitter, uint32_t &afar) {
-    const float4 *lights = m.lights;
-    emitted = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
-    emitter = kNone;
-    afar = kNone;
-    if (u_light.x < k.p_distant) {
-        float share;
-        const uint32_t light = pick_distant(lights, m.light_count, u_light.x / k.p_distant, share);
-        if (light != kNone && share > 0.0f && sample_light(lights, light, p, make_float2(u_light.y, u_light.z), s)) {
-            afar = light;
-            emitted = light_type(lights, light) == kLightDome ? dome_radiance<kSpectral>(lights, light, s.direction, lambda)
-                                                              : light_radiance<kSpectral>(lights, light, lambda);
-            return k.p_distant * share;
-        }
-        return 0.0f;
-    }
-    uint32_t chosen;
-    float tree_chance;
-    if (!tree_sample(m.tree, (u_light.x - k.p_distant) / fmaxf(1e-7f, 1.0f - k.p_distant), from, normal, chosen, tree_chance))
-        return 0.0f;
-    emitter = chosen;
-    const uint32_t code = __ldg(&m.tree.records[chosen]).x;
-    bool sampled;
-    if (code & kEmitterTriangle) {
-        sampled = sample_triangle<kSpectral>(m, code & ~kEmitterTriangle, p, make_float2(u_light.y, u_light.z), lambda, s, emitted);
-    } else {
-        sampled = sample_light(lights, code, p, make_float2(u_light.y, u_light.z), s);
-        if (sampled) emitted = light_radiance<kSpectral>(lights, code, lambda);
-    }
-    return sampled ? (1.0f - k.p_distant) * tree_chance : 0.0f;
-}
-
-struct ShadeOut {
-    bool next = false, shadow = false;
-    float4 o, d, so, sd, sc;
-};
-
-__device__ __forceinline__ float rgb_luminance(float3 c) {
-    return c.x * 0.2722287168f + c.y * 0.6740817658f + c.z * 0.0536895174f;
-}
-
-// A queue entry of a member with glossy materials (shade_miss.comp:12-51,
-// shade_surface.comp:48-312, every OpenPBR lobe): a miss, a light hit, or a surface's
-// emission, one light sample and one BSDF sample of the layered surface, on either side
-// of it when it transmits; with light tracing, the techniques weigh against light paths
-// from the tree's emitters and from afar. Out of line, so that the Lambertian members'
-// shading keeps its registers, and compiled once whatever the pass's variant: the
-// compiler fuses multiply-adds by the code around them, so one body keeps a member's
-// image the same bits alone and in any mix.
-template <bool kSpectral>
-__device__ __noinline__ void shade_glossy(const Wave &w, const Member &m, uint32_t sample, uint32_t round, uint32_t i,
-                                          float4 ro, ShadeOut &out) {
-    const Constants &k = *m.k;
-    const uint32_t q = round & 1u;
-    const float4 rd = w.ray_d[q][i], hit = w.hits[q][i];
-    const uint32_t path = __float_as_uint(ro.w) & kPathMask;
-    const uint4 pu = w.path[path];
-    const uint32_t pixel = pu.x, bounces = pu.y, total = bounces & 0xffu;
-    if (pixel == kNone) return;  // a converged pixel's (adaptive sampling)
-    const float ray_pdf = __uint_as_float(pu.w);
-    const float3 origin = xyz(ro), dir = xyz(rd);
-    float4 throughput = w.throughput[path];
-    float4 lambda = kSpectral ? w.lambda[path] : make_float4(0.0f, 0.0f, 0.0f, 0.0f);
-    float4 radiance = w.radiance[path];
-    const bool tracing = m.light_paths != 0u;
-    const float4 mis = tracing ? w.mis[path] : make_float4(0.0f, 0.0f, 0.0f, 0.0f);
-    const float4 vertex_row = w.vertex[path];
-    const float3 vertex = xyz(vertex_row);
-    const float4 *lights = m.lights;
-    const uint32_t what = __float_as_uint(hit.y);
-
-    if (what == kNone) {
-        float4 r = spec_of<kSpectral>(k.background_fit, k.background_rgb, lambda);
-        for (uint32_t light = 0; light < m.light_count; light++) {
-            const uint32_t type = light_type(lights, light);
-            if (type < kLightDistant) continue;
-            if (type == kLightDistant) {
-                const float cos_half = light_at(lights, light, 2).w;
-                if (cos_half >= 1.0f - 1e-7f || dot(dir, -xyz(light_at(lights, light, 3))) < cos_half) continue;
-            }
-            float weight = 1.0f;
-            if (total == 0u) {
-                if (!light_visible(lights, light)) continue;
-            } else if (ray_pdf > 0.0f) {
-                // With light tracing, paths from this light's disk weigh in too.
-                float traced = 0.0f;
-                if (tracing && emits_from_afar(lights, light) && mis.y > 0.0f)
-                    traced = mis.x * (afar_first_density(k, vertex, dir, mis.z) / mis.y) *
-                             (afar_emission_pdf(m, light, dir) / ray_pdf);
-                const float select = k.p_distant * light_at(lights, light, 6).y;
-                weight = mis_weight(light_hit_pdf(lights, light, make_float3(0.0f, 0.0f, 0.0f), dir, kInfinity) * select / ray_pdf,
-                                    traced);
-            }
-            r = r + (type == kLightDome ? dome_radiance<kSpectral>(lights, light, dir, lambda)
-                                        : light_radiance<kSpectral>(lights, light, lambda)) *
-                        weight;
-        }
-        float4 contribution = throughput * r;
-        const float largest = spec_max<kSpectral>(contribution);
-        if (total > 0u && k.clamp_indirect > 0.0f && largest > k.clamp_indirect)
-            contribution = contribution * (k.clamp_indirect / largest);
-        w.radiance[path] = radiance + contribution;
-        return;
-    }
-    if (what & kLightHit) {
-        const uint32_t light = what & ~kLightHit;
-        float weight = 1.0f;
-        if (total == 0u) {
-            if (!light_visible(lights, light)) return;
-        } else if (ray_pdf > 0.0f) {
-            const uint32_t emitter = (uint32_t)light_at(lights, light, 6).w;
-            const float reach = length(vertex - (origin + hit.x * dir));
-            const float chance = (1.0f - k.p_distant) * tree_pdf(m.tree, emitter, vertex, octahedral_decode(pu.z));
-            const float traced =
-                tracing ? camera_hit_ratio(m, mis, emitter, light_cos(lights, light, vertex, dir, reach), reach, ray_pdf) : 0.0f;
-            weight = mis_weight(light_hit_pdf(lights, light, vertex, dir, reach) * chance / ray_pdf, traced);
-        }
-        w.radiance[path] = radiance + clamped<kSpectral>(throughput * light_radiance<kSpectral>(lights, light, lambda) * weight,
-                                                          total, k.clamp_indirect);
-        return;
-    }
-
-    const uint32_t slot = what;
-    const float3 p0 = position_of(m, m.scene.indices[slot * 3]);
-    float3 geometric = normalize(cross(position_of(m, m.scene.indices[slot * 3 + 1]) - p0,
-                                       position_of(m, m.scene.indices[slot * 3 + 2]) - p0));
-    // Faces wind counter-clockwise seen from outside: a ray along the normal is leaving.
-    const bool inside = dot(geometric, dir) > 0.0f;
-    if (inside) geometric = -geometric;
-    const uint4 attributes = __ldg(&m.scene.shading[slot]);
-    const uint32_t material = attributes.w;
-    const float3 p = origin + hit.x * dir;
-    const float reach = length(vertex - p);
-    const float density = (total == 0u ? mis.w : ray_pdf) * fabsf(dot(dir, geometric)) / (reach * reach);
-    const float back_reach = mis.z / (reach * reach);
-    // A cut-out: pass straight through at the same bounce.
-    if (m.cutouts && passes_through(m.materials, material, hit.x, sample4(k.seed, pixel, sample, group_opacity(total)).x)) {
-        const float3 next = offset_origin(p, -geometric);
-        out.next = true;
-        out.o = make_float4(next.x, next.y, next.z, ro.w);
-        out.d = make_float4(dir.x, dir.y, dir.z, kInfinity);
-        return;
-    }
-    // A dispersive material ends the secondary wavelengths (openpbr.glsl:182-194): the
-    // hero carries the sample, and dispersive indices are taken at it from then on.
-    if (kSpectral && material_at(m, material, 12).w != 0.0f && lambda.y >= 0.0f) {
-        throughput = make_float4(throughput.x * 4.0f, 0.0f, 0.0f, 0.0f);
-        radiance = make_float4(radiance.x * 4.0f, 0.0f, 0.0f, 0.0f);
-        lambda = make_float4(lambda.x, -lambda.y, -lambda.z, -lambda.w);
-        w.lambda[path] = lambda;
-    }
-    const float hero = kSpectral && lambda.y < 0.0f ? lambda.x : 0.0f;
-
-    const float4 emission_row = material_at(m, material, 7);
-    if (emission_row.w > 0.0f) {
-        float weight = 1.0f;
-        const uint32_t emitter = m.tree.triangle_map ? __ldg(&m.tree.triangle_map[slot]) : kNone;
-        if (total > 0u && ray_pdf > 0.0f && emitter != kNone) {
-            const float chance = (1.0f - k.p_distant) * tree_pdf(m.tree, emitter, vertex, octahedral_decode(pu.z));
-            const float traced = tracing ? camera_hit_ratio(m, mis, emitter, fabsf(dot(dir, geometric)), reach, ray_pdf) : 0.0f;
-            weight = mis_weight(triangle_hit_pdf(m, slot, dir, reach) * chance / ray_pdf, traced);
-        }
-        radiance = radiance + clamped<kSpectral>(throughput * spec_of<kSpectral>(material_at(m, material, 6), xyz(emission_row), lambda) * weight,
-                                                 total, k.clamp_indirect);
-    }
-    if (total >= k.max_bounces) {
-        w.radiance[path] = radiance;
-        return;
-    }
-    float3 normal = normalize(octahedral_decode(attributes.x) * (1.0f - hit.z - hit.w) + octahedral_decode(attributes.y) * hit.z +
-                              octahedral_decode(attributes.z) * hit.w);
-    if (dot(normal, geometric) < 0.0f) normal = -normal;
-    Surface surface = surface_at(normal, geometric, material, inside);
-    const float3 wo = to_local(surface, -dir);
-    prepare_surface<kSpectral>(surface, wo, lambda, m.materials);
-    const float3 from = offset_origin(p, geometric);
-
-    const float4 u_light = sample4(k.seed, pixel, sample, group_light(total));
-    LightSample s;
-    float4 emitted;
-    uint32_t nee_emitter, afar;
-    const float chance = choose_light<kSpectral>(m, k, u_light, p, from, normal, lambda, s, emitted, nee_emitter, afar);
-    if (chance > 0.0f) {
-        const float side = dot(s.direction, geometric);
-        const float3 wi = to_local(surface, s.direction);
-        if ((side > 0.0f) == (wi.z > 0.0f) && (side > 0.0f || surface.p_transmission > 0.0f)) {
-            float bsdf_pdf;
-            const float4 f = evaluate_surface(surface, wi, wo, bsdf_pdf);
-            if (bsdf_pdf > 0.0f) {
-                const float light_pdf = s.pdf * chance;
-                float traced = 0.0f;
-                if (tracing && !s.delta && nee_emitter != kNone && density > 0.0f) {
-                    const float d2 = s.distance * s.distance;
-                    const float at_last =
-                        total == 0u ? 1.0f : light_sampler_pdf(surface, s.direction, -dir, m.materials, hero) * back_reach / mis.y;
-                    const float at_vertex = emission_direction_pdf(m, nee_emitter, s.cos_light) * fabsf(side) / d2 / density;
-                    const float at_light = emitter_area_pdf(m, nee_emitter) / (bsdf_pdf * s.cos_light / d2);
-                    traced = mis.x * at_last * at_vertex * at_light;
-                }
-                if (tracing && afar != kNone && emits_from_afar(lights, afar) && density > 0.0f) {
-                    const float at_last =
-                        total == 0u ? 1.0f : light_sampler_pdf(surface, s.direction, -dir, m.materials, hero) * back_reach / mis.y;
-                    const float at_vertex = afar_first_density(k, p, s.direction, fabsf(side)) / density;
-                    const float at_light = afar_emission_pdf(m, afar, s.direction) / bsdf_pdf;
-                    traced = mis.x * at_last * at_vertex * at_light;
-                }
-                const float weight = s.delta ? 1.0f : mis_weight(bsdf_pdf / light_pdf, traced * bsdf_pdf / light_pdf);
-                const float4 contribution = clamped<kSpectral>(throughput * f * emitted * (fabsf(wi.z) * (weight / light_pdf)),
-                                                               total, k.clamp_indirect);
-                const float3 target = p + s.direction * s.distance;
-                const float margin = 4e-4f * fmaxf(1.0f, fmaxf(fabsf(target.x), fmaxf(fabsf(target.y), fabsf(target.z))));
-                const float shadow_reach = s.distance >= kInfinity ? kInfinity : fmaxf(0.0f, s.distance - margin);
-                const float3 so = offset_origin(p, side > 0.0f ? geometric : -geometric);
-                out.shadow = true;
-                out.so = make_float4(so.x, so.y, so.z, ro.w);
-                out.sd = make_float4(s.direction.x, s.direction.y, s.direction.z, shadow_reach);
-                out.sc = contribution;
-            }
-        }
-    }
-    w.radiance[path] = radiance;
-
-    // One BSDF sample (sample_surface with u.xyw: the lobe pick is u.w).
-    const float4 u = sample4(k.seed, pixel, sample, group_bsdf(total));
-    float3 wi;
-    float pdf, pdf_again;
-    uint32_t lobe;
-    if (!sample_direction(surface, wo, make_float3(u.x, u.y, u.w), wi, pdf, lobe)) return;
-    const float4 weight = evaluate_surface(surface, wi, wo, pdf_again) * (fabsf(wi.z) / pdf);
-    const float3 direction = to_world(surface, wi);
-    // A shading normal can send a ray to the wrong side of the true surface.
-    const float side = dot(direction, geometric);
-    if ((side > 0.0f) != (wi.z > 0.0f)) return;
-    const uint32_t next_bounces = next_bounce(bounces, lobe, k.limits);
-    if (next_bounces == kNone) return;
-    throughput = throughput * weight;
-    const float survival_scale = fminf(vertex_row.w, 1e6f);
-    if (total + 1u >= 3u) {
-        const float survive = fminf(0.95f, spec_max<kSpectral>(throughput) * survival_scale);
-        if (u.z >= survive) return;
-        throughput = make_float4(throughput.x / survive, throughput.y / survive, throughput.z / survive, throughput.w / survive);
-    }
-    const float3 next = side > 0.0f ? from : offset_origin(p, -geometric);
-    if (tracing) {
-        const float at_last =
-            total == 0u ? 1.0f : light_sampler_pdf(surface, direction, -dir, m.materials, hero) * back_reach / mis.y;
-        w.mis[path] = make_float4(mis.x * at_last, density, fabsf(side), 0.0f);
-    }
-    w.path[path] = make_uint4(pixel, next_bounces, octahedral_encode(normal), __float_as_uint(pdf));
-    w.throughput[path] = throughput;
-    w.vertex[path] = make_float4(next.x, next.y, next.z, survival_scale);
-    out.next = true;
-    out.o = make_float4(next.x, next.y, next.z, ro.w);
-    out.d = make_float4(direction.x, direction.y, direction.z, kInfinity);
-}
-
-// One queue entry: a miss (shade_miss.comp:12-51), a light hit or a surface hit
-// (shade_surface.comp:48-312) of a member whose materials are all EON diffuse (OpenPBR with
-// no specular, metal, coat or transmission lobe), where the layered surface reduces to
-// EON with p_diffuse 1. kTracing: members of the pass may trace light paths, so camera
-// paths weigh their techniques against them. kGlossy: members with glossy materials take
-// shade_glossy instead.
-template <bool kSpectral, bool kTracing, bool kGlossy>
-__device__ __forceinline__ void shade_one(const Wave &w, const Member &m, uint32_t sample, uint32_t round, uint32_t i,
-                                          float4 ro, ShadeOut &out) {
-    if (kGlossy && m.glossy) return shade_glossy<kSpectral>(w, m, sample, round, i, ro, out);
-    const Constants &k = *m.k;
-    const uint32_t q = round & 1u;
-    const float4 rd = w.ray_d[q][i], hit = w.hits[q][i];
-    const uint32_t tag = __float_as_uint(ro.w);
-    const uint32_t path = tag & kPathMask;
-    uint4 pu = w.path[path];
-    const uint32_t pixel = pu.x, bounces = pu.y, total = bounces & 0xffu;
-    if (pixel == kNone) return;  // a converged pixel's (adaptive sampling)
-    const float ray_pdf = __uint_as_float(pu.w);
-    const float3 origin = xyz(ro), dir = xyz(rd);
-    float4 throughput = w.throughput[path];
-    const float4 lambda = kSpectral ? w.lambda[path] : make_float4(0.0f, 0.0f, 0.0f, 0.0f);
-    const uint32_t what = __float_as_uint(hit.y);
-    const float t = hit.x;
-    float4 radiance = w.radiance[path];
-    const float4 *lights = m.lights;
-    const bool tracing = kTracing && m.light_paths != 0u;
-    const float4 mis = tracing ? w.mis[path] : make_float4(0.0f, 0.0f, 0.0f, 0.0f);
-
-    if (what == kNone) {
-        float4 r = spec_of<kSpectral>(k.background_fit, k.background_rgb, lambda);
-        for (uint32_t light = 0; light < m.light_count; light++) {
-            const uint32_t type = light_type(lights, light);
-            if (type < kLightDistant) continue;
-            if (type == kLightDistant) {
-                const float cos_half = light_at(lights, light, 2).w;
-                if (cos_half >= 1.0f - 1e-7f || dot(dir, -xyz(light_at(lights, light, 3))) < cos_half) continue;
-            }
-            float weight = 1.0f;
-            if (total == 0u) {
-                if (!light_visible(lights, light)) continue;
-            } else if (ray_pdf > 0.0f) {
-                const float select = k.p_distant * light_at(lights, light, 6).y;
-                weight = mis_weight(light_hit_pdf(lights, light, make_float3(0.0f, 0.0f, 0.0f), dir, kInfinity) *
-                                        select / ray_pdf, 0.0f);
-            }
-            r = r + (type == kLightDome ? dome_radiance<kSpectral>(lights, light, dir, lambda)
-                                        : light_radiance<kSpectral>(lights, light, lambda)) *
-                        weight;
-        }
-        float4 contribution = throughput * r;
-        const float largest = spec_max<kSpectral>(contribution);
-        if (total > 0u && k.clamp_indirect > 0.0f && largest > k.clamp_indirect)
-            contribution = contribution * (k.clamp_indirect / largest);
-        w.radiance[path] = radiance + contribution;
-        return;
-    }
-    const float4 vertex_row = w.vertex[path];
-    const float3 vertex = xyz(vertex_row);
-    if (what & kLightHit) {
-        const uint32_t light = what & ~kLightHit;
-        float weight = 1.0f;
-        if (total == 0u) {
-            if (!light_visible(lights, light)) return;
-        } else if (ray_pdf > 0.0f) {
-            const uint32_t emitter = (uint32_t)light_at(lights, light, 6).w;
-            const float reach = length(vertex - (origin + t * dir));
-            const float chance = (1.0f - k.p_distant) * tree_pdf(m.tree, emitter, vertex, octahedral_decode(pu.z));
-            const float traced =
-                tracing ? camera_hit_ratio(m, mis, emitter, light_cos(lights, light, vertex, dir, reach), reach, ray_pdf) : 0.0f;
-            weight = mis_weight(light_hit_pdf(lights, light, vertex, dir, reach) * chance / ray_pdf, traced);
-        }
-        w.radiance[path] = radiance + clamped<kSpectral>(throughput * light_radiance<kSpectral>(lights, light, lambda) * weight,
-                                                          total, k.clamp_indirect);
-        return;
-    }
-
-    // A surface.
-    const uint32_t slot = what;
-    const float3 p0 = position_of(m, m.scene.indices[slot * 3]);
-    float3 geometric = normalize(cross(position_of(m, m.scene.indices[slot * 3 + 1]) - p0,
-                                       position_of(m, m.scene.indices[slot * 3 + 2]) - p0));
-    if (dot(geometric, dir) > 0.0f) geometric = -geometric;
-    const uint4 attributes = __ldg(&m.scene.shading[slot]);
-    const uint32_t material = attributes.w;
-    const float3 p = origin + t * dir;
-    const float reach = length(vertex - p);
-    // The camera's density of this vertex (area), and what turns the light sampler's pdf
-    // here toward the last vertex into that vertex's density (shade_surface.comp:91-94).
-    const float density = (total == 0u ? mis.w : ray_pdf) * fabsf(dot(dir, geometric)) / (reach * reach);
-    const float back_reach = mis.z / (reach * reach);
-    // A cut-out: pass straight through at the same bounce.
-    if (m.cutouts && passes_through(m.materials, material, hit.x, sample4(k.seed, pixel, sample, group_opacity(total)).x)) {
-        const float3 next = offset_origin(p, -geometric);
-        out.next = true;
-        out.o = make_float4(next.x, next.y, next.z, ro.w);
-        out.d = make_float4(dir.x, dir.y, dir.z, kInfinity);
-        return;
-    }
-
-    const float4 emission_row = material_at(m, material, 7);
-    if (emission_row.w > 0.0f) {
-        float weight = 1.0f;
-        const uint32_t emitter = m.tree.triangle_map ? __ldg(&m.tree.triangle_map[slot]) : kNone;
-        if (total > 0u && ray_pdf > 0.0f && emitter != kNone) {
-            const float chance = (1.0f - k.p_distant) * tree_pdf(m.tree, emitter, vertex, octahedral_decode(pu.z));
-            const float traced = tracing ? camera_hit_ratio(m, mis, emitter, fabsf(dot(dir, geometric)), reach, ray_pdf) : 0.0f;
-            weight = mis_weight(triangle_hit_pdf(m, slot, dir, reach) * chance / ray_pdf, traced);
-        }
-        radiance = radiance + clamped<kSpectral>(throughput * spec_of<kSpectral>(material_at(m, material, 6), xyz(emission_row), lambda) * weight,
-                                                 total, k.clamp_indirect);
-    }
-    if (total >= k.max_bounces) {
-        w.radiance[path] = radiance;
-        return;
-    }
-    const float hu = hit.z, hv = hit.w;
-    float3 normal = normalize(octahedral_decode(attributes.x) * (1.0f - hu - hv) + octahedral_decode(attributes.y) * hu +
-                              octahedral_decode(attributes.z) * hv);
-    if (dot(normal, geometric) < 0.0f) normal = -normal;
-    float3 tangent, bitangent;
-    basis(normal, tangent, bitangent);
-    const float3 wo = make_float3(-dot(dir, tangent), -dot(dir, bitangent), -dot(dir, normal));
-    const float4 base_rgb = material_at(m, material, 1);
-    const float4 base = spec_of<kSpectral>(material_at(m, material, 0), xyz(base_rgb), lambda) * base_rgb.w;
-    const float roughness = material_at(m, material, 10).y;
-    const float p_diffuse = fmaxf(rgb_luminance(xyz(base_rgb) * base_rgb.w), 0.0f) > 0.0f ? 1.0f : 0.0f;
-    const float3 from = offset_origin(p, geometric);
-
-    // One light sample: a distant light by power, or an emitter of the light tree.
-    const float4 u_light = sample4(k.seed, pixel, sample, group_light(total));
-    LightSample s;
-    float4 emitted = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
-    float chance = 0.0f;
-    bool sampled = false;
-    uint32_t nee_emitter = kNone;
-    if (u_light.x < k.p_distant) {
-        float share;
-        const uint32_t light = pick_distant(lights, m.light_count, u_light.x / k.p_distant, share);
-        if (light != kNone && share > 0.0f && sample_light(lights, light, p, make_float2(u_light.y, u_light.z), s)) {
-            chance = k.p_distant * share;
-            emitted = light_type(lights, light) == kLightDome ? dome_radiance<kSpectral>(lights, light, s.direction, lambda)
-                                                              : light_radiance<kSpectral>(lights, light, lambda);
-            sampled = true;
-        }
-    } else {
-        uint32_t emitter;
-        float tree_chance;
-        if (tree_sample(m.tree, (u_light.x - k.p_distant) / fmaxf(1e-7f, 1.0f - k.p_distant), from, normal, emitter, tree_chance)) {
-            chance = (1.0f - k.p_distant) * tree_chance;
-            nee_emitter = emitter;
-            const uint32_t code = __ldg(&m.tree.records[emitter]).x;
-            if (code & kEmitterTriangle) {
-                sampled = sample_triangle<kSpectral>(m, code & ~kEmitterTriangle, p, make_float2(u_light.y, u_light.z), lambda, s, emitted);
-            } else if (sample_light(lights, code, p, make_float2(u_light.y, u_light.z), s)) {
-                emitted = light_radiance<kSpectral>(lights, code, lambda);
-                sampled = true;
-            }
-        }
-    }
-    if (sampled && chance > 0.0f) {
-        const float side = dot(s.direction, geometric);
-        const float3 wi = make_float3(dot(s.direction, tangent), dot(s.direction, bitangent), dot(s.direction, normal));
-        if (side > 0.0f && wi.z > 0.0f && wo.z > 0.0f) {
-            const float bsdf_pdf = p_diffuse * wi.z / kPi;
-            if (bsdf_pdf > 0.0f) {
-                const float4 f = eon(base, roughness, wi, wo);
-                const float light_pdf = s.pdf * chance;
-                // The light tracer's density of this path over the camera path's BSDF ray
-                // reaching the same light point (shade_surface.comp:210-224).
-                float traced = 0.0f;
-                if (tracing && !s.delta && nee_emitter != kNone && density > 0.0f) {
-                    const float d2 = s.distance * s.distance;
-                    const float at_last =
-                        total == 0u ? 1.0f : light_sampler_pdf(p_diffuse, normal, geometric, s.direction, -dir) * back_reach / mis.y;
-                    const float at_vertex = emission_direction_pdf(m, nee_emitter, s.cos_light) * fabsf(side) / d2 / density;
-                    const float at_light = emitter_area_pdf(m, nee_emitter) / (bsdf_pdf * s.cos_light / d2);
-                    traced = mis.x * at_last * at_vertex * at_light;
-                }
-                const float weight = s.delta ? 1.0f : mis_weight(bsdf_pdf / light_pdf, traced * bsdf_pdf / light_pdf);
-                const float4 contribution = clamped<kSpectral>(throughput * f * emitted * (fabsf(wi.z) * (weight / light_pdf)),
-                                                               total, k.clamp_indirect);
-                const float3 target = p + s.direction * s.distance;
-                const float margin = 4e-4f * fmaxf(1.0f, fmaxf(fabsf(target.x), fmaxf(fabsf(target.y), fabsf(target.z))));
-                const float shadow_reach = s.distance >= kInfinity ? kInfinity : fmaxf(0.0f, s.distance - margin);
-                const float3 so = offset_origin(p, geometric);
-                out.shadow = true;
-                out.so = make_float4(so.x, so.y, so.z, ro.w);
-                out.sd = make_float4(s.direction.x, s.direction.y, s.direction.z, shadow_reach);
-                out.sc = contribution;
-            }
-        }
-    }
-    w.radiance[path] = radiance;
-
-    // One BSDF sample (sample_surface with u.xyw: the lobe pick is u.w).
-    const float4 u = sample4(k.seed, pixel, sample, group_bsdf(total));
-    if (wo.z <= 0.0f || !(u.w < p_diffuse)) return;
-    const float2 disk = concentric(make_float2(u.x, u.y));
-    const float3 wi = make_float3(disk.x, disk.y, sqrtf(fmaxf(0.0f, 1.0f - (disk.x * disk.x + disk.y * disk.y))));
-    if (wi.z == 0.0f) return;
-    const float pdf = p_diffuse * wi.z / kPi;
-    if (!(pdf > 0.0f)) return;
-    const float4 weight = eon(base, roughness, wi, wo) * (fabsf(wi.z) / pdf);
-    const float3 direction = tangent * wi.x + bitangent * wi.y + normal * wi.z;
-    const float side = dot(direction, geometric);
-    if ((side > 0.0f) != (wi.z > 0.0f)) return;
-    const uint32_t next_bounces = next_bounce(bounces, 0u, k.limits);
-    if (next_bounces == kNone) return;
-    throughput = throughput * weight;
-    const float survival_scale = fminf(vertex_row.w, 1e6f);
-    if (total + 1u >= 3u) {
-        const float survive = fminf(0.95f, spec_max<kSpectral>(throughput) * survival_scale);
-        if (u.z >= survive) return;
-        throughput = make_float4(throughput.x / survive, throughput.y / survive, throughput.z / survive, throughput.w / survive);
-    }
-    const float3 next = side > 0.0f ? from : offset_origin(p, -geometric);
-    if (tracing) {
-        // This vertex's factor of the light tracer's density, settled now that the light
-        // sampler's direction here is known (shade_surface.comp:304-307).
-        const float at_last =
-            total == 0u ? 1.0f : light_sampler_pdf(p_diffuse, normal, geometric, direction, -dir) * back_reach / mis.y;
-        w.mis[path] = make_float4(mis.x * at_last, density, fabsf(side), 0.0f);
-    }
-    w.path[path] = make_uint4(pixel, next_bounces, octahedral_encode(normal), __float_as_uint(pdf));
-    w.throughput[path] = throughput;
-    w.vertex[path] = make_float4(next.x, next.y, next.z, survival_scale);
-    out.next = true;
-    out.o = make_float4(next.x, next.y, next.z, ro.w);
-    out.d = make_float4(direction.x, direction.y, direction.z, kInfinity);
-}
-
-// A light path's hit (light_paths.glsl:31-189) on a member whose materials are all EON
-// diffuse: a light ends it; at a surface it connects to the camera -- a shadow ray carrying, in the film's
-// terms and MIS-weighted, what the camera would see of it to the pixel it projects to --
-// and scatters on by the BSDF as seen from where the light came, weighed by the BSDF as
-// the camera would evaluate it, with the shading-normal correction light paths need.
-template <bool kSpectral>
-__device__ __noinline__ void shade_light(const Wave &w, const Member &m, uint32_t sample, uint32_t round, uint32_t i,
+__device__ __noinline__ void camera_layered(const Wave &w, const Member &m, uint32_t sample, uint32_t round, uint32_t i,
                                             float4 ro, ShadeOut &out) {
-    const Constants &k = *m.k;
-    const uint32_t q = round & 1u;
-    const float4 hit = w.hits[q][i];
-    const uint32_t what = __float_as_uint(hit.y);
-    if (what == kNone || (what & kLightHit)) return;
-    const float4 rd = w.ray_d[q][i];
-    const uint32_t tag = __float_as_uint(ro.w);
-    const uint32_t path = tag & kPathMask;
-    const uint4 pu = w.path[path];
-    const uint32_t emitter = pu.x, bounces = pu.y, total = bounces & 0xffu;
-    const float ray_pdf = __uint_as_float(pu.w);
-    const float3 origin = xyz(ro), dir = xyz(rd);
-    float4 throughput = w.throughput[path];
-    const float4 lambda = kSpectral ? w.lambda[path] : make_float4(0.0f, 0.0f, 0.0f, 0.0f);
-    const float4 vertex_row = w.vertex[path];
-    const float4 mis = w.mis[path];
-    const uint32_t id = 0x80000000u | (m.light_band + tag_light_index(w, tag));
-
-    const uint32_t slot = what;
-    const float3 p0 = position_of(m, m.scene.indices[slot * 3]);
-    float3 geometric = normalize(cross(position_of(m, m.scene.indices[slot * 3 + 1]) - p0,
-                                       position_of(m, m.scene.indices[slot * 3 + 2]) - p0));
-    if (dot(geometric, dir) > 0.0f) geometric = -geometric;
-    const uint4 attributes = __ldg(&m.scene.shading[slot]);
-    const uint32_t material = attributes.w;
-    const float3 p = origin + hit.x * dir;
-    // A cut-out, as camera paths take it.
-    if (m.cutouts && passes_through(m.materials, attributes.w, hit.x, sample4(k.seed, id, sample, group_opacity(total)).x)) {
-        const float3 next = offset_origin(p, -geometric);
-        out.next = true;
-        out.o = make_float4(next.x, next.y, next.z, ro.w);
-        out.d = make_float4(dir.x, dir.y, dir.z, kInfinity);
-        return;
-    }
-    if (total >= k.max_bounces) return;
-    const float hu = hit.z, hv = hit.w;
-    float3 normal = normalize(octahedral_decode(attributes.x) * (1.0f - hu - hv) + octahedral_decode(attributes.y) * hu +
-                              octahedral_decode(attributes.z) * hv);
-    if (dot(normal, geometric) < 0.0f) normal = -normal;
-    const float4 u_lens = sample4(k.seed, id, sample, group_light(total));
-    const float3 lens = lens_point(m, make_float2(u_lens.x, u_lens.y));
-    uint32_t pixel = 0;
-    float3 to_point;
-    float camera_distance;
-    const bool on_film = camera_pixel(m, p, lens, pixel, to_point, camera_distance);
-    const float4 base_rgb = material_at(m, material, 1);
-    const float4 base = spec_of<kSpectral>(material_at(m, material, 0), xyz(base_rgb), lambda) * base_rgb.w;
-    const float roughness = material_at(m, material, 10).y;
-    const float p_diffuse = fmaxf(rgb_luminance(xyz(base_rgb) * base_rgb.w), 0.0f) > 0.0f ? 1.0f : 0.0f;
-    const float3 toward_light = -dir;
-    const float3 x_last = xyz(vertex_row);
-    const float reach = length(x_last - p);
-    const float cos_in = fabsf(dot(dir, geometric));
-    const float density = ray_pdf * cos_in / (reach * reach);
-    const float back_reach = mis.z / (reach * reach);
-    const float cos_shading_in = dot(toward_light, normal);
-    if (cos_shading_in <= 0.0f || cos_in < 1e-6f) return;
-    const float shading_in = cos_shading_in / cos_in;
-    const float L = (float)m.light_paths;
-
-    if (on_film) {
-        const float3 to_camera = -to_point;
-        const float side = dot(to_camera, geometric);
-        const float3 sn = side > 0.0f ? normal : -normal, sg = side > 0.0f ? geometric : -geometric;
-        float3 st, sb;
-        basis(sn, st, sb);
-        const float3 wo = make_float3(dot(to_camera, st), dot(to_camera, sb), dot(to_camera, sn));
-        const float3 wi = make_float3(dot(toward_light, st), dot(toward_light, sb), dot(toward_light, sn));
-        if ((dot(toward_light, sg) > 0.0f) == (wi.z > 0.0f) && wo.z > 0.0f && wi.z > 0.0f) {
-            const float camera_bsdf_pdf = p_diffuse * wi.z / kPi;
-            const float4 f = eon(base, roughness, wi, wo);
-            const float camera_density = camera_pdf(m, to_point) * fabsf(side) / (camera_distance * camera_distance);
-            const float4 contribution = throughput * f * (shading_in * camera_density / L);
-            if (spec_max<kSpectral>(contribution) > 0.0f) {
-                // The camera techniques' densities over this one's.
-                const float last = mis.y > 0.0f ? camera_bsdf_pdf * back_reach / mis.y : 0.0f;
-                const float ratio = mis.x * last * camera_density / density;
-                const float sample_ratio =
-                    total == 0u ? light_sample_ratio(m, k, emitter, sn, sg, p, x_last, camera_bsdf_pdf) : fmaxf(mis.w, 0.0f);
-                const float weight = mis_weight(ratio / L, ratio * sample_ratio / L);
-                const float margin = 4e-4f * fmaxf(1.0f, fmaxf(fabsf(p.x), fmaxf(fabsf(p.y), fabsf(p.z))));
-                const float3 so = offset_origin(p, sg);
-                const float3 value = spec_to_film<kSpectral>(contribution * weight, lambda, k);
-                out.shadow = true;
-                out.so = make_float4(so.x, so.y, so.z, ro.w);
-                out.sd = make_float4(to_camera.x, to_camera.y, to_camera.z, fmaxf(0.0f, camera_distance - margin));
-                out.sc = make_float4(value.x, value.y, value.z, __uint_as_float(pixel));
-            }
-        }
-    }
-
-    // Scatter on, unless the next vertex would be past the bounce limit.
-    if (total + 1u >= k.max_bounces) return;
-    const float4 u = sample4(k.seed, id, sample, group_bsdf(total));
-    float3 tangent, bitangent;
-    basis(normal, tangent, bitangent);
-    const float wo_light_z = dot(toward_light, normal);
-    if (wo_light_z <= 0.0f || !(u.w < p_diffuse)) return;
-    const float2 disk = concentric(make_float2(u.x, u.y));
-    const float3 wl = make_float3(disk.x, disk.y, sqrtf(fmaxf(0.0f, 1.0f - (disk.x * disk.x + disk.y * disk.y))));
-    if (wl.z == 0.0f) return;
-    const float light_pdf = p_diffuse * wl.z / kPi;
-    if (!(light_pdf > 0.0f)) return;
-    const float3 direction = tangent * wl.x + bitangent * wl.y + normal * wl.z;
-    const float side = dot(direction, geometric);
-    if ((side > 0.0f) != (wl.z > 0.0f)) return;
-    const float3 sn = side > 0.0f ? normal : -normal, sg = side > 0.0f ? geometric : -geometric;
-    float3 st, sb;
-    basis(sn, st, sb);
-    const float3 wo = make_float3(dot(direction, st), dot(direction, sb), dot(direction, sn));
-    const float3 wi = make_float3(dot(toward_light, st), dot(toward_light, sb), dot(toward_light, sn));
-    if ((dot(toward_light, sg) > 0.0f) != (wi.z > 0.0f)) return;
-    const bool lobe = wo.z > 0.0f && wi.z > 0.0f;
-    const float camera_bsdf_pdf = lobe ? p_diffuse * wi.z / kPi : 0.0f;
-    const float4 f = lobe ? eon(base, roughness, wi, wo) : make_float4(0.0f, 0.0f, 0.0f, 0.0f);
-    const uint32_t next_bounces = next_bounce(bounces, 0u, k.limits);
-    if (next_bounces == kNone) return;
-    throughput = throughput * f * (shading_in * fabsf(side) / light_pdf);
-    const float survival_scale = vertex_row.w;
-    if (total + 1u >= 3u) {
-        const float survive = fminf(0.95f, spec_max<kSpectral>(throughput) * survival_scale);
-        if (u.z >= survive) return;
-        throughput = make_float4(throughput.x / survive, throughput.y / survive, throughput.z / survive, throughput.w / survive);
-    }
-    if (!(spec_max<kSpectral>(throughput) > 0.0f)) return;
-    const float last = mis.y > 0.0f ? camera_bsdf_pdf * back_reach / mis.y : 0.0f;
-    const float sample_ratio = total == 0u ? light_sample_ratio(m, k, emitter, sn, sg, p, x_last, camera_bsdf_pdf) : mis.w;
-    const float3 next = offset_origin(p, side > 0.0f ? geometric : -geometric);
-    w.path[path] = make_uint4(emitter, next_bounces, 0u, __float_as_uint(light_pdf));
-    w.throughput[path] = throughput;
-    w.vertex[path] = make_float4(p.x, p.y, p.z, survival_scale);
-    w.mis[path] = make_float4(mis.x * last, density, fabsf(side), sample_ratio);
-    out.next = true;
-    out.o = make_float4(next.x, next.y, next.z, ro.w);
-    out.d = make_float4(direction.x, direction.y, direction.z, kInfinity);
+    shade_camera_path<kSpectral, true, LayeredOps>(w, m, sample, round, i, ro, out);
+}
+template <bool kSpectral>
+__device__ __noinline__ void light_layered(const Wave &w, const Member &m, uint32_t sample, uint32_t round, uint32_t i,
+                                           float4 ro, ShadeOut &out) {
+    shade_light_path<kSpectral, LayeredLightOps>(w, m, sample, round, i, ro, out);
+}
+template <bool kSpectral>
+__device__ __noinline__ void light_diffuse(const Wave &w, const Member &m, uint32_t sample, uint32_t round, uint32_t i,
+                                           float4 ro, ShadeOut &out) {
+    shade_light_path<kSpectral, DiffuseLightOps>(w, m, sample, round, i, ro, out);
 }
 
-// A light path's hit on a member with glossy materials (light_paths.glsl:31-189, every
-// OpenPBR lobe): the surface read once on the side light arrives from; the camera
-// connection evaluates it as the camera would see it (oriented toward the camera, or read
-// again from the other side), the scattering samples light_lobes' choice and weighs the
-// direction by the BSDF as a camera arriving along it evaluates it.
-template <bool kSpectral>
-__device__ __noinline__ void shade_light_glossy(const Wave &w, const Member &m, uint32_t sample, uint32_t round, uint32_t i,
-                                                float4 ro, ShadeOut &out) {
-    const Constants &k = *m.k;
-    const uint32_t q = round & 1u;
-    const float4 hit = w.hits[q][i];
-    const uint32_t what = __float_as_uint(hit.y);
-    if (what == kNone || (what & kLightHit)) return;
-    const float4 rd = w.ray_d[q][i];
-    const uint32_t tag = __float_as_uint(ro.w);
-    const uint32_t path = tag & kPathMask;
-    const uint4 pu = w.path[path];
-    const uint32_t emitter = pu.x, bounces = pu.y, total = bounces & 0xffu;
-    const float ray_pdf = __uint_as_float(pu.w);
-    const float3 origin = xyz(ro), dir = xyz(rd);
-    float4 throughput = w.throughput[path];
-    float4 lambda = kSpectral ? w.lambda[path] : make_float4(0.0f, 0.0f, 0.0f, 0.0f);
-    const float4 vertex_row = w.vertex[path];
-    const float4 mis = w.mis[path];
-    const uint32_t id = 0x80000000u | (m.light_band + tag_light_index(w, tag));
+// The octant of a direction (sign bits of x, y, z).
+__device__ __forceinline__ uint32_t octant_of(float4 d) {
+    return (d.x < 0.0f ? 1u : 0u) | (d.y < 0.0f ? 2u : 0u) | (d.z < 0.0f ? 4u : 0u);
+}
 
-    const uint32_t slot = what;
-    const float3 p0 = position_of(m, m.scene.indices[slot * 3]);
-    float3 geometric = normalize(cross(position_of(m, m.scene.indices[slot * 3 + 1]) - p0,
-                                       position_of(m, m.scene.indices[slot * 3 + 2]) - p0));
-    const bool back = dot(geometric, dir) > 0.0f;
-    if (back) geometric = -geometric;
-    const uint4 attributes = __ldg(&m.scene.shading[slot]);
-    const float3 p = origin + hit.x * dir;
-    // A cut-out, as camera paths take it.
-    if (m.cutouts && passes_through(m.materials, attributes.w, hit.x, sample4(k.seed, id, sample, group_opacity(total)).x)) {
-        const float3 next = offset_origin(p, -geometric);
-        out.next = true;
-        out.o = make_float4(next.x, next.y, next.z, ro.w);
-        out.d = make_float4(dir.x, dir.y, dir.z, kInfinity);
-        return;
-    }
-    if (total >= k.max_bounces) return;
-    // Dispersion ends the secondary wavelengths, as on camera paths.
-    if (kSpectral && material_at(m, attributes.w, 12).w != 0.0f && lambda.y >= 0.0f) {
-        throughput = make_float4(throughput.x * 4.0f, 0.0f, 0.0f, 0.0f);
-        lambda = make_float4(lambda.x, -lambda.y, -lambda.z, -lambda.w);
-        w.lambda[path] = lambda;
-    }
-    float3 normal = normalize(octahedral_decode(attributes.x) * (1.0f - hit.z - hit.w) + octahedral_decode(attributes.y) * hit.z +
-                              octahedral_decode(attributes.z) * hit.w);
-    if (dot(normal, geometric) < 0.0f) normal = -normal;
-    const float4 u_lens = sample4(k.seed, id, sample, group_light(total));
-    const float3 lens = lens_point(m, make_float2(u_lens.x, u_lens.y));
-    uint32_t pixel = 0;
-    float3 to_point;
-    float camera_distance;
-    const bool on_film = camera_pixel(m, p, lens, pixel, to_point, camera_distance);
-    Surface lit = surface_at(normal, geometric, attributes.w, back);
-    const float3 toward_light = -dir;
-    read_material(lit, m.materials, kSpectral && lambda.y < 0.0f ? lambda.x : 0.0f);
-    read_colors<kSpectral>(lit, m.materials, lambda);
-    const float3 x_last = xyz(vertex_row);
-    const float reach = length(x_last - p);
-    const float cos_in = fabsf(dot(dir, geometric));
-    float density = ray_pdf * cos_in / (reach * reach);
-    float back_reach = mis.z / (reach * reach);
-    // The first surface of a path from afar: its density on the disk's shadow, and the
-    // light's "point" is a direction (no distance to convert).
-    if (total == 0u && (emitter & kAfarEmitter)) {
-        density = afar_first_density(k, p, -dir, cos_in);
-        back_reach = 1.0f;
-        if (!(density > 0.0f)) return;
-    }
-    const float cos_shading_in = dot(toward_light, normal);
-    if (cos_shading_in <= 0.0f || cos_in < 1e-6f) return;
-    const float shading_in = cos_shading_in / cos_in;
-    const float L = (float)m.light_paths;
-
-    if (on_film) {
-        const float3 to_camera = -to_point;
-        const float side = dot(to_camera, geometric);
-        Surface seen = side > 0.0f ? lit : turned(lit);
-        const float3 wo = to_local(seen, to_camera), wi = to_local(seen, toward_light);
-        if ((dot(toward_light, seen.geometric) > 0.0f) == (wi.z > 0.0f) && wo.z > 0.0f) {
-            if (side > 0.0f) orient_surface(seen, wo);
-            else prepare_surface<kSpectral>(seen, wo, lambda, m.materials);
-            float camera_bsdf_pdf;
-            const float4 f = evaluate_surface(seen, wi, wo, camera_bsdf_pdf);
-            const float camera_density = camera_pdf(m, to_point) * fabsf(side) / (camera_distance * camera_distance);
-            const float4 contribution = throughput * f * (shading_in * camera_density / L);
-            if (spec_max<kSpectral>(contribution) > 0.0f) {
-                const float last = mis.y > 0.0f ? camera_bsdf_pdf * back_reach / mis.y : 0.0f;
-                const float ratio = mis.x * last * camera_density / density;
-                const float sample_ratio = total == 0u ? light_sample_ratio(m, k, emitter, seen.normal, seen.geometric, p, x_last,
-                                                                            toward_light, camera_bsdf_pdf)
-                                                       : fmaxf(mis.w, 0.0f);
-                const float weight = mis_weight(ratio / L, ratio * sample_ratio / L);
-                const float margin = 4e-4f * fmaxf(1.0f, fmaxf(fabsf(p.x), fmaxf(fabsf(p.y), fabsf(p.z))));
-                const float3 so = offset_origin(p, seen.geometric);
-                const float3 value = spec_to_film<kSpectral>(contribution * weight, lambda, k);
-                out.shadow = true;
-                out.so = make_float4(so.x, so.y, so.z, ro.w);
-                out.sd = make_float4(to_camera.x, to_camera.y, to_camera.z, fmaxf(0.0f, camera_distance - margin));
-                out.sc = make_float4(value.x, value.y, value.z, __uint_as_float(pixel));
-            }
+// A block-wide push of the threads that `want`, grouped by `key` (0..7): one atomic on
+// `counter` for the block, each key's rays contiguous in key order; returns this
+// thread's slot. Every thread of the block calls it; `bins` is shared scratch (9 words).
+__device__ __forceinline__ uint32_t block_push(uint32_t *counter, bool want, uint32_t key, uint32_t *bins) {
+    if (threadIdx.x < 9u) bins[threadIdx.x] = 0u;
+    __syncthreads();
+    const uint32_t rank = want ? atomicAdd(&bins[key], 1u) : 0u;
+    __syncthreads();
+    if (threadIdx.x == 0u) {
+        uint32_t total = 0;
+        for (uint32_t b = 0; b < 8u; b++) {
+            const uint32_t n = bins[b];
+            bins[b] = total;
+            total += n;
         }
+        bins[8] = total ? atomicAdd(counter, total) : 0u;
     }
-
-    // Scatter on, unless the next vertex would be past the bounce limit.
-    if (total + 1u >= k.max_bounces) return;
-    const float4 u = sample4(k.seed, id, sample, group_bsdf(total));
-    Surface choosing = lit;
-    light_lobes(choosing);
-    const float3 wo_light = to_local(lit, toward_light);
-    float3 wi_light;
-    float light_pdf;
-    uint32_t lobe;
-    if (!sample_direction(choosing, wo_light, make_float3(u.x, u.y, u.w), wi_light, light_pdf, lobe)) return;
-    const float3 direction = to_world(lit, wi_light);
-    const float side = dot(direction, geometric);
-    if ((side > 0.0f) != (wi_light.z > 0.0f)) return;
-    Surface seen = side > 0.0f ? lit : turned(lit);
-    const float3 wo = to_local(seen, direction), wi = to_local(seen, toward_light);
-    if ((dot(toward_light, seen.geometric) > 0.0f) != (wi.z > 0.0f)) return;
-    if (side > 0.0f) orient_surface(seen, wo);
-    else prepare_surface<kSpectral>(seen, wo, lambda, m.materials);
-    float camera_bsdf_pdf;
-    const float4 f = evaluate_surface(seen, wi, wo, camera_bsdf_pdf);
-    const uint32_t next_bounces = next_bounce(bounces, lobe, k.limits);
-    if (next_bounces == kNone) return;
-    throughput = throughput * f * (shading_in * fabsf(side) / light_pdf);
-    const float survival_scale = vertex_row.w;
-    if (total + 1u >= 3u) {
-        const float survive = fminf(0.95f, spec_max<kSpectral>(throughput) * survival_scale);
-        if (u.z >= survive) return;
-        throughput = make_float4(throughput.x / survive, throughput.y / survive, throughput.z / survive, throughput.w / survive);
-    }
-    if (!(spec_max<kSpectral>(throughput) > 0.0f)) return;
-    const float last = mis.y > 0.0f ? camera_bsdf_pdf * back_reach / mis.y : 0.0f;
-    const float sample_ratio =
-        total == 0u ? light_sample_ratio(m, k, emitter, seen.normal, seen.geometric, p, x_last, toward_light, camera_bsdf_pdf)
-                    : mis.w;
-    const float3 next = offset_origin(p, side > 0.0f ? geometric : -geometric);
-    w.path[path] = make_uint4(emitter, next_bounces, 0u, __float_as_uint(light_pdf));
-    w.throughput[path] = throughput;
-    w.vertex[path] = make_float4(p.x, p.y, p.z, survival_scale);
-    w.mis[path] = make_float4(mis.x * last, density, fabsf(side), sample_ratio);
-    out.next = true;
-    out.o = make_float4(next.x, next.y, next.z, ro.w);
-    out.d = make_float4(direction.x, direction.y, direction.z, kInfinity);
+    __syncthreads();
+    const uint32_t slot = bins[8] + bins[key] + rank;
+    __syncthreads();  // the next push rewrites the bins
+    return slot;
 }
 
 // Sorting keys of a shading tile: 0 for misses and light hits, 1 .. kSortBins - 2 for
@@ -1348,7 +181,12 @@ __global__ void __launch_bounds__(kShadeBlock, kGlossy ? 4 : 8) shade_kernel(Wav
     const uint32_t stride = gridDim.x * blockDim.x;
     uint32_t *next_counter = kLight ? light_counter(w, round + 1) : &w.counters[round + 1];
     uint32_t *shadow_counter = &w.counters[w.rounds + 1 + round];
-    // Shades queue entry k (all threads of the warp call it: the pushes are warp-wide).
+    // Outgoing rays are binned by octant in the rounds the plan's interval names (0: never).
+    const uint32_t interval = w.plan->head.bin_interval;
+    const bool binned = interval != 0u && round % interval == 0u;
+    __shared__ uint32_t bins[kSortBins];
+    // Shades queue entry k (all threads of the block call it: the pushes are warp- or
+    // block-wide).
     auto shade = [&](uint32_t k) {
         const uint32_t i = kLight ? w.pool - 1u - k : k;
         ShadeOut out;
@@ -1358,44 +196,58 @@ __global__ void __launch_bounds__(kShadeBlock, kGlossy ? 4 : 8) shade_kernel(Wav
             const Member &m = w.members[sg.member];
             if (kLight) {
                 if (kGlossy && m.glossy) {
-                    if (m.spectral) shade_light_glossy<true>(w, m, sg.sample, round, i, ro, out);
-                    else shade_light_glossy<false>(w, m, sg.sample, round, i, ro, out);
+                    if (m.spectral) light_layered<true>(w, m, sg.sample, round, i, ro, out);
+                    else light_layered<false>(w, m, sg.sample, round, i, ro, out);
                 } else if (m.spectral) {
-                    shade_light<true>(w, m, sg.sample, round, i, ro, out);
+                    light_diffuse<true>(w, m, sg.sample, round, i, ro, out);
                 } else {
-                    shade_light<false>(w, m, sg.sample, round, i, ro, out);
+                    light_diffuse<false>(w, m, sg.sample, round, i, ro, out);
                 }
+            } else if (kGlossy && m.glossy) {
+                if (m.spectral) camera_layered<true>(w, m, sg.sample, round, i, ro, out);
+                else camera_layered<false>(w, m, sg.sample, round, i, ro, out);
             } else if (m.spectral) {
-                shade_one<true, kTracing, kGlossy>(w, m, sg.sample, round, i, ro, out);
+                shade_camera_path<true, kTracing, DiffuseOps>(w, m, sg.sample, round, i, ro, out);
             } else {
-                shade_one<false, kTracing, kGlossy>(w, m, sg.sample, round, i, ro, out);
+                shade_camera_path<false, kTracing, DiffuseOps>(w, m, sg.sample, round, i, ro, out);
             }
             // Past the member's last round (cut-outs passed at its last bounces) a ray is
             // not traced, as the reference's pass loop ends there.
             if (round + 1u >= m.rounds) out.next = false;
         }
-        const uint32_t at = warp_push(next_counter, out.next);
+        uint32_t at, sat;
+        if (binned) {
+            // The block's rays, grouped by direction octant in the queue: the traversal's
+            // warps then take rays that order every node's children alike.
+            at = block_push(next_counter, out.next, octant_of(out.d), bins);
+            sat = block_push(shadow_counter, out.shadow, octant_of(out.sd), bins);
+        } else {
+            at = warp_push(next_counter, out.next);
+            sat = warp_push(shadow_counter, out.shadow);
+        }
         if (out.next) {
             const uint32_t slot = kLight ? w.pool - 1u - at : at;
             w.ray_o[nq][slot] = out.o;
             w.ray_d[nq][slot] = out.d;
         }
-        const uint32_t sat = warp_push(shadow_counter, out.shadow);
         if (out.shadow) {
             w.shadow_o[sat] = out.so;
             w.shadow_d[sat] = out.sd;
             w.shadow_c[sat] = out.sc;
         }
     };
-    if constexpr (kGlossy) {
-        // Layered surfaces branch by material: each block tile of the queue is ordered by
-        // what its entries shade before its warps take them, so a warp's lanes mostly
-        // follow one path through the lobes.
-        __shared__ uint32_t bins[kSortBins], order[kShadeBlock];
-        for (uint32_t tile = blockIdx.x * blockDim.x; tile < count; tile += stride)
+    // Every block takes tiles of blockDim.x queue entries (block-uniform, so a block may
+    // sort them, or its outgoing rays, in shared memory).
+    for (uint32_t tile = blockIdx.x * blockDim.x; tile < count; tile += stride) {
+        if constexpr (kGlossy) {
+            // Layered surfaces branch by material: each tile is ordered by what its entries
+            // shade before its warps take them, so a warp's lanes mostly follow one path
+            // through the lobes.
+            __shared__ uint32_t order[kShadeBlock];
             shade(tile + tile_order(w, q, tile, count, kLight, bins, order));
-    } else {
-        for (uint32_t k = blockIdx.x * blockDim.x + threadIdx.x; k - (threadIdx.x & 31u) < count; k += stride) shade(k);
+        } else {
+            shade(tile + threadIdx.x);
+        }
     }
 }
 
@@ -1734,6 +586,14 @@ struct WaveHost {
     // Tunables (lr_batch_tune): the BVH width asked for each scene-size class (0: the
     // default) and the most paths a pass takes.
     int class_width[kSizeClasses] = {0, 0, 0};
+    // ... the traversal kernels' block size (0: kTraceBlock) and the stack entries (0: the
+    // members' bound; a larger choice only when the tuner found it faster) per class.
+    int class_block[kSizeClasses] = {0, 0, 0};
+    int class_stack[kSizeClasses] = {0, 0, 0};
+    // Rounds whose outgoing rays the shade kernels group by direction octant: multiples of
+    // this (0: none). The wavefront compacts every round (warp- or block-aggregated
+    // pushes); this is how often it also sorts.
+    uint32_t bin_interval = 0;
     uint32_t fill = 0;
     // The most camera paths a pass takes (0: as many as fit): a renderer's band, so that
     // its passes are the reference's bands, light paths riding along in a sample's first.
@@ -1773,16 +633,15 @@ void mark(cudaStream_t stream, Marks *marks, int kind) {
     marks->push_back({e, kind});
 }
 
-// Records a pass's tracing on `stream` with traversal variant (W, kStack): camera, then
-// (closest, shade, shadow) for every round. With `marks`, an event follows each kernel
-// (profiling); kCount instantiates the counting traversals.
-template <int W, int kStack, bool kCount>
-void record_trace(const WaveHost *h, const Wave &w, int grid_trace, bool tracing, bool glossy, bool cutouts,
-                  cudaStream_t stream, Marks *marks) {
+// Records a pass's tracing on `stream` with traversal (width, stack entries) in blocks of
+// `block` threads: camera, then (closest, shade, shadow) for every round. With `marks`,
+// an event follows each kernel (profiling); `count` takes the counting traversals.
+void record_trace(const WaveHost *h, const Wave &w, int width, int stack, int block, bool count, int grid_trace,
+                  bool tracing, bool glossy, bool cutouts, cudaStream_t stream, Marks *marks) {
     camera_kernel<<<h->grid_shade, kShadeBlock, 0, stream>>>(w);
     mark(stream, marks, kCamera);
     for (uint32_t round = 0; round < w.rounds; round++) {
-        launch_closest(W, kStack, kCount, grid_trace, stream, w, round);
+        launch_closest(width, stack, block, count, grid_trace, stream, w, round);
         mark(stream, marks, kClosest);
         if (glossy) {
             if (tracing) {
@@ -1798,7 +657,7 @@ void record_trace(const WaveHost *h, const Wave &w, int grid_trace, bool tracing
             shade_kernel<false, false, false><<<h->grid_shade, kShadeBlock, 0, stream>>>(w, round);
         }
         mark(stream, marks, kSurface);
-        launch_shadow(W, kStack, kCount, cutouts, grid_trace, stream, w, round);
+        launch_shadow(width, stack, block, count, cutouts, grid_trace, stream, w, round);
         mark(stream, marks, kShadow);
     }
     LR_CUDA(cudaGetLastError());
@@ -1818,38 +677,42 @@ void record_finish(const WaveHost *h, const Wave &w, cudaStream_t stream, Marks 
     LR_CUDA(cudaGetLastError());
 }
 
-int trace_grid(int variant, int sms) { return closest_grid(variant / 1000, variant % 1000, sms); }
+// The traversal kernels' block sizes the autotuner tries; a variant names one by index.
+constexpr int kTraceBlocks[3] = {kTraceBlock, 64, 256};
 
-int grid_for(WaveHost *h, int variant) {
-    auto it = h->grid_trace.find(variant);
+// A pass's variant: its traversal (BVH width * 1000 + stack entries), plus kTracingVariant
+// when it holds light tracing, kGlossyVariant when it holds glossy materials,
+// kCutoutVariant when it holds cut-outs, and kBlockVariant times the index of the
+// traversal kernels' block size in kTraceBlocks.
+constexpr int kTracingVariant = 100000, kGlossyVariant = 200000, kCutoutVariant = 400000, kBlockVariant = 800000;
+
+int variant_block(int variant) { return kTraceBlocks[(variant / kBlockVariant) % 3]; }
+
+bool traversal_exists(int width, int stack) {
+    switch (width * 1000 + stack) {
+#define LR_CASE(wd, k) case wd * 1000 + k:
+        LR_TRAVERSALS(LR_CASE)
+#undef LR_CASE
+        return true;
+        default: return false;
+    }
+}
+
+int grid_for(WaveHost *h, int width, int stack, int block) {
+    const int key = width * 1000 + stack + block * 100000;
+    auto it = h->grid_trace.find(key);
     if (it != h->grid_trace.end()) return it->second;
-    const int g = trace_grid(variant, h->ctx->sm_count);
-    h->grid_trace[variant] = g;
+    const int g = closest_grid(width, stack, block, h->ctx->sm_count);
+    h->grid_trace[key] = g;
     return g;
 }
 
-// A pass's variant: its traversal (BVH width * 1000 + stack entries), plus kTracingVariant
-// when it holds light tracing, kGlossyVariant when it holds glossy materials and
-// kCutoutVariant when it holds cut-outs.
-constexpr int kTracingVariant = 100000, kGlossyVariant = 200000, kCutoutVariant = 400000;
-
 void record_trace_any(WaveHost *h, const Wave &w, int variant, cudaStream_t stream, Marks *marks) {
-    const bool count = h->profile == 2;
-    const bool tracing = (variant / kTracingVariant) & 1;
-    const bool glossy = (variant / kTracingVariant) & 2;
-    const bool cutouts = (variant / kTracingVariant) & 4;
+    const int flags = (variant / kTracingVariant) & 7;
     const int traversal = variant % kTracingVariant;
-    const int grid = grid_for(h, traversal);
-    switch (traversal) {
-#define LR_CASE(wd, k)                                                                        \
-    case wd * 1000 + k:                                                                       \
-        if (count) record_trace<wd, k, true>(h, w, grid, tracing, glossy, cutouts, stream, marks); \
-        else record_trace<wd, k, false>(h, w, grid, tracing, glossy, cutouts, stream, marks);      \
-        break;
-        LR_TRAVERSALS(LR_CASE)
-#undef LR_CASE
-        default: fail(LR_LIMIT, "no traversal variant for this scene");
-    }
+    const int width = traversal / 1000, stack = traversal % 1000, block = variant_block(variant);
+    const int grid = grid_for(h, width, stack, block);
+    record_trace(h, w, width, stack, block, h->profile >= 2, grid, flags & 1, flags & 2, flags & 4, stream, marks);
 }
 
 // Captures whatever `body` queues on a private stream as a graph.
@@ -2067,11 +930,18 @@ size_t staged_bytes(const Layout &lay) {
     return bytes;
 }
 
-// A member's loaded records (lights, light tree, materials, constants) from `L`.
+// A member's loaded records from `L`, in the layouts the kernels read: the emitter table
+// (lights, the finite and from-afar index lists, the textured dome's image), the light
+// tree's pair records, emitter records and triangle map, the per-material codes, the
+// constants. The vectors hold the host copies until they are staged.
 struct LoadedRecords {
     Constants k{};
     Layout lay;
-    size_t lights = 0, nodes = 0, links = 0, records = 0, map = 0, materials = 0, constants = 0;
+    DeviceLights lights;
+    DeviceTree tree;
+    std::vector<float> codes;
+    size_t p_lights = 0, p_finite = 0, p_afar = 0, p_texels = 0, p_cdf = 0, p_pairs = 0, p_records = 0, p_map = 0,
+           p_codes = 0, p_constants = 0;
 };
 
 void loaded_records(const Loaded &L, const lr_settings &settings, double emit_share, LoadedRecords &r) {
@@ -2096,29 +966,51 @@ void loaded_records(const Loaded &L, const lr_settings &settings, double emit_sh
     k.emit_radius = (float)L.emit_radius;
     k.emit_center = make_float3((float)L.emit_center.x, (float)L.emit_center.y, (float)L.emit_center.z);
     k.noise_threshold = (float)std::max(0.0, settings.noise_threshold);
-    r.lights = r.lay.add(L.lights.rows.data(), L.lights.rows.size() * 4);
-    r.nodes = r.lay.add(L.tree.nodes.data(), L.tree.nodes.size() * 4);
-    r.links = r.lay.add(L.tree.links.data(), L.tree.links.size() * 4);
-    r.records = r.lay.add(L.tree.records.data(), L.tree.records.size() * 4);
-    r.map = r.lay.add(L.tree.triangle_map.data(), L.tree.triangle_map.size() * 4);
-    r.materials = r.lay.add(L.materials.data(), L.materials.size() * 4);
-    r.constants = r.lay.add(&k, sizeof k);
+    r.lights = device_lights(L.lights);
+    r.tree = device_tree(L.tree);
+    for (const lr_openpbr &material : L.library) material_code(material, r.codes);
+    static_assert(sizeof(DeviceLight) == 32 * 4 && sizeof(TreePair) == 24 * 4 && sizeof(MaterialCode) == 64 * 4,
+                  "device record sizes");
+    r.p_lights = r.lay.add(r.lights.records.data(), r.lights.records.size() * 4);
+    r.p_finite = r.lay.add(r.lights.finite.data(), r.lights.finite.size() * 4);
+    r.p_afar = r.lay.add(r.lights.afar.data(), r.lights.afar.size() * 4);
+    r.p_texels = r.lay.add(r.lights.dome_texels.data(), r.lights.dome_texels.size() * 4);
+    r.p_cdf = r.lay.add(r.lights.dome_cdf.data(), r.lights.dome_cdf.size() * 4);
+    r.p_pairs = r.lay.add(r.tree.pairs.data(), r.tree.pairs.size() * 4);
+    r.p_records = r.lay.add(L.tree.records.data(), L.tree.records.size() * 4);
+    r.p_map = r.lay.add(L.tree.triangle_map.data(), L.tree.triangle_map.size() * 4);
+    r.p_codes = r.lay.add(r.codes.data(), r.codes.size() * 4);
+    r.p_constants = r.lay.add(&k, sizeof k);
 }
 
 // Points `m` at its loaded records in `block`.
 void set_loaded(Member &m, const LoadedRecords &r, const Loaded &L, void *block, const lr_settings &settings,
                 uint32_t rounds) {
     auto at = [&](size_t i) { return (void *)((char *)block + r.lay.parts[i].offset); };
-    m.lights = (const float4 *)at(r.lights);
-    m.light_count = (uint32_t)L.lights.count;
+    LightTable &T = m.lights;
+    T = LightTable{};
+    T.light = (const DeviceLight *)at(r.p_lights);
+    T.count = (uint32_t)L.lights.count;
+    T.finite = (const uint32_t *)at(r.p_finite);
+    T.finite_count = (uint32_t)r.lights.finite.size();
+    T.afar = (const uint32_t *)at(r.p_afar);
+    T.afar_count = (uint32_t)r.lights.afar.size();
+    if (r.lights.dome_light != kNone) {
+        T.dome.texels = (const float4 *)at(r.p_texels);
+        T.dome.cdf = (const float *)at(r.p_cdf);
+        T.dome.width = r.lights.dome_width;
+        T.dome.height = r.lights.dome_height;
+        T.dome.light = r.lights.dome_light;
+        T.dome.weight_sum = r.lights.dome_weight_sum;
+    }
     m.spectral = settings.spectral ? 1u : 0u;
-    m.tree.nodes = (const float4 *)at(r.nodes);
-    m.tree.links = (const uint2 *)at(r.links);
-    m.tree.records = (const uint4 *)at(r.records);
-    m.tree.triangle_map = L.tree.triangle_map.empty() ? nullptr : (const uint32_t *)at(r.map);
-    m.tree.node_count = (uint32_t)L.tree.node_count;
-    m.materials = (const float4 *)at(r.materials);
-    m.k = (const Constants *)at(r.constants);
+    m.tree = TreeTable{};
+    m.tree.pairs = (const TreePair *)at(r.p_pairs);
+    m.tree.records = (const uint4 *)at(r.p_records);
+    m.tree.triangle_map = L.tree.triangle_map.empty() ? nullptr : (const uint32_t *)at(r.p_map);
+    m.tree.root = r.tree.root;
+    m.materials = (const MaterialCode *)at(r.p_codes);
+    m.k = (const Constants *)at(r.p_constants);
     m.glossy = L.glossy ? 1u : 0u;
     m.cutouts = L.cutouts ? 1u : 0u;
     m.rounds = rounds;
@@ -2555,9 +1447,14 @@ bool launch_pass(WaveHost *h, bool dry = false, int only = -1) {
                                     [&](const std::pair<uint32_t, bool> &e) { return h->members[e.first].dev.glossy != 0u; });
     const bool cutouts = std::any_of(rec.members.begin(), rec.members.end(),
                                      [&](const std::pair<uint32_t, bool> &e) { return h->members[e.first].dev.cutouts != 0u; });
+    // The class's tuned stack, where the width's variants offer it and it holds the bound.
+    const int tuned_stack = h->class_stack[dominant];
+    if (tuned_stack > stack && traversal_exists(width, tuned_stack)) stack = tuned_stack;
+    const int block = h->class_block[dominant] ? h->class_block[dominant] : kTraceBlock;
+    const int block_index = block == kTraceBlocks[1] ? 1 : (block == kTraceBlocks[2] ? 2 : 0);
     const int variant = width * 1000 + stack + (tracing ? kTracingVariant : 0) + (glossy ? kGlossyVariant : 0) +
-                        (cutouts ? kCutoutVariant : 0);
-    staging->head = PlanHeader{n, used, converts, dry ? 1u : 0u, camera_paths, folds, adapts, 0u};
+                        (cutouts ? kCutoutVariant : 0) + block_index * kBlockVariant;
+    staging->head = PlanHeader{n, used, converts, dry ? 1u : 0u, camera_paths, folds, adapts, h->bin_interval};
     staging->display = PlanDisplay{0ull, h->display_scale, h->display_view, 0u, 0u};
     if (h->display_block && converts > 0) {
         rec.display_slot = free_display_slot(h);
@@ -2689,6 +1586,23 @@ double time_dry(WaveHost *h, int only, cudaEvent_t a, cudaEvent_t b) {
 // present, the BVH width (2, 4, 8; a width all its members fall back from is skipped)
 // whose passes of that class alone run fastest; then, with those widths, the pool fill
 // (a quarter, half or all of the pool) of the mixed passes.
+// The stacks of width `width`'s traversal variants that hold `bound` entries, smallest
+// first.
+std::vector<int> stacks_for(int width, int bound) {
+    std::vector<int> out;
+#define LR_CASE(wd, k) \
+    if (wd == width && k >= bound) out.push_back(k);
+    LR_TRAVERSALS(LR_CASE)
+#undef LR_CASE
+    std::sort(out.begin(), out.end());
+    return out;
+}
+
+// lr_batch_tune: per scene-size class, dry passes of that class's members alone at every
+// BVH width, every stack depth its variants offer above the members' bound, and the
+// traversal kernels at 64, 128 and 256 threads a block -- the fastest kept; then the
+// mixed passes at pool fill 1/4, 1/2 and all, and the interval at which the shade kernels
+// group outgoing rays by octant (never, every round, every second round).
 void wave_tune(WaveHost *h, lr_batch_tuning *out) {
     settle(h);
     if (!std::any_of(h->members.begin(), h->members.end(), has_work))
@@ -2699,6 +1613,7 @@ void wave_tune(WaveHost *h, lr_batch_tuning *out) {
     LR_CUDA(cudaEventCreate(&b));
     uint32_t tried = 0;
     h->fill = h->pool;
+    h->bin_interval = 0;
     for (int cls = 0; cls < kSizeClasses; cls++) {
         uint32_t members = 0;
         for (auto &mh : h->members)
@@ -2706,27 +1621,44 @@ void wave_tune(WaveHost *h, lr_batch_tuning *out) {
         if (out) out->class_members[cls] = members;
         if (!members) continue;
         double best = -1.0;
-        int best_width = 2;
+        int best_width = 2, best_stack = 0, best_block = 0;
         std::vector<std::vector<int>> seen;
         for (int width : {2, 4, 8}) {
             std::vector<int> got;
+            int effective = 2, bound = 0;
             for (auto &mh : h->members)
                 if (has_work(mh) && size_class(mh.dev.scene.triangle_count) == cls) {
                     const TraversalChoice c = choose_traversal(mh.dev.scene, width);
                     got.push_back(c.width * 1000 + c.stack);
+                    effective = c.width;
+                    bound = std::max(bound, c.stack);
                 }
             if (std::find(seen.begin(), seen.end(), got) != seen.end()) continue;
             seen.push_back(got);
             h->class_width[cls] = width;
-            const double rate = time_dry(h, cls, a, b);
-            tried++;
-            if (rate > best) {
-                best = rate;
-                best_width = width;
+            for (int stack : stacks_for(effective, bound)) {
+                for (int block : kTraceBlocks) {
+                    h->class_stack[cls] = stack;
+                    h->class_block[cls] = block;
+                    const double rate = time_dry(h, cls, a, b);
+                    tried++;
+                    if (rate > best) {
+                        best = rate;
+                        best_width = width;
+                        best_stack = stack;
+                        best_block = block;
+                    }
+                }
             }
         }
         h->class_width[cls] = best_width;
-        if (out) out->class_width[cls] = (uint32_t)best_width;
+        h->class_stack[cls] = best_stack;
+        h->class_block[cls] = best_block;
+        if (out) {
+            out->class_width[cls] = (uint32_t)best_width;
+            out->class_stack[cls] = (uint32_t)best_stack;
+            out->class_block[cls] = (uint32_t)best_block;
+        }
     }
     double best = -1.0;
     uint32_t best_fill = h->pool;
@@ -2740,13 +1672,25 @@ void wave_tune(WaveHost *h, lr_batch_tuning *out) {
             best_fill = fill;
         }
     }
+    h->fill = best_fill;
+    uint32_t best_interval = 0;
+    for (uint32_t interval : {1u, 2u}) {
+        h->bin_interval = interval;
+        const double rate = time_dry(h, -1, a, b);
+        tried++;
+        if (rate > best) {
+            best = rate;
+            best_interval = interval;
+        }
+    }
+    h->bin_interval = best_interval;
     cudaEventDestroy(a);
     cudaEventDestroy(b);
-    h->fill = best_fill;
     if (out) {
         out->fill = best_fill;
         out->paths_per_ms = best;
         out->candidates = tried;
+        out->bin_interval = best_interval;
         int widest = 0;
         for (int cls = 0; cls < kSizeClasses; cls++) widest = std::max(widest, h->class_width[cls]);
         out->width = (uint32_t)(widest ? widest : 2);

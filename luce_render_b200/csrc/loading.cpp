@@ -381,6 +381,215 @@ LightTree build_light_tree(const Scene &scene, const LightRecords &lights, const
     return tree;
 }
 
+namespace {
+
+float bits_of(uint32_t v) {
+    float f;
+    std::memcpy(&f, &v, 4);
+    return f;
+}
+
+uint32_t uint_of(float f) {
+    uint32_t v;
+    std::memcpy(&v, &f, 4);
+    return v;
+}
+
+}  // namespace
+
+DeviceLights device_lights(const LightRecords &records) {
+    DeviceLights out;
+    out.records.assign(records.count * 32, 0.0f);
+    for (size_t i = 0; i < records.count; i++) {
+        const float *row = &records.rows[i * 28];
+        float *d = &out.records[i * 32];
+        const uint32_t shape = (uint32_t)row[3];
+        const V3 u(row[4], row[5], row[6]), v(row[8], row[9], row[10]);
+        for (int k = 0; k < 3; k++) {
+            d[k] = row[k];          // centre
+            d[4 + k] = row[4 + k];  // half edge u, or the dome frame's x axis
+            d[8 + k] = row[8 + k];  // half edge v, or its y axis
+            d[12 + k] = row[12 + k];  // the direction light leaves along, or the frame's z axis
+        }
+        d[3] = bits_of(shape);
+        d[15] = row[15];  // area
+        if (shape == 0u || shape == 1u) {
+            const double uu = u.dot(u), vv = v.dot(v);
+            d[7] = uu > 0.0 ? (float)(1.0 / uu) : 0.0f;
+            d[11] = vv > 0.0 ? (float)(1.0 / vv) : 0.0f;
+            out.finite.push_back((uint32_t)i);
+        } else if (shape == 2u) {
+            const float r = row[7];
+            d[16] = r;
+            d[17] = r * r;
+            out.finite.push_back((uint32_t)i);
+        } else {
+            out.afar.push_back((uint32_t)i);
+            if (shape == 3u) {
+                const float cos_half = row[11];
+                const bool delta = cos_half >= 1.0f - 1e-7f;
+                d[16] = cos_half;
+                d[17] = delta ? 1.0f : (float)(1.0 / (2.0 * kPi * (1.0 - (double)cos_half)));
+                d[18] = delta ? 1.0f : 0.0f;
+            }
+        }
+        for (int k = 0; k < 4; k++) d[20 + k] = row[16 + k];  // spectral fit
+        for (int k = 0; k < 3; k++) d[24 + k] = row[20 + k];  // ACEScg radiance
+        d[27] = bits_of((uint32_t)row[23]);                   // flags
+        d[28] = row[24];                                      // kelvin
+        d[29] = row[25];                                      // share among lights from afar
+        d[30] = row[26];                                      // cumulative share
+        d[31] = bits_of(shape < 3u ? (uint32_t)row[27] : 0u);  // the tree's emitter (finite lights)
+    }
+    if (records.dome >= 0) {
+        // pack_lights keeps the textured dome's image after the records and says where in
+        // the dome's own record (see there).
+        const float *row = &records.rows[(size_t)records.dome * 28];
+        out.dome_light = (uint32_t)records.dome;
+        out.dome_weight_sum = row[0];
+        out.dome_width = uint_of(row[11]);
+        out.dome_height = uint_of(row[15]);
+        const size_t texel_base = (size_t)uint_of(row[7]) * 4, cdf_base = uint_of(row[27]);
+        const size_t texels = (size_t)out.dome_width * out.dome_height;
+        out.dome_texels.assign(records.rows.begin() + (long)texel_base, records.rows.begin() + (long)(texel_base + texels * 4));
+        out.dome_cdf.assign(records.rows.begin() + (long)cdf_base,
+                            records.rows.begin() + (long)(cdf_base + texels + out.dome_height));
+        float *d = &out.records[(size_t)records.dome * 32];
+        d[0] = d[1] = d[2] = 0.0f;  // the slots pack_lights borrowed
+        d[7] = d[11] = d[15] = 0.0f;
+        d[31] = 0.0f;  // a dome is no emitter of the tree
+    }
+    return out;
+}
+
+DeviceTree device_tree(const LightTree &tree) {
+    DeviceTree out;
+    if (tree.node_count == 0) return out;
+    // Pair slots for the interior nodes, in node order.
+    std::vector<uint32_t> slot(tree.node_count, 0xffffffffu);
+    uint32_t pairs = 0;
+    for (size_t n = 0; n < tree.node_count; n++)
+        if (!(tree.links[n * 2 + 1] & kLeafNode)) slot[n] = pairs++;
+    auto lead = [&](size_t n) {
+        return (tree.links[n * 2 + 1] & kLeafNode) ? (0x80000000u | tree.links[n * 2]) : slot[n];
+    };
+    out.root = lead(0);
+    out.pairs.assign((size_t)pairs * 24, 0.0f);
+    for (size_t n = 0; n < tree.node_count; n++) {
+        if (slot[n] == 0xffffffffu) continue;
+        float *pair = &out.pairs[(size_t)slot[n] * 24];
+        for (int side = 0; side < 2; side++) {
+            const size_t child = tree.links[n * 2] + (size_t)side;
+            const float *b = &tree.nodes[child * 12];  // lo, power; hi, cos theta_o; axis, cos theta_e
+            const V3 lo(b[0], b[1], b[2]), hi(b[4], b[5], b[6]);
+            const V3 centre = (lo + hi) * 0.5;
+            float *c = pair + side * 4, *a = pair + 8 + side * 4, *k = pair + 16 + side * 4;
+            c[0] = (float)centre.x;
+            c[1] = (float)centre.y;
+            c[2] = (float)centre.z;
+            c[3] = (float)(0.5 * (hi - lo).length());
+            a[0] = b[8];
+            a[1] = b[9];
+            a[2] = b[10];
+            a[3] = b[3];
+            const double cos_o = b[7];
+            k[0] = b[7];
+            k[1] = (float)std::sqrt(std::max(0.0, 1.0 - cos_o * cos_o));
+            k[2] = b[11];
+            k[3] = bits_of(lead(child));
+        }
+    }
+    return out;
+}
+
+namespace {
+
+double clamp01(double v) { return std::min(std::max(v, 0.0), 1.0); }
+
+// OpenPBR's GGX widths (x, y) from roughness and anisotropy.
+void ggx_widths(double roughness, double anisotropy, float out[2]) {
+    const double squeeze = 1.0 - anisotropy;
+    const double t = roughness * roughness * std::sqrt(2.0 / (1.0 + squeeze * squeeze));
+    out[0] = (float)std::max(t, 1e-4);
+    out[1] = (float)std::max(squeeze * t, 1e-4);
+}
+
+// The hemispherical average of a dielectric's Fresnel reflectance (the closed fit of
+// OpenPBR's reference code), computed in single precision as the kernels would.
+float fresnel_mean(float eta) {
+    return std::log((10893.0f * eta - 1438.2f) / (-774.4f * eta * eta + 10212.0f * eta + 1.0f));
+}
+
+}  // namespace
+
+void material_code(const lr_openpbr &m, std::vector<float> &out) {
+    const size_t at = out.size();
+    out.resize(at + 64, 0.0f);
+    float *c = &out[at];
+    auto colour = [&](int slot, const V3 &rgb, double scale, float luma_w) {
+        double fit[4];
+        fit_spectrum(V3(std::max(rgb.x, 0.0), std::max(rgb.y, 0.0), std::max(rgb.z, 0.0)), fit);
+        float *f = c + slot * 8;
+        for (int k = 0; k < 3; k++) f[k] = (float)fit[k];
+        f[3] = (float)(fit[3] * scale);
+        f[4] = (float)(rgb.x * scale);
+        f[5] = (float)(rgb.y * scale);
+        f[6] = (float)(rgb.z * scale);
+        f[7] = luma_w;
+    };
+    const V3 base(m.base_color[0], m.base_color[1], m.base_color[2]);
+    const V3 spec(m.specular_color[0], m.specular_color[1], m.specular_color[2]);
+    const V3 trans(m.transmission_color[0], m.transmission_color[1], m.transmission_color[2]);
+    const V3 coat(m.coat_color[0], m.coat_color[1], m.coat_color[2]);
+    const V3 glow = V3(m.emission_color[0], m.emission_color[1], m.emission_color[2]) * m.emission_luminance;
+    auto lum = [](const V3 &v) { return (float)luminance(v); };
+    colour(0, base, m.base_weight, std::max(lum(base * m.base_weight), 0.0f));
+    colour(1, spec, 1.0, std::max(lum(spec), 0.0f));
+    colour(2, trans, 1.0, std::max(lum(trans), 0.05f));
+    colour(3, coat, 1.0, lum(coat));
+    colour(4, glow, 1.0, (float)m.emission_luminance);
+    const double coat_w = clamp01(m.coat_weight);
+    float *w = c + 40;  // weights
+    w[0] = (float)clamp01(m.base_metalness);
+    w[1] = (float)std::max(m.specular_weight, 0.0);
+    w[2] = (float)clamp01(m.transmission_weight);
+    w[3] = (float)coat_w;
+    const double rough = clamp01(m.specular_roughness), coat_rough = clamp01(m.coat_roughness);
+    float *r = c + 44;  // roughnesses
+    r[0] = (float)m.base_diffuse_roughness;
+    r[1] = (float)rough;
+    r[2] = (float)coat_rough;
+    r[3] = (float)clamp01(m.coat_darkening);
+    const double aniso = clamp01(m.specular_roughness_anisotropy);
+    const float coat_eta = (float)std::max(m.coat_ior, 1.0001);
+    const double eta = std::max(m.specular_ior, 1.0001);
+    // The base under the coat: roughened (r^4 + 2 c^4)^(1/4), its index relative to the
+    // coat's; and bare.
+    const double r4 = std::pow(rough, 4.0), c4 = std::pow(coat_rough, 4.0);
+    const double coated_rough = rough * (1.0 - coat_w) + std::min(1.0, std::pow(r4 + 2.0 * c4, 0.25)) * coat_w;
+    double relative = eta / coat_eta;
+    if (relative < 1.0) relative = 1.0 / relative;
+    const float coated_ior = (float)std::max(eta * (1.0 - coat_w) + relative * coat_w, 1.0001);
+    float *coated = c + 48, *bare = c + 52, *coat_lobe = c + 56, *extra = c + 60;
+    ggx_widths(coated_rough, aniso, coated);
+    coated[2] = coated_ior;
+    coated[3] = fresnel_mean(coated_ior);
+    ggx_widths(rough, aniso, bare);
+    bare[2] = (float)eta;
+    bare[3] = fresnel_mean((float)eta);
+    ggx_widths(coat_rough, clamp01(m.coat_roughness_anisotropy), coat_lobe);
+    coat_lobe[2] = coat_eta;
+    coat_lobe[3] = fresnel_mean(coat_eta);
+    double cauchy = 0.0;
+    if (m.transmission_dispersion_scale > 0.0 && m.transmission_dispersion_abbe_number > 0.0 && m.transmission_weight > 0.0)
+        cauchy = (m.specular_ior - 1.0) * m.transmission_dispersion_scale /
+                 (m.transmission_dispersion_abbe_number * (1.0 / (486.1 * 486.1) - 1.0 / (656.3 * 656.3)));
+    extra[0] = (float)m.geometry_opacity;
+    extra[1] = (float)cauchy;
+    extra[2] = (float)eta;
+    extra[3] = (float)aniso;
+}
+
 void pack_material(const lr_openpbr &m, float program, std::vector<float> &out) {
     const V3 colors[5] = {V3(m.base_color[0], m.base_color[1], m.base_color[2]),
                           V3(m.specular_color[0], m.specular_color[1], m.specular_color[2]),

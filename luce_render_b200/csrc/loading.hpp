@@ -54,6 +54,31 @@ struct Loaded {
     V3 cmf_integrals;
 };
 
+// The lights as the integrator's kernels read them (emitters.cuh DeviceLight: 32 floats a
+// light; the bits of integers are stored as floats where a field is one), the finite
+// lights and the lights from afar by index, and the textured dome's image apart.
+struct DeviceLights {
+    std::vector<float> records;
+    std::vector<uint32_t> finite, afar;
+    std::vector<float> dome_texels, dome_cdf;  // 4 floats a texel; cumulative weights
+    uint32_t dome_light = 0xffffffffu, dome_width = 0, dome_height = 0;
+    float dome_weight_sum = 0.0f;
+};
+
+// The light tree as the kernels walk it (lighttree.cuh TreePair: 24 floats per interior
+// node, both children's bounds in the importance test's form), and where a walk starts.
+struct DeviceTree {
+    std::vector<float> pairs;
+    uint32_t root = 0xffffffffu;
+};
+
+// A material as the kernels read it (surface.cuh MaterialCode: 64 floats): what does not
+// depend on the hit, worked out once.
+void material_code(const lr_openpbr &m, std::vector<float> &out);
+
+DeviceLights device_lights(const LightRecords &records);
+DeviceTree device_tree(const LightTree &tree);
+
 Environment environment_of(const std::vector<float> &pixels, uint32_t width, uint32_t height, bool spectral);
 LightRecords pack_lights(const std::vector<lr_light> &lights, const std::vector<std::vector<float>> &images,
                          double radius, bool spectral);

@@ -9,7 +9,7 @@
 // (integrator.cu) take approximate division and flush denormals; nothing here depends on
 // them.
 #include "device.hpp"
-#include "shading.cuh"
+#include "emitters.cuh"
 #include "traverse.cuh"
 #include "wave.cuh"
 
@@ -21,15 +21,15 @@ namespace {
 // hands each warp 32 neighbouring queue entries at a time (neighbouring primary rays,
 // or rays a shading warp pushed together), which keeps its lanes on similar nodes.
 template <int W, int kStack, bool kCount>
-__global__ void __launch_bounds__(kTraceBlock) closest_kernel(Wave w, uint32_t round) {
-    __shared__ int stack[TracerOf<W, false, kStack, kCount>::kInts * kTraceBlock];
+__global__ void __launch_bounds__(kTraceBlockMax) closest_kernel(Wave w, uint32_t round) {
+    extern __shared__ int stack[];  // kInts entries a thread, strided by the block's size
     const uint32_t q = round & 1u;
     const uint32_t cameras = w.counters[round], count = cameras + *light_counter(w, round);
     bool overflow = false;
     Visits visits;
     const float4 *ray_o = w.ray_o[q], *ray_d = w.ray_d[q];
     float4 *hits = w.hits[q];
-    typename TracerOf<W, false, kStack, kCount>::type tr(stack + threadIdx.x, kTraceBlock);
+    typename TracerOf<W, false, kStack, kCount>::type tr(stack + threadIdx.x, blockDim.x);
     const uint32_t step = gridDim.x * blockDim.x;
     for (uint32_t j = blockIdx.x * blockDim.x + threadIdx.x; j < count; j += step) {
         // The camera paths' rays, then the light paths' from the queue's back.
@@ -55,16 +55,8 @@ __global__ void __launch_bounds__(kTraceBlock) closest_kernel(Wave w, uint32_t r
         const bool flow = sg.kind == kLightSegment;  // light paths follow light
         uint32_t what = tr.h.slot >= 0 ? (uint32_t)tr.h.slot : kNone;
         float t = tr.h.t;
-        const float4 *lights = m.lights;
-        const uint32_t light_count = m.light_count;
-        for (uint32_t light = 0; light < light_count; light++) {
-            if (round == 0 && !light_visible(lights, light)) continue;
-            const float tl = intersect_light(lights, light, tr.r.o, tr.r.d, t, flow);
-            if (tl < t) {
-                t = tl;
-                what = kLightHit | light;
-            }
-        }
+        const uint32_t light = nearest_light(m.lights, tr.r.o, tr.r.d, t, round == 0, flow);
+        if (light != kNone) what = kLightHit | light;
         hits[i] = make_float4(t, __uint_as_float(what), tr.h.u, tr.h.v);
     }
     if (overflow) atomicAdd(&w.status[0], 1);
@@ -75,12 +67,12 @@ __global__ void __launch_bounds__(kTraceBlock) closest_kernel(Wave w, uint32_t r
 // path's camera connection, unless a light the camera sees stands in it, splats its value
 // (in the film's terms) on its pixel in the lane's accumulator.
 template <int W, int kStack, bool kCount, bool kCutouts>
-__global__ void __launch_bounds__(kTraceBlock) shadow_kernel(Wave w, uint32_t round) {
-    __shared__ int stack[TracerOf<W, true, kStack, kCount>::kInts * kTraceBlock];
+__global__ void __launch_bounds__(kTraceBlockMax) shadow_kernel(Wave w, uint32_t round) {
+    extern __shared__ int stack[];
     const uint32_t count = w.counters[w.rounds + 1 + round];
     bool overflow = false;
     Visits visits;
-    typename TracerOf<W, true, kStack, kCount>::type tr(stack + threadIdx.x, kTraceBlock);
+    typename TracerOf<W, true, kStack, kCount>::type tr(stack + threadIdx.x, blockDim.x);
     const uint32_t step = gridDim.x * blockDim.x;
     for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < count; i += step) {
         const float4 o = w.shadow_o[i], d = w.shadow_d[i];
@@ -96,12 +88,7 @@ __global__ void __launch_bounds__(kTraceBlock) shadow_kernel(Wave w, uint32_t ro
         const Segment &sg = w.plan->seg[tag >> kPathBits];
         const Member &m = w.members[sg.member];
         const bool light_path = sg.kind == kLightSegment;
-        if (light_path) {
-            bool seen = false;
-            for (uint32_t light = 0; light < m.light_count && !seen; light++)
-                seen = light_visible(m.lights, light) && intersect_light(m.lights, light, xyz(o), xyz(d), d.w, true) < d.w;
-            if (seen) continue;
-        }
+        if (light_path && seen_light_between(m.lights, xyz(o), xyz(d), d.w)) continue;
         const DeviceScene s = m.scene;
         float kept = 1.0f;
         if (kCutouts && m.cutouts) {
@@ -109,7 +96,7 @@ __global__ void __launch_bounds__(kTraceBlock) shadow_kernel(Wave w, uint32_t ro
             // (1 - opacity) of the light at each; anything opaque blocks. Closest hits,
             // on the same stack (a variant of its own: passes without cut-outs keep the
             // leaner kernel).
-            typename TracerOf<W, false, kStack, kCount>::type walk(stack + threadIdx.x, kTraceBlock);
+            typename TracerOf<W, false, kStack, kCount>::type walk(stack + threadIdx.x, blockDim.x);
             float3 from = xyz(o);
             float remaining = d.w;
             bool through = false;
@@ -123,7 +110,7 @@ __global__ void __launch_bounds__(kTraceBlock) shadow_kernel(Wave w, uint32_t ro
                     break;
                 }
                 const uint32_t material = __ldg(&s.shading[walk.h.slot]).w;
-                kept *= 1.0f - fminf(fmaxf(__ldg(&m.materials[material * 16u + 12u]).x, 0.0f), 1.0f);
+                kept *= 1.0f - fminf(fmaxf(__ldg(&m.materials[material].extra).x, 0.0f), 1.0f);
                 if (kept < 1e-4f) kept = 0.0f;
                 const float3 p = from + xyz(d) * walk.h.t;
                 const float margin = 1e-4f * fmaxf(1.0f, fmaxf(fabsf(p.x), fmaxf(fabsf(p.y), fabsf(p.z))));
@@ -163,12 +150,20 @@ __global__ void __launch_bounds__(kTraceBlock) shadow_kernel(Wave w, uint32_t ro
 
 }  // namespace
 
-void launch_closest(int width, int stack, bool count, int grid, cudaStream_t stream, const Wave &w, uint32_t round) {
+// Shared memory a block of `block` threads needs for the stacks of variant (W, kStack):
+// the shadow kernel's cut-out walk takes the closest-hit tracer's, the larger.
+template <int W, int kStack>
+size_t stack_bytes(int block) {
+    return (size_t)TracerOf<W, false, kStack, false>::kInts * (size_t)block * sizeof(int);
+}
+
+void launch_closest(int width, int stack, int block, bool count, int grid, cudaStream_t stream, const Wave &w,
+                    uint32_t round) {
     switch (width * 1000 + stack) {
-#define LR_CASE(wd, k)                                                                           \
-    case wd * 1000 + k:                                                                          \
-        if (count) closest_kernel<wd, k, true><<<grid, kTraceBlock, 0, stream>>>(w, round);       \
-        else closest_kernel<wd, k, false><<<grid, kTraceBlock, 0, stream>>>(w, round);           \
+#define LR_CASE(wd, k)                                                                                      \
+    case wd * 1000 + k:                                                                                     \
+        if (count) closest_kernel<wd, k, true><<<grid, block, stack_bytes<wd, k>(block), stream>>>(w, round); \
+        else closest_kernel<wd, k, false><<<grid, block, stack_bytes<wd, k>(block), stream>>>(w, round);     \
         return;
         LR_TRAVERSALS(LR_CASE)
 #undef LR_CASE
@@ -176,29 +171,49 @@ void launch_closest(int width, int stack, bool count, int grid, cudaStream_t str
     }
 }
 
-void launch_shadow(int width, int stack, bool count, bool cutouts, int grid, cudaStream_t stream, const Wave &w,
-                   uint32_t round) {
+void launch_shadow(int width, int stack, int block, bool count, bool cutouts, int grid, cudaStream_t stream,
+                   const Wave &w, uint32_t round) {
     switch (width * 1000 + stack) {
 #define LR_CASE(wd, k)                                                                                  \
-    case wd * 1000 + k:                                                                                 \
-        if (count && cutouts) shadow_kernel<wd, k, true, true><<<grid, kTraceBlock, 0, stream>>>(w, round);    \
-        else if (count) shadow_kernel<wd, k, true, false><<<grid, kTraceBlock, 0, stream>>>(w, round);         \
-        else if (cutouts) shadow_kernel<wd, k, false, true><<<grid, kTraceBlock, 0, stream>>>(w, round);       \
-        else shadow_kernel<wd, k, false, false><<<grid, kTraceBlock, 0, stream>>>(w, round);                   \
-        return;
+    case wd * 1000 + k: {                                                                               \
+        const size_t bytes = stack_bytes<wd, k>(block);                                                 \
+        if (count && cutouts) shadow_kernel<wd, k, true, true><<<grid, block, bytes, stream>>>(w, round);    \
+        else if (count) shadow_kernel<wd, k, true, false><<<grid, block, bytes, stream>>>(w, round);         \
+        else if (cutouts) shadow_kernel<wd, k, false, true><<<grid, block, bytes, stream>>>(w, round);       \
+        else shadow_kernel<wd, k, false, false><<<grid, block, bytes, stream>>>(w, round);                   \
+        return;                                                                                         \
+    }
         LR_TRAVERSALS(LR_CASE)
 #undef LR_CASE
         default: fail(LR_LIMIT, "no traversal variant for this scene");
     }
 }
 
-int closest_grid(int width, int stack, int sm_count) {
+// Lets every kernel of variant (W, kStack) take `bytes` of dynamic shared memory (above
+// the default 48 KB for deep stacks in large blocks).
+template <int W, int kStack>
+void allow_stacks(size_t bytes) {
+    const int b = (int)bytes;
+    LR_CUDA(cudaFuncSetAttribute(closest_kernel<W, kStack, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, b));
+    LR_CUDA(cudaFuncSetAttribute(closest_kernel<W, kStack, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, b));
+    LR_CUDA(cudaFuncSetAttribute(shadow_kernel<W, kStack, false, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, b));
+    LR_CUDA(cudaFuncSetAttribute(shadow_kernel<W, kStack, false, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, b));
+    LR_CUDA(cudaFuncSetAttribute(shadow_kernel<W, kStack, true, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, b));
+    LR_CUDA(cudaFuncSetAttribute(shadow_kernel<W, kStack, true, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, b));
+}
+
+// Called (by the host, outside any stream capture) before a variant's first launch at a
+// block size: sets the kernels' shared-memory allowance and returns the resident grid.
+int closest_grid(int width, int stack, int block, int sm_count) {
     int per_sm = 0;
     switch (width * 1000 + stack) {
-#define LR_CASE(wd, k)                                                                                       \
-    case wd * 1000 + k:                                                                                      \
-        LR_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, closest_kernel<wd, k, false>, kTraceBlock, 0)); \
-        break;
+#define LR_CASE(wd, k)                                                                                        \
+    case wd * 1000 + k: {                                                                                     \
+        const size_t bytes = stack_bytes<wd, k>(block);                                                       \
+        allow_stacks<wd, k>(bytes);                                                                           \
+        LR_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, closest_kernel<wd, k, false>, block, bytes)); \
+        break;                                                                                                \
+    }
         LR_TRAVERSALS(LR_CASE)
 #undef LR_CASE
         default: fail(LR_LIMIT, "no traversal variant for this scene");

@@ -9,13 +9,16 @@
 #include <stdint.h>
 
 #include "device.hpp"
+#include "emitters.cuh"
+#include "lighttree.cuh"
 #include "shading.cuh"
+#include "surface.cuh"
 
 namespace lr {
 
-constexpr int kTraceBlock = 128;
+constexpr int kTraceBlock = 128;     // the traversal kernels' block size unless tuned
+constexpr int kTraceBlockMax = 256;  // the largest the autotuner tries (64, 128, 256)
 constexpr int kShadeBlock = 128;
-constexpr uint32_t kMaterialStride = 16;  // vec4 rows per material (openpbr.glsl:28)
 constexpr size_t kDefaultPool = 2097152;  // 2^21 paths (integrator.lucb:98)
 // A ray's tag: the path's pool index in the low bits, its segment in the high bits.
 constexpr uint32_t kPathBits = 23;
@@ -31,11 +34,10 @@ constexpr int kProfileRecord = 3;
 // One member of a wave: everything its paths read, fixed while it is a member.
 struct Member {
     DeviceScene scene;
-    const float4 *lights;
-    uint32_t light_count;
+    LightTable lights;
     uint32_t spectral;
-    TreeView tree;
-    const float4 *materials;
+    TreeTable tree;
+    const MaterialCode *materials;
     const Constants *k;
     float frame[16];
     float lens_radius, focus_distance;
@@ -85,7 +87,9 @@ struct Segment {
 // `camera_paths`: the pass's camera paths; `folds`: members whose light paths it traces.
 struct PlanHeader {
     uint32_t segments, paths, converts, dry;
-    uint32_t camera_paths, folds, adapts, reserved;
+    // bin_interval: the shade kernels group outgoing rays by direction octant in rounds
+    // that are multiples of it (0: never; an autotuner choice).
+    uint32_t camera_paths, folds, adapts, bin_interval;
 };
 
 // A renderer's display image for the pass (film_convert.comp:50-52): where the pass that
@@ -177,11 +181,13 @@ __device__ __forceinline__ uint32_t tag_light_index(const Wave &w, uint32_t tag)
 #define LR_TRAVERSALS(X) X(8, 32) X(8, 48) X(4, 32) X(4, 48) X(2, 32) X(2, 64) X(2, 96)
 
 // trace.cu: the closest-hit and shadow kernels of round `round` on `stream`, traversal
-// variant (width, stack); `count` instantiates the counting traversals, `cutouts` the
-// shadow walk through cut-outs. closest_grid: the resident grid of a variant.
-void launch_closest(int width, int stack, bool count, int grid, cudaStream_t stream, const Wave &w, uint32_t round);
-void launch_shadow(int width, int stack, bool count, bool cutouts, int grid, cudaStream_t stream, const Wave &w,
-                   uint32_t round);
-int closest_grid(int width, int stack, int sm_count);
+// variant (width, stack) in blocks of `block` threads (kTraceBlocks); `count`
+// instantiates the counting traversals, `cutouts` the shadow walk through cut-outs.
+// closest_grid: the resident grid of a variant at a block size.
+void launch_closest(int width, int stack, int block, bool count, int grid, cudaStream_t stream, const Wave &w,
+                    uint32_t round);
+void launch_shadow(int width, int stack, int block, bool count, bool cutouts, int grid, cudaStream_t stream,
+                   const Wave &w, uint32_t round);
+int closest_grid(int width, int stack, int block, int sm_count);
 
 }  // namespace lr
