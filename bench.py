@@ -519,9 +519,10 @@ def refit(lr, scenes, ctx, dist, repeats: int = 10) -> dict:
     info = gs.info
     entries = (int(sc.info.node_count) - 1) // 2
     # Bytes a refit must move at least once: the points and indices read, the triangle
-    # records written, both copies of the BVH2's boxes and the wide nodes' boxes written.
+    # records written, both copies of the BVH2's boxes, the 4-wide nodes' boxes and the
+    # compressed 8-wide nodes (96 bytes each) written.
     algorithmic = (12 * points + 12 * triangles + 48 * triangles + 96 * entries + 96 * int(info.wide4_nodes) +
-                   192 * int(info.wide8_nodes))
+                   96 * int(info.wide8_nodes))
     for b in buffers:
         ctx.free(b)
     gs.destroy()

@@ -131,8 +131,10 @@ TraversalChoice choose_traversal(const DeviceScene &s, int requested) {
         }
     }
     auto wide_stack = [](uint32_t bound) { return bound + 1 <= 32 ? 32 : (bound + 1 <= 48 ? 48 : 0); };
+    // The compressed 8-wide tree's stack holds one group a level.
+    auto group_stack = [](uint32_t bound) { return bound <= 16 ? 16 : (bound <= 32 ? 32 : 0); };
     // A scene built on the device has no wide collapses (null nodes).
-    if (requested == 8 && s.wide8.nodes && wide_stack(s.wide8.max_stack)) return {8, wide_stack(s.wide8.max_stack)};
+    if (requested == 8 && s.wide8.nodes && group_stack(s.wide8.max_stack)) return {8, group_stack(s.wide8.max_stack)};
     if (requested >= 4 && s.wide4.nodes && wide_stack(s.wide4.max_stack)) return {4, wide_stack(s.wide4.max_stack)};
     return {2, stack_for(s.depth)};
 }
@@ -163,8 +165,8 @@ void dispatch_exact(const lr_gpu_scene *gs, const float4 *rays, uint64_t n, floa
     if (n > 0xffffffffull) fail(LR_LIMIT, "a ray query holds at most 2^32 - 1 rays");
     const TraversalChoice c = choose_traversal(gs->scene, requested_width);
     switch (c.width * 1000 + c.stack) {
+        case 8016: launch_resident<8, kAny, 16, kCount>(gs, rays, n, hits, status, counts, stream); break;
         case 8032: launch_resident<8, kAny, 32, kCount>(gs, rays, n, hits, status, counts, stream); break;
-        case 8048: launch_resident<8, kAny, 48, kCount>(gs, rays, n, hits, status, counts, stream); break;
         case 4032: launch_resident<4, kAny, 32, kCount>(gs, rays, n, hits, status, counts, stream); break;
         case 4048: launch_resident<4, kAny, 48, kCount>(gs, rays, n, hits, status, counts, stream); break;
         case 2032: launch_resident<2, kAny, 32, kCount>(gs, rays, n, hits, status, counts, stream); break;

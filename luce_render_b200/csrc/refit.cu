@@ -13,7 +13,8 @@
 //      thread waiting on another;
 //   3. the watertight path's widened boxes from the exact ones, with the widening taken
 //      again from the new root box (2^-16 of the scene's scale, one more float step);
-//   4. the 4- and 8-wide collapses' child boxes, copied from the BVH2 slots they came from.
+//   4. the 4-wide collapse's child boxes, copied from the BVH2 slots they came from, and the
+//      compressed 8-wide nodes quantized again from those boxes (quantize.hpp).
 // With the points unchanged a refit leaves every array bit for bit as the upload made it,
 // and the boxes equal the host refit (lr_scene_move_points) of the same move exactly: boxes
 // are minima and maxima of the same floats, and the widening is the same float arithmetic.
@@ -22,6 +23,7 @@
 #include <cstring>
 
 #include "device.hpp"
+#include "quantize.hpp"
 
 namespace lr {
 namespace {
@@ -188,11 +190,11 @@ __global__ void widen_kernel(uint64_t count, const float4 *exact, float4 *widene
     }
 }
 
-// Step 4: wide node n's child slot i from the BVH2 slot (or the root) it was collapsed from;
-// empty slots keep their inverted boxes.
+// Step 4: 4-wide node n's child slot i from the BVH2 slot (or the root) it was collapsed
+// from; empty slots keep their inverted boxes.
 __global__ void wide_kernel(uint64_t slots, int width, const uint32_t *sources, const float4 *exact,
                             const float *root_box, float delta, float4 *nodes) {
-    const int per_node = width == 4 ? 7 : 14, planes = width / 4;
+    const int per_node = 7, planes = width / 4;
     for (uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; i < slots; i += (uint64_t)gridDim.x * blockDim.x) {
         const uint32_t source = sources[i];
         if (source == 0xffffffffu) continue;
@@ -212,6 +214,40 @@ __global__ void wide_kernel(uint64_t slots, int width, const uint32_t *sources, 
             base[((2 * k) * planes) * 4 + slot] = widen_lo(b.lo[k], delta);
             base[((2 * k + 1) * planes) * 4 + slot] = widen_hi(b.hi[k], delta);
         }
+    }
+}
+
+// Step 4 for the compressed 8-wide tree: node n quantized again (quantize.hpp) from its
+// children's BVH2 boxes (or the root's), widened as at upload; its links and child count
+// stay.
+__global__ void quantize_kernel(uint64_t count, const uint32_t *sources, const float4 *exact, const float *root_box,
+                                float delta, float4 *nodes) {
+    for (uint64_t n = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; n < count; n += (uint64_t)gridDim.x * blockDim.x) {
+        float *node = reinterpret_cast<float *>(nodes + n * kQNodeFloat4s);
+        const int children = (int)(__float_as_uint(node[3]) >> 24);
+        float lo[8][3], hi[8][3];
+        int links[8];
+        for (int c = 0; c < 8; c++) {
+            links[c] = __float_as_int(node[4 + c]);
+            if (c >= children) continue;
+            const uint32_t source = sources[n * 8 + c];
+            Box b;
+            if (source == kRefitRoot) {
+                for (int k = 0; k < 3; k++) {
+                    b.lo[k] = root_box[k];
+                    b.hi[k] = root_box[4 + k];
+                }
+            } else {
+                b = read_side(exact, source >> 1, source & 1u);
+            }
+            for (int k = 0; k < 3; k++) {
+                lo[c][k] = widen_lo(b.lo[k], delta);
+                hi[c][k] = widen_hi(b.hi[k], delta);
+            }
+        }
+        float out[kQNodeFloat4s * 4];
+        quantize_node(children, lo, hi, links, out);
+        for (int k = 0; k < kQNodeFloat4s * 4; k++) node[k] = out[k];
     }
 }
 
@@ -281,8 +317,8 @@ void refit_scene(lr_gpu_scene *gs, cudaStream_t stream) {
         wide_kernel<<<grid_for(gs->wide4_nodes * 4, sms), 256, 0, stream>>>(
             gs->wide4_nodes * 4, 4, gs->wide4_sources, exact, gs->root_box, delta, const_cast<float4 *>(s.wide4.nodes));
     if (s.wide8.width)
-        wide_kernel<<<grid_for(gs->wide8_nodes * 8, sms), 256, 0, stream>>>(
-            gs->wide8_nodes * 8, 8, gs->wide8_sources, exact, gs->root_box, delta, const_cast<float4 *>(s.wide8.nodes));
+        quantize_kernel<<<grid_for(gs->wide8_nodes, sms), 256, 0, stream>>>(
+            gs->wide8_nodes, gs->wide8_sources, exact, gs->root_box, delta, const_cast<float4 *>(s.wide8.nodes));
     LR_CUDA(cudaGetLastError());
     LR_CUDA(cudaStreamSynchronize(stream));
     gs->refits++;

@@ -19,6 +19,7 @@
 #include <stdint.h>
 
 #include "device.hpp"
+#include "quantize.hpp"
 
 namespace lr {
 
@@ -473,6 +474,166 @@ struct WideTracer {
     }
 };
 
+// The watertight traversal over the compressed 8-wide BVH (quantize.hpp): a visit loads
+// one 96-byte node, decodes its children's planes from bytes (one fused multiply-add per
+// plane: the step times the inverse direction and the origin's offset are set once a
+// node), tests the eight boxes together and orders the children it hits by entry
+// distance. The nearest is taken next; the rest stay behind as one *group* -- the node and
+// its remaining children in order, four bits each -- so a visit pushes at most one stack
+// entry (two ints in shared memory) however many children it hit, and the stack holds at
+// most the tree's interior depth. Leaves and triangles are the BVH2's, with the same tie
+// rule, so results equal the BVH2 path's bit for bit. Any-hit rays skip the ordering.
+template <bool kAny, int kStack, bool kCount>
+struct CompressedTracer {
+    Ray r;
+    float3 inv, oinv;
+    Shear sh;
+    Hit h;
+    int node;
+    int *base;
+    int stride;
+    int sp = 0;
+
+    __device__ __forceinline__ CompressedTracer(int *stack_base, int s) : base(stack_base), stride(s) {}
+
+    __device__ __forceinline__ bool start(const DeviceScene &s, const Ray &ray) {
+        r = ray;
+        h = Hit{r.tmax, -1, -1, 0.0f, 0.0f};
+        sp = 0;
+        const DeviceBvh &b = s.bvh;
+        if (b.empty) return false;
+        inv = safe_inverse(r.d);
+        oinv = neg_origin_times(r.o, inv);
+        sh = make_shear(r.o, r.d);
+        node = 0;
+        float enter;
+        return box_exact(b.root_lo[0], b.root_hi[0], b.root_lo[1], b.root_hi[1], b.root_lo[2], b.root_hi[2], inv, oinv,
+                         r.tmin, r.tmax, enter);
+    }
+
+    // Byte k (0..3) of w as a float, exactly: placed under the exponent of 2^23, less 2^23.
+    static __device__ __forceinline__ float byte_at(uint32_t w, int k) {
+        return __uint_as_float(__byte_perm(w, 0x4B000000u, (uint32_t)k | 0x7540u)) - 8388608.0f;
+    }
+
+    static __device__ __forceinline__ void order(float &ka, uint32_t &la, float &kb, uint32_t &lb) {
+        const bool swap = ka > kb;
+        const float k = swap ? kb : ka;
+        const uint32_t l = swap ? lb : la;
+        kb = swap ? ka : kb;
+        lb = swap ? la : lb;
+        ka = k;
+        la = l;
+    }
+
+    // Tests node n's children: the slots hit, nearest first, packed four bits each with
+    // their count in the top four bits; 0 when none is hit.
+    __device__ __forceinline__ uint32_t visit(const float4 *n) {
+        const float4 head = __ldg(n), px = __ldg(n + 3), py = __ldg(n + 4), pz = __ldg(n + 5);
+        const uint32_t meta = __float_as_uint(head.w);
+        const int count = (int)(meta >> 24);
+        const float ax = q_step(meta & 0xffu) * inv.x, ay = q_step((meta >> 8) & 0xffu) * inv.y,
+                    az = q_step((meta >> 16) & 0xffu) * inv.z;
+        const float bx = fmaf(head.x, inv.x, oinv.x), by = fmaf(head.y, inv.y, oinv.y), bz = fmaf(head.z, inv.z, oinv.z);
+        // The near and far plane bytes of each axis for this ray's direction signs.
+        const bool px_up = inv.x >= 0.0f, py_up = inv.y >= 0.0f, pz_up = inv.z >= 0.0f;
+        const uint32_t nx0 = __float_as_uint(px_up ? px.x : px.z), nx1 = __float_as_uint(px_up ? px.y : px.w);
+        const uint32_t fx0 = __float_as_uint(px_up ? px.z : px.x), fx1 = __float_as_uint(px_up ? px.w : px.y);
+        const uint32_t ny0 = __float_as_uint(py_up ? py.x : py.z), ny1 = __float_as_uint(py_up ? py.y : py.w);
+        const uint32_t fy0 = __float_as_uint(py_up ? py.z : py.x), fy1 = __float_as_uint(py_up ? py.w : py.y);
+        const uint32_t nz0 = __float_as_uint(pz_up ? pz.x : pz.z), nz1 = __float_as_uint(pz_up ? pz.y : pz.w);
+        const uint32_t fz0 = __float_as_uint(pz_up ? pz.z : pz.x), fz1 = __float_as_uint(pz_up ? pz.w : pz.y);
+        const float kMiss = __int_as_float(0x7f800000);
+        float key[8];
+        uint32_t slot[8];
+#pragma unroll
+        for (int c = 0; c < 8; c++) {
+            const int k = c & 3;
+            const uint32_t nx = c < 4 ? nx0 : nx1, fx = c < 4 ? fx0 : fx1;
+            const uint32_t ny = c < 4 ? ny0 : ny1, fy = c < 4 ? fy0 : fy1;
+            const uint32_t nz = c < 4 ? nz0 : nz1, fz = c < 4 ? fz0 : fz1;
+            const float e = fmax3(fmaf(byte_at(nx, k), ax, bx), fmaf(byte_at(ny, k), ay, by),
+                                  fmaxf(fmaf(byte_at(nz, k), az, bz), r.tmin));
+            const float l = fmin3(fmaf(byte_at(fx, k), ax, bx), fmaf(byte_at(fy, k), ay, by),
+                                  fminf(fmaf(byte_at(fz, k), az, bz), h.t)) * 1.0000003576f;
+            key[c] = c < count && e <= l ? e : kMiss;
+            slot[c] = (uint32_t)c;
+        }
+        if (!kAny) {
+            constexpr int kNet[19][2] = {{0, 2}, {1, 3}, {4, 6}, {5, 7}, {0, 4}, {1, 5}, {2, 6},
+                                         {3, 7}, {0, 1}, {2, 3}, {4, 5}, {6, 7}, {2, 4}, {3, 5},
+                                         {1, 4}, {3, 6}, {1, 2}, {3, 4}, {5, 6}};
+#pragma unroll
+            for (int i = 0; i < 19; i++) order(key[kNet[i][0]], slot[kNet[i][0]], key[kNet[i][1]], slot[kNet[i][1]]);
+        }
+        uint32_t packed = 0, hits = 0;
+#pragma unroll
+        for (int c = 7; c >= 0; c--)
+            if (key[c] != kMiss) {
+                packed = (packed << 4) | slot[c];
+                hits++;
+            }
+        return hits ? (hits << 28) | packed : 0u;
+    }
+
+    // Runs to the end of the ray's traversal.
+    __device__ __forceinline__ bool step(const DeviceScene &s, bool &overflow, Visits &visits) {
+        const float4 *nodes = s.wide8.nodes;
+        uint32_t group_node = 0, rest = 0;  // the group being walked: node and packed slots
+        int link = 0;                       // the wide root
+        for (;;) {
+            if (link >= 0) {
+                if (kCount) visits.nodes++;
+                const float4 *n = nodes + (size_t)link * kQNodeFloat4s;
+                const uint32_t hits = visit(n);
+                if (hits) {
+                    // The group walked so far waits on the stack; this node's is next.
+                    if (rest) {
+                        if (sp < kStack) {
+                            base[(2 * sp) * stride] = (int)group_node;
+                            base[(2 * sp + 1) * stride] = (int)rest;
+                            sp++;
+                        } else {
+                            overflow = true;
+                        }
+                    }
+                    group_node = (uint32_t)link;
+                    rest = hits;
+                }
+            } else {
+                uint32_t first, count;
+                leaf_range(link, first, count);
+                if (kCount) visits.tests += count;
+                for (uint32_t i = 0; i < count; i++) {
+                    const float4 *tri = s.tris + (size_t)(first + i) * 3;
+                    const float4 a = __ldg(tri), bb = __ldg(tri + 1), c = __ldg(tri + 2);
+                    const float limit = h.id >= 0 ? __int_as_float(__float_as_int(h.t) + 1) : r.tmax;
+                    float t, u, v;
+                    if (!watertight(sh, r.tmin, limit, a, bb, c, t, u, v)) continue;
+                    const int id = __float_as_int(a.w);
+                    if (h.id >= 0 && t == h.t && id > h.id) continue;
+                    h.t = t;
+                    h.id = id;
+                    h.slot = (int)(first + i);
+                    h.u = u;
+                    h.v = v;
+                    if (kAny) return true;
+                }
+            }
+            // The next child: from the group in hand, else from the stack.
+            if (!rest) {
+                if (sp == 0) return true;
+                sp--;
+                group_node = (uint32_t)base[(2 * sp) * stride];
+                rest = (uint32_t)base[(2 * sp + 1) * stride];
+            }
+            const uint32_t slot = rest & 0xfu, left = (rest >> 28) - 1u;
+            rest = left ? (left << 28) | ((rest & 0x0fffffffu) >> 4) : 0u;
+            link = __ldg(reinterpret_cast<const int *>(nodes + (size_t)group_node * kQNodeFloat4s + 1) + slot);
+        }
+    }
+};
+
 // The closest (or any) hit along r, watertight. `overflow` is set when a push was lost.
 template <bool kAny, int kStack, bool kCount = false>
 __device__ __forceinline__ Hit trace_exact(const DeviceScene &s, const Ray &r, int *stack_base, int stride,
@@ -484,12 +645,17 @@ __device__ __forceinline__ Hit trace_exact(const DeviceScene &s, const Ray &r, i
     return tr.h;
 }
 
-// The watertight tracer of a BVH width: 2 (the BVH2 itself), 4 or 8 (wide.cpp), and the
-// shared-memory ints per thread its stack takes.
+// The watertight tracer of a BVH width: 2 (the BVH2 itself), 4 or 8 (wide.cpp: 8 is the
+// compressed layout), and the shared-memory ints per thread its stack takes.
 template <int W, bool kAny, int kStack, bool kCount>
 struct TracerOf {
     using type = WideTracer<W, kAny, kStack, kCount>;
-    static constexpr int kInts = 1;  // the wide tracer's stack is in local memory
+    static constexpr int kInts = 1;  // the 4-wide tracer's stack is in local memory
+};
+template <bool kAny, int kStack, bool kCount>
+struct TracerOf<8, kAny, kStack, kCount> {
+    using type = CompressedTracer<kAny, kStack, kCount>;
+    static constexpr int kInts = 2 * kStack;  // (node, packed slots) a group
 };
 template <bool kAny, int kStack, bool kCount>
 struct TracerOf<2, kAny, kStack, kCount> {

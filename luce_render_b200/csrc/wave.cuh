@@ -178,7 +178,7 @@ __device__ __forceinline__ uint32_t tag_light_index(const Wave &w, uint32_t tag)
 }
 
 // The traversal variants a pass can take: (BVH width, stack entries).
-#define LR_TRAVERSALS(X) X(8, 32) X(8, 48) X(4, 32) X(4, 48) X(2, 32) X(2, 64) X(2, 96)
+#define LR_TRAVERSALS(X) X(8, 16) X(8, 32) X(4, 32) X(4, 48) X(2, 32) X(2, 64) X(2, 96)
 
 // trace.cu: the closest-hit and shadow kernels of round `round` on `stream`, traversal
 // variant (width, stack) in blocks of `block` threads (kTraceBlocks); `count`

@@ -5,13 +5,16 @@
 // records in the same leaf order; only interior levels are merged, which cuts the
 // dependent node fetches along a ray by about log2(W).
 //
-// Node layout (float4s, structure of arrays over the children so one load brings a plane
-// of every child): for W = 4, 7 float4 = 112 bytes -- lo.x, hi.x, lo.y, hi.y, lo.z, hi.z
-// of the 4 children, then their 4 links; for W = 8, 14 float4 = 224 bytes in the same
-// order, each plane two float4. Links: >= 0 a wide node, < 0 a leaf
-// (-1 - (first << 4 | count - 1)); an empty slot has an inverted box (lo +inf, hi -inf).
-// Boxes are widened outward like the BVH2 path's.
+// Node layouts. W = 4: float4s, structure of arrays over the children so one load brings
+// a plane of every child: 7 float4 = 112 bytes -- lo.x, hi.x, lo.y, hi.y, lo.z, hi.z of
+// the 4 children, then their 4 links; an empty slot has an inverted box (lo +inf, hi
+// -inf). W = 8: compressed, 96 bytes -- the node's origin and per-axis power-of-two steps,
+// 8 child links, and each child's planes as 8-bit multiples of the steps, rounded outward
+// (quantize.hpp). Links: >= 0 a wide node, < 0 a leaf (-1 - (first << 4 | count - 1)).
+// Boxes are widened outward like the BVH2 path's before they are stored or quantized.
 #include "wide.hpp"
+
+#include "quantize.hpp"
 
 #include <algorithm>
 #include <cmath>
@@ -87,12 +90,42 @@ WideBvh build_wide(const std::vector<lr_bvh_node> &nodes, int width, float delta
     }
     const size_t count = children_of.size();
     w.node_count = count;
-    w.nodes.assign(count * per_node * 4, 0.0f);
     w.sources.assign(count * width, 0xffffffffu);
     std::vector<uint32_t> index_of_bvh2(nodes.size(), 0xffffffffu);
     for (const Job &j : queue) index_of_bvh2[j.bvh2] = j.wide;
     // The wide root stands for BVH2 node 0 even when it is a leaf.
     std::vector<uint32_t> bound(count, 0);
+    if (width == 8) {
+        // Compressed: quantized child boxes (quantize.hpp), 96 bytes a node.
+        w.floats_per_node = kQNodeFloat4s;
+        w.nodes.assign(count * kQNodeFloat4s * 4, 0.0f);
+        for (size_t n = 0; n < count; n++) {
+            const auto &list = children_of[n];
+            float lo[8][3], hi[8][3];
+            int links[8] = {0};
+            for (size_t slot = 0; slot < list.size(); slot++) {
+                w.sources[n * width + slot] = list[slot];
+                const lr_bvh_node &c = nodes[list[slot]];
+                for (int k = 0; k < 3; k++) {
+                    lo[slot][k] = widen_down(c.lo[k], delta);
+                    hi[slot][k] = widen_up(c.hi[k], delta);
+                }
+                links[slot] = c.count > 0 ? leaf_link(c) : (int)index_of_bvh2[list[slot]];
+            }
+            quantize_node((int)list.size(), lo, hi, links, &w.nodes[n * kQNodeFloat4s * 4]);
+        }
+        // A traversal keeps one group of a node's unvisited children a level: the stack
+        // holds at most the tree's interior depth.
+        for (size_t n = count; n-- > 0;) {
+            uint32_t deepest = 0;
+            for (uint32_t c : children_of[n])
+                if (nodes[c].count == 0) deepest = std::max(deepest, bound[index_of_bvh2[c]]);
+            bound[n] = 1 + deepest;
+        }
+        w.max_stack = bound[0];
+        return w;
+    }
+    w.nodes.assign(count * per_node * 4, 0.0f);
     for (size_t n = 0; n < count; n++) {
         float *base = &w.nodes[n * per_node * 4];
         const auto &list = children_of[n];
