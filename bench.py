@@ -47,6 +47,9 @@ def parse():
     p.add_argument("--skip-cornell", action="store_true", help="leave out the glossy Cornell benchmark lines")
     p.add_argument("--skip-refit", action="store_true", help="leave out the moved-geometry refit line")
     p.add_argument("--refit-only", action="store_true", help="only the moved-geometry refit line (for profiling)")
+    p.add_argument("--trace-only", action="store_true",
+                   help="only the headline renderer's passes (--warmup, then --steps), for profiling; one JSON line")
+    p.add_argument("--width", type=int, default=0, help="with --trace-only: the BVH width (2, 4, 8; 0 the default)")
     p.add_argument("--cornell-only", action="store_true",
                    help="only the glossy Cornell benchmark lines (--steps samples each), one JSON line")
     p.add_argument("--served-seconds", type=float, default=60.0,
@@ -386,6 +389,7 @@ def served(lr, scenes, dist, seconds: float):
         "demand_msamples_s": demand / window / 1e6,
         "failures": failures,
         "uploads": stats_window["uploads"], "evictions": stats_window["evictions"],
+        "tunings": stats_window.get("tunings", 0),
         "queued_at_end": stats_window["queued"], "live_at_end": stats_window["live"],
         "timing": "host steady clock of the server, from submission; the stream is cut at its end",
     }
@@ -682,6 +686,31 @@ def main():
         return
     sc, lights, mats = build_scene(lr, scenes)
     info = sc.info
+    if args.trace_only:
+        # The headline renderer alone (two lanes, graphs): what a profiler captures.
+        if args.width:
+            os.environ["LUCE_RENDER_B200_BVH_WIDTH"] = str(args.width)
+        r = lr.Renderer.create(ctx, sc, settings_for(lr, W + K, spectral))
+        for _ in range(W):
+            r.advance_one()
+        r.wait()
+        s0 = r.stats()
+        ctx.synchronize()
+        ctx.timer_start()
+        for _ in range(K):
+            r.advance_one()
+        r.join()
+        ms = ctx.timer_stop()
+        r.finish()
+        s1 = r.stats()
+        r.destroy()
+        rays = (s1.closest_rays - s0.closest_rays) + (s1.shadow_rays - s0.shadow_rays)
+        if dist.rank == 0:
+            print(json.dumps({"trace_only": {"mrays_s": rays / (ms / 1e3) / 1e6, "ms_per_step": ms / K, "steps": K,
+                                             "width": args.width or 2}, "n_gpus": dist.world}))
+        ctx.close()
+        dist.close()
+        return
 
     # Work per ray, counted by the traversal kernels on one pass of the same workload.
     counter = lr.Renderer.create(ctx, sc, settings_for(lr, 1, spectral, profile=2))

@@ -596,6 +596,7 @@ typedef struct {
     uint64_t queued, live, scenes_resident;
     uint64_t bytes_in_use;  /* resident scenes, live sessions and the pool */
     double seconds;         /* since the server started */
+    uint64_t tunings;       /* autotuner runs on the live mix (from 32 live sessions, every 20 s) */
 } lr_server_stats;
 
 /* device 0, budget 150 GB, capacity 128, pool 2^22, max_bounces 12, probe_priority 1. */

@@ -268,7 +268,7 @@ class ServerStats(C.Structure):
     """lr_server_stats."""
     _fields_ = [(n, C.c_uint64) for n in ("sessions_done", "probes_done", "failed", "pixel_samples", "probe_rays",
                                           "uploads", "evictions", "queued", "live", "scenes_resident",
-                                          "bytes_in_use")] + [("seconds", C.c_double)]
+                                          "bytes_in_use")] + [("seconds", C.c_double), ("tunings", C.c_uint64)]
 
 
 _vp, _i32, _u32, _u64, _sz = C.c_void_p, C.c_int32, C.c_uint32, C.c_uint64, C.c_size_t

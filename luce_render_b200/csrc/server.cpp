@@ -83,6 +83,10 @@ struct lr_server {
     std::thread render_thread, probe_thread;
     Clock::time_point t0;
     lr_server_stats stats{};
+    // The batch's autotuner runs (lr_batch_tune) once enough sessions are live to stand for
+    // the mix, and again when the mix may have changed (every kRetune seconds).
+    double tuned_at = -1.0;
+    uint64_t tunings = 0;
 };
 
 namespace {
@@ -105,6 +109,10 @@ uint64_t dome_image_bytes(const lr_scene *scene) {
         }
     return 0;
 }
+
+// Live sessions that make the mix worth tuning for, and the seconds between tunings.
+constexpr size_t kTuneSessions = 32;
+constexpr double kRetune = 20.0;
 
 // The budget left for scenes and sessions once the pool is paid for.
 uint64_t available(const lr_server *s) {
@@ -271,7 +279,18 @@ void render_loop(lr_server *s) {
                 s->cv_done.wait_for(lk, std::chrono::milliseconds(20));
             continue;
         }
+        const double now = seconds_since(s->t0);
+        const bool retune = s->live.size() >= std::min<size_t>(kTuneSessions, s->cfg.capacity) &&
+                            (s->tuned_at < 0.0 || now - s->tuned_at > kRetune);
         lk.unlock();
+        if (retune) {
+            // Dry passes on the live sessions (films untouched): the BVH width, stack and
+            // block size per scene-size class, the pass fill and the ray sort interval.
+            const bool tuned = lr_batch_tune(s->batch, nullptr) == LR_OK;
+            std::lock_guard<std::mutex> note(s->mu);
+            if (tuned) s->tunings++;
+            s->tuned_at = seconds_since(s->t0);
+        }
         int32_t more = 0, in_flight = 0;
         int status = lr_batch_advance(s->batch, &more);
         if (status == LR_OK) status = lr_batch_wait(s->batch, &in_flight);
@@ -515,6 +534,7 @@ int lr_server_stats_get(lr_server *s, lr_server_stats *out) {
         out->scenes_resident = (uint64_t)std::count_if(s->scenes.begin(), s->scenes.end(),
                                                        [](const SceneSlot &x) { return x.gs != nullptr; });
         out->seconds = seconds_since(s->t0);
+        out->tunings = s->tunings;
     });
 }
 
