@@ -526,10 +526,12 @@ struct CompressedTracer {
         la = l;
     }
 
-    // Tests node n's children: the slots hit, nearest first, packed four bits each with
-    // their count in the top four bits; 0 when none is hit.
-    __device__ __forceinline__ uint32_t visit(const float4 *n) {
-        const float4 head = __ldg(n), px = __ldg(n + 3), py = __ldg(n + 4), pz = __ldg(n + 5);
+    // Tests node n's children. False when none is hit; else `next` is the nearest hit
+    // child's link and `more` the other hit slots, nearest first, four bits each with
+    // their count in the top four bits (0: none).
+    __device__ __forceinline__ bool visit(const float4 *n, int &next, uint32_t &more) {
+        const float4 head = __ldg(n), la = __ldg(n + 1), lb = __ldg(n + 2), px = __ldg(n + 3), py = __ldg(n + 4),
+                     pz = __ldg(n + 5);
         const uint32_t meta = __float_as_uint(head.w);
         const int count = (int)(meta >> 24);
         const float ax = q_step(meta & 0xffu) * inv.x, ay = q_step((meta >> 8) & 0xffu) * inv.y,
@@ -566,14 +568,25 @@ struct CompressedTracer {
 #pragma unroll
             for (int i = 0; i < 19; i++) order(key[kNet[i][0]], slot[kNet[i][0]], key[kNet[i][1]], slot[kNet[i][1]]);
         }
-        uint32_t packed = 0, hits = 0;
+        // The hit slots, nearest first: up to 8 nibbles in 64 bits.
+        uint64_t packed = 0;
+        uint32_t hits = 0;
 #pragma unroll
         for (int c = 7; c >= 0; c--)
             if (key[c] != kMiss) {
                 packed = (packed << 4) | slot[c];
                 hits++;
             }
-        return hits ? (hits << 28) | packed : 0u;
+        if (!hits) return false;
+        const uint32_t first = (uint32_t)packed & 0xfu;
+        more = hits > 1u ? ((hits - 1u) << 28) | (uint32_t)(packed >> 4) : 0u;
+        const int links[8] = {__float_as_int(la.x), __float_as_int(la.y), __float_as_int(la.z), __float_as_int(la.w),
+                              __float_as_int(lb.x), __float_as_int(lb.y), __float_as_int(lb.z), __float_as_int(lb.w)};
+        int chosen = links[0];
+#pragma unroll
+        for (int c = 1; c < 8; c++) chosen = first == (uint32_t)c ? links[c] : chosen;
+        next = chosen;
+        return true;
     }
 
     // Runs to the end of the ray's traversal.
@@ -585,20 +598,26 @@ struct CompressedTracer {
             if (link >= 0) {
                 if (kCount) visits.nodes++;
                 const float4 *n = nodes + (size_t)link * kQNodeFloat4s;
-                const uint32_t hits = visit(n);
-                if (hits) {
-                    // The group walked so far waits on the stack; this node's is next.
-                    if (rest) {
-                        if (sp < kStack) {
-                            base[(2 * sp) * stride] = (int)group_node;
-                            base[(2 * sp + 1) * stride] = (int)rest;
-                            sp++;
-                        } else {
-                            overflow = true;
+                int next;
+                uint32_t more;
+                if (visit(n, next, more)) {
+                    // The nearest hit child next; the group walked so far waits on the stack
+                    // and this node's other hit children become the group in hand.
+                    if (more) {
+                        if (rest) {
+                            if (sp < kStack) {
+                                base[(2 * sp) * stride] = (int)group_node;
+                                base[(2 * sp + 1) * stride] = (int)rest;
+                                sp++;
+                            } else {
+                                overflow = true;
+                            }
                         }
+                        group_node = (uint32_t)link;
+                        rest = more;
                     }
-                    group_node = (uint32_t)link;
-                    rest = hits;
+                    link = next;
+                    continue;
                 }
             } else {
                 uint32_t first, count;

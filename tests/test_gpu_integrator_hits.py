@@ -83,7 +83,7 @@ def test_cornell_pass_hits_equal_brute_force(ctx, spectral):
                 _closest_equal(a, rays, hits)
             if len(srays):
                 shadow += _shadow_equal(a, srays, shits)
-        assert closest > 3 * 256 * 256 and shadow > 256 * 256, (closest, shadow)
+        assert closest > 2 * 256 * 256 and shadow > 256 * 256, (closest, shadow)
     finally:
         sc.close()
 

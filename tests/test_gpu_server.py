@@ -38,7 +38,9 @@ def test_results_same_alone_and_in_the_mix(ctx):
     wave = pool * 16 * 15 + (1 << 20)
     biggest_scene = max(_upload_estimate(sc) for sc, _ in cs)
     biggest_session = max(s.c.width * s.c.height * 32 + (1 << 20) for _, s in cs)
-    budget = wave + biggest_scene + biggest_session
+    # The static probe array (LR_PROBE_STATIC_PIXELS face ids and distances) counts
+    # against the budget from the server's start.
+    budget = wave + biggest_scene + biggest_session + lr.PROBE_STATIC_PIXELS * 8
     server = lr.Server(lr.ServerSettings.default(budget_bytes=budget, capacity=2, pool=pool, max_bounces=12))
     try:
         ids = [server.add_scene(sc) for sc, _ in cs]
