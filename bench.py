@@ -50,6 +50,8 @@ def parse():
     p.add_argument("--trace-only", action="store_true",
                    help="only the headline renderer's passes (--warmup, then --steps), for profiling; one JSON line")
     p.add_argument("--width", type=int, default=0, help="with --trace-only: the BVH width (2, 4, 8; 0 the default)")
+    p.add_argument("--refill", type=int, default=-1,
+                   help="with --trace-only: idle lanes at which traversal warps refill (1-32; 0 grid-stride)")
     p.add_argument("--cornell-only", action="store_true",
                    help="only the glossy Cornell benchmark lines (--steps samples each), one JSON line")
     p.add_argument("--served-seconds", type=float, default=60.0,
@@ -690,6 +692,8 @@ def main():
         # The headline renderer alone (two lanes, graphs): what a profiler captures.
         if args.width:
             os.environ["LUCE_RENDER_B200_BVH_WIDTH"] = str(args.width)
+        if args.refill >= 0:
+            os.environ["LUCE_RENDER_B200_REFILL"] = str(args.refill)
         r = lr.Renderer.create(ctx, sc, settings_for(lr, W + K, spectral))
         for _ in range(W):
             r.advance_one()
@@ -707,7 +711,8 @@ def main():
         rays = (s1.closest_rays - s0.closest_rays) + (s1.shadow_rays - s0.shadow_rays)
         if dist.rank == 0:
             print(json.dumps({"trace_only": {"mrays_s": rays / (ms / 1e3) / 1e6, "ms_per_step": ms / K, "steps": K,
-                                             "width": args.width or 2}, "n_gpus": dist.world}))
+                                             "width": args.width or 2, "refill_at": max(args.refill, 0)},
+                              "n_gpus": dist.world}))
         ctx.close()
         dist.close()
         return

@@ -239,7 +239,8 @@ class BatchTuning(C.Structure):
     candidate's measured rate and how many candidates it timed."""
     _fields_ = [("width", C.c_uint32), ("fill", C.c_uint32), ("paths_per_ms", C.c_double),
                 ("candidates", C.c_uint32), ("class_width", C.c_uint32 * 3), ("class_members", C.c_uint32 * 3),
-                ("class_stack", C.c_uint32 * 3), ("class_block", C.c_uint32 * 3), ("bin_interval", C.c_uint32)]
+                ("class_stack", C.c_uint32 * 3), ("class_block", C.c_uint32 * 3), ("bin_interval", C.c_uint32),
+                ("refill_at", C.c_uint32)]
 
 
 class ServerSettings(C.Structure):
@@ -1056,14 +1057,16 @@ class Batch:
 
     def tune(self) -> dict:
         """Autotune, per scene-size class, BVH width, traversal stack depth and threads a
-        block, then paths a pass and the interval of octant sorts of outgoing rays, on the
-        members as they stand (images do not change)."""
+        block, then paths a pass, the interval of octant sorts of outgoing rays and the
+        traversal warps' refill point, on the members as they stand (images do not
+        change)."""
         t = BatchTuning()
         _check(lib.lr_batch_tune(self.handle, C.byref(t)))
         return {"width": int(t.width), "fill": int(t.fill), "paths_per_ms": float(t.paths_per_ms),
                 "candidates": int(t.candidates), "class_width": list(t.class_width),
                 "class_members": list(t.class_members), "class_stack": list(t.class_stack),
-                "class_block": list(t.class_block), "bin_interval": int(t.bin_interval)}
+                "class_block": list(t.class_block), "bin_interval": int(t.bin_interval),
+                "refill_at": int(t.refill_at)}
 
     def passes(self):
         rec, fin = C.c_uint64(), C.c_uint64()

@@ -131,10 +131,12 @@ TraversalChoice choose_traversal(const DeviceScene &s, int requested) {
         }
     }
     auto wide_stack = [](uint32_t bound) { return bound + 1 <= 32 ? 32 : (bound + 1 <= 48 ? 48 : 0); };
-    // The compressed 8-wide tree's stack holds one group a level.
+    // The compressed 8-wide tree's stack holds one group a level, a node index under 2^24
+    // beside its child ranks in one word.
     auto group_stack = [](uint32_t bound) { return bound <= 16 ? 16 : (bound <= 32 ? 32 : 0); };
     // A scene built on the device has no wide collapses (null nodes).
-    if (requested == 8 && s.wide8.nodes && group_stack(s.wide8.max_stack)) return {8, group_stack(s.wide8.max_stack)};
+    if (requested == 8 && s.wide8.nodes && s.wide8.node_count < (1ull << 24) && group_stack(s.wide8.max_stack))
+        return {8, group_stack(s.wide8.max_stack)};
     if (requested >= 4 && s.wide4.nodes && wide_stack(s.wide4.max_stack)) return {4, wide_stack(s.wide4.max_stack)};
     return {2, stack_for(s.depth)};
 }
@@ -555,8 +557,8 @@ int lr_gpu_scene_upload(lr_context *ctx, const lr_scene *scene, lr_gpu_scene **o
         s.faces = (const uint32_t *)(base + parts[5].offset);
         s.ids = (const uint32_t *)(base + parts[6].offset);
         s.shading = (const uint4 *)(base + parts[7].offset);
-        s.wide4 = DeviceWide{(const float4 *)(base + parts[8].offset), T ? 4 : 0, w4.max_stack};
-        s.wide8 = DeviceWide{(const float4 *)(base + parts[9].offset), T ? 8 : 0, w8.max_stack};
+        s.wide4 = DeviceWide{(const float4 *)(base + parts[8].offset), T ? 4 : 0, w4.max_stack, w4.node_count};
+        s.wide8 = DeviceWide{(const float4 *)(base + parts[9].offset), T ? 8 : 0, w8.max_stack, w8.node_count};
         gs->wide4_nodes = w4.node_count;
         gs->wide8_nodes = w8.node_count;
         gs->parents = (uint32_t *)(base + parts[10].offset);

@@ -36,7 +36,8 @@ struct DeviceBvh {
 struct DeviceWide {
     const float4 *nodes = nullptr;
     int width = 0;
-    uint32_t max_stack = 0;  // the most stack entries a traversal can hold
+    uint32_t max_stack = 0;   // the most stack entries a traversal can hold
+    uint64_t node_count = 0;
 };
 
 // A scene in HBM (GpuScene, device.lucb:16-38).

@@ -52,7 +52,7 @@ __global__ void __launch_bounds__(kShadeBlock) camera_kernel(Wave w) {
     const uint32_t paths = plan->head.paths;
     if (blockIdx.x == 0) {
         const uint32_t light_base = kLightCounters * w.rounds + 2;
-        for (uint32_t i = threadIdx.x; i < 4 * w.rounds + 2; i += blockDim.x)
+        for (uint32_t i = threadIdx.x; i < counter_slots(w.rounds); i += blockDim.x)
             w.counters[i] = i == 0 ? plan->head.camera_paths : (i == light_base ? paths - plan->head.camera_paths : 0u);
     }
     const uint32_t stride = gridDim.x * blockDim.x;
@@ -594,6 +594,8 @@ struct WaveHost {
     // this (0: none). The wavefront compacts every round (warp- or block-aggregated
     // pushes); this is how often it also sorts.
     uint32_t bin_interval = 0;
+    // Idle lanes at which a traversal warp takes new queue entries (0: grid-stride walks).
+    uint32_t refill_at = 0;
     uint32_t fill = 0;
     // The most camera paths a pass takes (0: as many as fit): a renderer's band, so that
     // its passes are the reference's bands, light paths riding along in a sample's first.
@@ -636,12 +638,12 @@ void mark(cudaStream_t stream, Marks *marks, int kind) {
 // Records a pass's tracing on `stream` with traversal (width, stack entries) in blocks of
 // `block` threads: camera, then (closest, shade, shadow) for every round. With `marks`,
 // an event follows each kernel (profiling); `count` takes the counting traversals.
-void record_trace(const WaveHost *h, const Wave &w, int width, int stack, int block, bool count, int grid_trace,
-                  bool tracing, bool glossy, bool cutouts, cudaStream_t stream, Marks *marks) {
+void record_trace(const WaveHost *h, const Wave &w, int width, int stack, int block, bool count, bool refill,
+                  int grid_trace, bool tracing, bool glossy, bool cutouts, cudaStream_t stream, Marks *marks) {
     camera_kernel<<<h->grid_shade, kShadeBlock, 0, stream>>>(w);
     mark(stream, marks, kCamera);
     for (uint32_t round = 0; round < w.rounds; round++) {
-        launch_closest(width, stack, block, count, grid_trace, stream, w, round);
+        launch_closest(width, stack, block, count, refill, grid_trace, stream, w, round);
         mark(stream, marks, kClosest);
         if (glossy) {
             if (tracing) {
@@ -657,7 +659,7 @@ void record_trace(const WaveHost *h, const Wave &w, int width, int stack, int bl
             shade_kernel<false, false, false><<<h->grid_shade, kShadeBlock, 0, stream>>>(w, round);
         }
         mark(stream, marks, kSurface);
-        launch_shadow(width, stack, block, count, cutouts, grid_trace, stream, w, round);
+        launch_shadow(width, stack, block, count, cutouts, refill, grid_trace, stream, w, round);
         mark(stream, marks, kShadow);
     }
     LR_CUDA(cudaGetLastError());
@@ -682,9 +684,11 @@ constexpr int kTraceBlocks[3] = {kTraceBlock, 64, 256};
 
 // A pass's variant: its traversal (BVH width * 1000 + stack entries), plus kTracingVariant
 // when it holds light tracing, kGlossyVariant when it holds glossy materials,
-// kCutoutVariant when it holds cut-outs, and kBlockVariant times the index of the
-// traversal kernels' block size in kTraceBlocks.
-constexpr int kTracingVariant = 100000, kGlossyVariant = 200000, kCutoutVariant = 400000, kBlockVariant = 800000;
+// kCutoutVariant when it holds cut-outs, kBlockVariant times the index of the traversal
+// kernels' block size in kTraceBlocks, and kRefillVariant when its traversal warps refill
+// idle lanes from the queue.
+constexpr int kTracingVariant = 100000, kGlossyVariant = 200000, kCutoutVariant = 400000, kBlockVariant = 800000,
+              kRefillVariant = 3 * kBlockVariant;
 
 int variant_block(int variant) { return kTraceBlocks[(variant / kBlockVariant) % 3]; }
 
@@ -698,11 +702,11 @@ bool traversal_exists(int width, int stack) {
     }
 }
 
-int grid_for(WaveHost *h, int width, int stack, int block) {
-    const int key = width * 1000 + stack + block * 100000;
+int grid_for(WaveHost *h, int width, int stack, int block, bool refill) {
+    const int key = width * 1000 + stack + block * 100000 + (refill ? 100000000 : 0);
     auto it = h->grid_trace.find(key);
     if (it != h->grid_trace.end()) return it->second;
-    const int g = closest_grid(width, stack, block, h->ctx->sm_count);
+    const int g = closest_grid(width, stack, block, refill, h->ctx->sm_count);
     h->grid_trace[key] = g;
     return g;
 }
@@ -711,8 +715,9 @@ void record_trace_any(WaveHost *h, const Wave &w, int variant, cudaStream_t stre
     const int flags = (variant / kTracingVariant) & 7;
     const int traversal = variant % kTracingVariant;
     const int width = traversal / 1000, stack = traversal % 1000, block = variant_block(variant);
-    const int grid = grid_for(h, width, stack, block);
-    record_trace(h, w, width, stack, block, h->profile >= 2, grid, flags & 1, flags & 2, flags & 4, stream, marks);
+    const bool count = h->profile >= 2, refill = variant >= kRefillVariant && !count;
+    const int grid = grid_for(h, width, stack, block, refill);
+    record_trace(h, w, width, stack, block, count, refill, grid, flags & 1, flags & 2, flags & 4, stream, marks);
 }
 
 // Captures whatever `body` queues on a private stream as a graph.
@@ -775,7 +780,7 @@ void lanes_create(WaveHost *h) {
             for (int j = 0; j < 3; j++) p_ray[q][j] = L.add(nullptr, P * 16);
         const size_t p_shadow_o = L.add(nullptr, P * 16), p_shadow_d = L.add(nullptr, P * 16);
         const size_t p_shadow_c = L.add(nullptr, P * 16);
-        const size_t p_counters = L.add(nullptr, (4 * (size_t)rounds + 2) * 4);
+        const size_t p_counters = L.add(nullptr, (size_t)counter_slots(rounds) * 4);
         const size_t p_plan = L.add(nullptr, sizeof(Plan));
         // Ray records (settings.profile = 3): three float4 per queue entry and round, for
         // the closest-hit and the shadow queue.
@@ -839,6 +844,12 @@ void wave_create(WaveHost *h, lr_context *ctx, uint64_t pool, uint32_t rounds, u
     h->capacity = capacity;
     h->profile = profile;
     h->lane_count = profile ? 1 : 2;
+    // The environment variable LUCE_RENDER_B200_REFILL (1 to 32) sets the idle lanes at
+    // which traversal warps refill until a tuner chooses, for measurement.
+    if (const char *env = std::getenv("LUCE_RENDER_B200_REFILL")) {
+        const int v = std::atoi(env);
+        if (v >= 1 && v <= 32) h->refill_at = (uint32_t)v;
+    }
     LR_CUDA(cudaSetDevice(ctx->device));
     {
         Layout L;
@@ -1453,8 +1464,10 @@ bool launch_pass(WaveHost *h, bool dry = false, int only = -1) {
     const int block = h->class_block[dominant] ? h->class_block[dominant] : kTraceBlock;
     const int block_index = block == kTraceBlocks[1] ? 1 : (block == kTraceBlocks[2] ? 2 : 0);
     const int variant = width * 1000 + stack + (tracing ? kTracingVariant : 0) + (glossy ? kGlossyVariant : 0) +
-                        (cutouts ? kCutoutVariant : 0) + block_index * kBlockVariant;
-    staging->head = PlanHeader{n, used, converts, dry ? 1u : 0u, camera_paths, folds, adapts, h->bin_interval};
+                        (cutouts ? kCutoutVariant : 0) + block_index * kBlockVariant +
+                        (h->refill_at ? kRefillVariant : 0);
+    staging->head = PlanHeader{n, used, converts, dry ? 1u : 0u, camera_paths, folds, adapts, h->bin_interval,
+                               h->refill_at, {0u, 0u, 0u}};
     staging->display = PlanDisplay{0ull, h->display_scale, h->display_view, 0u, 0u};
     if (h->display_block && converts > 0) {
         rec.display_slot = free_display_slot(h);
@@ -1518,7 +1531,7 @@ void launch_convert(WaveHost *h) {
     rec.number = h->recorded;
     rec.members.push_back({0u, false});
     rec.generations.push_back(mh.generation);
-    staging->head = PlanHeader{0u, 0u, 1u, 0u, 0u, 0u, 0u, 0u};
+    staging->head = PlanHeader{0u, 0u, 1u, 0u, 0u, 0u, 0u, 0u, 0u, {0u, 0u, 0u}};
     staging->convert[0] = 0u;
     staging->convert_samples[0] = mh.sample;
     rec.display_slot = free_display_slot(h);
@@ -1684,6 +1697,22 @@ void wave_tune(WaveHost *h, lr_batch_tuning *out) {
         }
     }
     h->bin_interval = best_interval;
+    // Persistent warps that refill their idle lanes from the queue, at 32 (a whole warp at
+    // a time), 16 or 8 idle lanes, against the grid-stride walks.
+    uint32_t best_refill = h->refill_at;
+    for (uint32_t refill : {0u, 32u, 16u, 8u}) {
+        if (refill == h->refill_at) continue;
+        const uint32_t kept = h->refill_at;
+        h->refill_at = refill;
+        const double rate = time_dry(h, -1, a, b);
+        tried++;
+        if (rate > best) {
+            best = rate;
+            best_refill = refill;
+        }
+        h->refill_at = kept;
+    }
+    h->refill_at = best_refill;
     cudaEventDestroy(a);
     cudaEventDestroy(b);
     if (out) {
@@ -1691,6 +1720,7 @@ void wave_tune(WaveHost *h, lr_batch_tuning *out) {
         out->paths_per_ms = best;
         out->candidates = tried;
         out->bin_interval = best_interval;
+        out->refill_at = best_refill;
         int widest = 0;
         for (int cls = 0; cls < kSizeClasses; cls++) widest = std::max(widest, h->class_width[cls]);
         out->width = (uint32_t)(widest ? widest : 2);
@@ -1968,7 +1998,8 @@ void create(lr_context *ctx, const lr_scene *scene, const lr_settings &settings,
                 trace_graph(&r->wave, r->wave.lanes[li],
                             c.width * 1000 + c.stack + (r->wave.members[0].dev.light_paths ? kTracingVariant : 0) +
                                 (r->wave.members[0].dev.glossy ? kGlossyVariant : 0) +
-                                (r->wave.members[0].dev.cutouts ? kCutoutVariant : 0));
+                                (r->wave.members[0].dev.cutouts ? kCutoutVariant : 0) +
+                                (r->wave.refill_at ? kRefillVariant : 0));
     } catch (...) {
         const bool owned = !r->wave.members.empty() && r->wave.members[0].used;
         wave_destroy(&r->wave);

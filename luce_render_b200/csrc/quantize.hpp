@@ -9,11 +9,14 @@
 // traversal stays conservative and the watertight hits exact.
 //
 // Node: 6 x 16 bytes (96 bytes, 16-byte aligned)
-//   [0]  origin x, y, z; w: biased exponents ex, ey, ez (bytes 0-2) and the child count (byte 3)
-//   [1]  child links 0-3, [2] child links 4-7 (>= 0 a node, < 0 a leaf: -1 - (first << 4 | count - 1))
-//   [3]  low x planes of children 0-7 (bytes), then their high x planes
+//   [0]  origin x, y, z; w: biased exponents ex, ey, ez (bytes 0-2) and the occupied
+//        slots (byte 3, bit s: slot s holds a child)
+//   [1]  child links of slots 0-3, [2] of slots 4-7 (>= 0 a node, < 0 a leaf:
+//        -1 - (first << 4 | count - 1))
+//   [3]  low x planes of slots 0-7 (bytes), then their high x planes
 //   [4]  the same for y, [5] for z
-// Unused slots hold an inverted box (low plane 255, high plane 0), which every ray misses.
+// Which child takes which slot is the builder's choice (wide.cpp orders them by direction
+// octant); an unused slot has link 0 and an inverted box (low plane 255, high plane 0).
 #pragma once
 
 #include <stdint.h>
@@ -47,17 +50,19 @@ LR_HD inline uint32_t q_exponent(float extent) {
 
 LR_HD inline float q_floor(float v) { return (float)(int64_t)(v >= 0.0f ? v : v - 0.99999994f); }
 
-// Writes one node (24 floats, as 6 float4s) from `count` (<= 8) child boxes lo/hi (3
-// floats each, already widened) and their links.
-LR_HD inline void quantize_node(int count, const float (*lo)[3], const float (*hi)[3], const int *links, float *out) {
-    float origin[3], top[3];
-    for (int k = 0; k < 3; k++) {
-        origin[k] = lo[0][k];
-        top[k] = hi[0][k];
-        for (int c = 1; c < count; c++) {
-            origin[k] = lo[c][k] < origin[k] ? lo[c][k] : origin[k];
-            top[k] = hi[c][k] > top[k] ? hi[c][k] : top[k];
+// Writes one node (24 floats, as 6 float4s) from the child boxes lo/hi (3 floats each,
+// already widened) and links of the slots set in `occupied` (at least one).
+LR_HD inline void quantize_node(uint32_t occupied, const float (*lo)[3], const float (*hi)[3], const int *links,
+                                float *out) {
+    float origin[3] = {0.0f, 0.0f, 0.0f}, top[3] = {0.0f, 0.0f, 0.0f};
+    bool any = false;
+    for (int c = 0; c < 8; c++) {
+        if (!((occupied >> c) & 1u)) continue;
+        for (int k = 0; k < 3; k++) {
+            origin[k] = !any || lo[c][k] < origin[k] ? lo[c][k] : origin[k];
+            top[k] = !any || hi[c][k] > top[k] ? hi[c][k] : top[k];
         }
+        any = true;
     }
     uint32_t exps[3];
     uint8_t planes[3][2][8];
@@ -68,7 +73,7 @@ LR_HD inline void quantize_node(int count, const float (*lo)[3], const float (*h
             const float s = q_step(e);
             bool fits = true;
             for (int c = 0; c < 8 && fits; c++) {
-                if (c >= count) {
+                if (!((occupied >> c) & 1u)) {
                     planes[k][0][c] = 255;
                     planes[k][1][c] = 0;
                     continue;
@@ -98,10 +103,10 @@ LR_HD inline void quantize_node(int count, const float (*lo)[3], const float (*h
         float f;
     } w;
     for (int k = 0; k < 3; k++) out[k] = origin[k];
-    w.u = exps[0] | exps[1] << 8 | exps[2] << 16 | (uint32_t)count << 24;
+    w.u = exps[0] | exps[1] << 8 | exps[2] << 16 | (occupied & 0xffu) << 24;
     out[3] = w.f;
     for (int c = 0; c < 8; c++) {
-        w.u = (uint32_t)(c < count ? links[c] : 0);
+        w.u = (uint32_t)(((occupied >> c) & 1u) ? links[c] : 0);
         out[4 + c] = w.f;
     }
     for (int k = 0; k < 3; k++) {

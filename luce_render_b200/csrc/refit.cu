@@ -218,18 +218,18 @@ __global__ void wide_kernel(uint64_t slots, int width, const uint32_t *sources, 
 }
 
 // Step 4 for the compressed 8-wide tree: node n quantized again (quantize.hpp) from its
-// children's BVH2 boxes (or the root's), widened as at upload; its links and child count
-// stay.
+// children's BVH2 boxes (or the root's), widened as at upload; its links and occupied
+// slots stay.
 __global__ void quantize_kernel(uint64_t count, const uint32_t *sources, const float4 *exact, const float *root_box,
                                 float delta, float4 *nodes) {
     for (uint64_t n = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; n < count; n += (uint64_t)gridDim.x * blockDim.x) {
         float *node = reinterpret_cast<float *>(nodes + n * kQNodeFloat4s);
-        const int children = (int)(__float_as_uint(node[3]) >> 24);
+        const uint32_t occupied = __float_as_uint(node[3]) >> 24;
         float lo[8][3], hi[8][3];
         int links[8];
         for (int c = 0; c < 8; c++) {
             links[c] = __float_as_int(node[4 + c]);
-            if (c >= children) continue;
+            if (!((occupied >> c) & 1u)) continue;
             const uint32_t source = sources[n * 8 + c];
             Box b;
             if (source == kRefitRoot) {
@@ -246,7 +246,7 @@ __global__ void quantize_kernel(uint64_t count, const uint32_t *sources, const f
             }
         }
         float out[kQNodeFloat4s * 4];
-        quantize_node(children, lo, hi, links, out);
+        quantize_node(occupied, lo, hi, links, out);
         for (int k = 0; k < kQNodeFloat4s * 4; k++) node[k] = out[k];
     }
 }

@@ -489,7 +489,7 @@ struct CompressedTracer {
     float3 inv, oinv;
     Shear sh;
     Hit h;
-    int node;
+    uint32_t oct;  // bit k: the direction's component k is negative (its inverse, here)
     int *base;
     int stride;
     int sp = 0;
@@ -505,7 +505,7 @@ struct CompressedTracer {
         inv = safe_inverse(r.d);
         oinv = neg_origin_times(r.o, inv);
         sh = make_shear(r.o, r.d);
-        node = 0;
+        oct = (inv.x < 0.0f ? 1u : 0u) | (inv.y < 0.0f ? 2u : 0u) | (inv.z < 0.0f ? 4u : 0u);
         float enter;
         return box_exact(b.root_lo[0], b.root_hi[0], b.root_lo[1], b.root_hi[1], b.root_lo[2], b.root_hi[2], inv, oinv,
                          r.tmin, r.tmax, enter);
@@ -516,38 +516,26 @@ struct CompressedTracer {
         return __uint_as_float(__byte_perm(w, 0x4B000000u, (uint32_t)k | 0x7540u)) - 8388608.0f;
     }
 
-    static __device__ __forceinline__ void order(float &ka, uint32_t &la, float &kb, uint32_t &lb) {
-        const bool swap = ka > kb;
-        const float k = swap ? kb : ka;
-        const uint32_t l = swap ? lb : la;
-        kb = swap ? ka : kb;
-        lb = swap ? la : lb;
-        ka = k;
-        la = l;
-    }
-
-    // Tests node n's children. False when none is hit; else `next` is the nearest hit
-    // child's link and `more` the other hit slots, nearest first, four bits each with
-    // their count in the top four bits (0: none).
+    // Tests node n's children. False when none is hit; else `next` is the link of the hit
+    // child of lowest rank (rank = slot ^ the ray's octant: the builder's nearest-first
+    // order for this direction) and `more` the ranks of the other hit children, one bit
+    // each (0: none).
     __device__ __forceinline__ bool visit(const float4 *n, int &next, uint32_t &more) {
         const float4 head = __ldg(n), la = __ldg(n + 1), lb = __ldg(n + 2), px = __ldg(n + 3), py = __ldg(n + 4),
                      pz = __ldg(n + 5);
         const uint32_t meta = __float_as_uint(head.w);
-        const int count = (int)(meta >> 24);
         const float ax = q_step(meta & 0xffu) * inv.x, ay = q_step((meta >> 8) & 0xffu) * inv.y,
                     az = q_step((meta >> 16) & 0xffu) * inv.z;
         const float bx = fmaf(head.x, inv.x, oinv.x), by = fmaf(head.y, inv.y, oinv.y), bz = fmaf(head.z, inv.z, oinv.z);
         // The near and far plane bytes of each axis for this ray's direction signs.
-        const bool px_up = inv.x >= 0.0f, py_up = inv.y >= 0.0f, pz_up = inv.z >= 0.0f;
+        const bool px_up = !(oct & 1u), py_up = !(oct & 2u), pz_up = !(oct & 4u);
         const uint32_t nx0 = __float_as_uint(px_up ? px.x : px.z), nx1 = __float_as_uint(px_up ? px.y : px.w);
         const uint32_t fx0 = __float_as_uint(px_up ? px.z : px.x), fx1 = __float_as_uint(px_up ? px.w : px.y);
         const uint32_t ny0 = __float_as_uint(py_up ? py.x : py.z), ny1 = __float_as_uint(py_up ? py.y : py.w);
         const uint32_t fy0 = __float_as_uint(py_up ? py.z : py.x), fy1 = __float_as_uint(py_up ? py.w : py.y);
         const uint32_t nz0 = __float_as_uint(pz_up ? pz.x : pz.z), nz1 = __float_as_uint(pz_up ? pz.y : pz.w);
         const uint32_t fz0 = __float_as_uint(pz_up ? pz.z : pz.x), fz1 = __float_as_uint(pz_up ? pz.w : pz.y);
-        const float kMiss = __int_as_float(0x7f800000);
-        float key[8];
-        uint32_t slot[8];
+        uint32_t mask = 0;
 #pragma unroll
         for (int c = 0; c < 8; c++) {
             const int k = c & 3;
@@ -558,42 +546,31 @@ struct CompressedTracer {
                                   fmaxf(fmaf(byte_at(nz, k), az, bz), r.tmin));
             const float l = fmin3(fmaf(byte_at(fx, k), ax, bx), fmaf(byte_at(fy, k), ay, by),
                                   fminf(fmaf(byte_at(fz, k), az, bz), h.t)) * 1.0000003576f;
-            key[c] = c < count && e <= l ? e : kMiss;
-            slot[c] = (uint32_t)c;
+            mask |= e <= l ? 1u << c : 0u;
         }
-        if (!kAny) {
-            constexpr int kNet[19][2] = {{0, 2}, {1, 3}, {4, 6}, {5, 7}, {0, 4}, {1, 5}, {2, 6},
-                                         {3, 7}, {0, 1}, {2, 3}, {4, 5}, {6, 7}, {2, 4}, {3, 5},
-                                         {1, 4}, {3, 6}, {1, 2}, {3, 4}, {5, 6}};
-#pragma unroll
-            for (int i = 0; i < 19; i++) order(key[kNet[i][0]], slot[kNet[i][0]], key[kNet[i][1]], slot[kNet[i][1]]);
-        }
-        // The hit slots, nearest first: up to 8 nibbles in 64 bits.
-        uint64_t packed = 0;
-        uint32_t hits = 0;
-#pragma unroll
-        for (int c = 7; c >= 0; c--)
-            if (key[c] != kMiss) {
-                packed = (packed << 4) | slot[c];
-                hits++;
-            }
-        if (!hits) return false;
-        const uint32_t first = (uint32_t)packed & 0xfu;
-        more = hits > 1u ? ((hits - 1u) << 28) | (uint32_t)(packed >> 4) : 0u;
+        mask &= meta >> 24;  // occupied slots only
+        if (!mask) return false;
+        // From slots to ranks: bit s moves to bit s ^ oct.
+        if (oct & 1u) mask = ((mask & 0x55u) << 1) | ((mask >> 1) & 0x55u);
+        if (oct & 2u) mask = ((mask & 0x33u) << 2) | ((mask >> 2) & 0x33u);
+        if (oct & 4u) mask = ((mask & 0x0fu) << 4) | ((mask >> 4) & 0x0fu);
+        const uint32_t slot = (uint32_t)(__ffs(mask) - 1) ^ oct;
+        more = mask & (mask - 1u);
         const int links[8] = {__float_as_int(la.x), __float_as_int(la.y), __float_as_int(la.z), __float_as_int(la.w),
                               __float_as_int(lb.x), __float_as_int(lb.y), __float_as_int(lb.z), __float_as_int(lb.w)};
         int chosen = links[0];
 #pragma unroll
-        for (int c = 1; c < 8; c++) chosen = first == (uint32_t)c ? links[c] : chosen;
+        for (int c = 1; c < 8; c++) chosen = slot == (uint32_t)c ? links[c] : chosen;
         next = chosen;
         return true;
     }
 
-    // Runs to the end of the ray's traversal.
+    // Runs to the end of the ray's traversal. A group is a node with the ranks of its hit
+    // children not yet visited: (node << 8) | ranks, one int on the stack.
     __device__ __forceinline__ bool step(const DeviceScene &s, bool &overflow, Visits &visits) {
         const float4 *nodes = s.wide8.nodes;
-        uint32_t group_node = 0, rest = 0;  // the group being walked: node and packed slots
-        int link = 0;                       // the wide root
+        uint32_t group = 0;  // the group being walked (no ranks left: none)
+        int link = 0;        // the wide root
         for (;;) {
             if (link >= 0) {
                 if (kCount) visits.nodes++;
@@ -604,17 +581,15 @@ struct CompressedTracer {
                     // The nearest hit child next; the group walked so far waits on the stack
                     // and this node's other hit children become the group in hand.
                     if (more) {
-                        if (rest) {
+                        if (group & 0xffu) {
                             if (sp < kStack) {
-                                base[(2 * sp) * stride] = (int)group_node;
-                                base[(2 * sp + 1) * stride] = (int)rest;
+                                base[sp * stride] = (int)group;
                                 sp++;
                             } else {
                                 overflow = true;
                             }
                         }
-                        group_node = (uint32_t)link;
-                        rest = more;
+                        group = ((uint32_t)link << 8) | more;
                     }
                     link = next;
                     continue;
@@ -640,15 +615,14 @@ struct CompressedTracer {
                 }
             }
             // The next child: from the group in hand, else from the stack.
-            if (!rest) {
+            if (!(group & 0xffu)) {
                 if (sp == 0) return true;
                 sp--;
-                group_node = (uint32_t)base[(2 * sp) * stride];
-                rest = (uint32_t)base[(2 * sp + 1) * stride];
+                group = (uint32_t)base[sp * stride];
             }
-            const uint32_t slot = rest & 0xfu, left = (rest >> 28) - 1u;
-            rest = left ? (left << 28) | ((rest & 0x0fffffffu) >> 4) : 0u;
-            link = __ldg(reinterpret_cast<const int *>(nodes + (size_t)group_node * kQNodeFloat4s + 1) + slot);
+            const uint32_t slot = (uint32_t)(__ffs(group & 0xffu) - 1) ^ oct;
+            group &= group - 1u;  // the lowest rank: a bit of the low byte
+            link = __ldg(reinterpret_cast<const int *>(nodes + (size_t)(group >> 8) * kQNodeFloat4s + 1) + slot);
         }
     }
 };
@@ -674,7 +648,7 @@ struct TracerOf {
 template <bool kAny, int kStack, bool kCount>
 struct TracerOf<8, kAny, kStack, kCount> {
     using type = CompressedTracer<kAny, kStack, kCount>;
-    static constexpr int kInts = 2 * kStack;  // (node, packed slots) a group
+    static constexpr int kInts = kStack;  // (node << 8) | ranks, a group
 };
 template <bool kAny, int kStack, bool kCount>
 struct TracerOf<2, kAny, kStack, kCount> {
@@ -698,6 +672,50 @@ __device__ __forceinline__ void trace_strided(const DeviceScene &s, uint32_t cou
             }
         }
         store(i, tr.h, tr.r);
+    }
+}
+
+// Persistent warps that replace finished rays from a shared queue (Aila and Laine,
+// "Understanding the Efficiency of Ray Traversal on GPUs", HPG 2009: dynamic fetch with
+// replacement of terminated rays). Each lane keeps one ray; once `refill_at` lanes of
+// the warp (1 to 32) have none, one lane takes that many consecutive queue entries with
+// one atomic on `next` (zero when the launch starts) and the idle lanes share them in
+// lane order. `begin(i, s)` loads ray i, its scene into `s` and starts the tracer: true
+// when there is a walk to take, else it has finished ray i itself; `end(i)` finishes ray
+// i after its walk. Finished walks wait for the refill to end, so that the lanes that
+// finished run `end` together rather than one or two at a time. The warp stays converged
+// around each ballot; a walk ends in a bounded number of steps, so every warp leaves once
+// the queue is drained.
+template <class Tracer, class Begin, class End>
+__device__ __forceinline__ void trace_refilling(Tracer &tr, uint32_t count, uint32_t *next, uint32_t refill_at,
+                                                Begin begin, End end, bool &overflow, Visits &visits) {
+    const uint32_t lane = threadIdx.x & 31u;
+    DeviceScene s;
+    uint32_t i = 0;
+    bool busy = false, ended = true, drained = false;
+    for (;;) {
+        const uint32_t idle = __ballot_sync(0xffffffffu, !busy);
+        const uint32_t want = (uint32_t)__popc(idle);
+        const bool last = drained && idle == 0xffffffffu;
+        if (last || (!drained && want >= refill_at)) {
+            if (!busy && !ended) {
+                end(i);
+                ended = true;
+            }
+            if (last) break;
+            uint32_t base = 0;
+            if (lane == 0) base = atomicAdd(next, want);
+            base = __shfl_sync(0xffffffffu, base, 0);
+            drained = base + want >= count;
+            if (!busy) {
+                i = base + (uint32_t)__popc(idle & ((1u << lane) - 1u));
+                if (i < count) {
+                    busy = begin(i, s);
+                    ended = !busy;
+                }
+            }
+        }
+        if (busy && tr.step(s, overflow, visits)) busy = false;
     }
 }
 

@@ -18,6 +18,10 @@ namespace lr {
 
 constexpr int kTraceBlock = 128;     // the traversal kernels' block size unless tuned
 constexpr int kTraceBlockMax = 256;  // the largest the autotuner tries (64, 128, 256)
+// Resident blocks of kTraceBlockMax the traversal kernels are built for: at most 64
+// registers a thread, so that 32 warps of an SM hide the node and triangle fetches (the
+// walk through cut-outs, a kernel of its own, takes what it needs).
+constexpr int kTraceMinBlocks = 4;
 constexpr int kShadeBlock = 128;
 constexpr size_t kDefaultPool = 2097152;  // 2^21 paths (integrator.lucb:98)
 // A ray's tag: the path's pool index in the low bits, its segment in the high bits.
@@ -90,6 +94,9 @@ struct PlanHeader {
     // bin_interval: the shade kernels group outgoing rays by direction octant in rounds
     // that are multiples of it (0: never; an autotuner choice).
     uint32_t camera_paths, folds, adapts, bin_interval;
+    // refill_at: the traversal kernels' persistent warps take new queue entries once this
+    // many of their lanes are idle (1 to 32; 0: grid-stride walks; an autotuner choice).
+    uint32_t refill_at, reserved[3];
 };
 
 // A renderer's display image for the pass (film_convert.comp:50-52): where the pass that
@@ -129,7 +136,9 @@ struct Wave {
     // Ray queues hold camera paths' rays from the front and light paths' from the back
     // (index pool - 1 - k), so that each kind shades in a launch of its own.
     // counters[r]: camera paths' rays of round r; counters[rounds + 1 + r]: shadow rays of
-    // round r; counters[kLightCounters * rounds + 2 + r] (light_counter): light paths' rays.
+    // round r; counters[kLightCounters * rounds + 2 + r] (light_counter): light paths' rays;
+    // counters[4 * rounds + 2 + 2r] and the one after (fetch_counter): the next closest and
+    // shadow queue entry of round r a refilling warp takes. counter_slots(rounds) in all.
     uint32_t *counters;
     unsigned long long *stats;  // closest rays, shadow rays, paths, passes, then traversal work
     int *status;
@@ -144,6 +153,10 @@ constexpr uint32_t kLightCounters = 2;
 __device__ __forceinline__ uint32_t *light_counter(const Wave &w, uint32_t round) {
     return &w.counters[kLightCounters * w.rounds + 2 + round];
 }
+__device__ __forceinline__ uint32_t *fetch_counter(const Wave &w, uint32_t round, bool shadow) {
+    return &w.counters[4 * w.rounds + 2 + 2 * round + (shadow ? 1u : 0u)];
+}
+constexpr uint32_t counter_slots(uint32_t rounds) { return 6 * rounds + 4; }
 
 __device__ __forceinline__ uint32_t warp_push(uint32_t *counter, bool want) {
     const unsigned mask = __ballot_sync(0xffffffffu, want);
@@ -182,12 +195,13 @@ __device__ __forceinline__ uint32_t tag_light_index(const Wave &w, uint32_t tag)
 
 // trace.cu: the closest-hit and shadow kernels of round `round` on `stream`, traversal
 // variant (width, stack) in blocks of `block` threads (kTraceBlocks); `count`
-// instantiates the counting traversals, `cutouts` the shadow walk through cut-outs.
-// closest_grid: the resident grid of a variant at a block size.
-void launch_closest(int width, int stack, int block, bool count, int grid, cudaStream_t stream, const Wave &w,
-                    uint32_t round);
-void launch_shadow(int width, int stack, int block, bool count, bool cutouts, int grid, cudaStream_t stream,
-                   const Wave &w, uint32_t round);
-int closest_grid(int width, int stack, int block, int sm_count);
+// instantiates the counting traversals, `cutouts` the shadow walk through cut-outs,
+// `refill` the persistent warps that refill idle lanes (trace_refilling; not with the
+// other two). closest_grid: the resident grid of a variant at a block size.
+void launch_closest(int width, int stack, int block, bool count, bool refill, int grid, cudaStream_t stream,
+                    const Wave &w, uint32_t round);
+void launch_shadow(int width, int stack, int block, bool count, bool cutouts, bool refill, int grid,
+                   cudaStream_t stream, const Wave &w, uint32_t round);
+int closest_grid(int width, int stack, int block, bool refill, int sm_count);
 
 }  // namespace lr

@@ -11,6 +11,12 @@
 // -inf). W = 8: compressed, 96 bytes -- the node's origin and per-axis power-of-two steps,
 // 8 child links, and each child's planes as 8-bit multiples of the steps, rounded outward
 // (quantize.hpp). Links: >= 0 a wide node, < 0 a leaf (-1 - (first << 4 | count - 1)).
+// The 8-wide node's children take slots by direction octant (Ylitie et al. 2017, section
+// 3.2): slot s stands for the direction whose component k is negative where bit k of s is
+// set, and children are placed greedily, the (child, slot) pair whose centroid lies
+// furthest back along the slot's direction first. A ray whose direction signs make octant
+// o then visits its hit children in the order of slot ^ o, nearest-first approximately,
+// without sorting them.
 // Boxes are widened outward like the BVH2 path's before they are stored or quantized.
 #include "wide.hpp"
 
@@ -32,6 +38,46 @@ float bits(int v) {
     float f;
     std::memcpy(&f, &v, sizeof f);
     return f;
+}
+
+// The slot of each of `m` (<= 8) children of a node by direction octant: repeatedly the
+// free (child, slot) pair with the smallest projection of the child's centroid, taken
+// from the node's centre, on the slot's direction (ties: lower child, then lower slot).
+void octant_slots(const lr_bvh_node *const *children, int m, int *slot_of) {
+    float centre[3];
+    for (int k = 0; k < 3; k++) {
+        float lo = children[0]->lo[k], hi = children[0]->hi[k];
+        for (int i = 1; i < m; i++) {
+            lo = std::min(lo, children[i]->lo[k]);
+            hi = std::max(hi, children[i]->hi[k]);
+        }
+        centre[k] = 0.5f * (lo + hi);
+    }
+    float cost[8][8];
+    for (int i = 0; i < m; i++)
+        for (int s = 0; s < 8; s++) {
+            float c = 0.0f;
+            for (int k = 0; k < 3; k++) {
+                const float offset = 0.5f * (children[i]->lo[k] + children[i]->hi[k]) - centre[k];
+                c += ((s >> k) & 1) ? -offset : offset;
+            }
+            cost[i][s] = c;
+        }
+    bool child_done[8] = {false}, slot_taken[8] = {false};
+    for (int round = 0; round < m; round++) {
+        int bi = -1, bs = -1;
+        for (int i = 0; i < m; i++) {
+            if (child_done[i]) continue;
+            for (int s = 0; s < 8; s++)
+                if (!slot_taken[s] && (bi < 0 || cost[i][s] < cost[bi][bs])) {
+                    bi = i;
+                    bs = s;
+                }
+        }
+        child_done[bi] = true;
+        slot_taken[bs] = true;
+        slot_of[bi] = bs;
+    }
 }
 
 }  // namespace
@@ -101,18 +147,26 @@ WideBvh build_wide(const std::vector<lr_bvh_node> &nodes, int width, float delta
         w.nodes.assign(count * kQNodeFloat4s * 4, 0.0f);
         for (size_t n = 0; n < count; n++) {
             const auto &list = children_of[n];
-            float lo[8][3], hi[8][3];
+            const int m = (int)list.size();
+            const lr_bvh_node *kids[8];
+            int slot_of[8];
+            for (int i = 0; i < m; i++) kids[i] = &nodes[list[i]];
+            octant_slots(kids, m, slot_of);
+            float lo[8][3] = {}, hi[8][3] = {};
             int links[8] = {0};
-            for (size_t slot = 0; slot < list.size(); slot++) {
-                w.sources[n * width + slot] = list[slot];
-                const lr_bvh_node &c = nodes[list[slot]];
+            uint32_t occupied = 0;
+            for (int i = 0; i < m; i++) {
+                const int slot = slot_of[i];
+                occupied |= 1u << slot;
+                w.sources[n * width + slot] = list[i];
+                const lr_bvh_node &c = *kids[i];
                 for (int k = 0; k < 3; k++) {
                     lo[slot][k] = widen_down(c.lo[k], delta);
                     hi[slot][k] = widen_up(c.hi[k], delta);
                 }
-                links[slot] = c.count > 0 ? leaf_link(c) : (int)index_of_bvh2[list[slot]];
+                links[slot] = c.count > 0 ? leaf_link(c) : (int)index_of_bvh2[list[i]];
             }
-            quantize_node((int)list.size(), lo, hi, links, &w.nodes[n * kQNodeFloat4s * 4]);
+            quantize_node(occupied, lo, hi, links, &w.nodes[n * kQNodeFloat4s * 4]);
         }
         // A traversal keeps one group of a node's unvisited children a level: the stack
         // holds at most the tree's interior depth.

@@ -110,6 +110,22 @@ def test_batch_limits(ctx, cases):
         lr.Batch(ctx, lr.BatchSettings.default(pool=0))
 
 
+@pytest.mark.parametrize("refill", [32, 8, 1])
+def test_refilling_warps_equal_grid_stride(ctx, cases, refill, monkeypatch):
+    # Traversal warps that hand idle lanes new queue entries once `refill` lanes are idle
+    # make the images the grid-stride walks make: a ray's result depends on it alone.
+    cs, uploads, alone = cases
+    monkeypatch.setenv("LUCE_RENDER_B200_REFILL", str(refill))
+    b = lr.Batch(ctx, lr.BatchSettings.default(pool=1500, max_bounces=12, capacity=16))
+    try:
+        members = [b.add(gs, sc, s) for gs, (sc, s) in zip(uploads, cs)]
+        b.finish()
+        for m, want in zip(members, alone):
+            assert np.array_equal(_bits(b.read(m)), _bits(want)), m
+    finally:
+        b.destroy()
+
+
 def test_tuning_changes_speed_not_images(ctx, cases):
     cs, uploads, alone = cases
     b = lr.Batch(ctx, lr.BatchSettings.default(pool=2048, max_bounces=12, capacity=16))
@@ -119,6 +135,7 @@ def test_tuning_changes_speed_not_images(ctx, cases):
             b.advance()
         t = b.tune()
         assert t["width"] in (2, 4, 8) and t["fill"] in (512, 1024, 2048)
+        assert t["refill_at"] in (0, 32, 16, 8) and t["bin_interval"] in (0, 1, 2)
         assert t["candidates"] >= 4 and t["paths_per_ms"] > 0
         # The cases hold scenes under 16k triangles and one of about 20k.
         assert t["class_members"][0] >= 1 and t["class_members"][1] == 1 and t["class_members"][2] == 0

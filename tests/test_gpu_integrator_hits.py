@@ -62,10 +62,12 @@ def _shadow_equal(a, rays, got):
     return np.count_nonzero(traced)
 
 
-@pytest.mark.parametrize("spectral", [True, False])
-def test_cornell_pass_hits_equal_brute_force(ctx, spectral):
+@pytest.mark.parametrize("spectral,refill", [(True, 0), (False, 0), (True, 16)])
+def test_cornell_pass_hits_equal_brute_force(ctx, spectral, refill, monkeypatch):
     # The 34-triangle Cornell box with its rect light at 256 x 256, one sample, eight
-    # bounces: every recorded ray of every round, closest and shadow, light tracing on.
+    # bounces: every recorded ray of every round, closest and shadow, light tracing on;
+    # grid-stride traversal, and warps refilling at 16 idle lanes.
+    monkeypatch.setenv("LUCE_RENDER_B200_REFILL", str(refill))
     sc = lr.compile_scene(scenes.cornell_meshes(True), [scenes.cornell_camera()], [scenes.cornell_light()],
                           scenes.cornell_materials())
     a = sc.arrays()
@@ -88,10 +90,13 @@ def test_cornell_pass_hits_equal_brute_force(ctx, spectral):
         sc.close()
 
 
-def test_million_triangle_pass_hits_equal_queries_and_brute_force(ctx):
+@pytest.mark.parametrize("refill", [0, 8])
+def test_million_triangle_pass_hits_equal_queries_and_brute_force(ctx, refill, monkeypatch):
     # The 1,048,576-triangle workload at 320 x 240, one sample, six bounces, spectral:
     # every ray of every round against lr_trace_rays; 4,096 rays of rounds 0 and 1 and
-    # 4,096 shadow rays of round 0 against the brute force.
+    # 4,096 shadow rays of round 0 against the brute force. Grid-stride traversal, and
+    # warps refilling at 8 idle lanes.
+    monkeypatch.setenv("LUCE_RENDER_B200_REFILL", str(refill))
     meshes, mats, lights, cam = scenes.incoherent_scene()
     sc = lr.compile_scene(meshes, [cam], lights, mats)
     a = sc.arrays()
