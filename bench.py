@@ -326,6 +326,8 @@ def served(lr, scenes, dist, seconds: float):
     ring = [(lr.PinnedArray((2_000_000,), np.uint32), lr.PinnedArray((2_000_000,), np.float32)) for _ in range(32)]
     submitted = []
     dist.barrier()
+    clocks = Clocks(dist.local)
+    clocks.ready()
     start = time.perf_counter()
     for k, (at, kind, scene, a, b) in enumerate(arrivals):
         while time.perf_counter() - start < at:
@@ -343,6 +345,7 @@ def served(lr, scenes, dist, seconds: float):
             submitted.append(("render", server.submit_render(ids[scene], s)))
     window = time.perf_counter() - start
     stats_window = server.stats()
+    clock_record = clocks.stop()
     # Probes still queued finish; sessions are cut at the end of the stream.
     for kind, rid in submitted:
         if kind == "probe":
@@ -392,6 +395,9 @@ def served(lr, scenes, dist, seconds: float):
         "failures": failures,
         "uploads": stats_window["uploads"], "evictions": stats_window["evictions"],
         "tunings": stats_window.get("tunings", 0),
+        "render_thread": {k: stats_window[k] for k in ("passes", "seconds_advance", "seconds_wait",
+                                                       "seconds_progress", "seconds_admit", "seconds_tune")},
+        "clocks": clock_record,
         "queued_at_end": stats_window["queued"], "live_at_end": stats_window["live"],
         "timing": "host steady clock of the server, from submission; the stream is cut at its end",
     }
@@ -435,6 +441,23 @@ def batched(lr, scenes, ctx, dist):
     batch_ms = dist.max(ctx.timer_stop())
     identical = all(np.array_equal(b.read(m).view(np.uint32), img.view(np.uint32)) for m, img in zip(members, alone))
     passes = b.stats().passes
+    # The same batch kept busy for `sustain` seconds (each member 32 more samples at a
+    # time), as a server is: the rate the device holds under its power limit.
+    sustain = 20.0
+    dist.barrier()
+    ctx.synchronize()
+    clocks = Clocks(dist.local)
+    clocks.ready()
+    shaded0 = b.stats().shaded
+    t0 = time.perf_counter()
+    ctx.timer_start()
+    while time.perf_counter() - t0 < sustain:
+        for m in members:
+            b.set_samples(m, b.info(m)[2] + BATCH_SPP)
+        b.finish()
+    sustained_ms = dist.max(ctx.timer_stop())
+    sustained_samples = b.stats().shaded - shaded0
+    sustained_clocks = clocks.stop()
     b.destroy()
     for gs in uploads:
         gs.destroy()
@@ -451,6 +474,10 @@ def batched(lr, scenes, ctx, dist):
         "loop_ms": loop_ms, "batched_ms": batch_ms,
         "loop_value": loop_rate, "batched_value": batch_rate, "speedup": loop_ms / batch_ms,
         "identical_images": identical, "pool": BATCH_POOL, "passes": passes, "tuning": tuning,
+        "sustained": {"seconds": sustained_ms / 1e3,
+                      "value": dist.sum(sustained_samples) / (sustained_ms / 1e3) / 1e6,
+                      "clocks": sustained_clocks,
+                      "note": "the tuned batch kept busy (32 more samples a member at a time) for 20 s"},
         "timing": "device (CUDA events on the context stream), renderers and batch members made beforehand",
     }
 

@@ -518,6 +518,12 @@ int lr_batch_read(lr_batch *batch, uint32_t member, float *rgba, uint64_t float_
 /* lr_renderer_read_async / _wait for a member of a batch. */
 int lr_batch_read_async(lr_batch *batch, uint32_t member, float *rgba, uint64_t count);
 int lr_batch_read_wait(lr_batch *batch);
+/* As lr_batch_read_async, and *ticket names the copy. lr_batch_read_landed sets *landed to
+ * 1 once the copy with `ticket` (and every copy queued before it) has arrived in host
+ * memory, else 0, without waiting. A member whose image is being read stays in the batch
+ * (lr_batch_remove after it landed). */
+int lr_batch_read_ticket(lr_batch *batch, uint32_t member, float *rgba, uint64_t count, uint64_t *ticket);
+int lr_batch_read_landed(lr_batch *batch, uint64_t ticket, int32_t *landed);
 /* The autotuner: times trial passes (which trace but change no film and move no member
  * on) on the members as they stand. For each scene-size class present (under 16k
  * triangles, under 128k, larger) it keeps the BVH width (2, 4, 8; a width all of the
@@ -600,6 +606,11 @@ typedef struct {
     uint64_t bytes_in_use;  /* resident scenes, live sessions and the pool */
     double seconds;         /* since the server started */
     uint64_t tunings;       /* autotuner runs on the live mix (from 32 live sessions, every 20 s) */
+    /* The render thread: passes it queued, and host seconds spent queueing them, waiting
+     * for the oldest in flight, noting progress (images out included), admitting, and
+     * tuning. */
+    uint64_t passes;
+    double seconds_advance, seconds_wait, seconds_progress, seconds_admit, seconds_tune;
 } lr_server_stats;
 
 /* device 0, budget 150 GB, capacity 128, pool 2^22, max_bounces 12, probe_priority 1. */

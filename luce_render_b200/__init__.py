@@ -269,7 +269,9 @@ class ServerStats(C.Structure):
     """lr_server_stats."""
     _fields_ = [(n, C.c_uint64) for n in ("sessions_done", "probes_done", "failed", "pixel_samples", "probe_rays",
                                           "uploads", "evictions", "queued", "live", "scenes_resident",
-                                          "bytes_in_use")] + [("seconds", C.c_double), ("tunings", C.c_uint64)]
+                                          "bytes_in_use")] + [("seconds", C.c_double), ("tunings", C.c_uint64),
+                                                              ("passes", C.c_uint64)] + [
+        (n, C.c_double) for n in ("seconds_advance", "seconds_wait", "seconds_progress", "seconds_admit", "seconds_tune")]
 
 
 _vp, _i32, _u32, _u64, _sz = C.c_void_p, C.c_int32, C.c_uint32, C.c_uint64, C.c_size_t
@@ -337,6 +339,8 @@ _SIGNATURES = {
     "lr_renderer_read_wait": (C.c_int, [_vp]),
     "lr_batch_read_async": (C.c_int, [_vp, _u32, C.POINTER(C.c_float), _u64]),
     "lr_batch_read_wait": (C.c_int, [_vp]),
+    "lr_batch_read_ticket": (C.c_int, [_vp, _u32, C.POINTER(C.c_float), _u64, C.POINTER(C.c_uint64)]),
+    "lr_batch_read_landed": (C.c_int, [_vp, _u64, C.POINTER(C.c_int32)]),
     "lr_batch_join": (C.c_int, [_vp]),
     "lr_renderer_kernel_times": (C.c_int, [_vp, C.POINTER(C.c_double)]),
     "lr_renderer_stats": (C.c_int, [_vp, C.POINTER(RenderStats)]),
@@ -1043,6 +1047,10 @@ class Batch:
     def finish(self) -> None:
         _check(lib.lr_batch_finish(self.handle))
 
+    def join(self) -> None:
+        """Waits for the passes in flight and retires them."""
+        _check(lib.lr_batch_join(self.handle))
+
     def info(self, member: int):
         """(samples done, samples planned, samples asked for)."""
         d, p, n = C.c_uint32(), C.c_uint32(), C.c_uint32()
@@ -1098,6 +1106,20 @@ class Batch:
 
     def read_wait(self) -> None:
         _check(lib.lr_batch_read_wait(self.handle))
+
+    def read_ticket(self, member: int, out: np.ndarray) -> int:
+        """read_async, returning a ticket for read_landed."""
+        if out.dtype != np.float32 or not out.flags.c_contiguous:
+            raise RenderError(INVALID, "reading the image needs four floats a pixel")
+        t = C.c_uint64()
+        _check(lib.lr_batch_read_ticket(self.handle, member, _fptr(out), out.size, C.byref(t)))
+        return int(t.value)
+
+    def read_landed(self, ticket: int) -> bool:
+        """Whether the copy with `ticket` (and every one before it) has arrived; never waits."""
+        v = C.c_int32()
+        _check(lib.lr_batch_read_landed(self.handle, ticket, C.byref(v)))
+        return bool(v.value)
 
     def kernel_times(self) -> np.ndarray:
         out = (C.c_double * 10)()

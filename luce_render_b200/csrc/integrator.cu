@@ -518,6 +518,10 @@ struct MemberHost {
     uint32_t light_next = 0;  // light paths of the current sample planned so far
     uint32_t max_bounces = 0;
     uint64_t last_pass = 0;  // the last pass (plus one) that traced it; 0: none
+    // Passes recorded when its memory and records were last queued (add, restart): a
+    // read before a later pass orders itself after those uploads.
+    uint64_t placed_at = 0;
+    uint64_t read_ticket = 0;  // its latest image read (member_read_async), 0: none
     // Restarts so far (integrator.lucb:572-582): passes of an older generation finish
     // uncounted; and what a restart needs again without reloading.
     uint32_t generation = 0;
@@ -607,6 +611,11 @@ struct WaveHost {
     cudaStream_t copy_stream = nullptr;
     cudaEvent_t read_done = nullptr;
     uint64_t reads = 0;
+    // Ticketed reads (member_read_ticket) in flight, oldest first, with the event each
+    // copy records; the newest ticket seen landed; events to reuse.
+    std::deque<std::pair<uint64_t, cudaEvent_t>> read_marks;
+    uint64_t reads_landed = 0;
+    std::vector<cudaEvent_t> spare_marks;
     // A renderer's display images (integrator.lucb:695-713): three rgba16f images of
     // `display_pixels`, the one shown (`front`, -1 none yet) and its size; a pass that ends
     // a sample writes one that is neither shown nor written by a pass in flight, and it
@@ -1135,6 +1144,8 @@ uint32_t member_add(WaveHost *h, const lr_gpu_scene *gs, lr_gpu_scene *owned, co
     mh.sample = mh.next_pixel = mh.done = mh.light_next = 0;
     mh.max_bounces = settings.max_bounces;
     mh.last_pass = 0;
+    mh.placed_at = h->recorded;
+    mh.read_ticket = 0;
     mh.view_pixels = pixels;
     mh.view_traced = traced.count > 0;
     mh.view_adaptive = adaptive;
@@ -1242,6 +1253,7 @@ void member_renew(WaveHost *h, uint32_t index, const lr_frame &frame, const lr_s
         mh.owned = owned;
     }
     mh.generation++;
+    mh.placed_at = h->recorded;
     mh.sample = mh.next_pixel = mh.done = mh.light_next = 0;
     mh.settings = chosen;
     mh.samples = chosen.samples;
@@ -1250,9 +1262,13 @@ void member_renew(WaveHost *h, uint32_t index, const lr_frame &frame, const lr_s
     mh.emit_share = emit_share;
 }
 
-void member_free(MemberHost &mh, cudaStream_t stream, cudaEvent_t reads = nullptr) {
-    // A read in flight may still copy from the member's image.
-    if (reads) cudaStreamWaitEvent(stream, reads, 0);
+// The event of read `ticket` while it may still be in flight, else null.
+cudaEvent_t read_in_flight(WaveHost *h, uint64_t ticket);
+
+void member_free(WaveHost *h, MemberHost &mh, cudaStream_t stream) {
+    // A read of the member's image still in flight finishes first.
+    if (h && mh.read_ticket)
+        if (cudaEvent_t e = read_in_flight(h, mh.read_ticket)) cudaStreamWaitEvent(stream, e, 0);
     if (mh.block) cudaFreeAsync(mh.block, stream);
     if (mh.view) cudaFreeAsync(mh.view, stream);
     if (mh.owned) lr_gpu_scene_destroy(mh.owned);
@@ -1262,7 +1278,7 @@ void member_free(MemberHost &mh, cudaStream_t stream, cudaEvent_t reads = nullpt
 // Frees members that asked to leave once no pass in flight traces them.
 void collect(WaveHost *h) {
     for (auto &mh : h->members)
-        if (mh.used && mh.leaving && mh.last_pass <= h->retired) member_free(mh, h->ctx->stream, h->read_done);
+        if (mh.used && mh.leaving && mh.last_pass <= h->retired) member_free(h, mh, h->ctx->stream);
 }
 
 bool has_work(const MemberHost &mh) { return mh.used && !mh.leaving && mh.sample < mh.samples; }
@@ -1776,10 +1792,14 @@ void wave_destroy(WaveHost *h) {
         if (e) cudaEventDestroy(e);
     if (h->copy_stream) cudaStreamSynchronize(h->copy_stream);
     for (auto &mh : h->members)
-        if (mh.used) member_free(mh, h->ctx->stream);
+        if (mh.used) member_free(nullptr, mh, h->ctx->stream);
     cudaStreamSynchronize(h->ctx->stream);
     h->staging.release();
     if (h->read_done) cudaEventDestroy(h->read_done);
+    for (auto &mark : h->read_marks) cudaEventDestroy(mark.second);
+    for (cudaEvent_t mark : h->spare_marks) cudaEventDestroy(mark);
+    h->read_marks.clear();
+    h->spare_marks.clear();
     if (h->copy_stream) cudaStreamDestroy(h->copy_stream);
     for (auto &[pass, gs] : h->retiring_scenes) lr_gpu_scene_destroy(gs);
     h->retiring_scenes.clear();
@@ -1853,30 +1873,73 @@ void member_read(WaveHost *h, uint32_t member, float *rgba, uint64_t count) {
     LR_CUDA(cudaStreamSynchronize(h->ctx->stream));
 }
 
-// Queues a copy of the member's image as the pass launched last leaves it into `rgba`
-// (pinned host memory, so that the copy runs beside the passes after it) and returns
-// without waiting; member_read_wait waits for every copy queued.
-void member_read_async(WaveHost *h, uint32_t member, float *rgba, uint64_t count) {
+// Whether the copy with `ticket` (and so every copy queued before it, on the one copy
+// stream) has arrived; never waits.
+bool member_read_landed(WaveHost *h, uint64_t ticket) {
+    while (!h->read_marks.empty()) {
+        const cudaError_t e = cudaEventQuery(h->read_marks.front().second);
+        if (e == cudaErrorNotReady) break;
+        LR_CUDA(e);
+        h->reads_landed = h->read_marks.front().first;
+        h->spare_marks.push_back(h->read_marks.front().second);
+        h->read_marks.pop_front();
+    }
+    return ticket <= h->reads_landed;
+}
+
+cudaEvent_t read_in_flight(WaveHost *h, uint64_t ticket) {
+    if (member_read_landed(h, ticket)) return nullptr;
+    for (auto &mark : h->read_marks)
+        if (mark.first >= ticket) return mark.second;
+    return h->read_done;
+}
+
+// Queues a copy of the member's image as the passes launched so far leave it into
+// `rgba` (pinned host memory, so that the copy runs beside the passes after it) and
+// returns its ticket without waiting; member_read_wait waits for every copy queued,
+// member_read_landed says whether one has arrived. The copy waits only for what last
+// wrote the image: the member's last pass while it may still run, or the uploads of
+// its memory when no pass has traced it since.
+uint64_t member_read_async(WaveHost *h, uint32_t member, float *rgba, uint64_t count) {
     MemberHost &mh = member_at(h, member);
     if (count != mh.dev.pixels * 4) fail(LR_INVALID, "reading the image needs four floats a pixel");
     if (!h->copy_stream) {
         LR_CUDA(cudaStreamCreateWithFlags(&h->copy_stream, cudaStreamNonBlocking));
         LR_CUDA(cudaEventCreateWithFlags(&h->read_done, cudaEventDisableTiming));
     }
-    // After the member's memory arrived (the context's stream) and the last pass launched.
-    cudaEvent_t ready;
-    LR_CUDA(cudaEventCreateWithFlags(&ready, cudaEventDisableTiming));
-    LR_CUDA(cudaEventRecord(ready, h->ctx->stream));
-    LR_CUDA(cudaStreamWaitEvent(h->copy_stream, ready, 0));
-    LR_CUDA(cudaEventDestroy(ready));
-    if (h->recorded > 0) LR_CUDA(cudaStreamWaitEvent(h->copy_stream, lane_of(h, h->recorded - 1).finished, 0));
+    if (mh.last_pass <= mh.placed_at) {
+        // No pass since its memory was queued on the context's stream.
+        cudaEvent_t ready;
+        LR_CUDA(cudaEventCreateWithFlags(&ready, cudaEventDisableTiming));
+        LR_CUDA(cudaEventRecord(ready, h->ctx->stream));
+        LR_CUDA(cudaStreamWaitEvent(h->copy_stream, ready, 0));
+        LR_CUDA(cudaEventDestroy(ready));
+    } else if (mh.last_pass > h->retired) {
+        // Its lane's event stands for that pass or a later one on the lane.
+        LR_CUDA(cudaStreamWaitEvent(h->copy_stream, lane_of(h, mh.last_pass - 1).finished, 0));
+    }
     LR_CUDA(cudaMemcpyAsync(rgba, mh.dev.image, count * 4, cudaMemcpyDeviceToHost, h->copy_stream));
     LR_CUDA(cudaEventRecord(h->read_done, h->copy_stream));
     h->reads++;
+    cudaEvent_t mark;
+    if (!h->spare_marks.empty()) {
+        mark = h->spare_marks.back();
+        h->spare_marks.pop_back();
+    } else {
+        LR_CUDA(cudaEventCreateWithFlags(&mark, cudaEventDisableTiming));
+    }
+    LR_CUDA(cudaEventRecord(mark, h->copy_stream));
+    h->read_marks.push_back({h->reads, mark});
+    mh.read_ticket = h->reads;
+    return h->reads;
 }
 
 void member_read_wait(WaveHost *h) {
     if (h->read_done) LR_CUDA(cudaEventSynchronize(h->read_done));
+}
+
+uint64_t member_read_ticket(WaveHost *h, uint32_t member, float *rgba, uint64_t count) {
+    return member_read_async(h, member, rgba, count);
 }
 
 }  // namespace
@@ -2441,6 +2504,20 @@ int lr_batch_read_wait(lr_batch *b) {
     return guarded([&] {
         if (!b) fail(LR_INVALID, "no batch");
         member_read_wait(&b->wave);
+    });
+}
+
+int lr_batch_read_ticket(lr_batch *b, uint32_t member, float *rgba, uint64_t count, uint64_t *ticket) {
+    return guarded([&] {
+        if (!b || !rgba || !ticket) fail(LR_INVALID, "no batch");
+        *ticket = member_read_ticket(&b->wave, member, rgba, count);
+    });
+}
+
+int lr_batch_read_landed(lr_batch *b, uint64_t ticket, int32_t *landed) {
+    return guarded([&] {
+        if (!b || !landed) fail(LR_INVALID, "no batch");
+        *landed = member_read_landed(&b->wave, ticket) ? 1 : 0;
     });
 }
 

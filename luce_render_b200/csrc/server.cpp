@@ -5,8 +5,11 @@
 //   sessions are admitted, in arrival order, while a live slot is free and the device
 //   memory budget holds their scene (uploaded on first use) and their film; idle scenes
 //   are evicted least recently used first to make room. Every live session advances in
-//   the same passes; the thread keeps one pass queued behind the one running, and
-//   between passes admits, retires and notes progress (first image, completion).
+//   the same passes; the thread keeps two passes in flight, and while the newer one runs
+//   admits, retires and notes progress (first image, completion). A
+//   finished session's image leaves through a pinned buffer, its copy queued beside the
+//   passes that follow and its session retired once it has landed; nothing the thread
+//   does between passes waits for the device.
 // - A probe thread runs probe queries on its own high-priority stream, so a probe's
 //   kernel starts ahead of the next render kernel instead of behind the queued passes.
 //   Probes go through lr_probe_static, which allocates nothing, up to its pixel limit.
@@ -17,6 +20,7 @@
 #include <atomic>
 #include <chrono>
 #include <condition_variable>
+#include <cstring>
 #include <deque>
 #include <mutex>
 #include <string>
@@ -58,7 +62,22 @@ struct Request {
     uint32_t samples = 0, samples_done = 0;
     uint64_t bytes = 0;  // device bytes a live session holds (film, image, lights)
     double submitted = -1, admitted = -1, first = -1, finished = -1;
+    // A finished session's image on its way out: the pinned buffer it lands in and the
+    // batch's ticket for the copy.
+    float *staging = nullptr;
+    uint64_t staging_bytes = 0, ticket = 0;
 };
+
+// Pinned host buffers that finished images land in before they are copied to the
+// caller's memory, so that a copy runs beside the passes after it rather than draining
+// them; reused by size (powers of two from 1 MiB), at most kStagingLimit bytes in all.
+constexpr uint64_t kStagingLimit = 1ull << 30;
+
+uint64_t staging_size(uint64_t bytes) {
+    uint64_t size = 1ull << 20;
+    while (size < bytes) size <<= 1;
+    return size;
+}
 
 double seconds_since(Clock::time_point t0) {
     return std::chrono::duration<double>(Clock::now() - t0).count();
@@ -87,6 +106,8 @@ struct lr_server {
     // the mix, and again when the mix may have changed (every kRetune seconds).
     double tuned_at = -1.0;
     uint64_t tunings = 0;
+    std::vector<std::pair<uint64_t, float *>> staging_free;  // (bytes, buffer)
+    uint64_t staging_total = 0;
 };
 
 namespace {
@@ -229,6 +250,77 @@ void admit(lr_server *s, std::unique_lock<std::mutex> &lk) {
     }
 }
 
+// A pinned buffer of at least `bytes` for a finished image, or null when the staging
+// limit is reached. Lock held (released while a buffer is allocated).
+float *take_staging(lr_server *s, std::unique_lock<std::mutex> &lk, uint64_t bytes, uint64_t &size) {
+    size = staging_size(bytes);
+    for (size_t i = 0; i < s->staging_free.size(); i++)
+        if (s->staging_free[i].first == size) {
+            float *buffer = s->staging_free[i].second;
+            s->staging_free.erase(s->staging_free.begin() + (long)i);
+            return buffer;
+        }
+    if (s->staging_total + size > kStagingLimit) return nullptr;
+    s->staging_total += size;
+    lk.unlock();
+    void *buffer = nullptr;
+    const cudaError_t e = cudaHostAlloc(&buffer, size, cudaHostAllocDefault);
+    lk.lock();
+    if (e != cudaSuccess) {
+        cudaGetLastError();
+        s->staging_total -= size;
+        return nullptr;
+    }
+    return (float *)buffer;
+}
+
+// Copies a finished session's image out: a ticketed read into a pinned buffer, landed
+// on a later call; or, with no buffer to spare, a read that waits. True once the image
+// is in the caller's memory (or failed: `status`). Lock held (released around copies).
+bool image_out(lr_server *s, std::unique_lock<std::mutex> &lk, Request &r, int &status, std::string &message) {
+    const uint64_t bytes = r.pixels * 16;
+    if (!r.staging) {
+        uint64_t size = 0;
+        float *buffer = take_staging(s, lk, bytes, size);
+        if (!buffer) {
+            lk.unlock();
+            if (lr_batch_read(s->batch, r.member, r.rgba, r.pixels * 4) != LR_OK) {
+                status = LR_DEVICE;
+                message = lr_last_error();
+            }
+            lk.lock();
+            return true;
+        }
+        r.staging = buffer;
+        r.staging_bytes = size;
+        lk.unlock();
+        const int e = lr_batch_read_ticket(s->batch, r.member, buffer, r.pixels * 4, &r.ticket);
+        const std::string why = e == LR_OK ? "" : lr_last_error();
+        lk.lock();
+        if (e != LR_OK) {
+            status = LR_DEVICE;
+            message = why;
+        } else {
+            return false;  // lands on a later call
+        }
+    } else {
+        int32_t landed = 0;
+        if (lr_batch_read_landed(s->batch, r.ticket, &landed) != LR_OK) {
+            status = LR_DEVICE;
+            message = lr_last_error();
+        } else if (!landed) {
+            return false;
+        } else {
+            lk.unlock();
+            std::memcpy(r.rgba, r.staging, bytes);
+            lk.lock();
+        }
+    }
+    s->staging_free.push_back({r.staging_bytes, r.staging});
+    r.staging = nullptr;
+    return true;
+}
+
 // Notes each live session's progress after a pass retired; retires finished ones. Lock
 // held (released while a finished image is copied out).
 void progress(lr_server *s, std::unique_lock<std::mutex> &lk) {
@@ -245,13 +337,9 @@ void progress(lr_server *s, std::unique_lock<std::mutex> &lk) {
         if (done >= r.samples) {
             int status = LR_OK;
             std::string message;
-            if (r.rgba) {
-                lk.unlock();
-                if (lr_batch_read(s->batch, r.member, r.rgba, r.pixels * 4) != LR_OK) {
-                    status = LR_DEVICE;
-                    message = lr_last_error();
-                }
-                lk.lock();
+            if (r.rgba && !image_out(s, lk, r, status, message)) {
+                i++;  // its image is on its way
+                continue;
             }
             lr_batch_remove(s->batch, r.member);
             SceneSlot &slot = s->scenes[r.scene];
@@ -269,9 +357,12 @@ void progress(lr_server *s, std::unique_lock<std::mutex> &lk) {
 
 void render_loop(lr_server *s) {
     std::unique_lock<std::mutex> lk(s->mu);
+    auto since = [](Clock::time_point t) { return std::chrono::duration<double>(Clock::now() - t).count(); };
     for (;;) {
         if (s->stopping) break;
+        Clock::time_point t = Clock::now();
         admit(s, lk);
+        s->stats.seconds_admit += since(t);
         if (s->live.empty()) {
             if (s->render_queue.empty())
                 s->cv_work.wait(lk, [&] { return s->stopping || !s->render_queue.empty(); });
@@ -285,24 +376,47 @@ void render_loop(lr_server *s) {
         lk.unlock();
         if (retune) {
             // Dry passes on the live sessions (films untouched): the BVH width, stack and
-            // block size per scene-size class, the pass fill and the ray sort interval.
+            // block size per scene-size class, the pass fill, the ray sort interval and
+            // the traversal warps' refill.
+            t = Clock::now();
             const bool tuned = lr_batch_tune(s->batch, nullptr) == LR_OK;
             std::lock_guard<std::mutex> note(s->mu);
             if (tuned) s->tunings++;
             s->tuned_at = seconds_since(s->t0);
+            s->stats.seconds_tune += since(t);
         }
+        // Two passes in flight (a pass queues only while fewer run), then the oldest
+        // retires: one pass always runs while this thread admits and retires sessions,
+        // and the two lanes overlap one pass's thin last rounds with the next one's first.
         int32_t more = 0, in_flight = 0;
+        t = Clock::now();
         int status = lr_batch_advance(s->batch, &more);
+        if (status == LR_OK) status = lr_batch_advance(s->batch, &more);
+        const double advancing = since(t);
+        t = Clock::now();
         if (status == LR_OK) status = lr_batch_wait(s->batch, &in_flight);
+        const double waiting = since(t);
         std::string message = status == LR_OK ? "" : lr_last_error();
         lk.lock();
+        s->stats.seconds_advance += advancing;
+        s->stats.seconds_wait += waiting;
+        s->stats.passes++;
         if (status != LR_OK) {
             // A device failure ends every live session with its status.
-            for (uint64_t id : s->live) finish_request(s, s->requests[id], status, message);
+            for (uint64_t id : s->live) {
+                Request &r = s->requests[id];
+                if (r.staging) {
+                    s->staging_free.push_back({r.staging_bytes, r.staging});
+                    r.staging = nullptr;
+                }
+                finish_request(s, r, status, message);
+            }
             s->live.clear();
             continue;
         }
+        t = Clock::now();
         progress(s, lk);
+        s->stats.seconds_progress += since(t);
     }
 }
 
@@ -401,7 +515,10 @@ int lr_server_create(const lr_server_settings *settings, lr_server **out) {
             lr_batch_settings_default(&bs);
             bs.pool = settings->pool;
             bs.max_bounces = settings->max_bounces;
-            bs.capacity = settings->capacity;
+            // Room beyond the live sessions: a session that finished keeps its member's
+            // slot until the passes in flight retire, and a new session admitted
+            // meanwhile must not wait for them.
+            bs.capacity = settings->capacity * 2 + 16;
             check(lr_batch_create(s->ctx, &bs, &s->batch));
             // The wave's own memory: 15 float4 arrays of pool entries, and small parts; and
             // the static probe array (lr_probe_static), which the device holds from the
@@ -551,7 +668,10 @@ void lr_server_destroy(lr_server *s) {
             }
         s->cv_done.notify_all();
     }
-    if (s->batch) lr_batch_destroy(s->batch);
+    if (s->batch) lr_batch_destroy(s->batch);  // waits for its copies
+    for (auto &r : s->requests)
+        if (r.staging) s->staging_free.push_back({r.staging_bytes, r.staging});
+    for (auto &b : s->staging_free) cudaFreeHost(b.second);
     for (auto &slot : s->scenes)
         if (slot.gs) lr_gpu_scene_destroy(slot.gs);
     if (s->load_ctx) lr_context_destroy(s->load_ctx);

@@ -1,9 +1,13 @@
 // A wide BVH for the watertight traversal path, collapsed from the reference's BVH2: each
-// wide node holds up to W (4 or 8) children, taken by repeatedly opening the child with the
-// largest surface area (the greedy collapse of Wald et al. 2008 and Ylitie et al. 2017).
-// Leaves are the BVH2's leaves unchanged, so the wide tree reaches the same triangle
-// records in the same leaf order; only interior levels are merged, which cuts the
-// dependent node fetches along a ray by about log2(W).
+// wide node holds up to W (4 or 8) children. Which BVH2 nodes become wide nodes is chosen
+// by the surface area heuristic over the BVH2's own topology (Ylitie, Karras and Laine,
+// HPG 2017, section 3.1, after Pinto 2010): a dynamic program gives every BVH2 node its
+// least cost when it fills 1 to W child slots of its parent -- as one child (a wide node
+// of its own, or a leaf) or opened, its two children sharing the slots -- and the tree is
+// read back from the root. A leaf child is a BVH2 leaf, or a BVH2 subtree of at most
+// `max_leaf` triangles taken whole (a subtree's triangles are one contiguous range of
+// the leaf order): the wide tree reaches the same triangle records, and since a closest
+// hit does not depend on the visiting order, the same hits.
 //
 // Node layouts. W = 4: float4s, structure of arrays over the children so one load brings
 // a plane of every child: 7 float4 = 112 bytes -- lo.x, hi.x, lo.y, hi.y, lo.z, hi.z of
@@ -24,6 +28,7 @@
 
 #include <algorithm>
 #include <cmath>
+#include <cstdlib>
 #include <cstring>
 
 namespace lr {
@@ -80,7 +85,102 @@ void octant_slots(const lr_bvh_node *const *children, int m, int *slot_of) {
     }
 }
 
+// The SAH collapse: per BVH2 node its triangle range and, for 1 to W slots, its least
+// cost and how it fills them.
+struct Collapse {
+    static constexpr float kNodeCost = 1.0f, kTriangleCost = 0.3f;
+    const std::vector<lr_bvh_node> &nodes;
+    int width, max_leaf;
+    std::vector<uint32_t> first, tris;  // the subtree's triangles: [first, first + tris)
+    std::vector<float> cost;            // per node, W entries: C(n, 1 .. W slots)
+    std::vector<uint8_t> split;         // per node and slots: the left child's share when opened, 0 whole
+    std::vector<uint8_t> leaf;          // taken whole, the node is a leaf (else a wide node)
+
+    Collapse(const std::vector<lr_bvh_node> &n, int w, int m) : nodes(n), width(w), max_leaf(m) {
+        const size_t N = nodes.size();
+        first.assign(N, 0);
+        tris.assign(N, 0);
+        cost.assign(N * width, 0.0f);
+        split.assign(N * width, 0);
+        leaf.assign(N, 0);
+        // Children come after their parent in the BVH2's numbering: a reverse sweep is a
+        // post-order.
+        for (size_t i = N; i-- > 0;) solve((uint32_t)i);
+    }
+
+    float C(uint32_t n, int slots) const { return cost[(size_t)n * width + slots - 1]; }
+
+    void solve(uint32_t n) {
+        const lr_bvh_node &node = nodes[n];
+        const float area = area_of(node);
+        float *c = &cost[(size_t)n * width];
+        if (node.count > 0) {
+            first[n] = node.first;
+            tris[n] = node.count;
+            leaf[n] = 1;
+            for (int i = 0; i < width; i++) c[i] = area * kTriangleCost * (float)node.count;
+            return;
+        }
+        const uint32_t l = node.first, r = node.first + 1;
+        if (l <= n || r >= nodes.size()) fail(LR_INVALID, "a BVH2 node's children must follow it");
+        first[n] = std::min(first[l], first[r]);
+        tris[n] = tris[l] + tris[r];
+        // Opened: the two children share i slots.
+        float opened[9];
+        uint8_t share[9] = {0};
+        for (int i = 2; i <= width; i++) {
+            opened[i] = INFINITY;
+            for (int k = 1; k < i; k++) {
+                const float v = C(l, k) + C(r, i - k);
+                if (v < opened[i]) {
+                    opened[i] = v;
+                    share[i] = (uint8_t)k;
+                }
+            }
+        }
+        const float as_node = area * kNodeCost + opened[width];
+        const float as_leaf = (int)tris[n] <= max_leaf ? area * kTriangleCost * (float)tris[n] : INFINITY;
+        leaf[n] = as_leaf < as_node;
+        c[0] = std::min(as_node, as_leaf);
+        split[(size_t)n * width + width - 1] = share[width];  // a wide node's own children
+        for (int i = 2; i <= width; i++) {
+            const bool whole = c[0] <= opened[i];
+            c[i - 1] = whole ? c[0] : opened[i];
+            if (i < width) split[(size_t)n * width + i - 1] = whole ? 0 : share[i];
+        }
+    }
+
+    // The children of wide node n: its two BVH2 children sharing W slots.
+    void children(uint32_t n, std::vector<uint32_t> &out) const {
+        const uint32_t k = split[(size_t)n * width + width - 1];
+        gather(nodes[n].first, (int)k, out);
+        gather(nodes[n].first + 1, width - (int)k, out);
+    }
+
+    // Node n in `slots` slots: whole (one child), or opened.
+    void gather(uint32_t n, int slots, std::vector<uint32_t> &out) const {
+        const uint32_t k = slots >= 2 && slots < width ? split[(size_t)n * width + slots - 1] : 0;
+        if (slots == 1 || nodes[n].count > 0 || k == 0) {
+            out.push_back(n);
+            return;
+        }
+        gather(nodes[n].first, (int)k, out);
+        gather(nodes[n].first + 1, slots - (int)k, out);
+    }
+
+    // Taken whole, node n is a leaf child.
+    bool is_leaf(uint32_t n) const { return leaf[n] != 0; }
+};
+
 }  // namespace
+
+int wide_leaf_triangles() {
+    if (const char *env = std::getenv("LUCE_RENDER_B200_WIDE_LEAF")) {
+        const int v = std::atoi(env);
+        if (v >= 0 && v <= 16) return v;
+    }
+    return kWideLeafTriangles;
+}
 
 WideBvh build_wide(const std::vector<lr_bvh_node> &nodes, int width, float delta,
                    float (*widen_down)(float, float), float (*widen_up)(float, float),
@@ -90,6 +190,7 @@ WideBvh build_wide(const std::vector<lr_bvh_node> &nodes, int width, float delta
     const int per_node = width == 4 ? 7 : 14;
     w.floats_per_node = per_node;
     if (nodes.empty() || nodes[0].lo[0] > nodes[0].hi[0]) return w;  // no triangles
+    const Collapse plan(nodes, width, wide_leaf_triangles());
     struct Job {
         uint32_t bvh2;    // the BVH2 node this wide node stands for
         uint32_t wide;    // its index
@@ -102,25 +203,16 @@ WideBvh build_wide(const std::vector<lr_bvh_node> &nodes, int width, float delta
             list.push_back(n);  // a leaf root: one leaf child
             return list;
         }
-        list = {nodes[n].first, nodes[n].first + 1};
-        while ((int)list.size() < width) {
-            int best = -1;
-            float best_area = -1.0f;
-            for (size_t i = 0; i < list.size(); i++) {
-                const lr_bvh_node &c = nodes[list[i]];
-                if (c.count > 0) continue;
-                const float a = area_of(c);
-                if (a > best_area) {
-                    best_area = a;
-                    best = (int)i;
-                }
-            }
-            if (best < 0) break;
-            const uint32_t open = list[best];
-            list.erase(list.begin() + best);
-            list.insert(list.begin() + best, {nodes[open].first, nodes[open].first + 1});
-        }
+        plan.children(n, list);
         return list;
+    };
+    // A child taken as a leaf: a BVH2 leaf, or a subtree's triangle range.
+    auto is_leaf = [&](uint32_t c) { return plan.is_leaf(c); };
+    auto link_of_leaf = [&](uint32_t c) {
+        lr_bvh_node range = nodes[c];
+        range.first = plan.first[c];
+        range.count = plan.tris[c];
+        return leaf_link(range);
     };
     // Breadth first: a node's interior children get consecutive indices.
     children_of.push_back(collapse(0));
@@ -128,7 +220,7 @@ WideBvh build_wide(const std::vector<lr_bvh_node> &nodes, int width, float delta
     for (size_t head = 0; head < queue.size(); head++) {
         const uint32_t wide = queue[head].wide;
         for (uint32_t c : children_of[wide]) {
-            if (nodes[c].count > 0) continue;
+            if (is_leaf(c)) continue;
             const uint32_t index = (uint32_t)children_of.size();
             children_of.push_back(collapse(c));
             queue.push_back({c, index});
@@ -164,7 +256,7 @@ WideBvh build_wide(const std::vector<lr_bvh_node> &nodes, int width, float delta
                     lo[slot][k] = widen_down(c.lo[k], delta);
                     hi[slot][k] = widen_up(c.hi[k], delta);
                 }
-                links[slot] = c.count > 0 ? leaf_link(c) : (int)index_of_bvh2[list[i]];
+                links[slot] = is_leaf(list[i]) ? link_of_leaf(list[i]) : (int)index_of_bvh2[list[i]];
             }
             quantize_node(occupied, lo, hi, links, &w.nodes[n * kQNodeFloat4s * 4]);
         }
@@ -173,7 +265,7 @@ WideBvh build_wide(const std::vector<lr_bvh_node> &nodes, int width, float delta
         for (size_t n = count; n-- > 0;) {
             uint32_t deepest = 0;
             for (uint32_t c : children_of[n])
-                if (nodes[c].count == 0) deepest = std::max(deepest, bound[index_of_bvh2[c]]);
+                if (!is_leaf(c)) deepest = std::max(deepest, bound[index_of_bvh2[c]]);
             bound[n] = 1 + deepest;
         }
         w.max_stack = bound[0];
@@ -194,7 +286,7 @@ WideBvh build_wide(const std::vector<lr_bvh_node> &nodes, int width, float delta
                     lo[k] = widen_down(c.lo[k], delta);
                     hi[k] = widen_up(c.hi[k], delta);
                 }
-                link = c.count > 0 ? leaf_link(c) : (int)index_of_bvh2[list[slot]];
+                link = is_leaf(list[slot]) ? link_of_leaf(list[slot]) : (int)index_of_bvh2[list[slot]];
             }
             for (int k = 0; k < 3; k++) {
                 base[((2 * k) * planes) * 4 + slot] = lo[k];
@@ -208,7 +300,7 @@ WideBvh build_wide(const std::vector<lr_bvh_node> &nodes, int width, float delta
     for (size_t n = count; n-- > 0;) {
         uint32_t deepest = 0;
         for (uint32_t c : children_of[n])
-            if (nodes[c].count == 0) deepest = std::max(deepest, bound[index_of_bvh2[c]]);
+            if (!is_leaf(c)) deepest = std::max(deepest, bound[index_of_bvh2[c]]);
         bound[n] = (uint32_t)children_of[n].size() - 1 + deepest;
     }
     w.max_stack = bound[0];

@@ -18,6 +18,12 @@ struct WideBvh {
     std::vector<uint32_t> sources;
 };
 
+// The most triangles of a BVH2 subtree the collapse may take as one leaf of a wide tree.
+// The environment variable LUCE_RENDER_B200_WIDE_LEAF (0 to 16; 0 keeps the BVH2's leaves)
+// overrides it, for tuning.
+constexpr int kWideLeafTriangles = 0;
+int wide_leaf_triangles();
+
 // Collapses the BVH2 `nodes` into a `width`-wide BVH (4 or 8). Child boxes are widened by
 // `delta` with the given rounding, leaves encoded by `leaf_link`.
 WideBvh build_wide(const std::vector<lr_bvh_node> &nodes, int width, float delta, float (*widen_down)(float, float),

@@ -126,6 +126,45 @@ def test_refilling_warps_equal_grid_stride(ctx, cases, refill, monkeypatch):
         b.destroy()
 
 
+def test_ticketed_reads_land_the_images(ctx, cases):
+    # Reads queued with tickets while the other members' passes still run land the same
+    # images a waiting read gives; each ticket lands, and later tickets land after earlier.
+    cs, uploads, alone = cases
+    b = lr.Batch(ctx, lr.BatchSettings.default(pool=1500, max_bounces=12, capacity=16))
+    pinned = []
+    try:
+        members = [b.add(gs, sc, s) for gs, (sc, s) in zip(uploads, cs)]
+        tickets = []
+
+        def read_finished():
+            for m, (sc, s) in zip(members, cs):
+                if any(t[0] == m for t in tickets) or b.info(m)[0] < s.c.samples:
+                    continue
+                buf = lr.PinnedArray((s.c.height, s.c.width, 4), np.float32)
+                pinned.append(buf)
+                tickets.append((m, b.read_ticket(m, buf.array), buf))
+
+        for _ in range(100000):
+            more = b.advance()
+            read_finished()
+            if not more:
+                break
+        b.finish()
+        read_finished()
+        assert len(tickets) == len(members)
+        for k, (m, t, buf) in enumerate(tickets):
+            for _ in range(10000):
+                if b.read_landed(t):
+                    break
+            assert b.read_landed(t)
+            assert all(b.read_landed(tickets[j][1]) for j in range(k))
+            assert np.array_equal(_bits(buf.array), _bits(alone[members.index(m)])), m
+    finally:
+        b.destroy()
+        for buf in pinned:
+            buf.close()
+
+
 def test_tuning_changes_speed_not_images(ctx, cases):
     cs, uploads, alone = cases
     b = lr.Batch(ctx, lr.BatchSettings.default(pool=2048, max_bounces=12, capacity=16))
