@@ -446,29 +446,74 @@ struct Layout {
 };
 
 // Pinned host memory that stages uploads, so that they queue on a stream without
-// waiting for the work ahead of them; reused once its last copies have run.
+// waiting for the work ahead of them: a ring of up to kChunks buffers, each reused once
+// its own copies have run, so that a new upload waits only when every buffer is still
+// being copied from. `copied` follows the latest upload queued (a lane waits on it).
 struct Staging {
-    char *ptr = nullptr;
-    size_t capacity = 0;
+    static constexpr int kChunks = 8;
+    struct Chunk {
+        char *ptr = nullptr;
+        size_t capacity = 0;
+        cudaEvent_t done = nullptr;  // after the copies from it
+        uint64_t queued_at = 0;      // 0: never queued
+    };
+    Chunk chunks[kChunks];
+    int count = 0, current = -1;
+    uint64_t uploads = 0;
     cudaEvent_t copied = nullptr;
 
+    static bool idle(const Chunk &c) {
+        if (!c.queued_at) return true;
+        const cudaError_t e = cudaEventQuery(c.done);
+        if (e == cudaErrorNotReady) return false;
+        LR_CUDA(e);
+        return true;
+    }
+
     char *take(size_t bytes) {
-        if (copied) LR_CUDA(cudaEventSynchronize(copied));
-        if (bytes > capacity) {
-            if (ptr) LR_CUDA(cudaFreeHost(ptr));
-            ptr = nullptr;
-            capacity = std::max<size_t>(bytes, 1u << 20);
-            LR_CUDA(cudaMallocHost((void **)&ptr, capacity));
+        int pick = -1;
+        // An idle buffer large enough; else an idle one to grow; else a new one; else the
+        // one queued longest ago, once its copies have run.
+        for (int i = 0; i < count && pick < 0; i++)
+            if (chunks[i].capacity >= bytes && idle(chunks[i])) pick = i;
+        for (int i = 0; i < count && pick < 0; i++)
+            if (idle(chunks[i])) pick = i;
+        if (pick < 0 && count < kChunks) pick = count++;
+        if (pick < 0) {
+            pick = 0;
+            for (int i = 1; i < count; i++)
+                if (chunks[i].queued_at < chunks[pick].queued_at) pick = i;
+            LR_CUDA(cudaEventSynchronize(chunks[pick].done));
         }
-        return ptr;
+        Chunk &c = chunks[pick];
+        if (bytes > c.capacity) {
+            if (c.ptr) LR_CUDA(cudaFreeHost(c.ptr));
+            c.ptr = nullptr;
+            c.capacity = std::max<size_t>(bytes, 1u << 20);
+            LR_CUDA(cudaMallocHost((void **)&c.ptr, c.capacity));
+        }
+        current = pick;
+        return c.ptr;
     }
     void queued(cudaStream_t stream) {
         if (!copied) LR_CUDA(cudaEventCreateWithFlags(&copied, cudaEventDisableTiming));
         LR_CUDA(cudaEventRecord(copied, stream));
+        if (current < 0) return;
+        Chunk &c = chunks[current];
+        if (!c.done) LR_CUDA(cudaEventCreateWithFlags(&c.done, cudaEventDisableTiming));
+        LR_CUDA(cudaEventRecord(c.done, stream));
+        c.queued_at = ++uploads;
+        current = -1;
     }
     void release() {
-        if (copied) cudaEventSynchronize(copied);
-        if (ptr) cudaFreeHost(ptr);
+        for (int i = 0; i < count; i++) {
+            Chunk &c = chunks[i];
+            if (c.done) {
+                cudaEventSynchronize(c.done);
+                cudaEventDestroy(c.done);
+            }
+            if (c.ptr) cudaFreeHost(c.ptr);
+        }
         if (copied) cudaEventDestroy(copied);
         *this = Staging{};
     }

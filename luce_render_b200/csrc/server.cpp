@@ -210,9 +210,16 @@ void finish_request(lr_server *s, Request &r, int status, const std::string &mes
     s->cv_done.notify_all();
 }
 
-// Admits queued sessions while slots and memory allow. Lock held.
+// Host seconds of admitting between two passes: one pass runs meanwhile (about a
+// millisecond or two), so a burst of admissions spreads over the gaps that follow.
+constexpr double kAdmitSeconds = 5e-4;
+
+// Admits queued sessions while slots and memory allow, for about kAdmitSeconds while
+// sessions are live (an idle server admits all it can). Lock held.
 void admit(lr_server *s, std::unique_lock<std::mutex> &lk) {
+    const Clock::time_point start = Clock::now();
     while (!s->render_queue.empty() && s->live.size() < s->cfg.capacity && !s->stopping) {
+        if (!s->live.empty() && std::chrono::duration<double>(Clock::now() - start).count() > kAdmitSeconds) return;
         const uint64_t id = s->render_queue.front();
         Request &r = s->requests[id];
         try {

@@ -5,6 +5,9 @@
 // the octahedral normal encoding of scene.lucb:400-412.
 #include <algorithm>
 #include <array>
+#include <cstring>
+#include <mutex>
+#include <unordered_map>
 
 #include "common.hpp"
 
@@ -92,7 +95,73 @@ V3 cmf_integrals() {
     return sum;
 }
 
+namespace {
+
+// The fit's fixed inputs, computed once: the observer at the fit's samples and its
+// per-channel integrals at 1 nm.
+struct FitTables {
+    std::array<V3, kFitSamples> observer;
+    V3 integrals;
+    M3 to_xyz;
+    FitTables() {
+        for (int at = 0; at < kFitSamples; at++) observer[at] = cmf(kLambdaMin + 5.0 * (double)at);
+        integrals = cmf_integrals();
+        to_xyz = acescg_to_xyz_e();
+    }
+};
+
+const FitTables &fit_tables() {
+    static const FitTables tables;
+    return tables;
+}
+
+void fit_spectrum_uncached(const V3 &rgb, double out[4]);
+
+// Fits by their colour's exact bits: a scene's materials are loaded again for every
+// render of it (a batch member, a server session), and a fit is a few hundred thousand
+// operations; the memo keeps at most kFitMemo of them.
+constexpr size_t kFitMemo = 1u << 18;
+
+struct FitKey {
+    uint64_t bits[3];
+    bool operator==(const FitKey &o) const {
+        return bits[0] == o.bits[0] && bits[1] == o.bits[1] && bits[2] == o.bits[2];
+    }
+};
+struct FitKeyHash {
+    size_t operator()(const FitKey &k) const {
+        uint64_t h = 1469598103934665603ull;
+        for (uint64_t b : k.bits) h = (h ^ b) * 1099511628211ull;
+        return (size_t)h;
+    }
+};
+
+}  // namespace
+
 void fit_spectrum(const V3 &rgb, double out[4]) {
+    static std::mutex lock;
+    static std::unordered_map<FitKey, std::array<double, 4>, FitKeyHash> memo;
+    FitKey key;
+    std::memcpy(&key.bits[0], &rgb.x, 8);
+    std::memcpy(&key.bits[1], &rgb.y, 8);
+    std::memcpy(&key.bits[2], &rgb.z, 8);
+    {
+        std::lock_guard<std::mutex> guard(lock);
+        auto it = memo.find(key);
+        if (it != memo.end()) {
+            for (int k = 0; k < 4; k++) out[k] = it->second[k];
+            return;
+        }
+    }
+    fit_spectrum_uncached(rgb, out);
+    std::lock_guard<std::mutex> guard(lock);
+    if (memo.size() >= kFitMemo) memo.clear();
+    memo.emplace(key, std::array<double, 4>{out[0], out[1], out[2], out[3]});
+}
+
+namespace {
+
+void fit_spectrum_uncached(const V3 &rgb, double out[4]) {
     double largest = std::max(rgb.x, std::max(rgb.y, rgb.z));
     if (largest <= 0.0) {
         out[0] = out[1] = out[2] = out[3] = 0.0;
@@ -103,10 +172,10 @@ void fit_spectrum(const V3 &rgb, double out[4]) {
         out[3] = 2.0 * largest;
         return;
     }
-    V3 target = acescg_to_xyz_e().apply(rgb * (0.5 / largest));
-    V3 integrals = cmf_integrals();
-    std::array<V3, kFitSamples> observer;
-    for (int at = 0; at < kFitSamples; at++) observer[at] = cmf(kLambdaMin + 5.0 * (double)at);
+    const FitTables &tables = fit_tables();
+    const V3 target = tables.to_xyz.apply(rgb * (0.5 / largest));
+    const V3 &integrals = tables.integrals;
+    const std::array<V3, kFitSamples> &observer = tables.observer;
     V3 k;
     for (int iteration = 0; iteration < 40; iteration++) {
         V3 r = fit_xyz(k, integrals, observer) - target;
@@ -126,6 +195,8 @@ void fit_spectrum(const V3 &rgb, double out[4]) {
     out[2] = k.z;
     out[3] = 2.0 * largest;
 }
+
+}  // namespace
 
 V3 blackbody_xyz(double kelvin) {
     V3 integrals = cmf_integrals(), sum;
