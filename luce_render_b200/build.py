@@ -77,7 +77,10 @@ def build(verbose: bool = False) -> Path:
             for src, log in pool.map(lambda j: _compile(*j), jobs):
                 if verbose and log:
                     print(f"--- {src.name}\n{log}", file=sys.stderr)
-    if jobs or not LIBRARY.exists():
+    # Link when anything compiled, or an object is newer than the library (compiled by
+    # another step since the last link).
+    stale = not LIBRARY.exists() or any(o.stat().st_mtime > LIBRARY.stat().st_mtime for o in objects)
+    if jobs or stale:
         tmp = LIBRARY.with_suffix(".so.tmp")
         cmd = [nvcc(), *ARCH, "-shared", "-o", str(tmp), *map(str, objects), "-lpthread"]
         proc = subprocess.run(cmd, capture_output=True, text=True)

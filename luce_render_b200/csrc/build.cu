@@ -4,9 +4,10 @@
 // host compiles without software trees (`compile_scene(trees = false)`, scene.lucb:111-129).
 // B200 has no ray-tracing cores, so the device builds the BVH2 the watertight path walks:
 //   1. the bounds of the triangles' centroids (one reduction launch);
-//   2. a 64-bit key a triangle: its centroid's 30-bit Morton code over those bounds above its
-//      own index, so keys are unique;
-//   3. the keys sorted (a radix sort);
+//   2. a triangle's 30-bit Morton code of its centroid over those bounds;
+//   3. the codes sorted stably with the triangles' indices (a least-significant-digit radix
+//      sort of this file's own, four passes of 8 bits), which leaves the 64-bit keys
+//      code << 32 | index -- unique, in ascending order;
 //   4. the triangles' indices, polygons, shading words, flat flags and source ids gathered
 //      into the sorted (leaf) order, one triangle a leaf;
 //   5. the hierarchy over the sorted keys (Karras, "Maximizing Parallelism in the
@@ -21,8 +22,6 @@
 // do not depend on the tree, so ids and distances equal the brute force bit for bit. The
 // tree is a linear BVH, shallower to build but slower to trace than the host's binned SAH,
 // and has no 4- or 8-wide collapse: every query on it takes the BVH2.
-#include <cub/device/device_radix_sort.cuh>
-
 #include <algorithm>
 #include <cmath>
 #include <memory>
@@ -81,7 +80,7 @@ __device__ __forceinline__ uint32_t spread(uint32_t v) {
 
 // Step 2.
 __global__ void keys_kernel(uint64_t count, const float *positions, const uint32_t *indices, const uint32_t *bounds,
-                            uint64_t *keys) {
+                            uint32_t *codes) {
     float lo[3], scale[3];
     for (int k = 0; k < 3; k++) {
         lo[k] = unordered(bounds[k]);
@@ -93,8 +92,132 @@ __global__ void keys_kernel(uint64_t count, const float *positions, const uint32
         const float v[3] = {c.x, c.y, c.z};
         uint32_t q[3];
         for (int k = 0; k < 3; k++) q[k] = (uint32_t)fminf(fmaxf((v[k] - lo[k]) * scale[k], 0.0f), 1023.0f);
-        const uint32_t code = (spread(q[0]) << 2) | (spread(q[1]) << 1) | spread(q[2]);
-        keys[t] = (uint64_t)code << 32 | t;
+        codes[t] = (spread(q[0]) << 2) | (spread(q[1]) << 1) | spread(q[2]);
+    }
+}
+
+// Step 3: a stable LSD radix sort of the codes with their indices, 8 bits a pass. A pass
+// is three launches over tiles of kSortTile codes (kSortThreads threads, kSortItems codes
+// each): every tile counts its digits (digit_counts_kernel); one block a digit turns that
+// digit's counts over the tiles into exclusive offsets and the digit's total (row_scan_kernel);
+// every tile then ranks its codes within each digit in input order and writes them after
+// the digits below and the tiles before (scatter_kernel). Inside a tile, warp w holds codes
+// w*256 .. w*256+255 with item k of lane l at k*32 + l, so the order (warp, item, lane) is the
+// input order; a warp ranks equal digits of one item with __match_any_sync and keeps a
+// count a digit in shared memory.
+constexpr int kSortThreads = 256, kSortItems = 8, kSortTile = kSortThreads * kSortItems, kRadix = 256;
+
+__global__ void __launch_bounds__(kSortThreads) digit_counts_kernel(uint64_t count, const uint32_t *codes, int shift,
+                                                                    uint32_t *counts) {
+    __shared__ uint32_t hist[kRadix];
+    hist[threadIdx.x] = 0;
+    __syncthreads();
+    const uint64_t base = (uint64_t)blockIdx.x * kSortTile;
+    for (int k = 0; k < kSortItems; k++) {
+        const uint64_t i = base + (uint64_t)k * kSortThreads + threadIdx.x;
+        if (i < count) atomicAdd(&hist[(codes[i] >> shift) & (kRadix - 1)], 1u);
+    }
+    __syncthreads();
+    counts[(size_t)threadIdx.x * gridDim.x + blockIdx.x] = hist[threadIdx.x];
+}
+
+// Exclusive scan of a block's values (one a thread, kSortThreads of them); *total the sum.
+__device__ __forceinline__ uint32_t block_exclusive(uint32_t v, uint32_t *warp_sums, uint32_t &total) {
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    uint32_t x = v;
+    for (int d = 1; d < 32; d <<= 1) {
+        const uint32_t y = __shfl_up_sync(0xffffffffu, x, d);
+        if (lane >= d) x += y;
+    }
+    if (lane == 31) warp_sums[warp] = x;
+    __syncthreads();
+    uint32_t before = 0;
+    total = 0;
+    for (int w = 0; w < kSortThreads / 32; w++) {
+        const uint32_t s = warp_sums[w];
+        if (w < warp) before += s;
+        total += s;
+    }
+    __syncthreads();
+    return before + x - v;
+}
+
+// Digit `blockIdx.x`'s counts over the `tiles` tiles become exclusive offsets; totals[d]
+// the digit's count.
+__global__ void __launch_bounds__(kSortThreads) row_scan_kernel(uint32_t tiles, uint32_t *counts, uint32_t *totals) {
+    __shared__ uint32_t warp_sums[kSortThreads / 32];
+    uint32_t *row = counts + (size_t)blockIdx.x * tiles;
+    uint32_t carry = 0;
+    for (uint32_t at = 0; at < tiles; at += kSortThreads) {
+        const uint32_t i = at + threadIdx.x;
+        const uint32_t v = i < tiles ? row[i] : 0u;
+        uint32_t total;
+        const uint32_t before = block_exclusive(v, warp_sums, total);
+        if (i < tiles) row[i] = carry + before;
+        carry += total;
+    }
+    if (threadIdx.x == 0) totals[blockIdx.x] = carry;
+}
+
+// One pass's scatter. `values` null: the indices are the positions (the first pass). With
+// `keys` the pass writes code << 32 | index there instead of codes and values (the last).
+__global__ void __launch_bounds__(kSortThreads) scatter_kernel(uint64_t count, const uint32_t *codes_in,
+                                                               const uint32_t *values_in, int shift,
+                                                               const uint32_t *counts, const uint32_t *totals,
+                                                               uint32_t *codes_out, uint32_t *values_out,
+                                                               uint64_t *keys) {
+    constexpr int kWarps = kSortThreads / 32;
+    __shared__ uint32_t warp_count[kWarps][kRadix];
+    __shared__ uint32_t tile_base[kRadix];
+    __shared__ uint32_t warp_sums[kWarps];
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    for (int w = 0; w < kWarps; w++) warp_count[w][threadIdx.x] = 0;
+    // The digit's start: the digits below it, then the tiles before this one.
+    uint32_t total;
+    const uint32_t below = block_exclusive(totals[threadIdx.x], warp_sums, total);
+    tile_base[threadIdx.x] = below + counts[(size_t)threadIdx.x * gridDim.x + blockIdx.x];
+    __syncthreads();
+    const uint64_t base = (uint64_t)blockIdx.x * kSortTile + (uint64_t)warp * (32 * kSortItems);
+    const uint32_t lower = (1u << lane) - 1u;
+    uint32_t code[kSortItems], value[kSortItems], rank[kSortItems];
+#pragma unroll
+    for (int k = 0; k < kSortItems; k++) {
+        const uint64_t i = base + (uint64_t)k * 32 + lane;
+        const bool valid = i < count;
+        code[k] = valid ? codes_in[i] : 0u;
+        value[k] = valid ? (values_in ? values_in[i] : (uint32_t)i) : 0u;
+        const uint32_t digit = (code[k] >> shift) & (kRadix - 1);
+        // Lanes past the end get keys of their own, so they match no one.
+        const uint32_t peers = __match_any_sync(0xffffffffu, valid ? digit : kRadix + (uint32_t)lane);
+        const uint32_t seen = warp_count[warp][digit];
+        rank[k] = seen + __popc(peers & lower);
+        __syncwarp();
+        if (valid && lane == __ffs(peers) - 1) warp_count[warp][digit] = seen + __popc(peers);
+        __syncwarp();
+    }
+    __syncthreads();
+    // Each digit's count over the warps before, in place.
+    {
+        uint32_t running = 0;
+        for (int w = 0; w < kWarps; w++) {
+            const uint32_t c = warp_count[w][threadIdx.x];
+            warp_count[w][threadIdx.x] = running;
+            running += c;
+        }
+    }
+    __syncthreads();
+#pragma unroll
+    for (int k = 0; k < kSortItems; k++) {
+        const uint64_t i = base + (uint64_t)k * 32 + lane;
+        if (i >= count) continue;
+        const uint32_t digit = (code[k] >> shift) & (kRadix - 1);
+        const uint64_t at = (uint64_t)tile_base[digit] + warp_count[warp][digit] + rank[k];
+        if (keys) {
+            keys[at] = (uint64_t)code[k] << 32 | value[k];
+        } else {
+            codes_out[at] = code[k];
+            values_out[at] = value[k];
+        }
     }
 }
 
@@ -258,16 +381,16 @@ int lr_gpu_scene_build(lr_context *ctx, const lr_scene *scene, lr_gpu_scene **ou
             *out = gs.release();  // every ray misses: the default root box is inverted and empty is set
             return;
         }
-        // Scratch: the compiled scene's triangles in their own order, two key arrays, the
-        // leaves' parents, the bounds and the depth, and the sort's temporary storage.
-        size_t sort_bytes = 0;
-        LR_CUDA(cub::DeviceRadixSort::SortKeys(nullptr, sort_bytes, (const uint64_t *)nullptr, (uint64_t *)nullptr,
-                                               (int64_t)T, 0, 62, stream));
-        size_t so[10], scratch_total = 0;
-        const size_t ss[10] = {T * 3 * sizeof(uint32_t), T * sizeof(uint32_t), T * sizeof(uint4), T,
-                               T * sizeof(uint32_t), T * sizeof(uint64_t), T * sizeof(uint64_t),
-                               T * sizeof(uint32_t), 8 * sizeof(uint32_t), sort_bytes};
-        for (int i = 0; i < 10; i++) {
+        // Scratch: the compiled scene's triangles in their own order, the sort's two code
+        // and index arrays, its per-tile digit counts and digit totals, the sorted keys,
+        // the leaves' parents, and the bounds and the depth.
+        const uint64_t tiles = (T + kSortTile - 1) / kSortTile;
+        size_t so[12], scratch_total = 0;
+        const size_t ss[12] = {T * 3 * sizeof(uint32_t), T * sizeof(uint32_t), T * sizeof(uint4), T,
+                               T * sizeof(uint32_t), 4 * T * sizeof(uint32_t), tiles * kRadix * sizeof(uint32_t),
+                               T * sizeof(uint64_t), T * sizeof(uint32_t), 8 * sizeof(uint32_t),
+                               kRadix * sizeof(uint32_t), 64};
+        for (int i = 0; i < 12; i++) {
             so[i] = scratch_total;
             scratch_total += align256(std::max<size_t>(ss[i], 64));
         }
@@ -278,8 +401,11 @@ int lr_gpu_scene_build(lr_context *ctx, const lr_scene *scene, lr_gpu_scene **ou
         uint4 *shading_in = (uint4 *)(sb + so[2]);
         uint8_t *flat_in = (uint8_t *)(sb + so[3]);
         uint32_t *ids_in = (uint32_t *)(sb + so[4]);
-        uint64_t *keys = (uint64_t *)(sb + so[5]), *sorted = (uint64_t *)(sb + so[6]);
-        uint32_t *leaf_parents = (uint32_t *)(sb + so[7]), *words = (uint32_t *)(sb + so[8]);
+        uint32_t *codes[2] = {(uint32_t *)(sb + so[5]), (uint32_t *)(sb + so[5]) + T};
+        uint32_t *values[2] = {(uint32_t *)(sb + so[5]) + 2 * T, (uint32_t *)(sb + so[5]) + 3 * T};
+        uint32_t *counts = (uint32_t *)(sb + so[6]), *totals = (uint32_t *)(sb + so[10]);
+        uint64_t *sorted = (uint64_t *)(sb + so[7]);
+        uint32_t *leaf_parents = (uint32_t *)(sb + so[8]), *words = (uint32_t *)(sb + so[9]);
         LR_CUDA(cudaMemcpyAsync(indices_in, scene->indices.data(), T * 3 * sizeof(uint32_t), cudaMemcpyHostToDevice, stream));
         LR_CUDA(cudaMemcpyAsync(faces_in, scene->faces.data(), T * sizeof(uint32_t), cudaMemcpyHostToDevice, stream));
         LR_CUDA(cudaMemcpyAsync(shading_in, scene->shading.data(), T * sizeof(uint4), cudaMemcpyHostToDevice, stream));
@@ -292,11 +418,18 @@ int lr_gpu_scene_build(lr_context *ctx, const lr_scene *scene, lr_gpu_scene **ou
         LR_CUDA(cudaMemsetAsync(leaf_parents, 0, T * sizeof(uint32_t), stream));
         const int sms = ctx->sm_count;
         bounds_kernel<<<grid_of(T, sms), 256, 0, stream>>>(T, positions, indices_in, words);
-        keys_kernel<<<grid_of(T, sms), 256, 0, stream>>>(T, positions, indices_in, words, keys);
+        keys_kernel<<<grid_of(T, sms), 256, 0, stream>>>(T, positions, indices_in, words, codes[0]);
         LR_CUDA(cudaGetLastError());
-        void *sort_temp = sb + so[9];
-        LR_CUDA(cub::DeviceRadixSort::SortKeys(sort_temp, sort_bytes, (const uint64_t *)keys, sorted, (int64_t)T, 0, 62,
-                                               stream));
+        if (tiles > 0xffffffffull) fail(LR_LIMIT, "too many triangles to sort on the device");
+        for (int pass = 0; pass < 4; pass++) {
+            const int in = pass & 1, out = in ^ 1, shift = 8 * pass;
+            digit_counts_kernel<<<(unsigned)tiles, kSortThreads, 0, stream>>>(T, codes[in], shift, counts);
+            row_scan_kernel<<<kRadix, kSortThreads, 0, stream>>>((uint32_t)tiles, counts, totals);
+            scatter_kernel<<<(unsigned)tiles, kSortThreads, 0, stream>>>(
+                T, codes[in], pass == 0 ? nullptr : values[in], shift, counts, totals, codes[out], values[out],
+                pass == 3 ? sorted : nullptr);
+        }
+        LR_CUDA(cudaGetLastError());
         gather_kernel<<<grid_of(T, sms), 256, 0, stream>>>(T, sorted, indices_in, faces_in, shading_in, flat_in, ids_in,
                                                            indices, faces, shading, gs->flat, ids);
         LR_CUDA(cudaGetLastError());
