@@ -24,7 +24,7 @@ namespace {
 // lanes new entries instead (trace_refilling), which keeps more lanes busy on
 // incoherent rays.
 template <int W, int kStack, bool kCount, bool kRefill>
-__global__ void __launch_bounds__(kTraceBlockMax, kTraceMinBlocks) closest_kernel(Wave w, uint32_t round) {
+__device__ __forceinline__ void closest_body(const Wave &w, uint32_t round) {
     extern __shared__ int stack[];  // kInts entries a thread, strided by the block's size
     const uint32_t q = round & 1u;
     const uint32_t cameras = w.counters[round], count = cameras + *light_counter(w, round);
@@ -83,6 +83,20 @@ __global__ void __launch_bounds__(kTraceBlockMax, kTraceMinBlocks) closest_kerne
     }
     if (overflow) atomicAdd(&w.status[0], 1);
     if (kCount) add_visits(&w.stats[4], visits);
+}
+
+template <int W, int kStack, bool kCount, bool kRefill>
+__global__ void __launch_bounds__(kTraceBlockMax, kTraceMinBlocks) closest_kernel(Wave w, uint32_t round) {
+    closest_body<W, kStack, kCount, kRefill>(w, round);
+}
+
+// The BVH2's grid-stride walk, the renderer's default, at 56 registers: nine blocks of 128
+// threads an SM instead of eight, for the latency of its dependent node fetches (8 bytes
+// spilled outside the walk). Measured on the headline pass over several boxes: 1,225-1,237
+// Mrays/s against 1,214-1,225 at 64 registers -- about 1 %, within what boxes differ by.
+template <int kStack>
+__global__ void __maxnreg__(56) closest_bvh2_kernel(Wave w, uint32_t round) {
+    closest_body<2, kStack, false, false>(w, round);
 }
 
 // intersect_shadow.comp:28-92: unblocked light samples join their path's radiance; a light
@@ -225,6 +239,7 @@ void launch_closest(int width, int stack, int block, bool count, bool refill, in
         const size_t bytes = stack_bytes<wd, k>(block);                                             \
         if (count) closest_kernel<wd, k, true, false><<<grid, block, bytes, stream>>>(w, round);    \
         else if (refill) closest_kernel<wd, k, false, true><<<grid, block, bytes, stream>>>(w, round); \
+        else if constexpr (wd == 2) closest_bvh2_kernel<k><<<grid, block, bytes, stream>>>(w, round); \
         else closest_kernel<wd, k, false, false><<<grid, block, bytes, stream>>>(w, round);         \
         return;                                                                                     \
     }
@@ -259,7 +274,8 @@ template <int W, int kStack>
 void allow_stacks(size_t bytes) {
     const int b = (int)bytes;
     const cudaFuncAttribute a = cudaFuncAttributeMaxDynamicSharedMemorySize;
-    LR_CUDA(cudaFuncSetAttribute(closest_kernel<W, kStack, false, false>, a, b));
+    if constexpr (W == 2) LR_CUDA(cudaFuncSetAttribute(closest_bvh2_kernel<kStack>, a, b));
+    else LR_CUDA(cudaFuncSetAttribute(closest_kernel<W, kStack, false, false>, a, b));
     LR_CUDA(cudaFuncSetAttribute(closest_kernel<W, kStack, false, true>, a, b));
     LR_CUDA(cudaFuncSetAttribute(closest_kernel<W, kStack, true, false>, a, b));
     LR_CUDA(cudaFuncSetAttribute(shadow_kernel<W, kStack, false, false, false>, a, b));
@@ -282,6 +298,8 @@ int closest_grid(int width, int stack, int block, bool refill, int sm_count) {
         if (refill)                                                                                           \
             LR_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, closest_kernel<wd, k, false, true>, block, \
                                                                   bytes));                                    \
+        else if constexpr (wd == 2)                                                                           \
+            LR_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, closest_bvh2_kernel<k>, block, bytes)); \
         else                                                                                                  \
             LR_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, closest_kernel<wd, k, false, false>, block, \
                                                                   bytes));                                    \
