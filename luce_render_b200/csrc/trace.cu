@@ -16,13 +16,29 @@
 namespace lr {
 namespace {
 
+// The queue walk of the traversal kernels: each warp takes the next 32 consecutive entries
+// (neighbouring primary rays, or rays a shading warp pushed together, so its lanes walk
+// similar nodes) with one atomic on `next` (zeroed by the pass's camera kernel) whenever
+// all its lanes are done, so warps that drew long rays take fewer batches and no warp
+// waits at the end for a fixed share. `body(j)` handles entry j.
+template <class Body>
+__device__ __forceinline__ void warp_batches(uint32_t count, uint32_t *next, Body body) {
+    const uint32_t lane = threadIdx.x & 31u;
+    for (;;) {
+        uint32_t base = 0;
+        if (lane == 0) base = atomicAdd(next, 32u);
+        base = __shfl_sync(0xffffffffu, base, 0);
+        if (base >= count) break;
+        if (base + lane < count) body(base + lane);
+    }
+}
+
 // intersect_closest.comp:45-76: the nearest triangle, then the analytic lights
 // before it (camera rays skip lights invisible to the camera). Two ways through the queue,
-// chosen by the plan: the grid-stride walk hands each warp 32 neighbouring entries at a
-// time (neighbouring primary rays, or rays a shading warp pushed together), which keeps
-// its lanes on similar nodes; with plan refill_at > 0 persistent warps hand finished
-// lanes new entries instead (trace_refilling), which keeps more lanes busy on
-// incoherent rays.
+// chosen by the plan: warp batches (warp_batches: 32 neighbouring entries a warp at a
+// time), which keep a warp's lanes on similar nodes; with plan refill_at > 0 persistent
+// warps hand finished lanes new entries one by one instead (trace_refilling), which keeps
+// more lanes busy on incoherent rays.
 template <int W, int kStack, bool kCount, bool kRefill>
 __device__ __forceinline__ void closest_body(const Wave &w, uint32_t round) {
     extern __shared__ int stack[];  // kInts entries a thread, strided by the block's size
@@ -69,8 +85,7 @@ __device__ __forceinline__ void closest_body(const Wave &w, uint32_t round) {
         trace_refilling(tr, count, fetch_counter(w, round, false), w.plan->head.refill_at, begin_or_end, end, overflow,
                         visits);
     } else {
-        const uint32_t step = gridDim.x * blockDim.x;
-        for (uint32_t j = blockIdx.x * blockDim.x + threadIdx.x; j < count; j += step) {
+        warp_batches(count, fetch_counter(w, round, false), [&](uint32_t j) {
             {
                 DeviceScene s;
                 if (begin(j, s)) {
@@ -79,7 +94,7 @@ __device__ __forceinline__ void closest_body(const Wave &w, uint32_t round) {
                 }
             }
             end(j);
-        }
+        });
     }
     if (overflow) atomicAdd(&w.status[0], 1);
     if (kCount) add_visits(&w.stats[4], visits);
@@ -201,13 +216,12 @@ __global__ void __launch_bounds__(kTraceBlockMax, kCutouts ? 1 : kTraceMinBlocks
     if (kRefill && !kCutouts) {
         trace_refilling(tr, count, fetch_counter(w, round, true), w.plan->head.refill_at, begin, end, overflow, visits);
     } else {
-        const uint32_t step = gridDim.x * blockDim.x;
-        for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < count; i += step) {
+        warp_batches(count, fetch_counter(w, round, true), [&](uint32_t i) {
             if (kCutouts) {
                 const Member &m = member_of(__float_as_uint(w.shadow_o[i].w));
                 if (m.cutouts) {
                     through_cutouts(i, m);
-                    continue;
+                    return;
                 }
             }
             DeviceScene s;
@@ -216,7 +230,7 @@ __global__ void __launch_bounds__(kTraceBlockMax, kCutouts ? 1 : kTraceMinBlocks
                 }
                 end(i);
             }
-        }
+        });
     }
     if (overflow) atomicAdd(&w.status[0], 1);
     if (kCount) add_visits(&w.stats[6], visits);
