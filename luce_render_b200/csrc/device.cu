@@ -21,6 +21,8 @@ void set_last_error(const char *message) { g_last_error = message; }
 namespace {
 
 constexpr int kBlock = 128;
+// Where the ray queries' batch cursor sits among a context's status words (in ints).
+constexpr int kBatchCursor = 8;
 
 struct ProbeFrame {
     float b[16];
@@ -83,11 +85,12 @@ __global__ void __launch_bounds__(kBlock) trace_kernel(DeviceScene s, const floa
 }
 
 // The watertight path over a ray list: a grid sized to the GPU's resident blocks, each
-// warp taking 32 consecutive rays at a time.
+// warp taking the next 32 consecutive rays (`next`, zeroed before the launch) as it
+// finishes the last.
 template <int W, bool kAny, int kStack, bool kCount>
 __global__ void __launch_bounds__(kBlock) trace_resident_kernel(DeviceScene s, const float4 *__restrict__ rays,
                                                                uint32_t n, float4 *__restrict__ hits, int *status,
-                                                               unsigned long long *counts) {
+                                                               unsigned long long *counts, uint32_t *next) {
     __shared__ int stack[TracerOf<W, kAny, kStack, kCount>::kInts * kBlock];
     bool overflow = false;
     Visits visits;
@@ -98,7 +101,7 @@ __global__ void __launch_bounds__(kBlock) trace_resident_kernel(DeviceScene s, c
     auto store = [&](uint32_t i, const Hit &h, const Ray &) {
         hits[i] = make_float4(h.t, __int_as_float(h.id), h.u, h.v);
     };
-    trace_strided<W, kAny, kStack, kCount>(s, n, stack + threadIdx.x, kBlock, load, store, overflow, visits);
+    trace_batched<W, kAny, kStack, kCount>(s, n, next, stack + threadIdx.x, kBlock, load, store, overflow, visits);
     note_overflow(status, overflow);
     if (kCount) add_visits(counts, visits);
 }
@@ -157,8 +160,10 @@ void launch_resident(const lr_gpu_scene *gs, const float4 *rays, uint64_t n, flo
     }
     const uint64_t needed = (n + kBlock - 1) / kBlock;
     const unsigned grid = (unsigned)std::min<uint64_t>(needed, (uint64_t)resident);
+    uint32_t *next = (uint32_t *)(status + kBatchCursor);
+    LR_CUDA(cudaMemsetAsync(next, 0, sizeof(uint32_t), stream));
     trace_resident_kernel<W, kAny, kStack, kCount><<<grid, kBlock, 0, stream>>>(gs->scene, rays, (uint32_t)n, hits,
-                                                                               status, counts);
+                                                                               status, counts, next);
 }
 
 template <bool kAny, bool kCount>
@@ -345,7 +350,8 @@ int lr_context_create_ex(int device, int priority, lr_context **out) {
         LR_CUDA(cudaStreamCreateWithPriority(&ctx->stream, cudaStreamNonBlocking, priority ? greatest : least));
         LR_CUDA(cudaEventCreate(&ctx->start));
         LR_CUDA(cudaEventCreate(&ctx->stop));
-        // Status words at byte 0, traversal counts at byte 16.
+        // Status words at byte 0, traversal counts at byte 16, the ray queries' batch
+        // cursor at byte 32 (kBatchCursor ints in).
         LR_CUDA(cudaMalloc(&ctx->status, 64));
         LR_CUDA(cudaMemsetAsync(ctx->status, 0, 64, ctx->stream));
         ctx->counts = (unsigned long long *)((char *)ctx->status + 16);

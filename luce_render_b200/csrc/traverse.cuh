@@ -656,17 +656,23 @@ struct TracerOf<2, kAny, kStack, kCount> {
     static constexpr int kInts = kStack;
 };
 
-// A resident grid over a queue of `count` rays: each warp takes 32 consecutive queue
-// entries at a time (neighbouring primary rays, or rays a shading warp pushed together),
-// which keeps its lanes on similar nodes. `load(i)` gives ray i and
-// `store(i, hit, ray)` takes its result. (Refilling lanes individually from the queue as
-// they finish was measured slower here: it breaks that coherence.)
+// A resident grid over a queue of `count` rays in warp batches: each warp takes the next
+// 32 consecutive entries (neighbouring primary rays keep its lanes on similar nodes) with
+// one atomic on `next` (zero at launch) whenever its lanes are done, so warps that drew
+// long rays take fewer batches. `load(i)` gives ray i and `store(i, hit, ray)` takes its
+// result.
 template <int W, bool kAny, int kStack, bool kCount, class Load, class Store>
-__device__ __forceinline__ void trace_strided(const DeviceScene &s, uint32_t count, int *stack_base, int stride,
-                                              Load load, Store store, bool &overflow, Visits &visits) {
+__device__ __forceinline__ void trace_batched(const DeviceScene &s, uint32_t count, uint32_t *next, int *stack_base,
+                                              int stride, Load load, Store store, bool &overflow, Visits &visits) {
     typename TracerOf<W, kAny, kStack, kCount>::type tr(stack_base, stride);
-    const uint32_t step = gridDim.x * blockDim.x;
-    for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < count; i += step) {
+    const uint32_t lane = threadIdx.x & 31u;
+    for (;;) {
+        uint32_t base = 0;
+        if (lane == 0) base = atomicAdd(next, 32u);
+        base = __shfl_sync(0xffffffffu, base, 0);
+        if (base >= count) break;
+        const uint32_t i = base + lane;
+        if (i >= count) continue;
         if (tr.start(s, load(i))) {
             while (!tr.step(s, overflow, visits)) {
             }
