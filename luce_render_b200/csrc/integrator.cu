@@ -178,7 +178,6 @@ template <bool kTracing, bool kGlossy, bool kLight>
 __global__ void __launch_bounds__(kShadeBlock, kGlossy ? 4 : 8) shade_kernel(Wave w, uint32_t round) {
     const uint32_t count = kLight ? *light_counter(w, round) : w.counters[round];
     const uint32_t q = round & 1u, nq = q ^ 1u;
-    const uint32_t stride = gridDim.x * blockDim.x;
     uint32_t *next_counter = kLight ? light_counter(w, round + 1) : &w.counters[round + 1];
     uint32_t *shadow_counter = &w.counters[w.rounds + 1 + round];
     // Outgoing rays are binned by octant in the rounds the plan's interval names (0: never).
@@ -237,8 +236,16 @@ __global__ void __launch_bounds__(kShadeBlock, kGlossy ? 4 : 8) shade_kernel(Wav
         }
     };
     // Every block takes tiles of blockDim.x queue entries (block-uniform, so a block may
-    // sort them, or its outgoing rays, in shared memory).
-    for (uint32_t tile = blockIdx.x * blockDim.x; tile < count; tile += stride) {
+    // sort them, or its outgoing rays, in shared memory), the next one from the round's
+    // cursor when it is done with the last, so blocks that drew slow paths take fewer.
+    __shared__ uint32_t next_tile;
+    uint32_t *cursor = shade_cursor(w, round, kLight);
+    for (;;) {
+        if (threadIdx.x == 0) next_tile = atomicAdd(cursor, blockDim.x);
+        __syncthreads();
+        const uint32_t tile = next_tile;
+        __syncthreads();
+        if (tile >= count) break;
         if constexpr (kGlossy) {
             // Layered surfaces branch by material: each tile is ordered by what its entries
             // shade before its warps take them, so a warp's lanes mostly follow one path

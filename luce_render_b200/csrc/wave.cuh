@@ -137,8 +137,10 @@ struct Wave {
     // (index pool - 1 - k), so that each kind shades in a launch of its own.
     // counters[r]: camera paths' rays of round r; counters[rounds + 1 + r]: shadow rays of
     // round r; counters[kLightCounters * rounds + 2 + r] (light_counter): light paths' rays;
-    // counters[4 * rounds + 2 + 2r] and the one after (fetch_counter): the next closest and
-    // shadow queue entry of round r a refilling warp takes. counter_slots(rounds) in all.
+    // counters[4 * rounds + 2 + 4r] .. + 3: the next closest and shadow queue entry of
+    // round r a traversal warp takes (fetch_counter), and the next entry of the camera and
+    // the light paths' queues a shade block takes (shade_cursor). counter_slots(rounds) in
+    // all, zeroed by each pass's camera kernel.
     uint32_t *counters;
     unsigned long long *stats;  // closest rays, shadow rays, paths, passes, then traversal work
     int *status;
@@ -154,9 +156,14 @@ __device__ __forceinline__ uint32_t *light_counter(const Wave &w, uint32_t round
     return &w.counters[kLightCounters * w.rounds + 2 + round];
 }
 __device__ __forceinline__ uint32_t *fetch_counter(const Wave &w, uint32_t round, bool shadow) {
-    return &w.counters[4 * w.rounds + 2 + 2 * round + (shadow ? 1u : 0u)];
+    return &w.counters[4 * w.rounds + 2 + 4 * round + (shadow ? 1u : 0u)];
 }
-constexpr uint32_t counter_slots(uint32_t rounds) { return 6 * rounds + 4; }
+// The next queue entry a shade kernel's block takes in round `round` (camera paths'
+// queue, or with `light` the light paths').
+__device__ __forceinline__ uint32_t *shade_cursor(const Wave &w, uint32_t round, bool light) {
+    return &w.counters[4 * w.rounds + 2 + 4 * round + (light ? 3u : 2u)];
+}
+constexpr uint32_t counter_slots(uint32_t rounds) { return 8 * rounds + 6; }
 
 __device__ __forceinline__ uint32_t warp_push(uint32_t *counter, bool want) {
     const unsigned mask = __ballot_sync(0xffffffffu, want);
