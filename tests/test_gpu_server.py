@@ -68,6 +68,14 @@ def test_results_same_alone_and_in_the_mix(ctx):
         assert st["evictions"] > 0 and st["uploads"] > len(cs)
         assert st["pixel_samples"] == sum(2 * s.c.width * s.c.height * s.c.samples for _, s in cs)
         assert st["bytes_in_use"] <= budget
+        # The render thread's own account: it queued passes and its host time adds up to
+        # no more than the server's life.
+        assert st["passes"] > 0
+        spent = sum(st[k] for k in ("seconds_advance", "seconds_wait", "seconds_progress", "seconds_admit",
+                                    "seconds_tune"))
+        assert all(st[k] >= 0.0 for k in ("seconds_advance", "seconds_wait", "seconds_progress", "seconds_admit",
+                                          "seconds_tune"))
+        assert 0.0 < spent <= st["seconds"] + 1e-3
     finally:
         server.destroy()
         for sc, _ in cs:
