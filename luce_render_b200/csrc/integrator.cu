@@ -911,6 +911,13 @@ void wave_create(WaveHost *h, lr_context *ctx, uint64_t pool, uint32_t rounds, u
         const int v = std::atoi(env);
         if (v >= 1 && v <= 32) h->refill_at = (uint32_t)v;
     }
+    // LUCE_RENDER_B200_TRACE_BLOCK (64, 128 or 256) sets the traversal kernels' block size
+    // of every size class until a tuner chooses, for measurement.
+    if (const char *env = std::getenv("LUCE_RENDER_B200_TRACE_BLOCK")) {
+        const int v = std::atoi(env);
+        if (v == 64 || v == 128 || v == 256)
+            for (int &b : h->class_block) b = v;
+    }
     LR_CUDA(cudaSetDevice(ctx->device));
     {
         Layout L;
