@@ -534,9 +534,10 @@ int lr_batch_read_landed(lr_batch *batch, uint64_t ticket, int32_t *landed);
  * pool fill (a quarter, half or all of the pool) for the mixed passes, and the fastest
  * interval at which the shade kernels group outgoing rays by direction octant (never,
  * every round, every second round; the queues are compacted every round regardless),
- * and whether the traversal kernels walk their queues grid-stride or as persistent warps
- * that refill idle lanes from the queue (at 32, 16 or 8 idle lanes). Images do not
- * change, only speed. */
+ * whether the traversal kernels walk their queues in warp batches or as persistent warps
+ * that refill idle lanes from the queue (at 32, 16 or 8 idle lanes), and from which round
+ * (2, 3, 4 or never) passes on the BVH2 trace their thin later rounds on the compressed
+ * 8-wide tree. Images do not change, only speed. */
 typedef struct {
     uint32_t width;            /* the widest BVH width chosen for any class */
     uint32_t fill;             /* paths a pass */
@@ -547,7 +548,8 @@ typedef struct {
     uint32_t class_stack[3];   /* traversal stack entries chosen per size class */
     uint32_t class_block[3];   /* traversal kernels' threads a block chosen per size class */
     uint32_t bin_interval;     /* rounds between sorts of outgoing rays by octant (0: none) */
-    uint32_t refill_at;        /* idle lanes at which traversal warps refill (0: grid-stride) */
+    uint32_t refill_at;        /* idle lanes at which traversal warps refill (0: warp batches) */
+    int32_t thin_from;         /* first round of a BVH2 pass on the compressed 8-wide tree (-1: none) */
 } lr_batch_tuning;
 int lr_batch_tune(lr_batch *batch, lr_batch_tuning *out);
 int lr_batch_passes(const lr_batch *batch, uint64_t *recorded, uint64_t *finished);

@@ -240,7 +240,7 @@ class BatchTuning(C.Structure):
     _fields_ = [("width", C.c_uint32), ("fill", C.c_uint32), ("paths_per_ms", C.c_double),
                 ("candidates", C.c_uint32), ("class_width", C.c_uint32 * 3), ("class_members", C.c_uint32 * 3),
                 ("class_stack", C.c_uint32 * 3), ("class_block", C.c_uint32 * 3), ("bin_interval", C.c_uint32),
-                ("refill_at", C.c_uint32)]
+                ("refill_at", C.c_uint32), ("thin_from", C.c_int32)]
 
 
 class ServerSettings(C.Structure):
@@ -1074,7 +1074,7 @@ class Batch:
                 "candidates": int(t.candidates), "class_width": list(t.class_width),
                 "class_members": list(t.class_members), "class_stack": list(t.class_stack),
                 "class_block": list(t.class_block), "bin_interval": int(t.bin_interval),
-                "refill_at": int(t.refill_at)}
+                "refill_at": int(t.refill_at), "thin_from": int(t.thin_from)}
 
     def passes(self):
         rec, fin = C.c_uint64(), C.c_uint64()

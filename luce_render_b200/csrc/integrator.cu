@@ -602,6 +602,16 @@ struct Graph {
     cudaGraphExec_t exec = nullptr;
 };
 
+// The default first round on the compressed 8-wide tree (WaveHost::thin_from).
+constexpr int kThinRound = 3;
+
+// A scene's compressed 8-wide tree as a pass variant's thin code: 1 or 2 for 16 or 32
+// group entries, 0 when it has none (a device-built scene, or one too deep or large).
+int thin_code(const DeviceScene &s) {
+    const TraversalChoice c = choose_traversal(s, 8);
+    return c.width != 8 ? 0 : (c.stack <= 16 ? 1 : 2);
+}
+
 // One of a wave's two lanes: a path pool with its queues, counters and plan, and the
 // stream its passes run on. Consecutive passes take turns on the lanes, so a pass's
 // last, thinly populated rounds run while the next pass's first rounds fill the GPU;
@@ -628,6 +638,13 @@ struct WaveHost {
     void *block = nullptr;  // the member table and stats, shared by the lanes
     Lane lanes[2];
     int lane_count = 2;     // 1 when profiling: kernel times are taken one pass at a time
+    // The first round traced on the compressed 8-wide tree when the pass walks the BVH2 and
+    // its members have one (-1: every round on the BVH2). The first rounds hold most of a
+    // pass's rays and the BVH2 traces them fastest; later rounds hold few, and each is as
+    // long as its slowest rays' chains of dependent node fetches, which the 8-wide tree
+    // shortens (measured: from round 3, 1,313 against 1,284-1,291 Mrays/s on the headline
+    // pass; from round 2 1,294, from round 4 1,298-1,303).
+    int thin_from = kThinRound;
     Member *d_members = nullptr;
     unsigned long long *d_stats = nullptr;
     std::vector<MemberHost> members;
@@ -700,11 +717,15 @@ void mark(cudaStream_t stream, Marks *marks, int kind) {
 // `block` threads: camera, then (closest, shade, shadow) for every round. With `marks`,
 // an event follows each kernel (profiling); `count` takes the counting traversals.
 void record_trace(const WaveHost *h, const Wave &w, int width, int stack, int block, bool count, bool refill,
-                  int grid_trace, bool tracing, bool glossy, bool cutouts, cudaStream_t stream, Marks *marks) {
+                  int grid_trace, bool tracing, bool glossy, bool cutouts, cudaStream_t stream, Marks *marks,
+                  int thin_stack, int thin_grid) {
     camera_kernel<<<h->grid_shade, kShadeBlock, 0, stream>>>(w);
     mark(stream, marks, kCamera);
     for (uint32_t round = 0; round < w.rounds; round++) {
-        launch_closest(width, stack, block, count, refill, grid_trace, stream, w, round);
+        // From round thin_from on (thin queues, latency-bound) the compressed 8-wide tree.
+        const bool thin = thin_stack && (int)round >= h->thin_from;
+        const int rw = thin ? 8 : width, rs = thin ? thin_stack : stack, rg = thin ? thin_grid : grid_trace;
+        launch_closest(rw, rs, block, count, refill, rg, stream, w, round);
         mark(stream, marks, kClosest);
         if (glossy) {
             if (tracing) {
@@ -720,7 +741,7 @@ void record_trace(const WaveHost *h, const Wave &w, int width, int stack, int bl
             shade_kernel<false, false, false><<<h->grid_shade, kShadeBlock, 0, stream>>>(w, round);
         }
         mark(stream, marks, kSurface);
-        launch_shadow(width, stack, block, count, cutouts, refill, grid_trace, stream, w, round);
+        launch_shadow(rw, rs, block, count, cutouts, refill, rg, stream, w, round);
         mark(stream, marks, kShadow);
     }
     LR_CUDA(cudaGetLastError());
@@ -746,10 +767,11 @@ constexpr int kTraceBlocks[3] = {kTraceBlock, 64, 256};
 // A pass's variant: its traversal (BVH width * 1000 + stack entries), plus kTracingVariant
 // when it holds light tracing, kGlossyVariant when it holds glossy materials,
 // kCutoutVariant when it holds cut-outs, kBlockVariant times the index of the traversal
-// kernels' block size in kTraceBlocks, and kRefillVariant when its traversal warps refill
-// idle lanes from the queue.
+// kernels' block size in kTraceBlocks, kRefillVariant when its traversal warps refill
+// idle lanes from the queue, and kThinVariant times 1 or 2 when its later rounds walk the
+// compressed 8-wide tree with 16 or 32 group entries.
 constexpr int kTracingVariant = 100000, kGlossyVariant = 200000, kCutoutVariant = 400000, kBlockVariant = 800000,
-              kRefillVariant = 3 * kBlockVariant;
+              kRefillVariant = 3 * kBlockVariant, kThinVariant = 2 * kRefillVariant;
 
 int variant_block(int variant) { return kTraceBlocks[(variant / kBlockVariant) % 3]; }
 
@@ -776,9 +798,13 @@ void record_trace_any(WaveHost *h, const Wave &w, int variant, cudaStream_t stre
     const int flags = (variant / kTracingVariant) & 7;
     const int traversal = variant % kTracingVariant;
     const int width = traversal / 1000, stack = traversal % 1000, block = variant_block(variant);
-    const bool count = h->profile >= 2, refill = variant >= kRefillVariant && !count;
+    const bool count = h->profile >= 2, refill = ((variant / kRefillVariant) & 1) && !count;
     const int grid = grid_for(h, width, stack, block, refill);
-    record_trace(h, w, width, stack, block, count, refill, grid, flags & 1, flags & 2, flags & 4, stream, marks);
+    const int thin = variant / kThinVariant;  // 0: none; 1, 2: the 8-wide tree with 16, 32 groups
+    const int thin_stack = thin == 1 ? 16 : (thin == 2 ? 32 : 0);
+    const int thin_grid = thin_stack ? grid_for(h, 8, thin_stack, block, refill) : 0;
+    record_trace(h, w, width, stack, block, count, refill, grid, flags & 1, flags & 2, flags & 4, stream, marks,
+                 thin_stack, thin_grid);
 }
 
 // Captures whatever `body` queues on a private stream as a graph.
@@ -910,6 +936,10 @@ void wave_create(WaveHost *h, lr_context *ctx, uint64_t pool, uint32_t rounds, u
     if (const char *env = std::getenv("LUCE_RENDER_B200_REFILL")) {
         const int v = std::atoi(env);
         if (v >= 1 && v <= 32) h->refill_at = (uint32_t)v;
+    }
+    if (const char *env = std::getenv("LUCE_RENDER_B200_THIN")) {
+        const int v = std::atoi(env);
+        if (v >= -1 && v <= 15) h->thin_from = v;
     }
     // LUCE_RENDER_B200_TRACE_BLOCK (64, 128 or 256) sets the traversal kernels' block size
     // of every size class until a tuner chooses, for measurement.
@@ -1538,9 +1568,22 @@ bool launch_pass(WaveHost *h, bool dry = false, int only = -1) {
     if (tuned_stack > stack && traversal_exists(width, tuned_stack)) stack = tuned_stack;
     const int block = h->class_block[dominant] ? h->class_block[dominant] : kTraceBlock;
     const int block_index = block == kTraceBlocks[1] ? 1 : (block == kTraceBlocks[2] ? 2 : 0);
+    // Thin rounds on the compressed 8-wide tree, where every member has one.
+    int thin = 0;
+    if (h->thin_from >= 0 && width == 2) {
+        // The deepest stack any member needs; none when a member has no such tree.
+        for (auto &[m, ended] : rec.members) {
+            const int code = thin_code(h->members[m].dev.scene);
+            if (code == 0) {
+                thin = 0;
+                break;
+            }
+            thin = std::max(thin, code);
+        }
+    }
     const int variant = width * 1000 + stack + (tracing ? kTracingVariant : 0) + (glossy ? kGlossyVariant : 0) +
                         (cutouts ? kCutoutVariant : 0) + block_index * kBlockVariant +
-                        (h->refill_at ? kRefillVariant : 0);
+                        (h->refill_at ? kRefillVariant : 0) + thin * kThinVariant;
     staging->head = PlanHeader{n, used, converts, dry ? 1u : 0u, camera_paths, folds, adapts, h->bin_interval,
                                h->refill_at, {0u, 0u, 0u}};
     staging->display = PlanDisplay{0ull, h->display_scale, h->display_view, 0u, 0u};
@@ -1788,6 +1831,22 @@ void wave_tune(WaveHost *h, lr_batch_tuning *out) {
         h->refill_at = kept;
     }
     h->refill_at = best_refill;
+    // Where passes that walk the BVH2 switch to the compressed 8-wide tree for their thin
+    // later rounds: from round 2, 3 or 4, or never.
+    int best_thin = h->thin_from;
+    for (int from : {-1, 2, 3, 4}) {
+        if (from == h->thin_from) continue;
+        const int kept = h->thin_from;
+        h->thin_from = from;
+        const double rate = time_dry(h, -1, a, b);
+        tried++;
+        if (rate > best) {
+            best = rate;
+            best_thin = from;
+        }
+        h->thin_from = kept;
+    }
+    h->thin_from = best_thin;
     cudaEventDestroy(a);
     cudaEventDestroy(b);
     if (out) {
@@ -1796,6 +1855,7 @@ void wave_tune(WaveHost *h, lr_batch_tuning *out) {
         out->candidates = tried;
         out->bin_interval = best_interval;
         out->refill_at = best_refill;
+        out->thin_from = best_thin;
         int widest = 0;
         for (int cls = 0; cls < kSizeClasses; cls++) widest = std::max(widest, h->class_width[cls]);
         out->width = (uint32_t)(widest ? widest : 2);
@@ -2121,7 +2181,8 @@ void create(lr_context *ctx, const lr_scene *scene, const lr_settings &settings,
                             c.width * 1000 + c.stack + (r->wave.members[0].dev.light_paths ? kTracingVariant : 0) +
                                 (r->wave.members[0].dev.glossy ? kGlossyVariant : 0) +
                                 (r->wave.members[0].dev.cutouts ? kCutoutVariant : 0) +
-                                (r->wave.refill_at ? kRefillVariant : 0));
+                                (r->wave.refill_at ? kRefillVariant : 0) +
+                                (r->wave.thin_from >= 0 && c.width == 2 ? thin_code(gs->scene) * kThinVariant : 0));
     } catch (...) {
         const bool owned = !r->wave.members.empty() && r->wave.members[0].used;
         wave_destroy(&r->wave);

@@ -126,6 +126,22 @@ def test_refilling_warps_equal_grid_stride(ctx, cases, refill, monkeypatch):
         b.destroy()
 
 
+@pytest.mark.parametrize("thin", [-1, 1, 3])
+def test_thin_rounds_on_the_wide_tree_equal(ctx, cases, thin, monkeypatch):
+    # Passes that trace their rounds from `thin` on over the compressed 8-wide tree (-1:
+    # none) make the images the BVH2 alone makes: the closest hit does not depend on the tree.
+    cs, uploads, alone = cases
+    monkeypatch.setenv("LUCE_RENDER_B200_THIN", str(thin))
+    b = lr.Batch(ctx, lr.BatchSettings.default(pool=1500, max_bounces=12, capacity=16))
+    try:
+        members = [b.add(gs, sc, s) for gs, (sc, s) in zip(uploads, cs)]
+        b.finish()
+        for m, want in zip(members, alone):
+            assert np.array_equal(_bits(b.read(m)), _bits(want)), m
+    finally:
+        b.destroy()
+
+
 def test_ticketed_reads_land_the_images(ctx, cases):
     # Reads queued with tickets while the other members' passes still run land the same
     # images a waiting read gives; each ticket lands, and later tickets land after earlier.
@@ -174,7 +190,7 @@ def test_tuning_changes_speed_not_images(ctx, cases):
             b.advance()
         t = b.tune()
         assert t["width"] in (2, 4, 8) and t["fill"] in (512, 1024, 2048)
-        assert t["refill_at"] in (0, 32, 16, 8) and t["bin_interval"] in (0, 1, 2)
+        assert t["refill_at"] in (0, 32, 16, 8) and t["bin_interval"] in (0, 1, 2) and t["thin_from"] in (-1, 2, 3, 4)
         assert t["candidates"] >= 4 and t["paths_per_ms"] > 0
         # The cases hold scenes under 16k triangles and one of about 20k.
         assert t["class_members"][0] >= 1 and t["class_members"][1] == 1 and t["class_members"][2] == 0
