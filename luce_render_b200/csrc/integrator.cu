@@ -1568,9 +1568,10 @@ bool launch_pass(WaveHost *h, bool dry = false, int only = -1) {
     if (tuned_stack > stack && traversal_exists(width, tuned_stack)) stack = tuned_stack;
     const int block = h->class_block[dominant] ? h->class_block[dominant] : kTraceBlock;
     const int block_index = block == kTraceBlocks[1] ? 1 : (block == kTraceBlocks[2] ? 2 : 0);
-    // Thin rounds on the compressed 8-wide tree, where every member has one.
+    // Thin rounds on the compressed 8-wide tree, where every member has one -- except in
+    // counting passes (settings.profile 2), whose visits and tests are the BVH2's work.
     int thin = 0;
-    if (h->thin_from >= 0 && width == 2) {
+    if (h->thin_from >= 0 && width == 2 && h->profile < 2) {
         // The deepest stack any member needs; none when a member has no such tree.
         for (auto &[m, ended] : rec.members) {
             const int code = thin_code(h->members[m].dev.scene);
@@ -2182,7 +2183,9 @@ void create(lr_context *ctx, const lr_scene *scene, const lr_settings &settings,
                                 (r->wave.members[0].dev.glossy ? kGlossyVariant : 0) +
                                 (r->wave.members[0].dev.cutouts ? kCutoutVariant : 0) +
                                 (r->wave.refill_at ? kRefillVariant : 0) +
-                                (r->wave.thin_from >= 0 && c.width == 2 ? thin_code(gs->scene) * kThinVariant : 0));
+                                (r->wave.thin_from >= 0 && c.width == 2 && r->wave.profile < 2
+                                     ? thin_code(gs->scene) * kThinVariant
+                                     : 0));
     } catch (...) {
         const bool owned = !r->wave.members.empty() && r->wave.members[0].used;
         wave_destroy(&r->wave);
