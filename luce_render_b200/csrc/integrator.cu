@@ -645,6 +645,10 @@ struct WaveHost {
     // shortens (measured: from round 3, 1,313 against 1,284-1,291 Mrays/s on the headline
     // pass; from round 2 1,294, from round 4 1,298-1,303).
     int thin_from = kThinRound;
+    // Whether thin rounds switch for any mix of members (the tuner measured it on the mix)
+    // or only when every member is a large scene (the default: measured faster there, and
+    // slower for small scenes such as the Cornell box).
+    bool thin_any = false;
     Member *d_members = nullptr;
     unsigned long long *d_stats = nullptr;
     std::vector<MemberHost> members;
@@ -937,9 +941,14 @@ void wave_create(WaveHost *h, lr_context *ctx, uint64_t pool, uint32_t rounds, u
         const int v = std::atoi(env);
         if (v >= 1 && v <= 32) h->refill_at = (uint32_t)v;
     }
+    // LUCE_RENDER_B200_THIN (-1 to 15) sets the first thin round on the 8-wide tree, for any
+    // mix of members, for measurement.
     if (const char *env = std::getenv("LUCE_RENDER_B200_THIN")) {
         const int v = std::atoi(env);
-        if (v >= -1 && v <= 15) h->thin_from = v;
+        if (v >= -1 && v <= 15) {
+            h->thin_from = v;
+            h->thin_any = true;
+        }
     }
     // LUCE_RENDER_B200_TRACE_BLOCK (64, 128 or 256) sets the traversal kernels' block size
     // of every size class until a tuner chooses, for measurement.
@@ -1571,7 +1580,10 @@ bool launch_pass(WaveHost *h, bool dry = false, int only = -1) {
     // Thin rounds on the compressed 8-wide tree, where every member has one -- except in
     // counting passes (settings.profile 2), whose visits and tests are the BVH2's work.
     int thin = 0;
-    if (h->thin_from >= 0 && width == 2 && h->profile < 2) {
+    const bool all_large = std::all_of(rec.members.begin(), rec.members.end(), [&](const std::pair<uint32_t, bool> &e) {
+        return size_class(h->members[e.first].dev.scene.triangle_count) == kSizeClasses - 1;
+    });
+    if (h->thin_from >= 0 && width == 2 && h->profile < 2 && (h->thin_any || all_large)) {
         // The deepest stack any member needs; none when a member has no such tree.
         for (auto &[m, ended] : rec.members) {
             const int code = thin_code(h->members[m].dev.scene);
@@ -1834,20 +1846,21 @@ void wave_tune(WaveHost *h, lr_batch_tuning *out) {
     h->refill_at = best_refill;
     // Where passes that walk the BVH2 switch to the compressed 8-wide tree for their thin
     // later rounds: from round 2, 3 or 4, or never.
-    int best_thin = h->thin_from;
+    // Every candidate timed on this mix (the choice then holds for any mix of members).
+    h->thin_any = true;
+    int best_thin = -1;
+    double best_thin_rate = -1.0;
     for (int from : {-1, 2, 3, 4}) {
-        if (from == h->thin_from) continue;
-        const int kept = h->thin_from;
         h->thin_from = from;
         const double rate = time_dry(h, -1, a, b);
         tried++;
-        if (rate > best) {
-            best = rate;
+        if (rate > best_thin_rate) {
+            best_thin_rate = rate;
             best_thin = from;
         }
-        h->thin_from = kept;
     }
     h->thin_from = best_thin;
+    best = std::max(best, best_thin_rate);
     cudaEventDestroy(a);
     cudaEventDestroy(b);
     if (out) {
@@ -2183,7 +2196,8 @@ void create(lr_context *ctx, const lr_scene *scene, const lr_settings &settings,
                                 (r->wave.members[0].dev.glossy ? kGlossyVariant : 0) +
                                 (r->wave.members[0].dev.cutouts ? kCutoutVariant : 0) +
                                 (r->wave.refill_at ? kRefillVariant : 0) +
-                                (r->wave.thin_from >= 0 && c.width == 2 && r->wave.profile < 2
+                                (r->wave.thin_from >= 0 && c.width == 2 && r->wave.profile < 2 &&
+                                         size_class(gs->scene.triangle_count) == kSizeClasses - 1
                                      ? thin_code(gs->scene) * kThinVariant
                                      : 0));
     } catch (...) {
