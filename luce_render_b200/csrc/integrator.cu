@@ -950,6 +950,12 @@ void wave_create(WaveHost *h, lr_context *ctx, uint64_t pool, uint32_t rounds, u
             h->thin_any = true;
         }
     }
+    // LUCE_RENDER_B200_BIN (0, 1 or 2) sets the rounds between octant sorts of outgoing rays
+    // until a tuner chooses, for measurement.
+    if (const char *env = std::getenv("LUCE_RENDER_B200_BIN")) {
+        const int v = std::atoi(env);
+        if (v >= 0 && v <= 2) h->bin_interval = (uint32_t)v;
+    }
     // LUCE_RENDER_B200_TRACE_BLOCK (64, 128 or 256) sets the traversal kernels' block size
     // of every size class until a tuner chooses, for measurement.
     if (const char *env = std::getenv("LUCE_RENDER_B200_TRACE_BLOCK")) {
