@@ -175,7 +175,7 @@ __device__ __forceinline__ uint32_t tile_order(const Wave &w, uint32_t q, uint32
 // in one launch, their two large bodies fought over the instruction cache (the glossy box
 // with light tracing: 4.2 -> 1.8 ms of shading a 512^2 sample).
 template <bool kTracing, bool kGlossy, bool kLight>
-__global__ void __launch_bounds__(kShadeBlock, kGlossy ? 4 : 8) shade_kernel(Wave w, uint32_t round) {
+__global__ void __launch_bounds__(kShadeBlock, (kGlossy ? 512 : 1024) / kShadeBlock) shade_kernel(Wave w, uint32_t round) {
     const uint32_t count = kLight ? *light_counter(w, round) : w.counters[round];
     const uint32_t q = round & 1u, nq = q ^ 1u;
     uint32_t *next_counter = kLight ? light_counter(w, round + 1) : &w.counters[round + 1];
