@@ -830,8 +830,9 @@ def main():
 
     # End to end through the public API: each step one pass and its image read back into
     # pinned host memory (the pass takes no new input: the scene stays resident). The reads
-    # are Renderer.read_async into two host buffers in turn, each copy running beside the
-    # next pass; the timed region ends when the last copy has landed.
+    # are Renderer.read_ticket into two host buffers in turn, each copy running beside the
+    # next pass; before a buffer is used again its last copy has landed (read_landed), and
+    # the timed region ends when the last copy has landed.
     e2e_r = lr.Renderer.create(ctx, sc, settings_for(lr, W + K, spectral, profile=0))
     hosts = [lr.PinnedArray((HEIGHT, WIDTH, 4), np.float32) for _ in range(2)]
     for step in range(W):
@@ -841,11 +842,12 @@ def main():
     e0 = e2e_r.stats()
     dist.barrier()
     start = time.perf_counter()
+    tickets = [0, 0]
     for step in range(K):
         e2e_r.advance_one()
-        if step >= 2:
-            e2e_r.read_wait()  # the buffer this read reuses is free again
-        e2e_r.read_async(hosts[step % 2].array)
+        while tickets[step % 2] and not e2e_r.read_landed(tickets[step % 2]):
+            time.sleep(2e-5)  # the copy that last filled this buffer
+        tickets[step % 2] = e2e_r.read_ticket(hosts[step % 2].array)
     e2e_r.read_wait()
     e2e_s = time.perf_counter() - start
     e1 = e2e_r.stats()

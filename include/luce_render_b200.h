@@ -386,6 +386,12 @@ int lr_renderer_read(lr_renderer *renderer, float *rgba, uint64_t float_count);
  * later never change a copy in flight. */
 int lr_renderer_read_async(lr_renderer *renderer, float *rgba, uint64_t count);
 int lr_renderer_read_wait(lr_renderer *renderer);
+/* As lr_renderer_read_async, and *ticket names the copy; lr_renderer_read_landed sets
+ * *landed to 1 once the copy with `ticket` (and every copy queued before it) has arrived,
+ * else 0, without waiting -- so a caller that cycles through a few buffers waits for the
+ * copy that last filled the buffer it reuses, not for the newest. */
+int lr_renderer_read_ticket(lr_renderer *renderer, float *rgba, uint64_t count, uint64_t *ticket);
+int lr_renderer_read_landed(lr_renderer *renderer, uint64_t ticket, int32_t *landed);
 /* Orders the context's stream after every pass queued so far, without waiting: work
  * the caller queues there afterwards (reading the device image, an event for timing)
  * sees their results. Passes run on two streams, taking turns; see lr_renderer_advance. */

@@ -337,6 +337,8 @@ _SIGNATURES = {
     "lr_renderer_set_display": (C.c_int, [_vp, C.c_double, C.c_int]),
     "lr_renderer_converged_pixels": (C.c_int, [_vp, C.POINTER(C.c_uint64)]),
     "lr_renderer_read_wait": (C.c_int, [_vp]),
+    "lr_renderer_read_ticket": (C.c_int, [_vp, C.POINTER(C.c_float), _u64, C.POINTER(C.c_uint64)]),
+    "lr_renderer_read_landed": (C.c_int, [_vp, _u64, C.POINTER(C.c_int32)]),
     "lr_batch_read_async": (C.c_int, [_vp, _u32, C.POINTER(C.c_float), _u64]),
     "lr_batch_read_wait": (C.c_int, [_vp]),
     "lr_batch_read_ticket": (C.c_int, [_vp, _u32, C.POINTER(C.c_float), _u64, C.POINTER(C.c_uint64)]),
@@ -906,6 +908,20 @@ class Renderer:
     def read_wait(self) -> None:
         """Waits for every copy read_async queued."""
         _check(lib.lr_renderer_read_wait(self.handle))
+
+    def read_ticket(self, out: np.ndarray) -> int:
+        """read_async, returning a ticket for read_landed."""
+        if out.dtype != np.float32 or out.size != self.width * self.height * 4 or not out.flags.c_contiguous:
+            raise RenderError(INVALID, "reading the image needs four floats a pixel")
+        t = C.c_uint64()
+        _check(lib.lr_renderer_read_ticket(self.handle, _fptr(out), out.size, C.byref(t)))
+        return int(t.value)
+
+    def read_landed(self, ticket: int) -> bool:
+        """Whether the copy with `ticket` (and every one before it) has arrived; never waits."""
+        v = C.c_int32()
+        _check(lib.lr_renderer_read_landed(self.handle, ticket, C.byref(v)))
+        return bool(v.value)
 
     def restart(self, frame: Frame) -> None:
         """Renderer.restart (integrator.lucb:463): start over through `frame`."""

@@ -2467,6 +2467,20 @@ int lr_renderer_read_wait(lr_renderer *r) {
     });
 }
 
+int lr_renderer_read_ticket(lr_renderer *r, float *rgba, uint64_t count, uint64_t *ticket) {
+    return guarded([&] {
+        if (!r || !rgba || !ticket) fail(LR_INVALID, "no renderer");
+        *ticket = member_read_ticket(&r->wave, 0, rgba, count);
+    });
+}
+
+int lr_renderer_read_landed(lr_renderer *r, uint64_t ticket, int32_t *landed) {
+    return guarded([&] {
+        if (!r || !landed) fail(LR_INVALID, "no renderer");
+        *landed = member_read_landed(&r->wave, ticket) ? 1 : 0;
+    });
+}
+
 int lr_renderer_join(lr_renderer *r) {
     return guarded([&] {
         if (!r) fail(LR_INVALID, "no renderer");

@@ -225,6 +225,43 @@ def test_renderer_read_async_is_the_image_of_its_pass(ctx):
         h.close()
 
 
+def test_renderer_read_tickets_land_in_order(ctx):
+    # Ticketed reads into two buffers in turn, each reused once its last copy has landed:
+    # every copy holds its pass's image, and a ticket lands no earlier than those before it.
+    sc = lr.compile_scene(scenes.cornell_meshes(True), [scenes.cornell_camera()], [scenes.cornell_light()],
+                          scenes.cornell_materials())
+    s = lr.RenderSettings.of(96, 64, 4)
+    s.max_bounces = 4
+    s.light_tracing = 0.0
+    s.c.material = lr.OpenPbr.lambert()
+    hosts = [lr.PinnedArray((64, 96, 4), np.float32) for _ in range(2)]
+    r = lr.Renderer.create(ctx, sc, s)
+    tickets, seen, last = [0, 0], [], 0
+    for step in range(4):
+        r.advance_one()
+        if tickets[step % 2]:
+            for _ in range(1000000):
+                if r.read_landed(tickets[step % 2]):
+                    break
+            assert r.read_landed(tickets[step % 2])
+            seen.append((step - 2, hosts[step % 2].array.copy()))
+        tickets[step % 2] = r.read_ticket(hosts[step % 2].array)
+        assert tickets[step % 2] > last
+        last = tickets[step % 2]
+    r.read_wait()
+    assert r.read_landed(tickets[0]) and r.read_landed(tickets[1])
+    seen += [(2, hosts[0].array.copy()), (3, hosts[1].array.copy())]
+    r.destroy()
+    for step, got in seen:
+        s.samples = step + 1
+        want = lr.Renderer.create(ctx, sc, s)
+        want.finish()
+        assert np.array_equal(got, want.read()), step
+        want.destroy()
+    for h in hosts:
+        h.close()
+
+
 def test_adaptive_sampling(ctx):
     # tests/gpu/integrator.lucb:334-358: a sphere under an area light, half the frame empty
     # sky: with adaptive sampling the image is the same within 1 % (it stops sampling only
