@@ -163,9 +163,10 @@ __device__ __forceinline__ uint32_t tile_order(const Wave &w, uint32_t q, uint32
     return mine;
 }
 
-// 8 blocks an SM (64 registers): shade_one wants 128, which leaves 16 warps an SM to hide
-// its memory latency; capped, it spills a little and runs 17 % faster (1.21 -> 1.01 ms a
-// 1080p pass on the 1M-triangle scene; 48 registers: 0.99 ms with twice the spills).
+// 1,024 threads an SM (64 registers): the diffuse camera-path shading wants 128, which
+// leaves 16 warps an SM to hide its memory latency; capped, it spills a little and runs
+// 17 % faster (1.21 -> 1.01 ms a 1080p pass on the 1M-triangle scene; 48 registers: 0.99 ms
+// with twice the spills).
 // kTracing: the pass holds light paths or camera paths that weigh against them; passes
 // without take the kernel without that code (it cost camera-only passes 16 %). kGlossy:
 // the pass holds a member with glossy materials, whose entries take the layered OpenPBR

@@ -59,7 +59,7 @@ struct Member {
     unsigned long long *splat;
     unsigned long long *splat_lane[2];
     // A material of the member's has a specular, metal, coat or transmission lobe: its
-    // surfaces take the layered OpenPBR shading (openpbr.cuh).
+    // surfaces take the layered OpenPBR shading (surface.cuh, paths.cuh).
     uint32_t glossy;
     // A material of the member's is a cut-out (geometry_opacity below 1), and the rounds
     // its passes trace: its bounces + 1, + 8 for rays passing through cut-outs at the same
