@@ -240,6 +240,26 @@ def test_bvh_widths_agree_bit_for_bit(ctx, incoherent, cornell):
                 assert nodes < base_nodes, (w, nodes, base_nodes)
 
 
+@pytest.mark.parametrize("leaf", [4, 16])
+def test_wide_trees_with_whole_subtree_leaves_agree(ctx, incoherent, leaf, monkeypatch):
+    # Wide trees that take BVH2 subtrees of up to `leaf` triangles whole as leaves (one
+    # contiguous range of the leaf order each) reach the same triangles: closest and any
+    # hits equal the BVH2 path's bit for bit.
+    sc, a, _ = incoherent
+    monkeypatch.setenv("LUCE_RENDER_B200_WIDE_LEAF", str(leaf))
+    gs = lr.GpuScene.upload(ctx, sc)
+    try:
+        rays = scenes.incoherent_rays(1 << 17, seed=21)
+        base = lr.trace_rays(ctx, gs, rays, width=2)
+        base_any = lr.trace_rays(ctx, gs, rays, width=2, any_hit=True)
+        for w in (4, 8):
+            assert np.array_equal(_as_bits(lr.trace_rays(ctx, gs, rays, width=w)), _as_bits(base)), w
+            anyh = lr.trace_rays(ctx, gs, rays, width=w, any_hit=True)
+            assert np.array_equal(lr.hit_ids(anyh) >= 0, lr.hit_ids(base_any) >= 0), w
+    finally:
+        gs.destroy()
+
+
 def test_million_triangles_properties_at_full_size(ctx, incoherent):
     # 2^21 incoherent rays: any-hit agrees with the existence of a closest hit, and
     # every closest hit re-tested alone (the oracle's watertight test on that one
